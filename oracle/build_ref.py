@@ -1,0 +1,155 @@
+"""Recipe: compile the HARM-COOL reference's own C sources into CPU checker
+libraries under oracle/_ref/<config>/ (TEST INFRASTRUCTURE ONLY).
+
+The reference fixes its grid size and physics switches at compile time in
+decs.h (decs.h:59-61, 110, 114, 117) and its torus parameters as literals in
+init.c (init.c:104-110).  For each configuration this recipe writes patched
+copies of those two files into oracle/_ref/<config>/gen/ and compiles every
+other source file where it lies in the reference tree.  The `-I-` option
+makes `#include "decs.h"` resolve to the patched copy instead of the file
+next to the including source.
+
+Switches: COOL_EOS 0 (the Fortran table generator needs gfortran, absent
+here), TRACERSDUMP 0, HDFDUMP 0 (no HDF5).  MPI_USED is on and the
+single-rank stand-in in oracle/fakempi provides MPI: with one rank the phi
+periodicity and opposite-phi polar ghosts are MPI self-exchanges
+(step_ch.c:189-198, bounds.c:161-275).  Floating point: SSE2, -O2 (the
+reference Makefile's level, Makefile:19), -ffp-contract=off; the Makefile's
+-mfpmath=387 (x87, Makefile:29) is dropped so results are reproducible.
+
+The patch also sizes the four opposite-phi slice tables N3+2 instead of N3:
+the reference indexes them with h in [1, N3] (mpi.c:337-422, bounds.c:194-230),
+one past their end, which overwrites neighbouring globals.
+
+Outputs per config: libharmref.so (reference objects + oracle/refdrv.cpp)
+and refbench (CPU timing binary).  Nothing is written outside oracle/_ref/.
+"""
+import os
+import re
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SRC = "/root/reference/src"
+OUT = os.path.join(HERE, "_ref")
+
+# name -> (N1, N2, N3, spin a, torus rin, torus rmax, beta)
+CONFIGS = {
+    # config 1 of the benchmark: 2D 128x128 Fishbone-Moncrief torus
+    "c1": (128, 128, 1, 0.9375, 6.0, 12.0, 100.0),
+    # small grids for fixtures and fast checks
+    "t2d": (32, 32, 1, 0.9375, 6.0, 12.0, 100.0),
+    "t3d": (16, 16, 4, 0.9375, 6.0, 12.0, 100.0),
+    "m3d": (32, 32, 8, 0.9375, 6.0, 12.0, 100.0),
+    # bounded CPU sample of the 288x256x256 workload: same r-theta grid, 4 phi planes
+    "c2s": (288, 256, 4, 0.9375, 6.0, 12.0, 100.0),
+}
+
+SOURCES = ["bounds", "coord", "diag", "dump", "fixup", "image", "interp", "main",
+           "metric", "lu", "phys", "ranc", "restart", "step_ch", "u2p_util",
+           "utoprim_1dfix1", "utoprim_1dvsq2fix1", "utoprim_2d", "random",
+           "utoprim_5d", "mpi"]
+
+
+def _sub1(pattern, repl, text, what):
+    new, n = re.subn(pattern, repl, text, count=1, flags=re.M)
+    if n != 1:
+        raise RuntimeError("patch failed: " + what)
+    return new
+
+
+def patch_decs(text, n1, n2, n3):
+    text = _sub1(r"^#define N1\s+\(\d+\)", "#define N1       (%d)" % n1, text, "N1")
+    text = _sub1(r"^#define N2\s+\(\d+\)", "#define N2       (%d)" % n2, text, "N2")
+    text = _sub1(r"^#define N3\s+\(\d+\)", "#define N3       (%d)" % n3, text, "N3")
+    text = _sub1(r"^#define COOL_EOS\s+\(1\)", "#define COOL_EOS  (0)", text, "COOL_EOS")
+    text = _sub1(r"^#define TRACERSDUMP \(1\)", "#define TRACERSDUMP (0)", text, "TRACERSDUMP")
+    text = _sub1(r"^#define HDFDUMP \(1\)", "#define HDFDUMP (0)", text, "HDFDUMP")
+    # the opposite-phi slice tables are indexed by h in [1, N3] (mpi.c:337-422)
+    # but declared with N3 entries: size them N3+2 so no neighbour is clobbered
+    text, n = re.subn(r"(slice_hopNPR2_m2|slice_hopNPR2_n1|slice_h_rankop|slice_h_hop)\[N3\]",
+                      r"\g<1>[N3+2]", text)
+    if n != 4:
+        raise RuntimeError("patch failed: slice tables")
+    return text
+
+
+def patch_defs(text):
+    text, n = re.subn(r"(slice_hopNPR2_m2|slice_hopNPR2_n1|slice_h_rankop|slice_h_hop)\[N3\]",
+                      r"\g<1>[N3+2]", text)
+    if n != 4:
+        raise RuntimeError("patch failed: defs.h slice tables")
+    return text
+
+
+def patch_init(text, a, rin, rmax, beta):
+    text = _sub1(r"^(\s*)a = 0\.6;", r"\g<1>a = %r;" % a, text, "a")
+    text = _sub1(r"^(\s*)rin = 4\.0;", r"\g<1>rin = %r;" % rin, text, "rin")
+    text = _sub1(r"^(\s*)rmax = 11\.8;", r"\g<1>rmax = %r;" % rmax, text, "rmax")
+    text = _sub1(r"^(\s*)beta = 50\.0 ;", r"\g<1>beta = %r ;" % beta, text, "beta")
+    return text
+
+
+def run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError("compile failed")
+
+
+def build_config(name, force=False):
+    n1, n2, n3, a, rin, rmax, beta = CONFIGS[name]
+    cdir = os.path.join(OUT, name)
+    gen = os.path.join(cdir, "gen")
+    obj = os.path.join(cdir, "obj")
+    lib = os.path.join(cdir, "libharmref.so")
+    exe = os.path.join(cdir, "refbench")
+    if not force and os.path.exists(lib) and os.path.exists(exe):
+        return lib
+    os.makedirs(gen, exist_ok=True)
+    os.makedirs(obj, exist_ok=True)
+    with open(os.path.join(REF_SRC, "decs.h")) as f:
+        decs = patch_decs(f.read(), n1, n2, n3)
+    with open(os.path.join(gen, "decs.h"), "w") as f:
+        f.write(decs)
+    with open(os.path.join(REF_SRC, "defs.h")) as f:
+        defs = patch_defs(f.read())
+    with open(os.path.join(gen, "defs.h"), "w") as f:
+        f.write(defs)
+    with open(os.path.join(REF_SRC, "init.c")) as f:
+        init = patch_init(f.read(), a, rin, rmax, beta)
+    with open(os.path.join(gen, "init.c"), "w") as f:
+        f.write(init)
+    flags = ["g++", "-O2", "-ffp-contract=off", "-fPIC", "-w", "-DMPI_USED",
+             "-Dmain=harm_reference_main", "-I" + gen, "-I-",
+             "-I" + os.path.join(HERE, "fakempi"), "-I" + REF_SRC]
+    objs = []
+    for s in SOURCES:
+        o = os.path.join(obj, s + ".o")
+        run(flags + ["-x", "c++", "-c", os.path.join(REF_SRC, s + ".c"), "-o", o])
+        objs.append(o)
+    o = os.path.join(obj, "init.o")
+    run(flags + ["-x", "c++", "-c", os.path.join(gen, "init.c"), "-o", o])
+    objs.append(o)
+    o = os.path.join(obj, "refdrv.o")
+    run(flags + ["-c", os.path.join(HERE, "refdrv.cpp"), "-o", o])
+    objs.append(o)
+    o = os.path.join(obj, "fakempi.o")
+    run(["gcc", "-O2", "-fPIC", "-c", os.path.join(HERE, "fakempi", "fakempi.c"), "-o", o])
+    objs.append(o)
+    run(["g++", "-shared", "-o", lib] + objs + ["-lm"])
+    run(["g++", "-O2", "-o", exe, os.path.join(HERE, "refbench.cpp"), lib,
+         "-Wl,-rpath,$ORIGIN", "-lm"])
+    return lib
+
+
+def build_all(force=False):
+    if not os.path.isdir(REF_SRC):
+        return []
+    return [build_config(n, force) for n in CONFIGS]
+
+
+if __name__ == "__main__":
+    names = sys.argv[1:] or list(CONFIGS)
+    for n in names:
+        print(build_config(n, force=True))
