@@ -1,0 +1,193 @@
+"""ctypes bindings for the CPU oracle and for the reference checker build.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, never by the product package.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+NPR, NPG = 8, 5
+
+
+class OraParams(ctypes.Structure):
+    _fields_ = [("n1", ctypes.c_int), ("n2", ctypes.c_int), ("n3", ctypes.c_int),
+                ("lim", ctypes.c_int), ("a", ctypes.c_double), ("gam", ctypes.c_double),
+                ("cour", ctypes.c_double), ("defcon", ctypes.c_double), ("tf", ctypes.c_double),
+                ("dx", ctypes.c_double * 4), ("startx", ctypes.c_double * 4)]
+
+
+class OraDiag(ctypes.Structure):
+    _fields_ = [("mdot", ctypes.c_double), ("edot", ctypes.c_double), ("ldot", ctypes.c_double),
+                ("mdot_in", ctypes.c_double), ("mdot_out", ctypes.c_double),
+                ("mass_curr", ctypes.c_double), ("mass_in", ctypes.c_double),
+                ("mass_out", ctypes.c_double), ("ndt", ctypes.c_double),
+                ("fail_code", ctypes.c_int), ("fail_h", ctypes.c_int), ("fail_i", ctypes.c_int),
+                ("fail_j", ctypes.c_int)]
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+_oracle_lib = None
+
+
+def oracle_lib():
+    global _oracle_lib
+    if _oracle_lib is None:
+        path = os.path.join(HERE, "_build", "libharm_oracle.so")
+        if not os.path.exists(path):
+            from . import build_oracle  # noqa: F401  (package import when available)
+        lib = ctypes.CDLL(path)
+        lib.ora_create.restype = ctypes.c_void_p
+        lib.ora_create.argtypes = [ctypes.POINTER(OraParams)] + [ctypes.POINTER(ctypes.c_double)] * 6
+        for name in ("ora_p", "ora_ph"):
+            getattr(lib, name).restype = ctypes.POINTER(ctypes.c_double)
+            getattr(lib, name).argtypes = [ctypes.c_void_p]
+        lib.ora_flux.restype = ctypes.POINTER(ctypes.c_double)
+        lib.ora_flux.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.ora_pflag.restype = ctypes.POINTER(ctypes.c_byte)
+        lib.ora_pflag.argtypes = [ctypes.c_void_p]
+        lib.ora_destroy.argtypes = [ctypes.c_void_p]
+        lib.ora_step_ch.argtypes = [ctypes.c_void_p]
+        lib.ora_set_time.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        lib.ora_get_time.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(ctypes.c_double)]
+        lib.ora_set_mass.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        lib.ora_get_diag.argtypes = [ctypes.c_void_p, ctypes.POINTER(OraDiag)]
+        for name in ("ora_fixup", "ora_bound_prim", "ora_fixup_utoprim"):
+            getattr(lib, name).argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib.ora_utoprim_2d.argtypes = [ctypes.c_double, dp, dp, dp, ctypes.c_double, dp]
+        lib.ora_utoprim_1dvsq2fix1.argtypes = [ctypes.c_double, dp, dp, dp, ctypes.c_double, dp,
+                                               ctypes.c_double]
+        lib.ora_utoprim_1dfix1.argtypes = [ctypes.c_double, dp, dp, dp, ctypes.c_double, dp,
+                                           ctypes.c_double]
+        lib.ora_face_flux.argtypes = [ctypes.c_double, ctypes.c_int, dp, dp, dp, dp,
+                                      ctypes.c_double, dp, dp]
+        _oracle_lib = lib
+    return _oracle_lib
+
+
+def make_params(n1, n2, n3, a, gam, cour, dx, startx, defcon=1.0, tf=20000.0, lim=0):
+    p = OraParams()
+    p.n1, p.n2, p.n3, p.lim = n1, n2, n3, lim
+    p.a, p.gam, p.cour, p.defcon, p.tf = a, gam, cour, defcon, tf
+    for k in range(4):
+        p.dx[k] = dx[k]
+        p.startx[k] = startx[k]
+    return p
+
+
+def shape3(n1, n2, n3):
+    return (n3 + 2 if n3 > 1 else 1, n1 + 4, n2 + 4)
+
+
+class Oracle:
+    """One oracle state: prims, fluxes and flags in the reference layout."""
+
+    def __init__(self, params, geom):
+        self.lib = oracle_lib()
+        self.params = params
+        self.geom = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in geom.items()}
+        g = self.geom
+        self.h = self.lib.ora_create(ctypes.byref(params), _dp(g["gcov"]), _dp(g["gcon"]),
+                                     _dp(g["gdet"]), _dp(g["conn"]), _dp(g["coords"]),
+                                     _dp(g["katm"]))
+        if not self.h:
+            raise ValueError("oracle rejected the grid size")
+        s3 = shape3(params.n1, params.n2, params.n3)
+        n = s3[0] * s3[1] * s3[2]
+        self.p = np.ctypeslib.as_array(self.lib.ora_p(self.h), shape=(n * NPR,)).reshape(s3 + (NPR,))
+        self.ph = np.ctypeslib.as_array(self.lib.ora_ph(self.h), shape=(n * NPR,)).reshape(s3 + (NPR,))
+        self.pflag = np.ctypeslib.as_array(self.lib.ora_pflag(self.h), shape=(n,)).reshape(s3)
+
+    def flux(self, d):
+        s3 = self.p.shape
+        n = s3[0] * s3[1] * s3[2] * NPR
+        return np.ctypeslib.as_array(self.lib.ora_flux(self.h, d), shape=(n,)).reshape(s3)
+
+    def set_time(self, t, dt):
+        self.lib.ora_set_time(self.h, t, dt)
+
+    def time(self):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        self.lib.ora_get_time(self.h, ctypes.byref(t), ctypes.byref(dt))
+        return t.value, dt.value
+
+    def set_mass(self, mass_in, mass_out):
+        self.lib.ora_set_mass(self.h, mass_in, mass_out)
+
+    def diag(self):
+        d = OraDiag()
+        self.lib.ora_get_diag(self.h, ctypes.byref(d))
+        return {f: getattr(d, f) for f, _ in OraDiag._fields_}
+
+    def step(self):
+        return self.lib.ora_step_ch(self.h)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                self.lib.ora_destroy(self.h)
+        except Exception:
+            pass
+
+
+class Reference:
+    """The reference's own step_ch() (oracle/_ref/<config>/libharmref.so).
+
+    One configuration per process: the reference keeps its state in globals."""
+
+    def __init__(self, config):
+        path = os.path.join(HERE, "_ref", config, "libharmref.so")
+        self.lib = lib = ctypes.CDLL(path)
+        lib.ref_get.restype = ctypes.c_double
+        lib.ref_get.argtypes = [ctypes.c_char_p]
+        lib.ref_set.argtypes = [ctypes.c_char_p, ctypes.c_double]
+        lib.ref_ptr.restype = ctypes.c_void_p
+        lib.ref_ptr.argtypes = [ctypes.c_char_p]
+        lib.ref_utoprim_2d.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_double)]
+        lib.ref_time_steps.restype = ctypes.c_double
+        lib.ref_init()
+        d = (ctypes.c_int * 16)()
+        lib.ref_dims(d)
+        self.n1, self.n2, self.n3, self.sn1, self.sn2, self.sn3 = d[0], d[1], d[2], d[3], d[4], d[5]
+        s3 = (self.sn3, self.sn1, self.sn2)
+        self.p = self._arr("p", s3 + (NPR,))
+        self.ph = self._arr("ph", s3 + (NPR,))
+        self.pflag = np.ctypeslib.as_array(
+            ctypes.cast(lib.ref_ptr(b"pflag"), ctypes.POINTER(ctypes.c_byte)), shape=s3)
+
+    def _arr(self, name, shape, dtype=ctypes.c_double):
+        ptr = ctypes.cast(self.lib.ref_ptr(name.encode()), ctypes.POINTER(dtype))
+        return np.ctypeslib.as_array(ptr, shape=shape)
+
+    def get(self, name):
+        return self.lib.ref_get(name.encode())
+
+    def set(self, name, value):
+        return self.lib.ref_set(name.encode(), float(value))
+
+    def geometry(self):
+        g2 = (self.sn1, self.sn2)
+        return {"gcov": self._arr("gcov", g2 + (NPG, 4, 4)).copy(),
+                "gcon": self._arr("gcon", g2 + (NPG, 4, 4)).copy(),
+                "gdet": self._arr("gdet", g2 + (NPG,)).copy(),
+                "conn": self._arr("conn", g2 + (4, 4, 4)).copy(),
+                "coords": self._arr("coords", g2 + (4,)).copy(),
+                "katm": self._arr("Katm", (self.sn1,)).copy()}
+
+    def params(self):
+        g = self.get
+        return make_params(self.n1, self.n2, self.n3, g("a"), g("gam"), g("cour"),
+                           [0.0, g("dx1"), g("dx2"), g("dx3")],
+                           [0.0, g("startx1"), g("startx2"), g("startx3")],
+                           defcon=g("defcon"), tf=g("tf"), lim=int(g("lim")))
+
+    def step(self):
+        self.lib.ref_step()
