@@ -1,0 +1,241 @@
+#!/usr/bin/env python
+"""Throughput of the HARM-COOL step_ch() path on B200, in zone-cycles/s.
+
+One step = one full predictor + corrector update of every active zone of the
+288x256x256 (r, theta, phi) Fishbone-Moncrief torus (a=0.9375, rin=6,
+rmax=12, beta=100, gamma-law 4/3, FP64), state resident on the GPU.  The
+torus comes from the library's own init (seeded, synthetic: no dataset).
+The state (6 GB of FP64 planes) is far larger than the 126 MB L2, so no
+flush is needed between steps.
+
+--impl ours       the CUDA path (default)
+--impl reference  the reference's own step_ch(), compiled from its C sources
+                  (oracle/_ref/c2s: the same r-theta grid with 4 phi planes),
+                  one process per host core, timed on the host
+
+With --gpus N (torchrun) every rank advances its own torus (replicas: the
+reference's MPI slab split is replaced by one domain per GPU, so there is no
+data-path collective); the timed region is bracketed by barriers and the
+slowest rank's device time is reported.
+"""
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+KERNELS_PER_STEP = 15  # predictor 6 + corrector 7 + mass diagnostics + finalize
+STATE_BYTES_PER_ZONE_CYCLE = 320  # p read twice, ph written and read, p written; 8 FP64 prims
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def reduce_max(x, world, local):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda:%d" % local)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits", "-lms", "100"],
+                                     stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        self.proc.wait()
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = max(smax, float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.strip() == "Active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def reference_cpu_rate(seconds_per_core=20.0, cores=None, min_steps=1):
+    """The reference's step_ch() on the 288x256x4 sample, one process per core.
+
+    Returns (zone-cycles/s summed over processes, cores used, sample text)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "c2s", "refbench")
+    if not os.path.exists(exe):
+        raise RuntimeError("reference checker build oracle/_ref/c2s is missing")
+    cores = cores or os.cpu_count() or 1
+    # one step of 288x256x4 is about 1 s per core; size the run to the time budget
+    steps = max(min_steps, int(seconds_per_core))
+    procs = [subprocess.Popen([exe, "1", str(steps)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                              cwd=os.path.dirname(exe)) for _ in range(cores)]
+    rates = []
+    for p in procs:
+        out, _ = p.communicate()
+        rates.append(json.loads(out.decode().strip().splitlines()[-1])["zone_cycles_per_s"])
+    sample = ("reference step_ch() on 288x256x4 (same r-theta grid, 4 phi planes), "
+              "%d step(s) after 1 warm-up, %d process(es)" % (steps, cores))
+    return sum(rates), cores, sample
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    rate, cores, sample = reference_cpu_rate(seconds_per_core=max(2.0, min(20.0, 4.0 * args.steps)))
+    line = {"metric": "zone-cycles/s 288x256x256 GRMHD step_ch (FP64)", "value": rate,
+            "unit": "zone-cycles/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * args.n1 * args.n2 * args.n3 / rate, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "FM torus %dx%dx%d, gamma-law, FP64, sampled as 288x256x4 slabs"
+                                   % (args.n1, args.n2, args.n3)},
+            "cpu_baseline": {"value": rate, "unit": "zone-cycles/s", "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": rate, "unit": "zone-cycles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import harm_cool_b200 as hc
+    pr = hc.torus_problem(args.n1, args.n2, args.n3)
+    ctx = hc.Context(pr, device=local)
+    ctx.init_torus()
+    zones = pr.zones
+    ctx.run(args.warmup)
+    sampler = ClockSampler(local)
+    barrier(world)
+    sampler.start()
+    ms = ctx.run_timed(args.steps)
+    clocks = sampler.stop()
+    barrier(world)
+    ms = reduce_max(ms, world, local)
+    value = zones * args.steps * world / (ms / 1e3)
+    d = ctx.diag()
+    # end to end through the host-array call: upload p, step, download p every step
+    import torch
+    pinned = torch.empty(pr.shape + (8,), dtype=torch.float64, pin_memory=True).numpy()
+    pinned[...] = ctx.get_prims()
+    ms_e2e = ctx.step_ch_host_timed(pinned, args.e2e_steps)
+    ms_e2e = reduce_max(ms_e2e, world, local)
+    e2e = zones * args.e2e_steps * world / (ms_e2e / 1e3)
+    bytes_host = int(np.prod(pr.shape)) * 8 * 8
+    # dominant kernel, timed alone on the context's stream
+    kms = ctx.time_kernels(reps=3)
+    dom = max(("flux", "update"), key=lambda k: kms[k])
+    peak, peak_kind = measured_peaks()
+    alg = {"flux": 64, "update": 192}[dom]  # FP64 state bytes per zone this kernel must move
+    achieved = zones * alg / (kms[dom] / 1e3) / 1e9
+    line = {"metric": "zone-cycles/s 288x256x256 GRMHD step_ch (FP64)", "value": value,
+            "unit": "zone-cycles/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "FM torus %dx%dx%d (a=0.9375, rin=6, rmax=12, beta=100), gamma-law, FP64"
+                                   % (args.n1, args.n2, args.n3),
+                       "parallelism": "replicas" if world > 1 else "single", "l2": "state > L2, no flush"},
+            "e2e": {"value": e2e, "unit": "zone-cycles/s", "h2d_bytes_per_step": bytes_host,
+                    "d2h_bytes_per_step": bytes_host, "path": "harm_step_ch_host (upload, step, download)"},
+            "gpu_launches": KERNELS_PER_STEP * args.steps,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": peak_kind,
+                         "step_frac": zones * STATE_BYTES_PER_ZONE_CYCLE / (ms / args.steps / 1e3) / 1e9 / peak},
+            "kernel_ms": kms, "clocks": clocks, "sim_time": ctx.time(), "fail_code": d["fail_code"]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, sample = reference_cpu_rate(seconds_per_core=10.0, cores=1)
+        line["cpu_baseline"] = {"value": rate, "unit": "zone-cycles/s", "cores": cores, "kind": "reference",
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n1", type=int, default=288)
+    ap.add_argument("--n2", type=int, default=256)
+    ap.add_argument("--n3", type=int, default=256)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        # host-only: rank 0 times the reference, the other ranks have nothing to do
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
+    world, rank, local = dist_setup()
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

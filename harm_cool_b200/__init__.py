@@ -1,0 +1,336 @@
+"""harm_cool_b200: HARM-COOL's per-zone GRMHD update (the step_ch() path) on B200.
+
+The Python layer is a thin host-side mirror of the reference's calling
+surface -- step_ch(), bound_prim(), fixup(), fixup_utoprim(), Utoprim_2d()
+(decs.h:548-608) -- over the C ABI in include/harm_b200.h.  All compute runs
+in libharm_b200.so's sm_100a kernels; there is no CPU path: without the
+library or without a B200 every compute call raises.
+
+Arrays use the reference's layouts: primitives p[SN3][SN1][SN2][8] float64,
+pflag int8 [SN3][SN1][SN2], geometry as set_grid() builds it.
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+
+__all__ = ["HarmError", "Params", "GridSpec", "TorusSpec", "Diag", "Problem", "Context",
+           "torus_problem", "set_points", "set_grid", "set_katm", "utoprim_2d_batch", "library",
+           "NPR", "NPG"]
+
+NPR, NPG = 8, 5
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libharm_b200.so")
+
+
+class HarmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("harm_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    """harm_params: run parameters (decs.h:263-283, init.c:104-125)."""
+    _fields_ = [("n1", ctypes.c_int), ("n2", ctypes.c_int), ("n3", ctypes.c_int), ("lim", ctypes.c_int),
+                ("a", ctypes.c_double), ("gam", ctypes.c_double), ("cour", ctypes.c_double),
+                ("defcon", ctypes.c_double), ("tf", ctypes.c_double),
+                ("dx", ctypes.c_double * 4), ("startx", ctypes.c_double * 4)]
+
+
+class GridSpec(ctypes.Structure):
+    """harm_grid_spec: modified Kerr-Schild grid (coord.c:61-81, 202-262)."""
+    _fields_ = [("n1", ctypes.c_int), ("n2", ctypes.c_int), ("n3", ctypes.c_int),
+                ("a", ctypes.c_double), ("Rin", ctypes.c_double), ("Rout", ctypes.c_double),
+                ("R0", ctypes.c_double), ("hslope", ctypes.c_double)]
+
+
+class TorusSpec(ctypes.Structure):
+    """harm_torus_spec: Fishbone-Moncrief torus (init.c:70-160)."""
+    _fields_ = [("rin", ctypes.c_double), ("rmax", ctypes.c_double), ("kappa", ctypes.c_double),
+                ("beta", ctypes.c_double)]
+
+
+class Diag(ctypes.Structure):
+    """harm_diag: per-step diagnostics (diag.c:437-580) and the first failure."""
+    _fields_ = [("mdot", ctypes.c_double), ("edot", ctypes.c_double), ("ldot", ctypes.c_double),
+                ("mdot_in", ctypes.c_double), ("mdot_out", ctypes.c_double),
+                ("mass_curr", ctypes.c_double), ("mass_in", ctypes.c_double),
+                ("mass_out", ctypes.c_double), ("ndt", ctypes.c_double),
+                ("fail_code", ctypes.c_int), ("fail_h", ctypes.c_int), ("fail_i", ctypes.c_int),
+                ("fail_j", ctypes.c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+_DP = ctypes.POINTER(ctypes.c_double)
+_BP = ctypes.POINTER(ctypes.c_byte)
+_lib = None
+
+# every symbol include/harm_b200.h declares, with its ctypes signature
+_SIGNATURES = {
+    "harm_last_error": (ctypes.c_char_p, []),
+    "harm_set_points": (ctypes.c_int, [ctypes.POINTER(GridSpec), _DP, _DP]),
+    "harm_set_grid": (ctypes.c_int, [ctypes.POINTER(GridSpec), _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
+    "harm_set_katm": (ctypes.c_int, [ctypes.POINTER(GridSpec), ctypes.c_double, _DP, _DP]),
+    "harm_create": (ctypes.c_int, [ctypes.POINTER(Params), _DP, _DP, _DP, _DP, _DP, _DP, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_void_p)]),
+    "harm_destroy": (None, [ctypes.c_void_p]),
+    "harm_init_torus": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GridSpec), ctypes.POINTER(TorusSpec)]),
+    "harm_put_prims": (ctypes.c_int, [ctypes.c_void_p, _DP, _BP]),
+    "harm_get_prims": (ctypes.c_int, [ctypes.c_void_p, _DP, _BP]),
+    "harm_set_time": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]),
+    "harm_get_time": (ctypes.c_int, [ctypes.c_void_p, _DP, _DP]),
+    "harm_set_mass": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]),
+    "harm_get_diag": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Diag)]),
+    "harm_step_ch": (ctypes.c_int, [ctypes.c_void_p]),
+    "harm_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "harm_step_ch_host": (ctypes.c_int, [ctypes.c_void_p, _DP]),
+    "harm_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "harm_run_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _DP]),
+    "harm_step_ch_host_timed": (ctypes.c_int, [ctypes.c_void_p, _DP, ctypes.c_int, _DP]),
+    "harm_time_kernels": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _DP]),
+    "harm_fixup": (ctypes.c_int, [ctypes.c_void_p, _DP]),
+    "harm_bound_prim": (ctypes.c_int, [ctypes.c_void_p, _DP]),
+    "harm_fixup_utoprim": (ctypes.c_int, [ctypes.c_void_p, _DP]),
+    "harm_utoprim_2d_batch": (ctypes.c_int, [_DP, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int),
+                                             ctypes.c_long, ctypes.c_double]),
+}
+
+
+def library():
+    """Load libharm_b200.so (built in-tree by harm_cool_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise HarmError(-3, "libharm_b200.so is not built; run harm_cool_b200.build.build()")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise HarmError(rc, library().harm_last_error().decode())
+    return rc
+
+
+def _dp(a):
+    return a.ctypes.data_as(_DP)
+
+
+def _shape3(n1, n2, n3):
+    return (n3 + 2 if n3 > 1 else 1, n1 + 4, n2 + 4)
+
+
+# ---------------------------------------------------------------------------
+# host-side grid set-up (no GPU needed)
+
+def set_points(gs):
+    dx = (ctypes.c_double * 4)()
+    sx = (ctypes.c_double * 4)()
+    _check(library().harm_set_points(ctypes.byref(gs), dx, sx))
+    return list(dx), list(sx)
+
+
+def set_grid(gs, dx, sx):
+    """Geometry of the 2D (r, theta) grid, reference layout (main.c:413-520)."""
+    sn1, sn2 = gs.n1 + 4, gs.n2 + 4
+    g = {"gcov": np.zeros((sn1, sn2, NPG, 4, 4)), "gcon": np.zeros((sn1, sn2, NPG, 4, 4)),
+         "gdet": np.zeros((sn1, sn2, NPG)), "conn": np.zeros((sn1, sn2, 4, 4, 4)),
+         "coords": np.zeros((sn1, sn2, 4))}
+    cdx = (ctypes.c_double * 4)(*dx)
+    csx = (ctypes.c_double * 4)(*sx)
+    _check(library().harm_set_grid(ctypes.byref(gs), cdx, csx, _dp(g["gcov"]), _dp(g["gcon"]),
+                                   _dp(g["gdet"]), _dp(g["conn"]), _dp(g["coords"])))
+    return g
+
+
+def set_katm(gs, gam, coords):
+    katm = np.zeros(gs.n1 + 4)
+    _check(library().harm_set_katm(ctypes.byref(gs), gam, _dp(np.ascontiguousarray(coords)), _dp(katm)))
+    return katm
+
+
+class Problem:
+    """Everything init() fixes before the first step: parameters, grid, torus, geometry."""
+
+    def __init__(self, params, grid, torus, geometry):
+        self.params, self.grid, self.torus, self.geometry = params, grid, torus, geometry
+
+    @property
+    def shape(self):
+        return _shape3(self.params.n1, self.params.n2, self.params.n3)
+
+    @property
+    def zones(self):
+        return self.params.n1 * self.params.n2 * self.params.n3
+
+
+def torus_problem(n1, n2, n3, a=0.9375, rin=6.0, rmax=12.0, beta=100.0, kappa=1.e-3, gam=4. / 3.,
+                  cour=0.9, hslope=0.3, Rout=100.0, R0=0.0, tf=20000.0, lim=0):
+    """The reference's torus set-up (init.c:70-160) for a given grid and torus.
+
+    Defaults are the benchmark torus: a=0.9375, rin=6, rmax=12, beta=100,
+    kappa=1e-3, gamma=4/3, hslope=0.3, Rout=100, inner radius 0.98 r_horizon."""
+    Rin = 0.98 * (1. + math.sqrt(1. - a * a))
+    gs = GridSpec(n1, n2, n3, a, Rin, Rout, R0, hslope)
+    dx, sx = set_points(gs)
+    geom = set_grid(gs, dx, sx)
+    geom["katm"] = set_katm(gs, gam, geom["coords"])
+    p = Params()
+    p.n1, p.n2, p.n3, p.lim = n1, n2, n3, lim
+    p.a, p.gam, p.cour, p.defcon, p.tf = a, gam, cour, 1.0, tf
+    for k in range(4):
+        p.dx[k] = dx[k]
+        p.startx[k] = sx[k]
+    return Problem(p, gs, TorusSpec(rin, rmax, kappa, beta), geom)
+
+
+def utoprim_2d_batch(U, gcov, gcon, gdet, prim, gam):
+    """Utoprim_2d() (utoprim_2d.c:126) on the device for n independent zones.
+
+    prim holds the guess on entry and the result on exit; returns the
+    reference's return codes."""
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    gcov = np.ascontiguousarray(gcov, dtype=np.float64)
+    gcon = np.ascontiguousarray(gcon, dtype=np.float64)
+    gdet = np.ascontiguousarray(gdet, dtype=np.float64)
+    assert prim.flags["C_CONTIGUOUS"] and prim.dtype == np.float64
+    n = U.shape[0]
+    ret = np.zeros(n, dtype=np.int32)
+    _check(library().harm_utoprim_2d_batch(_dp(U), _dp(gcov), _dp(gcon), _dp(gdet), _dp(prim),
+                                           ret.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n, gam))
+    return ret
+
+
+# ---------------------------------------------------------------------------
+# device context
+
+class Context:
+    """One grid's state resident on one GPU, driven like the reference's globals."""
+
+    def __init__(self, problem, device=0):
+        self.problem = problem
+        self.lib = library()
+        g = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in problem.geometry.items()}
+        self._geom = g
+        h = ctypes.c_void_p()
+        _check(self.lib.harm_create(ctypes.byref(problem.params), _dp(g["gcov"]), _dp(g["gcon"]),
+                                    _dp(g["gdet"]), _dp(g["conn"]), _dp(g["coords"]), _dp(g["katm"]),
+                                    device, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.harm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        return self.problem.shape
+
+    def init_torus(self):
+        """init() (init.c:70-472): the torus, resident on the device; t=0, dt=1e-5."""
+        pr = self.problem
+        _check(self.lib.harm_init_torus(self.h, ctypes.byref(pr.grid), ctypes.byref(pr.torus)))
+
+    def put_prims(self, p, pflag=None):
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        assert p.shape == self.shape + (NPR,)
+        fl = None
+        if pflag is not None:
+            pflag = np.ascontiguousarray(pflag, dtype=np.int8)
+            fl = pflag.ctypes.data_as(_BP)
+        _check(self.lib.harm_put_prims(self.h, _dp(p), fl))
+
+    def get_prims(self, with_flags=False):
+        p = np.empty(self.shape + (NPR,))
+        fl = np.empty(self.shape, dtype=np.int8) if with_flags else None
+        _check(self.lib.harm_get_prims(self.h, _dp(p), fl.ctypes.data_as(_BP) if with_flags else None))
+        return (p, fl) if with_flags else p
+
+    def set_time(self, t, dt):
+        _check(self.lib.harm_set_time(self.h, t, dt))
+
+    def time(self):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        _check(self.lib.harm_get_time(self.h, ctypes.byref(t), ctypes.byref(dt)))
+        return t.value, dt.value
+
+    def set_mass(self, mass_in, mass_out):
+        _check(self.lib.harm_set_mass(self.h, mass_in, mass_out))
+
+    def diag(self):
+        d = Diag()
+        _check(self.lib.harm_get_diag(self.h, ctypes.byref(d)))
+        return d.as_dict()
+
+    def step_ch(self):
+        """One full step (step_ch.c:90-140), asynchronous; see sync()."""
+        _check(self.lib.harm_step_ch(self.h))
+
+    def run(self, nsteps):
+        """nsteps steps replayed from one captured CUDA graph; synchronises."""
+        _check(self.lib.harm_run(self.h, nsteps))
+
+    def run_timed(self, nsteps):
+        """run() with the device time of the nsteps graph launches, in ms."""
+        ms = ctypes.c_double()
+        _check(self.lib.harm_run_timed(self.h, nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    def step_ch_host_timed(self, p, nsteps):
+        """nsteps of step_ch_host() (upload, step, download each) timed on the device, in ms."""
+        assert p.flags["C_CONTIGUOUS"] and p.dtype == np.float64 and p.shape == self.shape + (NPR,)
+        ms = ctypes.c_double()
+        _check(self.lib.harm_step_ch_host_timed(self.h, _dp(p), nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    KERNELS = ("flux", "update", "bound_prim", "fixup_utoprim", "diag_mass")
+
+    def time_kernels(self, reps=5):
+        """Average device ms per launch of each step kernel, launched on its own."""
+        ms = (ctypes.c_double * len(self.KERNELS))()
+        _check(self.lib.harm_time_kernels(self.h, reps, ms))
+        return dict(zip(self.KERNELS, list(ms)))
+
+    def sync(self):
+        _check(self.lib.harm_sync(self.h))
+
+    def step_ch_host(self, p):
+        """step_ch() on a host primitive array, in place (upload, step, download)."""
+        assert p.flags["C_CONTIGUOUS"] and p.dtype == np.float64 and p.shape == self.shape + (NPR,)
+        _check(self.lib.harm_step_ch_host(self.h, _dp(p)))
+
+    def _on_array(self, fn, pv):
+        assert pv.flags["C_CONTIGUOUS"] and pv.dtype == np.float64 and pv.shape == self.shape + (NPR,)
+        _check(fn(self.h, _dp(pv)))
+        return pv
+
+    def fixup(self, pv):
+        """fixup() (fixup.c:51-60) on a host array, in place."""
+        return self._on_array(self.lib.harm_fixup, pv)
+
+    def bound_prim(self, pv):
+        """bound_prim() (bounds.c:54-331) on a host array, in place."""
+        return self._on_array(self.lib.harm_bound_prim, pv)
+
+    def fixup_utoprim(self, pv, pflag=None):
+        """fixup_utoprim() (fixup.c:432-538) on a host array, in place; pflag, if
+        given, replaces the device's failure flags first."""
+        if pflag is not None:
+            cur = self.get_prims()
+            self.put_prims(cur, pflag)
+        return self._on_array(self.lib.harm_fixup_utoprim, pv)

@@ -1,0 +1,57 @@
+"""Build libharm_b200.so in-tree for sm_100a.
+
+The CUDA translation unit is compiled with -fmad=false: every multiply and
+add stays a separate IEEE operation, as in the reference's SSE2 build, which
+is what lets the FP64 path reproduce the reference bit for bit.  The host
+set-up code is compiled by g++ with the reference's own -O2 and
+-ffp-contract=off so that its libm calls and arithmetic match set_grid().
+"""
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libharm_b200.so")
+BUILD = os.path.join(HERE, "_build")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _sources():
+    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))] + [
+        os.path.join(ROOT, "include", "harm_b200.h")]
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    return r.stdout + r.stderr
+
+
+def build(force=False, verbose=False):
+    """Compile the library if any source is newer than it; return its path."""
+    if (not force and os.path.exists(LIB)
+            and os.path.getmtime(LIB) >= max(os.path.getmtime(s) for s in _sources())):
+        return LIB
+    os.makedirs(BUILD, exist_ok=True)
+    inc = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
+    host_o = os.path.join(BUILD, "host_setup.o")
+    _run(["g++", "-O2", "-ffp-contract=off", "-fPIC", "-std=c++17", "-c",
+          os.path.join(CSRC, "host_setup.cpp"), "-o", host_o] + inc)
+    kern_o = os.path.join(BUILD, "harm_kernels.o")
+    out = _run([NVCC] + ARCH + ["-O3", "-fmad=false", "-lineinfo", "-std=c++17",
+                                "-Xptxas", "-v", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+                                "-c", os.path.join(CSRC, "harm_kernels.cu"), "-o", kern_o] + inc)
+    if verbose:
+        print(out)
+    tmp = LIB + ".tmp"
+    _run([NVCC] + ARCH + ["-shared", "-o", tmp, kern_o, host_o, "-lcudart"])
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force=True, verbose=True)
+    print(LIB)

@@ -1,0 +1,1558 @@
+// B200 kernels and C ABI for HARM-COOL's step_ch() path.
+//
+// Device layout.  The reference keeps each primitive array as
+// p[SN3][SN1][SN2][8] on the host.  On the device every array is stored
+// plane by plane (structure of arrays), X[k][h][i][j] with j fastest, so a
+// warp reading one variable of 32 neighbouring theta zones reads 256
+// contiguous bytes.  Only the N3 active phi planes are stored: the
+// reference's two phi ghost planes are exact copies of planes N3 and 1 made by
+// MPI self-exchange (step_ch.c:183-198, 222-230, mpi.c:284-321), so here the
+// phi index simply wraps.  Geometry is axisymmetric and stored once per
+// (r, theta) point, 18 planes per face location (harm_phys.cuh) plus 40
+// connection planes and two floor planes.
+//
+// One step (step_ch.c:90-140) is, on one stream and without host sync:
+//   predictor : k_flux, k_update(dt/2) [flux-CT, source, inversion, floors],
+//               k_bound, k_fu_flip, k_fu_fix, k_bound
+//   corrector : k_flux (+Courant minima), k_update(dt), k_diag_flux,
+//               k_bound, k_fu_flip, k_fu_fix, k_bound
+//   k_diag_mass, k_finalize (diagnostic sums, next dt)
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "harm_b200.h"
+#include "harm_phys.cuh"
+#include "host_setup.h"
+
+namespace harm {
+
+// ---------------------------------------------------------------------------
+// device-side run state
+
+struct DevScalars {
+  double t, dt;
+  unsigned long long ndt_bits[3];  // per-direction Courant minima (bits of positive doubles)
+  double mdot, edot, ldot, mdot_in, mdot_out, mass_curr, mass_in, mass_out, ndt;
+  double bsq_max;                  // torus set-up only
+  unsigned long long bsq_bits;
+  int fail_code, fail_h, fail_i, fail_j;
+  int err;                         // HARM_E_DT when dt < 1e-9
+  int halted;                      // set after a failure: later steps do nothing
+  int nfail, fail_overflow;        // failed zones met by the current fixup_utoprim
+};
+
+// Problem description passed by value to every kernel.
+struct Grid {
+  int n1, n2, n3, sn1, sn2;
+  int istart, istop, jstart, jstop;
+  long ng;   // sn1*sn2, points per geometry plane
+  long nc;   // n3*sn1*sn2, cells per state plane
+  int lim;
+  double gam, cour, defcon, tf;
+  double dx1, dx2, dx3;
+};
+
+constexpr int FAIL_CAP = 8192;  // failed zones repaired through the sorted list
+constexpr int NTHR_FIX = 1024;
+
+struct Ctx {
+  Grid G;
+  Dims D;
+  harm_params prm;
+  int device;
+  cudaStream_t stream;
+  double *p, *ph;                // [8][nc]
+  double *F1, *F2, *F3;          // [8][nc]
+  signed char *pflag;            // [nc]
+  double *geo;                   // [4 locations][GEO_N][ng]: FACE1, FACE2, FACE3, CENT
+  double *conn;                  // [40][ng]
+  double *floors;                // [2][ng]
+  double *katm;                  // [sn1]
+  double *stage;                 // [8*nc] host-layout staging
+  signed char *stage_flag;       // [sn3*sn1*sn2]
+  int *fail_list;                // [FAIL_CAP]
+  double *fix_buf;               // [FAIL_CAP*8]
+  double *partials;              // [3][nparts]
+  int nparts;
+  DevScalars *sc;
+  cudaGraphExec_t graph_exec;
+  int graph_steps;
+  double *pinned;                // pinned host buffer for the host-array entry points
+  size_t pinned_bytes;
+};
+
+__device__ __forceinline__ void record_fail(DevScalars *sc, int code, int h, int i, int j)
+{
+  if (atomicCAS(&sc->fail_code, 0, code) == 0) {
+    sc->fail_h = h;
+    sc->fail_i = i;
+    sc->fail_j = j;
+  }
+}
+
+__device__ __forceinline__ long cidx(const Grid &G, int h, int i, int j)
+{
+  return ((long)h * G.sn1 + i) * G.sn2 + j;
+}
+
+__device__ __forceinline__ int hwrap(const Grid &G, int h)
+{
+  return h < 0 ? h + G.n3 : (h >= G.n3 ? h - G.n3 : h);
+}
+
+// geometry location slots on the device
+enum { L_FACE1 = 0, L_FACE2 = 1, L_FACE3 = 2, L_CENT = 3 };
+
+__device__ __forceinline__ const double *geo_at(const double *geo, const Grid &G, int loc)
+{
+  return geo + (long)loc * GEO_N * G.ng;
+}
+
+// ---------------------------------------------------------------------------
+// fluxes (step_ch.c:331-504): one thread per zone, its lower face in each
+// direction; slopes (interp.c:49-93) recomputed from the primitives
+
+__device__ void face_flux(double gam, int dir, const double *pl, const double *pr, const Geo &q, double *F,
+                          double &ctop, int *fail)
+{
+  State s;
+  double Fl[8], Ul[8], Fr[8], Ur[8], cmaxl, cminl, cmaxr, cminr;
+  get_state(pl, q, s, fail);
+  primtoflux(gam, pl, s, dir, q.g, Fl);
+  primtoflux(gam, pl, s, 0, q.g, Ul);
+  vchar(gam, pl, s, q, dir, cmaxl, cminl, fail);
+  get_state(pr, q, s, fail);
+  primtoflux(gam, pr, s, dir, q.g, Fr);
+  primtoflux(gam, pr, s, 0, q.g, Ur);
+  vchar(gam, pr, s, q, dir, cmaxr, cminr, fail);
+  double t1 = 0. > cmaxl ? 0. : cmaxl;
+  double cmax = fabs(t1 > cmaxr ? t1 : cmaxr);
+  double t2 = 0. > -cminl ? 0. : -cminl;
+  double cmin = fabs(t2 > -cminr ? t2 : -cminr);
+  ctop = cmax > cmin ? cmax : cmin;
+  // HLLF = 0, LAXF = 1 (step_ch.c:66-67): the local Lax-Friedrichs flux
+#pragma unroll
+  for (int k = 0; k < 8; k++) F[k] = 0.5 * (Fl[k] + Fr[k] - ctop * (Ur[k] - Ul[k]));
+}
+
+__device__ __forceinline__ double warp_min(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <bool FULL>
+__global__ void __launch_bounds__(128) k_flux(Grid G, const double *__restrict__ pb, double *__restrict__ F1,
+                                              double *__restrict__ F2, double *__restrict__ F3,
+                                              const double *__restrict__ geo, DevScalars *sc)
+{
+  if (sc->halted) return;
+  const int j = 1 + blockIdx.x * blockDim.x + threadIdx.x;  // theta, [jstart-1, jstop+1]
+  const int i = 1 + blockIdx.y * blockDim.y + threadIdx.y;  // r, [istart-1, istop+1]
+  const int h = blockIdx.z;
+  double dtmin[3] = {1.e9, 1.e9, 1.e9};
+  int fail = 0;
+  const bool in = (i <= G.sn1 - 2) && (j <= G.sn2 - 2);
+  if (in) {
+    const long c = cidx(G, h, i, j);
+    const long gi = (long)i * G.sn2 + j;
+    const bool active = i >= G.istart && i <= G.istop && j >= G.jstart && j <= G.jstop;
+    const int ndir = G.n3 > 1 ? 3 : 2;
+    for (int dir = 1; dir <= ndir; dir++) {
+      double *F = dir == 1 ? F1 : dir == 2 ? F2 : F3;
+      if (dir == 1 && i < G.istart) continue;
+      if (dir == 2 && j < G.jstart) continue;
+      if (dir == 2 && (j == G.jstart || j == G.jstop + 1)) {
+        // polar faces carry no flux (step_ch.c:412-416)
+#pragma unroll
+        for (int k = 0; k < 8; k++) F[k * G.nc + c] = 0.;
+        continue;
+      }
+      long o1, o2, o3;  // offsets of zone-2d, zone-d, zone+d
+      if (dir == 1) { o1 = c - 2 * G.sn2; o2 = c - G.sn2; o3 = c + G.sn2; }
+      else if (dir == 2) { o1 = c - 2; o2 = c - 1; o3 = c + 1; }
+      else {
+        o1 = cidx(G, hwrap(G, h - 2), i, j);
+        o2 = cidx(G, hwrap(G, h - 1), i, j);
+        o3 = cidx(G, hwrap(G, h + 1), i, j);
+      }
+      double pl[8], pr[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const double *P = pb + k * G.nc;
+        double a = __ldg(P + o1), b = __ldg(P + o2), z = __ldg(P + c), e = __ldg(P + o3);
+        pl[k] = b + 0.5 * slope_lim(G.lim, a, b, z);
+        pr[k] = z - 0.5 * slope_lim(G.lim, b, z, e);
+      }
+      Geo q;
+      load_geo(geo_at(geo, G, dir == 1 ? L_FACE1 : dir == 2 ? L_FACE2 : L_FACE3), G.ng, gi, q);
+      double Fz[8], ctop;
+      face_flux(G.gam, dir, pl, pr, q, Fz, ctop, &fail);
+#pragma unroll
+      for (int k = 0; k < 8; k++) F[k * G.nc + c] = Fz[k];
+      if (FULL && active) {
+        double dxd = dir == 1 ? G.dx1 : dir == 2 ? G.dx2 : G.dx3;
+        double dtij = G.cour * dxd / ctop;
+        if (dtij < dtmin[dir - 1]) dtmin[dir - 1] = dtij;
+      }
+    }
+    if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
+  }
+  if (FULL) {
+    __shared__ double red[3][4];
+    const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31, warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      double v = warp_min(dtmin[d]);
+      if (lane == 0) red[d][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      for (int d = 0; d < 3; d++) {
+        double v = fmin(fmin(red[d][0], red[d][1]), fmin(red[d][2], red[d][3]));
+        if (v < 1.e9) atomicMin(&sc->ndt_bits[d], (unsigned long long)__double_as_longlong(v));
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// update (step_ch.c:237-306) fused with flux_ct (step_ch.c:514-629, 726-798),
+// the flux boundary fixes (coord.c:264-324) and fixup() (fixup.c:51-60)
+
+struct Flux {
+  const double *F1, *F2, *F3;
+  Grid G;
+  __device__ double raw(int d, int k, int h, int i, int j) const
+  {
+    const double *F = d == 1 ? F1 : d == 2 ? F2 : F3;
+    return __ldg(F + k * G.nc + cidx(G, h, i, j));
+  }
+  // B-component of a raw face flux after fix_flux's polar reflection
+  // (coord.c:284-301): F1,F3[B2] at jstart-1 / jstop+1 mirror jstart / jstop
+  __device__ double rawB2(int d, int h, int i, int j) const
+  {
+    if (j == G.jstart - 1) return -raw(d, B2, h, i, G.jstart);
+    if (j == G.jstop + 1) return -raw(d, B2, h, i, G.jstop);
+    return raw(d, B2, h, i, j);
+  }
+  // 2D EMF (step_ch.c:546-547)
+  __device__ double emf2(int i, int j) const
+  {
+    return 0.25 * (rawB2(1, 0, i, j) + rawB2(1, 0, i, j - 1) - raw(2, B1, 0, i, j) - raw(2, B1, 0, i - 1, j));
+  }
+  // 3D EMFs (step_ch.c:754-764); h-1 wraps (phi periodic)
+  __device__ double e1(int h, int i, int j) const
+  {
+    int hm = hwrap(G, h - 1);
+    return 0.25 * ((raw(2, B3, h, i, j) + raw(2, B3, hm, i, j)) - (rawB2(3, h, i, j) + rawB2(3, h, i, j - 1)));
+  }
+  __device__ double e2(int h, int i, int j) const
+  {
+    int hm = hwrap(G, h - 1);
+    return 0.25 * ((raw(3, B1, h, i, j) + raw(3, B1, h, i - 1, j)) - (raw(1, B3, h, i, j) + raw(1, B3, hm, i, j)));
+  }
+  __device__ double e3(int h, int i, int j) const
+  {
+    return 0.25 * ((rawB2(1, h, i, j) + rawB2(1, h, i, j - 1)) - (raw(2, B1, h, i, j) + raw(2, B1, h, i - 1, j)));
+  }
+};
+
+template <bool THREE_D>
+__device__ void zone_fluxes(const Flux &FX, int h, int i, int j, double *f1m, double *f1p, double *f2m,
+                            double *f2p, double *f3m, double *f3p)
+{
+  const Grid &G = FX.G;
+  const int hp = THREE_D ? hwrap(G, h + 1) : 0;
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    f1m[k] = FX.raw(1, k, h, i, j);
+    f1p[k] = FX.raw(1, k, h, i + 1, j);
+    f2m[k] = FX.raw(2, k, h, i, j);
+    f2p[k] = FX.raw(2, k, h, i, j + 1);
+    if (THREE_D) {
+      f3m[k] = FX.raw(3, k, h, i, j);
+      f3p[k] = FX.raw(3, k, hp, i, j);
+    }
+  }
+  // no inflow of mass through the radial boundaries (coord.c:307-321)
+  if (i == G.istart && f1m[RHO] > 0) f1m[RHO] = 0;
+  if (i + 1 == G.istop + 1 && f1p[RHO] < 0) f1p[RHO] = 0;
+  if (!THREE_D) {
+    double eA = FX.emf2(i, j), eB = FX.emf2(i, j + 1), eC = FX.emf2(i + 1, j), eD = FX.emf2(i + 1, j + 1);
+    f1m[B1] = 0.;
+    f1m[B2] = 0.5 * (eA + eB);
+    f1m[B3] = FX.raw(1, B3, 0, i, j);
+    f1p[B1] = 0.;
+    f1p[B2] = 0.5 * (eC + eD);
+    f1p[B3] = FX.raw(1, B3, 0, i + 1, j);
+    f2m[B1] = -0.5 * (eA + eC);
+    f2m[B2] = 0.;
+    f2m[B3] = FX.raw(2, B3, 0, i, j);
+    f2p[B1] = -0.5 * (eB + eD);
+    f2p[B2] = 0.;
+    f2p[B3] = FX.raw(2, B3, 0, i, j + 1);
+  } else {
+    double e3a = FX.e3(h, i, j), e3b = FX.e3(h, i, j + 1), e3c = FX.e3(h, i + 1, j), e3d = FX.e3(h, i + 1, j + 1);
+    double e2a = FX.e2(h, i, j), e2b = FX.e2(hp, i, j), e2c = FX.e2(h, i + 1, j), e2d = FX.e2(hp, i + 1, j);
+    double e1a = FX.e1(h, i, j), e1b = FX.e1(hp, i, j), e1c = FX.e1(h, i, j + 1), e1d = FX.e1(hp, i, j + 1);
+    f1m[B1] = 0.;
+    f1m[B2] = 0.5 * (e3a + e3b);
+    f1m[B3] = -0.5 * (e2a + e2b);
+    f1p[B1] = 0.;
+    f1p[B2] = 0.5 * (e3c + e3d);
+    f1p[B3] = -0.5 * (e2c + e2d);
+    f2m[B1] = -0.5 * (e3a + e3c);
+    f2m[B2] = 0.;
+    f2m[B3] = 0.5 * (e1a + e1b);
+    f2p[B1] = -0.5 * (e3b + e3d);
+    f2p[B2] = 0.;
+    f2p[B3] = 0.5 * (e1c + e1d);
+    f3m[B1] = 0.5 * (e2a + e2c);
+    f3m[B2] = -0.5 * (e1a + e1c);
+    f3m[B3] = 0.;
+    f3p[B1] = 0.5 * (e2b + e2d);
+    f3p[B2] = -0.5 * (e1b + e1d);
+    f3p[B3] = 0.;
+  }
+}
+
+// source() (phys.c:165-207); conn stored as [k][min(nu,j)][max(nu,j)]
+__device__ __forceinline__ int conn_slot(int k, int a, int b)
+{
+  int lo = a < b ? a : b, hi = a < b ? b : a;
+  // pairs (lo,hi) with lo <= hi in row order: 00 01 02 03 11 12 13 22 23 33
+  int pair = lo == 0 ? hi : lo == 1 ? 3 + hi : lo == 2 ? 5 + hi : 9;
+  return k * 10 + pair;
+}
+
+__device__ void source(double gam, const double *pb, const Geo &q, const double *__restrict__ conn, long ng, long gi,
+                       double *dU, int *fail)
+{
+  State s;
+  get_state(pb, q, s, fail);
+  double mhd[4][4];
+#pragma unroll
+  for (int d = 0; d < 4; d++) mhd_calc(gam, pb, d, s, mhd[d]);
+#pragma unroll
+  for (int k = 0; k < 8; k++) dU[k] = 0.;
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      dU[UU] += mhd[j][k] * __ldg(conn + conn_slot(k, 0, j) * ng + gi);
+      dU[U1] += mhd[j][k] * __ldg(conn + conn_slot(k, 1, j) * ng + gi);
+      dU[U2] += mhd[j][k] * __ldg(conn + conn_slot(k, 2, j) * ng + gi);
+      dU[U3] += mhd[j][k] * __ldg(conn + conn_slot(k, 3, j) * ng + gi);
+    }
+#pragma unroll
+  for (int k = 0; k < 8; k++) dU[k] *= q.g;
+}
+
+template <bool FULL, bool THREE_D>
+__global__ void __launch_bounds__(128) k_update(Grid G, const double *__restrict__ pi, const double *__restrict__ pb,
+                                                double *__restrict__ pf, const double *__restrict__ F1,
+                                                const double *__restrict__ F2, const double *__restrict__ F3,
+                                                signed char *__restrict__ pflag, const double *__restrict__ geo,
+                                                const double *__restrict__ conn, const double *__restrict__ floors,
+                                                const double *__restrict__ katm, DevScalars *sc)
+{
+  if (sc->halted) return;
+  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
+  const int h = blockIdx.z;
+  if (i > G.istop || j > G.jstop) return;
+  const double Dt = FULL ? sc->dt : 0.5 * sc->dt;
+  const long c = cidx(G, h, i, j);
+  const long gi = (long)i * G.sn2 + j;
+  int fail = 0;
+  Geo q;
+  load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
+  double dU[8], U[8], pz[8];
+  {
+    double pbz[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) pbz[k] = __ldg(pb + k * G.nc + c);
+    source(G.gam, pbz, q, conn, G.ng, gi, dU, &fail);
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++) pz[k] = __ldg(pi + k * G.nc + c);
+  {
+    State s;
+    get_state(pz, q, s, &fail);
+    primtoflux(G.gam, pz, s, 0, q.g, U);
+  }
+  {
+    Flux FX{F1, F2, F3, G};
+    double f1m[8], f1p[8], f2m[8], f2p[8], f3m[8], f3p[8];
+    zone_fluxes<THREE_D>(FX, h, i, j, f1m, f1p, f2m, f2p, f3m, f3p);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      if (THREE_D)
+        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 - (f3p[k] - f3m[k]) / G.dx3 + dU[k]);
+      else
+        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 + dU[k]);
+    }
+  }
+  // inversion with the isentropic fall-backs (step_ch.c:265-300); the guess is pi
+  int flag = utoprim<0>(G.gam, 0., U, q, pz);
+  if (flag) {
+    double kap = __ldg(katm + i);
+    flag = utoprim<1>(G.gam, kap, U, q, pz);
+    if (flag) flag = utoprim<2>(G.gam, kap, U, q, pz);
+  }
+  signed char fl = (signed char)flag;
+  // floors and gamma limit (fixup(), fixup.c:142-383)
+  if (fixup1zone(G.gam, __ldg(floors + gi), __ldg(floors + G.ng + gi), q, pz, &fail)) fl = -33;
+#pragma unroll
+  for (int k = 0; k < 8; k++) pf[k * G.nc + c] = pz[k];
+  pflag[c] = fl;
+  if (fail) record_fail(sc, fail, h + (THREE_D ? 1 : 0), i, j);
+}
+
+// diag_flux() (diag.c:437-465): sums over the inner radial face, after the
+// mass-flux fix; one block, fixed summation order
+__global__ void k_diag_flux(Grid G, const double *__restrict__ F1, DevScalars *sc)
+{
+  if (sc->halted) return;
+  __shared__ double red[3][32];
+  double m = 0., e = 0., l = 0.;
+  const long n = (long)G.n3 * G.n2;
+  for (long t = threadIdx.x; t < n; t += blockDim.x) {
+    int h = (int)(t / G.n2), j = G.jstart + (int)(t % G.n2);
+    long c = cidx(G, h, G.istart, j);
+    double fr = F1[RHO * G.nc + c];
+    if (fr > 0) fr = 0;
+    m += fr * G.dx2 * G.dx3;
+    e += (F1[UU * G.nc + c] - fr) * G.dx2 * G.dx3;
+    l += F1[U3 * G.nc + c] * G.dx2 * G.dx3;
+  }
+  m = warp_sum(m);
+  e = warp_sum(e);
+  l = warp_sum(l);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = m;
+    red[1][threadIdx.x >> 5] = e;
+    red[2][threadIdx.x >> 5] = l;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int nw = blockDim.x >> 5;
+    double a = threadIdx.x < nw ? red[0][threadIdx.x] : 0.;
+    double b = threadIdx.x < nw ? red[1][threadIdx.x] : 0.;
+    double d = threadIdx.x < nw ? red[2][threadIdx.x] : 0.;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    d = warp_sum(d);
+    if (threadIdx.x == 0) {
+      sc->mdot = a;
+      sc->edot = -b;
+      sc->ldot = d;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// boundary conditions (bounds.c:54-331, polefix :381-436)
+//
+// Each thread owns one cell that bound_prim writes and computes its final
+// value directly from cells that bound_prim never writes, so no ordering is
+// needed: radial ghosts copy the edge zone, polefix rows copy row jstart+2
+// (linear ramp for U2, fields untouched), polar ghosts reflect (2D) or take
+// the opposite-phi plane (3D), U2 and B2 flip sign across the pole, and the
+// radial ghosts finally get inflow_check().
+
+struct BoundCell { int i, j; };
+
+__device__ __forceinline__ BoundCell bound_cell(const Grid &G, int t, int nrow)
+{
+  // columns i in {0,1,sn1-2,sn1-1} with every j, then rows with i in [2, sn1-3]
+  const int ncol = 4 * G.sn2;
+  BoundCell b;
+  if (t < ncol) {
+    int col = t / G.sn2;
+    b.i = col < 2 ? col : G.sn1 - 4 + col;
+    b.j = t % G.sn2;
+  } else {
+    int u = t - ncol;
+    int row = u / (G.sn1 - 4);
+    b.i = 2 + u % (G.sn1 - 4);
+    // rows: 0,1,sn2-2,sn2-1 then (3D) jstart, jstart+1, jstop-1, jstop
+    b.j = row < 2 ? row : row < 4 ? G.sn2 - 4 + row : (row == 4 ? G.jstart : row == 5 ? G.jstart + 1
+                                                                       : row == 6 ? G.jstop - 1 : G.jstop);
+    (void)nrow;
+  }
+  return b;
+}
+
+// value after the radial copy and (3D) polefix, for any column i, active row j
+template <bool THREE_D>
+__device__ __forceinline__ void polefixed(const Grid &G, const double *P, int h, int i, int j, double *v)
+{
+  const int ci = i < G.istart ? G.istart : (i > G.istop ? G.istop : i);
+  const long c = cidx(G, h, ci, j);
+  int jj = -1, jref = -1;
+  if (THREE_D) {
+    if (j == G.jstart) { jj = 0; jref = G.jstart + 2; }
+    else if (j == G.jstart + 1) { jj = 1; jref = G.jstart + 2; }
+    else if (j == G.jstop) { jj = 0; jref = G.jstop - 2; }
+    else if (j == G.jstop - 1) { jj = 1; jref = G.jstop - 2; }
+  }
+  if (jj >= 0) {
+    // bound_x2dn/up_polefix (bounds.c:381-436): fields kept, U2 ramped, the rest copied
+    const long cr = cidx(G, h, ci, jref);
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      double r = P[k * G.nc + cr];
+      v[k] = (k == U2) ? (jj + 0.5) / (2 + 0.5) * r : r;
+    }
+#pragma unroll
+    for (int k = 5; k < 8; k++) v[k] = P[k * G.nc + c];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] = P[k * G.nc + c];
+  }
+}
+
+template <bool THREE_D>
+__global__ void k_bound(Grid G, double *P, signed char *pflag, const double *__restrict__ geo, DevScalars *sc)
+{
+  if (sc->halted) return;
+  const int nrow = THREE_D ? 8 : 4;
+  const int ncell = 4 * G.sn2 + nrow * (G.sn1 - 4);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int h = blockIdx.y;
+  if (t >= ncell) return;
+  BoundCell b = bound_cell(G, t, nrow);
+  const int i = b.i, j = b.j;
+  double v[8];
+  signed char fl;
+  const bool rghost = i < G.istart || i > G.istop;
+  const int ci = i < G.istart ? G.istart : (i > G.istop ? G.istop : i);
+  if (j >= G.jstart && j <= G.jstop) {
+    if (!rghost && !THREE_D) return;  // nothing to do (2D rows only list ghosts)
+    polefixed<THREE_D>(G, P, h, i, j, v);
+    fl = pflag[cidx(G, h, ci, j)];
+  } else {
+    // polar ghosts: source row and plane
+    const bool low = j < G.jstart;
+    const int js = low ? (j == G.jstart - 1 ? G.jstart : G.jstart + 1) : (j == G.jstop + 1 ? G.jstop : G.jstop - 1);
+    const int hs = THREE_D ? (h + G.n3 / 2) % G.n3 : h;  // opposite-phi plane (mpi.c:374-386)
+    polefixed<THREE_D>(G, P, hs, i, js, v);
+    v[U2] *= -1.;
+    v[B2] *= -1.;
+    fl = pflag[cidx(G, h, ci, js)];
+  }
+  if (rghost) {
+    Geo q;
+    load_geo(geo_at(geo, G, L_CENT), G.ng, (long)i * G.sn2 + j, q);
+    int fail = 0;
+    inflow_check(v, q, i < G.istart ? 0 : 1, &fail);
+    if (fail) record_fail(sc, fail, h + (THREE_D ? 1 : 0), i, j);
+  }
+  const long c = cidx(G, h, i, j);
+  if (THREE_D && !rghost && j >= G.jstart && j <= G.jstop) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) P[k * G.nc + c] = v[k];  // polefix leaves the fields alone
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++) P[k * G.nc + c] = v[k];
+  pflag[c] = fl;
+}
+
+// ---------------------------------------------------------------------------
+// fixup_utoprim() (fixup.c:432-538)
+//
+// The reference flips pflag over all (i, j) of the active phi planes and
+// then repairs failed zones in loop order, in place.  Repairs from the edge
+// or corner stencils read only good zones, which the repair never changes;
+// the last-resort average reads every neighbour and so sees earlier repairs.
+// k_fu_flip flips the flags and lists the failed zones; k_fu_fix sorts the
+// list into loop order, precomputes the stencil repairs in parallel and then
+// replays the whole list in order on one thread, recomputing any zone whose
+// stencil choice changed or that needs the last-resort average.
+
+__global__ void k_fu_flip(Grid G, signed char *pflag, int *list, DevScalars *sc)
+{
+  if (sc->halted) return;
+  const long n = G.nc;
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    signed char f = pflag[c];
+    signed char nf = (signed char)(!f);
+    pflag[c] = nf;
+    if (nf == 0) {
+      int j = (int)(c % G.sn2), i = (int)((c / G.sn2) % G.sn1);
+      if (i >= G.istart && i <= G.istop && j >= G.jstart && j <= G.jstop) {
+        int slot = atomicAdd(&sc->nfail, 1);
+        if (slot < FAIL_CAP) list[slot] = (int)c;
+        else sc->fail_overflow = 1;
+      }
+    }
+  }
+}
+
+// 0: edge average, 1: corner average, 2: last resort (fixup.c:491-530)
+__device__ __forceinline__ int stencil_kind(const Grid &G, const signed char *pflag, long c)
+{
+  const long s = G.sn2;
+  bool pf2 = pflag[c + 1] != 0, pf4 = pflag[c + s] != 0, pf6 = pflag[c - 1] != 0, pf8 = pflag[c - s] != 0;
+  bool pf1 = pflag[c - s + 1] != 0, pf3 = pflag[c + s + 1] != 0, pf5 = pflag[c + s - 1] != 0,
+       pf7 = pflag[c - s - 1] != 0;
+  if (pf2 && pf4 && pf6 && pf8) return 0;
+  if (pf1 && pf3 && pf5 && pf7) return 1;
+  return 2;
+}
+
+__device__ void repair_zone(const Grid &G, const double *P, long c, int kind, double *v)
+{
+  const long s = G.sn2;
+#pragma unroll
+  for (int k = 0; k < 8; k++) v[k] = P[k * G.nc + c];
+  if (kind == 0) {
+    for (int k = 0; k < B1; k++) {
+      const double *X = P + k * G.nc;
+      v[k] = 0.25 * (X[c + 1] + X[c - 1] + X[c - s] + X[c + s]);
+    }
+  } else if (kind == 1) {
+    for (int k = 0; k < B1; k++) {
+      const double *X = P + k * G.nc;
+      v[k] = 0.25 * (X[c + s + 1] + X[c + s - 1] + X[c - s + 1] + X[c - s - 1]);
+    }
+  } else {
+    for (int k = RHO; k <= UU; k++) {
+      const double *X = P + k * G.nc;
+      v[k] = 0.5 * (0.25 * (X[c + 1] + X[c - 1] + X[c - s] + X[c + s])
+                    + 0.25 * (X[c + s + 1] + X[c + s - 1] + X[c - s + 1] + X[c - s - 1]));
+    }
+    v[U1] = v[U2] = v[U3] = 0.;
+  }
+}
+
+__device__ __forceinline__ void cell_hij(const Grid &G, long c, int &h, int &i, int &j)
+{
+  j = (int)(c % G.sn2);
+  i = (int)((c / G.sn2) % G.sn1);
+  h = (int)(c / ((long)G.sn2 * G.sn1));
+}
+
+__global__ void __launch_bounds__(NTHR_FIX) k_fu_fix(Grid G, double *P, signed char *pflag, int *list, double *fixbuf,
+                                                     const double *__restrict__ geo, const double *__restrict__ floors,
+                                                     DevScalars *sc)
+{
+  if (sc->halted) return;
+  __shared__ int keys[FAIL_CAP];
+  __shared__ signed char kinds[FAIL_CAP];
+  __shared__ int gfail;
+  const int n = sc->nfail;
+  if (n == 0) return;
+  const int tid = threadIdx.x;
+  if (tid == 0) gfail = 0;
+  const double *gC = geo_at(geo, G, L_CENT);
+  if (!sc->fail_overflow) {
+    // bitonic sort of the failed cells into loop order
+    int m = 1;
+    while (m < n) m <<= 1;
+    for (int t = tid; t < m; t += blockDim.x) keys[t] = t < n ? list[t] : 0x7fffffff;
+    __syncthreads();
+    for (int size = 2; size <= m; size <<= 1)
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int t = tid; t < m; t += blockDim.x) {
+          int u = t ^ stride;
+          if (u > t) {
+            bool up = (t & size) == 0;
+            int a = keys[t], b = keys[u];
+            if ((a > b) == up) { keys[t] = b; keys[u] = a; }
+          }
+        }
+        __syncthreads();
+      }
+    // parallel: stencil repairs from the flags as they stand now
+    for (int t = tid; t < n; t += blockDim.x) {
+      long c = keys[t];
+      int kind = stencil_kind(G, pflag, c);
+      kinds[t] = (signed char)kind;
+      if (kind < 2) {
+        double v[8];
+        repair_zone(G, P, c, kind, v);
+        int h, i, j;
+        cell_hij(G, c, h, i, j);
+        long gi = (long)i * G.sn2 + j;
+        Geo q;
+        load_geo(gC, G.ng, gi, q);
+        int fail = 0;
+        bool g33 = fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
+        if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
+        if (g33) kinds[t] = (signed char)(kinds[t] | 4);
+        for (int k = 0; k < 8; k++) fixbuf[(long)t * 8 + k] = v[k];
+      }
+    }
+    __syncthreads();
+    // in order, one thread
+    if (tid == 0) {
+      for (int t = 0; t < n; t++) {
+        long c = keys[t];
+        int kind = stencil_kind(G, pflag, c);
+        int pre = kinds[t] & 3;
+        double v[8];
+        bool g33;
+        int h, i, j;
+        cell_hij(G, c, h, i, j);
+        if (kind == pre && kind < 2) {
+          for (int k = 0; k < 8; k++) v[k] = fixbuf[(long)t * 8 + k];
+          g33 = (kinds[t] & 4) != 0;
+        } else {
+          repair_zone(G, P, c, kind, v);
+          long gi = (long)i * G.sn2 + j;
+          Geo q;
+          load_geo(gC, G.ng, gi, q);
+          int fail = 0;
+          g33 = fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
+          if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
+        }
+        for (int k = 0; k < 8; k++) P[k * G.nc + c] = v[k];
+        pflag[c] = g33 ? (signed char)-33 : (signed char)0;
+      }
+    }
+  } else if (tid == 0) {
+    // more failures than the list holds: the reference's loop, one thread
+    for (int h = 0; h < G.n3; h++)
+      for (int i = G.istart; i <= G.istop; i++)
+        for (int j = G.jstart; j <= G.jstop; j++) {
+          long c = cidx(G, h, i, j);
+          if (pflag[c] != 0) continue;
+          double v[8];
+          repair_zone(G, P, c, stencil_kind(G, pflag, c), v);
+          long gi = (long)i * G.sn2 + j;
+          Geo q;
+          load_geo(gC, G.ng, gi, q);
+          int fail = 0;
+          bool g33 = fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
+          if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
+          for (int k = 0; k < 8; k++) P[k * G.nc + c] = v[k];
+          pflag[c] = g33 ? (signed char)-33 : (signed char)0;
+        }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    sc->nfail = 0;
+    sc->fail_overflow = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// diag_mass() (diag.c:477-580, MDOTTYPE NEU_AGA_GHOST1) partial sums
+
+__global__ void __launch_bounds__(256) k_diag_mass(Grid G, const double *__restrict__ P, const double *__restrict__ geo,
+                                                   double *partials, int nparts, DevScalars *sc)
+{
+  if (sc->halted) return;
+  const double *gC = geo_at(geo, G, L_CENT);
+  double m = 0., din = 0., dout = 0.;
+  const long nact = (long)G.n3 * G.n1 * G.n2;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nact; t += (long)gridDim.x * blockDim.x) {
+    int j = G.jstart + (int)(t % G.n2);
+    int i = G.istart + (int)((t / G.n2) % G.n1);
+    int h = (int)(t / ((long)G.n2 * G.n1));
+    long gi = (long)i * G.sn2 + j;
+    m += P[RHO * G.nc + cidx(G, h, i, j)] * __ldg(gC + 17 * G.ng + gi) * G.dx1 * G.dx2 * G.dx3;
+  }
+  const long nrad = (long)G.n3 * G.n2;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < 2 * nrad; t += (long)gridDim.x * blockDim.x) {
+    bool inner = t < nrad;
+    long u = inner ? t : t - nrad;
+    int j = G.jstart + (int)(u % G.n2), h = (int)(u / G.n2);
+    int i = inner ? G.istart - 1 : G.istop + 1;
+    long c = cidx(G, h, i, j);
+    double pr[8];
+    for (int k = 0; k < 8; k++) pr[k] = P[k * G.nc + c];
+    Geo q;
+    load_geo(gC, G.ng, (long)i * G.sn2 + j, q);
+    double ucon[4];
+    int fail = 0;
+    ucon_calc(pr, q, ucon, &fail);
+    if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
+    double term = pr[RHO] * ucon[1] * q.g * G.dx2 * G.dx3;
+    if (inner) din += term;
+    else dout -= term;
+  }
+  __shared__ double red[3][8];
+  m = warp_sum(m);
+  din = warp_sum(din);
+  dout = warp_sum(dout);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) { red[0][w] = m; red[1][w] = din; red[2][w] = dout; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0., b = 0., d = 0.;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) { a += red[0][k]; b += red[1][k]; d += red[2][k]; }
+    partials[blockIdx.x] = a;
+    partials[nparts + blockIdx.x] = b;
+    partials[2 * nparts + blockIdx.x] = d;
+  }
+}
+
+// sums of the partials, mass counters, and the next time step (step_ch.c:119-137)
+__global__ void k_finalize(Grid G, const double *partials, int nparts, DevScalars *sc)
+{
+  if (sc->halted) return;
+  __shared__ double red[3][32];
+  double a = 0., b = 0., d = 0.;
+  for (int t = threadIdx.x; t < nparts; t += blockDim.x) {
+    a += partials[t];
+    b += partials[nparts + t];
+    d += partials[2 * nparts + t];
+  }
+  a = warp_sum(a);
+  b = warp_sum(b);
+  d = warp_sum(d);
+  if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = a; red[1][threadIdx.x >> 5] = b; red[2][threadIdx.x >> 5] = d; }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  a = b = d = 0.;
+  for (int k = 0; k < (int)(blockDim.x >> 5); k++) { a += red[0][k]; b += red[1][k]; d += red[2][k]; }
+  double dt = sc->dt;
+  sc->mass_curr = a;
+  sc->mdot_in = b;
+  sc->mdot_out = d;
+  sc->mass_in += b * dt;
+  sc->mass_out += d * dt;
+  double n1 = __longlong_as_double((long long)sc->ndt_bits[0]);
+  double n2 = __longlong_as_double((long long)sc->ndt_bits[1]);
+  double n3 = __longlong_as_double((long long)sc->ndt_bits[2]);
+  double ndt = G.n3 > 2 ? G.defcon * 1. / (1. / n1 + 1. / n2 + 1. / n3) : G.defcon * 1. / (1. / n1 + 1. / n2);
+  sc->ndt = ndt;
+  const unsigned long long big = (unsigned long long)__double_as_longlong(1.e9);
+  sc->ndt_bits[0] = sc->ndt_bits[1] = sc->ndt_bits[2] = big;
+  if (dt < 1.e-9) {
+    sc->err = HARM_E_DT;
+    sc->halted = 1;
+    return;
+  }
+  double t = sc->t + dt;
+  if (ndt > SAFE * dt) ndt = SAFE * dt;
+  dt = ndt;
+  if (t + dt > G.tf) dt = G.tf - t;
+  sc->t = t;
+  sc->dt = dt;
+  if (sc->fail_code) sc->halted = 1;
+}
+
+// ---------------------------------------------------------------------------
+// layout conversion between the host's p[h][i][j][8] and device planes
+
+__global__ void k_from_host(Grid G, int h0, const double *__restrict__ A, double *P, const signed char *fa,
+                            signed char *pflag)
+{
+  const long n = G.nc;
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    long hc = c + (long)h0 * G.sn1 * G.sn2;  // cell in the host array (skips the phi ghost plane)
+#pragma unroll
+    for (int k = 0; k < 8; k++) P[k * n + c] = A[hc * 8 + k];
+    if (fa) pflag[c] = fa[hc];
+  }
+}
+
+__global__ void k_to_host(Grid G, int h0, const double *__restrict__ P, double *A, const signed char *pflag,
+                          signed char *fa)
+{
+  // host planes: h0 ghost + n3 active + h0 ghost; ghosts are the periodic copies
+  const long plane = (long)G.sn1 * G.sn2;
+  const long nh = (long)(G.n3 + 2 * h0) * plane;
+  for (long hc = blockIdx.x * (long)blockDim.x + threadIdx.x; hc < nh; hc += (long)gridDim.x * blockDim.x) {
+    long hh = hc / plane, r = hc % plane;
+    long hd = hh - h0;
+    if (hd < 0) hd += G.n3;
+    if (hd >= G.n3) hd -= G.n3;
+    long c = hd * plane + r;
+#pragma unroll
+    for (int k = 0; k < 8; k++) A[hc * 8 + k] = P[k * G.nc + c];
+    if (fa) fa[hc] = pflag[c];
+  }
+}
+
+// fixup() alone over the active zones (harm_fixup)
+__global__ void k_fixup(Grid G, double *P, signed char *pflag, const double *__restrict__ geo,
+                        const double *__restrict__ floors, DevScalars *sc)
+{
+  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
+  const int h = blockIdx.z;
+  if (i > G.istop || j > G.jstop) return;
+  const long c = cidx(G, h, i, j), gi = (long)i * G.sn2 + j;
+  Geo q;
+  load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
+  double v[8];
+  for (int k = 0; k < 8; k++) v[k] = P[k * G.nc + c];
+  int fail = 0;
+  if (fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail)) pflag[c] = -33;
+  if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
+  for (int k = 0; k < 8; k++) P[k * G.nc + c] = v[k];
+}
+
+// Utoprim_2d over independent zones (harm_utoprim_2d_batch)
+__global__ void k_utoprim_batch(const double *U, const double *gcov, const double *gcon, const double *gdet,
+                                double *prim, int *ret, long n, double gam)
+{
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double *a = gcov + t * 16, *b = gcon + t * 16;
+  Geo q;
+  q.v00 = a[0]; q.v01 = a[1]; q.v03 = a[3]; q.v11 = a[5]; q.v13 = a[7]; q.v22 = a[10]; q.v33 = a[15];
+  q.n00 = b[0]; q.n01 = b[1]; q.n03 = b[3]; q.n10 = b[4]; q.n11 = b[5]; q.n13 = b[7]; q.n22 = b[10];
+  q.n30 = b[12]; q.n31 = b[13]; q.n33 = b[15];
+  q.g = gdet[t];
+  double u[8], p[8];
+  for (int k = 0; k < 8; k++) { u[k] = U[t * 8 + k]; p[k] = prim[t * 8 + k]; }
+  ret[t] = utoprim<0>(gam, 0., u, q, p);
+  for (int k = 0; k < 8; k++) prim[t * 8 + k] = p[k];
+}
+
+// torus set-up: b^2 maximum over the active zones, and the field rescaling (init.c:368-403)
+__global__ void k_bsq_max(Grid G, const double *__restrict__ P, const double *__restrict__ geo, DevScalars *sc)
+{
+  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
+  const int h = blockIdx.z;
+  if (i > G.istop || j > G.jstop) return;
+  const long c = cidx(G, h, i, j), gi = (long)i * G.sn2 + j;
+  Geo q;
+  load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
+  double v[8];
+  for (int k = 0; k < 8; k++) v[k] = P[k * G.nc + c];
+  State s;
+  int fail = 0;
+  get_state(v, q, s, &fail);
+  double bsq = dot4(s.bcon, s.bcov);
+  if (bsq > 0.) atomicMax(&sc->bsq_bits, (unsigned long long)__double_as_longlong(bsq));
+}
+
+__global__ void k_scale_field(Grid G, double *P, double norm)
+{
+  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
+  const int h = blockIdx.z;
+  if (i > G.istop || j > G.jstop) return;
+  const long c = cidx(G, h, i, j);
+  P[B1 * G.nc + c] *= norm;
+  P[B2 * G.nc + c] *= norm;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+thread_local std::string g_err;
+
+int fail_with(int code, const std::string &msg)
+{
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      return fail_with(HARM_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));         \
+  } while (0)
+
+int launch_step(Ctx *x);
+
+dim3 zone_grid(const Grid &G) { return dim3((G.n2 + 31) / 32, (G.n1 + 3) / 4, G.n3); }
+
+int launch_bound(Ctx *x, double *P)
+{
+  const Grid &G = x->G;
+  const int nrow = G.n3 > 1 ? 8 : 4;
+  const int ncell = 4 * G.sn2 + nrow * (G.sn1 - 4);
+  dim3 grid((ncell + 127) / 128, G.n3);
+  if (G.n3 > 1) k_bound<true><<<grid, 128, 0, x->stream>>>(G, P, x->pflag, x->geo, x->sc);
+  else k_bound<false><<<grid, 128, 0, x->stream>>>(G, P, x->pflag, x->geo, x->sc);
+  return HARM_OK;
+}
+
+int launch_fixup_utoprim(Ctx *x, double *P)
+{
+  const Grid &G = x->G;
+  k_fu_flip<<<148 * 8, 256, 0, x->stream>>>(G, x->pflag, x->fail_list, x->sc);
+  k_fu_fix<<<1, NTHR_FIX, 0, x->stream>>>(G, P, x->pflag, x->fail_list, x->fix_buf, x->geo, x->floors, x->sc);
+  return HARM_OK;
+}
+
+// advance() + fixup + bound_prim + fixup_utoprim + bound_prim (step_ch.c:101-117)
+template <bool FULL>
+void launch_half(Ctx *x, const double *pi, const double *pb, double *pf)
+{
+  const Grid &G = x->G;
+  dim3 fb(32, 4), fg((G.sn2 - 2 + 31) / 32, (G.sn1 - 2 + 3) / 4, G.n3);
+  k_flux<FULL><<<fg, fb, 0, x->stream>>>(G, pb, x->F1, x->F2, x->F3, x->geo, x->sc);
+  dim3 ub(32, 4);
+  if (G.n3 > 1)
+    k_update<FULL, true><<<zone_grid(G), ub, 0, x->stream>>>(G, pi, pb, pf, x->F1, x->F2, x->F3, x->pflag, x->geo,
+                                                               x->conn, x->floors, x->katm, x->sc);
+  else
+    k_update<FULL, false><<<zone_grid(G), ub, 0, x->stream>>>(G, pi, pb, pf, x->F1, x->F2, x->F3, x->pflag, x->geo,
+                                                                x->conn, x->floors, x->katm, x->sc);
+  if (FULL) k_diag_flux<<<1, 1024, 0, x->stream>>>(G, x->F1, x->sc);
+  launch_bound(x, pf);
+  launch_fixup_utoprim(x, pf);
+  launch_bound(x, pf);
+}
+
+int launch_step(Ctx *x)
+{
+  launch_half<false>(x, x->p, x->p, x->ph);
+  launch_half<true>(x, x->p, x->ph, x->p);
+  k_diag_mass<<<x->nparts, 256, 0, x->stream>>>(x->G, x->p, x->geo, x->partials, x->nparts, x->sc);
+  k_finalize<<<1, 1024, 0, x->stream>>>(x->G, x->partials, x->nparts, x->sc);
+  CK(cudaGetLastError());
+  return HARM_OK;
+}
+
+// structural checks on the host geometry: the device stores only the
+// non-zero, independent entries
+bool geometry_layout_ok(const Dims &d, const double *gcov, const double *gcon, const double *conn, std::string &why)
+{
+  static const int zero_slots[6][2] = {{0, 2}, {1, 2}, {2, 0}, {2, 1}, {2, 3}, {3, 2}};
+  for (long c = 0; c < d.plane(); c++)
+    for (int loc = 0; loc < 5; loc++) {
+      const double *a = gcov + (c * 5 + loc) * 16, *b = gcon + (c * 5 + loc) * 16;
+      for (auto &z : zero_slots)
+        if (a[z[0] * 4 + z[1]] != 0. || b[z[0] * 4 + z[1]] != 0.) { why = "metric entry expected to vanish is non-zero"; return false; }
+      for (int m = 0; m < 4; m++)
+        for (int n = 0; n < 4; n++)
+          if (a[m * 4 + n] != a[n * 4 + m]) { why = "gcov not symmetric"; return false; }
+    }
+  for (long c = 0; c < d.plane(); c++)
+    for (int k = 0; k < 4; k++)
+      for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++)
+          if (conn[c * 64 + k * 16 + a * 4 + b] != conn[c * 64 + k * 16 + b * 4 + a]) {
+            why = "connection not symmetric in its lower indices";
+            return false;
+          }
+  return true;
+}
+
+}  // namespace harm
+
+using namespace harm;
+
+struct harm_ctx {
+  Ctx x;
+};
+
+extern "C" const char *harm_last_error(void) { return g_err.c_str(); }
+
+static int ensure_pinned(Ctx *x, size_t bytes)
+{
+  if (x->pinned_bytes >= bytes) return HARM_OK;
+  if (x->pinned) cudaFreeHost(x->pinned);
+  x->pinned = nullptr;
+  x->pinned_bytes = 0;
+  CK(cudaMallocHost(&x->pinned, bytes));
+  x->pinned_bytes = bytes;
+  return HARM_OK;
+}
+
+extern "C" int harm_create(const harm_params *prm, const double *gcov, const double *gcon, const double *gdet,
+                           const double *conn, const double *coords, const double *katm, int device,
+                           harm_ctx **out)
+{
+  if (!prm || !gcov || !gcon || !gdet || !conn || !coords || !katm || !out) return fail_with(HARM_E_ARG, "null argument");
+  if (!valid_grid(prm->n1, prm->n2, prm->n3)) return fail_with(HARM_E_ARG, "grid must have n1>=4, n2>=8, n3==1 or even n3>=4");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0)
+    return fail_with(HARM_E_NODEV, "no CUDA device");
+  cudaDeviceProp dp;
+  CK(cudaGetDeviceProperties(&dp, device));
+  if (dp.major != 10) return fail_with(HARM_E_NODEV, "this build targets sm_100a (B200)");
+  Dims d = make_dims(prm->n1, prm->n2, prm->n3);
+  std::string why;
+  if (!geometry_layout_ok(d, gcov, gcon, conn, why)) return fail_with(HARM_E_ARG, why);
+  CK(cudaSetDevice(device));
+  harm_ctx *h = new harm_ctx();
+  Ctx *x = &h->x;
+  std::memset(x, 0, sizeof(Ctx));
+  x->D = d;
+  x->prm = *prm;
+  x->device = device;
+  Grid &G = x->G;
+  G.n1 = d.n1; G.n2 = d.n2; G.n3 = d.n3; G.sn1 = d.sn1; G.sn2 = d.sn2;
+  G.istart = d.istart; G.istop = d.istop; G.jstart = d.jstart; G.jstop = d.jstop;
+  G.ng = (long)d.sn1 * d.sn2;
+  G.nc = (long)d.n3 * G.ng;
+  G.lim = prm->lim;
+  G.gam = prm->gam; G.cour = prm->cour; G.defcon = prm->defcon; G.tf = prm->tf;
+  G.dx1 = prm->dx[1]; G.dx2 = prm->dx[2]; G.dx3 = prm->dx[3];
+  x->nparts = 148 * 4;
+  auto al = [&](void **p, size_t b) -> int { CK(cudaMalloc(p, b)); return HARM_OK; };
+  const size_t st = 8 * G.nc * sizeof(double);
+  int rc = HARM_OK;
+  rc |= al((void **)&x->p, st);
+  rc |= al((void **)&x->ph, st);
+  rc |= al((void **)&x->F1, st);
+  rc |= al((void **)&x->F2, st);
+  rc |= al((void **)&x->F3, d.n3 > 1 ? st : 8);
+  rc |= al((void **)&x->pflag, G.nc);
+  rc |= al((void **)&x->geo, 4 * GEO_N * G.ng * sizeof(double));
+  rc |= al((void **)&x->conn, 40 * G.ng * sizeof(double));
+  rc |= al((void **)&x->floors, 2 * G.ng * sizeof(double));
+  rc |= al((void **)&x->katm, d.sn1 * sizeof(double));
+  rc |= al((void **)&x->stage, (size_t)8 * d.cells() * sizeof(double));
+  rc |= al((void **)&x->stage_flag, d.cells());
+  rc |= al((void **)&x->fail_list, FAIL_CAP * sizeof(int));
+  rc |= al((void **)&x->fix_buf, FAIL_CAP * 8 * sizeof(double));
+  rc |= al((void **)&x->partials, 3 * x->nparts * sizeof(double));
+  rc |= al((void **)&x->sc, sizeof(DevScalars));
+  if (rc != HARM_OK) { harm_destroy(h); return HARM_E_CUDA; }
+  if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) { harm_destroy(h); return fail_with(HARM_E_CUDA, "stream"); }
+  // geometry planes
+  std::vector<double> hg((size_t)4 * GEO_N * G.ng), hc((size_t)40 * G.ng), hf((size_t)2 * G.ng);
+  static const int locs[4] = {0 /*FACE1*/, 1 /*FACE2*/, 4 /*FACE3*/, 3 /*CENT*/};
+  for (int L = 0; L < 4; L++)
+    for (long c = 0; c < G.ng; c++) {
+      const double *a = gcov + (c * 5 + locs[L]) * 16, *b = gcon + (c * 5 + locs[L]) * 16;
+      const double vals[GEO_N] = {a[0], a[1], a[3], a[5], a[7], a[10], a[15],
+                                  b[0], b[1], b[3], b[4], b[5], b[7], b[10], b[12], b[13], b[15],
+                                  gdet[c * 5 + locs[L]]};
+      for (int e = 0; e < GEO_N; e++) hg[((size_t)L * GEO_N + e) * G.ng + c] = vals[e];
+    }
+  for (long c = 0; c < G.ng; c++)
+    for (int k = 0; k < 4; k++)
+      for (int lo = 0; lo < 4; lo++)
+        for (int hi = lo; hi < 4; hi++) {
+          int pair = lo == 0 ? hi : lo == 1 ? 3 + hi : lo == 2 ? 5 + hi : 9;
+          hc[(size_t)(k * 10 + pair) * G.ng + c] = conn[c * 64 + k * 16 + lo * 4 + hi];
+        }
+  // radial floors get_rho_u_floor() (fixup.c:117-140), evaluated on the host
+  radial_floors(coords, prm->gam, G.ng, hf.data());
+  DevScalars s0;
+  std::memset(&s0, 0, sizeof(s0));
+  unsigned long long big;
+  double b9 = 1.e9;
+  std::memcpy(&big, &b9, 8);
+  s0.ndt_bits[0] = s0.ndt_bits[1] = s0.ndt_bits[2] = big;
+  s0.dt = 1.e-5;
+  if (cudaMemcpy(x->geo, hg.data(), hg.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(x->conn, hc.data(), hc.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(x->floors, hf.data(), hf.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(x->katm, katm, d.sn1 * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(x->sc, &s0, sizeof(s0), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(x->p, 0, st) != cudaSuccess || cudaMemset(x->ph, 0, st) != cudaSuccess ||
+      cudaMemset(x->F1, 0, st) != cudaSuccess || cudaMemset(x->F2, 0, st) != cudaSuccess ||
+      cudaMemset(x->pflag, 0, G.nc) != cudaSuccess) {
+    harm_destroy(h);
+    return fail_with(HARM_E_CUDA, "upload");
+  }
+  *out = h;
+  return HARM_OK;
+}
+
+extern "C" void harm_destroy(harm_ctx *h)
+{
+  if (!h) return;
+  Ctx *x = &h->x;
+  if (x->graph_exec) cudaGraphExecDestroy(x->graph_exec);
+  void *ptrs[] = {x->p, x->ph, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm,
+                  x->stage, x->stage_flag, x->fail_list, x->fix_buf, x->partials, x->sc};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (x->pinned) cudaFreeHost(x->pinned);
+  if (x->stream) cudaStreamDestroy(x->stream);
+  delete h;
+}
+
+static int put_prims(Ctx *x, const double *p, const signed char *pflag, double *dst)
+{
+  const Dims &d = x->D;
+  const int h0 = d.n3 > 1 ? 1 : 0;
+  const size_t nb = (size_t)8 * d.cells() * sizeof(double);
+  CK(cudaMemcpyAsync(x->stage, p, nb, cudaMemcpyHostToDevice, x->stream));
+  if (pflag) CK(cudaMemcpyAsync(x->stage_flag, pflag, d.cells(), cudaMemcpyHostToDevice, x->stream));
+  k_from_host<<<148 * 8, 256, 0, x->stream>>>(x->G, h0, x->stage, dst, pflag ? x->stage_flag : nullptr, x->pflag);
+  CK(cudaGetLastError());
+  return HARM_OK;
+}
+
+static int get_prims(Ctx *x, const double *src, double *p, signed char *pflag)
+{
+  const Dims &d = x->D;
+  const int h0 = d.n3 > 1 ? 1 : 0;
+  k_to_host<<<148 * 8, 256, 0, x->stream>>>(x->G, h0, src, x->stage, x->pflag, pflag ? x->stage_flag : nullptr);
+  CK(cudaGetLastError());
+  const size_t nb = (size_t)8 * d.cells() * sizeof(double);
+  if (p) CK(cudaMemcpyAsync(p, x->stage, nb, cudaMemcpyDeviceToHost, x->stream));
+  if (pflag) CK(cudaMemcpyAsync(pflag, x->stage_flag, d.cells(), cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  return HARM_OK;
+}
+
+extern "C" int harm_put_prims(harm_ctx *h, const double *p, const signed char *pflag)
+{
+  if (!h || !p) return fail_with(HARM_E_ARG, "null argument");
+  int rc = put_prims(&h->x, p, pflag, h->x.p);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->x.stream));
+  return HARM_OK;
+}
+
+extern "C" int harm_get_prims(harm_ctx *h, double *p, signed char *pflag)
+{
+  if (!h || (!p && !pflag)) return fail_with(HARM_E_ARG, "null argument");
+  return get_prims(&h->x, h->x.p, p, pflag);
+}
+
+static int read_scalars(Ctx *x, DevScalars *s)
+{
+  CK(cudaMemcpyAsync(s, x->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  return HARM_OK;
+}
+
+static int write_scalars(Ctx *x, const DevScalars *s)
+{
+  CK(cudaMemcpyAsync(x->sc, s, sizeof(DevScalars), cudaMemcpyHostToDevice, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  return HARM_OK;
+}
+
+extern "C" int harm_set_time(harm_ctx *h, double t, double dt)
+{
+  if (!h) return fail_with(HARM_E_ARG, "null context");
+  DevScalars s;
+  int rc = read_scalars(&h->x, &s);
+  if (rc) return rc;
+  s.t = t;
+  s.dt = dt;
+  s.err = 0;
+  s.halted = 0;
+  s.fail_code = 0;
+  return write_scalars(&h->x, &s);
+}
+
+extern "C" int harm_get_time(harm_ctx *h, double *t, double *dt)
+{
+  if (!h || !t || !dt) return fail_with(HARM_E_ARG, "null argument");
+  DevScalars s;
+  int rc = read_scalars(&h->x, &s);
+  if (rc) return rc;
+  *t = s.t;
+  *dt = s.dt;
+  return HARM_OK;
+}
+
+extern "C" int harm_set_mass(harm_ctx *h, double mass_in, double mass_out)
+{
+  if (!h) return fail_with(HARM_E_ARG, "null context");
+  DevScalars s;
+  int rc = read_scalars(&h->x, &s);
+  if (rc) return rc;
+  s.mass_in = mass_in;
+  s.mass_out = mass_out;
+  return write_scalars(&h->x, &s);
+}
+
+extern "C" int harm_get_diag(harm_ctx *h, harm_diag *d)
+{
+  if (!h || !d) return fail_with(HARM_E_ARG, "null argument");
+  DevScalars s;
+  int rc = read_scalars(&h->x, &s);
+  if (rc) return rc;
+  d->mdot = s.mdot; d->edot = s.edot; d->ldot = s.ldot;
+  d->mdot_in = s.mdot_in; d->mdot_out = s.mdot_out; d->mass_curr = s.mass_curr;
+  d->mass_in = s.mass_in; d->mass_out = s.mass_out; d->ndt = s.ndt;
+  d->fail_code = s.fail_code; d->fail_h = s.fail_h; d->fail_i = s.fail_i; d->fail_j = s.fail_j;
+  return HARM_OK;
+}
+
+extern "C" int harm_sync(harm_ctx *h)
+{
+  if (!h) return fail_with(HARM_E_ARG, "null context");
+  CK(cudaStreamSynchronize(h->x.stream));
+  CK(cudaGetLastError());
+  DevScalars s;
+  int rc = read_scalars(&h->x, &s);
+  if (rc) return rc;
+  if (s.err) return fail_with(s.err, "dt < 1e-9 (the reference exits with code 11)");
+  return HARM_OK;
+}
+
+extern "C" int harm_step_ch(harm_ctx *h)
+{
+  if (!h) return fail_with(HARM_E_ARG, "null context");
+  return launch_step(&h->x);
+}
+
+extern "C" int harm_run(harm_ctx *h, int nsteps)
+{
+  if (!h || nsteps < 0) return fail_with(HARM_E_ARG, "bad argument");
+  Ctx *x = &h->x;
+  if (!x->graph_exec) {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = launch_step(x);
+    cudaError_t e = cudaStreamEndCapture(x->stream, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail_with(HARM_E_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&x->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail_with(HARM_E_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+  }
+  for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(x->graph_exec, x->stream));
+  return harm_sync(h);
+}
+
+extern "C" int harm_step_ch_host(harm_ctx *h, double *p)
+{
+  if (!h || !p) return fail_with(HARM_E_ARG, "null argument");
+  Ctx *x = &h->x;
+  int rc = put_prims(x, p, nullptr, x->p);
+  if (rc) return rc;
+  rc = launch_step(x);
+  if (rc) return rc;
+  return get_prims(x, x->p, p, nullptr);
+}
+
+// the per-array entry points: upload into the half-step buffer, run, download
+static int on_host_array(harm_ctx *h, double *pv, int which)
+{
+  if (!h || !pv) return fail_with(HARM_E_ARG, "null argument");
+  Ctx *x = &h->x;
+  int rc = put_prims(x, pv, nullptr, x->ph);
+  if (rc) return rc;
+  const Grid &G = x->G;
+  if (which == 0) {
+    k_fixup<<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, x->ph, x->pflag, x->geo, x->floors, x->sc);
+  } else if (which == 1) {
+    launch_bound(x, x->ph);
+  } else {
+    launch_fixup_utoprim(x, x->ph);
+  }
+  CK(cudaGetLastError());
+  return get_prims(x, x->ph, pv, nullptr);
+}
+
+extern "C" int harm_fixup(harm_ctx *h, double *pv) { return on_host_array(h, pv, 0); }
+extern "C" int harm_bound_prim(harm_ctx *h, double *pv) { return on_host_array(h, pv, 1); }
+extern "C" int harm_fixup_utoprim(harm_ctx *h, double *pv) { return on_host_array(h, pv, 2); }
+
+extern "C" int harm_utoprim_2d_batch(const double *U, const double *gcov, const double *gcon, const double *gdet,
+                                     double *prim, int *ret, long n, double gam)
+{
+  if (!U || !gcov || !gcon || !gdet || !prim || !ret || n < 0) return fail_with(HARM_E_ARG, "null argument");
+  if (n == 0) return HARM_OK;
+  double *dU, *da, *db, *dg, *dp;
+  int *dr;
+  CK(cudaMalloc(&dU, n * 8 * 8));
+  CK(cudaMalloc(&da, n * 16 * 8));
+  CK(cudaMalloc(&db, n * 16 * 8));
+  CK(cudaMalloc(&dg, n * 8));
+  CK(cudaMalloc(&dp, n * 8 * 8));
+  CK(cudaMalloc(&dr, n * sizeof(int)));
+  CK(cudaMemcpy(dU, U, n * 64, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(da, gcov, n * 128, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(db, gcon, n * 128, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dg, gdet, n * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dp, prim, n * 64, cudaMemcpyHostToDevice));
+  k_utoprim_batch<<<(unsigned)((n + 127) / 128), 128>>>(dU, da, db, dg, dp, dr, n, gam);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(prim, dp, n * 64, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ret, dr, n * sizeof(int), cudaMemcpyDeviceToHost));
+  cudaFree(dU); cudaFree(da); cudaFree(db); cudaFree(dg); cudaFree(dp); cudaFree(dr);
+  return HARM_OK;
+}
+
+// init(): torus fields on the host, floors and boundaries on the device, the
+// loop potential on the host, its normalisation on the device (init.c:70-472)
+extern "C" int harm_init_torus(harm_ctx *h, const harm_grid_spec *g, const harm_torus_spec *tor)
+{
+  if (!h || !g || !tor) return fail_with(HARM_E_ARG, "null argument");
+  Ctx *x = &h->x;
+  const Dims &d = x->D;
+  if (g->n1 != d.n1 || g->n2 != d.n2 || g->n3 != d.n3) return fail_with(HARM_E_ARG, "grid spec does not match the context");
+  const size_t ncell = (size_t)d.cells();
+  std::vector<double> p(ncell * 8, 0.), gcov, gcon((size_t)d.plane() * 80), gdet((size_t)d.plane() * 5);
+  // the torus velocity transform needs the CENT inverse metric; recompute the grid on the host
+  {
+    std::vector<double> gv((size_t)d.plane() * 80), cn((size_t)d.plane() * 64), co((size_t)d.plane() * 4);
+    int rc = harm_set_grid(g, x->prm.dx, x->prm.startx, gv.data(), gcon.data(), gdet.data(), cn.data(), co.data());
+    if (rc) return rc;
+    gcov.swap(gv);
+  }
+  double rhomax, umax;
+  torus_hydro(*g, x->prm, *tor, gcov.data(), gcon.data(), p.data(), &rhomax, &umax);
+  for (int hh = d.hstart; hh <= d.hstop; hh++)
+    for (int i = d.istart; i <= d.istop; i++)
+      for (int j = d.jstart; j <= d.jstop; j++) {
+        double *pz = p.data() + (((size_t)hh * d.sn1 + i) * d.sn2 + j) * 8;
+        pz[0] /= rhomax;
+        pz[1] /= rhomax;
+      }
+  umax /= rhomax;
+  int rc = harm_put_prims(h, p.data(), nullptr);
+  if (rc) return rc;
+  const Grid &G = x->G;
+  k_fixup<<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, x->p, x->pflag, x->geo, x->floors, x->sc);
+  launch_bound(x, x->p);
+  rc = get_prims(x, x->p, p.data(), nullptr);
+  if (rc) return rc;
+  torus_field(d, x->prm, gdet.data(), p.data());
+  rc = harm_put_prims(h, p.data(), nullptr);
+  if (rc) return rc;
+  DevScalars s;
+  rc = read_scalars(x, &s);
+  if (rc) return rc;
+  s.bsq_bits = 0;
+  rc = write_scalars(x, &s);
+  if (rc) return rc;
+  k_bsq_max<<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, x->p, x->geo, x->sc);
+  rc = read_scalars(x, &s);
+  if (rc) return rc;
+  double bsq_max;
+  std::memcpy(&bsq_max, &s.bsq_bits, 8);
+  double beta_act = (x->prm.gam - 1.) * umax / (0.5 * bsq_max);
+  double norm = sqrt(beta_act / tor->beta);
+  k_scale_field<<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, x->p, norm);
+  k_fixup<<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, x->p, x->pflag, x->geo, x->floors, x->sc);
+  launch_bound(x, x->p);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(x->stream));
+  // main(): t = 0, dt = 1e-5 (init.c:122-123), mass counters from zero
+  rc = read_scalars(x, &s);
+  if (rc) return rc;
+  s.t = 0.;
+  s.dt = 1.e-5;
+  s.mass_in = s.mass_out = 0.;
+  s.fail_code = 0;
+  s.err = 0;
+  s.halted = 0;
+  return write_scalars(x, &s);
+}
+
+// ---------------------------------------------------------------------------
+// device-timed entry points
+
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ~EventPair()
+  {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+extern "C" int harm_run_timed(harm_ctx *h, int nsteps, double *ms)
+{
+  if (!h || !ms || nsteps < 0) return fail_with(HARM_E_ARG, "bad argument");
+  Ctx *x = &h->x;
+  int rc = harm_run(h, 0);  // capture the graph outside the timed region
+  if (rc) return rc;
+  EventPair e;
+  CK(cudaEventCreate(&e.a));
+  CK(cudaEventCreate(&e.b));
+  CK(cudaEventRecord(e.a, x->stream));
+  for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(x->graph_exec, x->stream));
+  CK(cudaEventRecord(e.b, x->stream));
+  CK(cudaEventSynchronize(e.b));
+  float f;
+  CK(cudaEventElapsedTime(&f, e.a, e.b));
+  *ms = f;
+  return harm_sync(h);
+}
+
+extern "C" int harm_step_ch_host_timed(harm_ctx *h, double *p, int nsteps, double *ms)
+{
+  if (!h || !p || !ms || nsteps < 0) return fail_with(HARM_E_ARG, "bad argument");
+  Ctx *x = &h->x;
+  EventPair e;
+  CK(cudaEventCreate(&e.a));
+  CK(cudaEventCreate(&e.b));
+  CK(cudaEventRecord(e.a, x->stream));
+  for (int s = 0; s < nsteps; s++) {
+    int rc = put_prims(x, p, nullptr, x->p);
+    if (rc) return rc;
+    rc = launch_step(x);
+    if (rc) return rc;
+    k_to_host<<<148 * 8, 256, 0, x->stream>>>(x->G, x->D.n3 > 1 ? 1 : 0, x->p, x->stage, x->pflag, nullptr);
+    CK(cudaMemcpyAsync(p, x->stage, (size_t)8 * x->D.cells() * sizeof(double), cudaMemcpyDeviceToHost,
+                       x->stream));
+  }
+  CK(cudaEventRecord(e.b, x->stream));
+  CK(cudaEventSynchronize(e.b));
+  float f;
+  CK(cudaEventElapsedTime(&f, e.a, e.b));
+  *ms = f;
+  return harm_sync(h);
+}
+
+extern "C" int harm_time_kernels(harm_ctx *h, int reps, double *ms)
+{
+  if (!h || !ms || reps < 1) return fail_with(HARM_E_ARG, "bad argument");
+  Ctx *x = &h->x;
+  const Grid &G = x->G;
+  DevScalars saved;
+  int rc = read_scalars(x, &saved);
+  if (rc) return rc;
+  // work on copies so the state is untouched: ph <- p, scratch output in stage
+  const size_t st = 8 * G.nc * sizeof(double);
+  double *scratch = x->stage;
+  CK(cudaMemcpyAsync(x->ph, x->p, st, cudaMemcpyDeviceToDevice, x->stream));
+  std::vector<signed char> flags((size_t)G.nc);
+  CK(cudaMemcpyAsync(flags.data(), x->pflag, G.nc, cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  EventPair e;
+  CK(cudaEventCreate(&e.a));
+  CK(cudaEventCreate(&e.b));
+  dim3 fb(32, 4), fg((G.sn2 - 2 + 31) / 32, (G.sn1 - 2 + 3) / 4, G.n3);
+  for (int kk = 0; kk < HARM_NKERNELS; kk++) {
+    // one untimed launch, then reps timed launches
+    for (int r = 0; r <= reps; r++) {
+      if (r == 1) CK(cudaEventRecord(e.a, x->stream));
+      switch (kk) {
+      case 0:
+        k_flux<true><<<fg, fb, 0, x->stream>>>(G, x->ph, x->F1, x->F2, x->F3, x->geo, x->sc);
+        break;
+      case 1:
+        if (G.n3 > 1)
+          k_update<true, true><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(
+              G, x->p, x->ph, scratch, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm, x->sc);
+        else
+          k_update<true, false><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(
+              G, x->p, x->ph, scratch, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm, x->sc);
+        break;
+      case 2:
+        launch_bound(x, x->ph);
+        break;
+      case 3:
+        launch_fixup_utoprim(x, x->ph);
+        break;
+      case 4:
+        k_diag_mass<<<x->nparts, 256, 0, x->stream>>>(G, x->ph, x->geo, x->partials, x->nparts, x->sc);
+        break;
+      }
+    }
+    CK(cudaEventRecord(e.b, x->stream));
+    CK(cudaEventSynchronize(e.b));
+    float f;
+    CK(cudaEventElapsedTime(&f, e.a, e.b));
+    ms[kk] = f / reps;
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(x->pflag, flags.data(), G.nc, cudaMemcpyHostToDevice, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  return write_scalars(x, &saved);
+}

@@ -1,0 +1,170 @@
+/*
+ * harm_b200.h -- C ABI of the B200 implementation of HARM-COOL's per-zone
+ * GRMHD update (the step_ch() path).
+ *
+ * Plain C types only.  Arrays use the reference's own layouts:
+ *   primitives   p[SN3][SN1][SN2][8]       (decs.h:190-197, main.c:318-342)
+ *   pflag        signed char [SN3][SN1][SN2]
+ *   gcov, gcon   [SN1][SN2][5][4][4]        (main.c:384-386; locations FACE1,
+ *   gdet         [SN1][SN2][5]               FACE2, CORN, CENT, FACE3)
+ *   conn         [SN1][SN2][4][4][4]         (main.c:384)
+ *   coords       [SN1][SN2][4]               (main.c:388)
+ *   katm         [SN1]                       (decs.h:306)
+ * with SN1 = N1+4, SN2 = N2+4, SN3 = N3+2 (N3 > 1) or 1 (N3 == 1).
+ *
+ * Every function returns 0 on success or a negative HARM_E* code; the text
+ * of the last error on the calling thread is available from
+ * harm_last_error().  Physical failures that the reference handles by
+ * calling fail() and exiting (diag.c:381-397) are reported instead through
+ * harm_diag.fail_code after the step that met them, and the state is left as
+ * the reference leaves it just before the exit.
+ */
+#ifndef HARM_B200_H
+#define HARM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HARM_NPR 8
+#define HARM_NPG 5
+
+enum {
+  HARM_OK = 0,
+  HARM_E_ARG = -1,      /* bad argument or grid size */
+  HARM_E_CUDA = -2,     /* a CUDA runtime call failed */
+  HARM_E_NODEV = -3,    /* no usable sm_100 device */
+  HARM_E_DT = -11,      /* dt < 1e-9: where the reference calls exit(11) (step_ch.c:126-129) */
+  HARM_E_TIMEOUT = -12  /* a bounded device-side wait ran out */
+};
+
+/* Run parameters (decs.h:263-283, init.c:104-125). */
+typedef struct harm_params {
+  int n1, n2, n3;   /* active zones in r, theta, phi; n3 == 1 or even n3 >= 4 */
+  int lim;          /* slope limiter: 0 MC, 1 van Leer, 2 minmod */
+  double a;         /* black-hole spin */
+  double gam;       /* adiabatic index */
+  double cour;      /* Courant number */
+  double defcon;    /* Courant safety factor (main.c:204) */
+  double tf;        /* end time: dt is clipped so that t never passes tf */
+  double dx[4];     /* coordinate spacing; dx[1..3] used */
+  double startx[4]; /* coordinate origin; startx[1..3] used */
+} harm_params;
+
+/* Modified Kerr-Schild grid (coord.c:61-81, 202-262). */
+typedef struct harm_grid_spec {
+  int n1, n2, n3;
+  double a;       /* spin */
+  double Rin;     /* inner radius of the grid */
+  double Rout;    /* outer radius of the grid */
+  double R0;      /* radial offset of the exponential map */
+  double hslope;  /* theta concentration */
+} harm_grid_spec;
+
+/* Fishbone-Moncrief torus (init.c:70-472). */
+typedef struct harm_torus_spec {
+  double rin;    /* torus inner edge */
+  double rmax;   /* radius of pressure maximum */
+  double kappa;  /* polytropic constant */
+  double beta;   /* target gas-to-magnetic pressure ratio */
+} harm_torus_spec;
+
+/* Per-step diagnostics (diag.c:437-580) and the first recorded failure. */
+typedef struct harm_diag {
+  double mdot, edot, ldot;
+  double mdot_in, mdot_out, mass_curr;
+  double mass_in, mass_out;
+  double ndt;       /* Courant time step proposed by the corrector */
+  int fail_code;    /* 0, or the fail() code the reference would exit with */
+  int fail_h, fail_i, fail_j;
+} harm_diag;
+
+const char *harm_last_error(void);
+
+/* ---- host-side grid set-up (CPU only; no device needed) ---- */
+
+/* set_points() (coord.c:202-262): dx[] and startx[] of the grid. */
+int harm_set_points(const harm_grid_spec *g, double dx[4], double startx[4]);
+
+/* set_grid() (main.c:413-520): metric, inverse metric, sqrt(-g), connection
+   and Boyer-Lindquist coordinates on the whole 2D (r, theta) grid. */
+int harm_set_grid(const harm_grid_spec *g, const double dx[4], const double startx[4],
+                  double *gcov, double *gcon, double *gdet, double *conn, double *coords);
+
+/* set_Katm() (fixup.c:555-585): entropy constant of the floor state per radius. */
+int harm_set_katm(const harm_grid_spec *g, double gam, const double *coords, double *katm);
+
+/* ---- device context: state resident on one GPU ---- */
+
+typedef struct harm_ctx harm_ctx;
+
+/* Allocate the device state for one grid and upload its geometry.
+   Replaces the reference's set_arrays()/set_grid() storage (main.c:288-520). */
+int harm_create(const harm_params *prm, const double *gcov, const double *gcon,
+                const double *gdet, const double *conn, const double *coords,
+                const double *katm, int device, harm_ctx **out);
+void harm_destroy(harm_ctx *ctx);
+
+/* Fishbone-Moncrief torus with a normalised poloidal loop, as init() builds it
+   (init.c:70-472), left resident on the device; sets t = 0, dt = 1e-5 and the
+   mass counters as main() does after init (main.c:166-182). */
+int harm_init_torus(harm_ctx *ctx, const harm_grid_spec *g, const harm_torus_spec *torus);
+
+/* Copy primitives (and optionally pflag) between host and device, reference layout. */
+int harm_put_prims(harm_ctx *ctx, const double *p, const signed char *pflag);
+int harm_get_prims(harm_ctx *ctx, double *p, signed char *pflag);
+
+int harm_set_time(harm_ctx *ctx, double t, double dt);
+int harm_get_time(harm_ctx *ctx, double *t, double *dt);
+int harm_set_mass(harm_ctx *ctx, double mass_in, double mass_out);
+int harm_get_diag(harm_ctx *ctx, harm_diag *d);
+
+/* step_ch() (step_ch.c:90-140): predictor to dt/2, floors, boundaries,
+   failure repair, corrector to dt, the same again, mass diagnostics and the
+   next dt.  Asynchronous on the context's stream; returns after launch. */
+int harm_step_ch(harm_ctx *ctx);
+
+/* n steps captured once into a CUDA graph and replayed; synchronises at the end
+   and returns HARM_E_DT if any step met dt < 1e-9. */
+int harm_run(harm_ctx *ctx, int nsteps);
+
+/* step_ch() on host primitives: upload p, one step, download p.  The call a
+   host that owns its primitive array (the reference's _p) makes per step. */
+int harm_step_ch_host(harm_ctx *ctx, double *p);
+
+/* ---- device-timed variants (CUDA events on the context's stream) ---- */
+
+/* harm_run() with the elapsed device time of the n graph launches in *ms. */
+int harm_run_timed(harm_ctx *ctx, int nsteps, double *ms);
+
+/* nsteps of harm_step_ch_host() (upload, step, download per step, p in
+   pinned host memory) with the elapsed device time in *ms. */
+int harm_step_ch_host_timed(harm_ctx *ctx, double *p, int nsteps, double *ms);
+
+/* Average device time per launch of the step's kernels, each launched reps
+   times on its own, into ms[HARM_NKERNELS] in this order: flux (all three
+   directions), update (flux-CT + source + inversion + floors), bound_prim,
+   fixup_utoprim (flag flip + repair), mass diagnostics.  The state is left as
+   it was. */
+#define HARM_NKERNELS 5
+int harm_time_kernels(harm_ctx *ctx, int reps, double *ms);
+
+/* Block until the context's stream is idle; returns any pending device error. */
+int harm_sync(harm_ctx *ctx);
+
+/* ---- the reference's per-array entry points, on host arrays of the context's shape ---- */
+
+int harm_fixup(harm_ctx *ctx, double *pv);                        /* fixup.c:51-60, decs.h:567 */
+int harm_bound_prim(harm_ctx *ctx, double *pv);                   /* bounds.c:54, decs.h:548 */
+int harm_fixup_utoprim(harm_ctx *ctx, double *pv);                /* fixup.c:432, decs.h:569 */
+
+/* Utoprim_2d() (utoprim_2d.c:126, decs.h:608) over n independent zones on the
+   device: U[n][8], gcov[n][16], gcon[n][16], gdet[n], prim[n][8] (guess in,
+   result out), ret[n] (the reference's return code).  Host arrays. */
+int harm_utoprim_2d_batch(const double *U, const double *gcov, const double *gcon,
+                          const double *gdet, double *prim, int *ret, long n, double gam);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -151,6 +151,24 @@ int ref_utoprim_2d(double *U, int i, int j, double *prim)
   return Utoprim_2d(U, geom.gcov, geom.gcon, geom.g, prim);
 }
 
+int ref_utoprim_fix(double *U, int i, int j, double *prim, double K, int which)
+{
+  struct of_geom geom;
+  get_geometry(0, i, j, CENT, &geom);
+  if (which == 1) return Utoprim_1dvsq2fix1(U, geom.gcov, geom.gcon, geom.g, prim, K);
+  return Utoprim_1dfix1(U, geom.gcov, geom.gcon, geom.g, prim, K);
+}
+
+/* conserved variables of a primitive state at zone (i, j), CENT (phys.c:99-105) */
+void ref_prim_to_U(double *pr, int i, int j, double *U)
+{
+  struct of_geom geom;
+  struct of_state q;
+  get_geometry(0, i, j, CENT, &geom);
+  get_state(pr, &geom, &q);
+  primtoU(pr, &q, &geom, U);
+}
+
 void ref_fixup(double *pv) { fixup(pv); }
 void ref_bound_prim(double *pv) { bound_prim(pv); }
 void ref_fixup_utoprim(double *pv) { fixup_utoprim(pv); }

@@ -1,0 +1,186 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle and the fixtures.
+
+The FP64 path is built with -fmad=false and keeps the reference's
+expression order, so it is expected to agree bit for bit with the
+reference.  The contract bound is 1e-12 relative per primitive after one step
+(relative to the field's largest magnitude on the grid); the tests assert
+that bound and also record how many zones agree exactly."""
+import numpy as np
+import pytest
+
+from helpers import active, field_rel_err, full_state, l1_rel, load_fixture, make_oracle, problem_from_fixture
+
+pytestmark = pytest.mark.gpu
+TOL_STEP = 1e-12
+
+
+@pytest.fixture(scope="module")
+def hc(harm_lib):
+    import harm_cool_b200
+    return harm_cool_b200
+
+
+@pytest.mark.parametrize("cfg", ["t2d", "t3d"])
+def test_init_torus_matches_reference(cfg, hc):
+    fx = load_fixture(cfg)
+    pr = problem_from_fixture(fx)
+    ctx = hc.Context(pr)
+    ctx.init_torus()
+    p, fl = ctx.get_prims(with_flags=True)
+    err = field_rel_err(active(pr, p), fx["p0"])
+    assert np.all(err <= 1e-14), err
+    assert ctx.time() == tuple(fx["t0"])
+
+
+@pytest.mark.parametrize("cfg", ["t2d", "t3d"])
+def test_steps_match_reference_fixtures(cfg, hc, oracle_built):
+    fx = load_fixture(cfg)
+    pr = problem_from_fixture(fx)
+    ctx = hc.Context(pr)
+    ctx.put_prims(full_state(pr, fx["p0"]), full_state(pr, fx["pflag0"]))
+    ctx.set_time(*fx["t0"])
+    done = 0
+    for n in (1, 2, 5):
+        while done < n:
+            ctx.step_ch()
+            done += 1
+        ctx.sync()
+        p, fl = ctx.get_prims(with_flags=True)
+        err = field_rel_err(active(pr, p), fx["p%d" % n])
+        assert np.all(err <= TOL_STEP * n), (n, err)
+        assert np.array_equal(active(pr, fl), fx["pflag%d" % n])
+        t, dt = ctx.time()
+        assert abs(t - fx["t%d" % n][0]) <= 1e-15 * abs(t) and abs(dt - fx["t%d" % n][1]) <= 1e-12 * dt
+        d = ctx.diag()
+        assert d["fail_code"] == 0
+        assert abs(d["mass_curr"] - fx["diag%d" % n][5]) <= 1e-13 * abs(fx["diag%d" % n][5])
+
+
+def run_both(hc, pr, nsteps):
+    """Same initial state (the GPU's init) on the GPU and on the oracle; nsteps each."""
+    ctx = hc.Context(pr)
+    ctx.init_torus()
+    p0, f0 = ctx.get_prims(with_flags=True)
+    o = make_oracle(pr)
+    o.p[...] = p0
+    o.pflag[...] = f0
+    o.set_time(*ctx.time())
+    ctx.run(nsteps)
+    for _ in range(nsteps):
+        assert o.step() == 0
+    p, fl = ctx.get_prims(with_flags=True)
+    return ctx, o, active(pr, p), active(pr, o.p), active(pr, fl), active(pr, o.pflag)
+
+
+def test_config1_first_step_and_100_steps(hc, oracle_built):
+    """128x128 torus: one step at 1e-12, then 100 steps with the L1 error stated."""
+    pr = hc.torus_problem(128, 128, 1)
+    ctx, o, g, c, fg, fc = run_both(hc, pr, 1)
+    err = field_rel_err(g, c)
+    assert np.all(err <= TOL_STEP), err
+    exact = np.mean(g == c)
+    print("config-1 step 1: max field-relative error per primitive", err, "exact fraction", exact)
+    ctx.run(99)
+    for _ in range(99):
+        assert o.step() == 0
+    g = active(pr, ctx.get_prims())
+    c = active(pr, o.p)
+    l1 = l1_rel(g, c)
+    print("config-1 after 100 steps: L1 relative error per primitive", l1)
+    assert np.all(l1 <= 1e-10), l1
+    assert ctx.diag()["fail_code"] == 0
+
+
+def test_3d_steps_match_oracle(hc, oracle_built):
+    pr = hc.torus_problem(32, 32, 8)
+    ctx, o, g, c, fg, fc = run_both(hc, pr, 3)
+    err = field_rel_err(g, c)
+    assert np.all(err <= 3 * TOL_STEP), err
+    assert np.array_equal(fg, fc)
+
+
+def _state_after_steps(hc, pr, n):
+    ctx = hc.Context(pr)
+    ctx.init_torus()
+    ctx.run(n)
+    return ctx
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 1), (16, 16, 4)])
+def test_bound_prim_and_fixup_match_oracle(shape, hc, oracle_built):
+    pr = hc.torus_problem(*shape)
+    ctx = _state_after_steps(hc, pr, 3)
+    p, fl = ctx.get_prims(with_flags=True)
+    rng = np.random.default_rng(7)
+    q = p.copy()
+    q[..., :5] *= 1. + 1e-2 * rng.standard_normal(q[..., :5].shape)
+    q[..., 0] = np.where(rng.random(q.shape[:3]) < 0.05, 1e-12, q[..., 0])   # below the floors
+    o = make_oracle(pr)
+    o.pflag[...] = fl
+    for name in ("fixup", "bound_prim"):
+        a = q.copy()
+        b = q.copy()
+        getattr(ctx, name)(a)
+        from oracle.pyoracle import oracle_lib
+        import ctypes
+        getattr(oracle_lib(), "ora_" + name)(o.h, b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        np.testing.assert_array_equal(active(pr, a), active(pr, b), err_msg=name)
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 1), (16, 16, 4)])
+def test_fixup_utoprim_repairs_like_oracle(shape, hc, oracle_built):
+    """Injected failure flags, including neighbouring failures that need the
+    last-resort average and so depend on the repair order."""
+    import ctypes
+    from oracle.pyoracle import oracle_lib
+    pr = hc.torus_problem(*shape)
+    ctx = _state_after_steps(hc, pr, 2)
+    p = ctx.get_prims()
+    fl = np.zeros(pr.shape, dtype=np.int8)
+    rng = np.random.default_rng(11)
+    act = active(pr, fl)
+    n1, n2 = pr.params.n1, pr.params.n2
+    for _ in range(40):
+        h = rng.integers(0, act.shape[0])
+        i = rng.integers(2, n1 + 2)
+        j = rng.integers(2, n2 + 2)
+        act[h, i, j] = 1
+        if rng.random() < 0.4:   # clusters
+            act[h, min(i + 1, n1 + 1), j] = 1
+            act[h, i, min(j + 1, n2 + 1)] = 101
+    a = p.copy()
+    b = p.copy()
+    # the reference flips the flags of bound_prim'd arrays; set ghosts as bound_prim would
+    ctx.put_prims(p, fl)
+    ctx.bound_prim(a)
+    o = make_oracle(pr)
+    o.pflag[...] = fl
+    lib = oracle_lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.ora_bound_prim(o.h, b.ctypes.data_as(dp))
+    np.testing.assert_array_equal(active(pr, a), active(pr, b))
+    ctx.put_prims(a, o.pflag.copy())
+    ctx.lib.harm_fixup_utoprim(ctx.h, a.ctypes.data_as(dp))
+    lib.ora_fixup_utoprim(o.h, b.ctypes.data_as(dp))
+    np.testing.assert_array_equal(active(pr, a), active(pr, b))
+    _, fg = ctx.get_prims(with_flags=True)
+    np.testing.assert_array_equal(active(pr, fg), active(pr, o.pflag))
+
+
+def test_utoprim_batch_matches_reference_kat(hc):
+    import os
+    from helpers import GOLDEN
+    kat = dict(np.load(os.path.join(GOLDEN, "kat_u2p.npz")))
+    fx = load_fixture("t2d")
+    pr = problem_from_fixture(fx)
+    g = pr.geometry
+    ij = kat["ij"]
+    gcov = np.stack([g["gcov"][i, j, 3].ravel() for i, j in ij])
+    gcon = np.stack([g["gcon"][i, j, 3].ravel() for i, j in ij])
+    gdet = np.array([g["gdet"][i, j, 3] for i, j in ij])
+    prim = kat["guess"].copy()
+    ret = hc.utoprim_2d_batch(kat["U"], gcov, gcon, gdet, prim, float(kat["gam"]))
+    np.testing.assert_array_equal(ret, kat["ret_2d"])
+    ok = ret == 0
+    err = np.max(np.abs(prim[ok] - kat["prim_2d"][ok]) / np.maximum(np.abs(kat["prim_2d"][ok]), 1e-300))
+    assert err <= 1e-13, err
