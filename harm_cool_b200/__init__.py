@@ -298,7 +298,7 @@ class Context:
         _check(self.lib.harm_step_ch_host_timed(self.h, _dp(p), nsteps, ctypes.byref(ms)))
         return ms.value
 
-    KERNELS = ("flux", "update", "bound_prim", "fixup_utoprim", "diag_mass")
+    KERNELS = ("flux", "update", "bound_prim", "fixup_utoprim", "diag")
 
     def time_kernels(self, reps=5):
         """Average device ms per launch of each step kernel, launched on its own."""

@@ -1504,55 +1504,57 @@ extern "C" int harm_time_kernels(harm_ctx *h, int reps, double *ms)
   if (!h || !ms || reps < 1) return fail_with(HARM_E_ARG, "bad argument");
   Ctx *x = &h->x;
   const Grid &G = x->G;
-  DevScalars saved;
-  int rc = read_scalars(x, &saved);
-  if (rc) return rc;
-  // work on copies so the state is untouched: ph <- p, scratch output in stage
-  const size_t st = 8 * G.nc * sizeof(double);
-  double *scratch = x->stage;
-  CK(cudaMemcpyAsync(x->ph, x->p, st, cudaMemcpyDeviceToDevice, x->stream));
-  std::vector<signed char> flags((size_t)G.nc);
-  CK(cudaMemcpyAsync(flags.data(), x->pflag, G.nc, cudaMemcpyDeviceToHost, x->stream));
-  CK(cudaStreamSynchronize(x->stream));
-  EventPair e;
-  CK(cudaEventCreate(&e.a));
-  CK(cudaEventCreate(&e.b));
+  // reps ordinary steps, launched one kernel at a time with an event after
+  // each, so every kernel is timed inside the sequence it runs in
+  const int nev = 16;
+  std::vector<cudaEvent_t> ev(nev);
+  for (auto &e : ev) CK(cudaEventCreate(&e));
+  double acc[HARM_NKERNELS] = {0, 0, 0, 0, 0};
   dim3 fb(32, 4), fg((G.sn2 - 2 + 31) / 32, (G.sn1 - 2 + 3) / 4, G.n3);
-  for (int kk = 0; kk < HARM_NKERNELS; kk++) {
-    // one untimed launch, then reps timed launches
-    for (int r = 0; r <= reps; r++) {
-      if (r == 1) CK(cudaEventRecord(e.a, x->stream));
-      switch (kk) {
-      case 0:
-        k_flux<true><<<fg, fb, 0, x->stream>>>(G, x->ph, x->F1, x->F2, x->F3, x->geo, x->sc);
-        break;
-      case 1:
-        if (G.n3 > 1)
-          k_update<true, true><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(
-              G, x->p, x->ph, scratch, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm, x->sc);
-        else
-          k_update<true, false><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(
-              G, x->p, x->ph, scratch, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm, x->sc);
-        break;
-      case 2:
-        launch_bound(x, x->ph);
-        break;
-      case 3:
-        launch_fixup_utoprim(x, x->ph);
-        break;
-      case 4:
-        k_diag_mass<<<x->nparts, 256, 0, x->stream>>>(G, x->ph, x->geo, x->partials, x->nparts, x->sc);
-        break;
+  int rc = HARM_OK;
+  for (int r = 0; r < reps && rc == HARM_OK; r++) {
+    int e = 0;
+    // slot of each interval: 0 flux, 1 update, 2 bound, 3 fixup_utoprim, 4 diag
+    int slot[nev];
+    CK(cudaEventRecord(ev[e++], x->stream));
+    for (int half = 0; half < 2; half++) {
+      const bool full = half == 1;
+      double *pi = x->p, *pb = full ? x->ph : x->p, *pf = full ? x->p : x->ph;
+      if (full) k_flux<true><<<fg, fb, 0, x->stream>>>(G, pb, x->F1, x->F2, x->F3, x->geo, x->sc);
+      else k_flux<false><<<fg, fb, 0, x->stream>>>(G, pb, x->F1, x->F2, x->F3, x->geo, x->sc);
+      slot[e] = 0; CK(cudaEventRecord(ev[e++], x->stream));
+      if (G.n3 > 1) {
+        if (full) k_update<true, true><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, pf, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm, x->sc);
+        else k_update<false, true><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, pf, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm, x->sc);
+      } else {
+        if (full) k_update<true, false><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, pf, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm, x->sc);
+        else k_update<false, false><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, pf, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm, x->sc);
       }
+      slot[e] = 1; CK(cudaEventRecord(ev[e++], x->stream));
+      if (full) {
+        k_diag_flux<<<1, 1024, 0, x->stream>>>(G, x->F1, x->sc);
+        slot[e] = 4; CK(cudaEventRecord(ev[e++], x->stream));
+      }
+      launch_bound(x, pf);
+      slot[e] = 2; CK(cudaEventRecord(ev[e++], x->stream));
+      launch_fixup_utoprim(x, pf);
+      slot[e] = 3; CK(cudaEventRecord(ev[e++], x->stream));
+      launch_bound(x, pf);
+      slot[e] = 2; CK(cudaEventRecord(ev[e++], x->stream));
     }
-    CK(cudaEventRecord(e.b, x->stream));
-    CK(cudaEventSynchronize(e.b));
-    float f;
-    CK(cudaEventElapsedTime(&f, e.a, e.b));
-    ms[kk] = f / reps;
+    k_diag_mass<<<x->nparts, 256, 0, x->stream>>>(G, x->p, x->geo, x->partials, x->nparts, x->sc);
+    k_finalize<<<1, 1024, 0, x->stream>>>(G, x->partials, x->nparts, x->sc);
+    slot[e] = 4; CK(cudaEventRecord(ev[e++], x->stream));
+    CK(cudaEventSynchronize(ev[e - 1]));
+    for (int k = 1; k < e; k++) {
+      float f;
+      CK(cudaEventElapsedTime(&f, ev[k - 1], ev[k]));
+      acc[slot[k]] += f;
+    }
   }
-  CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(x->pflag, flags.data(), G.nc, cudaMemcpyHostToDevice, x->stream));
-  CK(cudaStreamSynchronize(x->stream));
-  return write_scalars(x, &saved);
+  for (auto &e : ev) cudaEventDestroy(e);
+  // per launch: flux and update launch twice per step, bound 4x, fixup_utoprim 2x
+  const double per_step[HARM_NKERNELS] = {2, 2, 4, 2, 1};
+  for (int k = 0; k < HARM_NKERNELS; k++) ms[k] = acc[k] / (reps * per_step[k]);
+  return harm_sync(h);
 }

@@ -141,11 +141,12 @@ int harm_run_timed(harm_ctx *ctx, int nsteps, double *ms);
    pinned host memory) with the elapsed device time in *ms. */
 int harm_step_ch_host_timed(harm_ctx *ctx, double *p, int nsteps, double *ms);
 
-/* Average device time per launch of the step's kernels, each launched reps
-   times on its own, into ms[HARM_NKERNELS] in this order: flux (all three
-   directions), update (flux-CT + source + inversion + floors), bound_prim,
-   fixup_utoprim (flag flip + repair), mass diagnostics.  The state is left as
-   it was. */
+/* Runs reps ordinary steps launched kernel by kernel with a CUDA event after
+   each, and returns the average device time per launch of each kind, into
+   ms[HARM_NKERNELS] in this order: flux (all three directions), update
+   (flux-CT + source + inversion + floors), bound_prim, fixup_utoprim (flag
+   flip + repair), diagnostics (flux and mass sums, next dt, per step).  The
+   state advances by reps steps. */
 #define HARM_NKERNELS 5
 int harm_time_kernels(harm_ctx *ctx, int reps, double *ms);
 
