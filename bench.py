@@ -30,7 +30,14 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-KERNELS_PER_STEP = 15  # predictor 6 + corrector 7 + mass diagnostics + finalize
+
+
+def kernels_per_step(n3):
+    """Kernel launches of one step: per half step one flux kernel per direction,
+    update, bound_prim, flag flip, repair, bound_prim; the corrector adds the
+    flux diagnostics; then the mass diagnostics and the dt update."""
+    nflux = 3 if n3 > 1 else 2
+    return 2 * (nflux + 5) + 1 + 2
 STATE_BYTES_PER_ZONE_CYCLE = 320  # p read twice, ph written and read, p written; 8 FP64 prims
 
 
@@ -194,7 +201,7 @@ def run_ours(args, world, rank, local):
                        "parallelism": "replicas" if world > 1 else "single", "l2": "state > L2, no flush"},
             "e2e": {"value": e2e, "unit": "zone-cycles/s", "h2d_bytes_per_step": bytes_host,
                     "d2h_bytes_per_step": bytes_host, "path": "harm_step_ch_host (upload, step, download)"},
-            "gpu_launches": KERNELS_PER_STEP * args.steps,
+            "gpu_launches": kernels_per_step(args.n3) * args.steps,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                          "peak_source": peak_kind,

@@ -84,6 +84,7 @@ _SIGNATURES = {
     "harm_get_time": (ctypes.c_int, [ctypes.c_void_p, _DP, _DP]),
     "harm_set_mass": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]),
     "harm_get_diag": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Diag)]),
+    "harm_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "harm_step_ch": (ctypes.c_int, [ctypes.c_void_p]),
     "harm_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "harm_step_ch_host": (ctypes.c_int, [ctypes.c_void_p, _DP]),
@@ -276,6 +277,12 @@ class Context:
         d = Diag()
         _check(self.lib.harm_get_diag(self.h, ctypes.byref(d)))
         return d.as_dict()
+
+    FP64, MIXED = 0, 1
+
+    def set_precision(self, mode):
+        """Context.FP64 (default, bit-compatible with the reference) or Context.MIXED."""
+        _check(self.lib.harm_set_precision(self.h, mode))
 
     def step_ch(self):
         """One full step (step_ch.c:90-140), asynchronous; see sync()."""

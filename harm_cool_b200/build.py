@@ -30,6 +30,14 @@ def _run(cmd):
     return r.stdout + r.stderr
 
 
+# translation unit -> extra nvcc flags
+UNITS = {
+    "harm_api.cu": ["-fmad=false"],     # shared kernels and the C ABI
+    "harm_exact.cu": ["-fmad=false"],   # the FP64 step, bit-compatible with the reference
+    "harm_mixed.cu": ["-fmad=true"],    # the mixed-precision step
+}
+
+
 def build(force=False, verbose=False):
     """Compile the library if any source is newer than it; return its path."""
     if (not force and os.path.exists(LIB)
@@ -40,14 +48,17 @@ def build(force=False, verbose=False):
     host_o = os.path.join(BUILD, "host_setup.o")
     _run(["g++", "-O2", "-ffp-contract=off", "-fPIC", "-std=c++17", "-c",
           os.path.join(CSRC, "host_setup.cpp"), "-o", host_o] + inc)
-    kern_o = os.path.join(BUILD, "harm_kernels.o")
-    out = _run([NVCC] + ARCH + ["-O3", "-fmad=false", "-lineinfo", "-std=c++17",
-                                "-Xptxas", "-v", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
-                                "-c", os.path.join(CSRC, "harm_kernels.cu"), "-o", kern_o] + inc)
-    if verbose:
-        print(out)
+    objs = [host_o]
+    for unit, flags in UNITS.items():
+        o = os.path.join(BUILD, unit.replace(".cu", ".o"))
+        out = _run([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xptxas", "-v", "-Xcompiler", "-fPIC",
+                                    "-Xcompiler", "-ffp-contract=off", "-c", os.path.join(CSRC, unit),
+                                    "-o", o] + flags + inc)
+        if verbose:
+            print(out)
+        objs.append(o)
     tmp = LIB + ".tmp"
-    _run([NVCC] + ARCH + ["-shared", "-o", tmp, kern_o, host_o, "-lcudart"])
+    _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"])
     os.replace(tmp, LIB)
     return LIB
 

@@ -1,4 +1,6 @@
-// B200 kernels and C ABI for HARM-COOL's step_ch() path.
+// Kernels shared by both precision variants (boundaries, failure repair,
+// diagnostics, layout conversion, set-up helpers) and the C ABI of
+// libharm_b200.  Built with -fmad=false.
 //
 // Device layout.  The reference keeps each primitive array as
 // p[SN3][SN1][SN2][8] on the host.  On the device every array is stored
@@ -12,9 +14,9 @@
 // connection planes and two floor planes.
 //
 // One step (step_ch.c:90-140) is, on one stream and without host sync:
-//   predictor : k_flux, k_update(dt/2) [flux-CT, source, inversion, floors],
+//   predictor : k_flux x3, k_update(dt/2) [flux-CT, source, inversion, floors],
 //               k_bound, k_fu_flip, k_fu_fix, k_bound
-//   corrector : k_flux (+Courant minima), k_update(dt), k_diag_flux,
+//   corrector : k_flux x3 (+Courant minima), k_update(dt), k_diag_flux,
 //               k_bound, k_fu_flip, k_fu_fix, k_bound
 //   k_diag_mass, k_finalize (diagnostic sums, next dt)
 #include <cuda_runtime.h>
@@ -25,445 +27,9 @@
 #include <string>
 #include <vector>
 
-#include "harm_b200.h"
-#include "harm_phys.cuh"
-#include "host_setup.h"
+#include "harm_common.cuh"
 
 namespace harm {
-
-// ---------------------------------------------------------------------------
-// device-side run state
-
-struct DevScalars {
-  double t, dt;
-  unsigned long long ndt_bits[3];  // per-direction Courant minima (bits of positive doubles)
-  double mdot, edot, ldot, mdot_in, mdot_out, mass_curr, mass_in, mass_out, ndt;
-  double bsq_max;                  // torus set-up only
-  unsigned long long bsq_bits;
-  int fail_code, fail_h, fail_i, fail_j;
-  int err;                         // HARM_E_DT when dt < 1e-9
-  int halted;                      // set after a failure: later steps do nothing
-  int nfail, fail_overflow;        // failed zones met by the current fixup_utoprim
-};
-
-// Problem description passed by value to every kernel.
-struct Grid {
-  int n1, n2, n3, sn1, sn2;
-  int istart, istop, jstart, jstop;
-  long ng;   // sn1*sn2, points per geometry plane
-  long nc;   // n3*sn1*sn2, cells per state plane
-  int lim;
-  double gam, cour, defcon, tf;
-  double dx1, dx2, dx3;
-};
-
-constexpr int FAIL_CAP = 8192;  // failed zones repaired through the sorted list
-constexpr int NTHR_FIX = 1024;
-
-struct Ctx {
-  Grid G;
-  Dims D;
-  harm_params prm;
-  int device;
-  cudaStream_t stream;
-  double *p, *ph;                // [8][nc]
-  double *F1, *F2, *F3;          // [8][nc]
-  signed char *pflag;            // [nc]
-  double *geo;                   // [4 locations][GEO_N][ng]: FACE1, FACE2, FACE3, CENT
-  double *conn;                  // [40][ng]
-  double *floors;                // [2][ng]
-  double *katm;                  // [sn1]
-  double *stage;                 // [8*nc] host-layout staging
-  signed char *stage_flag;       // [sn3*sn1*sn2]
-  int *fail_list;                // [FAIL_CAP]
-  double *fix_buf;               // [FAIL_CAP*8]
-  double *partials;              // [3][nparts]
-  int nparts;
-  DevScalars *sc;
-  cudaGraphExec_t graph_exec;
-  int graph_steps;
-  double *pinned;                // pinned host buffer for the host-array entry points
-  size_t pinned_bytes;
-};
-
-__device__ __forceinline__ void record_fail(DevScalars *sc, int code, int h, int i, int j)
-{
-  if (atomicCAS(&sc->fail_code, 0, code) == 0) {
-    sc->fail_h = h;
-    sc->fail_i = i;
-    sc->fail_j = j;
-  }
-}
-
-__device__ __forceinline__ long cidx(const Grid &G, int h, int i, int j)
-{
-  return ((long)h * G.sn1 + i) * G.sn2 + j;
-}
-
-__device__ __forceinline__ int hwrap(const Grid &G, int h)
-{
-  return h < 0 ? h + G.n3 : (h >= G.n3 ? h - G.n3 : h);
-}
-
-// geometry location slots on the device
-enum { L_FACE1 = 0, L_FACE2 = 1, L_FACE3 = 2, L_CENT = 3 };
-
-__device__ __forceinline__ const double *geo_at(const double *geo, const Grid &G, int loc)
-{
-  return geo + (long)loc * GEO_N * G.ng;
-}
-
-// ---------------------------------------------------------------------------
-// fluxes (step_ch.c:331-504): one thread per zone, its lower face in each
-// direction; slopes (interp.c:49-93) recomputed from the primitives
-
-__device__ void face_flux(double gam, int dir, const double *pl, const double *pr, const Geo &q, double *F,
-                          double &ctop, int *fail)
-{
-  State s;
-  double Fl[8], Ul[8], Fr[8], Ur[8], cmaxl, cminl, cmaxr, cminr;
-  get_state(pl, q, s, fail);
-  primtoflux(gam, pl, s, dir, q.g, Fl);
-  primtoflux(gam, pl, s, 0, q.g, Ul);
-  vchar(gam, pl, s, q, dir, cmaxl, cminl, fail);
-  get_state(pr, q, s, fail);
-  primtoflux(gam, pr, s, dir, q.g, Fr);
-  primtoflux(gam, pr, s, 0, q.g, Ur);
-  vchar(gam, pr, s, q, dir, cmaxr, cminr, fail);
-  double t1 = 0. > cmaxl ? 0. : cmaxl;
-  double cmax = fabs(t1 > cmaxr ? t1 : cmaxr);
-  double t2 = 0. > -cminl ? 0. : -cminl;
-  double cmin = fabs(t2 > -cminr ? t2 : -cminr);
-  ctop = cmax > cmin ? cmax : cmin;
-  // HLLF = 0, LAXF = 1 (step_ch.c:66-67): the local Lax-Friedrichs flux
-#pragma unroll
-  for (int k = 0; k < 8; k++) F[k] = 0.5 * (Fl[k] + Fr[k] - ctop * (Ur[k] - Ul[k]));
-}
-
-__device__ __forceinline__ double warp_min(double v)
-{
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-
-__device__ __forceinline__ double warp_sum(double v)
-{
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-template <bool FULL>
-__global__ void __launch_bounds__(128) k_flux(Grid G, const double *__restrict__ pb, double *__restrict__ F1,
-                                              double *__restrict__ F2, double *__restrict__ F3,
-                                              const double *__restrict__ geo, DevScalars *sc)
-{
-  if (sc->halted) return;
-  const int j = 1 + blockIdx.x * blockDim.x + threadIdx.x;  // theta, [jstart-1, jstop+1]
-  const int i = 1 + blockIdx.y * blockDim.y + threadIdx.y;  // r, [istart-1, istop+1]
-  const int h = blockIdx.z;
-  double dtmin[3] = {1.e9, 1.e9, 1.e9};
-  int fail = 0;
-  const bool in = (i <= G.sn1 - 2) && (j <= G.sn2 - 2);
-  if (in) {
-    const long c = cidx(G, h, i, j);
-    const long gi = (long)i * G.sn2 + j;
-    const bool active = i >= G.istart && i <= G.istop && j >= G.jstart && j <= G.jstop;
-    const int ndir = G.n3 > 1 ? 3 : 2;
-    for (int dir = 1; dir <= ndir; dir++) {
-      double *F = dir == 1 ? F1 : dir == 2 ? F2 : F3;
-      if (dir == 1 && i < G.istart) continue;
-      if (dir == 2 && j < G.jstart) continue;
-      if (dir == 2 && (j == G.jstart || j == G.jstop + 1)) {
-        // polar faces carry no flux (step_ch.c:412-416)
-#pragma unroll
-        for (int k = 0; k < 8; k++) F[k * G.nc + c] = 0.;
-        continue;
-      }
-      long o1, o2, o3;  // offsets of zone-2d, zone-d, zone+d
-      if (dir == 1) { o1 = c - 2 * G.sn2; o2 = c - G.sn2; o3 = c + G.sn2; }
-      else if (dir == 2) { o1 = c - 2; o2 = c - 1; o3 = c + 1; }
-      else {
-        o1 = cidx(G, hwrap(G, h - 2), i, j);
-        o2 = cidx(G, hwrap(G, h - 1), i, j);
-        o3 = cidx(G, hwrap(G, h + 1), i, j);
-      }
-      double pl[8], pr[8];
-#pragma unroll
-      for (int k = 0; k < 8; k++) {
-        const double *P = pb + k * G.nc;
-        double a = __ldg(P + o1), b = __ldg(P + o2), z = __ldg(P + c), e = __ldg(P + o3);
-        pl[k] = b + 0.5 * slope_lim(G.lim, a, b, z);
-        pr[k] = z - 0.5 * slope_lim(G.lim, b, z, e);
-      }
-      Geo q;
-      load_geo(geo_at(geo, G, dir == 1 ? L_FACE1 : dir == 2 ? L_FACE2 : L_FACE3), G.ng, gi, q);
-      double Fz[8], ctop;
-      face_flux(G.gam, dir, pl, pr, q, Fz, ctop, &fail);
-#pragma unroll
-      for (int k = 0; k < 8; k++) F[k * G.nc + c] = Fz[k];
-      if (FULL && active) {
-        double dxd = dir == 1 ? G.dx1 : dir == 2 ? G.dx2 : G.dx3;
-        double dtij = G.cour * dxd / ctop;
-        if (dtij < dtmin[dir - 1]) dtmin[dir - 1] = dtij;
-      }
-    }
-    if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
-  }
-  if (FULL) {
-    __shared__ double red[3][4];
-    const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31, warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      double v = warp_min(dtmin[d]);
-      if (lane == 0) red[d][warp] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-      for (int d = 0; d < 3; d++) {
-        double v = fmin(fmin(red[d][0], red[d][1]), fmin(red[d][2], red[d][3]));
-        if (v < 1.e9) atomicMin(&sc->ndt_bits[d], (unsigned long long)__double_as_longlong(v));
-      }
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// update (step_ch.c:237-306) fused with flux_ct (step_ch.c:514-629, 726-798),
-// the flux boundary fixes (coord.c:264-324) and fixup() (fixup.c:51-60)
-
-struct Flux {
-  const double *F1, *F2, *F3;
-  Grid G;
-  __device__ double raw(int d, int k, int h, int i, int j) const
-  {
-    const double *F = d == 1 ? F1 : d == 2 ? F2 : F3;
-    return __ldg(F + k * G.nc + cidx(G, h, i, j));
-  }
-  // B-component of a raw face flux after fix_flux's polar reflection
-  // (coord.c:284-301): F1,F3[B2] at jstart-1 / jstop+1 mirror jstart / jstop
-  __device__ double rawB2(int d, int h, int i, int j) const
-  {
-    if (j == G.jstart - 1) return -raw(d, B2, h, i, G.jstart);
-    if (j == G.jstop + 1) return -raw(d, B2, h, i, G.jstop);
-    return raw(d, B2, h, i, j);
-  }
-  // 2D EMF (step_ch.c:546-547)
-  __device__ double emf2(int i, int j) const
-  {
-    return 0.25 * (rawB2(1, 0, i, j) + rawB2(1, 0, i, j - 1) - raw(2, B1, 0, i, j) - raw(2, B1, 0, i - 1, j));
-  }
-  // 3D EMFs (step_ch.c:754-764); h-1 wraps (phi periodic)
-  __device__ double e1(int h, int i, int j) const
-  {
-    int hm = hwrap(G, h - 1);
-    return 0.25 * ((raw(2, B3, h, i, j) + raw(2, B3, hm, i, j)) - (rawB2(3, h, i, j) + rawB2(3, h, i, j - 1)));
-  }
-  __device__ double e2(int h, int i, int j) const
-  {
-    int hm = hwrap(G, h - 1);
-    return 0.25 * ((raw(3, B1, h, i, j) + raw(3, B1, h, i - 1, j)) - (raw(1, B3, h, i, j) + raw(1, B3, hm, i, j)));
-  }
-  __device__ double e3(int h, int i, int j) const
-  {
-    return 0.25 * ((rawB2(1, h, i, j) + rawB2(1, h, i, j - 1)) - (raw(2, B1, h, i, j) + raw(2, B1, h, i - 1, j)));
-  }
-};
-
-template <bool THREE_D>
-__device__ void zone_fluxes(const Flux &FX, int h, int i, int j, double *f1m, double *f1p, double *f2m,
-                            double *f2p, double *f3m, double *f3p)
-{
-  const Grid &G = FX.G;
-  const int hp = THREE_D ? hwrap(G, h + 1) : 0;
-#pragma unroll
-  for (int k = 0; k < 5; k++) {
-    f1m[k] = FX.raw(1, k, h, i, j);
-    f1p[k] = FX.raw(1, k, h, i + 1, j);
-    f2m[k] = FX.raw(2, k, h, i, j);
-    f2p[k] = FX.raw(2, k, h, i, j + 1);
-    if (THREE_D) {
-      f3m[k] = FX.raw(3, k, h, i, j);
-      f3p[k] = FX.raw(3, k, hp, i, j);
-    }
-  }
-  // no inflow of mass through the radial boundaries (coord.c:307-321)
-  if (i == G.istart && f1m[RHO] > 0) f1m[RHO] = 0;
-  if (i + 1 == G.istop + 1 && f1p[RHO] < 0) f1p[RHO] = 0;
-  if (!THREE_D) {
-    double eA = FX.emf2(i, j), eB = FX.emf2(i, j + 1), eC = FX.emf2(i + 1, j), eD = FX.emf2(i + 1, j + 1);
-    f1m[B1] = 0.;
-    f1m[B2] = 0.5 * (eA + eB);
-    f1m[B3] = FX.raw(1, B3, 0, i, j);
-    f1p[B1] = 0.;
-    f1p[B2] = 0.5 * (eC + eD);
-    f1p[B3] = FX.raw(1, B3, 0, i + 1, j);
-    f2m[B1] = -0.5 * (eA + eC);
-    f2m[B2] = 0.;
-    f2m[B3] = FX.raw(2, B3, 0, i, j);
-    f2p[B1] = -0.5 * (eB + eD);
-    f2p[B2] = 0.;
-    f2p[B3] = FX.raw(2, B3, 0, i, j + 1);
-  } else {
-    double e3a = FX.e3(h, i, j), e3b = FX.e3(h, i, j + 1), e3c = FX.e3(h, i + 1, j), e3d = FX.e3(h, i + 1, j + 1);
-    double e2a = FX.e2(h, i, j), e2b = FX.e2(hp, i, j), e2c = FX.e2(h, i + 1, j), e2d = FX.e2(hp, i + 1, j);
-    double e1a = FX.e1(h, i, j), e1b = FX.e1(hp, i, j), e1c = FX.e1(h, i, j + 1), e1d = FX.e1(hp, i, j + 1);
-    f1m[B1] = 0.;
-    f1m[B2] = 0.5 * (e3a + e3b);
-    f1m[B3] = -0.5 * (e2a + e2b);
-    f1p[B1] = 0.;
-    f1p[B2] = 0.5 * (e3c + e3d);
-    f1p[B3] = -0.5 * (e2c + e2d);
-    f2m[B1] = -0.5 * (e3a + e3c);
-    f2m[B2] = 0.;
-    f2m[B3] = 0.5 * (e1a + e1b);
-    f2p[B1] = -0.5 * (e3b + e3d);
-    f2p[B2] = 0.;
-    f2p[B3] = 0.5 * (e1c + e1d);
-    f3m[B1] = 0.5 * (e2a + e2c);
-    f3m[B2] = -0.5 * (e1a + e1c);
-    f3m[B3] = 0.;
-    f3p[B1] = 0.5 * (e2b + e2d);
-    f3p[B2] = -0.5 * (e1b + e1d);
-    f3p[B3] = 0.;
-  }
-}
-
-// source() (phys.c:165-207); conn stored as [k][min(nu,j)][max(nu,j)]
-__device__ __forceinline__ int conn_slot(int k, int a, int b)
-{
-  int lo = a < b ? a : b, hi = a < b ? b : a;
-  // pairs (lo,hi) with lo <= hi in row order: 00 01 02 03 11 12 13 22 23 33
-  int pair = lo == 0 ? hi : lo == 1 ? 3 + hi : lo == 2 ? 5 + hi : 9;
-  return k * 10 + pair;
-}
-
-__device__ void source(double gam, const double *pb, const Geo &q, const double *__restrict__ conn, long ng, long gi,
-                       double *dU, int *fail)
-{
-  State s;
-  get_state(pb, q, s, fail);
-  double mhd[4][4];
-#pragma unroll
-  for (int d = 0; d < 4; d++) mhd_calc(gam, pb, d, s, mhd[d]);
-#pragma unroll
-  for (int k = 0; k < 8; k++) dU[k] = 0.;
-#pragma unroll
-  for (int j = 0; j < 4; j++)
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      dU[UU] += mhd[j][k] * __ldg(conn + conn_slot(k, 0, j) * ng + gi);
-      dU[U1] += mhd[j][k] * __ldg(conn + conn_slot(k, 1, j) * ng + gi);
-      dU[U2] += mhd[j][k] * __ldg(conn + conn_slot(k, 2, j) * ng + gi);
-      dU[U3] += mhd[j][k] * __ldg(conn + conn_slot(k, 3, j) * ng + gi);
-    }
-#pragma unroll
-  for (int k = 0; k < 8; k++) dU[k] *= q.g;
-}
-
-template <bool FULL, bool THREE_D>
-__global__ void __launch_bounds__(128) k_update(Grid G, const double *__restrict__ pi, const double *__restrict__ pb,
-                                                double *__restrict__ pf, const double *__restrict__ F1,
-                                                const double *__restrict__ F2, const double *__restrict__ F3,
-                                                signed char *__restrict__ pflag, const double *__restrict__ geo,
-                                                const double *__restrict__ conn, const double *__restrict__ floors,
-                                                const double *__restrict__ katm, DevScalars *sc)
-{
-  if (sc->halted) return;
-  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
-  const int h = blockIdx.z;
-  if (i > G.istop || j > G.jstop) return;
-  const double Dt = FULL ? sc->dt : 0.5 * sc->dt;
-  const long c = cidx(G, h, i, j);
-  const long gi = (long)i * G.sn2 + j;
-  int fail = 0;
-  Geo q;
-  load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
-  double dU[8], U[8], pz[8];
-  {
-    double pbz[8];
-#pragma unroll
-    for (int k = 0; k < 8; k++) pbz[k] = __ldg(pb + k * G.nc + c);
-    source(G.gam, pbz, q, conn, G.ng, gi, dU, &fail);
-  }
-#pragma unroll
-  for (int k = 0; k < 8; k++) pz[k] = __ldg(pi + k * G.nc + c);
-  {
-    State s;
-    get_state(pz, q, s, &fail);
-    primtoflux(G.gam, pz, s, 0, q.g, U);
-  }
-  {
-    Flux FX{F1, F2, F3, G};
-    double f1m[8], f1p[8], f2m[8], f2p[8], f3m[8], f3p[8];
-    zone_fluxes<THREE_D>(FX, h, i, j, f1m, f1p, f2m, f2p, f3m, f3p);
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      if (THREE_D)
-        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 - (f3p[k] - f3m[k]) / G.dx3 + dU[k]);
-      else
-        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 + dU[k]);
-    }
-  }
-  // inversion with the isentropic fall-backs (step_ch.c:265-300); the guess is pi
-  int flag = utoprim<0>(G.gam, 0., U, q, pz);
-  if (flag) {
-    double kap = __ldg(katm + i);
-    flag = utoprim<1>(G.gam, kap, U, q, pz);
-    if (flag) flag = utoprim<2>(G.gam, kap, U, q, pz);
-  }
-  signed char fl = (signed char)flag;
-  // floors and gamma limit (fixup(), fixup.c:142-383)
-  if (fixup1zone(G.gam, __ldg(floors + gi), __ldg(floors + G.ng + gi), q, pz, &fail)) fl = -33;
-#pragma unroll
-  for (int k = 0; k < 8; k++) pf[k * G.nc + c] = pz[k];
-  pflag[c] = fl;
-  if (fail) record_fail(sc, fail, h + (THREE_D ? 1 : 0), i, j);
-}
-
-// diag_flux() (diag.c:437-465): sums over the inner radial face, after the
-// mass-flux fix; one block, fixed summation order
-__global__ void k_diag_flux(Grid G, const double *__restrict__ F1, DevScalars *sc)
-{
-  if (sc->halted) return;
-  __shared__ double red[3][32];
-  double m = 0., e = 0., l = 0.;
-  const long n = (long)G.n3 * G.n2;
-  for (long t = threadIdx.x; t < n; t += blockDim.x) {
-    int h = (int)(t / G.n2), j = G.jstart + (int)(t % G.n2);
-    long c = cidx(G, h, G.istart, j);
-    double fr = F1[RHO * G.nc + c];
-    if (fr > 0) fr = 0;
-    m += fr * G.dx2 * G.dx3;
-    e += (F1[UU * G.nc + c] - fr) * G.dx2 * G.dx3;
-    l += F1[U3 * G.nc + c] * G.dx2 * G.dx3;
-  }
-  m = warp_sum(m);
-  e = warp_sum(e);
-  l = warp_sum(l);
-  if ((threadIdx.x & 31) == 0) {
-    red[0][threadIdx.x >> 5] = m;
-    red[1][threadIdx.x >> 5] = e;
-    red[2][threadIdx.x >> 5] = l;
-  }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    int nw = blockDim.x >> 5;
-    double a = threadIdx.x < nw ? red[0][threadIdx.x] : 0.;
-    double b = threadIdx.x < nw ? red[1][threadIdx.x] : 0.;
-    double d = threadIdx.x < nw ? red[2][threadIdx.x] : 0.;
-    a = warp_sum(a);
-    b = warp_sum(b);
-    d = warp_sum(d);
-    if (threadIdx.x == 0) {
-      sc->mdot = a;
-      sc->edot = -b;
-      sc->ldot = d;
-    }
-  }
-}
 
 // ---------------------------------------------------------------------------
 // boundary conditions (bounds.c:54-331, polefix :381-436)
@@ -962,17 +528,6 @@ int fail_with(int code, const std::string &msg)
   return code;
 }
 
-#define CK(call)                                                                                 \
-  do {                                                                                           \
-    cudaError_t e_ = (call);                                                                     \
-    if (e_ != cudaSuccess)                                                                       \
-      return fail_with(HARM_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));         \
-  } while (0)
-
-int launch_step(Ctx *x);
-
-dim3 zone_grid(const Grid &G) { return dim3((G.n2 + 31) / 32, (G.n1 + 3) / 4, G.n3); }
-
 int launch_bound(Ctx *x, double *P)
 {
   const Grid &G = x->G;
@@ -992,35 +547,14 @@ int launch_fixup_utoprim(Ctx *x, double *P)
   return HARM_OK;
 }
 
-// advance() + fixup + bound_prim + fixup_utoprim + bound_prim (step_ch.c:101-117)
-template <bool FULL>
-void launch_half(Ctx *x, const double *pi, const double *pb, double *pf)
+// diag_mass() and the next dt (step_ch.c:119-137)
+void launch_mass(Ctx *x)
 {
-  const Grid &G = x->G;
-  dim3 fb(32, 4), fg((G.sn2 - 2 + 31) / 32, (G.sn1 - 2 + 3) / 4, G.n3);
-  k_flux<FULL><<<fg, fb, 0, x->stream>>>(G, pb, x->F1, x->F2, x->F3, x->geo, x->sc);
-  dim3 ub(32, 4);
-  if (G.n3 > 1)
-    k_update<FULL, true><<<zone_grid(G), ub, 0, x->stream>>>(G, pi, pb, pf, x->F1, x->F2, x->F3, x->pflag, x->geo,
-                                                               x->conn, x->floors, x->katm, x->sc);
-  else
-    k_update<FULL, false><<<zone_grid(G), ub, 0, x->stream>>>(G, pi, pb, pf, x->F1, x->F2, x->F3, x->pflag, x->geo,
-                                                                x->conn, x->floors, x->katm, x->sc);
-  if (FULL) k_diag_flux<<<1, 1024, 0, x->stream>>>(G, x->F1, x->sc);
-  launch_bound(x, pf);
-  launch_fixup_utoprim(x, pf);
-  launch_bound(x, pf);
-}
-
-int launch_step(Ctx *x)
-{
-  launch_half<false>(x, x->p, x->p, x->ph);
-  launch_half<true>(x, x->p, x->ph, x->p);
   k_diag_mass<<<x->nparts, 256, 0, x->stream>>>(x->G, x->p, x->geo, x->partials, x->nparts, x->sc);
   k_finalize<<<1, 1024, 0, x->stream>>>(x->G, x->partials, x->nparts, x->sc);
-  CK(cudaGetLastError());
-  return HARM_OK;
 }
+
+int launch_step(Ctx *x) { return x->mode == HARM_MIXED ? mixed::launch_step(x) : exact::launch_step(x); }
 
 // structural checks on the host geometry: the device stores only the
 // non-zero, independent entries
@@ -1051,22 +585,15 @@ bool geometry_layout_ok(const Dims &d, const double *gcov, const double *gcon, c
 
 using namespace harm;
 
+namespace harm {
+int launch_step(Ctx *x);
+}
+
 struct harm_ctx {
   Ctx x;
 };
 
 extern "C" const char *harm_last_error(void) { return g_err.c_str(); }
-
-static int ensure_pinned(Ctx *x, size_t bytes)
-{
-  if (x->pinned_bytes >= bytes) return HARM_OK;
-  if (x->pinned) cudaFreeHost(x->pinned);
-  x->pinned = nullptr;
-  x->pinned_bytes = 0;
-  CK(cudaMallocHost(&x->pinned, bytes));
-  x->pinned_bytes = bytes;
-  return HARM_OK;
-}
 
 extern "C" int harm_create(const harm_params *prm, const double *gcov, const double *gcon, const double *gdet,
                            const double *conn, const double *coords, const double *katm, int device,
@@ -1168,7 +695,8 @@ extern "C" void harm_destroy(harm_ctx *h)
   Ctx *x = &h->x;
   if (x->graph_exec) cudaGraphExecDestroy(x->graph_exec);
   void *ptrs[] = {x->p, x->ph, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm,
-                  x->stage, x->stage_flag, x->fail_list, x->fix_buf, x->partials, x->sc};
+                  x->stage, x->stage_flag, x->fail_list, x->fix_buf, x->partials, x->sc,
+                  x->F1f, x->F2f, x->F3f, x->geo32};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (x->pinned) cudaFreeHost(x->pinned);
@@ -1279,15 +807,48 @@ extern "C" int harm_get_diag(harm_ctx *h, harm_diag *d)
   return HARM_OK;
 }
 
+namespace harm {
+int sync_status(Ctx *x)
+{
+  CK(cudaStreamSynchronize(x->stream));
+  CK(cudaGetLastError());
+  DevScalars s;
+  int rc = read_scalars(x, &s);
+  if (rc) return rc;
+  if (s.err) return fail_with(s.err, "dt < 1e-9 (the reference exits with code 11)");
+  return HARM_OK;
+}
+}  // namespace harm
+
 extern "C" int harm_sync(harm_ctx *h)
 {
   if (!h) return fail_with(HARM_E_ARG, "null context");
-  CK(cudaStreamSynchronize(h->x.stream));
-  CK(cudaGetLastError());
-  DevScalars s;
-  int rc = read_scalars(&h->x, &s);
-  if (rc) return rc;
-  if (s.err) return fail_with(s.err, "dt < 1e-9 (the reference exits with code 11)");
+  return sync_status(&h->x);
+}
+
+extern "C" int harm_set_precision(harm_ctx *h, int mode)
+{
+  if (!h || (mode != HARM_FP64 && mode != HARM_MIXED)) return fail_with(HARM_E_ARG, "bad argument");
+  Ctx *x = &h->x;
+  if (mode == HARM_MIXED && !x->F1f) {
+    const Grid &G = x->G;
+    const size_t fb = 8 * G.nc * sizeof(float);
+    CK(cudaMalloc(&x->F1f, fb));
+    CK(cudaMalloc(&x->F2f, fb));
+    CK(cudaMalloc(&x->F3f, G.n3 > 1 ? fb : 8));
+    CK(cudaMalloc(&x->geo32, (size_t)3 * GEO_N * G.ng * sizeof(float)));
+    // FP32 copy of the three face metrics (slots FACE1, FACE2, FACE3)
+    std::vector<double> hg((size_t)3 * GEO_N * G.ng);
+    std::vector<float> hf(hg.size());
+    CK(cudaMemcpy(hg.data(), x->geo, hg.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < hg.size(); k++) hf[k] = (float)hg[k];
+    CK(cudaMemcpy(x->geo32, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if (mode != x->mode && x->graph_exec) {
+    cudaGraphExecDestroy(x->graph_exec);
+    x->graph_exec = nullptr;
+  }
+  x->mode = mode;
   return HARM_OK;
 }
 
@@ -1503,58 +1064,5 @@ extern "C" int harm_time_kernels(harm_ctx *h, int reps, double *ms)
 {
   if (!h || !ms || reps < 1) return fail_with(HARM_E_ARG, "bad argument");
   Ctx *x = &h->x;
-  const Grid &G = x->G;
-  // reps ordinary steps, launched one kernel at a time with an event after
-  // each, so every kernel is timed inside the sequence it runs in
-  const int nev = 16;
-  std::vector<cudaEvent_t> ev(nev);
-  for (auto &e : ev) CK(cudaEventCreate(&e));
-  double acc[HARM_NKERNELS] = {0, 0, 0, 0, 0};
-  dim3 fb(32, 4), fg((G.sn2 - 2 + 31) / 32, (G.sn1 - 2 + 3) / 4, G.n3);
-  int rc = HARM_OK;
-  for (int r = 0; r < reps && rc == HARM_OK; r++) {
-    int e = 0;
-    // slot of each interval: 0 flux, 1 update, 2 bound, 3 fixup_utoprim, 4 diag
-    int slot[nev];
-    CK(cudaEventRecord(ev[e++], x->stream));
-    for (int half = 0; half < 2; half++) {
-      const bool full = half == 1;
-      double *pi = x->p, *pb = full ? x->ph : x->p, *pf = full ? x->p : x->ph;
-      if (full) k_flux<true><<<fg, fb, 0, x->stream>>>(G, pb, x->F1, x->F2, x->F3, x->geo, x->sc);
-      else k_flux<false><<<fg, fb, 0, x->stream>>>(G, pb, x->F1, x->F2, x->F3, x->geo, x->sc);
-      slot[e] = 0; CK(cudaEventRecord(ev[e++], x->stream));
-      if (G.n3 > 1) {
-        if (full) k_update<true, true><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, pf, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm, x->sc);
-        else k_update<false, true><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, pf, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm, x->sc);
-      } else {
-        if (full) k_update<true, false><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, pf, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm, x->sc);
-        else k_update<false, false><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, pf, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm, x->sc);
-      }
-      slot[e] = 1; CK(cudaEventRecord(ev[e++], x->stream));
-      if (full) {
-        k_diag_flux<<<1, 1024, 0, x->stream>>>(G, x->F1, x->sc);
-        slot[e] = 4; CK(cudaEventRecord(ev[e++], x->stream));
-      }
-      launch_bound(x, pf);
-      slot[e] = 2; CK(cudaEventRecord(ev[e++], x->stream));
-      launch_fixup_utoprim(x, pf);
-      slot[e] = 3; CK(cudaEventRecord(ev[e++], x->stream));
-      launch_bound(x, pf);
-      slot[e] = 2; CK(cudaEventRecord(ev[e++], x->stream));
-    }
-    k_diag_mass<<<x->nparts, 256, 0, x->stream>>>(G, x->p, x->geo, x->partials, x->nparts, x->sc);
-    k_finalize<<<1, 1024, 0, x->stream>>>(G, x->partials, x->nparts, x->sc);
-    slot[e] = 4; CK(cudaEventRecord(ev[e++], x->stream));
-    CK(cudaEventSynchronize(ev[e - 1]));
-    for (int k = 1; k < e; k++) {
-      float f;
-      CK(cudaEventElapsedTime(&f, ev[k - 1], ev[k]));
-      acc[slot[k]] += f;
-    }
-  }
-  for (auto &e : ev) cudaEventDestroy(e);
-  // per launch: flux and update launch twice per step, bound 4x, fixup_utoprim 2x
-  const double per_step[HARM_NKERNELS] = {2, 2, 4, 2, 1};
-  for (int k = 0; k < HARM_NKERNELS; k++) ms[k] = acc[k] / (reps * per_step[k]);
-  return harm_sync(h);
+  return x->mode == HARM_MIXED ? mixed::time_kernels(x, reps, ms) : exact::time_kernels(x, reps, ms);
 }

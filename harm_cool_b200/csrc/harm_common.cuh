@@ -1,0 +1,151 @@
+// Types and helpers shared by the CUDA translation units of libharm_b200.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "harm_b200.h"
+#include "harm_phys.cuh"
+#include "host_setup.h"
+
+namespace harm {
+
+// ---------------------------------------------------------------------------
+// device-side run state
+
+struct DevScalars {
+  double t, dt;
+  unsigned long long ndt_bits[3];  // per-direction Courant minima (bits of positive doubles)
+  double mdot, edot, ldot, mdot_in, mdot_out, mass_curr, mass_in, mass_out, ndt;
+  double bsq_max;                  // torus set-up only
+  unsigned long long bsq_bits;
+  int fail_code, fail_h, fail_i, fail_j;
+  int err;                         // HARM_E_DT when dt < 1e-9
+  int halted;                      // set after a failure: later steps do nothing
+  int nfail, fail_overflow;        // failed zones met by the current fixup_utoprim
+};
+
+// Problem description passed by value to every kernel.
+struct Grid {
+  int n1, n2, n3, sn1, sn2;
+  int istart, istop, jstart, jstop;
+  long ng;   // sn1*sn2, points per geometry plane
+  long nc;   // n3*sn1*sn2, cells per state plane
+  int lim;
+  double gam, cour, defcon, tf;
+  double dx1, dx2, dx3;
+};
+
+constexpr int FAIL_CAP = 8192;  // failed zones repaired through the sorted list
+constexpr int NTHR_FIX = 1024;
+
+struct Ctx {
+  Grid G;
+  Dims D;
+  harm_params prm;
+  int device;
+  cudaStream_t stream;
+  double *p, *ph;                // [8][nc]
+  double *F1, *F2, *F3;          // [8][nc]
+  signed char *pflag;            // [nc]
+  double *geo;                   // [4 locations][GEO_N][ng]: FACE1, FACE2, FACE3, CENT
+  double *conn;                  // [40][ng]
+  double *floors;                // [2][ng]
+  double *katm;                  // [sn1]
+  double *stage;                 // [8*nc] host-layout staging
+  signed char *stage_flag;       // [sn3*sn1*sn2]
+  int *fail_list;                // [FAIL_CAP]
+  double *fix_buf;               // [FAIL_CAP*8]
+  double *partials;              // [3][nparts]
+  int nparts;
+  DevScalars *sc;
+  cudaGraphExec_t graph_exec;
+  int graph_steps;
+  double *pinned;                // pinned host buffer for the host-array entry points
+  size_t pinned_bytes;
+  int mode;                      // HARM_FP64 or HARM_MIXED
+  float *F1f, *F2f, *F3f;        // mixed mode: FP32 face fluxes [8][nc]
+  float *geo32;                  // mixed mode: FP32 face geometry [3][GEO_N][ng]
+};
+
+__device__ __forceinline__ void record_fail(DevScalars *sc, int code, int h, int i, int j)
+{
+  if (atomicCAS(&sc->fail_code, 0, code) == 0) {
+    sc->fail_h = h;
+    sc->fail_i = i;
+    sc->fail_j = j;
+  }
+}
+
+__device__ __forceinline__ long cidx(const Grid &G, int h, int i, int j)
+{
+  return ((long)h * G.sn1 + i) * G.sn2 + j;
+}
+
+__device__ __forceinline__ int hwrap(const Grid &G, int h)
+{
+  return h < 0 ? h + G.n3 : (h >= G.n3 ? h - G.n3 : h);
+}
+
+// geometry location slots on the device
+enum { L_FACE1 = 0, L_FACE2 = 1, L_FACE3 = 2, L_CENT = 3 };
+
+__device__ __forceinline__ const double *geo_at(const double *geo, const Grid &G, int loc)
+{
+  return geo + (long)loc * GEO_N * G.ng;
+}
+
+__device__ __forceinline__ double warp_min(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+
+__device__ __forceinline__ float warp_minf(float v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// host helpers (harm_api.cu)
+
+extern thread_local std::string g_err;
+int fail_with(int code, const std::string &msg);
+
+#define CK(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      return ::harm::fail_with(HARM_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+inline dim3 zone_grid(const Grid &G) { return dim3((G.n2 + 31) / 32, (G.n1 + 3) / 4, G.n3); }
+
+// kernels shared by both precisions (harm_api.cu)
+int launch_bound(Ctx *x, double *P);
+int launch_fixup_utoprim(Ctx *x, double *P);
+void launch_mass(Ctx *x);
+int sync_status(Ctx *x);
+
+// one step and the per-kernel timing of each precision variant
+namespace exact {
+int launch_step(Ctx *x);
+int time_kernels(Ctx *x, int reps, double *ms);
+}
+namespace mixed {
+int launch_step(Ctx *x);
+int time_kernels(Ctx *x, int reps, double *ms);
+}
+
+}  // namespace harm

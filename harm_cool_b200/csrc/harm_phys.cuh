@@ -387,7 +387,7 @@ __device__ __forceinline__ double W_of_vsq_fix(const U2P &c, double vsq, double 
   return (rho + u + p) / gtmp;
 }
 
-__device__ int u2p_body_vsq2fix1(U2P &c, const double *U, const Geo &q, double *prim)
+static __device__ __noinline__ int u2p_body_vsq2fix1(U2P &c, const double *U, const Geo &q, double *prim)
 {
   double Bcon[4], Qcon[4], ncon[4], QdotB, utsq, p, rho0, u;
   u2p_scalars(c, U, q, Bcon, Qcon, ncon, QdotB);
@@ -445,7 +445,7 @@ __device__ int u2p_body_vsq2fix1(U2P &c, const double *U, const Geo &q, double *
 // ---- Utoprim_1dfix1 (utoprim_1dfix1.c) ----
 
 // gnr2 with func_gnr2_rho (:601-697, :818-838)
-__device__ int gnr2_rho(const U2P &c, double &x)
+static __device__ __noinline__ int gnr2_rho(const U2P &c, double &x)
 {
   const double GAMMA = c.gam;
   double f = 1., df = 1., errx = 1.;
@@ -477,7 +477,7 @@ __device__ int gnr2_rho(const U2P &c, double &x)
 }
 
 // func_1d_orig1 (:721-771)
-__device__ void func_1d_orig1(U2P &c, double W, double &dx, double &f, double &df)
+static __device__ __noinline__ void func_1d_orig1(U2P &c, double W, double &dx, double &f, double &df)
 {
   const double GAMMA = c.gam, K_atm = c.K_atm, Bsq = c.Bsq, QdotBsq = c.QdotBsq, Qtsq = c.Qtsq;
   c.W_for_gnr2 = W;
@@ -506,7 +506,7 @@ __device__ void func_1d_orig1(U2P &c, double W, double &dx, double &f, double &d
   df = -2. * f;
 }
 
-__device__ int u2p_body_fix1(U2P &c, const double *U, const Geo &q, double *prim)
+static __device__ __noinline__ int u2p_body_fix1(U2P &c, const double *U, const Geo &q, double *prim)
 {
   double Bcon[4], Qcon[4], ncon[4], QdotB, utsq;
   u2p_scalars(c, U, q, Bcon, Qcon, ncon, QdotB);
@@ -620,7 +620,7 @@ __device__ __forceinline__ double ut_calc_3vel(const double *v, const Geo &q)
 }
 
 // returns true if the zone's pflag must be set to -33 (gamma failure)
-__device__ bool fixup1zone(double gam, double rhoflr, double uuflr, const Geo &q, double *pv, int *fail)
+static __device__ bool fixup1zone(double gam, double rhoflr, double uuflr, const Geo &q, double *pv, int *fail)
 {
   double pre[8];
 #pragma unroll

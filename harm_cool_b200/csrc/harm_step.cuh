@@ -1,0 +1,489 @@
+// Kernels of one step that differ between the FP64 path and the mixed path:
+// the face fluxes, the update with flux-CT, and the flux diagnostics.
+// Included by harm_exact.cu (HARM_STEP_MIXED 0) and harm_mixed.cu (HARM_STEP_MIXED 1),
+// each inside its own namespace.
+//
+// FP64 path: everything in double, built with -fmad=false, bit-compatible
+// with the reference.  Mixed path: slopes, face states, the face metric,
+// get_state/primtoflux/vchar and the Lax-Friedrichs flux in float; face
+// fluxes stored as float; the flux divergence, flux-CT averaging, the
+// connection source, U accumulation, the Noble inversion and the floors in
+// double.
+#pragma once
+#include "harm_common.cuh"
+#if HARM_STEP_MIXED
+#include "harm_phys32.cuh"
+#endif
+
+namespace harm {
+namespace HARM_VARIANT {
+
+#if HARM_STEP_MIXED
+using flux_t = float;
+#else
+using flux_t = double;
+#endif
+
+#if !HARM_STEP_MIXED
+template <int DIR>
+__device__ __forceinline__ void face_flux(double gam, const double *pl, const double *pr, const Geo &q, double *F,
+                                          double &ctop, int *fail)
+{
+  State s;
+  double Fl[8], Ul[8], cmaxl, cminl, cmaxr, cminr;
+  get_state(pl, q, s, fail);
+  primtoflux(gam, pl, s, DIR, q.g, Fl);
+  primtoflux(gam, pl, s, 0, q.g, Ul);
+  vchar(gam, pl, s, q, DIR, cmaxl, cminl, fail);
+  get_state(pr, q, s, fail);
+  {
+    double Fr[8], Ur[8];
+    primtoflux(gam, pr, s, DIR, q.g, Fr);
+    primtoflux(gam, pr, s, 0, q.g, Ur);
+    vchar(gam, pr, s, q, DIR, cmaxr, cminr, fail);
+    double t1 = 0. > cmaxl ? 0. : cmaxl;
+    double cmax = fabs(t1 > cmaxr ? t1 : cmaxr);
+    double t2 = 0. > -cminl ? 0. : -cminl;
+    double cmin = fabs(t2 > -cminr ? t2 : -cminr);
+    ctop = cmax > cmin ? cmax : cmin;
+    // HLLF = 0, LAXF = 1 (step_ch.c:66-67): the local Lax-Friedrichs flux
+#pragma unroll
+    for (int k = 0; k < 8; k++) F[k] = 0.5 * (Fl[k] + Fr[k] - ctop * (Ur[k] - Ul[k]));
+  }
+}
+
+#endif
+
+// One thread per face of direction DIR.  Face ranges (step_ch.c:407): dir 1
+// i in [istart, istop+1], j in [jstart-1, jstop+1]; dir 2 i in [istart-1,
+// istop+1], j in [jstart, jstop+1] (the polar faces jstart and jstop+1 carry
+// no flux, :412-416); dir 3 i in [istart-1, istop+1], j in [jstart-1, jstop+1].
+template <int DIR, bool FULL>
+__global__ void __launch_bounds__(128) k_flux(Grid G, const double *__restrict__ pb, flux_t *__restrict__ F,
+                                              const double *__restrict__ geo, const float *__restrict__ geo32,
+                                              DevScalars *sc)
+{
+  if (sc->halted) return;
+  const int j = (DIR == 2 ? G.jstart : G.jstart - 1) + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (DIR == 1 ? G.istart : G.istart - 1) + blockIdx.y * blockDim.y + threadIdx.y;
+  const int h = blockIdx.z;
+  double dtmin = 1.e9;
+  const bool in = (i <= G.istop + 1) && (j <= G.jstop + 1);
+  if (in) {
+    const long c = cidx(G, h, i, j);
+    if (DIR == 2 && (j == G.jstart || j == G.jstop + 1)) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) F[k * G.nc + c] = 0.;
+    } else {
+      long o1, o2, o3;  // zone-2d, zone-d, zone+d
+      if (DIR == 1) { o1 = c - 2 * G.sn2; o2 = c - G.sn2; o3 = c + G.sn2; }
+      else if (DIR == 2) { o1 = c - 2; o2 = c - 1; o3 = c + 1; }
+      else {
+        o1 = cidx(G, hwrap(G, h - 2), i, j);
+        o2 = cidx(G, hwrap(G, h - 1), i, j);
+        o3 = cidx(G, hwrap(G, h + 1), i, j);
+      }
+#if HARM_STEP_MIXED
+      float pl[8], pr[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const double *P = pb + k * G.nc;
+        float a = (float)__ldg(P + o1), b = (float)__ldg(P + o2), z = (float)__ldg(P + c), e = (float)__ldg(P + o3);
+        pl[k] = b + 0.5f * slope_lim_f(G.lim, a, b, z);
+        pr[k] = z - 0.5f * slope_lim_f(G.lim, b, z, e);
+      }
+      GeoF q;
+      load_geo_f(geo32 + (long)(DIR - 1) * GEO_N * G.ng, G.ng, (long)i * G.sn2 + j, q);
+      float Fz[8], ctopf;
+      int fail = 0;
+      face_flux_f<DIR>((float)G.gam, pl, pr, q, Fz, ctopf, &fail);
+      const double ctop = (double)ctopf;
+#else
+      double pl[8], pr[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const double *P = pb + k * G.nc;
+        double a = __ldg(P + o1), b = __ldg(P + o2), z = __ldg(P + c), e = __ldg(P + o3);
+        pl[k] = b + 0.5 * slope_lim(G.lim, a, b, z);
+        pr[k] = z - 0.5 * slope_lim(G.lim, b, z, e);
+      }
+      Geo q;
+      load_geo(geo_at(geo, G, DIR == 1 ? L_FACE1 : DIR == 2 ? L_FACE2 : L_FACE3), G.ng, (long)i * G.sn2 + j, q);
+      double Fz[8], ctop;
+      int fail = 0;
+      face_flux<DIR>(G.gam, pl, pr, q, Fz, ctop, &fail);
+#endif
+#pragma unroll
+      for (int k = 0; k < 8; k++) F[k * G.nc + c] = Fz[k];
+      if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
+      if (FULL && i >= G.istart && i <= G.istop && j >= G.jstart && j <= G.jstop) {
+        const double dxd = DIR == 1 ? G.dx1 : DIR == 2 ? G.dx2 : G.dx3;
+        dtmin = G.cour * dxd / ctop;
+      }
+    }
+  }
+  if (FULL) {
+    __shared__ double red[4];
+    const int t = threadIdx.y * blockDim.x + threadIdx.x;
+    double v = warp_min(dtmin);
+    if ((t & 31) == 0) red[t >> 5] = v;
+    __syncthreads();
+    if (t == 0) {
+      v = fmin(fmin(red[0], red[1]), fmin(red[2], red[3]));
+      if (v < 1.e9) atomicMin(&sc->ndt_bits[DIR - 1], (unsigned long long)__double_as_longlong(v));
+    }
+  }
+}
+
+template <bool FULL>
+void launch_flux(const Grid &G, cudaStream_t st, const double *pb, flux_t *F1, flux_t *F2, flux_t *F3,
+                 const double *geo, const float *geo32, DevScalars *sc)
+{
+  dim3 b(32, 4);
+  dim3 g1((G.n2 + 2 + 31) / 32, (G.n1 + 1 + 3) / 4, G.n3);
+  dim3 g2((G.n2 + 1 + 31) / 32, (G.n1 + 2 + 3) / 4, G.n3);
+  dim3 g3((G.n2 + 2 + 31) / 32, (G.n1 + 2 + 3) / 4, G.n3);
+  k_flux<1, FULL><<<g1, b, 0, st>>>(G, pb, F1, geo, geo32, sc);
+  k_flux<2, FULL><<<g2, b, 0, st>>>(G, pb, F2, geo, geo32, sc);
+  if (G.n3 > 1) k_flux<3, FULL><<<g3, b, 0, st>>>(G, pb, F3, geo, geo32, sc);
+}
+
+// ---------------------------------------------------------------------------
+// update (step_ch.c:237-306) fused with flux_ct (step_ch.c:514-629, 726-798),
+// the flux boundary fixes (coord.c:264-324) and fixup() (fixup.c:51-60)
+
+struct Flux {
+  const flux_t *F1, *F2, *F3;
+  Grid G;
+  __device__ double raw(int d, int k, int h, int i, int j) const
+  {
+    const flux_t *F = d == 1 ? F1 : d == 2 ? F2 : F3;
+    return (double)__ldg(F + k * G.nc + cidx(G, h, i, j));
+  }
+  // B-component of a raw face flux after fix_flux's polar reflection
+  // (coord.c:284-301): F1,F3[B2] at jstart-1 / jstop+1 mirror jstart / jstop
+  __device__ double rawB2(int d, int h, int i, int j) const
+  {
+    if (j == G.jstart - 1) return -raw(d, B2, h, i, G.jstart);
+    if (j == G.jstop + 1) return -raw(d, B2, h, i, G.jstop);
+    return raw(d, B2, h, i, j);
+  }
+  // 2D EMF (step_ch.c:546-547)
+  __device__ double emf2(int i, int j) const
+  {
+    return 0.25 * (rawB2(1, 0, i, j) + rawB2(1, 0, i, j - 1) - raw(2, B1, 0, i, j) - raw(2, B1, 0, i - 1, j));
+  }
+  // 3D EMFs (step_ch.c:754-764); h-1 wraps (phi periodic)
+  __device__ double e1(int h, int i, int j) const
+  {
+    int hm = hwrap(G, h - 1);
+    return 0.25 * ((raw(2, B3, h, i, j) + raw(2, B3, hm, i, j)) - (rawB2(3, h, i, j) + rawB2(3, h, i, j - 1)));
+  }
+  __device__ double e2(int h, int i, int j) const
+  {
+    int hm = hwrap(G, h - 1);
+    return 0.25 * ((raw(3, B1, h, i, j) + raw(3, B1, h, i - 1, j)) - (raw(1, B3, h, i, j) + raw(1, B3, hm, i, j)));
+  }
+  __device__ double e3(int h, int i, int j) const
+  {
+    return 0.25 * ((rawB2(1, h, i, j) + rawB2(1, h, i, j - 1)) - (raw(2, B1, h, i, j) + raw(2, B1, h, i - 1, j)));
+  }
+};
+
+template <bool THREE_D>
+__device__ void zone_fluxes(const Flux &FX, int h, int i, int j, double *f1m, double *f1p, double *f2m,
+                            double *f2p, double *f3m, double *f3p)
+{
+  const Grid &G = FX.G;
+  const int hp = THREE_D ? hwrap(G, h + 1) : 0;
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    f1m[k] = FX.raw(1, k, h, i, j);
+    f1p[k] = FX.raw(1, k, h, i + 1, j);
+    f2m[k] = FX.raw(2, k, h, i, j);
+    f2p[k] = FX.raw(2, k, h, i, j + 1);
+    if (THREE_D) {
+      f3m[k] = FX.raw(3, k, h, i, j);
+      f3p[k] = FX.raw(3, k, hp, i, j);
+    }
+  }
+  // no inflow of mass through the radial boundaries (coord.c:307-321)
+  if (i == G.istart && f1m[RHO] > 0) f1m[RHO] = 0;
+  if (i + 1 == G.istop + 1 && f1p[RHO] < 0) f1p[RHO] = 0;
+  if (!THREE_D) {
+    double eA = FX.emf2(i, j), eB = FX.emf2(i, j + 1), eC = FX.emf2(i + 1, j), eD = FX.emf2(i + 1, j + 1);
+    f1m[B1] = 0.;
+    f1m[B2] = 0.5 * (eA + eB);
+    f1m[B3] = FX.raw(1, B3, 0, i, j);
+    f1p[B1] = 0.;
+    f1p[B2] = 0.5 * (eC + eD);
+    f1p[B3] = FX.raw(1, B3, 0, i + 1, j);
+    f2m[B1] = -0.5 * (eA + eC);
+    f2m[B2] = 0.;
+    f2m[B3] = FX.raw(2, B3, 0, i, j);
+    f2p[B1] = -0.5 * (eB + eD);
+    f2p[B2] = 0.;
+    f2p[B3] = FX.raw(2, B3, 0, i, j + 1);
+  } else {
+    double e3a = FX.e3(h, i, j), e3b = FX.e3(h, i, j + 1), e3c = FX.e3(h, i + 1, j), e3d = FX.e3(h, i + 1, j + 1);
+    double e2a = FX.e2(h, i, j), e2b = FX.e2(hp, i, j), e2c = FX.e2(h, i + 1, j), e2d = FX.e2(hp, i + 1, j);
+    double e1a = FX.e1(h, i, j), e1b = FX.e1(hp, i, j), e1c = FX.e1(h, i, j + 1), e1d = FX.e1(hp, i, j + 1);
+    f1m[B1] = 0.;
+    f1m[B2] = 0.5 * (e3a + e3b);
+    f1m[B3] = -0.5 * (e2a + e2b);
+    f1p[B1] = 0.;
+    f1p[B2] = 0.5 * (e3c + e3d);
+    f1p[B3] = -0.5 * (e2c + e2d);
+    f2m[B1] = -0.5 * (e3a + e3c);
+    f2m[B2] = 0.;
+    f2m[B3] = 0.5 * (e1a + e1b);
+    f2p[B1] = -0.5 * (e3b + e3d);
+    f2p[B2] = 0.;
+    f2p[B3] = 0.5 * (e1c + e1d);
+    f3m[B1] = 0.5 * (e2a + e2c);
+    f3m[B2] = -0.5 * (e1a + e1c);
+    f3m[B3] = 0.;
+    f3p[B1] = 0.5 * (e2b + e2d);
+    f3p[B2] = -0.5 * (e1b + e1d);
+    f3p[B3] = 0.;
+  }
+}
+
+// source() (phys.c:165-207); conn stored as [k][min(nu,j)][max(nu,j)]
+__device__ __forceinline__ int conn_slot(int k, int a, int b)
+{
+  int lo = a < b ? a : b, hi = a < b ? b : a;
+  // pairs (lo,hi) with lo <= hi in row order: 00 01 02 03 11 12 13 22 23 33
+  int pair = lo == 0 ? hi : lo == 1 ? 3 + hi : lo == 2 ? 5 + hi : 9;
+  return k * 10 + pair;
+}
+
+__device__ void source(double gam, const double *pb, const Geo &q, const double *__restrict__ conn, long ng, long gi,
+                       double *dU, int *fail)
+{
+  State s;
+  get_state(pb, q, s, fail);
+  double mhd[4][4];
+#pragma unroll
+  for (int d = 0; d < 4; d++) mhd_calc(gam, pb, d, s, mhd[d]);
+#pragma unroll
+  for (int k = 0; k < 8; k++) dU[k] = 0.;
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      dU[UU] += mhd[j][k] * __ldg(conn + conn_slot(k, 0, j) * ng + gi);
+      dU[U1] += mhd[j][k] * __ldg(conn + conn_slot(k, 1, j) * ng + gi);
+      dU[U2] += mhd[j][k] * __ldg(conn + conn_slot(k, 2, j) * ng + gi);
+      dU[U3] += mhd[j][k] * __ldg(conn + conn_slot(k, 3, j) * ng + gi);
+    }
+#pragma unroll
+  for (int k = 0; k < 8; k++) dU[k] *= q.g;
+}
+
+template <bool FULL, bool THREE_D>
+__global__ void __launch_bounds__(128) k_update(Grid G, const double *__restrict__ pi, const double *__restrict__ pb,
+                                                double *__restrict__ pf, const flux_t *__restrict__ F1,
+                                                const flux_t *__restrict__ F2, const flux_t *__restrict__ F3,
+                                                signed char *__restrict__ pflag, const double *__restrict__ geo,
+                                                const double *__restrict__ conn, const double *__restrict__ floors,
+                                                const double *__restrict__ katm, DevScalars *sc)
+{
+  if (sc->halted) return;
+  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
+  const int h = blockIdx.z;
+  if (i > G.istop || j > G.jstop) return;
+  const double Dt = FULL ? sc->dt : 0.5 * sc->dt;
+  const long c = cidx(G, h, i, j);
+  const long gi = (long)i * G.sn2 + j;
+  int fail = 0;
+  Geo q;
+  load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
+  double dU[8], U[8], pz[8];
+  {
+    double pbz[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) pbz[k] = __ldg(pb + k * G.nc + c);
+    source(G.gam, pbz, q, conn, G.ng, gi, dU, &fail);
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++) pz[k] = __ldg(pi + k * G.nc + c);
+  {
+    State s;
+    get_state(pz, q, s, &fail);
+    primtoflux(G.gam, pz, s, 0, q.g, U);
+  }
+  {
+    Flux FX{F1, F2, F3, G};
+    double f1m[8], f1p[8], f2m[8], f2p[8], f3m[8], f3p[8];
+    zone_fluxes<THREE_D>(FX, h, i, j, f1m, f1p, f2m, f2p, f3m, f3p);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      if (THREE_D)
+        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 - (f3p[k] - f3m[k]) / G.dx3 + dU[k]);
+      else
+        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 + dU[k]);
+    }
+  }
+  // inversion with the isentropic fall-backs (step_ch.c:265-300); the guess is pi
+  int flag = utoprim<0>(G.gam, 0., U, q, pz);
+  if (flag) {
+    double kap = __ldg(katm + i);
+    flag = utoprim<1>(G.gam, kap, U, q, pz);
+    if (flag) flag = utoprim<2>(G.gam, kap, U, q, pz);
+  }
+  signed char fl = (signed char)flag;
+  // floors and gamma limit (fixup(), fixup.c:142-383)
+  if (fixup1zone(G.gam, __ldg(floors + gi), __ldg(floors + G.ng + gi), q, pz, &fail)) fl = -33;
+#pragma unroll
+  for (int k = 0; k < 8; k++) pf[k * G.nc + c] = pz[k];
+  pflag[c] = fl;
+  if (fail) record_fail(sc, fail, h + (THREE_D ? 1 : 0), i, j);
+}
+
+// diag_flux() (diag.c:437-465): sums over the inner radial face, after the
+// mass-flux fix; one block, fixed summation order
+__global__ void k_diag_flux(Grid G, const flux_t *__restrict__ F1, DevScalars *sc)
+{
+  if (sc->halted) return;
+  __shared__ double red[3][32];
+  double m = 0., e = 0., l = 0.;
+  const long n = (long)G.n3 * G.n2;
+  for (long t = threadIdx.x; t < n; t += blockDim.x) {
+    int h = (int)(t / G.n2), j = G.jstart + (int)(t % G.n2);
+    long c = cidx(G, h, G.istart, j);
+    double fr = (double)F1[RHO * G.nc + c];
+    if (fr > 0) fr = 0;
+    m += fr * G.dx2 * G.dx3;
+    e += ((double)F1[UU * G.nc + c] - fr) * G.dx2 * G.dx3;
+    l += (double)F1[U3 * G.nc + c] * G.dx2 * G.dx3;
+  }
+  m = warp_sum(m);
+  e = warp_sum(e);
+  l = warp_sum(l);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = m;
+    red[1][threadIdx.x >> 5] = e;
+    red[2][threadIdx.x >> 5] = l;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int nw = blockDim.x >> 5;
+    double a = threadIdx.x < nw ? red[0][threadIdx.x] : 0.;
+    double b = threadIdx.x < nw ? red[1][threadIdx.x] : 0.;
+    double d = threadIdx.x < nw ? red[2][threadIdx.x] : 0.;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    d = warp_sum(d);
+    if (threadIdx.x == 0) {
+      sc->mdot = a;
+      sc->edot = -b;
+      sc->ldot = d;
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// one step of this variant
+
+struct Bufs {
+  flux_t *F1, *F2, *F3;
+};
+
+inline Bufs bufs(Ctx *x)
+{
+#if HARM_STEP_MIXED
+  return Bufs{x->F1f, x->F2f, x->F3f};
+#else
+  return Bufs{x->F1, x->F2, x->F3};
+#endif
+}
+
+template <bool FULL>
+void launch_update(Ctx *x, const double *pi, const double *pb, double *pf)
+{
+  const Grid &G = x->G;
+  Bufs B = bufs(x);
+  if (G.n3 > 1)
+    k_update<FULL, true><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, pf, B.F1, B.F2, B.F3, x->pflag,
+                                                                       x->geo, x->conn, x->floors, x->katm, x->sc);
+  else
+    k_update<FULL, false><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, pf, B.F1, B.F2, B.F3, x->pflag,
+                                                                        x->geo, x->conn, x->floors, x->katm, x->sc);
+}
+
+// advance() + fixup + bound_prim + fixup_utoprim + bound_prim (step_ch.c:101-117)
+template <bool FULL>
+void launch_half(Ctx *x, const double *pi, const double *pb, double *pf)
+{
+  Bufs B = bufs(x);
+  launch_flux<FULL>(x->G, x->stream, pb, B.F1, B.F2, B.F3, x->geo, x->geo32, x->sc);
+  launch_update<FULL>(x, pi, pb, pf);
+  if (FULL) k_diag_flux<<<1, 1024, 0, x->stream>>>(x->G, B.F1, x->sc);
+  launch_bound(x, pf);
+  launch_fixup_utoprim(x, pf);
+  launch_bound(x, pf);
+}
+
+int launch_step(Ctx *x)
+{
+  launch_half<false>(x, x->p, x->p, x->ph);
+  launch_half<true>(x, x->p, x->ph, x->p);
+  launch_mass(x);
+  CK(cudaGetLastError());
+  return HARM_OK;
+}
+
+// reps ordinary steps, one kernel at a time with an event after each, so
+// every kernel is timed inside the sequence it runs in; slots: flux, update,
+// bound_prim, fixup_utoprim, diagnostics
+int time_kernels(Ctx *x, int reps, double *ms)
+{
+  const Grid &G = x->G;
+  Bufs B = bufs(x);
+  const int nev = 16;
+  cudaEvent_t ev[nev];
+  for (auto &e : ev) CK(cudaEventCreate(&e));
+  double acc[HARM_NKERNELS] = {0, 0, 0, 0, 0};
+  for (int r = 0; r < reps; r++) {
+    int e = 0, slot[nev];
+    CK(cudaEventRecord(ev[e++], x->stream));
+    for (int half = 0; half < 2; half++) {
+      const bool full = half == 1;
+      double *pi = x->p, *pb = full ? x->ph : x->p, *pf = full ? x->p : x->ph;
+      if (full) launch_flux<true>(G, x->stream, pb, B.F1, B.F2, B.F3, x->geo, x->geo32, x->sc);
+      else launch_flux<false>(G, x->stream, pb, B.F1, B.F2, B.F3, x->geo, x->geo32, x->sc);
+      slot[e] = 0; CK(cudaEventRecord(ev[e++], x->stream));
+      if (full) launch_update<true>(x, pi, pb, pf);
+      else launch_update<false>(x, pi, pb, pf);
+      slot[e] = 1; CK(cudaEventRecord(ev[e++], x->stream));
+      if (full) {
+        k_diag_flux<<<1, 1024, 0, x->stream>>>(G, B.F1, x->sc);
+        slot[e] = 4; CK(cudaEventRecord(ev[e++], x->stream));
+      }
+      launch_bound(x, pf);
+      slot[e] = 2; CK(cudaEventRecord(ev[e++], x->stream));
+      launch_fixup_utoprim(x, pf);
+      slot[e] = 3; CK(cudaEventRecord(ev[e++], x->stream));
+      launch_bound(x, pf);
+      slot[e] = 2; CK(cudaEventRecord(ev[e++], x->stream));
+    }
+    launch_mass(x);
+    slot[e] = 4; CK(cudaEventRecord(ev[e++], x->stream));
+    CK(cudaEventSynchronize(ev[e - 1]));
+    for (int k = 1; k < e; k++) {
+      float f;
+      CK(cudaEventElapsedTime(&f, ev[k - 1], ev[k]));
+      acc[slot[k]] += f;
+    }
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  const double per_step[HARM_NKERNELS] = {2, 2, 4, 2, 1};
+  for (int k = 0; k < HARM_NKERNELS; k++) ms[k] = acc[k] / (reps * per_step[k]);
+  return sync_status(x);
+}
+
+}  // namespace HARM_VARIANT
+}  // namespace harm

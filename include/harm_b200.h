@@ -38,6 +38,13 @@ enum {
   HARM_E_TIMEOUT = -12  /* a bounded device-side wait ran out */
 };
 
+/* Arithmetic of the step (harm_set_precision). */
+enum {
+  HARM_FP64 = 0,   /* everything in FP64, bit-compatible with the reference (default) */
+  HARM_MIXED = 1   /* FP32 reconstruction, wave speeds and face fluxes; FP64 geometry
+                      source, accumulation, inversion and floors */
+};
+
 /* Run parameters (decs.h:263-283, init.c:104-125). */
 typedef struct harm_params {
   int n1, n2, n3;   /* active zones in r, theta, phi; n3 == 1 or even n3 >= 4 */
@@ -118,6 +125,10 @@ int harm_set_time(harm_ctx *ctx, double t, double dt);
 int harm_get_time(harm_ctx *ctx, double *t, double *dt);
 int harm_set_mass(harm_ctx *ctx, double mass_in, double mass_out);
 int harm_get_diag(harm_ctx *ctx, harm_diag *d);
+
+/* Select HARM_FP64 or HARM_MIXED for the following steps (no reference
+   counterpart: the reference is FP64 throughout). */
+int harm_set_precision(harm_ctx *ctx, int mode);
 
 /* step_ch() (step_ch.c:90-140): predictor to dt/2, floors, boundaries,
    failure repair, corrector to dt, the same again, mass diagnostics and the
