@@ -38,6 +38,7 @@ def kernels_per_step(n3):
     flux diagnostics; then the mass diagnostics and the dt update."""
     nflux = 3 if n3 > 1 else 2
     return 2 * (nflux + 5) + 1 + 2
+METRIC = "zone-cycles/s 288x256x256 GRMHD step_ch: FP64, mixed precision beside it"
 STATE_BYTES_PER_ZONE_CYCLE = 320  # p read twice, ph written and read, p written; 8 FP64 prims
 
 
@@ -148,34 +149,82 @@ def run_reference(args, world, rank):
     if rank != 0:
         return
     rate, cores, sample = reference_cpu_rate(seconds_per_core=max(2.0, min(20.0, 4.0 * args.steps)))
-    line = {"metric": "zone-cycles/s 288x256x256 GRMHD step_ch (FP64)", "value": rate,
+    line = {"metric": METRIC, "value": rate,
             "unit": "zone-cycles/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * args.n1 * args.n2 * args.n3 / rate, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "FM torus %dx%dx%d, gamma-law, FP64, sampled as 288x256x4 slabs"
-                                   % (args.n1, args.n2, args.n3)},
+            "config": {"workload": workload(args), "parallelism": "single",
+                       "sample": "the same r-theta grid with 4 phi planes per process"},
             "cpu_baseline": {"value": rate, "unit": "zone-cycles/s", "cores": cores, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": rate, "unit": "zone-cycles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
+def workload(args):
+    return ("FM torus %dx%dx%d (a=0.9375, rin=6, rmax=12, beta=100), gamma-law, FP64"
+            % (args.n1, args.n2, args.n3))
+
+
+def alg_bytes_per_zone(kernel, n3):
+    """Algorithmic DRAM bytes per zone of one launch group, FP64 state (8 B per
+    primitive, 8 primitives), averaged over the predictor and the corrector:
+    flux   per direction: read the zone's primitives, write its face flux;
+    update read pi (and pb in the corrector, where it differs from pi), read
+           the zone's face flux in each direction (each face is shared by two
+           zones), write pf and pflag."""
+    ndir = 3 if n3 > 1 else 2
+    if kernel == "flux":
+        return ndir * (64 + 64)
+    pred = 64 + ndir * 64 + 64 + 1
+    corr = pred + 64
+    return (pred + corr) / 2.0
+
+
+def measured_traffic(kernel, zones):
+    """DRAM bytes per launch group from the committed ncu capture, scaled by zones."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic_per_zone.json")
+    if not os.path.exists(path):
+        return None
+    d = json.load(open(path))
+    if kernel not in d:
+        return None
+    return d[kernel]["bytes_per_zone"] * zones
+
+
+def l1_errors(pa, pb):
+    """L1 of (pb - pa) over the active zones, relative to mean |pa|, per primitive."""
+    import numpy as np
+    names = ("rho", "u", "u1", "u2", "u3", "B1", "B2", "B3")
+    out = {}
+    for k, n in enumerate(names):
+        s = float(np.mean(np.abs(pa[..., k])))
+        out[n] = float(np.mean(np.abs(pb[..., k] - pa[..., k])) / s) if s > 0 else 0.0
+    return out
+
+
+def timed_run(hc, pr, local, world, steps, warmup, mixed):
+    ctx = hc.Context(pr, device=local)
+    ctx.init_torus()
+    if mixed:
+        ctx.set_precision(hc.Context.MIXED)
+    ctx.run(warmup)
+    sampler = ClockSampler(local)
+    barrier(world)
+    sampler.start()
+    ms = ctx.run_timed(steps)
+    clocks = sampler.stop()
+    barrier(world)
+    return ctx, reduce_max(ms, world, local), clocks
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import harm_cool_b200 as hc
     pr = hc.torus_problem(args.n1, args.n2, args.n3)
-    ctx = hc.Context(pr, device=local)
-    ctx.init_torus()
     zones = pr.zones
-    ctx.run(args.warmup)
-    sampler = ClockSampler(local)
-    barrier(world)
-    sampler.start()
-    ms = ctx.run_timed(args.steps)
-    clocks = sampler.stop()
-    barrier(world)
-    ms = reduce_max(ms, world, local)
+    ctx, ms, clocks = timed_run(hc, pr, local, world, args.steps, args.warmup, mixed=False)
     value = zones * args.steps * world / (ms / 1e3)
     d = ctx.diag()
     # end to end through the host-array call: upload p, step, download p every step
@@ -186,34 +235,48 @@ def run_ours(args, world, rank, local):
     ms_e2e = reduce_max(ms_e2e, world, local)
     e2e = zones * args.e2e_steps * world / (ms_e2e / 1e3)
     bytes_host = int(np.prod(pr.shape)) * 8 * 8
-    # dominant kernel, timed alone on the context's stream
+    del pinned
+    # dominant kernel, timed launch by launch inside ordinary steps on the context's stream
     kms = ctx.time_kernels(reps=3)
     dom = max(("flux", "update"), key=lambda k: kms[k])
     peak, peak_kind = measured_peaks()
-    alg = {"flux": 64, "update": 192}[dom]  # FP64 state bytes per zone this kernel must move
-    achieved = zones * alg / (kms[dom] / 1e3) / 1e9
-    line = {"metric": "zone-cycles/s 288x256x256 GRMHD step_ch (FP64)", "value": value,
-            "unit": "zone-cycles/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+    alg = alg_bytes_per_zone(dom, args.n3) * zones
+    achieved = alg / (kms[dom] / 1e3) / 1e9
+    traffic = measured_traffic(dom, zones)
+    line = {"metric": METRIC,
+            "value": value, "unit": "zone-cycles/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "FM torus %dx%dx%d (a=0.9375, rin=6, rmax=12, beta=100), gamma-law, FP64"
-                                   % (args.n1, args.n2, args.n3),
-                       "parallelism": "replicas" if world > 1 else "single", "l2": "state > L2, no flush"},
+            "config": {"workload": workload(args),
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "state (%.1f GB) > L2, no flush" % (zones * 64 * 2 / 1e9)},
             "e2e": {"value": e2e, "unit": "zone-cycles/s", "h2d_bytes_per_step": bytes_host,
                     "d2h_bytes_per_step": bytes_host, "path": "harm_step_ch_host (upload, step, download)"},
             "gpu_launches": kernels_per_step(args.n3) * args.steps,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                         "peak_source": peak_kind,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes": alg, "peak_source": peak_kind,
                          "step_frac": zones * STATE_BYTES_PER_ZONE_CYCLE / (ms / args.steps / 1e3) / 1e9 / peak},
             "kernel_ms": kms, "clocks": clocks, "sim_time": ctx.time(), "fail_code": d["fail_code"]}
+    if not args.no_mixed:
+        pa = ctx.get_prims()
+        ctx.close()
+        ctxm, msm, clocksm = timed_run(hc, pr, local, world, args.steps, args.warmup, mixed=True)
+        pb = ctxm.get_prims()
+        act = (slice(1, -1) if args.n3 > 1 else slice(None), slice(2, -2), slice(2, -2))
+        line["mixed"] = {"value": zones * args.steps * world / (msm / 1e3), "ms_per_step": msm / args.steps,
+                         "speedup_vs_fp64": ms / msm, "clocks": clocksm,
+                         "l1_vs_fp64": l1_errors(pa[act], pb[act]), "l1_after_steps": args.warmup + args.steps,
+                         "kernel_ms": ctxm.time_kernels(reps=3), "fail_code": ctxm.diag()["fail_code"]}
+        ctxm.close()
+    else:
+        ctx.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, sample = reference_cpu_rate(seconds_per_core=10.0, cores=1)
         line["cpu_baseline"] = {"value": rate, "unit": "zone-cycles/s", "cores": cores, "kind": "reference",
                                 "sample": sample}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    ctx.close()
 
 
 def main():
@@ -227,6 +290,7 @@ def main():
     ap.add_argument("--n3", type=int, default=256)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

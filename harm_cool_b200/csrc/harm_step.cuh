@@ -15,6 +15,14 @@
 #include "harm_phys32.cuh"
 #endif
 
+// resident blocks of 128 threads per SM that the register allocation must allow
+#ifndef HARM_FLUX_MINB
+#define HARM_FLUX_MINB 1
+#endif
+#ifndef HARM_UPDATE_MINB
+#define HARM_UPDATE_MINB 1
+#endif
+
 namespace harm {
 namespace HARM_VARIANT {
 
@@ -59,7 +67,7 @@ __device__ __forceinline__ void face_flux(double gam, const double *pl, const do
 // istop+1], j in [jstart, jstop+1] (the polar faces jstart and jstop+1 carry
 // no flux, :412-416); dir 3 i in [istart-1, istop+1], j in [jstart-1, jstop+1].
 template <int DIR, bool FULL>
-__global__ void __launch_bounds__(128) k_flux(Grid G, const double *__restrict__ pb, flux_t *__restrict__ F,
+__global__ void __launch_bounds__(128, HARM_FLUX_MINB) k_flux(Grid G, const double *__restrict__ pb, flux_t *__restrict__ F,
                                               const double *__restrict__ geo, const float *__restrict__ geo32,
                                               DevScalars *sc)
 {
@@ -282,7 +290,7 @@ __device__ void source(double gam, const double *pb, const Geo &q, const double 
 }
 
 template <bool FULL, bool THREE_D>
-__global__ void __launch_bounds__(128) k_update(Grid G, const double *__restrict__ pi, const double *__restrict__ pb,
+__global__ void __launch_bounds__(128, HARM_UPDATE_MINB) k_update(Grid G, const double *__restrict__ pi, const double *__restrict__ pb,
                                                 double *__restrict__ pf, const flux_t *__restrict__ F1,
                                                 const flux_t *__restrict__ F2, const flux_t *__restrict__ F3,
                                                 signed char *__restrict__ pflag, const double *__restrict__ geo,
