@@ -97,6 +97,8 @@ _SIGNATURES = {
     "harm_fixup_utoprim": (ctypes.c_int, [ctypes.c_void_p, _DP]),
     "harm_utoprim_2d_batch": (ctypes.c_int, [_DP, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int),
                                              ctypes.c_long, ctypes.c_double]),
+    "harm_utoprim_2d_batch_noalloc": (ctypes.c_int, [_DP, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int),
+                                                     ctypes.c_long, ctypes.c_double]),
 }
 
 

@@ -35,6 +35,7 @@ UNITS = {
     "harm_api.cu": ["-fmad=false"],     # shared kernels and the C ABI
     "harm_exact.cu": ["-fmad=false"],   # the FP64 step, bit-compatible with the reference
     "harm_mixed.cu": ["-fmad=true"],    # the mixed-precision step
+    "harm_noalloc.cu": ["-fmad=false"],  # batch inversion on a fixed device buffer
 }
 
 

@@ -176,6 +176,21 @@ int harm_fixup_utoprim(harm_ctx *ctx, double *pv);                /* fixup.c:432
 int harm_utoprim_2d_batch(const double *U, const double *gcov, const double *gcon,
                           const double *gdet, double *prim, int *ret, long n, double gam);
 
+/* The same inversion as harm_utoprim_2d_batch, for callers that cannot
+   allocate device memory: hosts whose GPU memory is already committed to a
+   resident simulation state or handed to another allocator, and hosts that
+   must not hit the device-wide synchronisation of cudaFree while other streams
+   run.  The device copies live in one fixed array inside the library (about
+   6.2 MiB per GPU, held until exit), so the call allocates nothing.  At most
+   HARM_U2P_NOALLOC_MAX zones per call (HARM_E_ARG beyond).  The first call on
+   a device looks up the array's device address; make it before any stream
+   capture.  Calls share the array, so calls that overlap on the GPU race.
+   Blocks until the results are in prim and ret.  No counterpart in the
+   reference. */
+#define HARM_U2P_NOALLOC_MAX 16384
+int harm_utoprim_2d_batch_noalloc(const double *U, const double *gcov, const double *gcon,
+                                  const double *gdet, double *prim, int *ret, long n, double gam);
+
 #ifdef __cplusplus
 }
 #endif
