@@ -194,13 +194,15 @@ def measured_traffic(kernel, zones):
 
 
 def l1_errors(pa, pb):
-    """L1 of (pb - pa) over the active zones, relative to mean |pa|, per primitive."""
+    """L1 of (pb - pa) over the active zones relative to the L1 of pa: for rho and
+    u, and for the velocity (u1..u3) and field (B1..B3) vectors as wholes, since a
+    single component (u2, B3) can be near zero in the whole torus early on."""
     import numpy as np
-    names = ("rho", "u", "u1", "u2", "u3", "B1", "B2", "B3")
+    groups = {"rho": [0], "u": [1], "v": [2, 3, 4], "B": [5, 6, 7]}
     out = {}
-    for k, n in enumerate(names):
-        s = float(np.mean(np.abs(pa[..., k])))
-        out[n] = float(np.mean(np.abs(pb[..., k] - pa[..., k])) / s) if s > 0 else 0.0
+    for n, ks in groups.items():
+        s = float(np.sum(np.abs(pa[..., ks])))
+        out[n] = float(np.sum(np.abs(pb[..., ks] - pa[..., ks])) / s) if s > 0 else 0.0
     return out
 
 

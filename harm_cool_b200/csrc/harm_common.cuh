@@ -66,6 +66,7 @@ struct Ctx {
   int mode;                      // HARM_FP64 or HARM_MIXED
   float *F1f, *F2f, *F3f;        // mixed mode: FP32 face fluxes [8][nc]
   float *geo32;                  // mixed mode: FP32 face geometry [3][GEO_N][ng]
+  double *Ubuf;                  // conserved variables between the two update launches [8][nc]
 };
 
 __device__ __forceinline__ void record_fail(DevScalars *sc, int code, int h, int i, int j)

@@ -22,6 +22,15 @@
 #ifndef HARM_UPDATE_MINB
 #define HARM_UPDATE_MINB 1
 #endif
+#ifndef HARM_CONS_MINB
+#define HARM_CONS_MINB 1
+#endif
+#ifndef HARM_INV_MINB
+#define HARM_INV_MINB 1
+#endif
+#ifndef HARM_SPLIT_UPDATE
+#define HARM_SPLIT_UPDATE 0
+#endif
 
 namespace harm {
 namespace HARM_VARIANT {
@@ -350,6 +359,102 @@ __global__ void __launch_bounds__(128, HARM_UPDATE_MINB) k_update(Grid G, const 
   if (fail) record_fail(sc, fail, h + (THREE_D ? 1 : 0), i, j);
 }
 
+// The same update in two launches, so that each holds fewer registers and
+// more warps stay resident: k_cons forms U (flux-CT and flux-boundary fixes,
+// flux divergence, connection source, primtoU of pi) into Ub; k_invert runs
+// the inversion with its fall-backs and the floors.  Same operations in the
+// same order as k_update.
+template <bool FULL, bool THREE_D>
+__global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const double *__restrict__ pi,
+                                                              const double *__restrict__ pb,
+                                                              const flux_t *__restrict__ F1,
+                                                              const flux_t *__restrict__ F2,
+                                                              const flux_t *__restrict__ F3,
+                                                              const double *__restrict__ geo,
+                                                              const double *__restrict__ conn,
+                                                              double *__restrict__ Ub, DevScalars *sc)
+{
+  if (sc->halted) return;
+  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
+  const int h = blockIdx.z;
+  if (i > G.istop || j > G.jstop) return;
+  const double Dt = FULL ? sc->dt : 0.5 * sc->dt;
+  const long c = cidx(G, h, i, j);
+  const long gi = (long)i * G.sn2 + j;
+  int fail = 0;
+  Geo q;
+  load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
+  double dU[8], U[8];
+  {
+    double pbz[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) pbz[k] = __ldg(pb + k * G.nc + c);
+    source(G.gam, pbz, q, conn, G.ng, gi, dU, &fail);
+  }
+  {
+    double pz[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) pz[k] = __ldg(pi + k * G.nc + c);
+    State s;
+    get_state(pz, q, s, &fail);
+    primtoflux(G.gam, pz, s, 0, q.g, U);
+  }
+  {
+    Flux FX{F1, F2, F3, G};
+    double f1m[8], f1p[8], f2m[8], f2p[8], f3m[8], f3p[8];
+    zone_fluxes<THREE_D>(FX, h, i, j, f1m, f1p, f2m, f2p, f3m, f3p);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      if (THREE_D)
+        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 - (f3p[k] - f3m[k]) / G.dx3 + dU[k]);
+      else
+        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 + dU[k]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++) Ub[k * G.nc + c] = U[k];
+  if (fail) record_fail(sc, fail, h + (THREE_D ? 1 : 0), i, j);
+}
+
+__global__ void __launch_bounds__(128, HARM_INV_MINB) k_invert(Grid G, const double *__restrict__ pi,
+                                                               const double *__restrict__ Ub,
+                                                               double *__restrict__ pf,
+                                                               signed char *__restrict__ pflag,
+                                                               const double *__restrict__ geo,
+                                                               const double *__restrict__ floors,
+                                                               const double *__restrict__ katm, DevScalars *sc)
+{
+  if (sc->halted) return;
+  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
+  const int h = blockIdx.z;
+  if (i > G.istop || j > G.jstop) return;
+  const long c = cidx(G, h, i, j);
+  const long gi = (long)i * G.sn2 + j;
+  int fail = 0;
+  Geo q;
+  load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
+  double U[8], pz[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    U[k] = __ldg(Ub + k * G.nc + c);
+    pz[k] = __ldg(pi + k * G.nc + c);
+  }
+  int flag = utoprim<0>(G.gam, 0., U, q, pz);
+  if (flag) {
+    double kap = __ldg(katm + i);
+    flag = utoprim<1>(G.gam, kap, U, q, pz);
+    if (flag) flag = utoprim<2>(G.gam, kap, U, q, pz);
+  }
+  signed char fl = (signed char)flag;
+  if (fixup1zone(G.gam, __ldg(floors + gi), __ldg(floors + G.ng + gi), q, pz, &fail)) fl = -33;
+#pragma unroll
+  for (int k = 0; k < 8; k++) pf[k * G.nc + c] = pz[k];
+  pflag[c] = fl;
+  if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
+}
+
 // diag_flux() (diag.c:437-465): sums over the inner radial face, after the
 // mass-flux fix; one block, fixed summation order
 __global__ void k_diag_flux(Grid G, const flux_t *__restrict__ F1, DevScalars *sc)
@@ -414,6 +519,17 @@ void launch_update(Ctx *x, const double *pi, const double *pb, double *pf)
 {
   const Grid &G = x->G;
   Bufs B = bufs(x);
+#if HARM_SPLIT_UPDATE
+  if (G.n3 > 1)
+    k_cons<FULL, true><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn,
+                                                                     x->Ubuf, x->sc);
+  else
+    k_cons<FULL, false><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn,
+                                                                      x->Ubuf, x->sc);
+  k_invert<<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->katm,
+                                                        x->sc);
+  return;
+#endif
   if (G.n3 > 1)
     k_update<FULL, true><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, pf, B.F1, B.F2, B.F3, x->pflag,
                                                                        x->geo, x->conn, x->floors, x->katm, x->sc);

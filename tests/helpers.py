@@ -60,3 +60,13 @@ def l1_rel(a, b):
         scale = np.mean(np.abs(b[..., k]))
         out.append(float(np.mean(np.abs(a[..., k] - b[..., k])) / scale) if scale > 0 else 0.)
     return np.array(out)
+
+
+def l1_groups(a, b):
+    """L1 of (a-b) relative to the L1 of b for rho, u, the velocity vector and the
+    field vector."""
+    out = {}
+    for n, ks in (("rho", [0]), ("u", [1]), ("v", [2, 3, 4]), ("B", [5, 6, 7])):
+        s = np.sum(np.abs(b[..., ks]))
+        out[n] = float(np.sum(np.abs(a[..., ks] - b[..., ks])) / s) if s > 0 else 0.
+    return out

@@ -11,7 +11,7 @@ over runs too long for the CPU."""
 import numpy as np
 import pytest
 
-from helpers import NAMES, active, l1_rel, make_oracle
+from helpers import NAMES, active, l1_groups, l1_rel, make_oracle
 
 pytestmark = pytest.mark.gpu
 L1_RHO_1000 = 1e-4
@@ -32,8 +32,10 @@ def _pair(hc, pr):
     return a, b
 
 
-def _report(tag, l1):
+def _report(tag, l1, grouped=None):
     print(tag, " ".join("%s=%.3e" % (n, v) for n, v in zip(NAMES, l1)))
+    if grouped:
+        print("    grouped:", " ".join("%s=%.3e" % kv for kv in grouped.items()))
 
 
 def test_mixed_2d_1000_steps_density_l1(hc):
@@ -47,7 +49,7 @@ def test_mixed_2d_1000_steps_density_l1(hc):
         pa, pb = active(pr, a.get_prims()), active(pr, b.get_prims())
         assert np.all(np.isfinite(pb))
         l1 = l1_rel(pb, pa)
-        _report("mixed vs FP64, 128x128, %d steps:" % n, l1)
+        _report("mixed vs FP64, 128x128, %d steps:" % n, l1, l1_groups(pb, pa))
     assert l1[0] <= L1_RHO_1000, l1
     assert b.diag()["fail_code"] == 0
     # the same number of steps advances the same simulated time to FP32 accuracy
@@ -64,7 +66,7 @@ def test_mixed_3d_steps_track_fp64(hc):
     b.run(200)
     pa, pb = active(pr, a.get_prims()), active(pr, b.get_prims())
     l1 = l1_rel(pb, pa)
-    _report("mixed vs FP64, 48x48x16, 200 steps:", l1)
+    _report("mixed vs FP64, 48x48x16, 200 steps:", l1, l1_groups(pb, pa))
     assert l1[0] <= L1_RHO_1000, l1
     assert b.diag()["fail_code"] == 0
 
