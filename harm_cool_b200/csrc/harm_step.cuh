@@ -15,21 +15,18 @@
 #include "harm_phys32.cuh"
 #endif
 
-// resident blocks of 128 threads per SM that the register allocation must allow
+// Resident blocks of 128 threads per SM that the register allocation must
+// allow, per kernel.  The kernels are bound by the latency of dependent FP64
+// instructions, so more resident warps beat the few spills the tighter
+// register budgets cost; each variant sets values measured best on a B200.
 #ifndef HARM_FLUX_MINB
 #define HARM_FLUX_MINB 1
-#endif
-#ifndef HARM_UPDATE_MINB
-#define HARM_UPDATE_MINB 1
 #endif
 #ifndef HARM_CONS_MINB
 #define HARM_CONS_MINB 1
 #endif
 #ifndef HARM_INV_MINB
 #define HARM_INV_MINB 1
-#endif
-#ifndef HARM_SPLIT_UPDATE
-#define HARM_SPLIT_UPDATE 0
 #endif
 
 namespace harm {
@@ -298,72 +295,14 @@ __device__ void source(double gam, const double *pb, const Geo &q, const double 
   for (int k = 0; k < 8; k++) dU[k] *= q.g;
 }
 
-template <bool FULL, bool THREE_D>
-__global__ void __launch_bounds__(128, HARM_UPDATE_MINB) k_update(Grid G, const double *__restrict__ pi, const double *__restrict__ pb,
-                                                double *__restrict__ pf, const flux_t *__restrict__ F1,
-                                                const flux_t *__restrict__ F2, const flux_t *__restrict__ F3,
-                                                signed char *__restrict__ pflag, const double *__restrict__ geo,
-                                                const double *__restrict__ conn, const double *__restrict__ floors,
-                                                const double *__restrict__ katm, DevScalars *sc)
-{
-  if (sc->halted) return;
-  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
-  const int h = blockIdx.z;
-  if (i > G.istop || j > G.jstop) return;
-  const double Dt = FULL ? sc->dt : 0.5 * sc->dt;
-  const long c = cidx(G, h, i, j);
-  const long gi = (long)i * G.sn2 + j;
-  int fail = 0;
-  Geo q;
-  load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
-  double dU[8], U[8], pz[8];
-  {
-    double pbz[8];
-#pragma unroll
-    for (int k = 0; k < 8; k++) pbz[k] = __ldg(pb + k * G.nc + c);
-    source(G.gam, pbz, q, conn, G.ng, gi, dU, &fail);
-  }
-#pragma unroll
-  for (int k = 0; k < 8; k++) pz[k] = __ldg(pi + k * G.nc + c);
-  {
-    State s;
-    get_state(pz, q, s, &fail);
-    primtoflux(G.gam, pz, s, 0, q.g, U);
-  }
-  {
-    Flux FX{F1, F2, F3, G};
-    double f1m[8], f1p[8], f2m[8], f2p[8], f3m[8], f3p[8];
-    zone_fluxes<THREE_D>(FX, h, i, j, f1m, f1p, f2m, f2p, f3m, f3p);
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      if (THREE_D)
-        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 - (f3p[k] - f3m[k]) / G.dx3 + dU[k]);
-      else
-        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 + dU[k]);
-    }
-  }
-  // inversion with the isentropic fall-backs (step_ch.c:265-300); the guess is pi
-  int flag = utoprim<0>(G.gam, 0., U, q, pz);
-  if (flag) {
-    double kap = __ldg(katm + i);
-    flag = utoprim<1>(G.gam, kap, U, q, pz);
-    if (flag) flag = utoprim<2>(G.gam, kap, U, q, pz);
-  }
-  signed char fl = (signed char)flag;
-  // floors and gamma limit (fixup(), fixup.c:142-383)
-  if (fixup1zone(G.gam, __ldg(floors + gi), __ldg(floors + G.ng + gi), q, pz, &fail)) fl = -33;
-#pragma unroll
-  for (int k = 0; k < 8; k++) pf[k * G.nc + c] = pz[k];
-  pflag[c] = fl;
-  if (fail) record_fail(sc, fail, h + (THREE_D ? 1 : 0), i, j);
-}
-
-// The same update in two launches, so that each holds fewer registers and
-// more warps stay resident: k_cons forms U (flux-CT and flux-boundary fixes,
-// flux divergence, connection source, primtoU of pi) into Ub; k_invert runs
-// the inversion with its fall-backs and the floors.  Same operations in the
-// same order as k_update.
+// The zone update (step_ch.c:237-306) in two launches, so that each holds
+// fewer registers and more warps stay resident to cover FP64 latency:
+// k_cons forms U -- flux_ct (step_ch.c:514-629, 726-798), the flux boundary
+// fixes (coord.c:264-324), source() (phys.c:165-207), primtoU of pi and the
+// flux divergence (step_ch.c:247-263) -- into Ub; k_invert runs Utoprim_2d
+// with the isentropic fall-backs (step_ch.c:265-300) and fixup()
+// (fixup.c:142-383).  The order of every floating-point operation is the
+// reference's.
 template <bool FULL, bool THREE_D>
 __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const double *__restrict__ pi,
                                                               const double *__restrict__ pb,
@@ -519,7 +458,6 @@ void launch_update(Ctx *x, const double *pi, const double *pb, double *pf)
 {
   const Grid &G = x->G;
   Bufs B = bufs(x);
-#if HARM_SPLIT_UPDATE
   if (G.n3 > 1)
     k_cons<FULL, true><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn,
                                                                      x->Ubuf, x->sc);
@@ -528,14 +466,6 @@ void launch_update(Ctx *x, const double *pi, const double *pb, double *pf)
                                                                       x->Ubuf, x->sc);
   k_invert<<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->katm,
                                                         x->sc);
-  return;
-#endif
-  if (G.n3 > 1)
-    k_update<FULL, true><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, pf, B.F1, B.F2, B.F3, x->pflag,
-                                                                       x->geo, x->conn, x->floors, x->katm, x->sc);
-  else
-    k_update<FULL, false><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, pf, B.F1, B.F2, B.F3, x->pflag,
-                                                                        x->geo, x->conn, x->floors, x->katm, x->sc);
 }
 
 // advance() + fixup + bound_prim + fixup_utoprim + bound_prim (step_ch.c:101-117)
