@@ -28,9 +28,16 @@
 #ifndef HARM_INV_MINB
 #define HARM_INV_MINB 1
 #endif
+// phi planes each block sweeps: consecutive planes of one (r, theta) tile
+// reuse its geometry and (for the phi-direction fluxes) its stencil from L1
+#ifndef HARM_HB
+#define HARM_HB 4
+#endif
 
 namespace harm {
 namespace HARM_VARIANT {
+
+inline dim3 zone_grid_hb(const Grid &G) { return dim3((G.n2 + 31) / 32, (G.n1 + 3) / 4, (G.n3 + HARM_HB - 1) / HARM_HB); }
 
 #if HARM_STEP_MIXED
 using flux_t = float;
@@ -80,10 +87,10 @@ __global__ void __launch_bounds__(128, HARM_FLUX_MINB) k_flux(Grid G, const doub
   if (sc->halted) return;
   const int j = (DIR == 2 ? G.jstart : G.jstart - 1) + blockIdx.x * blockDim.x + threadIdx.x;
   const int i = (DIR == 1 ? G.istart : G.istart - 1) + blockIdx.y * blockDim.y + threadIdx.y;
-  const int h = blockIdx.z;
+  const int h0 = blockIdx.z * HARM_HB, h1 = min(G.n3, h0 + HARM_HB);
   double dtmin = 1.e9;
   const bool in = (i <= G.istop + 1) && (j <= G.jstop + 1);
-  if (in) {
+  if (in) for (int h = h0; h < h1; h++) {
     const long c = cidx(G, h, i, j);
     if (DIR == 2 && (j == G.jstart || j == G.jstop + 1)) {
 #pragma unroll
@@ -132,7 +139,7 @@ __global__ void __launch_bounds__(128, HARM_FLUX_MINB) k_flux(Grid G, const doub
       if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
       if (FULL && i >= G.istart && i <= G.istop && j >= G.jstart && j <= G.jstop) {
         const double dxd = DIR == 1 ? G.dx1 : DIR == 2 ? G.dx2 : G.dx3;
-        dtmin = G.cour * dxd / ctop;
+        dtmin = fmin(dtmin, G.cour * dxd / ctop);
       }
     }
   }
@@ -154,9 +161,10 @@ void launch_flux(const Grid &G, cudaStream_t st, const double *pb, flux_t *F1, f
                  const double *geo, const float *geo32, DevScalars *sc)
 {
   dim3 b(32, 4);
-  dim3 g1((G.n2 + 2 + 31) / 32, (G.n1 + 1 + 3) / 4, G.n3);
-  dim3 g2((G.n2 + 1 + 31) / 32, (G.n1 + 2 + 3) / 4, G.n3);
-  dim3 g3((G.n2 + 2 + 31) / 32, (G.n1 + 2 + 3) / 4, G.n3);
+  const int gz = (G.n3 + HARM_HB - 1) / HARM_HB;
+  dim3 g1((G.n2 + 2 + 31) / 32, (G.n1 + 1 + 3) / 4, gz);
+  dim3 g2((G.n2 + 1 + 31) / 32, (G.n1 + 2 + 3) / 4, gz);
+  dim3 g3((G.n2 + 2 + 31) / 32, (G.n1 + 2 + 3) / 4, gz);
   k_flux<1, FULL><<<g1, b, 0, st>>>(G, pb, F1, geo, geo32, sc);
   k_flux<2, FULL><<<g2, b, 0, st>>>(G, pb, F2, geo, geo32, sc);
   if (G.n3 > 1) k_flux<3, FULL><<<g3, b, 0, st>>>(G, pb, F3, geo, geo32, sc);
@@ -272,11 +280,9 @@ __device__ __forceinline__ int conn_slot(int k, int a, int b)
   return k * 10 + pair;
 }
 
-__device__ void source(double gam, const double *pb, const Geo &q, const double *__restrict__ conn, long ng, long gi,
-                       double *dU, int *fail)
+__device__ __forceinline__ void source_of_state(double gam, const double *pb, const State &s, const Geo &q,
+                                                const double *__restrict__ conn, long ng, long gi, double *dU)
 {
-  State s;
-  get_state(pb, q, s, fail);
   double mhd[4][4];
 #pragma unroll
   for (int d = 0; d < 4; d++) mhd_calc(gam, pb, d, s, mhd[d]);
@@ -293,6 +299,14 @@ __device__ void source(double gam, const double *pb, const Geo &q, const double 
     }
 #pragma unroll
   for (int k = 0; k < 8; k++) dU[k] *= q.g;
+}
+
+__device__ void source(double gam, const double *pb, const Geo &q, const double *__restrict__ conn, long ng, long gi,
+                       double *dU, int *fail)
+{
+  State s;
+  get_state(pb, q, s, fail);
+  source_of_state(gam, pb, s, q, conn, ng, gi, dU);
 }
 
 // The zone update (step_ch.c:237-306) in two launches, so that each holds
@@ -316,22 +330,33 @@ __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const doub
   if (sc->halted) return;
   const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
   const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
-  const int h = blockIdx.z;
   if (i > G.istop || j > G.jstop) return;
   const double Dt = FULL ? sc->dt : 0.5 * sc->dt;
+  const int h0 = blockIdx.z * HARM_HB, h1 = min(G.n3, h0 + HARM_HB);
+  for (int h = h0; h < h1; h++) {
   const long c = cidx(G, h, i, j);
   const long gi = (long)i * G.sn2 + j;
   int fail = 0;
   Geo q;
   load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
   double dU[8], U[8];
-  {
-    double pbz[8];
+  if (!FULL) {
+    // the predictor advances from pi == pb (advance(p, p, ...), step_ch.c:101):
+    // one state serves both source() and primtoU()
+    double pz[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) pbz[k] = __ldg(pb + k * G.nc + c);
-    source(G.gam, pbz, q, conn, G.ng, gi, dU, &fail);
-  }
-  {
+    for (int k = 0; k < 8; k++) pz[k] = __ldg(pb + k * G.nc + c);
+    State s;
+    get_state(pz, q, s, &fail);
+    source_of_state(G.gam, pz, s, q, conn, G.ng, gi, dU);
+    primtoflux(G.gam, pz, s, 0, q.g, U);
+  } else {
+    {
+      double pbz[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) pbz[k] = __ldg(pb + k * G.nc + c);
+      source(G.gam, pbz, q, conn, G.ng, gi, dU, &fail);
+    }
     double pz[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) pz[k] = __ldg(pi + k * G.nc + c);
@@ -354,6 +379,7 @@ __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const doub
 #pragma unroll
   for (int k = 0; k < 8; k++) Ub[k * G.nc + c] = U[k];
   if (fail) record_fail(sc, fail, h + (THREE_D ? 1 : 0), i, j);
+  }
 }
 
 __global__ void __launch_bounds__(128, HARM_INV_MINB) k_invert(Grid G, const double *__restrict__ pi,
@@ -367,8 +393,9 @@ __global__ void __launch_bounds__(128, HARM_INV_MINB) k_invert(Grid G, const dou
   if (sc->halted) return;
   const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
   const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
-  const int h = blockIdx.z;
   if (i > G.istop || j > G.jstop) return;
+  const int h0 = blockIdx.z * HARM_HB, h1 = min(G.n3, h0 + HARM_HB);
+  for (int h = h0; h < h1; h++) {
   const long c = cidx(G, h, i, j);
   const long gi = (long)i * G.sn2 + j;
   int fail = 0;
@@ -392,6 +419,7 @@ __global__ void __launch_bounds__(128, HARM_INV_MINB) k_invert(Grid G, const dou
   for (int k = 0; k < 8; k++) pf[k * G.nc + c] = pz[k];
   pflag[c] = fl;
   if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
+  }
 }
 
 // diag_flux() (diag.c:437-465): sums over the inner radial face, after the
@@ -458,13 +486,14 @@ void launch_update(Ctx *x, const double *pi, const double *pb, double *pf)
 {
   const Grid &G = x->G;
   Bufs B = bufs(x);
+  const dim3 zg = zone_grid_hb(G);
   if (G.n3 > 1)
-    k_cons<FULL, true><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn,
+    k_cons<FULL, true><<<zg, dim3(32, 4), 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn,
                                                                      x->Ubuf, x->sc);
   else
-    k_cons<FULL, false><<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn,
+    k_cons<FULL, false><<<zg, dim3(32, 4), 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn,
                                                                       x->Ubuf, x->sc);
-  k_invert<<<zone_grid(G), dim3(32, 4), 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->katm,
+  k_invert<<<zg, dim3(32, 4), 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->katm,
                                                         x->sc);
 }
 
