@@ -12,4 +12,7 @@
 #ifndef HARM_INV_MINB
 #define HARM_INV_MINB 5    // 102 registers
 #endif
+#ifndef HARM_HB_FLUX
+#define HARM_HB_FLUX 8
+#endif
 #include "harm_step.cuh"

@@ -28,16 +28,23 @@
 #ifndef HARM_INV_MINB
 #define HARM_INV_MINB 1
 #endif
-// phi planes each block sweeps: consecutive planes of one (r, theta) tile
-// reuse its geometry and (for the phi-direction fluxes) its stencil from L1
-#ifndef HARM_HB
-#define HARM_HB 4
+// phi planes each block sweeps, for the flux and for the zone kernels:
+// consecutive planes of one (r, theta) tile reuse its geometry and (for the
+// phi-direction fluxes) its stencil from L1
+#ifndef HARM_HB_FLUX
+#define HARM_HB_FLUX 1
+#endif
+#ifndef HARM_HB_ZONE
+#define HARM_HB_ZONE 4
 #endif
 
 namespace harm {
 namespace HARM_VARIANT {
 
-inline dim3 zone_grid_hb(const Grid &G) { return dim3((G.n2 + 31) / 32, (G.n1 + 3) / 4, (G.n3 + HARM_HB - 1) / HARM_HB); }
+inline dim3 zone_grid_hb(const Grid &G)
+{
+  return dim3((G.n2 + 31) / 32, (G.n1 + 3) / 4, (G.n3 + HARM_HB_ZONE - 1) / HARM_HB_ZONE);
+}
 
 #if HARM_STEP_MIXED
 using flux_t = float;
@@ -87,7 +94,7 @@ __global__ void __launch_bounds__(128, HARM_FLUX_MINB) k_flux(Grid G, const doub
   if (sc->halted) return;
   const int j = (DIR == 2 ? G.jstart : G.jstart - 1) + blockIdx.x * blockDim.x + threadIdx.x;
   const int i = (DIR == 1 ? G.istart : G.istart - 1) + blockIdx.y * blockDim.y + threadIdx.y;
-  const int h0 = blockIdx.z * HARM_HB, h1 = min(G.n3, h0 + HARM_HB);
+  const int h0 = blockIdx.z * HARM_HB_FLUX, h1 = min(G.n3, h0 + HARM_HB_FLUX);
   double dtmin = 1.e9;
   const bool in = (i <= G.istop + 1) && (j <= G.jstop + 1);
   if (in) for (int h = h0; h < h1; h++) {
@@ -161,7 +168,7 @@ void launch_flux(const Grid &G, cudaStream_t st, const double *pb, flux_t *F1, f
                  const double *geo, const float *geo32, DevScalars *sc)
 {
   dim3 b(32, 4);
-  const int gz = (G.n3 + HARM_HB - 1) / HARM_HB;
+  const int gz = (G.n3 + HARM_HB_FLUX - 1) / HARM_HB_FLUX;
   dim3 g1((G.n2 + 2 + 31) / 32, (G.n1 + 1 + 3) / 4, gz);
   dim3 g2((G.n2 + 1 + 31) / 32, (G.n1 + 2 + 3) / 4, gz);
   dim3 g3((G.n2 + 2 + 31) / 32, (G.n1 + 2 + 3) / 4, gz);
@@ -332,7 +339,7 @@ __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const doub
   const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
   if (i > G.istop || j > G.jstop) return;
   const double Dt = FULL ? sc->dt : 0.5 * sc->dt;
-  const int h0 = blockIdx.z * HARM_HB, h1 = min(G.n3, h0 + HARM_HB);
+  const int h0 = blockIdx.z * HARM_HB_ZONE, h1 = min(G.n3, h0 + HARM_HB_ZONE);
   for (int h = h0; h < h1; h++) {
   const long c = cidx(G, h, i, j);
   const long gi = (long)i * G.sn2 + j;
@@ -394,7 +401,7 @@ __global__ void __launch_bounds__(128, HARM_INV_MINB) k_invert(Grid G, const dou
   const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
   const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
   if (i > G.istop || j > G.jstop) return;
-  const int h0 = blockIdx.z * HARM_HB, h1 = min(G.n3, h0 + HARM_HB);
+  const int h0 = blockIdx.z * HARM_HB_ZONE, h1 = min(G.n3, h0 + HARM_HB_ZONE);
   for (int h = h0; h < h1; h++) {
   const long c = cidx(G, h, i, j);
   const long gi = (long)i * G.sn2 + j;
