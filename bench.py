@@ -288,6 +288,63 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_ensemble(args):
+    """64 seeded 2D tori (N1, N2 from {96,128,192,256}, a, Rmax, beta drawn) advanced
+    as one ensemble -- one CUDA graph launch per step, mixed precision, tiles chosen
+    by the autotuner per resolution -- against the same 64 tori run one after the
+    other on the plain FP64 path.  Aggregate zone-cycles/s over all members."""
+    import harm_cool_b200 as hc
+    drawn = hc.ensemble_problems(args.members, seed=args.seed)
+    probs = [p for p, _ in drawn]
+    zones = sum(p.zones for p in probs)
+    # sequential plain runs: each torus alone, FP64, default tile
+    seq_ms = 0.0
+    for pr in probs:
+        c = hc.Context(pr)
+        c.init_torus()
+        c.run(args.warmup)
+        seq_ms += c.run_timed(args.steps)
+        c.close()
+    out = {}
+    for name, mixed in (("ensemble_mixed", True), ("ensemble_fp64", False)):
+        ctxs = []
+        tiles = {}
+        for pr in probs:
+            c = hc.Context(pr)
+            c.init_torus()
+            if mixed:
+                c.set_precision(hc.Context.MIXED)
+            key = (pr.params.n1, pr.params.n2)
+            if key not in tiles:
+                tiles[key] = c.autotune_tile(steps=3)
+            c.set_tile(*tiles[key])
+            ctxs.append(c)
+        ens = hc.Ensemble(ctxs)
+        ens.run(args.warmup)
+        sampler = ClockSampler(0)
+        sampler.start()
+        ms = ens.run_timed(args.steps)
+        clocks = sampler.stop()
+        out[name] = {"value": zones * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                     "tiles": {"%dx%d" % k: list(v) for k, v in tiles.items()}, "clocks": clocks,
+                     "fail_codes": sorted({c.diag()["fail_code"] for c in ctxs})}
+        ens.close()
+        for c in ctxs:
+            c.close()
+    seq = zones * args.steps / (seq_ms / 1e3)
+    line = {"metric": "aggregate zone-cycles/s, %d seeded 2D tori" % args.members,
+            "value": out["ensemble_mixed"]["value"], "unit": "zone-cycles/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64/f32 mixed",
+            "data": "synthetic", "config": {"workload": "ensemble of %d 2D tori, N1,N2 in {96,128,192,256}, "
+                                                        "a in [0,0.98], Rmax in [9,14], beta in [30,300], seed %d"
+                                                        % (args.members, args.seed),
+                                            "zones": zones},
+            "sequential_fp64": {"value": seq, "ms_per_step": seq_ms / args.steps},
+            "speedup_vs_sequential": out["ensemble_mixed"]["value"] / seq,
+            "members": drawn and [d for _, d in drawn], **out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -300,12 +357,19 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
+    ap.add_argument("--workload", choices=("torus", "ensemble"), default="torus",
+                    help="torus: the 288x256x256 step (default); ensemble: 64 seeded 2D tori")
+    ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         # host-only: rank 0 times the reference, the other ranks have nothing to do
         run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
+    if args.workload == "ensemble":
+        run_ensemble(args)
         return
     world, rank, local = dist_setup()
     try:

@@ -15,7 +15,7 @@ import os
 
 import numpy as np
 
-__all__ = ["HarmError", "Params", "GridSpec", "TorusSpec", "Diag", "Problem", "Context",
+__all__ = ["HarmError", "Params", "GridSpec", "TorusSpec", "Diag", "Problem", "Context", "Ensemble",
            "torus_problem", "set_points", "set_grid", "set_katm", "utoprim_2d_batch", "library",
            "NPR", "NPG"]
 
@@ -97,6 +97,15 @@ _SIGNATURES = {
     "harm_fixup_utoprim": (ctypes.c_int, [ctypes.c_void_p, _DP]),
     "harm_utoprim_2d_batch": (ctypes.c_int, [_DP, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int),
                                              ctypes.c_long, ctypes.c_double]),
+    "harm_set_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "harm_get_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "harm_autotune_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int)]),
+    "harm_ensemble_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+    "harm_ensemble_destroy": (None, [ctypes.c_void_p]),
+    "harm_ensemble_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "harm_ensemble_run_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _DP]),
     "harm_utoprim_2d_batch_noalloc": (ctypes.c_int, [_DP, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int),
                                                      ctypes.c_long, ctypes.c_double]),
 }
@@ -318,6 +327,21 @@ class Context:
     def sync(self):
         _check(self.lib.harm_sync(self.h))
 
+    def set_tile(self, bx, by):
+        """Threads per block of the face and zone kernels (bx theta x by r, 128 in all)."""
+        _check(self.lib.harm_set_tile(self.h, bx, by))
+
+    def tile(self):
+        bx, by = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.harm_get_tile(self.h, ctypes.byref(bx), ctypes.byref(by)))
+        return bx.value, by.value
+
+    def autotune_tile(self, steps=3):
+        """Time each candidate tile on this state (restored afterwards); keep the fastest."""
+        bx, by = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.harm_autotune_tile(self.h, steps, ctypes.byref(bx), ctypes.byref(by)))
+        return bx.value, by.value
+
     def step_ch_host(self, p):
         """step_ch() on a host primitive array, in place (upload, step, download)."""
         assert p.flags["C_CONTIGUOUS"] and p.dtype == np.float64 and p.shape == self.shape + (NPR,)
@@ -343,3 +367,54 @@ class Context:
             cur = self.get_prims()
             self.put_prims(cur, pflag)
         return self._on_array(self.lib.harm_fixup_utoprim, pv)
+
+
+class Ensemble:
+    """Independent grids on one GPU advanced together: one CUDA graph launch per
+    ensemble step, each member stepping with its own dt (harm_ensemble_*)."""
+
+    def __init__(self, contexts):
+        self.lib = library()
+        self.members = list(contexts)
+        arr = (ctypes.c_void_p * len(self.members))(*[c.h for c in self.members])
+        h = ctypes.c_void_p()
+        _check(self.lib.harm_ensemble_create(arr, len(self.members), ctypes.byref(h)))
+        self.h = h
+
+    def run(self, nsteps):
+        _check(self.lib.harm_ensemble_run(self.h, nsteps))
+
+    def run_timed(self, nsteps):
+        ms = ctypes.c_double()
+        _check(self.lib.harm_ensemble_run_timed(self.h, nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.harm_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ensemble_problems(n, seed=0, sizes=(96, 128, 192, 256), a_range=(0.0, 0.98), rmax_range=(9.0, 14.0),
+                      beta_range=(30.0, 300.0)):
+    """n seeded 2D tori for an ensemble run: N1 and N2 drawn independently from
+    sizes, spin a, pressure-maximum radius Rmax and plasma beta drawn uniformly;
+    the rest as the benchmark torus (rin=6, gamma=4/3, kappa=1e-3, hslope=0.3,
+    Rout=100, grid inner radius 0.98 r_horizon).  Returns [(problem, draw)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        n1 = int(rng.choice(sizes))
+        n2 = int(rng.choice(sizes))
+        a = float(rng.uniform(*a_range))
+        rmax = float(rng.uniform(*rmax_range))
+        beta = float(rng.uniform(*beta_range))
+        out.append((torus_problem(n1, n2, 1, a=a, rmax=rmax, beta=beta),
+                    {"n1": n1, "n2": n2, "a": a, "rmax": rmax, "beta": beta}))
+    return out

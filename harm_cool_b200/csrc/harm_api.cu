@@ -626,6 +626,8 @@ extern "C" int harm_create(const harm_params *prm, const double *gcov, const dou
   G.gam = prm->gam; G.cour = prm->cour; G.defcon = prm->defcon; G.tf = prm->tf;
   G.dx1 = prm->dx[1]; G.dx2 = prm->dx[2]; G.dx3 = prm->dx[3];
   x->nparts = 148 * 4;
+  x->tbx = 32;
+  x->tby = 4;
   auto al = [&](void **p, size_t b) -> int { CK(cudaMalloc(p, b)); return HARM_OK; };
   const size_t st = 8 * G.nc * sizeof(double);
   int rc = HARM_OK;
@@ -1066,4 +1068,219 @@ extern "C" int harm_time_kernels(harm_ctx *h, int reps, double *ms)
   if (!h || !ms || reps < 1) return fail_with(HARM_E_ARG, "bad argument");
   Ctx *x = &h->x;
   return x->mode == HARM_MIXED ? mixed::time_kernels(x, reps, ms) : exact::time_kernels(x, reps, ms);
+}
+
+// ---------------------------------------------------------------------------
+// tile shapes and their autotuner
+
+static bool tile_ok(int bx, int by) { return bx >= 8 && by >= 1 && bx * by == 128 && (bx & 7) == 0; }
+
+static void drop_graph(Ctx *x)
+{
+  if (x->graph_exec) {
+    cudaGraphExecDestroy(x->graph_exec);
+    x->graph_exec = nullptr;
+  }
+}
+
+extern "C" int harm_set_tile(harm_ctx *h, int bx, int by)
+{
+  if (!h || !tile_ok(bx, by)) return fail_with(HARM_E_ARG, "tile must be bx x by = 128 threads, bx a multiple of 8");
+  Ctx *x = &h->x;
+  if (x->tbx != bx || x->tby != by) drop_graph(x);
+  x->tbx = bx;
+  x->tby = by;
+  return HARM_OK;
+}
+
+extern "C" int harm_get_tile(harm_ctx *h, int *bx, int *by)
+{
+  if (!h || !bx || !by) return fail_with(HARM_E_ARG, "null argument");
+  *bx = h->x.tbx;
+  *by = h->x.tby;
+  return HARM_OK;
+}
+
+// Times `steps` ordinary steps per candidate tile, each trial from the same
+// saved state (primitives, flags, run scalars), and keeps the fastest; the
+// state is restored afterwards, so the run continues as if untouched.
+extern "C" int harm_autotune_tile(harm_ctx *h, int steps, int *bx, int *by)
+{
+  if (!h || steps < 1) return fail_with(HARM_E_ARG, "bad argument");
+  Ctx *x = &h->x;
+  static const int cand[][2] = {{32, 4}, {64, 2}, {16, 8}, {128, 1}};
+  const size_t pb = (size_t)8 * x->G.nc * sizeof(double);
+  DevScalars s0;
+  int rc = read_scalars(x, &s0);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(x->stage, x->p, pb, cudaMemcpyDeviceToDevice, x->stream));
+  CK(cudaMemcpyAsync(x->stage_flag, x->pflag, x->G.nc, cudaMemcpyDeviceToDevice, x->stream));
+  const int keep_x = x->tbx, keep_y = x->tby;
+  EventPair e;
+  CK(cudaEventCreate(&e.a));
+  CK(cudaEventCreate(&e.b));
+  float best = -1.f;
+  int bi = 0;
+  for (int c = 0; c < 4; c++) {
+    x->tbx = cand[c][0];
+    x->tby = cand[c][1];
+    rc = launch_step(x);  // warm-up, from the saved state
+    if (!rc) {
+      CK(cudaEventRecord(e.a, x->stream));
+      for (int s = 0; s < steps && !rc; s++) rc = launch_step(x);
+      CK(cudaEventRecord(e.b, x->stream));
+      CK(cudaEventSynchronize(e.b));
+      float f;
+      CK(cudaEventElapsedTime(&f, e.a, e.b));
+      if (best < 0.f || f < best) { best = f; bi = c; }
+    }
+    // back to the saved state for the next candidate (and for the caller)
+    CK(cudaMemcpyAsync(x->p, x->stage, pb, cudaMemcpyDeviceToDevice, x->stream));
+    CK(cudaMemcpyAsync(x->pflag, x->stage_flag, x->G.nc, cudaMemcpyDeviceToDevice, x->stream));
+    int wr = write_scalars(x, &s0);
+    if (wr) return wr;
+    if (rc) {
+      x->tbx = keep_x;
+      x->tby = keep_y;
+      return rc;
+    }
+  }
+  drop_graph(x);
+  x->tbx = cand[bi][0];
+  x->tby = cand[bi][1];
+  if (bx) *bx = x->tbx;
+  if (by) *by = x->tby;
+  return sync_status(x);
+}
+
+// ---------------------------------------------------------------------------
+// ensembles: independent grids advanced together by one graph launch per step
+
+struct harm_ensemble {
+  std::vector<Ctx *> members;
+  std::vector<int> mode, tbx, tby;  // member settings the graph was captured with
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t exec = nullptr;
+};
+
+static void ensemble_free(harm_ensemble *e)
+{
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  for (cudaEvent_t v : e->join) if (v) cudaEventDestroy(v);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+extern "C" int harm_ensemble_create(harm_ctx *const *members, int n, harm_ensemble **out)
+{
+  if (!members || n < 1 || !out) return fail_with(HARM_E_ARG, "bad argument");
+  for (int k = 0; k < n; k++) {
+    if (!members[k]) return fail_with(HARM_E_ARG, "null member");
+    if (members[k]->x.device != members[0]->x.device) return fail_with(HARM_E_ARG, "members on different devices");
+    for (int m = 0; m < k; m++)
+      if (members[m] == members[k]) return fail_with(HARM_E_ARG, "a context appears twice");
+  }
+  harm_ensemble *e = new harm_ensemble();
+  e->device = members[0]->x.device;
+  for (int k = 0; k < n; k++) e->members.push_back(&members[k]->x);
+  e->mode.assign(n, -1);
+  e->tbx.assign(n, 0);
+  e->tby.assign(n, 0);
+  e->join.assign(n, nullptr);
+  if (cudaSetDevice(e->device) != cudaSuccess || cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) {
+    ensemble_free(e);
+    return fail_with(HARM_E_CUDA, "ensemble stream");
+  }
+  for (int k = 0; k < n; k++)
+    if (cudaEventCreateWithFlags(&e->join[k], cudaEventDisableTiming) != cudaSuccess) {
+      ensemble_free(e);
+      return fail_with(HARM_E_CUDA, "ensemble events");
+    }
+  *out = e;
+  return HARM_OK;
+}
+
+extern "C" void harm_ensemble_destroy(harm_ensemble *e)
+{
+  if (e) ensemble_free(e);
+}
+
+// (Re)capture when a member's precision or tile changed since the last capture.
+static int ensemble_graph(harm_ensemble *e)
+{
+  bool same = e->exec != nullptr;
+  for (size_t k = 0; k < e->members.size() && same; k++) {
+    const Ctx *x = e->members[k];
+    same = x->mode == e->mode[k] && x->tbx == e->tbx[k] && x->tby == e->tby[k];
+  }
+  if (same) return HARM_OK;
+  if (e->exec) {
+    cudaGraphExecDestroy(e->exec);
+    e->exec = nullptr;
+  }
+  CK(cudaSetDevice(e->device));
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = HARM_OK;
+  cudaError_t ce = cudaEventRecord(e->fork, e->stream);
+  for (size_t k = 0; k < e->members.size() && ce == cudaSuccess && rc == HARM_OK; k++) {
+    Ctx *x = e->members[k];
+    ce = cudaStreamWaitEvent(x->stream, e->fork, 0);
+    if (ce == cudaSuccess) rc = launch_step(x);
+    if (ce == cudaSuccess && rc == HARM_OK) ce = cudaEventRecord(e->join[k], x->stream);
+    if (ce == cudaSuccess && rc == HARM_OK) ce = cudaStreamWaitEvent(e->stream, e->join[k], 0);
+    e->mode[k] = x->mode;
+    e->tbx[k] = x->tbx;
+    e->tby[k] = x->tby;
+  }
+  cudaError_t ee = cudaStreamEndCapture(e->stream, &g);
+  if (rc) return rc;
+  if (ce != cudaSuccess) return fail_with(HARM_E_CUDA, std::string("ensemble capture: ") + cudaGetErrorString(ce));
+  if (ee != cudaSuccess) return fail_with(HARM_E_CUDA, std::string("ensemble capture: ") + cudaGetErrorString(ee));
+  ce = cudaGraphInstantiate(&e->exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) return fail_with(HARM_E_CUDA, std::string("ensemble instantiate: ") + cudaGetErrorString(ce));
+  return HARM_OK;
+}
+
+static int ensemble_status(harm_ensemble *e)
+{
+  CK(cudaStreamSynchronize(e->stream));
+  for (Ctx *x : e->members) {
+    int rc = sync_status(x);
+    if (rc) return rc;
+  }
+  return HARM_OK;
+}
+
+extern "C" int harm_ensemble_run(harm_ensemble *e, int nsteps)
+{
+  if (!e || nsteps < 0) return fail_with(HARM_E_ARG, "bad argument");
+  int rc = ensemble_graph(e);
+  if (rc) return rc;
+  for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(e->exec, e->stream));
+  return ensemble_status(e);
+}
+
+extern "C" int harm_ensemble_run_timed(harm_ensemble *e, int nsteps, double *ms)
+{
+  if (!e || !ms || nsteps < 0) return fail_with(HARM_E_ARG, "bad argument");
+  int rc = ensemble_graph(e);
+  if (rc) return rc;
+  EventPair ev;
+  CK(cudaEventCreate(&ev.a));
+  CK(cudaEventCreate(&ev.b));
+  CK(cudaEventRecord(ev.a, e->stream));
+  for (int s = 0; s < nsteps; s++) CK(cudaGraphLaunch(e->exec, e->stream));
+  CK(cudaEventRecord(ev.b, e->stream));
+  CK(cudaEventSynchronize(ev.b));
+  float f;
+  CK(cudaEventElapsedTime(&f, ev.a, ev.b));
+  *ms = f;
+  return ensemble_status(e);
 }

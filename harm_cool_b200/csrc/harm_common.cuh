@@ -67,6 +67,7 @@ struct Ctx {
   float *F1f, *F2f, *F3f;        // mixed mode: FP32 face fluxes [8][nc]
   float *geo32;                  // mixed mode: FP32 face geometry [3][GEO_N][ng]
   double *Ubuf;                  // conserved variables between the two update launches [8][nc]
+  int tbx, tby;                  // tile of the zone and face kernels: theta x r threads, 128 in all
 };
 
 __device__ __forceinline__ void record_fail(DevScalars *sc, int code, int h, int i, int j)

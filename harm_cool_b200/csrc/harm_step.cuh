@@ -41,9 +41,10 @@
 namespace harm {
 namespace HARM_VARIANT {
 
-inline dim3 zone_grid_hb(const Grid &G)
+// blocks of tile.x (theta) by tile.y (r) zones, HARM_HB_ZONE phi planes each
+inline dim3 zone_grid_hb(const Grid &G, dim3 tile)
 {
-  return dim3((G.n2 + 31) / 32, (G.n1 + 3) / 4, (G.n3 + HARM_HB_ZONE - 1) / HARM_HB_ZONE);
+  return dim3((G.n2 + tile.x - 1) / tile.x, (G.n1 + tile.y - 1) / tile.y, (G.n3 + HARM_HB_ZONE - 1) / HARM_HB_ZONE);
 }
 
 #if HARM_STEP_MIXED
@@ -164,14 +165,13 @@ __global__ void __launch_bounds__(128, HARM_FLUX_MINB) k_flux(Grid G, const doub
 }
 
 template <bool FULL>
-void launch_flux(const Grid &G, cudaStream_t st, const double *pb, flux_t *F1, flux_t *F2, flux_t *F3,
+void launch_flux(const Grid &G, dim3 b, cudaStream_t st, const double *pb, flux_t *F1, flux_t *F2, flux_t *F3,
                  const double *geo, const float *geo32, DevScalars *sc)
 {
-  dim3 b(32, 4);
   const int gz = (G.n3 + HARM_HB_FLUX - 1) / HARM_HB_FLUX;
-  dim3 g1((G.n2 + 2 + 31) / 32, (G.n1 + 1 + 3) / 4, gz);
-  dim3 g2((G.n2 + 1 + 31) / 32, (G.n1 + 2 + 3) / 4, gz);
-  dim3 g3((G.n2 + 2 + 31) / 32, (G.n1 + 2 + 3) / 4, gz);
+  dim3 g1((G.n2 + 2 + b.x - 1) / b.x, (G.n1 + 1 + b.y - 1) / b.y, gz);
+  dim3 g2((G.n2 + 1 + b.x - 1) / b.x, (G.n1 + 2 + b.y - 1) / b.y, gz);
+  dim3 g3((G.n2 + 2 + b.x - 1) / b.x, (G.n1 + 2 + b.y - 1) / b.y, gz);
   k_flux<1, FULL><<<g1, b, 0, st>>>(G, pb, F1, geo, geo32, sc);
   k_flux<2, FULL><<<g2, b, 0, st>>>(G, pb, F2, geo, geo32, sc);
   if (G.n3 > 1) k_flux<3, FULL><<<g3, b, 0, st>>>(G, pb, F3, geo, geo32, sc);
@@ -493,14 +493,15 @@ void launch_update(Ctx *x, const double *pi, const double *pb, double *pf)
 {
   const Grid &G = x->G;
   Bufs B = bufs(x);
-  const dim3 zg = zone_grid_hb(G);
+  const dim3 tile(x->tbx, x->tby);
+  const dim3 zg = zone_grid_hb(G, tile);
   if (G.n3 > 1)
-    k_cons<FULL, true><<<zg, dim3(32, 4), 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn,
+    k_cons<FULL, true><<<zg, tile, 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn,
                                                                      x->Ubuf, x->sc);
   else
-    k_cons<FULL, false><<<zg, dim3(32, 4), 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn,
+    k_cons<FULL, false><<<zg, tile, 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn,
                                                                       x->Ubuf, x->sc);
-  k_invert<<<zg, dim3(32, 4), 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->katm,
+  k_invert<<<zg, tile, 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->katm,
                                                         x->sc);
 }
 
@@ -509,7 +510,7 @@ template <bool FULL>
 void launch_half(Ctx *x, const double *pi, const double *pb, double *pf)
 {
   Bufs B = bufs(x);
-  launch_flux<FULL>(x->G, x->stream, pb, B.F1, B.F2, B.F3, x->geo, x->geo32, x->sc);
+  launch_flux<FULL>(x->G, dim3(x->tbx, x->tby), x->stream, pb, B.F1, B.F2, B.F3, x->geo, x->geo32, x->sc);
   launch_update<FULL>(x, pi, pb, pf);
   if (FULL) k_diag_flux<<<1, 1024, 0, x->stream>>>(x->G, B.F1, x->sc);
   launch_bound(x, pf);
@@ -543,8 +544,9 @@ int time_kernels(Ctx *x, int reps, double *ms)
     for (int half = 0; half < 2; half++) {
       const bool full = half == 1;
       double *pi = x->p, *pb = full ? x->ph : x->p, *pf = full ? x->p : x->ph;
-      if (full) launch_flux<true>(G, x->stream, pb, B.F1, B.F2, B.F3, x->geo, x->geo32, x->sc);
-      else launch_flux<false>(G, x->stream, pb, B.F1, B.F2, B.F3, x->geo, x->geo32, x->sc);
+      const dim3 tile(x->tbx, x->tby);
+      if (full) launch_flux<true>(G, tile, x->stream, pb, B.F1, B.F2, B.F3, x->geo, x->geo32, x->sc);
+      else launch_flux<false>(G, tile, x->stream, pb, B.F1, B.F2, B.F3, x->geo, x->geo32, x->sc);
       slot[e] = 0; CK(cudaEventRecord(ev[e++], x->stream));
       if (full) launch_update<true>(x, pi, pb, pf);
       else launch_update<false>(x, pi, pb, pf);

@@ -164,6 +164,37 @@ int harm_time_kernels(harm_ctx *ctx, int reps, double *ms);
 /* Block until the context's stream is idle; returns any pending device error. */
 int harm_sync(harm_ctx *ctx);
 
+/* ---- tile shapes (no reference counterpart: the reference runs on CPUs) ---- */
+
+/* Threads per block of the face and zone kernels: bx along theta by by along r,
+   bx * by = 128, bx a multiple of 8 (default 32 x 4). */
+int harm_set_tile(harm_ctx *ctx, int bx, int by);
+int harm_get_tile(harm_ctx *ctx, int *bx, int *by);
+
+/* Autotuner: times `steps` steps with each candidate tile (32x4, 64x2, 16x8,
+   128x1), every trial from the same saved state, restores that state, keeps
+   the fastest tile and returns it in *bx, *by (either may be NULL). */
+int harm_autotune_tile(harm_ctx *ctx, int steps, int *bx, int *by);
+
+/* ---- ensembles: many independent grids on one GPU (no reference counterpart:
+   the reference advances one compile-time grid per run) ---- */
+
+typedef struct harm_ensemble harm_ensemble;
+
+/* Bind n contexts created on the same device.  Each ensemble step advances every
+   member by one step_ch() with its own dt, as harm_step_ch would; the members'
+   step sequences are captured as parallel branches of one CUDA graph, launched
+   once per ensemble step.  The members stay usable on their own; a member whose
+   precision or tile changes is re-captured at the next run. */
+int harm_ensemble_create(harm_ctx *const *members, int n, harm_ensemble **out);
+void harm_ensemble_destroy(harm_ensemble *ens);
+
+/* nsteps ensemble steps; synchronises and returns the first member error. */
+int harm_ensemble_run(harm_ensemble *ens, int nsteps);
+
+/* harm_ensemble_run() with the device time of the nsteps graph launches in *ms. */
+int harm_ensemble_run_timed(harm_ensemble *ens, int nsteps, double *ms);
+
 /* ---- the reference's per-array entry points, on host arrays of the context's shape ---- */
 
 int harm_fixup(harm_ctx *ctx, double *pv);                        /* fixup.c:51-60, decs.h:567 */
