@@ -147,10 +147,15 @@ __global__ void k_bound(Grid G, double *P, signed char *pflag, const double *__r
 // then repairs failed zones in loop order, in place.  Repairs from the edge
 // or corner stencils read only good zones, which the repair never changes;
 // the last-resort average reads every neighbour and so sees earlier repairs.
-// k_fu_flip flips the flags and lists the failed zones; k_fu_fix sorts the
-// list into loop order, precomputes the stencil repairs in parallel and then
-// replays the whole list in order on one thread, recomputing any zone whose
-// stencil choice changed or that needs the last-resort average.
+// k_fu_flip flips the flags and lists the failed zones.  For a few failures
+// k_fu_fix sorts the list into loop order, precomputes the stencil repairs in
+// parallel and then replays the whole list in order on one thread,
+// recomputing any zone whose stencil choice changed or that needs the
+// last-resort average.  For many failures k_fu_wave repairs them in
+// wavefronts instead: a repair reads only its own phi plane, and within a
+// plane zone (i, j) depends only on (i-1, j-1..j+1) and (i, j-1), all on
+// earlier lines 2i + j = const, so each plane is one block that sweeps those
+// lines in order with a barrier between them -- the loop order's results.
 
 __global__ void k_fu_flip(Grid G, signed char *pflag, int *list, DevScalars *sc)
 {
@@ -220,15 +225,16 @@ __global__ void __launch_bounds__(NTHR_FIX) k_fu_fix(Grid G, double *P, signed c
                                                      DevScalars *sc)
 {
   if (sc->halted) return;
-  __shared__ int keys[FAIL_CAP];
-  __shared__ signed char kinds[FAIL_CAP];
+  __shared__ int keys[FIX_LIST_MAX];
+  __shared__ signed char kinds[FIX_LIST_MAX];
   __shared__ int gfail;
   const int n = sc->nfail;
   if (n == 0) return;
+  if (n > FIX_LIST_MAX || sc->fail_overflow) return;  // k_fu_wave's case
   const int tid = threadIdx.x;
   if (tid == 0) gfail = 0;
   const double *gC = geo_at(geo, G, L_CENT);
-  if (!sc->fail_overflow) {
+  {
     // bitonic sort of the failed cells into loop order
     int m = 1;
     while (m < n) m <<= 1;
@@ -293,27 +299,54 @@ __global__ void __launch_bounds__(NTHR_FIX) k_fu_fix(Grid G, double *P, signed c
         pflag[c] = g33 ? (signed char)-33 : (signed char)0;
       }
     }
-  } else if (tid == 0) {
-    // more failures than the list holds: the reference's loop, one thread
-    for (int h = 0; h < G.n3; h++)
-      for (int i = G.istart; i <= G.istop; i++)
-        for (int j = G.jstart; j <= G.jstop; j++) {
-          long c = cidx(G, h, i, j);
-          if (pflag[c] != 0) continue;
-          double v[8];
-          repair_zone(G, P, c, stencil_kind(G, pflag, c), v);
-          long gi = (long)i * G.sn2 + j;
-          Geo q;
-          load_geo(gC, G.ng, gi, q);
-          int fail = 0;
-          bool g33 = fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
-          if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
-          for (int k = 0; k < 8; k++) P[k * G.nc + c] = v[k];
-          pflag[c] = g33 ? (signed char)-33 : (signed char)0;
-        }
   }
   __syncthreads();
   if (tid == 0) {
+    sc->nfail = 0;
+    sc->fail_overflow = 0;
+  }
+}
+
+// many failures: one block per phi plane, wavefronts 2i + j in order
+__global__ void __launch_bounds__(256) k_fu_wave(Grid G, double *P, signed char *pflag,
+                                                 const double *__restrict__ geo, const double *__restrict__ floors,
+                                                 DevScalars *sc)
+{
+  if (sc->halted) return;
+  const int n = sc->nfail;
+  if (n == 0) return;  // none, or k_fu_fix has repaired them
+  const int h = blockIdx.x;
+  const double *gC = geo_at(geo, G, L_CENT);
+  const int w0 = 2 * G.istart + G.jstart, w1 = 2 * G.istop + G.jstop;
+  for (int w = w0; w <= w1; w++) {
+    // i such that j = w - 2i lies in [jstart, jstop]
+    int ilo = (w - G.jstop + 1) / 2, ihi = (w - G.jstart) / 2;
+    if (ilo < G.istart) ilo = G.istart;
+    if (ihi > G.istop) ihi = G.istop;
+    for (int i = ilo + (int)threadIdx.x; i <= ihi; i += blockDim.x) {
+      const int j = w - 2 * i;
+      const long c = cidx(G, h, i, j);
+      if (pflag[c] != 0) continue;
+      double v[8];
+      repair_zone(G, P, c, stencil_kind(G, pflag, c), v);
+      const long gi = (long)i * G.sn2 + j;
+      Geo q;
+      load_geo(gC, G.ng, gi, q);
+      int fail = 0;
+      bool g33 = fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
+      if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
+      for (int k = 0; k < 8; k++) P[k * G.nc + c] = v[k];
+      pflag[c] = g33 ? (signed char)-33 : (signed char)0;
+    }
+    __syncthreads();
+  }
+  // the last block to finish clears the counters for the next call
+  __shared__ bool last;
+  __threadfence();
+  if (threadIdx.x == 0) last = atomicAdd(&sc->wave_done, 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    sc->wave_done = 0;
     sc->nfail = 0;
     sc->fail_overflow = 0;
   }
@@ -544,6 +577,7 @@ int launch_fixup_utoprim(Ctx *x, double *P)
   const Grid &G = x->G;
   k_fu_flip<<<148 * 8, 256, 0, x->stream>>>(G, x->pflag, x->fail_list, x->sc);
   k_fu_fix<<<1, NTHR_FIX, 0, x->stream>>>(G, P, x->pflag, x->fail_list, x->fix_buf, x->geo, x->floors, x->sc);
+  k_fu_wave<<<G.n3, 256, 0, x->stream>>>(G, P, x->pflag, x->geo, x->floors, x->sc);
   return HARM_OK;
 }
 

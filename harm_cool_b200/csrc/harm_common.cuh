@@ -23,6 +23,7 @@ struct DevScalars {
   int err;                         // HARM_E_DT when dt < 1e-9
   int halted;                      // set after a failure: later steps do nothing
   int nfail, fail_overflow;        // failed zones met by the current fixup_utoprim
+  int wave_done;                   // blocks of k_fu_wave finished (reset by the last)
 };
 
 // Problem description passed by value to every kernel.
@@ -36,7 +37,8 @@ struct Grid {
   double dx1, dx2, dx3;
 };
 
-constexpr int FAIL_CAP = 8192;  // failed zones repaired through the sorted list
+constexpr int FAIL_CAP = 8192;     // failed zones listed by k_fu_flip
+constexpr int FIX_LIST_MAX = 512;  // up to this many, repaired through the sorted list
 constexpr int NTHR_FIX = 1024;
 
 struct Ctx {

@@ -38,10 +38,10 @@ def test_ensemble_step_equals_solo_steps(hc, mixed):
     tiles = [None, (64, 2), (16, 8), None, (128, 1), None]
     ens_ctx = [_fresh(hc, pr, mixed, t) for pr, t in zip(probs, tiles)]
     ens = hc.Ensemble(ens_ctx)
-    ens.run(12)
+    ens.run(40)
     for pr, t, ce in zip(probs, tiles, ens_ctx):
         solo = _fresh(hc, pr, mixed, t)
-        solo.run(12)
+        solo.run(40)
         a, fa = ce.get_prims(with_flags=True)
         b, fb = solo.get_prims(with_flags=True)
         np.testing.assert_array_equal(a, b)
@@ -49,8 +49,9 @@ def test_ensemble_step_equals_solo_steps(hc, mixed):
         assert ce.time() == solo.time()
         assert ce.diag()["fail_code"] == 0
         solo.close()
-    # members keep their own dt: differently sized grids end at different times
-    assert len({c.time()[0] for c in ens_ctx}) > 1
+    # members keep their own dt: once the Courant limit binds (after the
+    # initial ramp of 1.3x per step), differently sized grids step differently
+    assert len({c.time()[1] for c in ens_ctx}) > 1
     # a member changed after binding is re-captured at the next run
     ens_ctx[0].set_tile(64, 2)
     ens.run(2)

@@ -127,10 +127,12 @@ def test_bound_prim_and_fixup_match_oracle(shape, hc, oracle_built):
         np.testing.assert_array_equal(active(pr, a), active(pr, b), err_msg=name)
 
 
-@pytest.mark.parametrize("shape", [(32, 32, 1), (16, 16, 4)])
-def test_fixup_utoprim_repairs_like_oracle(shape, hc, oracle_built):
+@pytest.mark.parametrize("shape,nfail", [((32, 32, 1), 40), ((16, 16, 4), 40), ((48, 40, 1), 700),
+                                         ((24, 20, 4), 900)])
+def test_fixup_utoprim_repairs_like_oracle(shape, nfail, hc, oracle_built):
     """Injected failure flags, including neighbouring failures that need the
-    last-resort average and so depend on the repair order."""
+    last-resort average and so depend on the repair order; few failures take
+    the sorted-list repair, many take the wavefront repair."""
     import ctypes
     from oracle.pyoracle import oracle_lib
     pr = hc.torus_problem(*shape)
@@ -140,7 +142,7 @@ def test_fixup_utoprim_repairs_like_oracle(shape, hc, oracle_built):
     rng = np.random.default_rng(11)
     act = active(pr, fl)
     n1, n2 = pr.params.n1, pr.params.n2
-    for _ in range(40):
+    for _ in range(nfail):
         h = rng.integers(0, act.shape[0])
         i = rng.integers(2, n1 + 2)
         j = rng.integers(2, n2 + 2)
