@@ -97,6 +97,11 @@ _SIGNATURES = {
     "harm_fixup_utoprim": (ctypes.c_int, [ctypes.c_void_p, _DP]),
     "harm_utoprim_2d_batch": (ctypes.c_int, [_DP, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int),
                                              ctypes.c_long, ctypes.c_double]),
+    "harm_tracers_init": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GridSpec), ctypes.POINTER(ctypes.c_long)]),
+    "harm_tracers_put": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GridSpec), ctypes.POINTER(ctypes.c_int), _DP,
+                                        ctypes.c_long]),
+    "harm_tracers_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]),
+    "harm_tracers_get": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), _DP, _BP]),
     "harm_set_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "harm_get_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "harm_autotune_tile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
@@ -326,6 +331,32 @@ class Context:
 
     def sync(self):
         _check(self.lib.harm_sync(self.h))
+
+    # tracer particles (tracers.c)
+    def tracers_init(self):
+        """init_tracers(): a tracer at every zone centre with rho > RHOMIN; returns the count."""
+        n = ctypes.c_long()
+        _check(self.lib.harm_tracers_init(self.h, ctypes.byref(self.problem.grid), ctypes.byref(n)))
+        return n.value
+
+    def tracers_put(self, ids, X):
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        _check(self.lib.harm_tracers_put(self.h, ctypes.byref(self.problem.grid),
+                                         ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(X), len(ids)))
+
+    def tracers(self):
+        """(ids[n][3], X[n][3], status[n]) of every tracer, retired ones included."""
+        n = ctypes.c_long()
+        _check(self.lib.harm_tracers_count(self.h, ctypes.byref(n)))
+        n = n.value
+        ids = np.zeros((n, 3), dtype=np.int32)
+        X = np.zeros((n, 3))
+        st = np.zeros(n, dtype=np.int8)
+        if n:
+            _check(self.lib.harm_tracers_get(self.h, ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(X),
+                                             st.ctypes.data_as(_BP)))
+        return ids, X, st
 
     def set_tile(self, bx, by):
         """Threads per block of the face and zone kernels (bx theta x by r, 128 in all)."""

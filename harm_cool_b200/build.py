@@ -36,6 +36,7 @@ UNITS = {
     "harm_exact.cu": ["-fmad=false"],   # the FP64 step, bit-compatible with the reference
     "harm_mixed.cu": ["-fmad=true"],    # the mixed-precision step
     "harm_noalloc.cu": ["-fmad=false"],  # batch inversion on a fixed device buffer
+    "harm_tracers.cu": ["-fmad=false"],  # tracer particles
 }
 
 

@@ -581,11 +581,20 @@ int launch_fixup_utoprim(Ctx *x, double *P)
   return HARM_OK;
 }
 
-// diag_mass() and the next dt (step_ch.c:119-137)
+// diag_mass(), update_tracers() and the next dt (step_ch.c:119-137)
 void launch_mass(Ctx *x)
 {
   k_diag_mass<<<x->nparts, 256, 0, x->stream>>>(x->G, x->p, x->geo, x->partials, x->nparts, x->sc);
+  if (x->ntr) launch_tracers(x);
   k_finalize<<<1, 1024, 0, x->stream>>>(x->G, x->partials, x->nparts, x->sc);
+}
+
+void invalidate_graph(Ctx *x)
+{
+  if (x->graph_exec) {
+    cudaGraphExecDestroy(x->graph_exec);
+    x->graph_exec = nullptr;
+  }
 }
 
 int launch_step(Ctx *x) { return x->mode == HARM_MIXED ? mixed::launch_step(x) : exact::launch_step(x); }
@@ -623,9 +632,6 @@ namespace harm {
 int launch_step(Ctx *x);
 }
 
-struct harm_ctx {
-  Ctx x;
-};
 
 extern "C" const char *harm_last_error(void) { return g_err.c_str(); }
 
@@ -733,7 +739,7 @@ extern "C" void harm_destroy(harm_ctx *h)
   if (x->graph_exec) cudaGraphExecDestroy(x->graph_exec);
   void *ptrs[] = {x->p, x->ph, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm,
                   x->stage, x->stage_flag, x->fail_list, x->fix_buf, x->partials, x->sc,
-                  x->F1f, x->F2f, x->F3f, x->geo32, x->Ubuf};
+                  x->F1f, x->F2f, x->F3f, x->geo32, x->Ubuf, x->trX, x->trids, x->trst};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (x->pinned) cudaFreeHost(x->pinned);
@@ -1109,19 +1115,12 @@ extern "C" int harm_time_kernels(harm_ctx *h, int reps, double *ms)
 
 static bool tile_ok(int bx, int by) { return bx >= 8 && by >= 1 && bx * by == 128 && (bx & 7) == 0; }
 
-static void drop_graph(Ctx *x)
-{
-  if (x->graph_exec) {
-    cudaGraphExecDestroy(x->graph_exec);
-    x->graph_exec = nullptr;
-  }
-}
 
 extern "C" int harm_set_tile(harm_ctx *h, int bx, int by)
 {
   if (!h || !tile_ok(bx, by)) return fail_with(HARM_E_ARG, "tile must be bx x by = 128 threads, bx a multiple of 8");
   Ctx *x = &h->x;
-  if (x->tbx != bx || x->tby != by) drop_graph(x);
+  if (x->tbx != bx || x->tby != by) invalidate_graph(x);
   x->tbx = bx;
   x->tby = by;
   return HARM_OK;
@@ -1179,7 +1178,7 @@ extern "C" int harm_autotune_tile(harm_ctx *h, int steps, int *bx, int *by)
       return rc;
     }
   }
-  drop_graph(x);
+  invalidate_graph(x);
   x->tbx = cand[bi][0];
   x->tby = cand[bi][1];
   if (bx) *bx = x->tbx;
@@ -1193,6 +1192,7 @@ extern "C" int harm_autotune_tile(harm_ctx *h, int steps, int *bx, int *by)
 struct harm_ensemble {
   std::vector<Ctx *> members;
   std::vector<int> mode, tbx, tby;  // member settings the graph was captured with
+  std::vector<long> ntr;
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t fork = nullptr;
@@ -1224,6 +1224,7 @@ extern "C" int harm_ensemble_create(harm_ctx *const *members, int n, harm_ensemb
   e->mode.assign(n, -1);
   e->tbx.assign(n, 0);
   e->tby.assign(n, 0);
+  e->ntr.assign(n, -1);
   e->join.assign(n, nullptr);
   if (cudaSetDevice(e->device) != cudaSuccess || cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) {
@@ -1250,7 +1251,7 @@ static int ensemble_graph(harm_ensemble *e)
   bool same = e->exec != nullptr;
   for (size_t k = 0; k < e->members.size() && same; k++) {
     const Ctx *x = e->members[k];
-    same = x->mode == e->mode[k] && x->tbx == e->tbx[k] && x->tby == e->tby[k];
+    same = x->mode == e->mode[k] && x->tbx == e->tbx[k] && x->tby == e->tby[k] && x->ntr == e->ntr[k];
   }
   if (same) return HARM_OK;
   if (e->exec) {
@@ -1271,6 +1272,7 @@ static int ensemble_graph(harm_ensemble *e)
     e->mode[k] = x->mode;
     e->tbx[k] = x->tbx;
     e->tby[k] = x->tby;
+    e->ntr[k] = x->ntr;
   }
   cudaError_t ee = cudaStreamEndCapture(e->stream, &g);
   if (rc) return rc;

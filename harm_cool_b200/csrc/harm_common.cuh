@@ -37,6 +37,14 @@ struct Grid {
   double dx1, dx2, dx3;
 };
 
+// tracer particles (tracers.c): the grid as the reference's coord() and
+// bl_coord() see it, in the reference's own indices (h from 1 in 3D)
+struct TrParams {
+  double sx1, sx2, sx3, dx1, dx2, dx3;
+  double R0, hslope, Rin, Rout, thmin, thmax;
+  int n3, istart, istop, jstart, jstop, hstart, hstop;
+};
+
 constexpr int FAIL_CAP = 8192;     // failed zones listed by k_fu_flip
 constexpr int FIX_LIST_MAX = 512;  // up to this many, repaired through the sorted list
 constexpr int NTHR_FIX = 1024;
@@ -70,6 +78,11 @@ struct Ctx {
   float *geo32;                  // mixed mode: FP32 face geometry [3][GEO_N][ng]
   double *Ubuf;                  // conserved variables between the two update launches [8][nc]
   int tbx, tby;                  // tile of the zone and face kernels: theta x r threads, 128 in all
+  long ntr;                      // tracer particles
+  double *trX;                   // [3][ntr] code coordinates X1, X2, X3
+  int *trids;                    // [ntr][3] labels (i, j, h)
+  signed char *trst;             // [ntr] 0 active, 1 in, 2 out, 3 jet, -1 dropped
+  TrParams trp;
 };
 
 __device__ __forceinline__ void record_fail(DevScalars *sc, int code, int h, int i, int j)
@@ -142,6 +155,9 @@ int launch_fixup_utoprim(Ctx *x, double *P);
 void launch_mass(Ctx *x);
 int sync_status(Ctx *x);
 
+void launch_tracers(Ctx *x);     // update_tracers() (harm_tracers.cu)
+void invalidate_graph(Ctx *x);   // a captured step no longer matches the context
+
 // one step and the per-kernel timing of each precision variant
 namespace exact {
 int launch_step(Ctx *x);
@@ -153,3 +169,7 @@ int time_kernels(Ctx *x, int reps, double *ms);
 }
 
 }  // namespace harm
+
+struct harm_ctx {
+  harm::Ctx x;
+};

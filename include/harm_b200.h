@@ -164,6 +164,26 @@ int harm_time_kernels(harm_ctx *ctx, int reps, double *ms);
 /* Block until the context's stream is idle; returns any pending device error. */
 int harm_sync(harm_ctx *ctx);
 
+/* ---- tracer particles (tracers.c) ----
+   Tracers live on the device with the state.  Once a context has tracers,
+   every step moves them after the mass diagnostics, as step_ch() calls
+   update_tracers(dt) (step_ch.c:121-123).  ids[n][3] are labels (the zone i, j, h
+   a tracer started in, as tracers.c names its files); X[n][3] are code
+   coordinates X1, X2, X3; status[n] is 0 while active, 1 after falling in
+   (r < inner tracer radius or theta outside [0, pi]), 2 after leaving through the
+   outer tracer radius inside the theta window [0.02 pi, 0.98 pi], 3 after leaving
+   in the jet, -1 when the zone search failed -- where the reference erases the
+   tracer and moves its file to tracers/in, out or jet.  g gives R0 and hslope. */
+
+/* init_tracers() (tracers.c:109-188): one tracer at the centre of every active zone
+   whose zone holds rho > RHOMIN, in the reference's loop order; *count tracers. */
+int harm_tracers_init(harm_ctx *ctx, const harm_grid_spec *g, long *count);
+/* Replace the tracers with n given ones, all active. */
+int harm_tracers_put(harm_ctx *ctx, const harm_grid_spec *g, const int *ids, const double *X, long n);
+int harm_tracers_count(harm_ctx *ctx, long *n);
+/* Read back all tracers, retired ones included (any pointer may be NULL). */
+int harm_tracers_get(harm_ctx *ctx, int *ids, double *X, signed char *status);
+
 /* ---- tile shapes (no reference counterpart: the reference runs on CPUs) ---- */
 
 /* Threads per block of the face and zone kernels: bx along theta by by along r,

@@ -43,7 +43,11 @@ CONFIGS = {
     "m3d": (32, 32, 8, 0.9375, 6.0, 12.0, 100.0),
     # bounded CPU sample of the 288x256x256 workload: same r-theta grid, 4 phi planes
     "c2s": (288, 256, 4, 0.9375, 6.0, 12.0, 100.0),
+    # with the reference's tracer particles (TRACERSDUMP on, tracers.c)
+    "r2d": (32, 32, 1, 0.9375, 6.0, 12.0, 100.0),
+    "r3d": (16, 16, 4, 0.9375, 6.0, 12.0, 100.0),
 }
+TRACER_CONFIGS = ("r2d", "r3d")
 
 SOURCES = ["bounds", "coord", "diag", "dump", "fixup", "image", "interp", "main",
            "metric", "lu", "phys", "ranc", "restart", "step_ch", "u2p_util",
@@ -58,12 +62,13 @@ def _sub1(pattern, repl, text, what):
     return new
 
 
-def patch_decs(text, n1, n2, n3):
+def patch_decs(text, n1, n2, n3, tracers=False):
     text = _sub1(r"^#define N1\s+\(\d+\)", "#define N1       (%d)" % n1, text, "N1")
     text = _sub1(r"^#define N2\s+\(\d+\)", "#define N2       (%d)" % n2, text, "N2")
     text = _sub1(r"^#define N3\s+\(\d+\)", "#define N3       (%d)" % n3, text, "N3")
     text = _sub1(r"^#define COOL_EOS\s+\(1\)", "#define COOL_EOS  (0)", text, "COOL_EOS")
-    text = _sub1(r"^#define TRACERSDUMP \(1\)", "#define TRACERSDUMP (0)", text, "TRACERSDUMP")
+    if not tracers:
+        text = _sub1(r"^#define TRACERSDUMP \(1\)", "#define TRACERSDUMP (0)", text, "TRACERSDUMP")
     text = _sub1(r"^#define HDFDUMP \(1\)", "#define HDFDUMP (0)", text, "HDFDUMP")
     # the opposite-phi slice tables are indexed by h in [1, N3] (mpi.c:337-422)
     # but declared with N3 entries: size them N3+2 so no neighbour is clobbered
@@ -108,8 +113,9 @@ def build_config(name, force=False):
         return lib
     os.makedirs(gen, exist_ok=True)
     os.makedirs(obj, exist_ok=True)
+    tracers = name in TRACER_CONFIGS
     with open(os.path.join(REF_SRC, "decs.h")) as f:
-        decs = patch_decs(f.read(), n1, n2, n3)
+        decs = patch_decs(f.read(), n1, n2, n3, tracers)
     with open(os.path.join(gen, "decs.h"), "w") as f:
         f.write(decs)
     with open(os.path.join(REF_SRC, "defs.h")) as f:
@@ -124,7 +130,7 @@ def build_config(name, force=False):
              "-Dmain=harm_reference_main", "-I" + gen, "-I-",
              "-I" + os.path.join(HERE, "fakempi"), "-I" + REF_SRC]
     objs = []
-    for s in SOURCES:
+    for s in SOURCES + (["tracers"] if tracers else []):
         o = os.path.join(obj, s + ".o")
         run(flags + ["-x", "c++", "-c", os.path.join(REF_SRC, s + ".c"), "-o", o])
         objs.append(o)
@@ -134,6 +140,12 @@ def build_config(name, force=False):
     o = os.path.join(obj, "refdrv.o")
     run(flags + ["-c", os.path.join(HERE, "refdrv.cpp"), "-o", o])
     objs.append(o)
+    if tracers:
+        # tracers.c scales its dump files by RHO_UNIT and T_UNIT, defined in cooleos.c,
+        # which needs the Fortran EOS; the checker reads no dump file
+        o = os.path.join(obj, "tracer_units.o")
+        run(flags + ["-c", os.path.join(HERE, "tracer_units.cpp"), "-o", o])
+        objs.append(o)
     o = os.path.join(obj, "fakempi.o")
     run(["gcc", "-O2", "-fPIC", "-c", os.path.join(HERE, "fakempi", "fakempi.c"), "-o", o])
     objs.append(o)

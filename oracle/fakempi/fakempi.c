@@ -9,7 +9,8 @@
  *    array of a basic type; Sendrecv to/from this rank packs the send box and
  *    unpacks it into the receive box (through a bounce buffer, because the
  *    reference sends and receives on the same array);
- *  - Isend/Irecv to this rank are matched by tag at MPI_Waitall.
+ *  - Isend/Irecv to this rank are matched by tag at MPI_Waitall;
+ *  - a blocking Send to this rank is buffered until the Recv with its tag.
  */
 #include "mpi.h"
 #include <stdio.h>
@@ -188,18 +189,44 @@ int MPI_Allreduce(const void *sbuf, void *rbuf, int count, MPI_Datatype t, MPI_O
   return 0;
 }
 
-/* point-to-point between distinct ranks cannot happen in a one-rank world */
+/* blocking self messages of basic types (the tracer hand-over,
+   tracers.c:266-289): a send to this rank is buffered, as an eager MPI
+   implementation would, and the receive with the same tag takes it */
+#define MAXMSG 1024
+typedef struct { int tag; size_t bytes; void *data; } msg_t;
+static msg_t g_msg[MAXMSG];
+static int g_nmsg = 0;
+
 int MPI_Send(const void *buf, int count, MPI_Datatype t, int dest, int tag, MPI_Comm c)
 {
-  (void)buf; (void)count; (void)t; (void)tag; (void)c;
+  (void)c;
   if (dest == MPI_PROC_NULL) return 0;
-  fprintf(stderr, "fakempi: MPI_Send in a one-rank world\n"); abort();
+  if (dest != 0 || !is_basic(t) || g_nmsg >= MAXMSG) { fprintf(stderr, "fakempi: unsupported MPI_Send\n"); abort(); }
+  size_t b = payload_bytes(t, count);
+  void *d = malloc(b ? b : 1);
+  if (!d) abort();
+  memcpy(d, buf, b);
+  g_msg[g_nmsg].tag = tag;
+  g_msg[g_nmsg].bytes = b;
+  g_msg[g_nmsg].data = d;
+  g_nmsg++;
+  return 0;
 }
 int MPI_Recv(void *buf, int count, MPI_Datatype t, int source, int tag, MPI_Comm c, MPI_Status *st)
 {
-  (void)buf; (void)count; (void)t; (void)tag; (void)c; (void)st;
+  (void)c; (void)st;
   if (source == MPI_PROC_NULL) return 0;
-  fprintf(stderr, "fakempi: MPI_Recv in a one-rank world\n"); abort();
+  if (source != 0 || !is_basic(t)) { fprintf(stderr, "fakempi: unsupported MPI_Recv\n"); abort(); }
+  for (int k = 0; k < g_nmsg; k++)
+    if (g_msg[k].tag == tag) {
+      size_t b = payload_bytes(t, count);
+      if (b != g_msg[k].bytes) { fprintf(stderr, "fakempi: MPI_Recv size mismatch\n"); abort(); }
+      memcpy(buf, g_msg[k].data, b);
+      free(g_msg[k].data);
+      g_msg[k] = g_msg[--g_nmsg];
+      return 0;
+    }
+  fprintf(stderr, "fakempi: MPI_Recv with no matching send (tag %d)\n", tag); abort();
 }
 
 /* nonblocking self messages: queue them and match sends to receives by tag */

@@ -22,6 +22,14 @@ enum { RHO, UU, U1, U2, U3, B1, B2, B3 };
 enum { FACE1, FACE2, CORN, CENT, FACE3 };
 enum { MC, VANL, MINM };
 
+/* the <math.h> values the reference uses (not declared under -std=c99) */
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+#ifndef M_PI_2
+#define M_PI_2 1.57079632679489661923
+#endif
+
 /* decs.h:127-158 */
 #define RHOMIN (1.e-6)
 #define UUMIN (1.e-8)
@@ -73,6 +81,14 @@ struct ora_state {
   ora_diag d;
   /* current zone, for the failure record (metric.c:269-272) */
   int ch, ci, cj;
+  /* tracer particles (tracers.c:19-35): labels, code coordinates X1..X3,
+     status (0 active, 1 fell in, 2 left inside the theta window, 3 left in
+     the jet, -1 dropped by the search); R0 and hslope for bl_coord() */
+  long ntr;
+  int *tr_ids;
+  double *tr_X;
+  signed char *tr_st;
+  double R0, hslope;
 };
 
 /* ------------------------------------------------------------------ */
@@ -1343,6 +1359,208 @@ double ora_advance(ora_state *s, double *pi, double *pb, double Dt, double *pf, 
 }
 
 /* step_ch.c:90-140 */
+/* ------------------------------------------------------------------ */
+/* tracer particles (tracers.c)                                         */
+
+/* coord() (metric.c:62-115) for the CENT and FACE3 locations, single rank */
+static void coord_x(const ora_state *s, int h, int i, int j, int loc, double *X)
+{
+  i -= 2;
+  j -= 2;
+  h -= s->prm.n3 > 1 ? 1 : 0;
+  X[0] = 1.;
+  X[1] = s->prm.startx[1] + (i + 0.5) * s->prm.dx[1];
+  X[2] = s->prm.startx[2] + (j + 0.5) * s->prm.dx[2];
+  if (loc == FACE3 || s->prm.n3 <= 2) X[3] = s->prm.startx[3] + h * s->prm.dx[3];
+  else X[3] = s->prm.startx[3] + (h + 0.5) * s->prm.dx[3];
+}
+
+/* search_tracer() (tracers.c:39-98): the zone below the tracer along each axis */
+static int search_tracer(const ora_state *s, const double *XX, int *hh, int *ii, int *jj)
+{
+  double Xl[4], Xr[4];
+  int ok;
+  coord_x(s, s->hstart, s->istart - 1, s->jstart - 1, CENT, Xl);
+  if (XX[1] < Xl[1] || XX[2] < Xl[2]) return 0;
+  *hh = 0;
+  ok = 0;
+  for (int i = s->istart - 1; i <= s->istop; i++) {
+    coord_x(s, s->hstart, i, s->jstart, CENT, Xl);
+    coord_x(s, s->hstart, i + 1, s->jstart, CENT, Xr);
+    if (XX[1] >= Xl[1] && XX[1] < Xr[1]) { *ii = i; ok = 1; break; }
+  }
+  if (!ok) return 0;
+  ok = 0;
+  for (int j = s->jstart - 1; j <= s->jstop; j++) {
+    coord_x(s, s->hstart, s->istart, j, CENT, Xl);
+    coord_x(s, s->hstart, s->istart, j + 1, CENT, Xr);
+    if (XX[2] >= Xl[2] && XX[2] < Xr[2]) { *jj = j; ok = 1; break; }
+  }
+  if (!ok) return 0;
+  if (s->prm.n3 > 2) {
+    ok = 0;
+    for (int h = s->hstart; h <= s->hstop; h++) {
+      coord_x(s, h, s->istart, s->jstart, FACE3, Xl);
+      coord_x(s, h + 1, s->istart, s->jstart, FACE3, Xr);
+      if (XX[3] >= Xl[3] && XX[3] < Xr[3]) { *hh = h; ok = 1; break; }
+    }
+    if (!ok) return 0;
+  }
+  return 1;
+}
+
+/* ucon_fun() (tracers.c:257-269): u^mu with the spatial parts divided by u^t */
+static void ucon_fun(ora_state *s, int h, int i, int j, double *ucon)
+{
+  geom_t g;
+  get_geometry(s, h, i, j, CENT, &g);
+  ucon_calc(s, PV(s, s->p, h, i, j), &g, ucon);
+  ucon[1] /= ucon[0];
+  ucon[2] /= ucon[0];
+  ucon[3] /= ucon[0];
+}
+
+/* linear_interpolation() (tracers.c:193-254) of ucon_fun, VALDIM = 4 */
+static void interp_ucon(ora_state *s, const double *tX, int hh, int ii, int jj, double *val)
+{
+  const int WPH = s->prm.n3 > 2 ? 2 : 1;
+  double XX[2][2][2][4], valt[2][2][2][4], tmp1[2][2][4], tmp2[2][4];
+  for (int l3 = 0; l3 < WPH; l3++)
+    for (int l1 = 0; l1 < 2; l1++)
+      for (int l2 = 0; l2 < 2; l2++) {
+        coord_x(s, hh + l3, ii + l1, jj + l2, CENT, XX[l3][l1][l2]);
+        ucon_fun(s, hh + l3, ii + l1, jj + l2, valt[l3][l1][l2]);
+      }
+  for (int l3 = 0; l3 < WPH; l3++)
+    for (int l1 = 0; l1 < 2; l1++) {
+      double T1 = 1.0 / (XX[l3][l1][1][2] - XX[l3][l1][0][2]);
+      double T2 = tX[2] - XX[l3][l1][0][2];
+      for (int k = 0; k < 4; k++) {
+        double ypval = (valt[l3][l1][1][k] - valt[l3][l1][0][k]) * T1;
+        tmp1[l3][l1][k] = valt[l3][l1][0][k] + T2 * ypval;
+      }
+    }
+  for (int l3 = 0; l3 < WPH; l3++) {
+    double T1 = 1.0 / (XX[l3][1][1][1] - XX[l3][0][0][1]);
+    double T2 = tX[1] - XX[l3][0][0][1];
+    for (int k = 0; k < 4; k++) {
+      double ypval = (tmp1[l3][1][k] - tmp1[l3][0][k]) * T1;
+      tmp2[l3][k] = tmp1[l3][0][k] + T2 * ypval;
+    }
+  }
+  if (WPH == 1) {
+    for (int k = 0; k < 4; k++) val[k] = tmp2[0][k];
+  } else {
+    double T1 = 1.0 / (XX[1][1][1][3] - XX[0][0][0][3]);
+    double T2 = tX[3] - XX[0][0][0][3];
+    for (int k = 0; k < 4; k++) {
+      double ypval = (tmp2[1][k] - tmp2[0][k]) * T1;
+      val[k] = tmp2[0][k] + T2 * ypval;
+    }
+  }
+}
+
+/* bl_coord() (coord.c:61-124) with gammie_coords, Rbr < 0, COORDSINGFIX */
+static void bl_coord_rth(const ora_state *s, const double *X, double *r, double *th)
+{
+  *r = exp(X[1]) + s->R0;
+  double t = M_PI_2 * (1. + X[2]) + ((1. - s->hslope) / 2.) * sin(M_PI * (1. + X[2]));
+  if (fabs(t) < 1.E-20) t = t >= 0 ? 1.E-20 : -1.E-20;
+  if (fabs(M_PI - t) < 1.E-20) t = t >= M_PI ? M_PI + 1.E-20 : M_PI - 1.E-20;
+  *th = t;
+}
+
+/* update_tracers() (tracers.c:298-429), one rank: move each active tracer by
+   the interpolated u^i/u^t over Dt, then retire those that fell in or left */
+static void update_tracers(ora_state *s, double Dt)
+{
+  const double Rin = exp(s->prm.startx[1] - 0.5 * s->prm.dx[1]) + s->R0;           /* :121 */
+  const double Rout = 0.8 * (exp(s->prm.startx[1] + s->prm.n1 * s->prm.dx[1]) + s->R0);
+  const double thmin = 0.02 * M_PI, thmax = 0.98 * M_PI;
+  /* the phi-periodic ghost plane the interpolation reads (tracers.c:313-318) */
+  if (s->prm.n3 > 2)
+    memcpy(PV(s, s->p, s->hstop + 1, 0, 0), PV(s, s->p, s->hstart, 0, 0),
+           (size_t)s->sn1 * s->sn2 * NPR * sizeof(double));
+  for (long k = 0; k < s->ntr; k++) {
+    if (s->tr_st[k]) continue;
+    double X[4] = {0., s->tr_X[3 * k], s->tr_X[3 * k + 1], s->tr_X[3 * k + 2]};
+    int hh, ii, jj;
+    if (!search_tracer(s, X, &hh, &ii, &jj)) { s->tr_st[k] = -1; continue; }
+    double ucon[4];
+    interp_ucon(s, X, hh, ii, jj, ucon);
+    for (int m = 1; m < 4; m++) X[m] += ucon[m] * Dt;
+    double r, th;
+    bl_coord_rth(s, X, &r, &th);
+    for (int m = 1; m < 4; m++) s->tr_X[3 * k + m - 1] = X[m];
+    if (r < Rin || th < 0 || th > M_PI) s->tr_st[k] = 1;
+    else if (r >= Rout) s->tr_st[k] = (th >= thmin && th <= thmax) ? 2 : 3;
+  }
+  if (s->prm.n3 > 2)  /* tracers.c:385-408: back into [0, 2 pi] */
+    for (long k = 0; k < s->ntr; k++) {
+      if (s->tr_st[k]) continue;
+      double *x3 = &s->tr_X[3 * k + 2];
+      if (*x3 < 0.) *x3 += 2. * M_PI;
+      else if (*x3 > 2. * M_PI) *x3 -= 2. * M_PI;
+    }
+}
+
+static void tracers_alloc(ora_state *s, long n)
+{
+  free(s->tr_ids); free(s->tr_X); free(s->tr_st);
+  s->ntr = n;
+  s->tr_ids = (int *)calloc(3 * (size_t)(n ? n : 1), sizeof(int));
+  s->tr_X = (double *)calloc(3 * (size_t)(n ? n : 1), sizeof(double));
+  s->tr_st = (signed char *)calloc((size_t)(n ? n : 1), 1);
+}
+
+void ora_tracers_geometry(ora_state *s, double R0, double hslope)
+{
+  s->R0 = R0;
+  s->hslope = hslope;
+}
+
+/* init_tracers() (tracers.c:109-188): one tracer per zone centre whose zone
+   (found by the search) has rho > RHOMIN, in h, i, j loop order */
+long ora_tracers_init(ora_state *s)
+{
+  const int n1 = s->prm.n1, n2 = s->prm.n2, n3 = s->prm.n3;
+  long cnt = 0;
+  int *ids = (int *)malloc(3 * sizeof(int) * (size_t)n1 * n2 * n3);
+  double *X = (double *)malloc(3 * sizeof(double) * (size_t)n1 * n2 * n3);
+  for (int h = 0; h < n3; h++)
+    for (int i = 0; i < n1; i++)
+      for (int j = 0; j < n2; j++) {
+        double tX[4] = {0., s->prm.startx[1] + (i + 0.5) * s->prm.dx[1],
+                        s->prm.startx[2] + (j + 0.5) * s->prm.dx[2], s->prm.startx[3] + h * s->prm.dx[3]};
+        int hh, ii, jj;
+        if (search_tracer(s, tX, &hh, &ii, &jj) && PV(s, s->p, hh, ii, jj)[RHO] > RHOMIN) {
+          ids[3 * cnt] = i; ids[3 * cnt + 1] = j; ids[3 * cnt + 2] = h;
+          X[3 * cnt] = tX[1]; X[3 * cnt + 1] = tX[2]; X[3 * cnt + 2] = tX[3];
+          cnt++;
+        }
+      }
+  ora_tracers_put(s, ids, X, cnt);
+  free(ids);
+  free(X);
+  return cnt;
+}
+
+void ora_tracers_put(ora_state *s, const int *ids, const double *X, long n)
+{
+  tracers_alloc(s, n);
+  memcpy(s->tr_ids, ids, 3 * sizeof(int) * (size_t)n);
+  memcpy(s->tr_X, X, 3 * sizeof(double) * (size_t)n);
+}
+
+long ora_tracers_count(const ora_state *s) { return s->ntr; }
+
+void ora_tracers_get(const ora_state *s, int *ids, double *X, signed char *status)
+{
+  memcpy(ids, s->tr_ids, 3 * sizeof(int) * (size_t)s->ntr);
+  memcpy(X, s->tr_X, 3 * sizeof(double) * (size_t)s->ntr);
+  memcpy(status, s->tr_st, (size_t)s->ntr);
+}
+
 int ora_step_ch(ora_state *s)
 {
   double ndt;
@@ -1357,6 +1575,7 @@ int ora_step_ch(ora_state *s)
   ora_fixup_utoprim(s, s->p);
   ora_bound_prim(s, s->p);
   diag_mass(s, s->dt);
+  if (s->ntr) update_tracers(s, s->dt);  /* step_ch.c:121-123 */
   s->d.ndt = ndt;
   if (s->dt < 1.e-9) return 11;
   s->t += s->dt;
@@ -1415,6 +1634,7 @@ void ora_destroy(ora_state *s)
   free(s->p); free(s->ph); free(s->dq); free(s->F1); free(s->F2); free(s->F3);
   free(s->e1); free(s->e2); free(s->e3); free(s->pflag);
   free(s->gcov); free(s->gcon); free(s->gdet); free(s->conn); free(s->coords); free(s->katm);
+  free(s->tr_ids); free(s->tr_X); free(s->tr_st);
   free(s);
 }
 

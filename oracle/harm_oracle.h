@@ -86,6 +86,16 @@ void ora_face_flux(double gam, int dir, const double pl[8], const double pr[8],
                    const double *gcov, const double *gcon, double gdet,
                    double F[8], double *ctop);
 
+/* tracer particles (tracers.c): ids[n][3] labels (i, j, h), X[n][3] code
+   coordinates X1..X3, status[n] 0 active, 1 fell in, 2 left inside the theta
+   window, 3 left in the jet, -1 dropped by the search.  Once tracers exist,
+   ora_step_ch() moves them after diag_mass (step_ch.c:121-123).  bl_coord()
+   needs the grid's R0 and hslope. */
+void ora_tracers_geometry(ora_state *s, double R0, double hslope);
+long ora_tracers_init(ora_state *s);
+void ora_tracers_put(ora_state *s, const int *ids, const double *X, long n);
+long ora_tracers_count(const ora_state *s);
+void ora_tracers_get(const ora_state *s, int *ids, double *X, signed char *status);
 #ifdef __cplusplus
 }
 #endif

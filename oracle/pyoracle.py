@@ -68,6 +68,14 @@ def oracle_lib():
                                            ctypes.c_double]
         lib.ora_face_flux.argtypes = [ctypes.c_double, ctypes.c_int, dp, dp, dp, dp,
                                       ctypes.c_double, dp, dp]
+        ip = ctypes.POINTER(ctypes.c_int)
+        lib.ora_tracers_geometry.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        lib.ora_tracers_init.restype = ctypes.c_long
+        lib.ora_tracers_init.argtypes = [ctypes.c_void_p]
+        lib.ora_tracers_put.argtypes = [ctypes.c_void_p, ip, dp, ctypes.c_long]
+        lib.ora_tracers_count.restype = ctypes.c_long
+        lib.ora_tracers_count.argtypes = [ctypes.c_void_p]
+        lib.ora_tracers_get.argtypes = [ctypes.c_void_p, ip, dp, ctypes.POINTER(ctypes.c_byte)]
         _oracle_lib = lib
     return _oracle_lib
 
@@ -129,6 +137,27 @@ class Oracle:
     def step(self):
         return self.lib.ora_step_ch(self.h)
 
+    # tracer particles (tracers.c)
+    def tracers_init(self, R0, hslope):
+        self.lib.ora_tracers_geometry(self.h, R0, hslope)
+        return self.lib.ora_tracers_init(self.h)
+
+    def tracers_put(self, ids, X, R0, hslope):
+        self.lib.ora_tracers_geometry(self.h, R0, hslope)
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        self.lib.ora_tracers_put(self.h, ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(X), len(ids))
+
+    def tracers(self):
+        """(ids[n][3], X[n][3], status[n]) for every tracer, retired ones included."""
+        n = self.lib.ora_tracers_count(self.h)
+        ids = np.zeros((n, 3), dtype=np.int32)
+        X = np.zeros((n, 3))
+        st = np.zeros(n, dtype=np.int8)
+        self.lib.ora_tracers_get(self.h, ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(X),
+                                 st.ctypes.data_as(ctypes.POINTER(ctypes.c_byte)))
+        return ids, X, st
+
     def __del__(self):
         try:
             if getattr(self, "h", None):
@@ -153,6 +182,8 @@ class Reference:
         lib.ref_utoprim_2d.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_double)]
         lib.ref_time_steps.restype = ctypes.c_double
+        if hasattr(lib, "ref_tracers_count"):
+            lib.ref_tracers_count.restype = ctypes.c_long
         lib.ref_init()
         d = (ctypes.c_int * 16)()
         lib.ref_dims(d)
@@ -169,6 +200,21 @@ class Reference:
 
     def get(self, name):
         return self.lib.ref_get(name.encode())
+
+    def tracers(self):
+        """The reference's tracer list (tracers.c:24): ids[n][3] = (i, j, h), X[n][3]."""
+        n = self.lib.ref_tracers_count()
+        ids = np.zeros((n, 3), dtype=np.int32)
+        X = np.zeros((n, 3))
+        self.lib.ref_tracers_get(ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                 X.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return ids, X
+
+    def set_tracers(self, ids, X):
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        self.lib.ref_tracers_set(ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                 X.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.c_long(len(ids)))
 
     def set(self, name, value):
         return self.lib.ref_set(name.encode(), float(value))

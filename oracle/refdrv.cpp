@@ -14,6 +14,7 @@
  * sources, with decs.h resolved to a per-configuration patched copy.
  */
 #include "decs.h"
+#include <vector>
 #include <string.h>
 #include <time.h>
 #include <unistd.h>
@@ -24,6 +25,9 @@ void set_MPI(int argc, char *argv[]);
 #endif
 double advance(double *_pi, double *_pb, double Dt, double *_pf, int fullstep);
 double fluxcalc(double *_pr, double *_F, const int dir, const int fullstep);
+#if TRACERSDUMP
+void init_tracers(void);
+#endif
 
 static int g_stdout_saved = -1;
 
@@ -64,6 +68,9 @@ int ref_init(void)
     ZLOOP { mass_start += p[h][i][j][RHO] * gdet[i][j][CENT] * dx[RR] * dx[TH] * dx[PH]; }
   }
   diag_mass(0.);
+#if TRACERSDUMP
+  init_tracers();  /* main.c:184-186 */
+#endif
   defcon = 1.;
   quiet(0);
   return 0;
@@ -193,4 +200,35 @@ double ref_time_steps(int warm, int steps)
   return (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
 }
 
+#if TRACERSDUMP
+} /* extern "C" */
+/* the tracer list of tracers.c (tracers.c:19-24) */
+struct of_tracer {
+  int h, i, j;
+  double X[NDIM];
+};
+extern std::vector<of_tracer> vtr;
+extern "C" {
+long ref_tracers_count(void) { return (long)vtr.size(); }
+/* ids[n][3] = (i, j, h) of the zone each tracer started in, X[n][3] = X1, X2, X3 */
+void ref_tracers_get(int *ids, double *X)
+{
+  for (size_t k = 0; k < vtr.size(); k++) {
+    ids[3 * k] = vtr[k].i; ids[3 * k + 1] = vtr[k].j; ids[3 * k + 2] = vtr[k].h;
+    X[3 * k] = vtr[k].X[1]; X[3 * k + 1] = vtr[k].X[2]; X[3 * k + 2] = vtr[k].X[3];
+  }
+}
+/* replace the tracer list: ids[n][3] = (i, j, h) labels, X[n][3] = X1, X2, X3 */
+void ref_tracers_set(const int *ids, const double *X, long n)
+{
+  vtr.clear();
+  for (long k = 0; k < n; k++) {
+    of_tracer t;
+    t.i = ids[3 * k]; t.j = ids[3 * k + 1]; t.h = ids[3 * k + 2];
+    t.X[0] = 0.;
+    t.X[1] = X[3 * k]; t.X[2] = X[3 * k + 1]; t.X[3] = X[3 * k + 2];
+    vtr.push_back(t);
+  }
+}
+#endif
 } /* extern "C" */

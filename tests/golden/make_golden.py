@@ -8,6 +8,9 @@ files).  Fixtures hold only generated numbers:
                 calls of step_ch(), with t, dt and the diagnostics.
   kat_u2p.npz   Utoprim_2d / Utoprim_1dvsq2fix1 / Utoprim_1dfix1 inputs and
                 outputs on perturbed zones of the 2D torus.
+  tracers_<config>.npz  the reference's tracer particles (tracers.c) after
+                init_tracers() and after steps, and a seeded custom tracer
+                list carried through 25 more steps.
 Each configuration runs in its own process: the reference keeps its state in
 globals.
 """
@@ -53,6 +56,76 @@ def one_config(cfg):
         out["t%d" % n] = np.array([ref.get("t"), ref.get("dt")])
         out["diag%d" % n] = np.array([ref.get(s) for s in SCALARS])
     np.savez_compressed(os.path.join(HERE, cfg + ".npz"), **out)
+
+
+def custom_tracers(ref, rng, n=240):
+    """A seeded tracer set over the whole grid, with tracers close to the inner
+    radius (they fall in), beyond the outer tracer radius inside and outside the
+    theta window (they leave as out and jet), and a few outside the grid (the
+    search fails and they are dropped)."""
+    import math
+    sx = [0., ref.get("startx1"), ref.get("startx2"), ref.get("startx3")]
+    dx = [0., ref.get("dx1"), ref.get("dx2"), ref.get("dx3")]
+    n1, n2, n3 = ref.n1, ref.n2, ref.n3
+    R0, hslope = ref.get("R0"), ref.get("hslope")
+    x1lo, x1hi = sx[1] - 0.5 * dx[1], sx[1] + (n1 + 0.5) * dx[1]
+    x2lo, x2hi = sx[2] - 0.5 * dx[2], sx[2] + (n2 + 0.5) * dx[2]
+    x3hi = sx[3] + n3 * dx[3]
+    rout_t = 0.8 * (math.exp(sx[1] + n1 * dx[1]) + R0)
+    X = []
+    for k in range(n):
+        kind = k % 6
+        x2 = rng.uniform(x2lo, x2hi)
+        x3 = rng.uniform(sx[3], x3hi) if n3 > 1 else 0.
+        if kind == 0:     # near the inner tracer radius
+            x1 = sx[1] - 0.5 * dx[1] + rng.uniform(1e-6, 2e-2)
+        elif kind == 1:   # beyond the outer tracer radius
+            x1 = math.log(rout_t - R0) + rng.uniform(1e-6, 0.5 * dx[1])
+        elif kind == 2:   # outside the grid (dropped by the search)
+            x1 = x1lo - rng.uniform(0.1, 1.) * dx[1] if rng.random() < 0.5 else x1hi + rng.uniform(1., 2.) * dx[1]
+        else:
+            x1 = rng.uniform(sx[1], sx[1] + n1 * dx[1])
+        X.append((x1, x2, x3))
+    ids = np.array([(1000 + k, 0, 0) for k in range(n)], dtype=np.int32)
+    return ids, np.array(X)
+
+
+def tracer_config(cfg):
+    """The reference's tracers (tracers.c, TRACERSDUMP on): init_tracers() after
+    init, the list after 1, 2 and 5 steps, then a custom seeded list set after
+    step 5 and read back after steps 6, 10 and 30."""
+    sys.path.insert(0, ROOT)
+    from oracle.pyoracle import Reference
+    ref = Reference(cfg)
+    hs = slice(1, ref.n3 + 1) if ref.n3 > 1 else slice(0, 1)
+    out = {"n": np.array([ref.n1, ref.n2, ref.n3])}
+    for name in ("a", "gam", "cour", "defcon", "tf", "Rin", "Rout", "hslope", "R0",
+                 "dx1", "dx2", "dx3", "startx1", "startx2", "startx3"):
+        out["par_" + name] = np.array(ref.get(name))
+    out["p0"] = ref.p[hs].copy()
+    out["pflag0"] = ref.pflag[hs].copy()
+    out["t0"] = np.array([ref.get("t"), ref.get("dt")])
+    out["tr_ids0"], out["tr_X0"] = ref.tracers()
+    done = 0
+    for nstep in (1, 2, 5, 6, 10, 30):
+        while done < nstep:
+            ref.step()
+            done += 1
+            if done == 5:
+                out["p5"] = ref.p[hs].copy()
+                out["pflag5"] = ref.pflag[hs].copy()
+                out["t5"] = np.array([ref.get("t"), ref.get("dt")])
+                out["mass5"] = np.array([ref.get("mass_in"), ref.get("mass_out")])
+                out["tr_ids5"], out["tr_X5"] = ref.tracers()
+                ids, X = custom_tracers(ref, np.random.default_rng(7 + ref.n3))
+                out["cu_ids"], out["cu_X"] = ids, X
+                ref.set_tracers(ids, X)
+        if nstep < 5:
+            out["tr_ids%d" % nstep], out["tr_X%d" % nstep] = ref.tracers()
+        elif nstep > 5:
+            out["cu_ids%d" % nstep], out["cu_X%d" % nstep] = ref.tracers()
+            out["p%d" % nstep] = ref.p[hs].copy()
+    np.savez_compressed(os.path.join(HERE, "tracers_" + cfg + ".npz"), **out)
 
 
 def kat_u2p():
@@ -110,14 +183,16 @@ if __name__ == "__main__":
     if len(sys.argv) > 1:
         if sys.argv[1] == "kat":
             kat_u2p()
+        elif sys.argv[1].startswith("tracers_"):
+            tracer_config(sys.argv[1][len("tracers_"):])
         else:
             one_config(sys.argv[1])
         sys.exit(0)
     sys.path.insert(0, ROOT)
     from oracle import build_ref
-    for cfg in ("t2d", "t3d"):
+    for cfg in ("t2d", "t3d", "r2d", "r3d"):
         build_ref.build_config(cfg, force=True)
-    for arg in ("t2d", "t3d", "kat"):
+    for arg in ("t2d", "t3d", "kat", "tracers_r2d", "tracers_r3d"):
         subprocess.run([sys.executable, os.path.abspath(__file__), arg], check=True,
                        stderr=subprocess.DEVNULL)
     for f in sorted(os.listdir(HERE)):
