@@ -51,6 +51,12 @@ class TorusSpec(ctypes.Structure):
                 ("beta", ctypes.c_double)]
 
 
+class Integrals(ctypes.Structure):
+    """harm_integrals: diag()'s sums and the largest div B (diag.c:113-230)."""
+    _fields_ = [("mass", ctypes.c_double), ("ang_mom", ctypes.c_double), ("energy", ctypes.c_double),
+                ("divbmax", ctypes.c_double), ("imax", ctypes.c_int * 3)]
+
+
 class Diag(ctypes.Structure):
     """harm_diag: per-step diagnostics (diag.c:437-580) and the first failure."""
     _fields_ = [("mdot", ctypes.c_double), ("edot", ctypes.c_double), ("ldot", ctypes.c_double),
@@ -97,6 +103,7 @@ _SIGNATURES = {
     "harm_fixup_utoprim": (ctypes.c_int, [ctypes.c_void_p, _DP]),
     "harm_utoprim_2d_batch": (ctypes.c_int, [_DP, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int),
                                              ctypes.c_long, ctypes.c_double]),
+    "harm_diag_integrals": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Integrals)]),
     "harm_tracers_init": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GridSpec), ctypes.POINTER(ctypes.c_long)]),
     "harm_tracers_put": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GridSpec), ctypes.POINTER(ctypes.c_int), _DP,
                                         ctypes.c_long]),
@@ -331,6 +338,12 @@ class Context:
 
     def sync(self):
         _check(self.lib.harm_sync(self.h))
+
+    def integrals(self):
+        """diag()'s integrals: mass, angular momentum, energy, divbmax and its zone."""
+        d = Integrals()
+        _check(self.lib.harm_diag_integrals(self.h, ctypes.byref(d)))
+        return {"rmed": d.mass, "pp": d.ang_mom, "e": d.energy, "divbmax": d.divbmax, "imax": list(d.imax)}
 
     # tracer particles (tracers.c)
     def tracers_init(self):

@@ -37,6 +37,7 @@ UNITS = {
     "harm_mixed.cu": ["-fmad=true"],    # the mixed-precision step
     "harm_noalloc.cu": ["-fmad=false"],  # batch inversion on a fixed device buffer
     "harm_tracers.cu": ["-fmad=false"],  # tracer particles
+    "harm_diag.cu": ["-fmad=false"],     # diag() integrals and div B
 }
 
 

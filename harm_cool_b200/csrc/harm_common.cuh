@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <string>
 
 #include "harm_b200.h"
@@ -24,6 +25,8 @@ struct DevScalars {
   int halted;                      // set after a failure: later steps do nothing
   int nfail, fail_overflow;        // failed zones met by the current fixup_utoprim
   int wave_done;                   // blocks of k_fu_wave finished (reset by the last)
+  unsigned long long divb_bits;    // diagnostics: bits of max |div B| (a positive double)
+  long long divb_loc;              // and its first zone in loop order
 };
 
 // Problem description passed by value to every kernel.

@@ -164,6 +164,18 @@ int harm_time_kernels(harm_ctx *ctx, int reps, double *ms);
 /* Block until the context's stream is idle; returns any pending device error. */
 int harm_sync(harm_ctx *ctx);
 
+/* ---- diagnostics ---- */
+
+/* diag()'s integrals (diag.c:113-230) over the active zones of the current state. */
+typedef struct harm_integrals {
+  double mass;      /* sum of U[RHO] dV (rmed) */
+  double ang_mom;   /* sum of U[U3] dV (pp) */
+  double energy;    /* sum of U[UU] dV (e) */
+  double divbmax;   /* largest |div B| in the flux-CT form */
+  int imax[3];      /* its zone: r, theta, phi indices from 0 (the first in loop order) */
+} harm_integrals;
+int harm_diag_integrals(harm_ctx *ctx, harm_integrals *out);
+
 /* ---- tracer particles (tracers.c) ----
    Tracers live on the device with the state.  Once a context has tracers,
    every step moves them after the mass diagnostics, as step_ch() calls

@@ -1561,6 +1561,69 @@ void ora_tracers_get(const ora_state *s, int *ids, double *X, signed char *statu
   memcpy(status, s->tr_st, (size_t)s->ntr);
 }
 
+/* ------------------------------------------------------------------ */
+/* diag() integrals and the divergence of B (diag.c:113-230)            */
+
+void ora_diag_integrals(ora_state *s, double *out4, int *imax)
+{
+  const double dx1 = s->prm.dx[1], dx2 = s->prm.dx[2], dx3 = s->prm.dx[3];
+  const double dV = dx1 * dx2 * dx3;  /* main.c:427 */
+  double pp = 0., e = 0., rmed = 0., divbmax = 0.;
+  imax[0] = imax[1] = imax[2] = 0;
+  /* the phi ghost plane below the first one (diag.c:121-129: plane hstop -> plane 0) */
+  if (s->prm.n3 > 2)
+    memcpy(PV(s, s->p, 0, 0, 0), PV(s, s->p, s->hstop, 0, 0), (size_t)s->sn1 * s->sn2 * NPR * sizeof(double));
+  for (int h = s->hstart; h <= s->hstop; h++)
+    for (int i = s->istart; i <= s->istop; i++)
+      for (int j = s->jstart; j <= s->jstop; j++) {
+        geom_t g;
+        state_t q;
+        double U[NPR], divb;
+        get_geometry(s, h, i, j, CENT, &g);
+        get_state(s, PV(s, s->p, h, i, j), &g, &q);
+        primtoflux(s->prm.gam, PV(s, s->p, h, i, j), &q, 0, &g, U);
+        rmed += U[RHO] * dV;
+        pp += U[U3] * dV;
+        e += U[UU] * dV;
+#define P_(hh, ii, jj, k) PV(s, s->p, hh, ii, jj)[k]
+#define G_(ii, jj) s->gdet[((size_t)(ii) * s->sn2 + (jj)) * NPG + CENT]
+        if (s->prm.n3 > 2) {
+          divb = fabs(0.25 * (P_(h, i, j, B1) * G_(i, j) + P_(h - 1, i, j, B1) * G_(i, j)
+                              + P_(h, i, j - 1, B1) * G_(i, j - 1) + P_(h - 1, i, j - 1, B1) * G_(i, j - 1)
+                              - P_(h, i - 1, j, B1) * G_(i - 1, j) - P_(h - 1, i - 1, j, B1) * G_(i - 1, j)
+                              - P_(h, i - 1, j - 1, B1) * G_(i - 1, j - 1)
+                              - P_(h - 1, i - 1, j - 1, B1) * G_(i - 1, j - 1)) / dx1
+                      + 0.25 * (P_(h, i, j, B2) * G_(i, j) + P_(h - 1, i, j, B2) * G_(i, j)
+                                + P_(h, i - 1, j, B2) * G_(i - 1, j) + P_(h - 1, i - 1, j, B2) * G_(i - 1, j)
+                                - P_(h, i, j - 1, B2) * G_(i, j - 1) - P_(h - 1, i, j - 1, B2) * G_(i, j - 1)
+                                - P_(h, i - 1, j - 1, B2) * G_(i - 1, j - 1)
+                                - P_(h - 1, i - 1, j - 1, B2) * G_(i - 1, j - 1)) / dx2
+                      + 0.25 * (P_(h, i, j, B3) * G_(i, j) + P_(h, i - 1, j, B3) * G_(i - 1, j)
+                                + P_(h, i, j - 1, B3) * G_(i, j - 1) + P_(h, i - 1, j - 1, B3) * G_(i - 1, j - 1)
+                                - P_(h - 1, i, j, B3) * G_(i, j) - P_(h - 1, i - 1, j, B3) * G_(i - 1, j)
+                                - P_(h - 1, i, j - 1, B3) * G_(i, j - 1)
+                                - P_(h - 1, i - 1, j - 1, B3) * G_(i - 1, j - 1)) / dx3);
+        } else {
+          divb = fabs(0.5 * (P_(h, i, j, B1) * G_(i, j) + P_(h, i, j - 1, B1) * G_(i, j - 1)
+                             - P_(h, i - 1, j, B1) * G_(i - 1, j) - P_(h, i - 1, j - 1, B1) * G_(i - 1, j - 1)) / dx1
+                      + 0.5 * (P_(h, i, j, B2) * G_(i, j) + P_(h, i - 1, j, B2) * G_(i - 1, j)
+                               - P_(h, i, j - 1, B2) * G_(i, j - 1) - P_(h, i - 1, j - 1, B2) * G_(i - 1, j - 1)) / dx2);
+        }
+#undef P_
+#undef G_
+        if (divb > divbmax) {
+          imax[0] = i - 2;
+          imax[1] = j - 2;
+          imax[2] = s->prm.n3 == 1 ? 0 : h - 1;
+          divbmax = divb;
+        }
+      }
+  out4[0] = rmed;
+  out4[1] = pp;
+  out4[2] = e;
+  out4[3] = divbmax;
+}
+
 int ora_step_ch(ora_state *s)
 {
   double ndt;

@@ -96,6 +96,10 @@ long ora_tracers_init(ora_state *s);
 void ora_tracers_put(ora_state *s, const int *ids, const double *X, long n);
 long ora_tracers_count(const ora_state *s);
 void ora_tracers_get(const ora_state *s, int *ids, double *X, signed char *status);
+/* diag()'s integrals (diag.c:113-230) over the active zones of the state's p:
+   out[0] = sum U[RHO] dV, out[1] = sum U[U3] dV, out[2] = sum U[UU] dV,
+   out[3] = max |div B| (flux-CT definition), imax = its zone (r, theta, phi from 0) */
+void ora_diag_integrals(ora_state *s, double *out, int *imax);
 #ifdef __cplusplus
 }
 #endif

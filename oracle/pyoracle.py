@@ -76,6 +76,7 @@ def oracle_lib():
         lib.ora_tracers_count.restype = ctypes.c_long
         lib.ora_tracers_count.argtypes = [ctypes.c_void_p]
         lib.ora_tracers_get.argtypes = [ctypes.c_void_p, ip, dp, ctypes.POINTER(ctypes.c_byte)]
+        lib.ora_diag_integrals.argtypes = [ctypes.c_void_p, dp, ip]
         _oracle_lib = lib
     return _oracle_lib
 
@@ -136,6 +137,13 @@ class Oracle:
 
     def step(self):
         return self.lib.ora_step_ch(self.h)
+
+    def diag_integrals(self):
+        """diag()'s sums (mass, angular momentum, energy), divbmax and its zone."""
+        out = np.zeros(4)
+        imax = np.zeros(3, dtype=np.int32)
+        self.lib.ora_diag_integrals(self.h, _dp(out), imax.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        return {"rmed": out[0], "pp": out[1], "e": out[2], "divbmax": out[3], "imax": imax.tolist()}
 
     # tracer particles (tracers.c)
     def tracers_init(self, R0, hslope):
@@ -200,6 +208,21 @@ class Reference:
 
     def get(self, name):
         return self.lib.ref_get(name.encode())
+
+    def diag_init(self):
+        """diag(INIT_OUT): (rmed, pp, e) as ener.out prints them (%10.5g), divbmax as the
+        LOG line prints it (%g) and its zone (i, j, h from 0) (diag.c:312-326)."""
+        import re
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            os.mkdir(os.path.join(d, "dumps"))
+            if self.lib.ref_diag_init(d.encode()) != 0:
+                raise RuntimeError("diag(INIT_OUT) failed")
+            ener = open(os.path.join(d, "ener.out")).read().split()
+            log = open(os.path.join(d, "diag_stderr.txt")).read()
+        m = re.search(r"divbmax:\s+(-?\d+)\s+(-?\d+)\s+(-?\d+)\s+(\S+)", log)
+        return {"rmed": float(ener[1]), "pp": float(ener[2]), "e": float(ener[3]),
+                "divbmax": float(m.group(4)), "imax": [int(m.group(1)), int(m.group(2)), int(m.group(3))]}
 
     def tracers(self):
         """The reference's tracer list (tracers.c:24): ids[n][3] = (i, j, h), X[n][3]."""

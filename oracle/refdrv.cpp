@@ -187,6 +187,27 @@ double ref_advance(double *pi, double *pb, double Dt, double *pf, int fullstep)
   return r;
 }
 
+/* diag(INIT_OUT) (diag.c:59-375) run in directory dir (which must hold a dumps/
+   subdirectory): it appends the energy line to dir/ener.out and writes its LOG
+   line, with divbmax and its zone, to dir/diag_stderr.txt */
+int ref_diag_init(const char *dir)
+{
+  char cwd[4096];
+  if (!getcwd(cwd, sizeof(cwd)) || chdir(dir)) return -1;
+  fflush(stderr);
+  int saved = dup(2);
+  int fd = open("diag_stderr.txt", O_WRONLY | O_CREAT | O_TRUNC, 0644);
+  dup2(fd, 2);
+  close(fd);
+  quiet(1);
+  diag(INIT_OUT);
+  quiet(0);
+  fflush(stderr);
+  dup2(saved, 2);
+  close(saved);
+  return chdir(cwd);
+}
+
 /* CPU throughput of the reference's step_ch(): warm-up steps, then timed steps */
 double ref_time_steps(int warm, int steps)
 {

@@ -8,6 +8,8 @@ files).  Fixtures hold only generated numbers:
                 calls of step_ch(), with t, dt and the diagnostics.
   kat_u2p.npz   Utoprim_2d / Utoprim_1dvsq2fix1 / Utoprim_1dfix1 inputs and
                 outputs on perturbed zones of the 2D torus.
+  diag_<config>.npz  diag(INIT_OUT)'s printed integrals and divbmax with its
+                zone, on the state after 5 steps.
   tracers_<config>.npz  the reference's tracer particles (tracers.c) after
                 init_tracers() and after steps, and a seeded custom tracer
                 list carried through 25 more steps.
@@ -128,6 +130,20 @@ def tracer_config(cfg):
     np.savez_compressed(os.path.join(HERE, "tracers_" + cfg + ".npz"), **out)
 
 
+def diag_config(cfg):
+    """diag(INIT_OUT) of the reference after 5 steps (the state of <cfg>.npz's p5):
+    the printed integrals and divbmax with its zone."""
+    sys.path.insert(0, ROOT)
+    from oracle.pyoracle import Reference
+    ref = Reference(cfg)
+    for _ in range(5):
+        ref.step()
+    d = ref.diag_init()
+    np.savez_compressed(os.path.join(HERE, "diag_" + cfg + ".npz"),
+                        printed=np.array([d["rmed"], d["pp"], d["e"], d["divbmax"]]),
+                        imax=np.array(d["imax"], dtype=np.int32))
+
+
 def kat_u2p():
     sys.path.insert(0, ROOT)
     import ctypes
@@ -183,6 +199,8 @@ if __name__ == "__main__":
     if len(sys.argv) > 1:
         if sys.argv[1] == "kat":
             kat_u2p()
+        elif sys.argv[1].startswith("diag_"):
+            diag_config(sys.argv[1][len("diag_"):])
         elif sys.argv[1].startswith("tracers_"):
             tracer_config(sys.argv[1][len("tracers_"):])
         else:
@@ -192,7 +210,7 @@ if __name__ == "__main__":
     from oracle import build_ref
     for cfg in ("t2d", "t3d", "r2d", "r3d"):
         build_ref.build_config(cfg, force=True)
-    for arg in ("t2d", "t3d", "kat", "tracers_r2d", "tracers_r3d"):
+    for arg in ("t2d", "t3d", "kat", "tracers_r2d", "tracers_r3d", "diag_t2d", "diag_t3d"):
         subprocess.run([sys.executable, os.path.abspath(__file__), arg], check=True,
                        stderr=subprocess.DEVNULL)
     for f in sorted(os.listdir(HERE)):
