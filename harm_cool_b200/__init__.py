@@ -51,6 +51,25 @@ class TorusSpec(ctypes.Structure):
                 ("beta", ctypes.c_double)]
 
 
+class RestartHeader(ctypes.Structure):
+    """harm_restart_header: the reference's restart header (restart.c:103-136)."""
+    _fields_ = [("n1", ctypes.c_int), ("n2", ctypes.c_int), ("n3", ctypes.c_int),
+                ("t", ctypes.c_double), ("tf", ctypes.c_double), ("nstep", ctypes.c_int),
+                ("a", ctypes.c_double), ("gam", ctypes.c_double), ("cour", ctypes.c_double),
+                ("DTd", ctypes.c_double), ("DTl", ctypes.c_double), ("DTi", ctypes.c_double),
+                ("DTr", ctypes.c_int), ("dump_cnt", ctypes.c_int), ("image_cnt", ctypes.c_int),
+                ("rdump_cnt", ctypes.c_int), ("dt", ctypes.c_double), ("lim", ctypes.c_int),
+                ("failed", ctypes.c_int), ("Rin", ctypes.c_double), ("Rout", ctypes.c_double),
+                ("hslope", ctypes.c_double), ("R0", ctypes.c_double), ("mass_start", ctypes.c_double),
+                ("mass_in", ctypes.c_double), ("mass_out", ctypes.c_double), ("tdump", ctypes.c_double),
+                ("timage", ctypes.c_double), ("tlog", ctypes.c_double), ("defcon", ctypes.c_double),
+                ("nfailed", ctypes.c_int), ("Rbr", ctypes.c_double), ("cyl_R0", ctypes.c_double),
+                ("cyl_Th0", ctypes.c_double), ("ener_size", ctypes.c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class Integrals(ctypes.Structure):
     """harm_integrals: diag()'s sums and the largest div B (diag.c:113-230)."""
     _fields_ = [("mass", ctypes.c_double), ("ang_mom", ctypes.c_double), ("energy", ctypes.c_double),
@@ -103,6 +122,10 @@ _SIGNATURES = {
     "harm_fixup_utoprim": (ctypes.c_int, [ctypes.c_void_p, _DP]),
     "harm_utoprim_2d_batch": (ctypes.c_int, [_DP, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int),
                                              ctypes.c_long, ctypes.c_double]),
+    "harm_restart_write": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RestartHeader), ctypes.POINTER(GridSpec),
+                                          ctypes.c_char_p]),
+    "harm_restart_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(GridSpec),
+                                         ctypes.POINTER(RestartHeader)]),
     "harm_diag_integrals": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Integrals)]),
     "harm_tracers_init": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GridSpec), ctypes.POINTER(ctypes.c_long)]),
     "harm_tracers_put": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GridSpec), ctypes.POINTER(ctypes.c_int), _DP,
@@ -338,6 +361,26 @@ class Context:
 
     def sync(self):
         _check(self.lib.harm_sync(self.h))
+
+    def restart_write(self, path, **fields):
+        """restart_write(): the state in the reference's restart format; header fields
+        the device does not own come from `fields` (defaults: this problem's parameters,
+        zeros elsewhere)."""
+        pr = self.problem
+        hd = RestartHeader()
+        hd.tf, hd.a, hd.gam, hd.cour = pr.params.tf, pr.params.a, pr.params.gam, pr.params.cour
+        hd.lim, hd.defcon = pr.params.lim, pr.params.defcon
+        hd.Rin, hd.Rout, hd.hslope, hd.R0 = pr.grid.Rin, pr.grid.Rout, pr.grid.hslope, pr.grid.R0
+        hd.Rbr = -1.0
+        for k, v in fields.items():
+            setattr(hd, k, v)
+        _check(self.lib.harm_restart_write(self.h, ctypes.byref(hd), ctypes.byref(pr.grid), path.encode()))
+
+    def restart_read(self, path):
+        """restart_init(): state, time, mass counters and tracers from a restart file."""
+        hd = RestartHeader()
+        _check(self.lib.harm_restart_read(self.h, path.encode(), ctypes.byref(self.problem.grid), ctypes.byref(hd)))
+        return hd.as_dict()
 
     def integrals(self):
         """diag()'s integrals: mass, angular momentum, energy, divbmax and its zone."""

@@ -38,6 +38,7 @@ UNITS = {
     "harm_noalloc.cu": ["-fmad=false"],  # batch inversion on a fixed device buffer
     "harm_tracers.cu": ["-fmad=false"],  # tracer particles
     "harm_diag.cu": ["-fmad=false"],     # diag() integrals and div B
+    "harm_restart.cu": ["-fmad=false"],  # restart files in the reference's format
 }
 
 

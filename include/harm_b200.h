@@ -164,6 +164,37 @@ int harm_time_kernels(harm_ctx *ctx, int reps, double *ms);
 /* Block until the context's stream is idle; returns any pending device error. */
 int harm_sync(harm_ctx *ctx);
 
+/* ---- restart files (restart.c, the reference's ASCII format) ---- */
+
+/* The restart header in file order (restart.c:103-136).  On write, t, dt,
+   mass_in and mass_out come from the context and the other fields from the
+   caller (they are the host driver's: output cadence, counters, the grid's
+   parameters); on read, every field is returned. */
+typedef struct harm_restart_header {
+  int n1, n2, n3;
+  double t, tf;
+  int nstep;
+  double a, gam, cour, DTd, DTl, DTi;
+  int DTr, dump_cnt, image_cnt, rdump_cnt;
+  double dt;
+  int lim, failed;
+  double Rin, Rout, hslope, R0, mass_start, mass_in, mass_out, tdump, timage, tlog, defcon;
+  int nfailed;
+  double Rbr, cyl_R0, cyl_Th0;
+  int ener_size;  /* the ener.out size stored after the body (restart.c:150-158) */
+} harm_restart_header;
+
+/* restart_write() (restart.c:73-186): the context's primitives (phi ghost planes as
+   periodic copies), and its active tracers when it has any (tracers.c:565-603;
+   per-tracer file sizes written as 0).  g is needed only when there are tracers. */
+int harm_restart_write(harm_ctx *ctx, const harm_restart_header *hdr, const harm_grid_spec *g,
+                       const char *path);
+/* restart_init()/restart_read() (restart.c:197-383): primitives, t, dt, mass
+   counters and tracers into the context, pflag cleared, then bound_prim as the
+   reference does after reading.  The file's grid, spin and adiabatic index must
+   match the context's. */
+int harm_restart_read(harm_ctx *ctx, const char *path, const harm_grid_spec *g, harm_restart_header *hdr);
+
 /* ---- diagnostics ---- */
 
 /* diag()'s integrals (diag.c:113-230) over the active zones of the current state. */

@@ -209,6 +209,30 @@ class Reference:
     def get(self, name):
         return self.lib.ref_get(name.encode())
 
+    def restart_write(self):
+        """restart_write(): the reference's restart file, as text."""
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            os.mkdir(os.path.join(d, "dumps"))
+            if self.lib.ref_restart_write(d.encode()) != 0:
+                raise RuntimeError("restart_write failed")
+            return open(os.path.join(d, "dumps", "rdump1.0_1x1x1")).read()
+
+    def restart_init(self, text):
+        """restart_init() from the given restart file text; re-binds the arrays."""
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            os.mkdir(os.path.join(d, "dumps"))
+            with open(os.path.join(d, "dumps", "rdump1.0_1x1x1"), "w") as f:
+                f.write(text)
+            if self.lib.ref_restart_init(d.encode()) != 0:
+                raise RuntimeError("restart_init failed")
+        s3 = (self.sn3, self.sn1, self.sn2)
+        self.p = self._arr("p", s3 + (NPR,))
+        self.ph = self._arr("ph", s3 + (NPR,))
+        self.pflag = np.ctypeslib.as_array(
+            ctypes.cast(self.lib.ref_ptr(b"pflag"), ctypes.POINTER(ctypes.c_byte)), shape=s3)
+
     def diag_init(self):
         """diag(INIT_OUT): (rmed, pp, e) as ener.out prints them (%10.5g), divbmax as the
         LOG line prints it (%g) and its zone (i, j, h from 0) (diag.c:312-326)."""

@@ -208,6 +208,47 @@ int ref_diag_init(const char *dir)
   return chdir(cwd);
 }
 
+/* restart_write() (restart.c:73-186) in directory dir (with a dumps/
+   subdirectory): the file ends up as dir/dumps/rdump1.0_1x1x1 */
+int ref_restart_write(const char *dir)
+{
+  char cwd[4096];
+  if (!getcwd(cwd, sizeof(cwd)) || chdir(dir)) return -1;
+  quiet(1);
+  fflush(stderr);
+  int saved = dup(2);
+  int fd = open("/dev/null", O_WRONLY);
+  dup2(fd, 2);
+  close(fd);
+  restart_write();
+  fflush(stderr);
+  dup2(saved, 2);
+  close(saved);
+  quiet(0);
+  return chdir(cwd);
+}
+
+/* restart_init() (restart.c:197-303) from dir/dumps/: the reference's own
+   reader; it allocates new global arrays, so callers fetch pointers again */
+int ref_restart_init(const char *dir)
+{
+  char cwd[4096];
+  if (!getcwd(cwd, sizeof(cwd)) || chdir(dir)) return -1;
+  quiet(1);
+  fflush(stderr);
+  int saved = dup(2);
+  int fd = open("/dev/null", O_WRONLY);
+  dup2(fd, 2);
+  close(fd);
+  int ok = restart_init();
+  fflush(stderr);
+  dup2(saved, 2);
+  close(saved);
+  quiet(0);
+  if (chdir(cwd)) return -1;
+  return ok ? 0 : -2;
+}
+
 /* CPU throughput of the reference's step_ch(): warm-up steps, then timed steps */
 double ref_time_steps(int warm, int steps)
 {

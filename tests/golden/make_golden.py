@@ -10,6 +10,7 @@ files).  Fixtures hold only generated numbers:
                 outputs on perturbed zones of the 2D torus.
   diag_<config>.npz  diag(INIT_OUT)'s printed integrals and divbmax with its
                 zone, on the state after 5 steps.
+  restart_<config>.npz  restart_write()'s file after 5 steps, as text.
   tracers_<config>.npz  the reference's tracer particles (tracers.c) after
                 init_tracers() and after steps, and a seeded custom tracer
                 list carried through 25 more steps.
@@ -144,6 +145,20 @@ def diag_config(cfg):
                         imax=np.array(d["imax"], dtype=np.int32))
 
 
+def restart_config(cfg):
+    """restart_write() of the reference after 5 steps (the state of
+    <cfg>.npz's p5, or tracers_<cfg>.npz's for a configuration with tracers):
+    the file's text."""
+    sys.path.insert(0, ROOT)
+    from oracle.pyoracle import Reference
+    ref = Reference(cfg)
+    for _ in range(5):
+        ref.step()
+    text = ref.restart_write()
+    np.savez_compressed(os.path.join(HERE, "restart_" + cfg + ".npz"),
+                        text=np.frombuffer(text.encode(), dtype=np.uint8))
+
+
 def kat_u2p():
     sys.path.insert(0, ROOT)
     import ctypes
@@ -199,6 +214,8 @@ if __name__ == "__main__":
     if len(sys.argv) > 1:
         if sys.argv[1] == "kat":
             kat_u2p()
+        elif sys.argv[1].startswith("restart_"):
+            restart_config(sys.argv[1][len("restart_"):])
         elif sys.argv[1].startswith("diag_"):
             diag_config(sys.argv[1][len("diag_"):])
         elif sys.argv[1].startswith("tracers_"):
@@ -210,7 +227,8 @@ if __name__ == "__main__":
     from oracle import build_ref
     for cfg in ("t2d", "t3d", "r2d", "r3d"):
         build_ref.build_config(cfg, force=True)
-    for arg in ("t2d", "t3d", "kat", "tracers_r2d", "tracers_r3d", "diag_t2d", "diag_t3d"):
+    for arg in ("t2d", "t3d", "kat", "tracers_r2d", "tracers_r3d", "diag_t2d", "diag_t3d",
+                "restart_r2d", "restart_t3d"):
         subprocess.run([sys.executable, os.path.abspath(__file__), arg], check=True,
                        stderr=subprocess.DEVNULL)
     for f in sorted(os.listdir(HERE)):
