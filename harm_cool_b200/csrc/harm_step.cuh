@@ -31,9 +31,6 @@
 // phi planes each block sweeps, for the flux and for the zone kernels:
 // consecutive planes of one (r, theta) tile reuse its geometry and (for the
 // phi-direction fluxes) its stencil from L1
-#ifndef HARM_FLUX_PARK
-#define HARM_FLUX_PARK 0
-#endif
 #ifndef HARM_HB_FLUX
 #define HARM_HB_FLUX 1
 #endif
@@ -57,46 +54,6 @@ using flux_t = double;
 #endif
 
 #if !HARM_STEP_MIXED
-// The same face flux with the left state's flux, conserved variables and
-// wave speeds parked in shared memory (18 doubles per thread, stride 128)
-// while the right state is computed, so that they hold no registers then.
-template <int DIR>
-__device__ __forceinline__ void face_flux_parked(double gam, const double *pl, const double *pr, const Geo &q,
-                                                 double *F, double &ctop, int *fail, volatile double *park)
-{
-  {
-    State s;
-    double Fl[8], Ul[8], cmaxl, cminl;
-    get_state(pl, q, s, fail);
-    primtoflux(gam, pl, s, DIR, q.g, Fl);
-    primtoflux(gam, pl, s, 0, q.g, Ul);
-    vchar(gam, pl, s, q, DIR, cmaxl, cminl, fail);
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      park[k * 128] = Fl[k];
-      park[(8 + k) * 128] = Ul[k];
-    }
-    park[16 * 128] = cmaxl;
-    park[17 * 128] = cminl;
-  }
-  State s;
-  double cmaxr, cminr;
-  get_state(pr, q, s, fail);
-  vchar(gam, pr, s, q, DIR, cmaxr, cminr, fail);
-  const double cmaxl = park[16 * 128], cminl = park[17 * 128];
-  double t1 = 0. > cmaxl ? 0. : cmaxl;
-  double cmax = fabs(t1 > cmaxr ? t1 : cmaxr);
-  double t2 = 0. > -cminl ? 0. : -cminl;
-  double cmin = fabs(t2 > -cminr ? t2 : -cminr);
-  ctop = cmax > cmin ? cmax : cmin;
-  double Fr[8], Ur[8];
-  primtoflux(gam, pr, s, DIR, q.g, Fr);
-  primtoflux(gam, pr, s, 0, q.g, Ur);
-  // HLLF = 0, LAXF = 1 (step_ch.c:66-67): the local Lax-Friedrichs flux
-#pragma unroll
-  for (int k = 0; k < 8; k++) F[k] = 0.5 * (park[k * 128] + Fr[k] - ctop * (Ur[k] - park[(8 + k) * 128]));
-}
-
 template <int DIR>
 __device__ __forceinline__ void face_flux(double gam, const double *pl, const double *pr, const Geo &q, double *F,
                                           double &ctop, int *fail)
@@ -139,9 +96,6 @@ __global__ void __launch_bounds__(128, HARM_FLUX_MINB) k_flux(Grid G, const doub
   const int j = (DIR == 2 ? G.jstart : G.jstart - 1) + blockIdx.x * blockDim.x + threadIdx.x;
   const int i = (DIR == 1 ? G.istart : G.istart - 1) + blockIdx.y * blockDim.y + threadIdx.y;
   const int h0 = blockIdx.z * HARM_HB_FLUX, h1 = min(G.n3, h0 + HARM_HB_FLUX);
-#if HARM_FLUX_PARK && !HARM_STEP_MIXED
-  __shared__ double park[18 * 128];
-#endif
   double dtmin = 1.e9;
   const bool in = (i <= G.istop + 1) && (j <= G.jstop + 1);
   if (in) for (int h = h0; h < h1; h++) {
@@ -186,12 +140,7 @@ __global__ void __launch_bounds__(128, HARM_FLUX_MINB) k_flux(Grid G, const doub
       load_geo(geo_at(geo, G, DIR == 1 ? L_FACE1 : DIR == 2 ? L_FACE2 : L_FACE3), G.ng, (long)i * G.sn2 + j, q);
       double Fz[8], ctop;
       int fail = 0;
-#if HARM_FLUX_PARK
-      face_flux_parked<DIR>(G.gam, pl, pr, q, Fz, ctop, &fail,
-                            park + threadIdx.y * blockDim.x + threadIdx.x);
-#else
       face_flux<DIR>(G.gam, pl, pr, q, Fz, ctop, &fail);
-#endif
 #endif
 #pragma unroll
       for (int k = 0; k < 8; k++) F[k * G.nc + c] = Fz[k];
@@ -440,6 +389,17 @@ __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const doub
   }
 }
 
+// the isentropic fall-backs (step_ch.c:277-300), kept out of line: most
+// zones never take them, and inlined they crowd the kernel's hot code out of
+// the instruction cache
+static __device__ __noinline__ int inversion_fallbacks(double gam, double kap, const double *U, const Geo &q,
+                                                       double *pz)
+{
+  int flag = utoprim<1>(gam, kap, U, q, pz);
+  if (flag) flag = utoprim<2>(gam, kap, U, q, pz);
+  return flag;
+}
+
 __global__ void __launch_bounds__(128, HARM_INV_MINB) k_invert(Grid G, const double *__restrict__ pi,
                                                                const double *__restrict__ Ub,
                                                                double *__restrict__ pf,
@@ -466,11 +426,7 @@ __global__ void __launch_bounds__(128, HARM_INV_MINB) k_invert(Grid G, const dou
     pz[k] = __ldg(pi + k * G.nc + c);
   }
   int flag = utoprim<0>(G.gam, 0., U, q, pz);
-  if (flag) {
-    double kap = __ldg(katm + i);
-    flag = utoprim<1>(G.gam, kap, U, q, pz);
-    if (flag) flag = utoprim<2>(G.gam, kap, U, q, pz);
-  }
+  if (flag) flag = inversion_fallbacks(G.gam, __ldg(katm + i), U, q, pz);
   signed char fl = (signed char)flag;
   if (fixup1zone(G.gam, __ldg(floors + gi), __ldg(floors + G.ng + gi), q, pz, &fail)) fl = -33;
 #pragma unroll
