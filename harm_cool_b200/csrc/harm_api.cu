@@ -665,6 +665,14 @@ extern "C" int harm_create(const harm_params *prm, const double *gcov, const dou
   G.lim = prm->lim;
   G.gam = prm->gam; G.cour = prm->cour; G.defcon = prm->defcon; G.tf = prm->tf;
   G.dx1 = prm->dx[1]; G.dx2 = prm->dx[2]; G.dx3 = prm->dx[3];
+  // the mixed path keeps the connection source in FP64 within 2 r_H of the
+  // black hole (r from the Boyer-Lindquist coordinates of the zone centres)
+  {
+    const double rH = 1. + sqrt(1. - prm->a * prm->a);
+    G.isrc32 = G.istop + 1;
+    for (int i = G.istart; i <= G.istop; i++)
+      if (coords[((long)i * d.sn2 + G.jstart) * 4 + 1] >= 2. * rH) { G.isrc32 = i; break; }
+  }
   x->nparts = 148 * 4;
   x->tbx = 32;
   x->tby = 4;
@@ -739,7 +747,7 @@ extern "C" void harm_destroy(harm_ctx *h)
   if (x->graph_exec) cudaGraphExecDestroy(x->graph_exec);
   void *ptrs[] = {x->p, x->ph, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm,
                   x->stage, x->stage_flag, x->fail_list, x->fix_buf, x->partials, x->sc,
-                  x->F1f, x->F2f, x->F3f, x->geo32, x->Ubuf, x->trX, x->trids, x->trst};
+                  x->F1f, x->F2f, x->F3f, x->geo32, x->conn32, x->Ubuf, x->trX, x->trids, x->trst};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (x->pinned) cudaFreeHost(x->pinned);
@@ -879,13 +887,19 @@ extern "C" int harm_set_precision(harm_ctx *h, int mode)
     CK(cudaMalloc(&x->F1f, fb));
     CK(cudaMalloc(&x->F2f, fb));
     CK(cudaMalloc(&x->F3f, G.n3 > 1 ? fb : 8));
-    CK(cudaMalloc(&x->geo32, (size_t)3 * GEO_N * G.ng * sizeof(float)));
-    // FP32 copy of the three face metrics (slots FACE1, FACE2, FACE3)
-    std::vector<double> hg((size_t)3 * GEO_N * G.ng);
+    CK(cudaMalloc(&x->geo32, (size_t)4 * GEO_N * G.ng * sizeof(float)));
+    CK(cudaMalloc(&x->conn32, (size_t)40 * G.ng * sizeof(float)));
+    // FP32 copies of the metric at FACE1, FACE2, FACE3, CENT and of the connection
+    std::vector<double> hg((size_t)4 * GEO_N * G.ng);
     std::vector<float> hf(hg.size());
     CK(cudaMemcpy(hg.data(), x->geo, hg.size() * sizeof(double), cudaMemcpyDeviceToHost));
     for (size_t k = 0; k < hg.size(); k++) hf[k] = (float)hg[k];
     CK(cudaMemcpy(x->geo32, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    std::vector<double> hc((size_t)40 * G.ng);
+    std::vector<float> hcf(hc.size());
+    CK(cudaMemcpy(hc.data(), x->conn, hc.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < hc.size(); k++) hcf[k] = (float)hc[k];
+    CK(cudaMemcpy(x->conn32, hcf.data(), hcf.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
   if (mode != x->mode && x->graph_exec) {
     cudaGraphExecDestroy(x->graph_exec);

@@ -38,6 +38,7 @@ struct Grid {
   int lim;
   double gam, cour, defcon, tf;
   double dx1, dx2, dx3;
+  int isrc32;  // mixed path: first radial index whose connection source runs in float (r >= 2 r_H)
 };
 
 // tracer particles (tracers.c): the grid as the reference's coord() and
@@ -78,7 +79,8 @@ struct Ctx {
   size_t pinned_bytes;
   int mode;                      // HARM_FP64 or HARM_MIXED
   float *F1f, *F2f, *F3f;        // mixed mode: FP32 face fluxes [8][nc]
-  float *geo32;                  // mixed mode: FP32 face geometry [3][GEO_N][ng]
+  float *geo32;                  // mixed mode: FP32 geometry [4 locations][GEO_N][ng]
+  float *conn32;                 // mixed mode: FP32 connection [40][ng]
   double *Ubuf;                  // conserved variables between the two update launches [8][nc]
   int tbx, tby;                  // tile of the zone and face kernels: theta x r threads, 128 in all
   long ntr;                      // tracer particles

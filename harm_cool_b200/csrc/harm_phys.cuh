@@ -335,6 +335,10 @@ __device__ __forceinline__ void u2p_velocities(const U2P &c, const double *Qcon,
 }
 
 // utoprim_2d.c:219-362 on the rescaled U
+// the mixed path's two-phase Newton solve (harm_phys32.cuh)
+__device__ __forceinline__ int gnr_2d_mixed(const U2P &c, double *x);
+
+template <bool MIXED = false>
 __device__ __forceinline__ int u2p_body_2d(U2P &c, const double *U, const Geo &q, double *prim)
 {
   double Bcon[4], Qcon[4], ncon[4], QdotB, utsq;
@@ -358,7 +362,9 @@ __device__ __forceinline__ int u2p_body_2d(U2P &c, const double *U, const Geo &q
   x[0] = fabs(W_last);
   double vsq0 = fabs(vsq_calc(c, W_last));
   x[1] = (vsq0 > 1.) ? (1.0 - 1.e-15) : vsq0;
-  int retval = gnr_2d(c, x);
+  int retval;
+  if constexpr (MIXED) retval = gnr_2d_mixed(c, x);
+  else retval = gnr_2d(c, x);
   double W = x[0], vsq = x[1];
   if ((retval != 0) || (W == FAIL_VAL)) return retval * 100 + 1;
   if (W <= 0. || W > W_TOO_BIG) return 3;
@@ -572,7 +578,7 @@ static __device__ __noinline__ int u2p_body_fix1(U2P &c, const double *U, const 
 
 // the U and prim rescaling around every inversion (utoprim_2d.c:126-176);
 // which: 0 Utoprim_2d, 1 Utoprim_1dvsq2fix1, 2 Utoprim_1dfix1
-template <int which>
+template <int which, bool MIXED = false>
 __device__ __forceinline__ int utoprim(double gam, double K, const double *U, const Geo &q, double *prim)
 {
   double Ut[8], pt[8];
@@ -593,7 +599,7 @@ __device__ __forceinline__ int utoprim(double gam, double K, const double *U, co
   c.gam = gam;
   c.K_atm = K;
   int ret;
-  if (which == 0) ret = u2p_body_2d(c, Ut, q, pt);
+  if (which == 0) ret = u2p_body_2d<MIXED>(c, Ut, q, pt);
   else if (which == 1) ret = u2p_body_vsq2fix1(c, Ut, q, pt);
   else ret = u2p_body_fix1(c, Ut, q, pt);
   if (ret == 0) {

@@ -180,4 +180,118 @@ __device__ __forceinline__ void face_flux_f(float gam, const float *pl, const fl
   for (int k = 0; k < 8; k++) F[k] = 0.5f * (Fl[k] + Fr[k] - ctop * (Ur[k] - Ul[k]));
 }
 
+// ---------------------------------------------------------------------------
+// the mixed path's zone update
+
+// source() (phys.c:165-207) in float: dU_nu = sqrt(-g) T^kappa_lambda
+// Gamma^lambda_{nu kappa}, on an FP32 copy of the connection (stored as
+// [k][min(nu,j)][max(nu,j)] like the FP64 planes); used away from the horizon
+__device__ __forceinline__ void source_f(float gam, const float *pr, const GeoF &q, const float *__restrict__ conn,
+                                         long ng, long gi, double *dU, int *fail)
+{
+  StateF s;
+  get_state_f(pr, q, s, fail);
+  const float r = pr[RHO], u = pr[UU];
+  const float P = (gam - 1.f) * u;
+  const float bsq = dot4f(s.bcon, s.bcov);
+  const float eta = P + r + u + bsq;
+  const float ptot = P + 0.5f * bsq;
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const float t = eta * s.ucon[j] * s.ucov[k] + (j == k ? ptot : 0.f) - s.bcon[j] * s.bcov[k];
+#pragma unroll
+      for (int nu = 0; nu < 4; nu++) {
+        const int lo = nu < j ? nu : j, hi = nu < j ? j : nu;
+        const int pair = lo == 0 ? hi : lo == 1 ? 3 + hi : lo == 2 ? 5 + hi : 9;
+        acc[nu] += t * __ldg(conn + (long)(k * 10 + pair) * ng + gi);
+      }
+    }
+#pragma unroll
+  for (int k = 0; k < 8; k++) dU[k] = 0.;
+  dU[UU] = (double)(acc[0] * q.g);
+  dU[U1] = (double)(acc[1] * q.g);
+  dU[U2] = (double)(acc[2] * q.g);
+  dU[U3] = (double)(acc[3] * q.g);
+}
+
+// func_vsq() (utoprim_2d.c:562-624, gamma-law) in float: the Newton step only
+__device__ __forceinline__ float newton_step_f(float GAMMA, float Bsq, float QdotBsq, float Qtsq, float Qdotn, float D,
+                                               float W, float vsq, float &dW, float &dv)
+{
+  const float Wsq = W * W;
+  const float gtmp = 1.f - vsq;
+  const float sg = sqrtf(gtmp);
+  const float p_tmp = (GAMMA - 1.f) * (W * gtmp - D * sg) / GAMMA;
+  const float dPdW = (GAMMA - 1.f) * gtmp / GAMMA;
+  const float dPdvsq = (GAMMA - 1.f) * (0.5f * D / sg - W) / GAMMA;
+  const float t2 = -0.5f * Bsq + dPdvsq;
+  const float t3 = Bsq + W;
+  const float t4 = t3 * t3;
+  const float t9 = 1.f / Wsq;
+  const float t11 = Qtsq - vsq * t4 + QdotBsq * (Bsq + 2.f * W) * t9;
+  const float t16 = QdotBsq * t9;
+  const float t18 = -Qdotn - 0.5f * Bsq * (1.f + vsq) + 0.5f * t16 - W + p_tmp;
+  const float t21 = 1.f / t3;
+  const float t23 = 1.f / W;
+  const float t24 = t16 * t23;
+  const float t25 = -1.f + dPdW - t24;
+  const float t35 = t25 * t3 + (Bsq - 2.f * dPdvsq) * (QdotBsq + vsq * Wsq * W) * t9 * t23;
+  const float t36 = 1.f / t35;
+  dW = -(t2 * t11 + t4 * t18) * t21 * t36;
+  dv = -(-t25 * t11 - 2.f * (vsq + t24) * t3 * t18) * t21 * t36;
+  return t11 * t11 + t18 * t18;
+}
+
+// The 2D Newton solve of the mixed path: Newton steps in float from the
+// reference's starting point until the relative step falls below 1e-5, then
+// FP64 Newton steps (the residual and Jacobian of func_vsq, the reference's
+// validate_x clamps) until it falls below NEWT_TOL.  Falls back to the FP64
+// solve from the start when the float phase leaves the finite range.
+__device__ __forceinline__ int gnr_2d_mixed(const U2P &c, double *x)
+{
+  float W = (float)x[0], vsq = (float)x[1];
+  const float G = (float)c.gam, Bsq = (float)c.Bsq, QB = (float)c.QdotBsq, Qt = (float)c.Qtsq, Qn = (float)c.Qdotn,
+              D = (float)c.D;
+  bool ok = isfinite(W) && isfinite(vsq) && W > 0.f;
+  for (int n = 0; n < MAX_NEWT_ITER && ok; n++) {
+    float dW, dv;
+    newton_step_f(G, Bsq, QB, Qt, Qn, D, W, vsq, dW, dv);
+    const float W0 = W;
+    W += dW;
+    vsq += dv;
+    float errx = (W == 0.f) ? fabsf(dW) : fabsf(dW / W);
+    errx += (vsq == 0.f) ? fabsf(dv) : fabsf(dv / vsq);
+    W = fabsf(W);
+    W = (W > 1.e20f) ? W0 : W;
+    vsq = vsq < 0.f ? 0.f : vsq;
+    vsq = vsq > 1.f ? 1.f - 1.e-7f : vsq;
+    ok = isfinite(W) && isfinite(vsq) && W > 0.f;
+    if (errx <= 1.e-5f) break;
+  }
+  if (ok) {
+    x[0] = (double)W;
+    x[1] = (double)vsq;
+  }
+  double f = 1., df = 1., dx[2], errx = 1.;
+  for (int n = 0; n < MAX_NEWT_ITER; n++) {
+    func_vsq(c, x, dx, f, df);
+    const double x0 = x[0];
+    x[0] += dx[0];
+    x[1] += dx[1];
+    errx = (x[0] == 0.) ? fabs(dx[0]) : fabs(dx[0] / x[0]);
+    errx += (x[1] == 0.) ? fabs(dx[1]) : fabs(dx[1] / x[1]);
+    x[0] = fabs(x[0]);
+    x[0] = (x[0] > W_TOO_BIG) ? x0 : x[0];
+    x[1] = (x[1] < 0.) ? 0. : x[1];
+    x[1] = (x[1] > 1.) ? (1. - 1.e-15) : x[1];
+    if (fabs(errx) <= NEWT_TOL) break;
+  }
+  if (!isfinite(f) || !isfinite(df)) return 2;
+  if (fabs(errx) > MIN_NEWT_TOL) return 1;
+  return 0;
+}
+
 }  // namespace harm

@@ -332,6 +332,8 @@ __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const doub
                                                               const flux_t *__restrict__ F3,
                                                               const double *__restrict__ geo,
                                                               const double *__restrict__ conn,
+                                                              const float *__restrict__ geo32,
+                                                              const float *__restrict__ conn32,
                                                               double *__restrict__ Ub, DevScalars *sc)
 {
   if (sc->halted) return;
@@ -339,6 +341,9 @@ __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const doub
   const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
   if (i > G.istop || j > G.jstop) return;
   const double Dt = FULL ? sc->dt : 0.5 * sc->dt;
+#if HARM_STEP_MIXED
+  const double idx1 = 1. / G.dx1, idx2 = 1. / G.dx2, idx3 = 1. / G.dx3;
+#endif
   const int h0 = blockIdx.z * HARM_HB_ZONE, h1 = min(G.n3, h0 + HARM_HB_ZONE);
   for (int h = h0; h < h1; h++) {
   const long c = cidx(G, h, i, j);
@@ -347,6 +352,23 @@ __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const doub
   Geo q;
   load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
   double dU[8], U[8];
+#if HARM_STEP_MIXED
+  if (i >= G.isrc32) {
+    // away from the horizon: the connection source in float (harm_phys32.cuh)
+    float pf32[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) pf32[k] = (float)__ldg(pb + k * G.nc + c);
+    GeoF qf;
+    load_geo_f(geo32 + (long)L_CENT * GEO_N * G.ng, G.ng, gi, qf);
+    source_f((float)G.gam, pf32, qf, conn32, G.ng, gi, dU, &fail);
+    double pz[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) pz[k] = __ldg(pi + k * G.nc + c);
+    State s;
+    get_state(pz, q, s, &fail);
+    primtoflux(G.gam, pz, s, 0, q.g, U);
+  } else
+#endif
   if (!FULL) {
     // the predictor advances from pi == pb (advance(p, p, ...), step_ch.c:101):
     // one state serves both source() and primtoU()
@@ -377,10 +399,18 @@ __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const doub
     zone_fluxes<THREE_D>(FX, h, i, j, f1m, f1p, f2m, f2p, f3m, f3p);
 #pragma unroll
     for (int k = 0; k < 8; k++) {
+#if HARM_STEP_MIXED
+      // reciprocal multiplies in place of the divisions: same sum, last-bit rounding
+      if (THREE_D)
+        U[k] += Dt * (-(f1p[k] - f1m[k]) * idx1 - (f2p[k] - f2m[k]) * idx2 - (f3p[k] - f3m[k]) * idx3 + dU[k]);
+      else
+        U[k] += Dt * (-(f1p[k] - f1m[k]) * idx1 - (f2p[k] - f2m[k]) * idx2 + dU[k]);
+#else
       if (THREE_D)
         U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 - (f3p[k] - f3m[k]) / G.dx3 + dU[k]);
       else
         U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 + dU[k]);
+#endif
     }
   }
 #pragma unroll
@@ -425,7 +455,7 @@ __global__ void __launch_bounds__(128, HARM_INV_MINB) k_invert(Grid G, const dou
     U[k] = __ldg(Ub + k * G.nc + c);
     pz[k] = __ldg(pi + k * G.nc + c);
   }
-  int flag = utoprim<0>(G.gam, 0., U, q, pz);
+  int flag = utoprim<0, (bool)HARM_STEP_MIXED>(G.gam, 0., U, q, pz);
   if (flag) flag = inversion_fallbacks(G.gam, __ldg(katm + i), U, q, pz);
   signed char fl = (signed char)flag;
   if (fixup1zone(G.gam, __ldg(floors + gi), __ldg(floors + G.ng + gi), q, pz, &fail)) fl = -33;
@@ -503,11 +533,11 @@ void launch_update(Ctx *x, const double *pi, const double *pb, double *pf)
   const dim3 tile(x->tbx, x->tby);
   const dim3 zg = zone_grid_hb(G, tile);
   if (G.n3 > 1)
-    k_cons<FULL, true><<<zg, tile, 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn,
-                                                                     x->Ubuf, x->sc);
+    k_cons<FULL, true><<<zg, tile, 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn, x->geo32,
+                                                   x->conn32, x->Ubuf, x->sc);
   else
-    k_cons<FULL, false><<<zg, tile, 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn,
-                                                                      x->Ubuf, x->sc);
+    k_cons<FULL, false><<<zg, tile, 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn, x->geo32,
+                                                    x->conn32, x->Ubuf, x->sc);
   k_invert<<<zg, tile, 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->katm,
                                                         x->sc);
 }
