@@ -13,6 +13,6 @@
 #define HARM_INV_MINB 5    // 102 registers
 #endif
 #ifndef HARM_HB_FLUX
-#define HARM_HB_FLUX 8
+#define HARM_HB_FLUX 4
 #endif
 #include "harm_step.cuh"
