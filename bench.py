@@ -178,13 +178,14 @@ def alg_bytes_per_zone(kernel, n3):
     """Algorithmic DRAM bytes per zone of one launch group, FP64 state (8 B per
     primitive, 8 primitives), averaged over the predictor and the corrector:
     flux   per direction: read the zone's primitives, write its face flux;
-    update read pi (and pb in the corrector, where it differs from pi), read
-           the zone's face flux in each direction (each face is shared by two
-           zones), write pf and pflag."""
+    update k_cons reads pi (and pb in the corrector, where it differs from pi)
+           and the zone's face flux in each direction (each face is shared by
+           two zones) and writes U; k_invert reads U and pi and writes pf and
+           pflag."""
     ndir = 3 if n3 > 1 else 2
     if kernel == "flux":
         return ndir * (64 + 64)
-    pred = 64 + ndir * 64 + 64 + 1
+    pred = (64 + ndir * 64 + 64) + (64 + 64 + 64 + 1)
     corr = pred + 64
     return (pred + corr) / 2.0
 
