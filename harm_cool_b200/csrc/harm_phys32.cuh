@@ -183,6 +183,9 @@ __device__ __forceinline__ void face_flux_f(float gam, const float *pl, const fl
 // ---------------------------------------------------------------------------
 // the mixed path's zone update
 
+// relative Newton step at which the float phase hands over to FP64
+constexpr float F32_NEWT_TOL = 1.e-5f;
+
 // source() (phys.c:165-207) in float: dU_nu = sqrt(-g) T^kappa_lambda
 // Gamma^lambda_{nu kappa}, on an FP32 copy of the connection (stored as
 // [k][min(nu,j)][max(nu,j)] like the FP64 planes); used away from the horizon
@@ -269,7 +272,7 @@ __device__ __forceinline__ int gnr_2d_mixed(const U2P &c, double *x)
     vsq = vsq < 0.f ? 0.f : vsq;
     vsq = vsq > 1.f ? 1.f - 1.e-7f : vsq;
     ok = isfinite(W) && isfinite(vsq) && W > 0.f;
-    if (errx <= 1.e-5f) break;
+    if (errx <= F32_NEWT_TOL) break;
   }
   if (ok) {
     x[0] = (double)W;
