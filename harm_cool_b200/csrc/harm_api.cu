@@ -973,8 +973,14 @@ extern "C" int harm_utoprim_2d_batch(const double *U, const double *gcov, const 
 {
   if (!U || !gcov || !gcon || !gdet || !prim || !ret || n < 0) return fail_with(HARM_E_ARG, "null argument");
   if (n == 0) return HARM_OK;
-  double *dU, *da, *db, *dg, *dp;
-  int *dr;
+  // device copies, freed on every return
+  struct Buffers {
+    double *dU = nullptr, *da = nullptr, *db = nullptr, *dg = nullptr, *dp = nullptr;
+    int *dr = nullptr;
+    ~Buffers() { cudaFree(dU); cudaFree(da); cudaFree(db); cudaFree(dg); cudaFree(dp); cudaFree(dr); }
+  } B;
+  double *&dU = B.dU, *&da = B.da, *&db = B.db, *&dg = B.dg, *&dp = B.dp;
+  int *&dr = B.dr;
   CK(cudaMalloc(&dU, n * 8 * 8));
   CK(cudaMalloc(&da, n * 16 * 8));
   CK(cudaMalloc(&db, n * 16 * 8));
@@ -990,7 +996,6 @@ extern "C" int harm_utoprim_2d_batch(const double *U, const double *gcov, const 
   CK(cudaGetLastError());
   CK(cudaMemcpy(prim, dp, n * 64, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(ret, dr, n * sizeof(int), cudaMemcpyDeviceToHost));
-  cudaFree(dU); cudaFree(da); cudaFree(db); cudaFree(dg); cudaFree(dp); cudaFree(dr);
   return HARM_OK;
 }
 
