@@ -293,24 +293,28 @@ def run_ensemble(args):
     """64 seeded 2D tori (N1, N2 from {96,128,192,256}, a, Rmax, beta drawn) advanced
     as one ensemble -- one CUDA graph launch per step, mixed precision, tiles chosen
     by the autotuner per resolution -- against the same 64 tori run one after the
-    other on the plain FP64 path.  Aggregate zone-cycles/s over all members."""
+    other on the plain FP64 path.  Aggregate zone-cycles/s over all members.  Some
+    draws fail the inversion in most zones every step and run far slower than the
+    rest; the same comparison is also reported without them."""
     import harm_cool_b200 as hc
     drawn = hc.ensemble_problems(args.members, seed=args.seed)
     probs = [p for p, _ in drawn]
-    zones = sum(p.zones for p in probs)
     # sequential plain runs: each torus alone, FP64, default tile
-    seq_ms = 0.0
+    solo_ms = []
     for pr in probs:
         c = hc.Context(pr)
         c.init_torus()
         c.run(args.warmup)
-        seq_ms += c.run_timed(args.steps)
+        solo_ms.append(c.run_timed(args.steps) / args.steps)
         c.close()
-    out = {}
-    for name, mixed in (("ensemble_mixed", True), ("ensemble_fp64", False)):
-        ctxs = []
-        tiles = {}
-        for pr in probs:
+    med = sorted(solo_ms)[len(solo_ms) // 2]
+    heavy = [k for k, m in enumerate(solo_ms) if m > 20 * med]
+    subsets = {"all": list(range(len(probs))), "without_failure_heavy": [k for k in range(len(probs)) if k not in heavy]}
+
+    def ensemble(members, mixed):
+        ctxs, tiles = [], {}
+        for k in members:
+            pr = probs[k]
             c = hc.Context(pr)
             c.init_torus()
             if mixed:
@@ -324,25 +328,35 @@ def run_ensemble(args):
         ens.run(args.warmup)
         sampler = ClockSampler(0)
         sampler.start()
-        ms = ens.run_timed(args.steps)
+        ms = ens.run_timed(args.steps) / args.steps
         clocks = sampler.stop()
-        out[name] = {"value": zones * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
-                     "tiles": {"%dx%d" % k: list(v) for k, v in tiles.items()}, "clocks": clocks,
-                     "fail_codes": sorted({c.diag()["fail_code"] for c in ctxs})}
+        fails = sorted({c.diag()["fail_code"] for c in ctxs})
         ens.close()
         for c in ctxs:
             c.close()
-    seq = zones * args.steps / (seq_ms / 1e3)
+        zones = sum(probs[k].zones for k in members)
+        return {"value": zones / (ms / 1e3), "ms_per_step": ms, "zones": zones,
+                "tiles": {"%dx%d" % k: list(v) for k, v in tiles.items()}, "clocks": clocks, "fail_codes": fails}
+
+    out = {}
+    for name, members in subsets.items():
+        zones = sum(probs[k].zones for k in members)
+        seq_ms = sum(solo_ms[k] for k in members)
+        r = {"members": len(members), "zones": zones,
+             "sequential_fp64": {"value": zones / (seq_ms / 1e3), "ms_per_step": seq_ms},
+             "ensemble_mixed": ensemble(members, True)}
+        if name == "all":
+            r["ensemble_fp64"] = ensemble(members, False)
+        r["speedup_vs_sequential"] = r["ensemble_mixed"]["value"] / r["sequential_fp64"]["value"]
+        out[name] = r
     line = {"metric": "aggregate zone-cycles/s, %d seeded 2D tori" % args.members,
-            "value": out["ensemble_mixed"]["value"], "unit": "zone-cycles/s", "n_gpus": 1,
+            "value": out["all"]["ensemble_mixed"]["value"], "unit": "zone-cycles/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64/f32 mixed",
             "data": "synthetic", "config": {"workload": "ensemble of %d 2D tori, N1,N2 in {96,128,192,256}, "
                                                         "a in [0,0.98], Rmax in [9,14], beta in [30,300], seed %d"
-                                                        % (args.members, args.seed),
-                                            "zones": zones},
-            "sequential_fp64": {"value": seq, "ms_per_step": seq_ms / args.steps},
-            "speedup_vs_sequential": out["ensemble_mixed"]["value"] / seq,
-            "members": drawn and [d for _, d in drawn], **out}
+                                                        % (args.members, args.seed)},
+            "failure_heavy_members": heavy, "solo_ms_per_step": solo_ms,
+            "members": [d for _, d in drawn], **out}
     print(json.dumps(line), flush=True)
 
 
