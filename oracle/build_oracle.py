@@ -1,4 +1,4 @@
-"""Compile the CPU oracle (harm_oracle.c) into oracle/_build/libharm_oracle.so.
+"""Compile the CPU oracle (harm_oracle.c, cooleos_oracle.c) into oracle/_build/libharm_oracle.so.
 
 TEST INFRASTRUCTURE ONLY.  -ffp-contract=off keeps every multiply and add
 separate, as the reference compiled for SSE2 does, so the restatement can be
@@ -12,14 +12,14 @@ OUT = os.path.join(HERE, "_build", "libharm_oracle.so")
 
 
 def build(force=False):
-    src = os.path.join(HERE, "harm_oracle.c")
+    srcs = [os.path.join(HERE, f) for f in ("harm_oracle.c", "cooleos_oracle.c")]
     hdr = os.path.join(HERE, "harm_oracle.h")
     if (not force and os.path.exists(OUT)
-            and os.path.getmtime(OUT) > max(os.path.getmtime(src), os.path.getmtime(hdr))):
+            and os.path.getmtime(OUT) > max(os.path.getmtime(f) for f in srcs + [hdr])):
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
     subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-std=c99",
-                    "-Wall", "-Wno-unused-variable", src, "-o", OUT, "-lm"], check=True)
+                    "-Wall", "-Wno-unused-variable"] + srcs + ["-o", OUT, "-lm"], check=True)
     return OUT
 
 

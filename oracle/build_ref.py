@@ -48,6 +48,11 @@ CONFIGS = {
     "r3d": (16, 16, 4, 0.9375, 6.0, 12.0, 100.0),
 }
 TRACER_CONFIGS = ("r2d", "r3d")
+# COOL_EOS on (the reference's own torus literals, whose spin matches cooleos.c's
+# bhs = 0.6, cooleos.c:103), with oracle/eos_standin.c in place of the Fortran
+# table generator
+CONFIGS["ce2d"] = (32, 32, 1, 0.6, 4.0, 11.8, 50.0)
+COOL_CONFIGS = ("ce2d",)
 
 SOURCES = ["bounds", "coord", "diag", "dump", "fixup", "image", "interp", "main",
            "metric", "lu", "phys", "ranc", "restart", "step_ch", "u2p_util",
@@ -62,11 +67,12 @@ def _sub1(pattern, repl, text, what):
     return new
 
 
-def patch_decs(text, n1, n2, n3, tracers=False):
+def patch_decs(text, n1, n2, n3, tracers=False, cool=False):
     text = _sub1(r"^#define N1\s+\(\d+\)", "#define N1       (%d)" % n1, text, "N1")
     text = _sub1(r"^#define N2\s+\(\d+\)", "#define N2       (%d)" % n2, text, "N2")
     text = _sub1(r"^#define N3\s+\(\d+\)", "#define N3       (%d)" % n3, text, "N3")
-    text = _sub1(r"^#define COOL_EOS\s+\(1\)", "#define COOL_EOS  (0)", text, "COOL_EOS")
+    if not cool:
+        text = _sub1(r"^#define COOL_EOS\s+\(1\)", "#define COOL_EOS  (0)", text, "COOL_EOS")
     if not tracers:
         text = _sub1(r"^#define TRACERSDUMP \(1\)", "#define TRACERSDUMP (0)", text, "TRACERSDUMP")
     text = _sub1(r"^#define HDFDUMP \(1\)", "#define HDFDUMP (0)", text, "HDFDUMP")
@@ -114,29 +120,53 @@ def build_config(name, force=False):
     os.makedirs(gen, exist_ok=True)
     os.makedirs(obj, exist_ok=True)
     tracers = name in TRACER_CONFIGS
+    cool = name in COOL_CONFIGS
     with open(os.path.join(REF_SRC, "decs.h")) as f:
-        decs = patch_decs(f.read(), n1, n2, n3, tracers)
+        decs = patch_decs(f.read(), n1, n2, n3, tracers, cool)
     with open(os.path.join(gen, "decs.h"), "w") as f:
         f.write(decs)
     with open(os.path.join(REF_SRC, "defs.h")) as f:
         defs = patch_defs(f.read())
     with open(os.path.join(gen, "defs.h"), "w") as f:
         f.write(defs)
-    with open(os.path.join(REF_SRC, "init.c")) as f:
-        init = patch_init(f.read(), a, rin, rmax, beta)
+    if cool:
+        init = open(os.path.join(REF_SRC, "init.c")).read()   # its own literals
+    else:
+        with open(os.path.join(REF_SRC, "init.c")) as f:
+            init = patch_init(f.read(), a, rin, rmax, beta)
     with open(os.path.join(gen, "init.c"), "w") as f:
         f.write(init)
+    if cool:
+        # cooleos.c with the table fill in this process (no forked workers,
+        # cooleos.c:47-51), cache files that can never be found or written (a stale
+        # file from another generator would otherwise be loaded, cache4d.c:45-120),
+        # and the checker hooks appended to the same translation unit
+        src = open(os.path.join(REF_SRC, "cooleos.c")).read()
+        src = _sub1(r"^#define CACHETHREADS 4", "#define CACHETHREADS 0", src, "CACHETHREADS mpi")
+        src = _sub1(r"^#define CACHETHREADS 6", "#define CACHETHREADS 0", src, "CACHETHREADS")
+        src = _sub1(r'sprintf \(fname, "cache/cache_blh_', 'sprintf (fname, "/dev/null/cache_blh_',
+                    src, "cache file")
+        src += '\n#include "%s"\n' % os.path.join(HERE, "cool_hooks.inc")
+        with open(os.path.join(gen, "cooleos.c"), "w") as f:
+            f.write(src)
     flags = ["g++", "-O2", "-ffp-contract=off", "-fPIC", "-w", "-DMPI_USED",
              "-Dmain=harm_reference_main", "-I" + gen, "-I-",
              "-I" + os.path.join(HERE, "fakempi"), "-I" + REF_SRC]
     objs = []
-    for s in SOURCES + (["tracers"] if tracers else []):
+    for s in SOURCES + (["tracers"] if tracers else []) + (["cache4d", "akima"] if cool else []):
         o = os.path.join(obj, s + ".o")
         run(flags + ["-x", "c++", "-c", os.path.join(REF_SRC, s + ".c"), "-o", o])
         objs.append(o)
     o = os.path.join(obj, "init.o")
     run(flags + ["-x", "c++", "-c", os.path.join(gen, "init.c"), "-o", o])
     objs.append(o)
+    if cool:
+        o = os.path.join(obj, "cooleos.o")
+        run(flags + ["-x", "c++", "-c", os.path.join(gen, "cooleos.c"), "-o", o])
+        objs.append(o)
+        o = os.path.join(obj, "eos_standin.o")
+        run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-c", os.path.join(HERE, "eos_standin.c"), "-o", o])
+        objs.append(o)
     o = os.path.join(obj, "refdrv.o")
     run(flags + ["-c", os.path.join(HERE, "refdrv.cpp"), "-o", o])
     objs.append(o)

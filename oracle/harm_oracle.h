@@ -100,6 +100,23 @@ void ora_tracers_get(const ora_state *s, int *ids, double *X, signed char *statu
    out[0] = sum U[RHO] dV, out[1] = sum U[U3] dV, out[2] = sum U[UU] dV,
    out[3] = max |div B| (flux-CT definition), imax = its zone (r, theta, phi from 0) */
 void ora_diag_integrals(ora_state *s, double *out, int *imax);
+
+/* run-time COOL_EOS (cooleos_oracle.c): tables of the values e, p, Qnu, tau, Yee
+   (cooleos.c:32-37) at the nodes of a rho axis xa[nx] and a T axis ya[ny], one table
+   per radial index, val[ntab][nx][ny][nd] (the reference's MValues order), with the
+   unit and range constants of cooleos.c:83-135, 840-940 */
+enum { ORA_EOS_E = 0, ORA_EOS_P = 1 };
+typedef struct {
+  int nx, ny, nd, ntab;
+  const double *xa, *ya, *val;
+  double rho_unit, u_unit, p_unit, kbol, mav, cl, rho_min, rho_max, t_min, t_max, hh, gam;
+} OraEos;
+double ora_eos_pressure(const OraEos *E, int tab, double rho0, double u, double *lastT);
+double ora_eos_dpdu(const OraEos *E, int tab, double rho0, double u, double *lastT);
+double ora_eos_dpdrho(const OraEos *E, int tab, double rho0, double u, double *lastT);
+void ora_eos_batch(const OraEos *E, int what, long n, const int *tab, const double *rho0, const double *u,
+                   double *lastT, double *out);
+int ora_eos_value(const OraEos *E, int tab, int d, double rho, double T, double *val, double *der);
 #ifdef __cplusplus
 }
 #endif

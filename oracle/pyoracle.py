@@ -174,6 +174,84 @@ class Oracle:
             pass
 
 
+EOS_CONSTANTS = ("rho_unit", "u_unit", "p_unit", "kbol", "mav", "cl", "rho_min", "rho_max",
+                 "t_min", "t_max", "hh", "gam")
+
+
+class OraEos(ctypes.Structure):
+    _fields_ = ([("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nd", ctypes.c_int), ("ntab", ctypes.c_int),
+                 ("xa", ctypes.POINTER(ctypes.c_double)), ("ya", ctypes.POINTER(ctypes.c_double)),
+                 ("val", ctypes.POINTER(ctypes.c_double))]
+                + [(n, ctypes.c_double) for n in EOS_CONSTANTS])
+
+
+class EosTables:
+    """Run-time COOL_EOS tables: rho axis xa[nx], T axis ya[ny], values
+    val[ntab][nx][ny][nd] (e, p, Qnu, tau, Yee per node, cooleos.c:32-37) and the
+    unit and range constants (cooleos.c:83-135, 840-940) as a dict."""
+
+    def __init__(self, xa, ya, val, consts):
+        self.xa = np.ascontiguousarray(xa, dtype=np.float64)
+        self.ya = np.ascontiguousarray(ya, dtype=np.float64)
+        self.val = np.ascontiguousarray(val, dtype=np.float64)
+        self.consts = dict(consts)
+        self.ntab, self.nx, self.ny, self.nd = self.val.shape
+
+    def struct(self):
+        e = OraEos(nx=self.nx, ny=self.ny, nd=self.nd, ntab=self.ntab, xa=_dp(self.xa), ya=_dp(self.ya),
+                   val=_dp(self.val), **{k: float(self.consts[k]) for k in EOS_CONSTANTS})
+        e._keep = self
+        return e
+
+
+class OracleEos:
+    """The CPU restatement of the run-time EOS (cooleos_oracle.c) on given tables."""
+
+    WHAT = {"pressure": 0, "dpdu": 1, "dpdrho": 2}
+
+    def __init__(self, tables):
+        self.lib = oracle_lib()
+        self.tables = tables
+        self.s = tables.struct()
+
+    def batch(self, what, tab, rho0, u, lastT):
+        """what in pressure/dpdu/dpdrho, one call per entry in order; returns
+        (out, lastT after)."""
+        tab = np.ascontiguousarray(tab, dtype=np.int32)
+        rho0 = np.ascontiguousarray(rho0, dtype=np.float64)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        lt = np.array(lastT, dtype=np.float64)
+        out = np.zeros(len(tab))
+        self.lib.ora_eos_batch(ctypes.byref(self.s), self.WHAT[what], ctypes.c_long(len(tab)),
+                               tab.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(rho0), _dp(u), _dp(lt),
+                               _dp(out))
+        return out, lt
+
+    def value(self, tab, d, rho, T, der=False):
+        v, dv = ctypes.c_double(), ctypes.c_double()
+        ok = self.lib.ora_eos_value(ctypes.byref(self.s), tab, d, ctypes.c_double(rho), ctypes.c_double(T),
+                                    ctypes.byref(v), ctypes.byref(dv) if der else None)
+        if not ok:
+            return None
+        return (v.value, dv.value) if der else v.value
+
+
+class _QuietStdout:
+    """Silence file descriptor 1 (the reference prints progress on stdout)."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        fd = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(fd, 1)
+        os.close(fd)
+
+    def __exit__(self, *exc):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
 class Reference:
     """The reference's own step_ch() (oracle/_ref/<config>/libharmref.so).
 
@@ -284,3 +362,58 @@ class Reference:
 
     def step(self):
         self.lib.ref_step()
+
+    # run-time COOL_EOS (COOL_EOS checker builds only; oracle/cool_hooks.inc)
+    def cool_constants(self):
+        c = np.zeros(len(EOS_CONSTANTS))
+        self.lib.ref_cool_constants(_dp(c))
+        return dict(zip(EOS_CONSTANTS, c.tolist()))
+
+    def cool_tables(self):
+        """Every node of every per-radius table, computed by the reference's own
+        table fill, as EosTables."""
+        d = (ctypes.c_int * 4)()
+        self.lib.ref_cool_dims(d)
+        nx, ny, nd, ntab = d[0], d[1], d[2], d[3]
+        xa, ya = np.zeros(nx), np.zeros(ny)
+        val = np.zeros((ntab, nx, ny, nd))
+        hd = ctypes.c_double()
+        with _QuietStdout():
+            for i in range(ntab):
+                self.lib.ref_cool_table(i, _dp(xa), _dp(ya), _dp(val[i]), ctypes.byref(hd))
+        return EosTables(xa, ya, val, self.cool_constants())
+
+    def cool_batch(self, what, tab, rho0, u, lastT):
+        """pressure/dpdu/dpdrho through the reference's own functions, one call per
+        entry in order, each entry with its own guess; returns (out, lastT after)."""
+        fn = {"pressure": self.lib.ref_cool_pressure, "dpdu": self.lib.ref_cool_dpdu,
+              "dpdrho": self.lib.ref_cool_dpdrho}[what]
+        fn.restype = ctypes.c_double
+        fn.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+        out = np.zeros(len(tab))
+        lt = np.array(lastT, dtype=np.float64)
+        with _QuietStdout():
+            for k in range(len(tab)):
+                t = ctypes.c_double(lt[k])
+                out[k] = fn(int(tab[k]), float(rho0[k]), float(u[k]), ctypes.byref(t))
+                lt[k] = t.value
+        return out, lt
+
+    def cool_lastT(self):
+        a = np.zeros((self.sn3, self.sn1, self.sn2))
+        self.lib.ref_cool_lastT_get(_dp(a))
+        return a
+
+    def set_cool_lastT(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self.lib.ref_cool_lastT_set(_dp(a))
+
+    def utoprim_5d(self, U, h, i, j, prim, lastT):
+        """Utoprim_5d at zone (h, i, j) entered as advance() enters it; returns
+        (code, prim after, lastT after)."""
+        U = np.array(U, dtype=np.float64)
+        pr = np.array(prim, dtype=np.float64)
+        t = ctypes.c_double(lastT)
+        with _QuietStdout():
+            r = self.lib.ref_utoprim_5d(_dp(U), h, i, j, _dp(pr), ctypes.byref(t))
+        return r, pr, t.value

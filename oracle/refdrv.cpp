@@ -19,6 +19,7 @@
 #include <time.h>
 #include <unistd.h>
 #include <fcntl.h>
+#include <signal.h>
 
 #ifdef MPI_USED
 void set_MPI(int argc, char *argv[]);
@@ -59,7 +60,17 @@ int ref_init(void)
   MPI_Comm_size(MPI_COMM_WORLD, &nprocs);
   set_MPI(argc, argv);
 #endif
+#if COOL_EOS
+  /* SetupCache_CoolEOS (cooleos.c:977-986) installs process-wide signal handlers:
+     keep the caller's */
+  static const int sigs[] = {SIGINT, SIGQUIT, SIGHUP, SIGTERM, SIGCHLD};
+  struct sigaction saved[5];
+  for (int k = 0; k < 5; k++) sigaction(sigs[k], NULL, &saved[k]);
+#endif
   init();
+#if COOL_EOS
+  for (int k = 0; k < 5; k++) sigaction(sigs[k], &saved[k], NULL);
+#endif
   {
     double (*p)[SN1][SN2][NPR] = (double (*)[SN1][SN2][NPR])(_p);
     double (*gdet)[SN2][NPG] = (double (*)[SN2][NPG])(_gdet);
