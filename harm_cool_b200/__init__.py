@@ -15,7 +15,7 @@ import os
 
 import numpy as np
 
-__all__ = ["HarmError", "Params", "GridSpec", "TorusSpec", "Diag", "Problem", "Context", "Ensemble",
+__all__ = ["HarmError", "Params", "GridSpec", "TorusSpec", "Diag", "Problem", "Context", "Ensemble", "Eos",
            "torus_problem", "set_points", "set_grid", "set_katm", "utoprim_2d_batch", "library",
            "NPR", "NPG"]
 
@@ -89,6 +89,15 @@ class Diag(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+EOS_CONSTANTS = ("rho_unit", "u_unit", "p_unit", "kbol", "mav", "cl", "rho_min", "rho_max",
+                 "t_min", "t_max", "hh", "gam")
+
+
+class EosDesc(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("ntab", ctypes.c_int)] + [
+        (n, ctypes.c_double) for n in EOS_CONSTANTS]
+
+
 _DP = ctypes.POINTER(ctypes.c_double)
 _BP = ctypes.POINTER(ctypes.c_byte)
 _lib = None
@@ -143,6 +152,10 @@ _SIGNATURES = {
     "harm_ensemble_run_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _DP]),
     "harm_utoprim_2d_batch_noalloc": (ctypes.c_int, [_DP, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int),
                                                      ctypes.c_long, ctypes.c_double]),
+    "harm_eos_create": (ctypes.c_int, [ctypes.POINTER(EosDesc), _DP, _DP, _DP, ctypes.POINTER(ctypes.c_void_p)]),
+    "harm_eos_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "harm_eos_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_long, ctypes.POINTER(ctypes.c_int),
+                                      _DP, _DP, _DP, _DP]),
 }
 
 
@@ -254,6 +267,58 @@ def utoprim_2d_batch(U, gcov, gcon, gdet, prim, gam):
     _check(library().harm_utoprim_2d_batch(_dp(U), _dp(gcov), _dp(gcon), _dp(gdet), _dp(prim),
                                            ret.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n, gam))
     return ret
+
+
+class Eos:
+    """Run-time COOL_EOS tables on the device (the reference's per-radius cacheT
+    tables, SetupCache_CoolEOS, cooleos.c:825-992) and batch calls of
+    pressure_rho0_u_CoolEOS / dpdu_calc_CoolEOS / dpdrho_calc_CoolEOS.
+
+    xaxis[nx] (rho, g/cm^3), yaxis[ny] (T, K), values[ntab][nx][ny][5] with
+    e, p, Qnu, tau, Yee per node, consts: the unit and range constants named in
+    EOS_CONSTANTS."""
+
+    WHAT = {"pressure": 0, "dpdu": 1, "dpdrho": 2}
+
+    def __init__(self, xaxis, yaxis, values, consts):
+        self.xaxis = np.ascontiguousarray(xaxis, dtype=np.float64)
+        self.yaxis = np.ascontiguousarray(yaxis, dtype=np.float64)
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        ntab, nx, ny, nd = v.shape
+        if nd != 5 or nx != len(self.xaxis) or ny != len(self.yaxis):
+            raise ValueError("values must be [ntab][nx][ny][5]")
+        d = EosDesc(nx=nx, ny=ny, ntab=ntab, **{k: float(consts[k]) for k in EOS_CONSTANTS})
+        h = ctypes.c_void_p()
+        _check(library().harm_eos_create(ctypes.byref(d), _dp(self.xaxis), _dp(self.yaxis), _dp(v), ctypes.byref(h)))
+        self.h = h
+        self.ntab, self.consts = ntab, dict(consts)
+
+    def batch(self, what, tab, rho0, u, lastT):
+        """One call per entry, each from its own temperature guess; returns
+        (values, guesses after)."""
+        tab = np.ascontiguousarray(tab, dtype=np.int32)
+        rho0 = np.ascontiguousarray(rho0, dtype=np.float64)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        lt = np.array(lastT, dtype=np.float64)
+        out = np.zeros(len(tab))
+        _check(library().harm_eos_batch(self.h, self.WHAT[what], len(tab),
+                                        tab.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(rho0), _dp(u),
+                                        _dp(lt), _dp(out)))
+        return out, lt
+
+    def pressure(self, tab, rho0, u, lastT):
+        return self.batch("pressure", tab, rho0, u, lastT)
+
+    def close(self):
+        if getattr(self, "h", None):
+            library().harm_eos_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------

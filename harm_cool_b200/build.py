@@ -39,6 +39,7 @@ UNITS = {
     "harm_tracers.cu": ["-fmad=false"],  # tracer particles
     "harm_diag.cu": ["-fmad=false"],     # diag() integrals and div B
     "harm_restart.cu": ["-fmad=false"],  # restart files in the reference's format
+    "harm_eos.cu": ["-fmad=false"],      # run-time COOL_EOS tables and batch calls
 }
 
 
@@ -53,14 +54,21 @@ def build(force=False, verbose=False):
     _run(["g++", "-O2", "-ffp-contract=off", "-fPIC", "-std=c++17", "-c",
           os.path.join(CSRC, "host_setup.cpp"), "-o", host_o] + inc)
     objs = [host_o]
-    for unit, flags in UNITS.items():
+
+    def compile_unit(item):
+        unit, flags = item
         o = os.path.join(BUILD, unit.replace(".cu", ".o"))
         out = _run([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xptxas", "-v", "-Xcompiler", "-fPIC",
                                     "-Xcompiler", "-ffp-contract=off", "-c", os.path.join(CSRC, unit),
                                     "-o", o] + flags + inc)
-        if verbose:
-            print(out)
-        objs.append(o)
+        return o, out
+
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as pool:
+        for o, out in pool.map(compile_unit, UNITS.items()):
+            if verbose:
+                print(out)
+            objs.append(o)
     tmp = LIB + ".tmp"
     _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"])
     os.replace(tmp, LIB)

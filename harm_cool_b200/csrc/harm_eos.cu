@@ -1,0 +1,132 @@
+// Run-time COOL_EOS tables on the device and the batch entry points
+// (harm_eos_create, harm_eos_batch).  The tables are the ones the reference
+// builds once per radial index on the host (SetupCache_CoolEOS,
+// cooleos.c:825-992): the caller builds them the same way and hands them over.
+#include <vector>
+
+#include "harm_common.cuh"
+#include "harm_eos.cuh"
+
+struct harm_eos {
+  harm::EosDev d;
+  double *axes = nullptr;  // xa[nx] then ya[ny]
+  double *vals = nullptr;  // [EOS_ND][ntab][nx][ny]
+  int device = 0;
+};
+
+namespace harm {
+
+__global__ void k_eos_batch(EosDev E, int what, long n, const int *__restrict__ tab, const double *__restrict__ rho0,
+                            const double *__restrict__ u, double *__restrict__ lastT, double *__restrict__ out)
+{
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  EosCursor c;
+  c.tab = tab[k];
+  c.T = lastT[k];
+  c.memo = false;
+  double r;
+  if (what == HARM_EOS_PRESSURE) r = eos_pressure(E, c, rho0[k], u[k]);
+  else if (what == HARM_EOS_DPDU) r = eos_dpdu(E, c, rho0[k], u[k]);
+  else r = eos_dpdrho(E, c, rho0[k], u[k]);
+  out[k] = r;
+  lastT[k] = c.T;
+}
+
+}  // namespace harm
+
+using harm::fail_with;
+
+extern "C" int harm_eos_create(const harm_eos_desc *dsc, const double *xaxis, const double *yaxis,
+                               const double *values, harm_eos **out)
+{
+  if (!dsc || !xaxis || !yaxis || !values || !out) return fail_with(HARM_E_ARG, "null argument");
+  *out = nullptr;
+  if (dsc->nx < 3 || dsc->ny < 3 || dsc->ntab < 1) return fail_with(HARM_E_ARG, "tables need 3 or more nodes per axis");
+  for (int k = 1; k < dsc->nx; k++)
+    if (!(xaxis[k] > xaxis[k - 1])) return fail_with(HARM_E_ARG, "rho axis not increasing");
+  for (int k = 1; k < dsc->ny; k++)
+    if (!(yaxis[k] > yaxis[k - 1])) return fail_with(HARM_E_ARG, "T axis not increasing");
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  harm_eos *e = new harm_eos();
+  e->device = dev;
+  const long nx = dsc->nx, ny = dsc->ny, nt = dsc->ntab, plane = nx * ny;
+  // reference node order [ntab][nx][ny][5] -> one plane per value [5][ntab][nx][ny]
+  std::vector<double> v((size_t)harm::EOS_ND * nt * plane);
+  for (long t = 0; t < nt; t++)
+    for (long q = 0; q < plane; q++)
+      for (int d = 0; d < harm::EOS_ND; d++)
+        v[((size_t)d * nt + t) * plane + q] = values[((size_t)t * plane + q) * harm::EOS_ND + d];
+  cudaError_t err = cudaMalloc(&e->axes, (nx + ny) * sizeof(double));
+  if (err == cudaSuccess) err = cudaMalloc(&e->vals, v.size() * sizeof(double));
+  if (err == cudaSuccess) err = cudaMemcpy(e->axes, xaxis, nx * sizeof(double), cudaMemcpyHostToDevice);
+  if (err == cudaSuccess) err = cudaMemcpy(e->axes + nx, yaxis, ny * sizeof(double), cudaMemcpyHostToDevice);
+  if (err == cudaSuccess) err = cudaMemcpy(e->vals, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (err != cudaSuccess) {
+    cudaFree(e->axes);
+    cudaFree(e->vals);
+    delete e;
+    return fail_with(HARM_E_CUDA, std::string("EOS tables: ") + cudaGetErrorString(err));
+  }
+  harm::EosDev &d = e->d;
+  d.nx = dsc->nx;
+  d.ny = dsc->ny;
+  d.ntab = dsc->ntab;
+  d.xa = e->axes;
+  d.ya = e->axes + nx;
+  d.val = e->vals;
+  d.rho_unit = dsc->rho_unit;
+  d.u_unit = dsc->u_unit;
+  d.p_unit = dsc->p_unit;
+  d.kbol = dsc->kbol;
+  d.mav = dsc->mav;
+  d.cl = dsc->cl;
+  d.rho_min = dsc->rho_min;
+  d.rho_max = dsc->rho_max;
+  d.t_min = dsc->t_min;
+  d.t_max = dsc->t_max;
+  d.hh = dsc->hh;
+  d.gam = dsc->gam;
+  *out = e;
+  return HARM_OK;
+}
+
+extern "C" int harm_eos_destroy(harm_eos *e)
+{
+  if (!e) return HARM_OK;
+  cudaFree(e->axes);
+  cudaFree(e->vals);
+  delete e;
+  return HARM_OK;
+}
+
+extern "C" int harm_eos_batch(harm_eos *e, int what, long n, const int *tab, const double *rho0, const double *u,
+                              double *lastT, double *out)
+{
+  if (!e || !tab || !rho0 || !u || !lastT || !out || n < 0) return fail_with(HARM_E_ARG, "null argument");
+  if (what != HARM_EOS_PRESSURE && what != HARM_EOS_DPDU && what != HARM_EOS_DPDRHO)
+    return fail_with(HARM_E_ARG, "unknown EOS quantity");
+  for (long k = 0; k < n; k++)
+    if (tab[k] < 0 || tab[k] >= e->d.ntab) return fail_with(HARM_E_ARG, "table index out of range");
+  if (n == 0) return HARM_OK;
+  struct Buffers {
+    int *t = nullptr;
+    double *r = nullptr, *uu = nullptr, *T = nullptr, *o = nullptr;
+    ~Buffers() { cudaFree(t); cudaFree(r); cudaFree(uu); cudaFree(T); cudaFree(o); }
+  } B;
+  CK(cudaMalloc(&B.t, n * sizeof(int)));
+  CK(cudaMalloc(&B.r, n * sizeof(double)));
+  CK(cudaMalloc(&B.uu, n * sizeof(double)));
+  CK(cudaMalloc(&B.T, n * sizeof(double)));
+  CK(cudaMalloc(&B.o, n * sizeof(double)));
+  CK(cudaMemcpy(B.t, tab, n * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(B.r, rho0, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(B.uu, u, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(B.T, lastT, n * sizeof(double), cudaMemcpyHostToDevice));
+  harm::k_eos_batch<<<(unsigned)((n + 127) / 128), 128>>>(e->d, what, n, B.t, B.r, B.uu, B.T, B.o);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(out, B.o, n * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(lastT, B.T, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return HARM_OK;
+}

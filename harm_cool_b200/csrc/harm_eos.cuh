@@ -1,0 +1,303 @@
+// Run-time COOL_EOS on the device: the reference's per-radius (rho, T) tables,
+// Akima interpolation on a window of 3 or 4 nodes per axis, the Newton solve
+// for T and the pressure with its gamma-law fall-backs.
+//
+// Reference: pressure_rho0_u_CoolEOS (cooleos.c:314-444), the residual and its
+// derivative (cooleos.c:198-300), mnewtc<1> (mnewt.h:105-205),
+// Cache4d::getvalues in SPLINE mode (cache4d.c:863-1134) with calcbox
+// (cache4d.c:408-439) and dvec_bracket (akima.c:314-336), interpolate_akima
+// (akima.c:9-161), spline_akima_der (akima.c:259-298), dpdu_calc_CoolEOS and
+// dpdrho_calc_CoolEOS (cooleos.c:667-741).  Built with -fmad=false and every
+// expression in the reference's order, the FP64 results are the reference's bit
+// for bit.  Two changes that cannot alter a result:
+//  * an Akima window's cubic is formed only for the interval the evaluation
+//    selects (the reference forms all of them and uses one);
+//  * the Newton loop stops when a step is refused (the reference repeats the
+//    identical pass until its 300 iterations are spent).
+// The temperature guess that the reference keeps per zone behind the global
+// LastT pointer (InitCache_CoolEOS, cooleos.c:770-807) travels in an EosCursor.
+// A cursor remembers its last call: a call with bit-identical arguments that
+// starts from the guess the last call left returns the last result, which is
+// what the reference computes for it (a converged guess passes the residual test
+// at once; a failed solve left the guess unchanged and fails the same way).
+#pragma once
+#include <math_constants.h>
+
+#include <cstdint>
+
+namespace harm {
+
+// value planes of a table set (cooleos.c:32-37)
+enum { EOS_E = 0, EOS_P = 1, EOS_QNU = 2, EOS_TAU = 3, EOS_YEE = 4, EOS_ND = 5 };
+
+struct EosDev {
+  int nx, ny, ntab;
+  const double *xa, *ya;   // rho axis [nx], T axis [ny]
+  const double *val;       // [EOS_ND][ntab][nx][ny]
+  double rho_unit, u_unit, p_unit, kbol, mav, cl;
+  double rho_min, rho_max, t_min, t_max, hh, gam;
+};
+
+struct EosCursor {
+  int tab;          // radial index of the table (cacheT[i])
+  double T;         // the zone's temperature guess (*LastT)
+  bool memo;
+  double m_rho, m_u, m_p, m_T;
+};
+
+__device__ __forceinline__ bool same_bits(double a, double b)
+{
+  return __double_as_longlong(a) == __double_as_longlong(b);
+}
+
+// calcbox(SPLINE) of dvec_bracket: window [lo, lo + n - 1] of 3 or 4 nodes.  The
+// bracket is the smallest k in [1, n-2] with v < x[k], else n-1 (1-based left
+// index); a bisection over the increasing axis finds the same k.
+__device__ __forceinline__ void eos_window(int n, const double *__restrict__ x, double v, int &lo, int &cnt)
+{
+  int a = 1, b = n - 1;  // answer in [a, b]; b = n - 1 when no node qualifies
+  while (a < b) {
+    int m = (a + b) >> 1;
+    if (v < __ldg(x + m)) b = m;
+    else a = m + 1;
+  }
+  const int left = a;  // 1-based left end of the bracket; the right end is left + 1
+  int l0 = left - 2, r0 = left + 1;  // 0-based: one node below and one above the bracket
+  if (l0 < 0) l0 = 0;
+  if (r0 >= n) r0 = n - 1;
+  lo = l0;
+  cnt = r0 - l0 + 1;
+}
+
+// Akima node derivative from the four slopes around the node (akima.c:96-113)
+__device__ __forceinline__ double akima_node(double t0, double t1, double t2, double t3)
+{
+  double d0 = t3 - t2;
+  if (d0 < 0.0) d0 *= -1.0;
+  double d1 = t1 - t0;
+  if (d1 < 0.0) d1 *= -1.0;
+  if ((d0 + d1) < 1e-9) return 0.5 * (t1 + t2);
+  return (d0 * t1 + d1 * t2) / (d0 + d1);
+}
+
+// slopes of an Akima window of SI nodes with the two extrapolated intervals on
+// each side (akima.c:34-94): mm[0..SI+2]
+template <int SI>
+__device__ __forceinline__ void akima_slopes(const double *x, const double *y, double *mm)
+{
+#pragma unroll
+  for (int k = 0; k < SI - 1; k++) mm[k + 2] = (y[k + 1] - y[k]) / (x[k + 1] - x[k]);
+  double xl1 = x[0] + x[1] - x[2];
+  double xl0 = xl1 + x[0] - x[1];
+  double yl1 = (x[0] - xl1) * (mm[3] - 2.0 * mm[2]) + y[0];
+  mm[1] = (y[0] - yl1) / (x[0] - xl1);
+  double yl0 = (xl1 - xl0) * (mm[2] - 2.0 * mm[1]) + yl1;
+  mm[0] = (yl1 - yl0) / (xl1 - xl0);
+  double xr2 = x[SI - 1] + x[SI - 2] - x[SI - 3];
+  double xr3 = xr2 + x[SI - 1] - x[SI - 2];
+  double yr2 = (2.0 * mm[SI] - mm[SI - 1]) * (xr2 - x[SI - 1]) + y[SI - 1];
+  mm[SI + 1] = (yr2 - y[SI - 1]) / (xr2 - x[SI - 1]);
+  double yr3 = (2.0 * mm[SI + 1] - mm[SI]) * (xr3 - xr2) + yr2;
+  mm[SI + 2] = (yr3 - yr2) / (xr3 - xr2);
+}
+
+// the interval interpolate_akima's search selects for t (akima.c:140-152)
+template <int SI>
+__device__ __forceinline__ int akima_interval(const double *x, double t)
+{
+  int i = (t > x[1]) ? 1 : 0;
+  if (SI == 4 && t > x[2]) i = 2;
+  return i;
+}
+
+// the cubic of interval i evaluated at t (akima.c:115-158)
+template <int SI>
+__device__ __forceinline__ double akima_at(const double *x, const double *y, const double *mm, int i, double t)
+{
+  double xi = x[0], xi1 = x[1], yi = y[0], yi1 = y[1];
+  double a0 = mm[0], a1 = mm[1], a2 = mm[2], a3 = mm[3], a4 = mm[4];
+  if (i >= 1) { xi = x[1]; xi1 = x[2]; yi = y[1]; yi1 = y[2]; a0 = mm[1]; a1 = mm[2]; a2 = mm[3]; a3 = mm[4]; a4 = mm[5]; }
+  if (SI == 4 && i >= 2) { xi = x[2]; xi1 = x[3]; yi = y[2]; yi1 = y[3]; a0 = mm[2]; a1 = mm[3]; a2 = mm[4]; a3 = mm[5]; a4 = mm[6]; }
+  const double si = akima_node(a0, a1, a2, a3), si1 = akima_node(a1, a2, a3, a4);
+  const double d0 = xi1 - xi;
+  const double d1 = yi1 - yi;
+  const double t2 = d1 / d0;
+  const double c1 = (3.0 * t2 - 2.0 * si - si1) / d0;
+  const double c2 = (si + si1 - 2.0 * t2) / (d0 * d0);
+  const double u = t - xi;
+  return yi + si * u + c1 * u * u + c2 * u * u * u;
+}
+
+// one Akima window: the value at t, and with DER the central difference of
+// spline_akima_der (h = t * 1e-6)
+template <int SI, bool DER>
+__device__ __forceinline__ void akima_window(const double *x, const double *y, double t, double &v, double &dv)
+{
+  double mm[SI + 3];
+  akima_slopes<SI>(x, y, mm);
+  v = akima_at<SI>(x, y, mm, akima_interval<SI>(x, t), t);
+  if (DER) {
+    const double h = t * 1.0E-6;
+    const double tm = t - h, tp = t + h;
+    const double vm = akima_at<SI>(x, y, mm, akima_interval<SI>(x, tm), tm);
+    const double vp = akima_at<SI>(x, y, mm, akima_interval<SI>(x, tp), tp);
+    dv = (vp - vm) / (2.0 * h);
+  }
+}
+
+// getvalues at (rho, T) for one value plane: Akima along T on each rho row of
+// the window, then along rho (cache4d.c:1086-1127)
+template <int SX, int SY, bool DER>
+__device__ __noinline__ void eos_value_w(const EosDev &E, const double *__restrict__ plane, int x0, int y0, double rho,
+                                         double T, double &val, double &der)
+{
+  double xw[SX], yw[SY], row[SX], rowd[SX];
+#pragma unroll
+  for (int k = 0; k < SX; k++) xw[k] = __ldg(E.xa + x0 + k);
+#pragma unroll
+  for (int k = 0; k < SY; k++) yw[k] = __ldg(E.ya + y0 + k);
+#pragma unroll
+  for (int r = 0; r < SX; r++) {
+    const double *src = plane + (long)(x0 + r) * E.ny + y0;
+    double ys[SY];
+#pragma unroll
+    for (int k = 0; k < SY; k++) ys[k] = __ldg(src + k);
+    double d = 0.;
+    akima_window<SY, DER>(yw, ys, T, row[r], d);
+    rowd[r] = d;
+  }
+  double unused;
+  akima_window<SX, false>(xw, row, rho, val, unused);
+  if (DER) akima_window<SX, false>(xw, rowd, rho, der, unused);
+}
+
+// returns false outside the table (the reference's getvalues returns 0 there
+// without writing its outputs, cache4d.c:899-911)
+template <bool DER>
+__device__ __forceinline__ bool eos_value(const EosDev &E, int tab, int d, double rho, int x0, int sx, double T,
+                                          double &val, double &der)
+{
+  if (!(T >= __ldg(E.ya)) || !(T <= __ldg(E.ya + E.ny - 1))) return false;
+  int y0, sy;
+  eos_window(E.ny, E.ya, T, y0, sy);
+  const double *plane = E.val + ((long)d * E.ntab + tab) * E.nx * E.ny;
+  if (sx == 4) {
+    if (sy == 4) eos_value_w<4, 4, DER>(E, plane, x0, y0, rho, T, val, der);
+    else eos_value_w<4, 3, DER>(E, plane, x0, y0, rho, T, val, der);
+  } else {
+    if (sy == 4) eos_value_w<3, 4, DER>(E, plane, x0, y0, rho, T, val, der);
+    else eos_value_w<3, 3, DER>(E, plane, x0, y0, rho, T, val, der);
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool eos_rho_window(const EosDev &E, double rho, int &x0, int &sx)
+{
+  if (!(rho >= __ldg(E.xa)) || !(rho <= __ldg(E.xa + E.nx - 1))) return false;
+  eos_window(E.nx, E.xa, rho, x0, sx);
+  return true;
+}
+
+// mnewtc<1>(300, x, 1e-6, minx, maxx) on (e - e(rho, T)) / e; returns berr
+__device__ __noinline__ double eos_newton_T(const EosDev &E, int tab, double rho, bool rho_in, int x0, int sx,
+                                            double e, double &x, double minx, double maxx)
+{
+  double best = x, besterr = 1.0E100;
+  for (int k = 1; k <= 300; k++) {
+    double ecur = CUDART_NAN, dcur = CUDART_NAN;
+    if (rho_in) {
+      double v, dv;
+      if (eos_value<true>(E, tab, EOS_E, rho, x0, sx, x, v, dv)) { ecur = v; dcur = dv; }
+    }
+    const double F = (e - ecur) / e;
+    const double D = -dcur / e;
+    double bet = -F;
+    double errf = 0.0;
+    errf += fabs(bet);
+    if (errf <= 1.0E-6) return errf;
+    if (errf < besterr) { besterr = errf; best = x; }
+    if (fabs(D) > 0.0) bet = bet / D;
+    const double nv = x + bet;
+    if (nv >= minx && nv <= maxx && nv != x) x = nv;
+    else break;
+  }
+  x = best;
+  return besterr;
+}
+
+// pressure_rho0_u_CoolEOS (cooleos.c:314-444) with the guess in c.T
+__device__ __noinline__ double eos_pressure(const EosDev &E, EosCursor &c, double rho0, double u)
+{
+  if (c.memo && same_bits(rho0, c.m_rho) && same_bits(u, c.m_u) && same_bits(c.T, c.m_T)) return c.m_p;
+  const double rho = rho0 * E.rho_unit;
+  const double e = u * E.u_unit;
+  const double hh = E.hh;
+  double p;
+  if (c.T == 0.0) {
+    const double corrfact = 1.0;
+    c.T = (E.gam - 1.) * u / rho0 / E.kbol * E.mav * E.cl * E.cl * corrfact;
+    if (c.T < E.t_min * (1.0 + hh)) c.T = E.t_min * (1.0 + hh);
+  }
+  if (rho < E.rho_min) p = (E.gam - 1.) * u;
+  else if (rho > E.rho_max) p = (E.gam - 1.) * u;
+  else if (e < 0.0) p = 0.0;
+  else {
+    const double minx = E.t_min * (1.0 + hh), maxx = E.t_max * (1.0 - hh);
+    int x0 = 0, sx = 4;
+    const bool rho_in = eos_rho_window(E, rho, x0, sx);
+    double x = c.T;
+    const double berr = eos_newton_T(E, c.tab, rho, rho_in, x0, sx, e, x, minx, maxx);
+    if (berr > 1.0E-6) p = (E.gam - 1.) * u;
+    else {
+      double v = CUDART_NAN, unused;
+      if (rho_in) {
+        double w;
+        if (eos_value<false>(E, c.tab, EOS_P, rho, x0, sx, x, w, unused)) v = w;
+      }
+      c.T = x;
+      p = v / E.p_unit;
+    }
+  }
+  c.memo = true;
+  c.m_rho = rho0;
+  c.m_u = u;
+  c.m_p = p;
+  c.m_T = c.T;
+  return p;
+}
+
+// dpdu_calc_CoolEOS (cooleos.c:667-704)
+__device__ __forceinline__ double eos_dpdu(const EosDev &E, EosCursor &c, double rho0, double u)
+{
+  const double h = u * E.hh / E.u_unit;
+  const double uP = u + h;
+  double uM = u - h;
+  if (uM > 0) {
+    const double pP = eos_pressure(E, c, rho0, uP);
+    const double pM = eos_pressure(E, c, rho0, uM);
+    return (pP - pM) / (2.0 * h);
+  }
+  uM = u;
+  const double pP = eos_pressure(E, c, rho0, uP);
+  const double pM = eos_pressure(E, c, rho0, uM);
+  return (pP - pM) / (h);
+}
+
+// dpdrho_calc_CoolEOS (cooleos.c:706-741)
+__device__ __forceinline__ double eos_dpdrho(const EosDev &E, EosCursor &c, double rho0, double u)
+{
+  const double h = rho0 * E.hh / E.rho_unit;
+  const double rhoP = rho0 + h;
+  double rhoM = rho0 - h;
+  if (rhoM > 0) {
+    const double pP = eos_pressure(E, c, rhoP, u);
+    const double pM = eos_pressure(E, c, rhoM, u);
+    return (pP - pM) / (2.0 * h);
+  }
+  rhoM = rho0;
+  const double pP = eos_pressure(E, c, rhoP, u);
+  const double pM = eos_pressure(E, c, rhoM, u);
+  return (pP - pM) / (h);
+}
+
+}  // namespace harm

@@ -285,6 +285,38 @@ int harm_utoprim_2d_batch(const double *U, const double *gcov, const double *gco
 int harm_utoprim_2d_batch_noalloc(const double *U, const double *gcov, const double *gcon,
                                   const double *gdet, double *prim, int *ret, long n, double gam);
 
+/* ---- run-time COOL_EOS (cooleos.c, cache4d.c, akima.c, mnewt.h) ---- */
+
+/* Tables of one EOS: per radial index t (the reference's cacheT[t],
+   cooleos.c:70, 825-992) the values e, p, Qnu, tau, Yee (cooleos.c:32-37) at
+   the nodes of a rho axis and a T axis, values[ntab][nx][ny][5] in the
+   reference's node order (Cache4d MValues, cache4d.c:1043).  The tables are
+   built on the host, as the reference builds them (calc_cache_val,
+   cooleos.c:171-194); the units and ranges are cooleos.c's constants
+   (cooleos.c:83-135, 840-940); gam is the gamma-law fall-back's index. */
+typedef struct harm_eos harm_eos;
+typedef struct harm_eos_desc {
+  int nx, ny, ntab;
+  double rho_unit, u_unit, p_unit;  /* RHO_UNIT, U_UNIT, P_UNIT */
+  double kbol, mav, cl;             /* KBOL, MAV, CL of the initial T guess */
+  double rho_min, rho_max;          /* rhoMin, rhoMax (g/cm^3) */
+  double t_min, t_max;              /* TMin, TMax (K) */
+  double hh;                        /* relative margin and difference step, 1e-6 */
+  double gam;
+} harm_eos_desc;
+int harm_eos_create(const harm_eos_desc *desc, const double *xaxis, const double *yaxis,
+                    const double *values, harm_eos **out);
+int harm_eos_destroy(harm_eos *eos);
+
+/* pressure_rho0_u_CoolEOS (cooleos.c:314-444), dpdu_calc_CoolEOS and
+   dpdrho_calc_CoolEOS (cooleos.c:667-741) for n independent entries, each with
+   its table index tab[k] and its temperature guess lastT[k] (the zone's *LastT
+   after InitCache_CoolEOS, cooleos.c:770-807; 0 = none yet), updated in place.
+   Host arrays; out[k] receives the value. */
+enum { HARM_EOS_PRESSURE = 0, HARM_EOS_DPDU = 1, HARM_EOS_DPDRHO = 2 };
+int harm_eos_batch(harm_eos *eos, int what, long n, const int *tab, const double *rho0,
+                   const double *u, double *lastT, double *out);
+
 #ifdef __cplusplus
 }
 #endif

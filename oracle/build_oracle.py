@@ -12,7 +12,7 @@ OUT = os.path.join(HERE, "_build", "libharm_oracle.so")
 
 
 def build(force=False):
-    srcs = [os.path.join(HERE, f) for f in ("harm_oracle.c", "cooleos_oracle.c")]
+    srcs = [os.path.join(HERE, f) for f in ("harm_oracle.c", "cooleos_oracle.c", "eos_standin.c")]
     hdr = os.path.join(HERE, "harm_oracle.h")
     if (not force and os.path.exists(OUT)
             and os.path.getmtime(OUT) > max(os.path.getmtime(f) for f in srcs + [hdr])):

@@ -228,3 +228,63 @@ int ora_eos_value(const OraEos *E, int tab, int d, double rho, double T, double 
 {
   return table_value(E, tab, d, rho, T, val, der);
 }
+
+/* ---- the tables themselves: SetupCache_CoolEOS (cooleos.c:825-992) with the
+   stand-in generator of eos_standin.c in place of abundance_ ---- */
+
+void abundance_(double *rho, double *T, double *HdFac, double *e, double *p, double *Qnu, double *tau,
+                double *xnee, double *xnep);
+
+/* unit and range constants (cooleos.c:83-135, 840-940, 849-855) */
+void ora_eos_constants(double gam, double *o)
+{
+  const double GNEWT = 6.6742867e-8, MSUN = 1.9892e33, KBOL = 1.3e-16, CL = 2.99792458e10;
+  const double MP = 1.67262163783e-24, ME = 9.10956e-28, MN = 1.67492729e-24, MHE = 6.6465e-24;
+  const double MAV = (MP + MN + 2. * ME + MHE) / 5.;
+  const double M_BLH = 3. * MSUN;
+  const double L_UNIT = GNEWT * M_BLH / (CL * CL);
+  const double RHO_SCALE = 1.5e-5, USCALE = 1.0;
+  const double M_UNIT = RHO_SCALE * MSUN;
+  const double RHO_UNIT = M_UNIT / (L_UNIT * L_UNIT * L_UNIT);
+  const double U_UNIT = RHO_UNIT * CL * CL * USCALE;
+  o[0] = RHO_UNIT; o[1] = U_UNIT; o[2] = U_UNIT; o[3] = KBOL; o[4] = MAV; o[5] = CL;
+  o[6] = 1.e2; o[7] = 1.e15; o[8] = 1.e4; o[9] = 1.e18; o[10] = 1.0E-6; o[11] = gam;
+}
+
+/* Cache4d::setindices, LOGARITHMIC axis (cache4d.c:336-343) */
+void ora_eos_axis(int n, double min, double max, double *v)
+{
+  double delta = (log10(max) - log10(min)) / (n - 1);
+  for (int r = 0; r < n; r++) v[r] = pow(10.0, log10(min) + delta * r);
+}
+
+/* HdFac of the table of a zone at radius r (cooleos.c:945-960) */
+double ora_eos_hdfac(double r)
+{
+  const double GNEWT = 6.6742867e-8, MSUN = 1.9892e33, CL = 2.99792458e10;
+  const double M_BLH = 3. * MSUN, bhs = 0.6;
+  double cs = 1.0;
+  double omega = CL * CL * CL / GNEWT / M_BLH / (bhs + pow(r, 1.5));
+  return cs / omega;
+}
+
+/* every node of one table through calc_cache_val (cooleos.c:171-194):
+   val[nx][ny][5] */
+void ora_eos_fill(int nx, int ny, const double *xa, const double *ya, double hdfac, double *val)
+{
+  for (int ix = 0; ix < nx; ix++)
+    for (int iy = 0; iy < ny; iy++) {
+      double ro = xa[ix], te = ya[iy], hd = hdfac;
+      double e, p, Qnu, tau, xnee, xnep;
+      abundance_(&ro, &te, &hd, &e, &p, &Qnu, &tau, &xnee, &xnep);
+      double *v = val + ((size_t)ix * ny + iy) * 5;
+      v[0] = e; v[1] = p; v[2] = Qnu; v[3] = tau; v[4] = (xnee - xnep) / (ro / 1.66e15);
+    }
+}
+
+/* the radius of the zone centre of radial index i (coord(), bl_coord() of
+   coord.c for the modified Kerr-Schild grid), as SetupCache_CoolEOS takes it */
+double ora_zone_r(double startx1, double dx1, double R0, int i)
+{
+  return exp(startx1 + ((i - 2) + 0.5) * dx1) + R0;
+}

@@ -236,6 +236,33 @@ class OracleEos:
         return (v.value, dv.value) if der else v.value
 
 
+def standin_tables(startx1, dx1, R0, sn1, gam, nx=72, ny=72, rho=(1.e2, 1.e15), T=(1.e4, 1.e18)):
+    """The tables SetupCache_CoolEOS builds (cooleos.c:825-992) for radial indices
+    0..sn1-1 of a grid, with oracle/eos_standin.c as the generator, and the unit
+    and range constants: what the COOL_EOS checker build computes."""
+    lib = oracle_lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.ora_eos_hdfac.restype = ctypes.c_double
+    lib.ora_eos_hdfac.argtypes = [ctypes.c_double]
+    lib.ora_zone_r.restype = ctypes.c_double
+    lib.ora_zone_r.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    lib.ora_eos_axis.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, dp]
+    lib.ora_eos_fill.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_double, dp]
+    lib.ora_eos_constants.argtypes = [ctypes.c_double, dp]
+    xa, ya = np.zeros(nx), np.zeros(ny)
+    lib.ora_eos_axis(nx, rho[0], rho[1], _dp(xa))
+    lib.ora_eos_axis(ny, T[0], T[1], _dp(ya))
+    val = np.zeros((sn1, nx, ny, 5))
+    for i in range(sn1):
+        hd = lib.ora_eos_hdfac(lib.ora_zone_r(startx1, dx1, R0, i))
+        lib.ora_eos_fill(nx, ny, _dp(xa), _dp(ya), hd, _dp(val[i]))
+    c = np.zeros(len(EOS_CONSTANTS))
+    lib.ora_eos_constants(gam, _dp(c))
+    consts = dict(zip(EOS_CONSTANTS, c.tolist()))
+    consts["rho_min"], consts["rho_max"], consts["t_min"], consts["t_max"] = rho[0], rho[1], T[0], T[1]
+    return EosTables(xa, ya, val, consts)
+
+
 class _QuietStdout:
     """Silence file descriptor 1 (the reference prints progress on stdout)."""
 

@@ -14,6 +14,8 @@ files).  Fixtures hold only generated numbers:
   tracers_<config>.npz  the reference's tracer particles (tracers.c) after
                 init_tracers() and after steps, and a seeded custom tracer
                 list carried through 25 more steps.
+  eos_<config>.npz  the run-time COOL_EOS of a COOL_EOS build: digests of its
+                tables, pressure/dpdu/dpdrho on seeded entries.
 Each configuration runs in its own process: the reference keeps its state in
 globals.
 """
@@ -210,6 +212,39 @@ def kat_u2p():
     np.savez_compressed(os.path.join(HERE, "kat_u2p.npz"), **res)
 
 
+def eos_inputs(rng, ntab, n):
+    """Seeded (table, rho0, u, T guess) entries over the run-time EOS's branches:
+    table range, gamma-law below rhoMin / above rhoMax, e < 0, no guess yet
+    (LastT == 0), solves that fail at the top of the T range."""
+    tab = rng.integers(0, ntab, n)
+    rho0 = 10 ** rng.uniform(-11, 4, n)
+    u = rho0 * 10 ** rng.uniform(-9, 8, n) * np.where(rng.uniform(size=n) < 0.05, -1.0, 1.0)
+    lastT = np.where(rng.uniform(size=n) < 0.3, 0.0, 10 ** rng.uniform(4.0, 17.9, n))
+    return tab.astype(np.int32), rho0, u, lastT
+
+
+def eos_config(cfg):
+    """The reference's run-time EOS (COOL_EOS checker build, oracle/eos_standin.c
+    as the table generator): its tables' digest and pressure, dp/du, dp/drho with
+    the guesses they leave, on seeded entries."""
+    sys.path.insert(0, ROOT)
+    from oracle.pyoracle import Reference
+    ref = Reference(cfg)
+    T = ref.cool_tables()
+    out = {"grid": np.array([ref.get("startx1"), ref.get("dx1"), ref.get("R0"), ref.get("gam")]),
+           "sn1": np.array(ref.sn1), "sha_tables": np.array(sha(T.val)),
+           "sha_axes": np.array(sha(np.concatenate([T.xa, T.ya]))),
+           "consts": np.array([T.consts[k] for k in sorted(T.consts)]),
+           "const_names": np.array(sorted(T.consts))}
+    tab, rho0, u, lastT = eos_inputs(np.random.default_rng(2024), T.ntab, 3000)
+    out.update(tab=tab, rho0=rho0, u=u, lastT=lastT)
+    for what in ("pressure", "dpdu", "dpdrho"):
+        v, lt = ref.cool_batch(what, tab, rho0, u, lastT)
+        out[what] = v
+        out[what + "_lastT"] = lt
+    np.savez_compressed(os.path.join(HERE, "eos_%s.npz" % cfg), **out)
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1:
         if sys.argv[1] == "kat":
@@ -220,15 +255,17 @@ if __name__ == "__main__":
             diag_config(sys.argv[1][len("diag_"):])
         elif sys.argv[1].startswith("tracers_"):
             tracer_config(sys.argv[1][len("tracers_"):])
+        elif sys.argv[1].startswith("eos_"):
+            eos_config(sys.argv[1][len("eos_"):])
         else:
             one_config(sys.argv[1])
         sys.exit(0)
     sys.path.insert(0, ROOT)
     from oracle import build_ref
-    for cfg in ("t2d", "t3d", "r2d", "r3d"):
+    for cfg in ("t2d", "t3d", "r2d", "r3d", "ce2d"):
         build_ref.build_config(cfg, force=True)
     for arg in ("t2d", "t3d", "kat", "tracers_r2d", "tracers_r3d", "diag_t2d", "diag_t3d",
-                "restart_r2d", "restart_t3d"):
+                "restart_r2d", "restart_t3d", "eos_ce2d"):
         subprocess.run([sys.executable, os.path.abspath(__file__), arg], check=True,
                        stderr=subprocess.DEVNULL)
     for f in sorted(os.listdir(HERE)):
