@@ -156,6 +156,11 @@ _SIGNATURES = {
     "harm_eos_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "harm_eos_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_long, ctypes.POINTER(ctypes.c_int),
                                       _DP, _DP, _DP, _DP]),
+    "harm_utoprim_5d_batch": (ctypes.c_int, [ctypes.c_void_p, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int), _DP,
+                                             _DP, ctypes.POINTER(ctypes.c_int), ctypes.c_long]),
+    "harm_set_eos": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "harm_get_eos_guess": (ctypes.c_int, [ctypes.c_void_p, _DP]),
+    "harm_put_eos_guess": (ctypes.c_int, [ctypes.c_void_p, _DP]),
 }
 
 
@@ -309,6 +314,24 @@ class Eos:
     def pressure(self, tab, rho0, u, lastT):
         return self.batch("pressure", tab, rho0, u, lastT)
 
+    def utoprim_5d(self, U, gcov, gcon, gdet, tab, lastT, prim):
+        """Utoprim_5d (utoprim_5d.c:179) for n independent zones with tables tab[n]
+        and guesses lastT[n]; prim holds the guess on entry and the result on
+        exit.  Returns (codes, guesses after)."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        gcov = np.ascontiguousarray(gcov, dtype=np.float64)
+        gcon = np.ascontiguousarray(gcon, dtype=np.float64)
+        gdet = np.ascontiguousarray(gdet, dtype=np.float64)
+        tab = np.ascontiguousarray(tab, dtype=np.int32)
+        lt = np.array(lastT, dtype=np.float64)
+        assert prim.flags["C_CONTIGUOUS"] and prim.dtype == np.float64
+        n = U.shape[0]
+        ret = np.zeros(n, dtype=np.int32)
+        _check(library().harm_utoprim_5d_batch(self.h, _dp(U), _dp(gcov), _dp(gcon), _dp(gdet),
+                                               tab.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(lt), _dp(prim),
+                                               ret.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n))
+        return ret, lt
+
     def close(self):
         if getattr(self, "h", None):
             library().harm_eos_destroy(self.h)
@@ -394,6 +417,23 @@ class Context:
     def set_precision(self, mode):
         """Context.FP64 (default, bit-compatible with the reference) or Context.MIXED."""
         _check(self.lib.harm_set_precision(self.h, mode))
+
+    def set_eos(self, eos):
+        """Step with COOL_EOS on the given Eos tables (one per radial index,
+        N1+4 of them); None goes back to the gamma-law step."""
+        _check(self.lib.harm_set_eos(self.h, eos.h if eos is not None else None))
+        self._eos = eos  # the tables must outlive the attachment
+
+    def eos_guess(self):
+        """The per-zone temperature guesses _aLastT[SN3][SN1][SN2] (cooleos.c:69)."""
+        a = np.zeros(self.shape)
+        _check(self.lib.harm_get_eos_guess(self.h, _dp(a)))
+        return a
+
+    def put_eos_guess(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.shape == self.shape
+        _check(self.lib.harm_put_eos_guess(self.h, _dp(a)))
 
     def step_ch(self):
         """One full step (step_ch.c:90-140), asynchronous; see sync()."""

@@ -597,7 +597,11 @@ void invalidate_graph(Ctx *x)
   }
 }
 
-int launch_step(Ctx *x) { return x->mode == HARM_MIXED ? mixed::launch_step(x) : exact::launch_step(x); }
+int launch_step(Ctx *x)
+{
+  if (x->cool) return cool_launch_step(x);
+  return x->mode == HARM_MIXED ? mixed::launch_step(x) : exact::launch_step(x);
+}
 
 // structural checks on the host geometry: the device stores only the
 // non-zero, independent entries
@@ -747,7 +751,8 @@ extern "C" void harm_destroy(harm_ctx *h)
   if (x->graph_exec) cudaGraphExecDestroy(x->graph_exec);
   void *ptrs[] = {x->p, x->ph, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm,
                   x->stage, x->stage_flag, x->fail_list, x->fix_buf, x->partials, x->sc,
-                  x->F1f, x->F2f, x->F3f, x->geo32, x->conn32, x->Ubuf, x->trX, x->trids, x->trst};
+                  x->F1f, x->F2f, x->F3f, x->geo32, x->conn32, x->Ubuf, x->trX, x->trids, x->trst,
+                  x->lastT};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (x->pinned) cudaFreeHost(x->pinned);
@@ -881,6 +886,7 @@ extern "C" int harm_set_precision(harm_ctx *h, int mode)
 {
   if (!h || (mode != HARM_FP64 && mode != HARM_MIXED)) return fail_with(HARM_E_ARG, "bad argument");
   Ctx *x = &h->x;
+  if (x->cool && mode != HARM_FP64) return fail_with(HARM_E_ARG, "the COOL_EOS step runs in FP64");
   if (mode == HARM_MIXED && !x->F1f) {
     const Grid &G = x->G;
     const size_t fb = 8 * G.nc * sizeof(float);
@@ -919,6 +925,13 @@ extern "C" int harm_run(harm_ctx *h, int nsteps)
 {
   if (!h || nsteps < 0) return fail_with(HARM_E_ARG, "bad argument");
   Ctx *x = &h->x;
+  if (x->cool && x->cool_seed) {
+    // the seeding step runs outside the graph, which holds the ordinary step
+    if (nsteps == 0) return HARM_OK;
+    int rc = launch_step(x);
+    if (rc) return rc;
+    nsteps--;
+  }
   if (!x->graph_exec) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
@@ -1084,6 +1097,7 @@ extern "C" int harm_run_timed(harm_ctx *h, int nsteps, double *ms)
   Ctx *x = &h->x;
   int rc = harm_run(h, 0);  // capture the graph outside the timed region
   if (rc) return rc;
+  if (!x->graph_exec) return fail_with(HARM_E_ARG, "COOL_EOS: run the seeding step before timing");
   EventPair e;
   CK(cudaEventCreate(&e.a));
   CK(cudaEventCreate(&e.b));
@@ -1126,6 +1140,7 @@ extern "C" int harm_time_kernels(harm_ctx *h, int reps, double *ms)
 {
   if (!h || !ms || reps < 1) return fail_with(HARM_E_ARG, "bad argument");
   Ctx *x = &h->x;
+  if (x->cool) return fail_with(HARM_E_ARG, "per-kernel timing is for the gamma-law step");
   return x->mode == HARM_MIXED ? mixed::time_kernels(x, reps, ms) : exact::time_kernels(x, reps, ms);
 }
 
@@ -1160,6 +1175,7 @@ extern "C" int harm_autotune_tile(harm_ctx *h, int steps, int *bx, int *by)
 {
   if (!h || steps < 1) return fail_with(HARM_E_ARG, "bad argument");
   Ctx *x = &h->x;
+  if (x->cool) return fail_with(HARM_E_ARG, "the tile autotuner is for the gamma-law step");
   static const int cand[][2] = {{32, 4}, {64, 2}, {16, 8}, {128, 1}};
   const size_t pb = (size_t)8 * x->G.nc * sizeof(double);
   DevScalars s0;
@@ -1233,6 +1249,7 @@ extern "C" int harm_ensemble_create(harm_ctx *const *members, int n, harm_ensemb
   if (!members || n < 1 || !out) return fail_with(HARM_E_ARG, "bad argument");
   for (int k = 0; k < n; k++) {
     if (!members[k]) return fail_with(HARM_E_ARG, "null member");
+    if (members[k]->x.cool) return fail_with(HARM_E_ARG, "ensembles hold gamma-law members");
     if (members[k]->x.device != members[0]->x.device) return fail_with(HARM_E_ARG, "members on different devices");
     for (int m = 0; m < k; m++)
       if (members[m] == members[k]) return fail_with(HARM_E_ARG, "a context appears twice");

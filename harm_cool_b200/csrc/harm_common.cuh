@@ -6,6 +6,7 @@
 #include <string>
 
 #include "harm_b200.h"
+#include "harm_eos.cuh"
 #include "harm_phys.cuh"
 #include "host_setup.h"
 
@@ -88,6 +89,10 @@ struct Ctx {
   int *trids;                    // [ntr][3] labels (i, j, h)
   signed char *trst;             // [ntr] 0 active, 1 in, 2 out, 3 jet, -1 dropped
   TrParams trp;
+  bool cool;                     // COOL_EOS step with the run-time EOS below
+  EosDev eos;                    // the attached tables (owned by the caller's harm_eos)
+  double *lastT;                 // [nc] per-zone temperature guesses (_aLastT)
+  bool cool_seed;                // the next step may meet zones without a guess
 };
 
 __device__ __forceinline__ void record_fail(DevScalars *sc, int code, int h, int i, int j)
@@ -161,6 +166,7 @@ void launch_mass(Ctx *x);
 int sync_status(Ctx *x);
 
 void launch_tracers(Ctx *x);     // update_tracers() (harm_tracers.cu)
+int cool_launch_step(Ctx *x);    // the COOL_EOS step (harm_cool.cu)
 void invalidate_graph(Ctx *x);   // a captured step no longer matches the context
 
 // one step and the per-kernel timing of each precision variant
@@ -177,4 +183,11 @@ int time_kernels(Ctx *x, int reps, double *ms);
 
 struct harm_ctx {
   harm::Ctx x;
+};
+
+struct harm_eos {
+  harm::EosDev d;
+  double *axes = nullptr;  // xa[nx] then ya[ny]
+  double *vals = nullptr;  // [EOS_ND][ntab][nx][ny]
+  int device = 0;
 };

@@ -7,13 +7,6 @@
 #include "harm_common.cuh"
 #include "harm_eos.cuh"
 
-struct harm_eos {
-  harm::EosDev d;
-  double *axes = nullptr;  // xa[nx] then ya[ny]
-  double *vals = nullptr;  // [EOS_ND][ntab][nx][ny]
-  int device = 0;
-};
-
 namespace harm {
 
 __global__ void k_eos_batch(EosDev E, int what, long n, const int *__restrict__ tab, const double *__restrict__ rho0,
@@ -49,6 +42,11 @@ extern "C" int harm_eos_create(const harm_eos_desc *dsc, const double *xaxis, co
     if (!(yaxis[k] > yaxis[k - 1])) return fail_with(HARM_E_ARG, "T axis not increasing");
   int dev = 0;
   CK(cudaGetDevice(&dev));
+  // the EOS calls nest deeper than the default 1 KiB per-thread stack of this
+  // process's context (Utoprim_5d -> Jacobian -> pressure -> T solve -> table)
+  size_t stack = 0;
+  CK(cudaDeviceGetLimit(&stack, cudaLimitStackSize));
+  if (stack < 4096) CK(cudaDeviceSetLimit(cudaLimitStackSize, 4096));
   harm_eos *e = new harm_eos();
   e->device = dev;
   const long nx = dsc->nx, ny = dsc->ny, nt = dsc->ntab, plane = nx * ny;

@@ -199,7 +199,7 @@ __device__ __forceinline__ bool eos_rho_window(const EosDev &E, double rho, int 
 }
 
 // mnewtc<1>(300, x, 1e-6, minx, maxx) on (e - e(rho, T)) / e; returns berr
-__device__ __noinline__ double eos_newton_T(const EosDev &E, int tab, double rho, bool rho_in, int x0, int sx,
+static __device__ __noinline__ double eos_newton_T(const EosDev &E, int tab, double rho, bool rho_in, int x0, int sx,
                                             double e, double &x, double minx, double maxx)
 {
   double best = x, besterr = 1.0E100;
@@ -226,7 +226,7 @@ __device__ __noinline__ double eos_newton_T(const EosDev &E, int tab, double rho
 }
 
 // pressure_rho0_u_CoolEOS (cooleos.c:314-444) with the guess in c.T
-__device__ __noinline__ double eos_pressure(const EosDev &E, EosCursor &c, double rho0, double u)
+static __device__ __noinline__ double eos_pressure(const EosDev &E, EosCursor &c, double rho0, double u)
 {
   if (c.memo && same_bits(rho0, c.m_rho) && same_bits(u, c.m_u) && same_bits(c.T, c.m_T)) return c.m_p;
   const double rho = rho0 * E.rho_unit;

@@ -317,6 +317,27 @@ enum { HARM_EOS_PRESSURE = 0, HARM_EOS_DPDU = 1, HARM_EOS_DPDRHO = 2 };
 int harm_eos_batch(harm_eos *eos, int what, long n, const int *tab, const double *rho0,
                    const double *u, double *lastT, double *out);
 
+/* Utoprim_5d() (utoprim_5d.c:179-245, the COOL_EOS inversion) over n
+   independent zones: U, gcov, gcon, gdet, prim as harm_utoprim_2d_batch, tab[n]
+   the table (radial index) of each zone and lastT[n] its temperature guess,
+   updated in place. */
+int harm_utoprim_5d_batch(const harm_eos *eos, const double *U, const double *gcov,
+                          const double *gcon, const double *gdet, const int *tab, double *lastT,
+                          double *prim, int *ret, long n);
+
+/* Step the context with COOL_EOS (decs.h:110): the run-time EOS pressure in
+   the fluxes, wave speeds, source and primtoU, and Utoprim_5d as the
+   inversion (step_ch.c:241-300, 437-441).  The tables must have ntab = N1+4,
+   table t serving radial index t, and must outlive the attachment; NULL
+   detaches them (back to the gamma-law step).  FP64 only.  The context keeps
+   the per-zone temperature guesses _aLastT (cooleos.c:69, 836), all unset at
+   first, as the reference's calloc leaves them. */
+int harm_set_eos(harm_ctx *ctx, const harm_eos *eos);
+/* The guesses in the reference's layout double[SN3][SN1][SN2].  After
+   harm_put_eos_guess the next step is a seeding step (see harm_run). */
+int harm_get_eos_guess(harm_ctx *ctx, double *lastT);
+int harm_put_eos_guess(harm_ctx *ctx, const double *lastT);
+
 #ifdef __cplusplus
 }
 #endif

@@ -435,6 +435,15 @@ class Reference:
         a = np.ascontiguousarray(a, dtype=np.float64)
         self.lib.ref_cool_lastT_set(_dp(a))
 
+    def cool_prim_to_U(self, pr, h, i, j, lastT):
+        """primtoU at zone (h, i, j) with the zone's guess; returns (U, lastT after)."""
+        pr = np.array(pr, dtype=np.float64)
+        U = np.zeros(NPR)
+        t = ctypes.c_double(lastT)
+        with _QuietStdout():
+            self.lib.ref_cool_prim_to_U(_dp(pr), h, i, j, _dp(U), ctypes.byref(t))
+        return U, t.value
+
     def utoprim_5d(self, U, h, i, j, prim, lastT):
         """Utoprim_5d at zone (h, i, j) entered as advance() enters it; returns
         (code, prim after, lastT after)."""

@@ -16,6 +16,9 @@ files).  Fixtures hold only generated numbers:
                 list carried through 25 more steps.
   eos_<config>.npz  the run-time COOL_EOS of a COOL_EOS build: digests of its
                 tables, pressure/dpdu/dpdrho on seeded entries.
+  cool_<config>.npz  step_ch() of a COOL_EOS build: states, flags, times and
+                temperature guesses after init() and steps; Utoprim_5d known
+                answers.
 Each configuration runs in its own process: the reference keeps its state in
 globals.
 """
@@ -245,6 +248,66 @@ def eos_config(cfg):
     np.savez_compressed(os.path.join(HERE, "eos_%s.npz" % cfg), **out)
 
 
+COOL_STEPS = (1, 2, 5, 12)
+
+
+def cool_config(cfg):
+    """step_ch() with COOL_EOS on (COOL_EOS checker build): the state, flags,
+    times and temperature guesses after init() and after 1, 2, 5, 12 steps; then
+    Utoprim_5d known answers on perturbed zones of the last state."""
+    sys.path.insert(0, ROOT)
+    from oracle.pyoracle import Reference
+    ref = Reference(cfg)
+    hs = slice(1, ref.n3 + 1) if ref.n3 > 1 else slice(0, 1)
+    out = {"n": np.array([ref.n1, ref.n2, ref.n3])}
+    for name in ("a", "gam", "cour", "defcon", "tf", "Rin", "Rout", "hslope", "R0",
+                 "dx1", "dx2", "dx3", "startx1", "startx2", "startx3"):
+        out["par_" + name] = np.array(ref.get(name))
+    out["p0"] = ref.p[hs].copy()
+    out["pflag0"] = ref.pflag[hs].copy()
+    out["t0"] = np.array([ref.get("t"), ref.get("dt")])
+    out["lastT0"] = ref.cool_lastT()
+    done = 0
+    from oracle.pyoracle import _QuietStdout
+    for n in COOL_STEPS:
+        with _QuietStdout():
+            while done < n:
+                ref.step()
+                done += 1
+        out["p%d" % n] = ref.p[hs].copy()
+        out["pflag%d" % n] = ref.pflag[hs].copy()
+        out["t%d" % n] = np.array([ref.get("t"), ref.get("dt")])
+        out["lastT%d" % n] = ref.cool_lastT()
+        out["diag%d" % n] = np.array([ref.get(s) for s in SCALARS])
+    # Utoprim_5d on perturbed states of active zones, each with its own guess
+    rng = np.random.default_rng(55)
+    last = ref.cool_lastT()
+    p = ref.p[hs].copy()
+    g = ref.geometry()
+    rows = []
+    for k in range(240):
+        h = 0 if ref.n3 == 1 else int(rng.integers(1, ref.n3 + 1))
+        i = int(rng.integers(2, ref.n1 + 2))
+        j = int(rng.integers(2, ref.n2 + 2))
+        pz = p[h - (1 if ref.n3 > 1 else 0), i, j].copy()
+        pert = pz.copy()
+        pert[:5] *= 1.0 + 1e-3 * rng.uniform(-1, 1, 5)
+        U, _ = ref.cool_prim_to_U(pert, h, i, j, last[h, i, j])
+        r, res, lt = ref.utoprim_5d(U, h, i, j, pz, last[h, i, j])
+        rows.append((h, i, j, U, pz, last[h, i, j], r, res, lt))
+    out["u5_hij"] = np.array([r[:3] for r in rows], dtype=np.int32)
+    out["u5_U"] = np.array([r[3] for r in rows])
+    out["u5_guess"] = np.array([r[4] for r in rows])
+    out["u5_lastT"] = np.array([r[5] for r in rows])
+    out["u5_ret"] = np.array([r[6] for r in rows], dtype=np.int32)
+    out["u5_prim"] = np.array([r[7] for r in rows])
+    out["u5_lastT_after"] = np.array([r[8] for r in rows])
+    out["u5_gcov"] = np.array([g["gcov"][r[1], r[2], 3] for r in rows])
+    out["u5_gcon"] = np.array([g["gcon"][r[1], r[2], 3] for r in rows])
+    out["u5_gdet"] = np.array([g["gdet"][r[1], r[2], 3] for r in rows])
+    np.savez_compressed(os.path.join(HERE, "cool_%s.npz" % cfg), **out)
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1:
         if sys.argv[1] == "kat":
@@ -257,6 +320,8 @@ if __name__ == "__main__":
             tracer_config(sys.argv[1][len("tracers_"):])
         elif sys.argv[1].startswith("eos_"):
             eos_config(sys.argv[1][len("eos_"):])
+        elif sys.argv[1].startswith("cool_"):
+            cool_config(sys.argv[1][len("cool_"):])
         else:
             one_config(sys.argv[1])
         sys.exit(0)
@@ -265,7 +330,7 @@ if __name__ == "__main__":
     for cfg in ("t2d", "t3d", "r2d", "r3d", "ce2d"):
         build_ref.build_config(cfg, force=True)
     for arg in ("t2d", "t3d", "kat", "tracers_r2d", "tracers_r3d", "diag_t2d", "diag_t3d",
-                "restart_r2d", "restart_t3d", "eos_ce2d"):
+                "restart_r2d", "restart_t3d", "eos_ce2d", "cool_ce2d"):
         subprocess.run([sys.executable, os.path.abspath(__file__), arg], check=True,
                        stderr=subprocess.DEVNULL)
     for f in sorted(os.listdir(HERE)):

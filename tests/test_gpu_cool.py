@@ -1,0 +1,146 @@
+"""GPU: the COOL_EOS step (step_ch() with the run-time EOS and Utoprim_5d)
+against the reference's own COOL_EOS build, through tests/golden/cool_ce2d.npz.
+
+The reference's loops visit zones one after another and each zone's EOS calls
+continue from the temperature guess its previous call left; the device keeps
+that chain per zone (and seeds the first step row by row), so the FP64 result
+is expected bit for bit: primitives, flags, t, dt and the guesses.  The tables
+are the ones the reference's build makes (oracle/eos_standin.c in place of its
+Fortran generator), rebuilt by the oracle and checked against the reference's
+digest in test_oracle_cooleos."""
+import numpy as np
+import pytest
+
+from helpers import active, full_state, load_fixture, problem_from_fixture
+
+pytestmark = pytest.mark.gpu
+STEPS = (1, 2, 5, 12)
+
+
+@pytest.fixture(scope="module")
+def hc(harm_lib):
+    import harm_cool_b200
+    return harm_cool_b200
+
+
+@pytest.fixture(scope="module")
+def fx():
+    return load_fixture("cool_ce2d")
+
+
+@pytest.fixture(scope="module")
+def eos(hc, fx, oracle_built):
+    from oracle.pyoracle import standin_tables
+    T = standin_tables(float(fx["par_startx1"]), float(fx["par_dx1"]), float(fx["par_R0"]),
+                       int(fx["n"][0]) + 4, float(fx["par_gam"]))
+    e = hc.Eos(T.xa, T.ya, T.val, T.consts)
+    yield e
+    e.close()
+
+
+def _problem(hc, fx):
+    pr = problem_from_fixture(fx)
+    pr.torus = hc.TorusSpec(4.0, 11.8, 1.e-3, 50.0)   # the torus of init.c:108-117
+    return pr
+
+
+def _bits_equal(a, b):
+    return np.array_equal(np.ascontiguousarray(a).view(np.int64), np.ascontiguousarray(b).view(np.int64))
+
+
+def test_cool_init_matches_reference(hc, fx):
+    pr = _problem(hc, fx)
+    ctx = hc.Context(pr)
+    ctx.init_torus()
+    p = ctx.get_prims()
+    assert _bits_equal(active(pr, p), fx["p0"])
+    assert ctx.time() == tuple(fx["t0"])
+    ctx.close()
+
+
+def _compare(pr, ctx, fx, n):
+    p, fl = ctx.get_prims(with_flags=True)
+    g = active(pr, p)
+    ok = g.view(np.int64) == fx["p%d" % n].view(np.int64)
+    assert ok.all(), (n, int((~ok).sum()), np.argwhere(~ok)[:5].tolist())
+    assert np.array_equal(active(pr, fl), fx["pflag%d" % n]), n
+    assert ctx.time() == tuple(fx["t%d" % n]), n
+    assert _bits_equal(ctx.eos_guess(), fx["lastT%d" % n]), n
+    # the diagnostics are device reductions in another summation order
+    d = ctx.diag()
+    assert d["fail_code"] == 0
+    for k, name in enumerate(("mdot", "edot", "ldot")):
+        ref = fx["diag%d" % n][k]
+        assert abs(d[name] - ref) <= 1e-12 * max(abs(ref), 1e-300), (n, name, d[name], ref)
+    ref = fx["diag%d" % n][5]
+    assert abs(d["mass_curr"] - ref) <= 1e-13 * abs(ref), n
+
+
+def test_cool_steps_match_reference(hc, fx, eos):
+    pr = _problem(hc, fx)
+    ctx = hc.Context(pr)
+    ctx.put_prims(full_state(pr, fx["p0"]), full_state(pr, fx["pflag0"]))
+    ctx.set_time(*fx["t0"])
+    ctx.set_eos(eos)
+    assert not ctx.eos_guess().any()
+    done = 0
+    for n in STEPS:
+        ctx.run(n - done)     # the first call runs the seeding step, then the graph
+        done = n
+        _compare(pr, ctx, fx, n)
+    ctx.close()
+
+
+def test_cool_step_by_step_matches_run(hc, fx, eos):
+    """harm_step_ch one step at a time (no graph) gives the same states."""
+    pr = _problem(hc, fx)
+    ctx = hc.Context(pr)
+    ctx.put_prims(full_state(pr, fx["p0"]), full_state(pr, fx["pflag0"]))
+    ctx.set_time(*fx["t0"])
+    ctx.set_eos(eos)
+    for _ in range(5):
+        ctx.step_ch()
+    ctx.sync()
+    _compare(pr, ctx, fx, 5)
+    ctx.close()
+
+
+def test_cool_resume_from_saved_guesses(hc, fx, eos):
+    """State and guesses of step 5 put back: steps 6..12 as the reference."""
+    pr = _problem(hc, fx)
+    ctx = hc.Context(pr)
+    ctx.set_eos(eos)
+    ctx.put_prims(full_state(pr, fx["p5"]), full_state(pr, fx["pflag5"]))
+    ctx.set_time(*fx["t5"])
+    ctx.set_mass(*fx["diag5"][6:8])
+    ctx.put_eos_guess(fx["lastT5"])
+    ctx.run(7)
+    _compare(pr, ctx, fx, 12)
+    ctx.close()
+
+
+def test_utoprim_5d_matches_reference_kat(hc, fx, eos):
+    n = len(fx["u5_ret"])
+    prim = np.ascontiguousarray(fx["u5_guess"].copy())
+    ret, lt = eos.utoprim_5d(fx["u5_U"], fx["u5_gcov"].reshape(n, 16), fx["u5_gcon"].reshape(n, 16), fx["u5_gdet"],
+                             fx["u5_hij"][:, 1], fx["u5_lastT"], prim)
+    assert np.array_equal(ret, fx["u5_ret"])
+    assert _bits_equal(prim, fx["u5_prim"])
+    assert _bits_equal(lt, fx["u5_lastT_after"])
+
+
+def test_cool_context_rules(hc, fx, eos):
+    pr = _problem(hc, fx)
+    ctx = hc.Context(pr)
+    ctx.init_torus()
+    ctx.set_eos(eos)
+    with pytest.raises(hc.HarmError):
+        ctx.set_precision(hc.Context.MIXED)
+    small = hc.Context(hc.torus_problem(16, 16, 1))
+    with pytest.raises(hc.HarmError):
+        small.set_eos(eos)      # 20 radial indices, 36 tables
+    ctx.set_eos(None)           # back to the gamma-law step
+    ctx.run(2)
+    assert ctx.diag()["fail_code"] == 0
+    small.close()
+    ctx.close()
