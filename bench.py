@@ -360,6 +360,76 @@ def run_ensemble(args):
     print(json.dumps(line), flush=True)
 
 
+def run_cool(args):
+    """The COOL_EOS step on the 256x256 torus of the reference's init.c literals
+    (a=0.6, rin=4, rmax=11.8, beta=50; cooleos.c's 3 Msun hole and units), FP64,
+    with the reference's 72x72 per-radius tables built on the host by the
+    synthetic ideal-gas-plus-radiation generator of harm_cool_b200.eos_tables in
+    place of the Fortran EOS.  The first step seeds the per-zone temperature
+    guesses row by row and runs outside the timed region."""
+    import numpy as np
+    import harm_cool_b200 as hc
+    from harm_cool_b200 import eos_tables
+    n = args.cool_n
+    pr = hc.torus_problem(n, n, 1, a=0.6, rin=4.0, rmax=11.8, beta=50.0)
+    xa, ya, val, consts = eos_tables.build_tables(eos_tables.zone_radii(pr), gam=pr.params.gam)
+    eos = hc.Eos(xa, ya, val, consts)
+    ctx = hc.Context(pr)
+    ctx.init_torus()
+    ctx.set_eos(eos)
+    t0 = time.perf_counter()
+    ctx.run(1)                       # the seeding step
+    seed_s = time.perf_counter() - t0
+    ctx.run(args.warmup - 1)
+    # a few ms per step: time enough steps for the clock sampler to see the run
+    args.steps = max(args.steps, 200)
+    sampler = ClockSampler(0)
+    sampler.start()
+    ms = ctx.run_timed(args.steps)
+    clocks = sampler.stop()
+    zones = pr.zones
+    value = zones * args.steps / (ms / 1e3)
+    kms = ctx.time_kernels(reps=2)
+    import torch
+    pinned = torch.empty(pr.shape + (8,), dtype=torch.float64, pin_memory=True).numpy()
+    pinned[...] = ctx.get_prims()
+    ms_e2e = ctx.step_ch_host_timed(pinned, args.e2e_steps)
+    bytes_host = int(np.prod(pr.shape)) * 8 * 8
+    dom = max(("flux", "update"), key=lambda k: kms[k])
+    peak, peak_kind = measured_peaks()
+    alg = alg_bytes_per_zone(dom, 1) * zones
+    achieved = alg / (kms[dom] / 1e3) / 1e9
+    d = ctx.diag()
+    line = {"metric": "zone-cycles/s %dx%d GRMHD step_ch with COOL_EOS" % (n, n), "value": value,
+            "unit": "zone-cycles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "FM torus %dx%d (a=0.6, rin=4, rmax=11.8, beta=50), COOL_EOS, 72x72 "
+                                   "per-radius tables (rho 1e2-1e15, T 1e4-1e18), synthetic generator" % (n, n),
+                       "l2": "tables (%.0f MB) stay in L2; state per step is small" % (val.nbytes / 1e6)},
+            "seeding_step_s": seed_s,
+            "e2e": {"value": zones * args.e2e_steps / (ms_e2e / 1e3), "unit": "zone-cycles/s",
+                    "h2d_bytes_per_step": bytes_host, "d2h_bytes_per_step": bytes_host,
+                    "path": "harm_step_ch_host (upload, step, download)"},
+            "gpu_launches": kernels_per_step(1) * args.steps,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "algorithmic_bytes": alg,
+                         "peak_source": peak_kind,
+                         "note": "the T solves make these kernels FP64-latency bound, not HBM bound"},
+            "kernel_ms": kms, "clocks": clocks, "sim_time": ctx.time(), "fail_code": d["fail_code"]}
+    ctx.close()
+    eos.close()
+    if not args.no_cpu_baseline:
+        exe = os.path.join(ROOT, "oracle", "_ref", "ce%d" % n, "refbench")
+        if os.path.exists(exe):
+            out = subprocess.run([exe, "1", "1"], capture_output=True, text=True, cwd=os.path.dirname(exe)).stdout
+            r = json.loads(out.strip().splitlines()[-1])
+            line["cpu_baseline"] = {"value": r["zone_cycles_per_s"], "unit": "zone-cycles/s", "cores": 1,
+                                    "kind": "reference", "sample": "reference COOL_EOS step_ch() on %dx%d, "
+                                    "1 step after 1 warm-up, oracle/eos_standin.c tables" % (n, n)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -372,8 +442,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
-    ap.add_argument("--workload", choices=("torus", "ensemble"), default="torus",
-                    help="torus: the 288x256x256 step (default); ensemble: 64 seeded 2D tori")
+    ap.add_argument("--workload", choices=("torus", "ensemble", "cool"), default="torus",
+                    help="torus: the 288x256x256 step (default); ensemble: 64 seeded 2D tori; "
+                         "cool: the 256x256 COOL_EOS step")
+    ap.add_argument("--cool-n", type=int, default=256)
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--seed", type=int, default=0)
     args = ap.parse_args()
@@ -385,6 +457,9 @@ def main():
         return
     if args.workload == "ensemble":
         run_ensemble(args)
+        return
+    if args.workload == "cool":
+        run_cool(args)
         return
     world, rank, local = dist_setup()
     try:

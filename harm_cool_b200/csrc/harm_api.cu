@@ -1140,7 +1140,7 @@ extern "C" int harm_time_kernels(harm_ctx *h, int reps, double *ms)
 {
   if (!h || !ms || reps < 1) return fail_with(HARM_E_ARG, "bad argument");
   Ctx *x = &h->x;
-  if (x->cool) return fail_with(HARM_E_ARG, "per-kernel timing is for the gamma-law step");
+  if (x->cool) return cool_time_kernels(x, reps, ms);
   return x->mode == HARM_MIXED ? mixed::time_kernels(x, reps, ms) : exact::time_kernels(x, reps, ms);
 }
 

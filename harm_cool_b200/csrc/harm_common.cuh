@@ -167,6 +167,7 @@ int sync_status(Ctx *x);
 
 void launch_tracers(Ctx *x);     // update_tracers() (harm_tracers.cu)
 int cool_launch_step(Ctx *x);    // the COOL_EOS step (harm_cool.cu)
+int cool_time_kernels(Ctx *x, int reps, double *ms);
 void invalidate_graph(Ctx *x);   // a captured step no longer matches the context
 
 // one step and the per-kernel timing of each precision variant

@@ -452,3 +452,68 @@ extern "C" int harm_utoprim_5d_batch(const harm_eos *eos, const double *U, const
   CK(cudaMemcpy(lastT, B.T, n * 8, cudaMemcpyDeviceToHost));
   return HARM_OK;
 }
+
+namespace harm {
+
+// reps ordinary COOL_EOS steps, one launch group at a time with an event after
+// each (slots as the gamma-law variants': flux, update, bound_prim,
+// fixup_utoprim, diagnostics); the seeding step, if pending, runs first, untimed
+int cool_time_kernels(Ctx *x, int reps, double *ms)
+{
+  if (x->cool_seed) {
+    int rc = cool_launch_step(x);
+    if (rc) return rc;
+  }
+  const Grid &G = x->G;
+  const int nev = 16;
+  cudaEvent_t ev[nev];
+  for (auto &e : ev) CK(cudaEventCreate(&e));
+  double acc[HARM_NKERNELS] = {0, 0, 0, 0, 0};
+  const dim3 tile(x->tbx, x->tby);
+  const dim3 zg((G.n2 + tile.x - 1) / tile.x, (G.n1 + tile.y - 1) / tile.y, G.n3);
+  for (int r = 0; r < reps; r++) {
+    int e = 0, slot[nev];
+    CK(cudaEventRecord(ev[e++], x->stream));
+    for (int half = 0; half < 2; half++) {
+      const bool full = half == 1;
+      double *pi = x->p, *pb = full ? x->ph : x->p, *pf = full ? x->p : x->ph;
+      if (full) cool::launch_flux_cool<true>(x, pb, false);
+      else cool::launch_flux_cool<false>(x, pb, false);
+      slot[e] = 0; CK(cudaEventRecord(ev[e++], x->stream));
+      if (G.n3 > 1) {
+        if (full) cool::k_cons_cool<true, true><<<zg, tile, 0, x->stream>>>(G, pi, pb, x->F1, x->F2, x->F3, x->geo, x->conn, x->eos, x->lastT, x->Ubuf, x->sc);
+        else cool::k_cons_cool<false, true><<<zg, tile, 0, x->stream>>>(G, pi, pb, x->F1, x->F2, x->F3, x->geo, x->conn, x->eos, x->lastT, x->Ubuf, x->sc);
+      } else {
+        if (full) cool::k_cons_cool<true, false><<<zg, tile, 0, x->stream>>>(G, pi, pb, x->F1, x->F2, x->F3, x->geo, x->conn, x->eos, x->lastT, x->Ubuf, x->sc);
+        else cool::k_cons_cool<false, false><<<zg, tile, 0, x->stream>>>(G, pi, pb, x->F1, x->F2, x->F3, x->geo, x->conn, x->eos, x->lastT, x->Ubuf, x->sc);
+      }
+      cool::k_invert_cool<<<zg, tile, 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->eos,
+                                                      x->lastT, x->sc);
+      slot[e] = 1; CK(cudaEventRecord(ev[e++], x->stream));
+      if (full) {
+        cool::k_diag_flux<<<1, 1024, 0, x->stream>>>(G, x->F1, x->sc);
+        slot[e] = 4; CK(cudaEventRecord(ev[e++], x->stream));
+      }
+      launch_bound(x, pf);
+      slot[e] = 2; CK(cudaEventRecord(ev[e++], x->stream));
+      launch_fixup_utoprim(x, pf);
+      slot[e] = 3; CK(cudaEventRecord(ev[e++], x->stream));
+      launch_bound(x, pf);
+      slot[e] = 2; CK(cudaEventRecord(ev[e++], x->stream));
+    }
+    launch_mass(x);
+    slot[e] = 4; CK(cudaEventRecord(ev[e++], x->stream));
+    CK(cudaEventSynchronize(ev[e - 1]));
+    for (int k = 1; k < e; k++) {
+      float f;
+      CK(cudaEventElapsedTime(&f, ev[k - 1], ev[k]));
+      acc[slot[k]] += f;
+    }
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  const double per_step[HARM_NKERNELS] = {2, 2, 4, 2, 1};
+  for (int k = 0; k < HARM_NKERNELS; k++) ms[k] = acc[k] / (reps * per_step[k]);
+  return sync_status(x);
+}
+
+}  // namespace harm
