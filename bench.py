@@ -236,6 +236,8 @@ def run_ours(args, world, rank, local):
     zones = pr.zones
     ctx, ms, clocks = timed_run(hc, pr, local, world, args.steps, args.warmup, mixed=False)
     value = zones * args.steps * world / (ms / 1e3)
+    # the state after warmup + steps, for the mixed run's L1 at the same step
+    pa = ctx.get_prims() if not args.no_mixed else None
     d = ctx.diag()
     # end to end through the host-array call: upload p, step, download p every step
     import torch
@@ -269,7 +271,6 @@ def run_ours(args, world, rank, local):
                          "step_frac": zones * STATE_BYTES_PER_ZONE_CYCLE / (ms / args.steps / 1e3) / 1e9 / peak},
             "kernel_ms": kms, "clocks": clocks, "sim_time": ctx.time(), "fail_code": d["fail_code"]}
     if not args.no_mixed:
-        pa = ctx.get_prims()
         ctx.close()
         ctxm, msm, clocksm = timed_run(hc, pr, local, world, args.steps, args.warmup, mixed=True)
         pb = ctxm.get_prims()
@@ -387,6 +388,7 @@ def run_cool(args):
     sampler.start()
     ms = ctx.run_timed(args.steps)
     clocks = sampler.stop()
+    pa = ctx.get_prims()          # after warmup + steps, for the mixed run's L1
     zones = pr.zones
     value = zones * args.steps / (ms / 1e3)
     kms = ctx.time_kernels(reps=2)
@@ -418,6 +420,27 @@ def run_cool(args):
                          "note": "the T solves make these kernels FP64-latency bound, not HBM bound"},
             "kernel_ms": kms, "clocks": clocks, "sim_time": ctx.time(), "fail_code": d["fail_code"]}
     ctx.close()
+    if not args.no_mixed:
+        # the face physics' EOS calls in FP32, the same steps
+        cm = hc.Context(pr)
+        cm.init_torus()
+        cm.set_precision(hc.Context.MIXED)
+        cm.set_eos(eos)
+        cm.run(args.warmup)
+        sampler = ClockSampler(0)
+        sampler.start()
+        msm = cm.run_timed(args.steps)
+        clocksm = sampler.stop()
+        pb = cm.get_prims()
+        act = (slice(None), slice(2, -2), slice(2, -2))
+        if args.dump_cool:
+            import numpy as np
+            np.savez_compressed(args.dump_cool, fp64=pa, mixed=pb)
+        line["mixed"] = {"value": zones * args.steps / (msm / 1e3), "ms_per_step": msm / args.steps,
+                         "speedup_vs_fp64": ms / msm, "clocks": clocksm, "kernel_ms": cm.time_kernels(reps=2),
+                         "l1_vs_fp64": l1_errors(pa[act], pb[act]), "l1_after_steps": args.warmup + args.steps,
+                         "fail_code": cm.diag()["fail_code"]}
+        cm.close()
     eos.close()
     if not args.no_cpu_baseline:
         exe = os.path.join(ROOT, "oracle", "_ref", "ce%d" % n, "refbench")
@@ -446,6 +469,7 @@ def main():
                     help="torus: the 288x256x256 step (default); ensemble: 64 seeded 2D tori; "
                          "cool: the 256x256 COOL_EOS step")
     ap.add_argument("--cool-n", type=int, default=256)
+    ap.add_argument("--dump-cool", default=None, help="save the FP64 and mixed COOL_EOS states (npz)")
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--seed", type=int, default=0)
     args = ap.parse_args()

@@ -154,8 +154,8 @@ _SIGNATURES = {
                                                      ctypes.c_long, ctypes.c_double]),
     "harm_eos_create": (ctypes.c_int, [ctypes.POINTER(EosDesc), _DP, _DP, _DP, ctypes.POINTER(ctypes.c_void_p)]),
     "harm_eos_destroy": (ctypes.c_int, [ctypes.c_void_p]),
-    "harm_eos_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_long, ctypes.POINTER(ctypes.c_int),
-                                      _DP, _DP, _DP, _DP]),
+    "harm_eos_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_long,
+                                      ctypes.POINTER(ctypes.c_int), _DP, _DP, _DP, _DP]),
     "harm_utoprim_5d_batch": (ctypes.c_int, [ctypes.c_void_p, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int), _DP,
                                              _DP, ctypes.POINTER(ctypes.c_int), ctypes.c_long]),
     "harm_set_eos": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
@@ -298,15 +298,15 @@ class Eos:
         self.h = h
         self.ntab, self.consts = ntab, dict(consts)
 
-    def batch(self, what, tab, rho0, u, lastT):
+    def batch(self, what, tab, rho0, u, lastT, mixed=False):
         """One call per entry, each from its own temperature guess; returns
-        (values, guesses after)."""
+        (values, guesses after).  mixed: interpolation and T solve in FP32."""
         tab = np.ascontiguousarray(tab, dtype=np.int32)
         rho0 = np.ascontiguousarray(rho0, dtype=np.float64)
         u = np.ascontiguousarray(u, dtype=np.float64)
         lt = np.array(lastT, dtype=np.float64)
         out = np.zeros(len(tab))
-        _check(library().harm_eos_batch(self.h, self.WHAT[what], len(tab),
+        _check(library().harm_eos_batch(self.h, self.WHAT[what], 1 if mixed else 0, len(tab),
                                         tab.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(rho0), _dp(u),
                                         _dp(lt), _dp(out)))
         return out, lt

@@ -886,7 +886,7 @@ extern "C" int harm_set_precision(harm_ctx *h, int mode)
 {
   if (!h || (mode != HARM_FP64 && mode != HARM_MIXED)) return fail_with(HARM_E_ARG, "bad argument");
   Ctx *x = &h->x;
-  if (x->cool && mode != HARM_FP64) return fail_with(HARM_E_ARG, "the COOL_EOS step runs in FP64");
+  if (x->cool && mode == HARM_MIXED && !x->eos.f32) return fail_with(HARM_E_ARG, "table values span more than float holds");
   if (mode == HARM_MIXED && !x->F1f) {
     const Grid &G = x->G;
     const size_t fb = 8 * G.nc * sizeof(float);

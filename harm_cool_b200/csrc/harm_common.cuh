@@ -190,5 +190,6 @@ struct harm_eos {
   harm::EosDev d;
   double *axes = nullptr;  // xa[nx] then ya[ny]
   double *vals = nullptr;  // [EOS_ND][ntab][nx][ny]
+  float *f32 = nullptr;    // xa32[nx], ya32[ny], e32 and p32 [ntab][nx][ny]
   int device = 0;
 };

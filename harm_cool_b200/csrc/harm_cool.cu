@@ -2,6 +2,8 @@
 // pressure in the face fluxes, wave speeds, source and primtoU, and Utoprim_5d
 // in place of Utoprim_2d and its isentropic fall-backs (step_ch.c:241-300,
 // 437-441).  FP64, built with -fmad=false: the reference's results bit for bit.
+// In mixed precision the face fluxes' and wave speeds' EOS calls interpolate
+// and solve in FP32; the update (source, primtoU, Utoprim_5d) stays FP64.
 //
 // The temperature guess of each zone (_aLastT[SN3][SN1][SN2], cooleos.c:69,
 // 836) lives in Ctx::lastT.  The reference runs its loops one zone after
@@ -42,21 +44,21 @@ __device__ __forceinline__ EosCursor init_cache(const Grid &G, double *lastT, in
   return c;
 }
 
-template <int DIR>
+template <int DIR, bool F32>
 __device__ __forceinline__ void face_flux_cool(const EosDev &E, EosCursor &c, const double *pl, const double *pr,
                                                const Geo &q, double *F, double &ctop, int *fail)
 {
   State s;
   double Fl[8], Ul[8], cmaxl, cminl, cmaxr, cminr;
   get_state(pl, q, s, fail);
-  primtoflux_cool(E, c, pl, s, DIR, q.g, Fl);
-  primtoflux_cool(E, c, pl, s, 0, q.g, Ul);
-  vchar_cool(E, c, pl, s, q, DIR, cmaxl, cminl, fail);
+  primtoflux_cool<F32>(E, c, pl, s, DIR, q.g, Fl);
+  primtoflux_cool<F32>(E, c, pl, s, 0, q.g, Ul);
+  vchar_cool<F32>(E, c, pl, s, q, DIR, cmaxl, cminl, fail);
   get_state(pr, q, s, fail);
   double Fr[8], Ur[8];
-  primtoflux_cool(E, c, pr, s, DIR, q.g, Fr);
-  primtoflux_cool(E, c, pr, s, 0, q.g, Ur);
-  vchar_cool(E, c, pr, s, q, DIR, cmaxr, cminr, fail);
+  primtoflux_cool<F32>(E, c, pr, s, DIR, q.g, Fr);
+  primtoflux_cool<F32>(E, c, pr, s, 0, q.g, Ur);
+  vchar_cool<F32>(E, c, pr, s, q, DIR, cmaxr, cminr, fail);
   double t1 = 0. > cmaxl ? 0. : cmaxl;
   double cmax = fabs(t1 > cmaxr ? t1 : cmaxr);
   double t2 = 0. > -cminl ? 0. : -cminl;
@@ -68,7 +70,7 @@ __device__ __forceinline__ void face_flux_cool(const EosDev &E, EosCursor &c, co
 
 // one face of direction DIR (step_ch.c:407-487); returns the Courant limit of
 // an active face, 1e9 otherwise
-template <int DIR, bool FULL>
+template <int DIR, bool FULL, bool F32>
 __device__ __noinline__ double one_face(const Grid &G, const double *__restrict__ pb, double *__restrict__ F,
                                         const double *__restrict__ geo, const EosDev &E, double *lastT,
                                         DevScalars *sc, int h, int i, int j)
@@ -100,7 +102,7 @@ __device__ __noinline__ double one_face(const Grid &G, const double *__restrict_
   EosCursor cur = init_cache(G, lastT, h, i, j);
   double Fz[8], ctop;
   int fail = 0;
-  face_flux_cool<DIR>(E, cur, pl, pr, q, Fz, ctop, &fail);
+  face_flux_cool<DIR, F32>(E, cur, pl, pr, q, Fz, ctop, &fail);
   lastT[c] = cur.T;
 #pragma unroll
   for (int k = 0; k < 8; k++) F[k * G.nc + c] = Fz[k];
@@ -128,7 +130,7 @@ __device__ __forceinline__ void reduce_dt(DevScalars *sc, int dir, double dtmin)
 }
 
 // one thread per face; face ranges as k_flux's
-template <int DIR, bool FULL>
+template <int DIR, bool FULL, bool F32>
 __global__ void __launch_bounds__(128) k_flux_cool(Grid G, const double *__restrict__ pb, double *__restrict__ F,
                                                    const double *__restrict__ geo, EosDev E, double *lastT,
                                                    DevScalars *sc)
@@ -138,13 +140,14 @@ __global__ void __launch_bounds__(128) k_flux_cool(Grid G, const double *__restr
   const int i = (DIR == 1 ? G.istart : G.istart - 1) + blockIdx.y * blockDim.y + threadIdx.y;
   const int h = blockIdx.z;
   double dtmin = 1.e9;
-  if ((i <= G.istop + 1) && (j <= G.jstop + 1)) dtmin = one_face<DIR, FULL>(G, pb, F, geo, E, lastT, sc, h, i, j);
+  if ((i <= G.istop + 1) && (j <= G.jstop + 1))
+    dtmin = one_face<DIR, FULL, F32>(G, pb, F, geo, E, lastT, sc, h, i, j);
   reduce_dt<FULL>(sc, DIR, dtmin);
 }
 
 // the seeding form: one thread per (phi, r) row, theta faces in the
 // reference's order (j innermost, step_ch.c:407)
-template <int DIR, bool FULL>
+template <int DIR, bool FULL, bool F32>
 __global__ void __launch_bounds__(128) k_flux_cool_rows(Grid G, const double *__restrict__ pb, double *__restrict__ F,
                                                         const double *__restrict__ geo, EosDev E, double *lastT,
                                                         DevScalars *sc)
@@ -155,33 +158,41 @@ __global__ void __launch_bounds__(128) k_flux_cool_rows(Grid G, const double *__
   double dtmin = 1.e9;
   if (i <= G.istop + 1)
     for (int j = (DIR == 2 ? G.jstart : G.jstart - 1); j <= G.jstop + 1; j++)
-      dtmin = fmin(dtmin, one_face<DIR, FULL>(G, pb, F, geo, E, lastT, sc, h, i, j));
+      dtmin = fmin(dtmin, one_face<DIR, FULL, F32>(G, pb, F, geo, E, lastT, sc, h, i, j));
   reduce_dt<FULL>(sc, DIR, dtmin);
 }
 
-template <bool FULL>
-void launch_flux_cool(Ctx *x, const double *pb, bool rows)
+template <bool FULL, bool F32>
+void launch_flux_cool_p(Ctx *x, const double *pb, bool rows)
 {
   const Grid &G = x->G;
   const EosDev &E = x->eos;
   if (rows) {
     const dim3 b(128, 1);
-    k_flux_cool_rows<1, FULL><<<dim3((G.n1 + 1 + 127) / 128, G.n3), b, 0, x->stream>>>(G, pb, x->F1, x->geo, E,
-                                                                                       x->lastT, x->sc);
-    k_flux_cool_rows<2, FULL><<<dim3((G.n1 + 2 + 127) / 128, G.n3), b, 0, x->stream>>>(G, pb, x->F2, x->geo, E,
-                                                                                       x->lastT, x->sc);
+    k_flux_cool_rows<1, FULL, F32><<<dim3((G.n1 + 1 + 127) / 128, G.n3), b, 0, x->stream>>>(G, pb, x->F1, x->geo, E,
+                                                                                            x->lastT, x->sc);
+    k_flux_cool_rows<2, FULL, F32><<<dim3((G.n1 + 2 + 127) / 128, G.n3), b, 0, x->stream>>>(G, pb, x->F2, x->geo, E,
+                                                                                            x->lastT, x->sc);
     if (G.n3 > 1)
-      k_flux_cool_rows<3, FULL><<<dim3((G.n1 + 2 + 127) / 128, G.n3), b, 0, x->stream>>>(G, pb, x->F3, x->geo, E,
-                                                                                         x->lastT, x->sc);
+      k_flux_cool_rows<3, FULL, F32><<<dim3((G.n1 + 2 + 127) / 128, G.n3), b, 0, x->stream>>>(
+          G, pb, x->F3, x->geo, E, x->lastT, x->sc);
     return;
   }
   const dim3 b(x->tbx, x->tby);
   dim3 g1((G.n2 + 2 + b.x - 1) / b.x, (G.n1 + 1 + b.y - 1) / b.y, G.n3);
   dim3 g2((G.n2 + 1 + b.x - 1) / b.x, (G.n1 + 2 + b.y - 1) / b.y, G.n3);
   dim3 g3((G.n2 + 2 + b.x - 1) / b.x, (G.n1 + 2 + b.y - 1) / b.y, G.n3);
-  k_flux_cool<1, FULL><<<g1, b, 0, x->stream>>>(G, pb, x->F1, x->geo, E, x->lastT, x->sc);
-  k_flux_cool<2, FULL><<<g2, b, 0, x->stream>>>(G, pb, x->F2, x->geo, E, x->lastT, x->sc);
-  if (G.n3 > 1) k_flux_cool<3, FULL><<<g3, b, 0, x->stream>>>(G, pb, x->F3, x->geo, E, x->lastT, x->sc);
+  k_flux_cool<1, FULL, F32><<<g1, b, 0, x->stream>>>(G, pb, x->F1, x->geo, E, x->lastT, x->sc);
+  k_flux_cool<2, FULL, F32><<<g2, b, 0, x->stream>>>(G, pb, x->F2, x->geo, E, x->lastT, x->sc);
+  if (G.n3 > 1) k_flux_cool<3, FULL, F32><<<g3, b, 0, x->stream>>>(G, pb, x->F3, x->geo, E, x->lastT, x->sc);
+}
+
+// the face physics' EOS calls in FP32 in mixed precision, FP64 otherwise
+template <bool FULL>
+void launch_flux_cool(Ctx *x, const double *pb, bool rows)
+{
+  if (x->mode == HARM_MIXED) launch_flux_cool_p<FULL, true>(x, pb, rows);
+  else launch_flux_cool_p<FULL, false>(x, pb, rows);
 }
 
 // source() with COOL_EOS (phys.c:165-207)
@@ -374,7 +385,7 @@ extern "C" int harm_set_eos(harm_ctx *h, const harm_eos *eos)
   }
   if (eos->device != x->device) return fail_with(HARM_E_ARG, "EOS tables on another device");
   if (eos->d.ntab != x->G.sn1) return fail_with(HARM_E_ARG, "COOL_EOS needs one table per radial index (N1+4)");
-  if (x->mode != HARM_FP64) return fail_with(HARM_E_ARG, "the COOL_EOS step runs in FP64");
+  if (x->mode == HARM_MIXED && !eos->d.f32) return fail_with(HARM_E_ARG, "table values span more than float holds");
   if (!x->lastT) {
     CK(cudaMalloc(&x->lastT, (size_t)x->G.nc * sizeof(double)));
     CK(cudaMemsetAsync(x->lastT, 0, (size_t)x->G.nc * sizeof(double), x->stream));

@@ -29,7 +29,16 @@ __device__ __forceinline__ void mhd_calc_cool(double r, double u, double P, int 
     mhd[j] = eta * s.ucon[dir] * s.ucov[j] + ptot * (dir == j ? 1. : 0.) - s.bcon[dir] * s.bcov[j];
 }
 
+// the EOS calls of the face physics: FP64 (the reference's arithmetic) or the
+// mixed-precision interpolation
+template <bool F32>
+__device__ __forceinline__ double face_pressure(const EosDev &E, EosCursor &c, double rho, double u)
+{
+  return F32 ? eos_pressure_f(E, c, rho, u) : eos_pressure(E, c, rho, u);
+}
+
 // primtoflux() with COOL_EOS (phys.c:59-96)
+template <bool F32 = false>
 __device__ __forceinline__ void primtoflux_cool(const EosDev &E, EosCursor &c, const double *pr, const State &s,
                                                 int dir, double g, double *flux)
 {
@@ -37,7 +46,7 @@ __device__ __forceinline__ void primtoflux_cool(const EosDev &E, EosCursor &c, c
   flux[RHO] = pr[RHO] * s.ucon[dir];
   {
     const double rho = pr[RHO], u = pr[UU];
-    const double p = eos_pressure(E, c, rho, u);
+    const double p = face_pressure<F32>(E, c, rho, u);
     mhd_calc_cool(rho, u, p, dir, s, mhd);
   }
   flux[UU] = mhd[0] + flux[RHO];
@@ -53,12 +62,13 @@ __device__ __forceinline__ void primtoflux_cool(const EosDev &E, EosCursor &c, c
 
 // vchar() with COOL_EOS and COOL_EOS_SIMPLECS 0 (phys.c:337-476): the sound
 // speed of Ibanez et al. from dp/drho and dp/de; no fail() on the clamps
+template <bool F32 = false>
 __device__ __forceinline__ void vchar_cool(const EosDev &E, EosCursor &c, const double *pr, const State &s,
                                            const Geo &q, int js, double &vmax, double &vmin, int *fail)
 {
   double bsq = dot4(s.bcon, s.bcov);
   double rho = pr[RHO], u = pr[UU];
-  double p = eos_pressure(E, c, rho, u);
+  double p = face_pressure<F32>(E, c, rho, u);
   double EF = rho + u + p;
   double EE = bsq + EF;
   double va2 = bsq / EE;
@@ -66,8 +76,8 @@ __device__ __forceinline__ void vchar_cool(const EosDev &E, EosCursor &c, const 
   {
     double e = u / rho;
     double enthalpy = 1.0 + e + p / rho;
-    double dpdrho = eos_dpdrho(E, c, rho, u);
-    double dpde = eos_dpdu(E, c, rho, u) * rho;
+    double dpdrho = F32 ? eos_dpdrho_f(E, c, rho, u) : eos_dpdrho(E, c, rho, u);
+    double dpde = (F32 ? eos_dpdu_f(E, c, rho, u) : eos_dpdu(E, c, rho, u)) * rho;
     cs2 = (dpdrho + p / rho / rho * dpde) / enthalpy;
   }
   double cms2 = cs2 + va2 - cs2 * va2;

@@ -2,6 +2,7 @@
 // (harm_eos_create, harm_eos_batch).  The tables are the ones the reference
 // builds once per radial index on the host (SetupCache_CoolEOS,
 // cooleos.c:825-992): the caller builds them the same way and hands them over.
+#include <cmath>
 #include <vector>
 
 #include "harm_common.cuh"
@@ -9,8 +10,9 @@
 
 namespace harm {
 
-__global__ void k_eos_batch(EosDev E, int what, long n, const int *__restrict__ tab, const double *__restrict__ rho0,
-                            const double *__restrict__ u, double *__restrict__ lastT, double *__restrict__ out)
+__global__ void k_eos_batch(EosDev E, int what, int f32, long n, const int *__restrict__ tab,
+                            const double *__restrict__ rho0, const double *__restrict__ u, double *__restrict__ lastT,
+                            double *__restrict__ out)
 {
   const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -19,11 +21,36 @@ __global__ void k_eos_batch(EosDev E, int what, long n, const int *__restrict__ 
   c.T = lastT[k];
   c.memo = false;
   double r;
-  if (what == HARM_EOS_PRESSURE) r = eos_pressure(E, c, rho0[k], u[k]);
-  else if (what == HARM_EOS_DPDU) r = eos_dpdu(E, c, rho0[k], u[k]);
-  else r = eos_dpdrho(E, c, rho0[k], u[k]);
+  if (f32) {
+    if (what == HARM_EOS_PRESSURE) r = eos_pressure_f(E, c, rho0[k], u[k]);
+    else if (what == HARM_EOS_DPDU) r = eos_dpdu_f(E, c, rho0[k], u[k]);
+    else r = eos_dpdrho_f(E, c, rho0[k], u[k]);
+  } else {
+    if (what == HARM_EOS_PRESSURE) r = eos_pressure(E, c, rho0[k], u[k]);
+    else if (what == HARM_EOS_DPDU) r = eos_dpdu(E, c, rho0[k], u[k]);
+    else r = eos_dpdrho(E, c, rho0[k], u[k]);
+  }
   out[k] = r;
   lastT[k] = c.T;
+}
+
+// the power of two that centres a plane's magnitudes (log scale) in the float
+// range; 0 when they span more than float can hold
+static double f32_scale(const std::vector<double> &v, size_t off, size_t n)
+{
+  double lo = 0., hi = 0.;
+  for (size_t k = 0; k < n; k++) {
+    double a = fabs(v[off + k]);
+    if (!(a < 1e308)) return 0.;
+    if (a > 0. && (lo == 0. || a < lo)) lo = a;
+    if (a > hi) hi = a;
+  }
+  if (hi == 0.) return 1.;
+  int elo, ehi;
+  frexp(lo, &elo);
+  frexp(hi, &ehi);
+  if (ehi - elo > 240) return 0.;
+  return ldexp(1.0, -(elo + ehi) / 2);
 }
 
 }  // namespace harm
@@ -61,13 +88,37 @@ extern "C" int harm_eos_create(const harm_eos_desc *dsc, const double *xaxis, co
   if (err == cudaSuccess) err = cudaMemcpy(e->axes, xaxis, nx * sizeof(double), cudaMemcpyHostToDevice);
   if (err == cudaSuccess) err = cudaMemcpy(e->axes + nx, yaxis, ny * sizeof(double), cudaMemcpyHostToDevice);
   if (err == cudaSuccess) err = cudaMemcpy(e->vals, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice);
+  // float copies of the axes and of the e and p planes, scaled into range
+  const size_t np = (size_t)nt * plane;
+  const double se = harm::f32_scale(v, (size_t)harm::EOS_E * np, np);
+  const double sp = harm::f32_scale(v, (size_t)harm::EOS_P * np, np);
+  const bool f32 = se > 0. && sp > 0.;
+  if (f32 && err == cudaSuccess) {
+    std::vector<float> f(nx + ny + 2 * np);
+    for (long k = 0; k < nx; k++) f[k] = (float)xaxis[k];
+    for (long k = 0; k < ny; k++) f[nx + k] = (float)yaxis[k];
+    for (size_t k = 0; k < np; k++) {
+      f[nx + ny + k] = (float)(v[(size_t)harm::EOS_E * np + k] * se);
+      f[nx + ny + np + k] = (float)(v[(size_t)harm::EOS_P * np + k] * sp);
+    }
+    err = cudaMalloc(&e->f32, f.size() * sizeof(float));
+    if (err == cudaSuccess) err = cudaMemcpy(e->f32, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice);
+  }
   if (err != cudaSuccess) {
     cudaFree(e->axes);
     cudaFree(e->vals);
+    cudaFree(e->f32);
     delete e;
     return fail_with(HARM_E_CUDA, std::string("EOS tables: ") + cudaGetErrorString(err));
   }
   harm::EosDev &d = e->d;
+  d.f32 = f32 ? 1 : 0;
+  d.xa32 = f32 ? e->f32 : nullptr;
+  d.ya32 = f32 ? e->f32 + nx : nullptr;
+  d.e32 = f32 ? e->f32 + nx + ny : nullptr;
+  d.p32 = f32 ? e->f32 + nx + ny + np : nullptr;
+  d.se = se;
+  d.sp = sp;
   d.nx = dsc->nx;
   d.ny = dsc->ny;
   d.ntab = dsc->ntab;
@@ -95,16 +146,19 @@ extern "C" int harm_eos_destroy(harm_eos *e)
   if (!e) return HARM_OK;
   cudaFree(e->axes);
   cudaFree(e->vals);
+  cudaFree(e->f32);
   delete e;
   return HARM_OK;
 }
 
-extern "C" int harm_eos_batch(harm_eos *e, int what, long n, const int *tab, const double *rho0, const double *u,
-                              double *lastT, double *out)
+extern "C" int harm_eos_batch(harm_eos *e, int what, int precision, long n, const int *tab, const double *rho0,
+                              const double *u, double *lastT, double *out)
 {
   if (!e || !tab || !rho0 || !u || !lastT || !out || n < 0) return fail_with(HARM_E_ARG, "null argument");
   if (what != HARM_EOS_PRESSURE && what != HARM_EOS_DPDU && what != HARM_EOS_DPDRHO)
     return fail_with(HARM_E_ARG, "unknown EOS quantity");
+  if (precision != HARM_FP64 && precision != HARM_MIXED) return fail_with(HARM_E_ARG, "bad precision");
+  if (precision == HARM_MIXED && !e->d.f32) return fail_with(HARM_E_ARG, "table values span more than float holds");
   for (long k = 0; k < n; k++)
     if (tab[k] < 0 || tab[k] >= e->d.ntab) return fail_with(HARM_E_ARG, "table index out of range");
   if (n == 0) return HARM_OK;
@@ -122,7 +176,8 @@ extern "C" int harm_eos_batch(harm_eos *e, int what, long n, const int *tab, con
   CK(cudaMemcpy(B.r, rho0, n * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(B.uu, u, n * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(B.T, lastT, n * sizeof(double), cudaMemcpyHostToDevice));
-  harm::k_eos_batch<<<(unsigned)((n + 127) / 128), 128>>>(e->d, what, n, B.t, B.r, B.uu, B.T, B.o);
+  harm::k_eos_batch<<<(unsigned)((n + 127) / 128), 128>>>(e->d, what, precision == HARM_MIXED, n, B.t, B.r, B.uu,
+                                                           B.T, B.o);
   CK(cudaGetLastError());
   CK(cudaMemcpy(out, B.o, n * sizeof(double), cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(lastT, B.T, n * sizeof(double), cudaMemcpyDeviceToHost));

@@ -36,12 +36,18 @@ struct EosDev {
   const double *val;       // [EOS_ND][ntab][nx][ny]
   double rho_unit, u_unit, p_unit, kbol, mav, cl;
   double rho_min, rho_max, t_min, t_max, hh, gam;
+  // FP32 copies for the mixed-precision interpolation: axes, and e and p
+  // scaled by powers of two (se, sp) into the float range; f32 = 0 when the
+  // tables do not fit
+  int f32;
+  const float *xa32, *ya32, *e32, *p32;  // [ntab][nx][ny] each
+  double se, sp;
 };
 
 struct EosCursor {
   int tab;          // radial index of the table (cacheT[i])
   double T;         // the zone's temperature guess (*LastT)
-  bool memo;
+  bool memo, m_f32;
   double m_rho, m_u, m_p, m_T;
 };
 
@@ -228,7 +234,8 @@ static __device__ __noinline__ double eos_newton_T(const EosDev &E, int tab, dou
 // pressure_rho0_u_CoolEOS (cooleos.c:314-444) with the guess in c.T
 static __device__ __noinline__ double eos_pressure(const EosDev &E, EosCursor &c, double rho0, double u)
 {
-  if (c.memo && same_bits(rho0, c.m_rho) && same_bits(u, c.m_u) && same_bits(c.T, c.m_T)) return c.m_p;
+  if (c.memo && !c.m_f32 && same_bits(rho0, c.m_rho) && same_bits(u, c.m_u) && same_bits(c.T, c.m_T))
+    return c.m_p;
   const double rho = rho0 * E.rho_unit;
   const double e = u * E.u_unit;
   const double hh = E.hh;
@@ -259,6 +266,7 @@ static __device__ __noinline__ double eos_pressure(const EosDev &E, EosCursor &c
     }
   }
   c.memo = true;
+  c.m_f32 = false;
   c.m_rho = rho0;
   c.m_u = u;
   c.m_p = p;
@@ -298,6 +306,223 @@ __device__ __forceinline__ double eos_dpdrho(const EosDev &E, EosCursor &c, doub
   const double pP = eos_pressure(E, c, rhoP, u);
   const double pM = eos_pressure(E, c, rhoM, u);
   return (pP - pM) / (h);
+}
+
+// ---------------------------------------------------------------------------
+// Mixed precision: the same solve with the tables, the Akima windows and the
+// Newton iteration in float.  Differences from the FP64 path, all within its
+// 1e-6 solve tolerance: e and p are scaled by powers of two into the float
+// range; an Akima node derivative is formed as a weighted mean (the FP64
+// form's products overflow float); the T-derivative of e is the derivative of
+// the interpolating cubic instead of spline_akima_der's central difference,
+// which float cannot resolve at h = T * 1e-6.  The branches (table range,
+// e < 0) and the gamma-law fall-backs are the FP64 path's, and a solve that
+// float cannot bring to the tolerance is redone in FP64, so that a zone falls
+// back to the gamma law only where the FP64 path does (but for solves that
+// FP64 fails and float passes).
+
+__device__ __forceinline__ void eos_window_f(int n, const float *__restrict__ x, float v, int &lo, int &cnt)
+{
+  int a = 1, b = n - 1;
+  while (a < b) {
+    int m = (a + b) >> 1;
+    if (v < __ldg(x + m)) b = m;
+    else a = m + 1;
+  }
+  int l0 = a - 2, r0 = a + 1;
+  if (l0 < 0) l0 = 0;
+  if (r0 >= n) r0 = n - 1;
+  lo = l0;
+  cnt = r0 - l0 + 1;
+}
+
+__device__ __forceinline__ float akima_node_f(float t0, float t1, float t2, float t3)
+{
+  const float d0 = fabsf(t3 - t2), d1 = fabsf(t1 - t0);
+  const float s = d0 + d1;
+  if (!(s >= 1e-30f)) return 0.5f * (t1 + t2);
+  const float w = __fdividef(d0, s);
+  return __fmaf_rn(w, t1 - t2, t2);
+}
+
+template <int SI>
+__device__ __forceinline__ void akima_slopes_f(const float *x, const float *y, float *mm)
+{
+#pragma unroll
+  for (int k = 0; k < SI - 1; k++) mm[k + 2] = __fdividef(y[k + 1] - y[k], x[k + 1] - x[k]);
+  const float xl1 = x[0] + x[1] - x[2];
+  const float xl0 = xl1 + x[0] - x[1];
+  const float yl1 = __fmaf_rn(x[0] - xl1, mm[3] - 2.f * mm[2], y[0]);
+  mm[1] = __fdividef(y[0] - yl1, x[0] - xl1);
+  const float yl0 = __fmaf_rn(xl1 - xl0, mm[2] - 2.f * mm[1], yl1);
+  mm[0] = __fdividef(yl1 - yl0, xl1 - xl0);
+  const float xr2 = x[SI - 1] + x[SI - 2] - x[SI - 3];
+  const float xr3 = xr2 + x[SI - 1] - x[SI - 2];
+  const float yr2 = __fmaf_rn(2.f * mm[SI] - mm[SI - 1], xr2 - x[SI - 1], y[SI - 1]);
+  mm[SI + 1] = __fdividef(yr2 - y[SI - 1], xr2 - x[SI - 1]);
+  const float yr3 = __fmaf_rn(2.f * mm[SI + 1] - mm[SI], xr3 - xr2, yr2);
+  mm[SI + 2] = __fdividef(yr3 - yr2, xr3 - xr2);
+}
+
+// value (and with DER the derivative) of the cubic of the interval t falls in
+template <int SI, bool DER>
+__device__ __forceinline__ void akima_window_f(const float *x, const float *y, float t, float &v, float &dv)
+{
+  float mm[SI + 3];
+  akima_slopes_f<SI>(x, y, mm);
+  int i = (t > x[1]) ? 1 : 0;
+  if (SI == 4 && t > x[2]) i = 2;
+  float xi = x[0], xi1 = x[1], yi = y[0], yi1 = y[1];
+  float a0 = mm[0], a1 = mm[1], a2 = mm[2], a3 = mm[3], a4 = mm[4];
+  if (i >= 1) { xi = x[1]; xi1 = x[2]; yi = y[1]; yi1 = y[2]; a0 = mm[1]; a1 = mm[2]; a2 = mm[3]; a3 = mm[4]; a4 = mm[5]; }
+  if (SI == 4 && i >= 2) { xi = x[2]; xi1 = x[3]; yi = y[2]; yi1 = y[3]; a0 = mm[2]; a1 = mm[3]; a2 = mm[4]; a3 = mm[5]; a4 = mm[6]; }
+  const float si = akima_node_f(a0, a1, a2, a3), si1 = akima_node_f(a1, a2, a3, a4);
+  const float d0 = xi1 - xi;
+  const float rd = __fdividef(1.f, d0);
+  const float t2 = (yi1 - yi) * rd;
+  const float c1 = (3.f * t2 - 2.f * si - si1) * rd;
+  const float c2 = (si + si1 - 2.f * t2) * rd * rd;
+  const float u = t - xi;
+  v = __fmaf_rn(__fmaf_rn(__fmaf_rn(c2, u, c1), u, si), u, yi);
+  if (DER) dv = __fmaf_rn(__fmaf_rn(3.f * c2, u, 2.f * c1), u, si);
+}
+
+template <int SX, int SY, bool DER>
+__device__ __noinline__ void eos_value_wf(const EosDev &E, const float *__restrict__ plane, int x0, int y0, float rho,
+                                          float T, float &val, float &der)
+{
+  float xw[SX], yw[SY], row[SX], rowd[SX];
+#pragma unroll
+  for (int k = 0; k < SX; k++) xw[k] = __ldg(E.xa32 + x0 + k);
+#pragma unroll
+  for (int k = 0; k < SY; k++) yw[k] = __ldg(E.ya32 + y0 + k);
+#pragma unroll
+  for (int r = 0; r < SX; r++) {
+    const float *src = plane + (long)(x0 + r) * E.ny + y0;
+    float ys[SY];
+#pragma unroll
+    for (int k = 0; k < SY; k++) ys[k] = __ldg(src + k);
+    float d = 0.f;
+    akima_window_f<SY, DER>(yw, ys, T, row[r], d);
+    rowd[r] = d;
+  }
+  float unused;
+  akima_window_f<SX, false>(xw, row, rho, val, unused);
+  if (DER) akima_window_f<SX, false>(xw, rowd, rho, der, unused);
+}
+
+template <bool DER>
+__device__ __forceinline__ bool eos_value_f(const EosDev &E, int tab, const float *planes, float rho, int x0, int sx,
+                                            float T, float &val, float &der)
+{
+  if (!(T >= __ldg(E.ya32)) || !(T <= __ldg(E.ya32 + E.ny - 1))) return false;
+  int y0, sy;
+  eos_window_f(E.ny, E.ya32, T, y0, sy);
+  const float *plane = planes + (long)tab * E.nx * E.ny;
+  if (sx == 4) {
+    if (sy == 4) eos_value_wf<4, 4, DER>(E, plane, x0, y0, rho, T, val, der);
+    else eos_value_wf<4, 3, DER>(E, plane, x0, y0, rho, T, val, der);
+  } else {
+    if (sy == 4) eos_value_wf<3, 4, DER>(E, plane, x0, y0, rho, T, val, der);
+    else eos_value_wf<3, 3, DER>(E, plane, x0, y0, rho, T, val, der);
+  }
+  return true;
+}
+
+// mnewtc<1>'s iteration in float; returns berr
+static __device__ __noinline__ float eos_newton_T_f(const EosDev &E, int tab, float rho, bool rho_in, int x0, int sx,
+                                                    float e, float &x, float minx, float maxx)
+{
+  float best = x, besterr = 1.0e30f;
+  for (int k = 1; k <= 300; k++) {
+    float ecur = CUDART_NAN_F, dcur = CUDART_NAN_F;
+    if (rho_in) {
+      float v, dv;
+      if (eos_value_f<true>(E, tab, E.e32, rho, x0, sx, x, v, dv)) { ecur = v; dcur = dv; }
+    }
+    const float re = __fdividef(1.f, e);
+    const float F = (e - ecur) * re;
+    const float D = -dcur * re;
+    float bet = -F;
+    const float errf = fabsf(bet);
+    if (errf <= 1.0e-6f) return errf;
+    if (errf < besterr) { besterr = errf; best = x; }
+    if (fabsf(D) > 0.f) bet = bet / D;
+    const float nv = x + bet;
+    if (nv >= minx && nv <= maxx && nv != x) x = nv;
+    else break;
+  }
+  x = best;
+  return besterr;
+}
+
+// pressure_rho0_u_CoolEOS with the interpolation and the solve in float
+static __device__ __noinline__ double eos_pressure_f(const EosDev &E, EosCursor &c, double rho0, double u)
+{
+  if (c.memo && c.m_f32 && same_bits(rho0, c.m_rho) && same_bits(u, c.m_u) && same_bits(c.T, c.m_T)) return c.m_p;
+  const double rho = rho0 * E.rho_unit;
+  const double e = u * E.u_unit;
+  const double hh = E.hh;
+  double p;
+  if (c.T == 0.0) {
+    c.T = (E.gam - 1.) * u / rho0 / E.kbol * E.mav * E.cl * E.cl;
+    if (c.T < E.t_min * (1.0 + hh)) c.T = E.t_min * (1.0 + hh);
+  }
+  if (rho < E.rho_min) p = (E.gam - 1.) * u;
+  else if (rho > E.rho_max) p = (E.gam - 1.) * u;
+  else if (e < 0.0) p = 0.0;
+  else {
+    const float minx = (float)(E.t_min * (1.0 + hh)), maxx = (float)(E.t_max * (1.0 - hh));
+    const float rf = (float)rho;
+    int x0 = 0, sx = 4;
+    bool rho_in = rf >= __ldg(E.xa32) && rf <= __ldg(E.xa32 + E.nx - 1);
+    if (rho_in) eos_window_f(E.nx, E.xa32, rf, x0, sx);
+    float x = (float)c.T;
+    const float berr = eos_newton_T_f(E, c.tab, rf, rho_in, x0, sx, (float)(e * E.se), x, minx, maxx);
+    if (!(berr <= 1.0e-6f)) {
+      // float could not reach the tolerance: the FP64 solve decides, so the
+      // table-or-gamma-law branch is the FP64 path's
+      p = eos_pressure(E, c, rho0, u);
+    } else {
+      float v = CUDART_NAN_F, unused;
+      if (rho_in) {
+        float w;
+        if (eos_value_f<false>(E, c.tab, E.p32, rf, x0, sx, x, w, unused)) v = w;
+      }
+      c.T = (double)x;
+      p = (double)v / E.sp / E.p_unit;
+    }
+  }
+  c.memo = true;
+  c.m_f32 = true;
+  c.m_rho = rho0;
+  c.m_u = u;
+  c.m_p = p;
+  c.m_T = c.T;
+  return p;
+}
+
+// dpdu_calc_CoolEOS and dpdrho_calc_CoolEOS over the float solve
+__device__ __forceinline__ double eos_dpdu_f(const EosDev &E, EosCursor &c, double rho0, double u)
+{
+  const double h = u * E.hh / E.u_unit;
+  const double uP = u + h;
+  double uM = u - h;
+  if (uM > 0) return (eos_pressure_f(E, c, rho0, uP) - eos_pressure_f(E, c, rho0, uM)) / (2.0 * h);
+  uM = u;
+  const double pP = eos_pressure_f(E, c, rho0, uP);
+  return (pP - eos_pressure_f(E, c, rho0, uM)) / (h);
+}
+
+__device__ __forceinline__ double eos_dpdrho_f(const EosDev &E, EosCursor &c, double rho0, double u)
+{
+  const double h = rho0 * E.hh / E.rho_unit;
+  const double rhoP = rho0 + h;
+  double rhoM = rho0 - h;
+  if (rhoM > 0) return (eos_pressure_f(E, c, rhoP, u) - eos_pressure_f(E, c, rhoM, u)) / (2.0 * h);
+  rhoM = rho0;
+  const double pP = eos_pressure_f(E, c, rhoP, u);
+  return (pP - eos_pressure_f(E, c, rhoM, u)) / (h);
 }
 
 }  // namespace harm

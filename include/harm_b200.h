@@ -312,10 +312,13 @@ int harm_eos_destroy(harm_eos *eos);
    dpdrho_calc_CoolEOS (cooleos.c:667-741) for n independent entries, each with
    its table index tab[k] and its temperature guess lastT[k] (the zone's *LastT
    after InitCache_CoolEOS, cooleos.c:770-807; 0 = none yet), updated in place.
-   Host arrays; out[k] receives the value. */
+   Host arrays; out[k] receives the value.  precision HARM_FP64: the reference's
+   arithmetic, bit for bit; HARM_MIXED: the tables, the interpolation and the T
+   solve in FP32 (same branches and fall-backs; HARM_E_ARG when the tables'
+   values span more than FP32 holds). */
 enum { HARM_EOS_PRESSURE = 0, HARM_EOS_DPDU = 1, HARM_EOS_DPDRHO = 2 };
-int harm_eos_batch(harm_eos *eos, int what, long n, const int *tab, const double *rho0,
-                   const double *u, double *lastT, double *out);
+int harm_eos_batch(harm_eos *eos, int what, int precision, long n, const int *tab,
+                   const double *rho0, const double *u, double *lastT, double *out);
 
 /* Utoprim_5d() (utoprim_5d.c:179-245, the COOL_EOS inversion) over n
    independent zones: U, gcov, gcon, gdet, prim as harm_utoprim_2d_batch, tab[n]
@@ -329,7 +332,9 @@ int harm_utoprim_5d_batch(const harm_eos *eos, const double *U, const double *gc
    the fluxes, wave speeds, source and primtoU, and Utoprim_5d as the
    inversion (step_ch.c:241-300, 437-441).  The tables must have ntab = N1+4,
    table t serving radial index t, and must outlive the attachment; NULL
-   detaches them (back to the gamma-law step).  FP64 only.  The context keeps
+   detaches them (back to the gamma-law step).  With HARM_MIXED the face
+   fluxes' and wave speeds' EOS calls run in FP32 (see harm_eos_batch), the
+   update stays FP64.  The context keeps
    the per-zone temperature guesses _aLastT (cooleos.c:69, 836), all unset at
    first, as the reference's calloc leaves them. */
 int harm_set_eos(harm_ctx *ctx, const harm_eos *eos);

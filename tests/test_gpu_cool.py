@@ -135,7 +135,7 @@ def test_cool_context_rules(hc, fx, eos):
     ctx.init_torus()
     ctx.set_eos(eos)
     with pytest.raises(hc.HarmError):
-        ctx.set_precision(hc.Context.MIXED)
+        ctx.autotune_tile(steps=1)      # the tile autotuner times the gamma-law step
     small = hc.Context(hc.torus_problem(16, 16, 1))
     with pytest.raises(hc.HarmError):
         small.set_eos(eos)      # 20 radial indices, 36 tables
@@ -144,3 +144,32 @@ def test_cool_context_rules(hc, fx, eos):
     assert ctx.diag()["fail_code"] == 0
     small.close()
     ctx.close()
+
+
+def test_cool_mixed_tracks_fp64(hc, eos):
+    """The COOL_EOS step with the face physics' EOS calls in FP32 against the FP64
+    COOL_EOS step: density L1 within 1e-4 after 300 steps of a 64x64 torus."""
+    from harm_cool_b200 import eos_tables
+    pr = hc.torus_problem(64, 64, 1, a=0.6, rin=4.0, rmax=11.8, beta=50.0)
+    xa, ya, val, consts = eos_tables.build_tables(eos_tables.zone_radii(pr), gam=pr.params.gam)
+    E = hc.Eos(xa, ya, val, consts)
+    a = hc.Context(pr)
+    a.init_torus()
+    a.set_eos(E)
+    b = hc.Context(pr)
+    b.init_torus()
+    b.set_precision(hc.Context.MIXED)
+    b.set_eos(E)
+    for n in (1, 300):
+        a.run(n if n == 1 else n - 1)
+        b.run(n if n == 1 else n - 1)
+    pa, pb = a.get_prims(), b.get_prims()
+    assert np.all(np.isfinite(pb))
+    from helpers import l1_groups, l1_rel
+    l1 = l1_rel(pb, pa)
+    print("COOL_EOS mixed vs FP64, 64x64, 300 steps:", l1_groups(pb, pa))
+    assert l1[0] <= 1e-4, l1
+    assert b.diag()["fail_code"] == 0
+    a.close()
+    b.close()
+    E.close()

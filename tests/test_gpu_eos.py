@@ -84,3 +84,37 @@ def test_device_eos_rejects_bad_tables(harm_lib, tables):
     with pytest.raises(hc.HarmError):
         e.batch("pressure", [T.ntab], [1.0], [1.0], [0.0])
     e.close()
+
+
+# mixed precision: tables, Akima windows and the T solve in FP32, against the
+# FP64 oracle from the same guesses.  Both solves stop at a residual of 1e-6 in
+# e, so the FP64 pressure itself depends on its starting guess at about that
+# level; the FP32 pressure is held to 2e-5 relative where both solved from the
+# table.
+P32_TOL = 2e-5
+
+
+def test_device_eos_fp32_against_fp64_oracle(dev, tables):
+    from oracle.pyoracle import OracleEos
+    from golden.make_golden import eos_inputs
+    T, _ = tables
+    O = OracleEos(T)
+    tab, rho0, u, lastT = eos_inputs(np.random.default_rng(21), T.ntab, 50000)
+    a, la = dev.batch("pressure", tab, rho0, u, lastT, mixed=True)
+    b, lb = O.batch("pressure", tab, rho0, u, lastT)
+    gam = T.consts["gam"]
+    gl_a = a == (gam - 1.) * u
+    gl_b = b == (gam - 1.) * u
+    both = ~gl_a & ~gl_b & (u > 0)
+    rel = np.abs(a[both] / b[both] - 1.)
+    print("FP32 EOS: %d table solves, max rel %.2e, median %.2e; branch agreement %.5f"
+          % (both.sum(), rel.max(), np.median(rel), np.mean(gl_a == gl_b)))
+    assert both.sum() > 20000
+    assert rel.max() <= P32_TOL
+    # the fall-backs (outside the table, e < 0) are the FP64 path's, exactly
+    out = (rho0 * T.consts["rho_unit"] < T.consts["rho_min"]) | (rho0 * T.consts["rho_unit"] > T.consts["rho_max"])
+    assert np.array_equal(a[out], b[out])
+    assert np.mean(gl_a == gl_b) > 0.99
+    # the temperatures agree to the solve tolerance
+    trel = np.abs(la[both] / lb[both] - 1.)
+    assert trel.max() <= 1e-4, trel.max()
