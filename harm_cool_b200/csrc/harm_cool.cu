@@ -21,6 +21,18 @@
 // face.
 #define HARM_VARIANT cool
 #define HARM_STEP_MIXED 0
+// resident blocks of 128 threads per SM that the COOL_EOS kernels' register
+// budgets must allow (measured on a B200: 3 for the faces, 168 registers, is
+// 3 % faster than 1; the update kernels lose with more than 1)
+#ifndef HARM_COOL_FLUX_MINB
+#define HARM_COOL_FLUX_MINB 3
+#endif
+#ifndef HARM_COOL_CONS_MINB
+#define HARM_COOL_CONS_MINB 1
+#endif
+#ifndef HARM_COOL_INV_MINB
+#define HARM_COOL_INV_MINB 1
+#endif
 #define HARM_FLUX_MINB 1
 #define HARM_CONS_MINB 1
 #define HARM_INV_MINB 1
@@ -131,7 +143,7 @@ __device__ __forceinline__ void reduce_dt(DevScalars *sc, int dir, double dtmin)
 
 // one thread per face; face ranges as k_flux's
 template <int DIR, bool FULL, bool F32>
-__global__ void __launch_bounds__(128) k_flux_cool(Grid G, const double *__restrict__ pb, double *__restrict__ F,
+__global__ void __launch_bounds__(128, HARM_COOL_FLUX_MINB) k_flux_cool(Grid G, const double *__restrict__ pb, double *__restrict__ F,
                                                    const double *__restrict__ geo, EosDev E, double *lastT,
                                                    DevScalars *sc)
 {
@@ -224,7 +236,7 @@ __device__ __noinline__ void source_cool(const EosDev &E, EosCursor &c, const do
 // the update's first half (step_ch.c:241-263): source(pb), primtoU(pi) and the
 // flux divergence, with flux-CT and the flux boundary fixes, into Ub
 template <bool FULL, bool THREE_D>
-__global__ void __launch_bounds__(128) k_cons_cool(Grid G, const double *__restrict__ pi, const double *__restrict__ pb,
+__global__ void __launch_bounds__(128, HARM_COOL_CONS_MINB) k_cons_cool(Grid G, const double *__restrict__ pi, const double *__restrict__ pb,
                                                    const double *__restrict__ F1, const double *__restrict__ F2,
                                                    const double *__restrict__ F3, const double *__restrict__ geo,
                                                    const double *__restrict__ conn, EosDev E, double *lastT,
@@ -279,7 +291,7 @@ __global__ void __launch_bounds__(128) k_cons_cool(Grid G, const double *__restr
 
 // the update's second half (step_ch.c:265-268) and fixup() (fixup.c:51-60):
 // Utoprim_5d from the guess pi, no isentropic fall-backs under COOL_EOS
-__global__ void __launch_bounds__(128) k_invert_cool(Grid G, const double *__restrict__ pi,
+__global__ void __launch_bounds__(128, HARM_COOL_INV_MINB) k_invert_cool(Grid G, const double *__restrict__ pi,
                                                      const double *__restrict__ Ub, double *__restrict__ pf,
                                                      signed char *__restrict__ pflag, const double *__restrict__ geo,
                                                      const double *__restrict__ floors, EosDev E, double *lastT,

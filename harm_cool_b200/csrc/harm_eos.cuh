@@ -116,9 +116,19 @@ __device__ __forceinline__ int akima_interval(const double *x, double t)
   return i;
 }
 
-// the cubic of interval i evaluated at t (akima.c:115-158)
+// the cubic of interval i (akima.c:115-135): its left node, value, slope and
+// the two higher coefficients
+struct AkimaCubic {
+  double xi, yi, si, c1, c2;
+  __device__ __forceinline__ double at(double t) const
+  {
+    const double u = t - xi;
+    return yi + si * u + c1 * u * u + c2 * u * u * u;
+  }
+};
+
 template <int SI>
-__device__ __forceinline__ double akima_at(const double *x, const double *y, const double *mm, int i, double t)
+__device__ __forceinline__ AkimaCubic akima_cubic(const double *x, const double *y, const double *mm, int i)
 {
   double xi = x[0], xi1 = x[1], yi = y[0], yi1 = y[1];
   double a0 = mm[0], a1 = mm[1], a2 = mm[2], a3 = mm[3], a4 = mm[4];
@@ -128,25 +138,32 @@ __device__ __forceinline__ double akima_at(const double *x, const double *y, con
   const double d0 = xi1 - xi;
   const double d1 = yi1 - yi;
   const double t2 = d1 / d0;
-  const double c1 = (3.0 * t2 - 2.0 * si - si1) / d0;
-  const double c2 = (si + si1 - 2.0 * t2) / (d0 * d0);
-  const double u = t - xi;
-  return yi + si * u + c1 * u * u + c2 * u * u * u;
+  AkimaCubic c;
+  c.xi = xi;
+  c.yi = yi;
+  c.si = si;
+  c.c1 = (3.0 * t2 - 2.0 * si - si1) / d0;
+  c.c2 = (si + si1 - 2.0 * t2) / (d0 * d0);
+  return c;
 }
 
-// one Akima window: the value at t, and with DER the central difference of
-// spline_akima_der (h = t * 1e-6)
+// one Akima window: the value at t (akima.c:137-158), and with DER the central
+// difference of spline_akima_der (h = t * 1e-6).  Points that fall in the same
+// interval share its cubic, formed once.
 template <int SI, bool DER>
 __device__ __forceinline__ void akima_window(const double *x, const double *y, double t, double &v, double &dv)
 {
   double mm[SI + 3];
   akima_slopes<SI>(x, y, mm);
-  v = akima_at<SI>(x, y, mm, akima_interval<SI>(x, t), t);
+  const int i = akima_interval<SI>(x, t);
+  const AkimaCubic c = akima_cubic<SI>(x, y, mm, i);
+  v = c.at(t);
   if (DER) {
     const double h = t * 1.0E-6;
     const double tm = t - h, tp = t + h;
-    const double vm = akima_at<SI>(x, y, mm, akima_interval<SI>(x, tm), tm);
-    const double vp = akima_at<SI>(x, y, mm, akima_interval<SI>(x, tp), tp);
+    const int im = akima_interval<SI>(x, tm), ip = akima_interval<SI>(x, tp);
+    const double vm = im == i ? c.at(tm) : akima_cubic<SI>(x, y, mm, im).at(tm);
+    const double vp = ip == i ? c.at(tp) : akima_cubic<SI>(x, y, mm, ip).at(tp);
     dv = (vp - vm) / (2.0 * h);
   }
 }
