@@ -4,7 +4,8 @@
 // round.  Layout: the header (restart.c:103-136: ints as "%10d", doubles as
 // "%32.22e", which prints 23 significant digits and so round-trips every
 // double), a newline, every cell of p[SN3][SN1][SN2][8] one line per cell,
-// the size of ener.out, and, when tracers exist, the tracer section.
+// the size of ener.out, when tracers exist the tracer section, and with COOL_EOS
+// every zone's temperature guess.
 //
 // The reference's phi ghost planes hold whatever its last MPI exchange left
 // there; they are never read before the next exchange refills them.  This
@@ -12,6 +13,7 @@
 // file sizes (the reference stats its tracer files) are written as 0: this
 // library keeps no tracer files.
 #include <cstdio>
+#include <string>
 #include <vector>
 
 #include "harm_common.cuh"
@@ -150,6 +152,14 @@ extern "C" int harm_restart_write(harm_ctx *h, const harm_restart_header *hdr, c
       fprintf(f, FI, 0);
     }
   }
+  // COOL_EOS: every zone's temperature guess, _aLastT[SN3][SN1][SN2]
+  // (restart_write_CoolEOS, cooleos.c:996-1013)
+  if (x->cool) {
+    std::vector<double> T(d.cells());
+    rc = harm_get_eos_guess(h, T.data());
+    if (rc) return rc;
+    for (double v : T) fprintf(f, FD, v);
+  }
   if (ferror(f)) return fail_with(HARM_E_ARG, std::string("write error on ") + path);
   return HARM_OK;
 }
@@ -220,26 +230,48 @@ extern "C" int harm_restart_read(harm_ctx *h, const char *path, const harm_grid_
   if (rc) return rc;
   rc = harm_set_mass(h, r.mass_in, r.mass_out);
   if (rc) return rc;
-  // tracers, when the file has them (restart_read_tracers, tracers.c:608-652)
-  double tr[8];
-  int cnt = 0, got = 0;
-  for (int k = 0; k < 8; k++) got += fscanf(f, "%lf", &tr[k]) == 1;
-  if (got == 8 && fscanf(f, "%d", &cnt) == 1 && cnt >= 0) {
+  // the tail: the tracer section when the file has one (restart_read_tracers,
+  // tracers.c:608-652), then for a COOL_EOS context the zones' temperature
+  // guesses (restart_read_CoolEOS, cooleos.c:1018-1030)
+  std::vector<std::string> tok;
+  {
+    char buf[128];
+    while (fscanf(f, "%127s", buf) == 1) tok.push_back(buf);
+  }
+  const size_t nguess = x->cool ? (size_t)d.cells() : 0;
+  if (tok.size() < nguess) return fail_with(HARM_E_ARG, "truncated COOL_EOS section");
+  const size_t ntr_tok = tok.size() - nguess;
+  if (ntr_tok > 0) {
+    size_t k = 0;
+    auto next_d = [&](double &v) { return k < ntr_tok && sscanf(tok[k++].c_str(), "%lf", &v) == 1; };
+    auto next_i = [&](int &v) { return k < ntr_tok && sscanf(tok[k++].c_str(), "%d", &v) == 1; };
+    double tr;
+    int cnt = 0;
+    ok = true;
+    for (int m = 0; m < 8; m++) ok &= next_d(tr);
+    ok &= next_i(cnt) && cnt >= 0;
+    if (!ok) return fail_with(HARM_E_ARG, "truncated tracer section");
     if (!g) return fail_with(HARM_E_ARG, "restart file has tracers: pass the grid spec");
     std::vector<int> ids(3 * (size_t)cnt);
     std::vector<double> X(3 * (size_t)cnt);
-    for (int k = 0; k < cnt; k++) {
+    for (int m = 0; m < cnt; m++) {
       double x0;
       int size;
-      ok = fscanf(f, "%d %d %d", &ids[3 * k], &ids[3 * k + 1], &ids[3 * k + 2]) == 3;
-      ok &= fscanf(f, "%lf %lf %lf %lf", &x0, &X[3 * k], &X[3 * k + 1], &X[3 * k + 2]) == 4;
-      ok &= fscanf(f, "%d", &size) == 1;
+      ok = next_i(ids[3 * m]) && next_i(ids[3 * m + 1]) && next_i(ids[3 * m + 2]);
+      ok = ok && next_d(x0) && next_d(X[3 * m]) && next_d(X[3 * m + 1]) && next_d(X[3 * m + 2]);
+      ok = ok && next_i(size);
       if (!ok) return fail_with(HARM_E_ARG, "truncated tracer section");
     }
+    if (k != ntr_tok) return fail_with(HARM_E_ARG, "unexpected data after the tracer section");
     rc = harm_tracers_put(h, g, ids.data(), X.data(), cnt);
     if (rc) return rc;
-  } else if (got != 0) {
-    return fail_with(HARM_E_ARG, "truncated tracer section");
+  }
+  if (nguess) {
+    std::vector<double> T(nguess);
+    for (size_t m = 0; m < nguess; m++)
+      if (sscanf(tok[ntr_tok + m].c_str(), "%lf", &T[m]) != 1) return fail_with(HARM_E_ARG, "bad COOL_EOS section");
+    rc = harm_put_eos_guess(h, T.data());
+    if (rc) return rc;
   }
   *hdr = r;
   return harm_sync(h);

@@ -17,8 +17,8 @@ files).  Fixtures hold only generated numbers:
   eos_<config>.npz  the run-time COOL_EOS of a COOL_EOS build: digests of its
                 tables, pressure/dpdu/dpdrho on seeded entries.
   cool_<config>.npz  step_ch() of a COOL_EOS build: states, flags, times and
-                temperature guesses after init() and steps; Utoprim_5d known
-                answers.
+                temperature guesses after init() and steps; the restart file
+                after 5 steps; Utoprim_5d known answers.
 Each configuration runs in its own process: the reference keeps its state in
 globals.
 """
@@ -279,6 +279,9 @@ def cool_config(cfg):
         out["t%d" % n] = np.array([ref.get("t"), ref.get("dt")])
         out["lastT%d" % n] = ref.cool_lastT()
         out["diag%d" % n] = np.array([ref.get(s) for s in SCALARS])
+        if n == 5:
+            with _QuietStdout():
+                out["restart5"] = np.frombuffer(ref.restart_write().encode(), dtype=np.uint8)
     # Utoprim_5d on perturbed states of active zones, each with its own guess
     rng = np.random.default_rng(55)
     last = ref.cool_lastT()

@@ -173,3 +173,44 @@ def test_cool_mixed_tracks_fp64(hc, eos):
     a.close()
     b.close()
     E.close()
+
+
+def test_cool_restart_matches_reference(hc, fx, eos, tmp_path):
+    """restart_write() of a COOL_EOS run ends with every zone's temperature guess
+    (restart_write_CoolEOS, cooleos.c:996-1013): the device's file matches the
+    reference's after 5 steps, and reading the reference's file continues the
+    run exactly (steps 6..12)."""
+    from test_gpu_restart import _header_fields
+    ref = fx["restart5"].tobytes().decode()
+    pr = _problem(hc, fx)
+    ctx = hc.Context(pr)
+    ctx.set_eos(eos)
+    ctx.put_prims(full_state(pr, fx["p5"]), full_state(pr, fx["pflag5"]))
+    ctx.set_time(*fx["t5"])
+    ctx.set_mass(*fx["diag5"][6:8])
+    ctx.put_eos_guess(fx["lastT5"])
+    h = _header_fields(ref)
+    fields = {k: v for k, v in h.items() if k not in ("n1", "n2", "n3", "t", "dt", "mass_in", "mass_out")}
+    refl = ref.split("\n")
+    tail = refl[-1].split()
+    path = str(tmp_path / "rdump")
+    ctx.restart_write(path, ener_size=int(tail[0]), **fields)
+    ours = open(path).read().split("\n")
+    assert ours[0] == refl[0]
+    cells = int(np.prod(pr.shape))
+    for c in range(1, 1 + cells):
+        assert ours[c] == refl[c], c
+    assert ours[-1].split()[1:] == tail[1:]      # the guesses, as the reference prints them
+    ctx.close()
+    path2 = tmp_path / "rdump_ref"
+    path2.write_text(ref)
+    c2 = hc.Context(pr)
+    c2.set_eos(eos)
+    c2.init_torus()
+    c2.restart_read(str(path2))
+    assert np.array_equal(active(pr, c2.get_prims()), fx["p5"])
+    assert _bits_equal(c2.eos_guess(), fx["lastT5"])
+    c2.run(7)
+    assert _bits_equal(active(pr, c2.get_prims()), fx["p12"])
+    assert _bits_equal(c2.eos_guess(), fx["lastT12"])
+    c2.close()
