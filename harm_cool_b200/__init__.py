@@ -73,7 +73,9 @@ class RestartHeader(ctypes.Structure):
 class Integrals(ctypes.Structure):
     """harm_integrals: diag()'s sums and the largest div B (diag.c:113-230)."""
     _fields_ = [("mass", ctypes.c_double), ("ang_mom", ctypes.c_double), ("energy", ctypes.c_double),
-                ("divbmax", ctypes.c_double), ("imax", ctypes.c_int * 3)]
+                ("divbmax", ctypes.c_double), ("imax", ctypes.c_int * 3),
+                ("lnu", ctypes.c_double), ("lnu_rho", ctypes.c_double), ("lnu_rho_2", ctypes.c_double),
+                ("lnu2", ctypes.c_double)]
 
 
 class Diag(ctypes.Structure):
@@ -95,7 +97,7 @@ EOS_CONSTANTS = ("rho_unit", "u_unit", "p_unit", "kbol", "mav", "cl", "rho_min",
 
 class EosDesc(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("ntab", ctypes.c_int)] + [
-        (n, ctypes.c_double) for n in EOS_CONSTANTS]
+        (n, ctypes.c_double) for n in EOS_CONSTANTS] + [("l_unit", ctypes.c_double)]
 
 
 _DP = ctypes.POINTER(ctypes.c_double)
@@ -152,7 +154,8 @@ _SIGNATURES = {
     "harm_ensemble_run_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _DP]),
     "harm_utoprim_2d_batch_noalloc": (ctypes.c_int, [_DP, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int),
                                                      ctypes.c_long, ctypes.c_double]),
-    "harm_eos_create": (ctypes.c_int, [ctypes.POINTER(EosDesc), _DP, _DP, _DP, ctypes.POINTER(ctypes.c_void_p)]),
+    "harm_eos_create": (ctypes.c_int, [ctypes.POINTER(EosDesc), _DP, _DP, _DP, _DP,
+                                       ctypes.POINTER(ctypes.c_void_p)]),
     "harm_eos_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "harm_eos_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_long,
                                       ctypes.POINTER(ctypes.c_int), _DP, _DP, _DP, _DP]),
@@ -281,7 +284,8 @@ class Eos:
 
     xaxis[nx] (rho, g/cm^3), yaxis[ny] (T, K), values[ntab][nx][ny][5] with
     e, p, Qnu, tau, Yee per node, consts: the unit and range constants named in
-    EOS_CONSTANTS."""
+    EOS_CONSTANTS, and for the cooling diagnostics "l_unit" and "hdfac" (each
+    table's HdFac)."""
 
     WHAT = {"pressure": 0, "dpdu": 1, "dpdrho": 2}
 
@@ -292,9 +296,15 @@ class Eos:
         ntab, nx, ny, nd = v.shape
         if nd != 5 or nx != len(self.xaxis) or ny != len(self.yaxis):
             raise ValueError("values must be [ntab][nx][ny][5]")
-        d = EosDesc(nx=nx, ny=ny, ntab=ntab, **{k: float(consts[k]) for k in EOS_CONSTANTS})
+        d = EosDesc(nx=nx, ny=ny, ntab=ntab, l_unit=float(consts.get("l_unit", 0.0)),
+                    **{k: float(consts[k]) for k in EOS_CONSTANTS})
+        hd = consts.get("hdfac")
+        hd = None if hd is None else np.ascontiguousarray(hd, dtype=np.float64)
+        if hd is not None and len(hd) != ntab:
+            raise ValueError("hdfac needs one value per table")
         h = ctypes.c_void_p()
-        _check(library().harm_eos_create(ctypes.byref(d), _dp(self.xaxis), _dp(self.yaxis), _dp(v), ctypes.byref(h)))
+        _check(library().harm_eos_create(ctypes.byref(d), _dp(self.xaxis), _dp(self.yaxis), _dp(v),
+                                         _dp(hd) if hd is not None else None, ctypes.byref(h)))
         self.h = h
         self.ntab, self.consts = ntab, dict(consts)
 
@@ -491,7 +501,8 @@ class Context:
         """diag()'s integrals: mass, angular momentum, energy, divbmax and its zone."""
         d = Integrals()
         _check(self.lib.harm_diag_integrals(self.h, ctypes.byref(d)))
-        return {"rmed": d.mass, "pp": d.ang_mom, "e": d.energy, "divbmax": d.divbmax, "imax": list(d.imax)}
+        return {"rmed": d.mass, "pp": d.ang_mom, "e": d.energy, "divbmax": d.divbmax, "imax": list(d.imax),
+                "lnu": d.lnu, "lnu_rho": d.lnu_rho, "lnu_rho_2": d.lnu_rho_2, "lnu2": d.lnu2}
 
     # tracer particles (tracers.c)
     def tracers_init(self):

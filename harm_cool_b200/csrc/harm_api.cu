@@ -700,6 +700,7 @@ extern "C" int harm_create(const harm_params *prm, const double *gcov, const dou
   rc |= al((void **)&x->partials, 3 * x->nparts * sizeof(double));
   rc |= al((void **)&x->sc, sizeof(DevScalars));
   rc |= al((void **)&x->Ubuf, st);
+  rc |= al((void **)&x->coolgeo, 2 * G.ng * sizeof(double));
   if (rc != HARM_OK) { harm_destroy(h); return HARM_E_CUDA; }
   if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) { harm_destroy(h); return fail_with(HARM_E_CUDA, "stream"); }
   // geometry planes
@@ -722,6 +723,13 @@ extern "C" int harm_create(const harm_params *prm, const double *gcov, const dou
         }
   // radial floors get_rho_u_floor() (fixup.c:117-140), evaluated on the host
   radial_floors(coords, prm->gam, G.ng, hf.data());
+  // zone-centre r and |r tan theta| (get_coord, metric.c:446-458; diag.c:238-242)
+  std::vector<double> hcg((size_t)2 * G.ng);
+  for (long c = 0; c < G.ng; c++) {
+    const double r = coords[c * 4 + 1], th = coords[c * 4 + 2];
+    hcg[c] = r;
+    hcg[G.ng + c] = fabs(r * tan(th));
+  }
   DevScalars s0;
   std::memset(&s0, 0, sizeof(s0));
   unsigned long long big;
@@ -732,6 +740,7 @@ extern "C" int harm_create(const harm_params *prm, const double *gcov, const dou
   if (cudaMemcpy(x->geo, hg.data(), hg.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(x->conn, hc.data(), hc.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(x->floors, hf.data(), hf.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(x->coolgeo, hcg.data(), hcg.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(x->katm, katm, d.sn1 * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(x->sc, &s0, sizeof(s0), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemset(x->p, 0, st) != cudaSuccess || cudaMemset(x->ph, 0, st) != cudaSuccess ||
@@ -752,7 +761,7 @@ extern "C" void harm_destroy(harm_ctx *h)
   void *ptrs[] = {x->p, x->ph, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm,
                   x->stage, x->stage_flag, x->fail_list, x->fix_buf, x->partials, x->sc,
                   x->F1f, x->F2f, x->F3f, x->geo32, x->conn32, x->Ubuf, x->trX, x->trids, x->trst,
-                  x->lastT};
+                  x->lastT, x->coolgeo, x->cooldiag};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (x->pinned) cudaFreeHost(x->pinned);

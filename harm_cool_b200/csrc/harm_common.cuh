@@ -93,6 +93,8 @@ struct Ctx {
   EosDev eos;                    // the attached tables (owned by the caller's harm_eos)
   double *lastT;                 // [nc] per-zone temperature guesses (_aLastT)
   bool cool_seed;                // the next step may meet zones without a guess
+  double *coolgeo;               // [2][ng] r and |r tan theta| at zone centres (diag.c:225-249)
+  double *cooldiag;              // COOL_EOS diagnostics scratch (harm_diag.cu)
 };
 
 __device__ __forceinline__ void record_fail(DevScalars *sc, int code, int h, int i, int j)

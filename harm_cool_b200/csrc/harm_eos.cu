@@ -58,7 +58,7 @@ static double f32_scale(const std::vector<double> &v, size_t off, size_t n)
 using harm::fail_with;
 
 extern "C" int harm_eos_create(const harm_eos_desc *dsc, const double *xaxis, const double *yaxis,
-                               const double *values, harm_eos **out)
+                               const double *values, const double *hdfac, harm_eos **out)
 {
   if (!dsc || !xaxis || !yaxis || !values || !out) return fail_with(HARM_E_ARG, "null argument");
   *out = nullptr;
@@ -83,10 +83,13 @@ extern "C" int harm_eos_create(const harm_eos_desc *dsc, const double *xaxis, co
     for (long q = 0; q < plane; q++)
       for (int d = 0; d < harm::EOS_ND; d++)
         v[((size_t)d * nt + t) * plane + q] = values[((size_t)t * plane + q) * harm::EOS_ND + d];
-  cudaError_t err = cudaMalloc(&e->axes, (nx + ny) * sizeof(double));
+  // axes, then each table's HdFac when given
+  cudaError_t err = cudaMalloc(&e->axes, (nx + ny + nt) * sizeof(double));
   if (err == cudaSuccess) err = cudaMalloc(&e->vals, v.size() * sizeof(double));
   if (err == cudaSuccess) err = cudaMemcpy(e->axes, xaxis, nx * sizeof(double), cudaMemcpyHostToDevice);
   if (err == cudaSuccess) err = cudaMemcpy(e->axes + nx, yaxis, ny * sizeof(double), cudaMemcpyHostToDevice);
+  if (err == cudaSuccess && hdfac)
+    err = cudaMemcpy(e->axes + nx + ny, hdfac, nt * sizeof(double), cudaMemcpyHostToDevice);
   if (err == cudaSuccess) err = cudaMemcpy(e->vals, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice);
   // float copies of the axes and of the e and p planes, scaled into range
   const size_t np = (size_t)nt * plane;
@@ -137,6 +140,8 @@ extern "C" int harm_eos_create(const harm_eos_desc *dsc, const double *xaxis, co
   d.t_max = dsc->t_max;
   d.hh = dsc->hh;
   d.gam = dsc->gam;
+  d.hdfac = hdfac ? e->axes + nx + ny : nullptr;
+  d.l_unit = dsc->l_unit;
   *out = e;
   return HARM_OK;
 }

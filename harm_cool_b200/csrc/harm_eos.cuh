@@ -42,6 +42,10 @@ struct EosDev {
   int f32;
   const float *xa32, *ya32, *e32, *p32;  // [ntab][nx][ny] each
   double se, sp;
+  // CoolVal_rho0_u_CoolEOS: each table's HdFac (cooleos.c:945-960, null when not
+  // given) and L_UNIT
+  const double *hdfac;
+  double l_unit;
 };
 
 struct EosCursor {
@@ -289,6 +293,73 @@ static __device__ __noinline__ double eos_pressure(const EosDev &E, EosCursor &c
   c.m_p = p;
   c.m_T = c.T;
   return p;
+}
+
+// the cooling values of CoolVal_rho0_u_CoolEOS (decs.h:251-258)
+enum { COOL_LAMBDA_SIM = 0, COOL_P = 1, COOL_Hd = 2, COOL_Qnu = 3, COOL_Tau = 4, COOL_T = 5, COOL_Yee = 6,
+       NCOOLVAL = 7 };
+
+// CoolVal_rho0_u_CoolEOS (cooleos.c:479-662): p, T, the disc scale height, the
+// neutrino emissivity and cooling rate, tau and Yee at (rho0, u) of the zone at
+// radius r, with the zone's guess in c.T.  Unlike the pressure it has no e < 0
+// branch, and it tests the table range before setting a first guess.
+static __device__ __noinline__ void eos_coolval(const EosDev &E, EosCursor &c, double rho0, double u, double r,
+                                                double *cv)
+{
+  const double SMALL_ = 1.e-20;
+  const double rho = rho0 * E.rho_unit;
+  const double e = u * E.u_unit;
+  const double hh = E.hh;
+  const double HdFac = E.hdfac[c.tab];
+  bool gamma_law = rho < E.rho_min || rho > E.rho_max;
+  double x = 0.;
+  int x0 = 0, sx = 4;
+  bool rho_in = false;
+  if (!gamma_law) {
+    if (c.T == 0.0) {
+      const double corrfact = 1.0;
+      c.T = (E.gam - 1.) * u / rho0 / E.kbol * E.mav * E.cl * E.cl * corrfact;
+      if (c.T < E.t_min * (1.0 + hh)) c.T = E.t_min * (1.0 + hh);
+    }
+    const double minx = E.t_min * (1.0 + hh), maxx = E.t_max * (1.0 - hh);
+    rho_in = eos_rho_window(E, rho, x0, sx);
+    x = c.T;
+    const double berr = eos_newton_T(E, c.tab, rho, rho_in, x0, sx, e, x, minx, maxx);
+    gamma_law = berr > 1.0E-6;
+  }
+  c.memo = false;
+  if (gamma_law) {
+    cv[COOL_P] = (E.gam - 1.) * u;
+    cv[COOL_LAMBDA_SIM] = SMALL_;
+    cv[COOL_Qnu] = SMALL_;
+    const double Hd = HdFac * E.cl * sqrt(cv[COOL_P] * E.p_unit / (rho * E.cl * E.cl + e));
+    cv[COOL_Hd] = Hd / E.l_unit;
+    cv[COOL_T] = (E.gam - 1.) * u / rho0 / E.kbol * E.mav * E.cl * E.cl;
+    cv[COOL_Tau] = 0.0;
+    cv[COOL_Yee] = 0.0;
+    return;
+  }
+  double val[EOS_ND];
+#pragma unroll
+  for (int d = 0; d < EOS_ND; d++) {
+    double v = CUDART_NAN, unused;
+    if (rho_in) {
+      double w;
+      if (eos_value<false>(E, c.tab, d, rho, x0, sx, x, w, unused)) v = w;
+    }
+    val[d] = v;
+  }
+  c.T = x;
+  const double Hd = HdFac * E.cl * sqrt(val[EOS_P] / (rho * E.cl * E.cl + val[EOS_E]));
+  const double Hdisk = 0.5 * r * E.l_unit;
+  const double lambda_cgs = val[EOS_QNU] / Hdisk;
+  cv[COOL_LAMBDA_SIM] = lambda_cgs / (E.rho_unit * E.cl * E.cl * E.cl / E.l_unit);
+  cv[COOL_Hd] = Hd / E.l_unit;
+  cv[COOL_Qnu] = val[EOS_QNU] / (E.rho_unit * E.cl * E.cl * E.cl / E.l_unit);
+  cv[COOL_P] = val[EOS_P] / E.p_unit;
+  cv[COOL_T] = x;
+  cv[COOL_Tau] = val[EOS_TAU] > 0 ? val[EOS_TAU] : 0.0;
+  cv[COOL_Yee] = val[EOS_YEE];
 }
 
 // dpdu_calc_CoolEOS (cooleos.c:667-704)

@@ -37,7 +37,8 @@ P_UNIT = U_UNIT
 def constants(gam, rho=(1.e2, 1.e15), T=(1.e4, 1.e18)):
     """The unit and range constants harm_cool_b200.Eos takes."""
     return {"rho_unit": RHO_UNIT, "u_unit": U_UNIT, "p_unit": P_UNIT, "kbol": KBOL, "mav": MAV, "cl": CL,
-            "rho_min": rho[0], "rho_max": rho[1], "t_min": T[0], "t_max": T[1], "hh": 1.0e-6, "gam": gam}
+            "rho_min": rho[0], "rho_max": rho[1], "t_min": T[0], "t_max": T[1], "hh": 1.0e-6, "gam": gam,
+            "l_unit": L_UNIT}
 
 
 def log_axis(n, lo, hi):
@@ -74,7 +75,8 @@ def ideal_gas_radiation(rho, T, hd):
 def build_tables(radii, generator=ideal_gas_radiation, nx=72, ny=72, rho=(1.e2, 1.e15), T=(1.e4, 1.e18),
                  gam=4. / 3.):
     """Tables for the given radial indices: (xaxis, yaxis, values[ntab][nx][ny][5],
-    constants), values packed as calc_cache_val packs them (cooleos.c:171-194)."""
+    constants with each table's HdFac), values packed as calc_cache_val packs them
+    (cooleos.c:171-194)."""
     xa, ya = log_axis(nx, *rho), log_axis(ny, *T)
     R, TT = np.meshgrid(xa, ya, indexing="ij")
     val = np.zeros((len(radii), nx, ny, 5))
@@ -82,4 +84,6 @@ def build_tables(radii, generator=ideal_gas_radiation, nx=72, ny=72, rho=(1.e2, 
         e, p, qnu, tau, xnee, xnep = generator(R, TT, hdfac(r))
         val[t, ..., 0], val[t, ..., 1], val[t, ..., 2], val[t, ..., 3] = e, p, qnu, tau
         val[t, ..., 4] = (xnee - xnep) / (R / 1.66e15)
-    return xa, ya, val, constants(gam, rho, T)
+    c = constants(gam, rho, T)
+    c["hdfac"] = np.array([hdfac(r) for r in radii])
+    return xa, ya, val, c

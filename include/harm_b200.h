@@ -204,7 +204,17 @@ typedef struct harm_integrals {
   double energy;    /* sum of U[UU] dV (e) */
   double divbmax;   /* largest |div B| in the flux-CT form */
   int imax[3];      /* its zone: r, theta, phi indices from 0 (the first in loop order) */
+  /* with COOL_EOS (diag.c:137-251, ener.out columns 10-13): the neutrino
+     luminosities from CoolVal_rho0_u_CoolEOS; 0 otherwise */
+  double lnu;       /* sum of Lambda_sim sqrt(-g) */
+  double lnu_rho;   /* sum of Lambda_sim sqrt(-g) rho / sum of sqrt(-g) rho */
+  double lnu_rho_2; /* sum of sqrt(-g) rho */
+  double lnu2;      /* per (phi, r) row, Qnu sqrt(-g) at the first theta from the equator
+                       where |r tan theta| reaches the row's mean scale height */
 } harm_integrals;
+/* With COOL_EOS tables attached, this also moves each zone's temperature guess
+   as diag() does (InitCache_CoolEOS, primtoU, CoolVal_rho0_u_CoolEOS per zone,
+   diag.c:137-149); those guesses carry into the following steps. */
 int harm_diag_integrals(harm_ctx *ctx, harm_integrals *out);
 
 /* ---- tracer particles (tracers.c) ----
@@ -293,7 +303,9 @@ int harm_utoprim_2d_batch_noalloc(const double *U, const double *gcov, const dou
    reference's node order (Cache4d MValues, cache4d.c:1043).  The tables are
    built on the host, as the reference builds them (calc_cache_val,
    cooleos.c:171-194); the units and ranges are cooleos.c's constants
-   (cooleos.c:83-135, 840-940); gam is the gamma-law fall-back's index. */
+   (cooleos.c:83-135, 840-940); gam is the gamma-law fall-back's index.
+   hdfac[ntab] (each table's HdFac, cooleos.c:945-960) and l_unit serve the
+   cooling values of harm_diag_integrals; hdfac may be NULL without them. */
 typedef struct harm_eos harm_eos;
 typedef struct harm_eos_desc {
   int nx, ny, ntab;
@@ -303,9 +315,10 @@ typedef struct harm_eos_desc {
   double t_min, t_max;              /* TMin, TMax (K) */
   double hh;                        /* relative margin and difference step, 1e-6 */
   double gam;
+  double l_unit;                    /* L_UNIT (cm) */
 } harm_eos_desc;
 int harm_eos_create(const harm_eos_desc *desc, const double *xaxis, const double *yaxis,
-                    const double *values, harm_eos **out);
+                    const double *values, const double *hdfac, harm_eos **out);
 int harm_eos_destroy(harm_eos *eos);
 
 /* pressure_rho0_u_CoolEOS (cooleos.c:314-444), dpdu_calc_CoolEOS and

@@ -253,13 +253,17 @@ def standin_tables(startx1, dx1, R0, sn1, gam, nx=72, ny=72, rho=(1.e2, 1.e15), 
     lib.ora_eos_axis(nx, rho[0], rho[1], _dp(xa))
     lib.ora_eos_axis(ny, T[0], T[1], _dp(ya))
     val = np.zeros((sn1, nx, ny, 5))
+    hdfac = np.zeros(sn1)
     for i in range(sn1):
-        hd = lib.ora_eos_hdfac(lib.ora_zone_r(startx1, dx1, R0, i))
-        lib.ora_eos_fill(nx, ny, _dp(xa), _dp(ya), hd, _dp(val[i]))
+        hdfac[i] = lib.ora_eos_hdfac(lib.ora_zone_r(startx1, dx1, R0, i))
+        lib.ora_eos_fill(nx, ny, _dp(xa), _dp(ya), hdfac[i], _dp(val[i]))
     c = np.zeros(len(EOS_CONSTANTS))
     lib.ora_eos_constants(gam, _dp(c))
     consts = dict(zip(EOS_CONSTANTS, c.tolist()))
     consts["rho_min"], consts["rho_max"], consts["t_min"], consts["t_max"] = rho[0], rho[1], T[0], T[1]
+    # L_UNIT = GNEWT M_BLH / CL^2 (cooleos.c:109), the same operations as the C
+    consts["l_unit"] = 6.6742867e-8 * (3. * 1.9892e33) / (2.99792458e10 * 2.99792458e10)
+    consts["hdfac"] = hdfac
     return EosTables(xa, ya, val, consts)
 
 
@@ -351,7 +355,8 @@ class Reference:
             log = open(os.path.join(d, "diag_stderr.txt")).read()
         m = re.search(r"divbmax:\s+(-?\d+)\s+(-?\d+)\s+(-?\d+)\s+(\S+)", log)
         return {"rmed": float(ener[1]), "pp": float(ener[2]), "e": float(ener[3]),
-                "divbmax": float(m.group(4)), "imax": [int(m.group(1)), int(m.group(2)), int(m.group(3))]}
+                "divbmax": float(m.group(4)), "imax": [int(m.group(1)), int(m.group(2)), int(m.group(3))],
+                "ener": [float(v) for v in ener]}
 
     def tracers(self):
         """The reference's tracer list (tracers.c:24): ids[n][3] = (i, j, h), X[n][3]."""
@@ -392,9 +397,9 @@ class Reference:
 
     # run-time COOL_EOS (COOL_EOS checker builds only; oracle/cool_hooks.inc)
     def cool_constants(self):
-        c = np.zeros(len(EOS_CONSTANTS))
+        c = np.zeros(len(EOS_CONSTANTS) + 1)
         self.lib.ref_cool_constants(_dp(c))
-        return dict(zip(EOS_CONSTANTS, c.tolist()))
+        return dict(zip(EOS_CONSTANTS + ("l_unit",), c.tolist()))
 
     def cool_tables(self):
         """Every node of every per-radius table, computed by the reference's own
@@ -404,11 +409,15 @@ class Reference:
         nx, ny, nd, ntab = d[0], d[1], d[2], d[3]
         xa, ya = np.zeros(nx), np.zeros(ny)
         val = np.zeros((ntab, nx, ny, nd))
+        hdfac = np.zeros(ntab)
         hd = ctypes.c_double()
         with _QuietStdout():
             for i in range(ntab):
                 self.lib.ref_cool_table(i, _dp(xa), _dp(ya), _dp(val[i]), ctypes.byref(hd))
-        return EosTables(xa, ya, val, self.cool_constants())
+                hdfac[i] = hd.value
+        consts = self.cool_constants()
+        consts["hdfac"] = hdfac
+        return EosTables(xa, ya, val, consts)
 
     def cool_batch(self, what, tab, rho0, u, lastT):
         """pressure/dpdu/dpdrho through the reference's own functions, one call per

@@ -237,8 +237,9 @@ def eos_config(cfg):
     out = {"grid": np.array([ref.get("startx1"), ref.get("dx1"), ref.get("R0"), ref.get("gam")]),
            "sn1": np.array(ref.sn1), "sha_tables": np.array(sha(T.val)),
            "sha_axes": np.array(sha(np.concatenate([T.xa, T.ya]))),
-           "consts": np.array([T.consts[k] for k in sorted(T.consts)]),
-           "const_names": np.array(sorted(T.consts))}
+           "consts": np.array([T.consts[k] for k in sorted(T.consts) if k != "hdfac"]),
+           "const_names": np.array(sorted(k for k in T.consts if k != "hdfac")),
+           "hdfac": T.consts["hdfac"]}
     tab, rho0, u, lastT = eos_inputs(np.random.default_rng(2024), T.ntab, 3000)
     out.update(tab=tab, rho0=rho0, u=u, lastT=lastT)
     for what in ("pressure", "dpdu", "dpdrho"):
@@ -282,6 +283,13 @@ def cool_config(cfg):
         if n == 5:
             with _QuietStdout():
                 out["restart5"] = np.frombuffer(ref.restart_write().encode(), dtype=np.uint8)
+    # diag(INIT_OUT) on the state after the last step: ener.out's integrals and
+    # COOL_EOS luminosities (diag.c:316-320), and the guesses diag() leaves
+    with _QuietStdout():
+        dg = ref.diag_init()
+    out["diag_cool_ener"] = np.array(dg["ener"])
+    out["diag_cool_divb"] = np.array([dg["divbmax"]] + dg["imax"])
+    out["lastT_after_diag"] = ref.cool_lastT()
     # Utoprim_5d on perturbed states of active zones, each with its own guess
     rng = np.random.default_rng(55)
     last = ref.cool_lastT()

@@ -214,3 +214,29 @@ def test_cool_restart_matches_reference(hc, fx, eos, tmp_path):
     assert _bits_equal(active(pr, c2.get_prims()), fx["p12"])
     assert _bits_equal(c2.eos_guess(), fx["lastT12"])
     c2.close()
+
+
+def test_cool_diag_matches_reference(hc, fx, eos):
+    """diag() with COOL_EOS on the state after 12 steps: the integrals and the
+    neutrino luminosities as ener.out prints them (diag.c:316-320: %10.5g for
+    t, rmed, pp, e; %15.8g for lnu, lnu_rho, lnu_rho_2, lnu2), divbmax and its
+    zone, and the guesses diag() leaves (bit for bit: its InitCache, primtoU and
+    CoolVal calls move them)."""
+    pr = _problem(hc, fx)
+    ctx = hc.Context(pr)
+    ctx.set_eos(eos)
+    ctx.put_prims(full_state(pr, fx["p12"]), full_state(pr, fx["pflag12"]))
+    ctx.set_time(*fx["t12"])
+    ctx.put_eos_guess(fx["lastT12"])
+    ctx.run(0)
+    d = ctx.integrals()
+    ener = fx["diag_cool_ener"]
+    for k, name in ((1, "rmed"), (2, "pp"), (3, "e")):
+        assert float("%10.5g" % d[name]) == ener[k], (name, d[name], ener[k])
+    for k, name in ((9, "lnu"), (10, "lnu_rho"), (11, "lnu_rho_2"), (12, "lnu2")):
+        assert float("%15.8g" % d[name]) == ener[k], (name, d[name], ener[k])
+    divb = fx["diag_cool_divb"]
+    assert float("%g" % d["divbmax"]) == divb[0]
+    assert d["imax"] == [int(v) for v in divb[1:]]
+    assert _bits_equal(ctx.eos_guess(), fx["lastT_after_diag"])
+    ctx.close()
