@@ -361,13 +361,33 @@ def run_ensemble(args):
     print(json.dumps(line), flush=True)
 
 
+def tracers_by_density(np, pr, p, n, seed):
+    """n tracer particles at zone centres drawn with probability proportional to
+    the zone's rest mass rho sqrt(-g) dV (seeded); labels (i, j, h) of the zone."""
+    g = pr.geometry["gdet"][:, :, 3]
+    sn1, sn2 = g.shape
+    rho = np.zeros((sn1, sn2))
+    rho[2:-2, 2:-2] = np.maximum(p[0, 2:-2, 2:-2, 0], 0.0)
+    w = (rho * g).ravel()
+    rng = np.random.default_rng(seed)
+    pick = rng.choice(w.size, size=n, p=w / w.sum())
+    i, j = pick // sn2, pick % sn2
+    prm = pr.params
+    X = np.zeros((n, 3))
+    X[:, 0] = prm.startx[1] + ((i - 2) + 0.5) * prm.dx[1]
+    X[:, 1] = prm.startx[2] + ((j - 2) + 0.5) * prm.dx[2]
+    ids = np.stack([i, j, np.zeros(n, dtype=np.int64)], axis=1)
+    return ids, X
+
+
 def run_cool(args):
     """The COOL_EOS step on the 256x256 torus of the reference's init.c literals
     (a=0.6, rin=4, rmax=11.8, beta=50; cooleos.c's 3 Msun hole and units), FP64,
     with the reference's 72x72 per-radius tables built on the host by the
     synthetic ideal-gas-plus-radiation generator of harm_cool_b200.eos_tables in
-    place of the Fortran EOS.  The first step seeds the per-zone temperature
-    guesses row by row and runs outside the timed region."""
+    place of the Fortran EOS, and 1e5 tracer particles seeded in proportion to
+    the rest mass.  The first step seeds the per-zone temperature guesses row by
+    row and runs outside the timed region."""
     import numpy as np
     import harm_cool_b200 as hc
     from harm_cool_b200 import eos_tables
@@ -378,6 +398,8 @@ def run_cool(args):
     ctx = hc.Context(pr)
     ctx.init_torus()
     ctx.set_eos(eos)
+    ids, X = tracers_by_density(np, pr, ctx.get_prims(), args.cool_tracers, args.seed)
+    ctx.tracers_put(ids, X)
     t0 = time.perf_counter()
     ctx.run(1)                       # the seeding step
     seed_s = time.perf_counter() - t0
@@ -407,7 +429,8 @@ def run_cool(args):
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": "FM torus %dx%d (a=0.6, rin=4, rmax=11.8, beta=50), COOL_EOS, 72x72 "
-                                   "per-radius tables (rho 1e2-1e15, T 1e4-1e18), synthetic generator" % (n, n),
+                                   "per-radius tables (rho 1e2-1e15, T 1e4-1e18), synthetic generator, "
+                                   "%d tracers seeded by rest mass" % (n, n, args.cool_tracers),
                        "l2": "tables (%.0f MB) stay in L2; state per step is small" % (val.nbytes / 1e6)},
             "seeding_step_s": seed_s,
             "e2e": {"value": zones * args.e2e_steps / (ms_e2e / 1e3), "unit": "zone-cycles/s",
@@ -426,6 +449,7 @@ def run_cool(args):
         cm.init_torus()
         cm.set_precision(hc.Context.MIXED)
         cm.set_eos(eos)
+        cm.tracers_put(ids, X)
         cm.run(args.warmup)
         sampler = ClockSampler(0)
         sampler.start()
@@ -469,6 +493,7 @@ def main():
                     help="torus: the 288x256x256 step (default); ensemble: 64 seeded 2D tori; "
                          "cool: the 256x256 COOL_EOS step")
     ap.add_argument("--cool-n", type=int, default=256)
+    ap.add_argument("--cool-tracers", type=int, default=100000)
     ap.add_argument("--dump-cool", default=None, help="save the FP64 and mixed COOL_EOS states (npz)")
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--seed", type=int, default=0)
