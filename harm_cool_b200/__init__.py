@@ -162,6 +162,8 @@ _SIGNATURES = {
     "harm_utoprim_5d_batch": (ctypes.c_int, [ctypes.c_void_p, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int), _DP,
                                              _DP, ctypes.POINTER(ctypes.c_int), ctypes.c_long]),
     "harm_set_eos": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "harm_dump_write": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RestartHeader), ctypes.POINTER(GridSpec),
+                                       ctypes.c_char_p]),
     "harm_get_eos_guess": (ctypes.c_int, [ctypes.c_void_p, _DP]),
     "harm_put_eos_guess": (ctypes.c_int, [ctypes.c_void_p, _DP]),
 }
@@ -490,6 +492,19 @@ class Context:
         for k, v in fields.items():
             setattr(hd, k, v)
         _check(self.lib.harm_restart_write(self.h, ctypes.byref(hd), ctypes.byref(pr.grid), path.encode()))
+
+    def dump_write(self, path, **fields):
+        """dump(): the reference's ASCII dump of the state; header fields as for
+        restart_write()."""
+        pr = self.problem
+        hd = RestartHeader()
+        hd.tf, hd.a, hd.gam, hd.cour = pr.params.tf, pr.params.a, pr.params.gam, pr.params.cour
+        hd.lim, hd.defcon = pr.params.lim, pr.params.defcon
+        hd.Rin, hd.Rout, hd.hslope, hd.R0 = pr.grid.Rin, pr.grid.Rout, pr.grid.hslope, pr.grid.R0
+        hd.Rbr = -1.0
+        for k, v in fields.items():
+            setattr(hd, k, v)
+        _check(self.lib.harm_dump_write(self.h, ctypes.byref(hd), ctypes.byref(pr.grid), path.encode()))
 
     def restart_read(self, path):
         """restart_init(): state, time, mass counters and tracers from a restart file."""

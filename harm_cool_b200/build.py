@@ -41,6 +41,7 @@ UNITS = {
     "harm_restart.cu": ["-fmad=false"],  # restart files in the reference's format
     "harm_eos.cu": ["-fmad=false"],      # run-time COOL_EOS tables and batch calls
     "harm_cool.cu": ["-fmad=false"],     # the COOL_EOS step and Utoprim_5d
+    "harm_dump.cu": ["-fmad=false"],     # the ASCII dump format
 }
 
 

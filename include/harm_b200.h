@@ -195,6 +195,16 @@ int harm_restart_write(harm_ctx *ctx, const harm_restart_header *hdr, const harm
    match the context's. */
 int harm_restart_read(harm_ctx *ctx, const char *path, const harm_grid_spec *g, harm_restart_header *hdr);
 
+/* dump() (dump.c:1710-2047, the ASCII dump of HDFDUMP 0) of the device state
+   into the file at path: the header line (from hdr's fields and the context's
+   t, dt and grid), then one line per active zone in the reference's order with
+   its coordinates, primitives, cooling values (zeros without COOL_EOS), div B,
+   u^mu, u_mu, b^mu, b_mu, wave speeds, sqrt(-g), |v|, sound speed, radial
+   velocity and Mach number; hdr->failed != 0 stops each line after div B, as
+   the reference does.  g gives R0 and hslope.  With COOL_EOS the zones'
+   temperature guesses move as the reference's dump() moves them. */
+int harm_dump_write(harm_ctx *ctx, const harm_restart_header *hdr, const harm_grid_spec *g, const char *path);
+
 /* ---- diagnostics ---- */
 
 /* diag()'s integrals (diag.c:113-230) over the active zones of the current state. */

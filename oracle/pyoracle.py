@@ -342,6 +342,16 @@ class Reference:
         self.pflag = np.ctypeslib.as_array(
             ctypes.cast(self.lib.ref_ptr(b"pflag"), ctypes.POINTER(ctypes.c_byte)), shape=s3)
 
+    def dump(self):
+        """dump() (dump.c:1710-2047): the reference's ASCII dump of the state, as text."""
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "dump")
+            with _QuietStdout():
+                if self.lib.ref_dump(path.encode()) != 0:
+                    raise RuntimeError("dump failed")
+            return open(path).read()
+
     def diag_init(self):
         """diag(INIT_OUT): (rmed, pp, e) as ener.out prints them (%10.5g), divbmax as the
         LOG line prints it (%g) and its zone (i, j, h from 0) (diag.c:312-326)."""

@@ -260,6 +260,19 @@ int ref_restart_init(const char *dir)
   return ok ? 0 : -2;
 }
 
+/* the reference's ASCII dump() (dump.c:1710-2047) of the current state, into
+   the file at path; the header's counters are the globals as they stand */
+int ref_dump(const char *path)
+{
+  FILE *fp = fopen(path, "w");
+  if (!fp) return -1;
+  quiet(1);
+  dump(fp);
+  quiet(0);
+  fclose(fp);
+  return 0;
+}
+
 /* CPU throughput of the reference's step_ch(): warm-up steps, then timed steps */
 double ref_time_steps(int warm, int steps)
 {

@@ -18,7 +18,10 @@ files).  Fixtures hold only generated numbers:
                 tables, pressure/dpdu/dpdrho on seeded entries.
   cool_<config>.npz  step_ch() of a COOL_EOS build: states, flags, times and
                 temperature guesses after init() and steps; the restart file
-                after 5 steps; Utoprim_5d known answers.
+                after 5 steps; diag() and dump() after 12 steps with the guesses
+                they leave; Utoprim_5d known answers.
+  dump_<config>.npz  dump()'s ASCII dump after 5 steps: header line and the
+                sha256 of every zone line.
 Each configuration runs in its own process: the reference keeps its state in
 globals.
 """
@@ -215,6 +218,27 @@ def kat_u2p():
     np.savez_compressed(os.path.join(HERE, "kat_u2p.npz"), **res)
 
 
+def dump_digest(text):
+    """A dump's header line, the sha256 of every zone line and the first two lines."""
+    lines = text.split("\n")
+    assert lines[-1] == ""
+    zl = lines[1:-1]
+    return {"header": np.frombuffer(lines[0].encode(), dtype=np.uint8),
+            "sha": np.array([hashlib.sha256(l.encode()).hexdigest() for l in zl]),
+            "first": np.frombuffer("\n".join(zl[:2]).encode(), dtype=np.uint8)}
+
+
+def dump_config(cfg):
+    """dump() (the ASCII dump, dump.c:1710-2047) of the state after 5 steps."""
+    sys.path.insert(0, ROOT)
+    from oracle.pyoracle import Reference, _QuietStdout
+    ref = Reference(cfg)
+    with _QuietStdout():
+        for _ in range(5):
+            ref.step()
+    np.savez_compressed(os.path.join(HERE, "dump_%s.npz" % cfg), **dump_digest(ref.dump()))
+
+
 def eos_inputs(rng, ntab, n):
     """Seeded (table, rho0, u, T guess) entries over the run-time EOS's branches:
     table range, gamma-law below rhoMin / above rhoMax, e < 0, no guess yet
@@ -290,6 +314,10 @@ def cool_config(cfg):
     out["diag_cool_ener"] = np.array(dg["ener"])
     out["diag_cool_divb"] = np.array([dg["divbmax"]] + dg["imax"])
     out["lastT_after_diag"] = ref.cool_lastT()
+    # then dump(), which moves the guesses too
+    dd = dump_digest(ref.dump())
+    out.update({"dump_" + k: v for k, v in dd.items()})
+    out["lastT_after_dump"] = ref.cool_lastT()
     # Utoprim_5d on perturbed states of active zones, each with its own guess
     rng = np.random.default_rng(55)
     last = ref.cool_lastT()
@@ -333,6 +361,8 @@ if __name__ == "__main__":
             eos_config(sys.argv[1][len("eos_"):])
         elif sys.argv[1].startswith("cool_"):
             cool_config(sys.argv[1][len("cool_"):])
+        elif sys.argv[1].startswith("dump_"):
+            dump_config(sys.argv[1][len("dump_"):])
         else:
             one_config(sys.argv[1])
         sys.exit(0)
@@ -341,7 +371,7 @@ if __name__ == "__main__":
     for cfg in ("t2d", "t3d", "r2d", "r3d", "ce2d"):
         build_ref.build_config(cfg, force=True)
     for arg in ("t2d", "t3d", "kat", "tracers_r2d", "tracers_r3d", "diag_t2d", "diag_t3d",
-                "restart_r2d", "restart_t3d", "eos_ce2d", "cool_ce2d"):
+                "restart_r2d", "restart_t3d", "eos_ce2d", "cool_ce2d", "dump_t2d", "dump_t3d"):
         subprocess.run([sys.executable, os.path.abspath(__file__), arg], check=True,
                        stderr=subprocess.DEVNULL)
     for f in sorted(os.listdir(HERE)):
