@@ -52,9 +52,10 @@ TRACER_CONFIGS = ("r2d", "r3d")
 # bhs = 0.6, cooleos.c:103), with oracle/eos_standin.c in place of the Fortran
 # table generator
 CONFIGS["ce2d"] = (32, 32, 1, 0.6, 4.0, 11.8, 50.0)
+CONFIGS["ce3d"] = (16, 16, 4, 0.6, 4.0, 11.8, 50.0)
 # the 256x256 COOL_EOS torus, for the CPU timing beside the device step
 CONFIGS["ce256"] = (256, 256, 1, 0.6, 4.0, 11.8, 50.0)
-COOL_CONFIGS = ("ce2d", "ce256")
+COOL_CONFIGS = ("ce2d", "ce3d", "ce256")
 
 SOURCES = ["bounds", "coord", "diag", "dump", "fixup", "image", "interp", "main",
            "metric", "lu", "phys", "ranc", "restart", "step_ch", "u2p_util",

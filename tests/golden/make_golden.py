@@ -368,10 +368,10 @@ if __name__ == "__main__":
         sys.exit(0)
     sys.path.insert(0, ROOT)
     from oracle import build_ref
-    for cfg in ("t2d", "t3d", "r2d", "r3d", "ce2d"):
+    for cfg in ("t2d", "t3d", "r2d", "r3d", "ce2d", "ce3d"):
         build_ref.build_config(cfg, force=True)
     for arg in ("t2d", "t3d", "kat", "tracers_r2d", "tracers_r3d", "diag_t2d", "diag_t3d",
-                "restart_r2d", "restart_t3d", "eos_ce2d", "cool_ce2d", "dump_t2d", "dump_t3d"):
+                "restart_r2d", "restart_t3d", "eos_ce2d", "cool_ce2d", "cool_ce3d", "dump_t2d", "dump_t3d"):
         subprocess.run([sys.executable, os.path.abspath(__file__), arg], check=True,
                        stderr=subprocess.DEVNULL)
     for f in sorted(os.listdir(HERE)):

@@ -55,9 +55,10 @@ def test_dump_matches_reference(cfg, hc, tmp_path):
     ctx.close()
 
 
-def test_cool_dump_matches_reference(hc, tmp_path, oracle_built):
+@pytest.mark.parametrize("cfg", ["ce2d", "ce3d"])
+def test_cool_dump_matches_reference(cfg, hc, tmp_path, oracle_built):
     from oracle.pyoracle import standin_tables
-    fx = load_fixture("cool_ce2d")
+    fx = load_fixture("cool_" + cfg)
     T = standin_tables(float(fx["par_startx1"]), float(fx["par_dx1"]), float(fx["par_R0"]), int(fx["n"][0]) + 4,
                        float(fx["par_gam"]))
     eos = hc.Eos(T.xa, T.ya, T.val, T.consts)
