@@ -650,7 +650,7 @@ extern "C" int harm_create(const harm_params *prm, const double *gcov, const dou
     return fail_with(HARM_E_NODEV, "no CUDA device");
   cudaDeviceProp dp;
   CK(cudaGetDeviceProperties(&dp, device));
-  if (dp.major != 10) return fail_with(HARM_E_NODEV, "this build targets sm_100a (B200)");
+  if (dp.major != 10) return fail_with(HARM_E_NODEV, "the library is compiled for sm_100a (B200)");
   Dims d = make_dims(prm->n1, prm->n2, prm->n3);
   std::string why;
   if (!geometry_layout_ok(d, gcov, gcon, conn, why)) return fail_with(HARM_E_ARG, why);
