@@ -46,14 +46,10 @@ namespace cool {
 // radial index i; a zone without a guess takes its theta neighbour's
 __device__ __forceinline__ EosCursor init_cache(const Grid &G, double *lastT, int h, int i, int j)
 {
-  EosCursor c;
-  c.tab = i;
-  c.memo = false;
   const long z = cidx(G, h, i, j);
   double T = lastT[z];
   if (T == 0.0 && j > G.jstart) T = lastT[z - 1];
-  c.T = T;
-  return c;
+  return eos_cursor(i, T);
 }
 
 template <int DIR, bool F32>
@@ -373,10 +369,7 @@ __global__ void k_utoprim_5d_batch(EosDev E, const double *U, const double *gcov
   q.g = gdet[t];
   double u[8], p[8];
   for (int k = 0; k < 8; k++) { u[k] = U[t * 8 + k]; p[k] = prim[t * 8 + k]; }
-  EosCursor c;
-  c.tab = tab[t];
-  c.T = lastT[t];
-  c.memo = false;
+  EosCursor c = eos_cursor(tab[t], lastT[t]);
   ret[t] = utoprim_5d(E, c, u, q, p);
   lastT[t] = c.T;
   for (int k = 0; k < 8; k++) prim[t * 8 + k] = p[k];

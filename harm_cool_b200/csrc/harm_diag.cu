@@ -138,12 +138,9 @@ __device__ __forceinline__ void cool_zone(const Grid &G, const double *__restric
   for (int k = 0; k < 8; k++) pr[k] = __ldg(P + k * G.nc + c);
   Geo q;
   load_geo(gC, G.ng, gi, q);
-  EosCursor cur;
-  cur.tab = i;
-  cur.memo = false;
   double T = lastT[c];
   if (T == 0.0 && j > G.jstart) T = lastT[c - 1];
-  cur.T = T;
+  EosCursor cur = eos_cursor(i, T);
   State s;
   int fail = 0;
   get_state(pr, q, s, &fail);

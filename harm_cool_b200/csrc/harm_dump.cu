@@ -68,10 +68,8 @@ __device__ void dump_zone(const Grid &G, const double *__restrict__ P, const dou
   double pr[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) o[k] = pr[k] = __ldg(P + k * G.nc + c);
-  EosCursor cur;
+  EosCursor cur = eos_cursor(i, 0.0);
   if (COOL) {
-    cur.tab = i;
-    cur.memo = false;
     double T = lastT[c];
     if (T == 0.0 && j > G.jstart) T = lastT[c - 1];
     cur.T = T;

@@ -16,10 +16,7 @@ __global__ void k_eos_batch(EosDev E, int what, int f32, long n, const int *__re
 {
   const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (k >= n) return;
-  EosCursor c;
-  c.tab = tab[k];
-  c.T = lastT[k];
-  c.memo = false;
+  EosCursor c = eos_cursor(tab[k], lastT[k]);
   double r;
   if (f32) {
     if (what == HARM_EOS_PRESSURE) r = eos_pressure_f(E, c, rho0[k], u[k]);

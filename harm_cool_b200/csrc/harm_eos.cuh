@@ -48,12 +48,49 @@ struct EosDev {
   double l_unit;
 };
 
+// the cubic of interval i (akima.c:115-135): its left node, value, slope and
+// the two higher coefficients
+struct AkimaCubic {
+  double xi, yi, si, c1, c2;
+  __device__ __forceinline__ double at(double t) const
+  {
+    const double u = t - xi;
+    return yi + si * u + c1 * u * u + c2 * u * u * u;
+  }
+};
+
+// The T-direction cubics of one value plane's window, one per rho row, kept
+// while the window (table, rho window, T window) and each row's interval stay
+// the same: a cubic depends on nothing else, so a kept one is the one the
+// reference forms again.
+struct AkimaRowCache {
+  int tab, x0, y0, sx, sy;  // tab < 0: empty
+  int iv[4];                // each row's interval (-1: none kept)
+  AkimaCubic c[4];
+};
+
 struct EosCursor {
   int tab;          // radial index of the table (cacheT[i])
   double T;         // the zone's temperature guess (*LastT)
   bool memo, m_f32;
   double m_rho, m_u, m_p, m_T;
+  bool keep;             // keep cubics between evaluations
+  AkimaRowCache ce, cp;  // cubics of the e and p windows last used
 };
+
+// a cursor on table tab with guess T, nothing remembered
+__device__ __forceinline__ EosCursor eos_cursor(int tab, double T, bool keep = true)
+{
+  EosCursor c;
+  c.tab = tab;
+  c.T = T;
+  c.memo = false;
+  c.m_f32 = false;
+  c.keep = keep;
+  c.ce.tab = -1;
+  c.cp.tab = -1;
+  return c;
+}
 
 __device__ __forceinline__ bool same_bits(double a, double b)
 {
@@ -120,17 +157,6 @@ __device__ __forceinline__ int akima_interval(const double *x, double t)
   return i;
 }
 
-// the cubic of interval i (akima.c:115-135): its left node, value, slope and
-// the two higher coefficients
-struct AkimaCubic {
-  double xi, yi, si, c1, c2;
-  __device__ __forceinline__ double at(double t) const
-  {
-    const double u = t - xi;
-    return yi + si * u + c1 * u * u + c2 * u * u * u;
-  }
-};
-
 template <int SI>
 __device__ __forceinline__ AkimaCubic akima_cubic(const double *x, const double *y, const double *mm, int i)
 {
@@ -173,25 +199,61 @@ __device__ __forceinline__ void akima_window(const double *x, const double *y, d
 }
 
 // getvalues at (rho, T) for one value plane: Akima along T on each rho row of
-// the window, then along rho (cache4d.c:1086-1127)
+// the window, then along rho (cache4d.c:1086-1127).  With a cache, a row whose
+// T-interval is the one kept reuses its cubic.
 template <int SX, int SY, bool DER>
-__device__ __noinline__ void eos_value_w(const EosDev &E, const double *__restrict__ plane, int x0, int y0, double rho,
-                                         double T, double &val, double &der)
+__device__ __noinline__ void eos_value_w(const EosDev &E, const double *__restrict__ plane, int tab, int x0, int y0,
+                                         double rho, double T, double &val, double &der, AkimaRowCache *cache)
 {
   double xw[SX], yw[SY], row[SX], rowd[SX];
 #pragma unroll
   for (int k = 0; k < SX; k++) xw[k] = __ldg(E.xa + x0 + k);
 #pragma unroll
   for (int k = 0; k < SY; k++) yw[k] = __ldg(E.ya + y0 + k);
+  if (cache && !(cache->tab == tab && cache->x0 == x0 && cache->y0 == y0 && cache->sx == SX && cache->sy == SY)) {
+    cache->tab = tab;
+    cache->x0 = x0;
+    cache->y0 = y0;
+    cache->sx = SX;
+    cache->sy = SY;
+#pragma unroll
+    for (int r = 0; r < 4; r++) cache->iv[r] = -1;
+  }
+  const int i = akima_interval<SY>(yw, T);
+  // spline_akima_der's points (akima.c:259-298)
+  const double h = T * 1.0E-6;
+  const double tm = T - h, tp = T + h;
+  const int im = DER ? akima_interval<SY>(yw, tm) : i, ip = DER ? akima_interval<SY>(yw, tp) : i;
 #pragma unroll
   for (int r = 0; r < SX; r++) {
     const double *src = plane + (long)(x0 + r) * E.ny + y0;
-    double ys[SY];
+    double ys[SY], mm[SY + 3];
+    bool have = false;
+    AkimaCubic c;
+    if (cache && cache->iv[r] == i) {
+      c = cache->c[r];
+    } else {
 #pragma unroll
-    for (int k = 0; k < SY; k++) ys[k] = __ldg(src + k);
-    double d = 0.;
-    akima_window<SY, DER>(yw, ys, T, row[r], d);
-    rowd[r] = d;
+      for (int k = 0; k < SY; k++) ys[k] = __ldg(src + k);
+      akima_slopes<SY>(yw, ys, mm);
+      have = true;
+      c = akima_cubic<SY>(yw, ys, mm, i);
+      if (cache) {
+        cache->c[r] = c;
+        cache->iv[r] = i;
+      }
+    }
+    row[r] = c.at(T);
+    if (DER) {
+      if ((im != i || ip != i) && !have) {
+#pragma unroll
+        for (int k = 0; k < SY; k++) ys[k] = __ldg(src + k);
+        akima_slopes<SY>(yw, ys, mm);
+      }
+      const double vm = im == i ? c.at(tm) : akima_cubic<SY>(yw, ys, mm, im).at(tm);
+      const double vp = ip == i ? c.at(tp) : akima_cubic<SY>(yw, ys, mm, ip).at(tp);
+      rowd[r] = (vp - vm) / (2.0 * h);
+    }
   }
   double unused;
   akima_window<SX, false>(xw, row, rho, val, unused);
@@ -202,18 +264,18 @@ __device__ __noinline__ void eos_value_w(const EosDev &E, const double *__restri
 // without writing its outputs, cache4d.c:899-911)
 template <bool DER>
 __device__ __forceinline__ bool eos_value(const EosDev &E, int tab, int d, double rho, int x0, int sx, double T,
-                                          double &val, double &der)
+                                          double &val, double &der, AkimaRowCache *cache = nullptr)
 {
   if (!(T >= __ldg(E.ya)) || !(T <= __ldg(E.ya + E.ny - 1))) return false;
   int y0, sy;
   eos_window(E.ny, E.ya, T, y0, sy);
   const double *plane = E.val + ((long)d * E.ntab + tab) * E.nx * E.ny;
   if (sx == 4) {
-    if (sy == 4) eos_value_w<4, 4, DER>(E, plane, x0, y0, rho, T, val, der);
-    else eos_value_w<4, 3, DER>(E, plane, x0, y0, rho, T, val, der);
+    if (sy == 4) eos_value_w<4, 4, DER>(E, plane, tab, x0, y0, rho, T, val, der, cache);
+    else eos_value_w<4, 3, DER>(E, plane, tab, x0, y0, rho, T, val, der, cache);
   } else {
-    if (sy == 4) eos_value_w<3, 4, DER>(E, plane, x0, y0, rho, T, val, der);
-    else eos_value_w<3, 3, DER>(E, plane, x0, y0, rho, T, val, der);
+    if (sy == 4) eos_value_w<3, 4, DER>(E, plane, tab, x0, y0, rho, T, val, der, cache);
+    else eos_value_w<3, 3, DER>(E, plane, tab, x0, y0, rho, T, val, der, cache);
   }
   return true;
 }
@@ -227,14 +289,14 @@ __device__ __forceinline__ bool eos_rho_window(const EosDev &E, double rho, int 
 
 // mnewtc<1>(300, x, 1e-6, minx, maxx) on (e - e(rho, T)) / e; returns berr
 static __device__ __noinline__ double eos_newton_T(const EosDev &E, int tab, double rho, bool rho_in, int x0, int sx,
-                                            double e, double &x, double minx, double maxx)
+                                            double e, double &x, double minx, double maxx, AkimaRowCache *ce)
 {
   double best = x, besterr = 1.0E100;
   for (int k = 1; k <= 300; k++) {
     double ecur = CUDART_NAN, dcur = CUDART_NAN;
     if (rho_in) {
       double v, dv;
-      if (eos_value<true>(E, tab, EOS_E, rho, x0, sx, x, v, dv)) { ecur = v; dcur = dv; }
+      if (eos_value<true>(E, tab, EOS_E, rho, x0, sx, x, v, dv, ce)) { ecur = v; dcur = dv; }
     }
     const double F = (e - ecur) / e;
     const double D = -dcur / e;
@@ -274,13 +336,13 @@ static __device__ __noinline__ double eos_pressure(const EosDev &E, EosCursor &c
     int x0 = 0, sx = 4;
     const bool rho_in = eos_rho_window(E, rho, x0, sx);
     double x = c.T;
-    const double berr = eos_newton_T(E, c.tab, rho, rho_in, x0, sx, e, x, minx, maxx);
+    const double berr = eos_newton_T(E, c.tab, rho, rho_in, x0, sx, e, x, minx, maxx, c.keep ? &c.ce : nullptr);
     if (berr > 1.0E-6) p = (E.gam - 1.) * u;
     else {
       double v = CUDART_NAN, unused;
       if (rho_in) {
         double w;
-        if (eos_value<false>(E, c.tab, EOS_P, rho, x0, sx, x, w, unused)) v = w;
+        if (eos_value<false>(E, c.tab, EOS_P, rho, x0, sx, x, w, unused, c.keep ? &c.cp : nullptr)) v = w;
       }
       c.T = x;
       p = v / E.p_unit;
@@ -324,7 +386,7 @@ static __device__ __noinline__ void eos_coolval(const EosDev &E, EosCursor &c, d
     const double minx = E.t_min * (1.0 + hh), maxx = E.t_max * (1.0 - hh);
     rho_in = eos_rho_window(E, rho, x0, sx);
     x = c.T;
-    const double berr = eos_newton_T(E, c.tab, rho, rho_in, x0, sx, e, x, minx, maxx);
+    const double berr = eos_newton_T(E, c.tab, rho, rho_in, x0, sx, e, x, minx, maxx, c.keep ? &c.ce : nullptr);
     gamma_law = berr > 1.0E-6;
   }
   c.memo = false;
