@@ -251,14 +251,18 @@ __device__ __forceinline__ float newton_step_f(float GAMMA, float Bsq, float Qdo
 // The 2D Newton solve of the mixed path: Newton steps in float from the
 // reference's starting point until the relative step falls below 1e-5, then
 // FP64 Newton steps (the residual and Jacobian of func_vsq, the reference's
-// validate_x clamps) until it falls below NEWT_TOL.  Falls back to the FP64
-// solve from the start when the float phase leaves the finite range.
+// validate_x clamps) until it falls below NEWT_TOL.  When the float phase
+// converged and the first FP64 step is itself below 1e-5 -- it confirms the
+// float answer to that accuracy, and a Newton step from there squares the
+// error -- that step ends the solve.  Falls back to the FP64 solve from the
+// start when the float phase leaves the finite range.
 __device__ __forceinline__ int gnr_2d_mixed(const U2P &c, double *x)
 {
   float W = (float)x[0], vsq = (float)x[1];
   const float G = (float)c.gam, Bsq = (float)c.Bsq, QB = (float)c.QdotBsq, Qt = (float)c.Qtsq, Qn = (float)c.Qdotn,
               D = (float)c.D;
   bool ok = isfinite(W) && isfinite(vsq) && W > 0.f;
+  bool f32_conv = false;
   for (int n = 0; n < MAX_NEWT_ITER && ok; n++) {
     float dW, dv;
     newton_step_f(G, Bsq, QB, Qt, Qn, D, W, vsq, dW, dv);
@@ -272,7 +276,10 @@ __device__ __forceinline__ int gnr_2d_mixed(const U2P &c, double *x)
     vsq = vsq < 0.f ? 0.f : vsq;
     vsq = vsq > 1.f ? 1.f - 1.e-7f : vsq;
     ok = isfinite(W) && isfinite(vsq) && W > 0.f;
-    if (errx <= F32_NEWT_TOL) break;
+    if (errx <= F32_NEWT_TOL) {
+      f32_conv = ok;
+      break;
+    }
   }
   if (ok) {
     x[0] = (double)W;
@@ -291,6 +298,10 @@ __device__ __forceinline__ int gnr_2d_mixed(const U2P &c, double *x)
     x[1] = (x[1] < 0.) ? 0. : x[1];
     x[1] = (x[1] > 1.) ? (1. - 1.e-15) : x[1];
     if (fabs(errx) <= NEWT_TOL) break;
+    if (n == 0 && f32_conv && errx <= (double)F32_NEWT_TOL) {
+      errx = 0.;
+      break;
+    }
   }
   if (!isfinite(f) || !isfinite(df)) return 2;
   if (fabs(errx) > MIN_NEWT_TOL) return 1;
