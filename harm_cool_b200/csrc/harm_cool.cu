@@ -2,8 +2,9 @@
 // pressure in the face fluxes, wave speeds, source and primtoU, and Utoprim_5d
 // in place of Utoprim_2d and its isentropic fall-backs (step_ch.c:241-300,
 // 437-441).  FP64, built with -fmad=false: the reference's results bit for bit.
-// In mixed precision the face fluxes' and wave speeds' EOS calls interpolate
-// and solve in FP32; the update (source, primtoU, Utoprim_5d) stays FP64.
+// In mixed precision the EOS calls of the face fluxes, the wave speeds, the
+// source and primtoU interpolate and solve in FP32; Utoprim_5d, whose 5D Newton
+// needs its pressure to 1e-10, stays FP64, as does all other arithmetic.
 //
 // The temperature guess of each zone (_aLastT[SN3][SN1][SN2], cooleos.c:69,
 // 836) lives in Ctx::lastT.  The reference runs its loops one zone after
@@ -204,13 +205,14 @@ void launch_flux_cool(Ctx *x, const double *pb, bool rows)
 }
 
 // source() with COOL_EOS (phys.c:165-207)
+template <bool F32>
 __device__ __noinline__ void source_cool(const EosDev &E, EosCursor &c, const double *pb, const State &s, const Geo &q,
                                          const double *__restrict__ conn, long ng, long gi, double *dU)
 {
   double mhd[4][4];
   {
     const double rho = pb[RHO], u = pb[UU];
-    const double p = eos_pressure(E, c, rho, u);
+    const double p = face_pressure<F32>(E, c, rho, u);
 #pragma unroll
     for (int d = 0; d < 4; d++) mhd_calc_cool(rho, u, p, d, s, mhd[d]);
   }
@@ -230,8 +232,10 @@ __device__ __noinline__ void source_cool(const EosDev &E, EosCursor &c, const do
 }
 
 // the update's first half (step_ch.c:241-263): source(pb), primtoU(pi) and the
-// flux divergence, with flux-CT and the flux boundary fixes, into Ub
-template <bool FULL, bool THREE_D>
+// flux divergence, with flux-CT and the flux boundary fixes, into Ub.  F32 (mixed
+// precision): the source's and primtoU's pressures from the FP32 interpolation
+// (all else FP64, the accumulation of U included)
+template <bool FULL, bool THREE_D, bool F32>
 __global__ void __launch_bounds__(128, HARM_COOL_CONS_MINB) k_cons_cool(Grid G, const double *__restrict__ pi, const double *__restrict__ pb,
                                                    const double *__restrict__ F1, const double *__restrict__ F2,
                                                    const double *__restrict__ F3, const double *__restrict__ geo,
@@ -257,7 +261,7 @@ __global__ void __launch_bounds__(128, HARM_COOL_CONS_MINB) k_cons_cool(Grid G, 
     for (int k = 0; k < 8; k++) pbz[k] = pb[k * G.nc + c];
     State s;
     get_state(pbz, q, s, &fail);
-    source_cool(E, cur, pbz, s, q, conn, G.ng, gi, dU);
+    source_cool<F32>(E, cur, pbz, s, q, conn, G.ng, gi, dU);
   }
   {
     double pz[8];
@@ -265,7 +269,7 @@ __global__ void __launch_bounds__(128, HARM_COOL_CONS_MINB) k_cons_cool(Grid G, 
     for (int k = 0; k < 8; k++) pz[k] = pi[k * G.nc + c];
     State s;
     get_state(pz, q, s, &fail);
-    primtoflux_cool(E, cur, pz, s, 0, q.g, U);
+    primtoflux_cool<F32>(E, cur, pz, s, 0, q.g, U);
   }
   lastT[c] = cur.T;
   {
@@ -320,6 +324,26 @@ __global__ void __launch_bounds__(128, HARM_COOL_INV_MINB) k_invert_cool(Grid G,
   if (fail) record_fail(sc, fail, h + (G.n3 > 1 ? 1 : 0), i, j);
 }
 
+template <bool FULL, bool THREE_D, bool F32>
+void launch_cons_cool_p(Ctx *x, const double *pi, const double *pb, dim3 zg, dim3 tile)
+{
+  k_cons_cool<FULL, THREE_D, F32><<<zg, tile, 0, x->stream>>>(x->G, pi, pb, x->F1, x->F2, x->F3, x->geo, x->conn,
+                                                              x->eos, x->lastT, x->Ubuf, x->sc);
+}
+
+template <bool FULL>
+void launch_cons_cool(Ctx *x, const double *pi, const double *pb, dim3 zg, dim3 tile)
+{
+  const bool f32 = x->mode == HARM_MIXED;
+  if (x->G.n3 > 1) {
+    if (f32) launch_cons_cool_p<FULL, true, true>(x, pi, pb, zg, tile);
+    else launch_cons_cool_p<FULL, true, false>(x, pi, pb, zg, tile);
+  } else {
+    if (f32) launch_cons_cool_p<FULL, false, true>(x, pi, pb, zg, tile);
+    else launch_cons_cool_p<FULL, false, false>(x, pi, pb, zg, tile);
+  }
+}
+
 template <bool FULL>
 void launch_half(Ctx *x, const double *pi, const double *pb, double *pf, bool rows)
 {
@@ -327,12 +351,7 @@ void launch_half(Ctx *x, const double *pi, const double *pb, double *pf, bool ro
   launch_flux_cool<FULL>(x, pb, rows);
   const dim3 tile(x->tbx, x->tby);
   const dim3 zg((G.n2 + tile.x - 1) / tile.x, (G.n1 + tile.y - 1) / tile.y, G.n3);
-  if (G.n3 > 1)
-    k_cons_cool<FULL, true><<<zg, tile, 0, x->stream>>>(G, pi, pb, x->F1, x->F2, x->F3, x->geo, x->conn, x->eos,
-                                                        x->lastT, x->Ubuf, x->sc);
-  else
-    k_cons_cool<FULL, false><<<zg, tile, 0, x->stream>>>(G, pi, pb, x->F1, x->F2, x->F3, x->geo, x->conn, x->eos,
-                                                         x->lastT, x->Ubuf, x->sc);
+  launch_cons_cool<FULL>(x, pi, pb, zg, tile);
   k_invert_cool<<<zg, tile, 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->eos, x->lastT,
                                             x->sc);
   if (FULL) k_diag_flux<<<1, 1024, 0, x->stream>>>(G, x->F1, x->sc);
@@ -496,13 +515,8 @@ int cool_time_kernels(Ctx *x, int reps, double *ms)
       if (full) cool::launch_flux_cool<true>(x, pb, false);
       else cool::launch_flux_cool<false>(x, pb, false);
       slot[e] = 0; CK(cudaEventRecord(ev[e++], x->stream));
-      if (G.n3 > 1) {
-        if (full) cool::k_cons_cool<true, true><<<zg, tile, 0, x->stream>>>(G, pi, pb, x->F1, x->F2, x->F3, x->geo, x->conn, x->eos, x->lastT, x->Ubuf, x->sc);
-        else cool::k_cons_cool<false, true><<<zg, tile, 0, x->stream>>>(G, pi, pb, x->F1, x->F2, x->F3, x->geo, x->conn, x->eos, x->lastT, x->Ubuf, x->sc);
-      } else {
-        if (full) cool::k_cons_cool<true, false><<<zg, tile, 0, x->stream>>>(G, pi, pb, x->F1, x->F2, x->F3, x->geo, x->conn, x->eos, x->lastT, x->Ubuf, x->sc);
-        else cool::k_cons_cool<false, false><<<zg, tile, 0, x->stream>>>(G, pi, pb, x->F1, x->F2, x->F3, x->geo, x->conn, x->eos, x->lastT, x->Ubuf, x->sc);
-      }
+      if (full) cool::launch_cons_cool<true>(x, pi, pb, zg, tile);
+      else cool::launch_cons_cool<false>(x, pi, pb, zg, tile);
       cool::k_invert_cool<<<zg, tile, 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->eos,
                                                       x->lastT, x->sc);
       slot[e] = 1; CK(cudaEventRecord(ev[e++], x->stream));
