@@ -513,6 +513,7 @@ __global__ void k_utoprim_batch(const double *U, const double *gcov, const doubl
   q.v00 = a[0]; q.v01 = a[1]; q.v03 = a[3]; q.v11 = a[5]; q.v13 = a[7]; q.v22 = a[10]; q.v33 = a[15];
   q.n00 = b[0]; q.n01 = b[1]; q.n03 = b[3]; q.n10 = b[4]; q.n11 = b[5]; q.n13 = b[7]; q.n22 = b[10];
   q.n30 = b[12]; q.n31 = b[13]; q.n33 = b[15];
+  q.alpha = 1. / sqrt(-q.n00);
   q.g = gdet[t];
   double u[8], p[8];
   for (int k = 0; k < 8; k++) { u[k] = U[t * 8 + k]; p[k] = prim[t * 8 + k]; }
@@ -711,7 +712,7 @@ extern "C" int harm_create(const harm_params *prm, const double *gcov, const dou
       const double *a = gcov + (c * 5 + locs[L]) * 16, *b = gcon + (c * 5 + locs[L]) * 16;
       const double vals[GEO_N] = {a[0], a[1], a[3], a[5], a[7], a[10], a[15],
                                   b[0], b[1], b[3], b[4], b[5], b[7], b[10], b[12], b[13], b[15],
-                                  gdet[c * 5 + locs[L]]};
+                                  gdet[c * 5 + locs[L]], 1. / sqrt(-b[0])};
       for (int e = 0; e < GEO_N; e++) hg[((size_t)L * GEO_N + e) * G.ng + c] = vals[e];
     }
   for (long c = 0; c < G.ng; c++)

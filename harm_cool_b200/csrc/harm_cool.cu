@@ -385,6 +385,7 @@ __global__ void k_utoprim_5d_batch(EosDev E, const double *U, const double *gcov
   q.v00 = a[0]; q.v01 = a[1]; q.v03 = a[3]; q.v11 = a[5]; q.v13 = a[7]; q.v22 = a[10]; q.v33 = a[15];
   q.n00 = b[0]; q.n01 = b[1]; q.n03 = b[3]; q.n10 = b[4]; q.n11 = b[5]; q.n13 = b[7]; q.n22 = b[10];
   q.n30 = b[12]; q.n31 = b[13]; q.n33 = b[15];
+  q.alpha = 1. / sqrt(-q.n00);
   q.g = gdet[t];
   double u[8], p[8];
   for (int k = 0; k < 8; k++) { u[k] = U[t * 8 + k]; p[k] = prim[t * 8 + k]; }

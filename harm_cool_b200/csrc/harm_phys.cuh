@@ -35,8 +35,9 @@ struct Geo {
   double v00, v01, v03, v11, v13, v22, v33;                      // gcov
   double n00, n01, n03, n10, n11, n13, n22, n30, n31, n33;       // gcon
   double g;                                                      // sqrt(-det g)
+  double alpha;  // 1/sqrt(-g^tt), as ucon_calc and the inversion form it (phys.c:238)
 };
-constexpr int GEO_N = 18;
+constexpr int GEO_N = 19;
 
 // geometry planes: [GEO_N][ng], entry e of point gi at G[e*ng + gi]
 __device__ __forceinline__ void load_geo(const double *__restrict__ G, long ng, long gi, Geo &q)
@@ -48,6 +49,7 @@ __device__ __forceinline__ void load_geo(const double *__restrict__ G, long ng, 
   q.n10 = __ldg(G + 10 * ng + gi); q.n11 = __ldg(G + 11 * ng + gi); q.n13 = __ldg(G + 12 * ng + gi);
   q.n22 = __ldg(G + 13 * ng + gi); q.n30 = __ldg(G + 14 * ng + gi); q.n31 = __ldg(G + 15 * ng + gi);
   q.n33 = __ldg(G + 16 * ng + gi); q.g = __ldg(G + 17 * ng + gi);
+  q.alpha = __ldg(G + 18 * ng + gi);
 }
 
 struct State {
@@ -84,7 +86,7 @@ __device__ __forceinline__ int gamma_calc(const double *pr, const Geo &q, double
 // ucon_calc() (phys.c:232-252); sets *fail on a gamma failure
 __device__ __forceinline__ void ucon_calc(const double *pr, const Geo &q, double *ucon, int *fail)
 {
-  double alpha = 1. / sqrt(-q.n00);
+  const double alpha = q.alpha;
   double b1 = q.n01 * alpha * alpha, b2 = 0. * alpha * alpha, b3 = q.n03 * alpha * alpha;
   double gamma;
   if (gamma_calc(pr, q, gamma)) *fail = FAIL_GAMMA;
@@ -586,7 +588,7 @@ __device__ __forceinline__ int utoprim(double gam, double K, const double *U, co
   prim[B2] = U[B2] / q.g;
   prim[B3] = U[B3] / q.g;
   if (U[0] <= 0.) return -100;
-  double alpha = 1.0 / sqrt(-q.n00);
+  const double alpha = q.alpha;
   Ut[RHO] = alpha * U[RHO] / q.g;
   Ut[UU] = alpha * (U[UU] - U[RHO]) / q.g;
 #pragma unroll
@@ -670,7 +672,7 @@ static __device__ bool fixup1zone(double gam, double rhoflr, double uuflr, const
 #pragma unroll
     for (int k = 0; k < 4; k++) ucon[k] = ut * vcon[k];
     // ucon_to_utcon (phys.c:255-270)
-    double alpha = 1. / sqrt(-q.n00);
+    const double alpha = q.alpha;
     double gm = alpha * ucon[0];
     double be[4] = {0., q.n01 * alpha * alpha, 0. * alpha * alpha, q.n03 * alpha * alpha};
 #pragma unroll
@@ -701,7 +703,7 @@ __device__ __forceinline__ void inflow_check(double *pr, const Geo &q, int type,
     pr[U1] /= gamma;
     pr[U2] /= gamma;
     pr[U3] /= gamma;
-    double alpha = 1. / sqrt(-q.n00);
+    const double alpha = q.alpha;
     double beta1 = q.n01 * alpha * alpha;
     pr[U1] = beta1 / alpha;
     double a = pr[U1], b = pr[U2], d = pr[U3];
