@@ -9,8 +9,11 @@ other source file where it lies in the reference tree.  The `-I-` option
 makes `#include "decs.h"` resolve to the patched copy instead of the file
 next to the including source.
 
-Switches: COOL_EOS 0 (the Fortran table generator needs gfortran, absent
-here), TRACERSDUMP 0, HDFDUMP 0 (no HDF5).  MPI_USED is on and the
+Switches: COOL_EOS 0 except in the COOL_EOS configurations, which compile the
+reference's run-time EOS (cooleos.c, cache4d.c, akima.c) with oracle/eos_standin.c
+in place of the Fortran table generator (gfortran is absent here), the table fill
+in this process and the cache files turned off; TRACERSDUMP 0 except in the
+tracer configurations; HDFDUMP 0 (no HDF5).  MPI_USED is on and the
 single-rank stand-in in oracle/fakempi provides MPI: with one rank the phi
 periodicity and opposite-phi polar ghosts are MPI self-exchanges
 (step_ch.c:189-198, bounds.c:161-275).  Floating point: SSE2, -O2 (the
