@@ -118,3 +118,18 @@ def test_device_eos_fp32_against_fp64_oracle(dev, tables):
     # the temperatures agree to the solve tolerance
     trel = np.abs(la[both] / lb[both] - 1.)
     assert trel.max() <= 1e-4, trel.max()
+
+
+def test_fp32_refused_for_tables_beyond_float_range(harm_lib, tables):
+    """Values spanning more than float's exponent range: the FP64 path still
+    serves them, the FP32 path is refused (no silent overflow)."""
+    import harm_cool_b200 as hc
+    T, _ = tables
+    v = T.val.copy()
+    v[0, 0, 0, 0] = 1e-300        # e spans far more than 2^240
+    e = hc.Eos(T.xa, T.ya, v, T.consts)
+    a, _ = e.batch("pressure", [5], [1.0], [1e-2], [0.0])
+    assert np.isfinite(a).all()
+    with pytest.raises(hc.HarmError):
+        e.batch("pressure", [5], [1.0], [1e-2], [0.0], mixed=True)
+    e.close()
