@@ -126,6 +126,7 @@ _SIGNATURES = {
     "harm_step_ch_host": (ctypes.c_int, [ctypes.c_void_p, _DP]),
     "harm_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "harm_run_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _DP]),
+    "harm_adjoint_mass_in": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _DP, _DP, _DP]),
     "harm_step_ch_host_timed": (ctypes.c_int, [ctypes.c_void_p, _DP, ctypes.c_int, _DP]),
     "harm_time_kernels": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _DP]),
     "harm_fixup": (ctypes.c_int, [ctypes.c_void_p, _DP]),
@@ -505,6 +506,18 @@ class Context:
         for k, v in fields.items():
             setattr(hd, k, v)
         _check(self.lib.harm_dump_write(self.h, ctypes.byref(hd), ctypes.byref(pr.grid), path.encode()))
+
+    def adjoint_mass_in(self, nsteps, checkpoint_every=10):
+        """Discrete adjoint of nsteps steps (2D gamma-law FP64 step): runs them from
+        the current state and returns (J, grad, ms) -- J the mass that crossed the
+        inner boundary (the change of mass_in, diag.c:578), grad = dJ/dp of the state
+        at the call in get_prims' layout, ms the device time of the forward pass and
+        of the reverse sweep."""
+        J = ctypes.c_double()
+        grad = np.zeros(self.shape + (NPR,))
+        ms = (ctypes.c_double * 2)()
+        _check(self.lib.harm_adjoint_mass_in(self.h, nsteps, checkpoint_every, ctypes.byref(J), _dp(grad), ms))
+        return J.value, grad, (ms[0], ms[1])
 
     def restart_read(self, path):
         """restart_init(): state, time, mass counters and tracers from a restart file."""

@@ -42,6 +42,7 @@ UNITS = {
     "harm_eos.cu": ["-fmad=false"],      # run-time COOL_EOS tables and batch calls
     "harm_cool.cu": ["-fmad=false"],     # the COOL_EOS step and Utoprim_5d
     "harm_dump.cu": ["-fmad=false"],     # the ASCII dump format
+    "harm_adjoint.cu": ["-fmad=false"],  # the discrete adjoint (values identical to the step's)
 }
 
 

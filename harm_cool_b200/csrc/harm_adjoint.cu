@@ -1,0 +1,807 @@
+// Discrete adjoint of K steps of step_ch() (2D, gamma-law, FP64).
+//
+// Objective: the mass that crosses the inner radial boundary during the K
+// steps, J = sum_n dt^n din^n -- the reference's mass_in (diag.c:578,
+// mass_in += mdot_in*Dt), din^n = sum_j rho u^1 sqrt(-g) dx2 dx3 over the
+// inner ghost row of the step's result (diag_mass, MDOTTYPE NEU_AGA_GHOST1,
+// diag.c:486-515).  Output: dJ/dp of the state the K steps start from, every
+// cell of every primitive (ghost cells included, since the first step's
+// stencils read them).
+//
+// Method.  The state p^n of every checkpoint_every-th step is kept on a forward
+// pass; the reverse sweep recomputes each segment from its checkpoint with the
+// step's own kernels (exact::launch_step_rec), keeping the intermediates of
+// every step (StepRec), and then walks the steps backwards.  Each part of a
+// step is transposed where it is linear (flux-CT averaging, the flux
+// divergence, bound_prim copies, fixup_utoprim stencils) and linearised with
+// forward-mode dual numbers (harm_dual.cuh) where it is not: the limited face
+// states and the Lax-Friedrichs flux (limiter branches and the wave-speed
+// choice frozen at the forward's), primtoU, the connection source, fixup()
+// floors and inflow_check().  The inversion is differentiated through its
+// converged solution by the implicit-function theorem: Utoprim_2d returns the
+// z with primtoU(z) = U, so dz/dU = (dprimtoU/dz)^-1; the isentropic
+// fall-backs replace the energy row by their constraint u = K rho^gam/(gam-1).
+// A zone whose inversion failed keeps its guess (the step's p^n) and U[B]/gdet.
+// The time step is part of the chain: dt^{n+1} = min(ndt, 1.3 dt^n) with
+// ndt = defcon/(1/n1 + 1/n2) and n_d the Courant minimum over the corrector's
+// faces (step_ch.c:126-137, 477-484), so the face that set each minimum gets
+// the adjoint of its wave speed.
+//
+// Every kernel of the reverse sweep reads recorded values only; the values
+// the dual numbers carry are the step's own (the same IEEE operations), so
+// every branch the linearisation takes is the branch the step took.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "harm_common.cuh"
+#include "harm_bound.cuh"
+#include "harm_dual.cuh"
+
+namespace harm {
+namespace adj {
+
+constexpr int NWF = 4;  // tangent directions per pass of a face flux (16 inputs: 4 passes)
+constexpr int FU_THREADS = 1024;
+enum { ERR_FAILS = 1, ERR_SINGULAR = 2 };
+
+using D8 = Dual<8>;
+
+// ---------------------------------------------------------------------------
+// objective: dt^n * din^n on the inner ghost row of p^{n+1} (diag.c:499)
+
+__global__ void k_adj_din(Grid G, const double *__restrict__ P, const double *__restrict__ geo, double *lam, double w)
+{
+  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > G.jstop) return;
+  const int i = G.istart - 1;
+  const long c = cidx(G, 0, i, j);
+  D8 pr[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) pr[k] = D8::seed(P[k * G.nc + c], k);
+  Geo q;
+  load_geo(geo_at(geo, G, L_CENT), G.ng, (long)i * G.sn2 + j, q);
+  D8 ucon[4];
+  int fail = 0;
+  ucon_calc(pr, q, ucon, &fail);
+  D8 term = pr[RHO] * ucon[1] * q.g * G.dx2 * G.dx3;
+#pragma unroll
+  for (int k = 0; k < 8; k++) lam[k * G.nc + c] += w * term.d[k];
+}
+
+// ---------------------------------------------------------------------------
+// bound_prim (bounds.c:54-331) transposed: each ghost cell's adjoint goes to
+// the active cell it was copied from, through the sign flips and
+// inflow_check(); the ghost's own adjoint ends (its old value was overwritten).
+// X holds the values bound_prim copied (its active cells).
+
+__global__ void k_adj_bound(Grid G, const double *__restrict__ X, const double *__restrict__ geo, double *lam)
+{
+  const int ncell = 4 * G.sn2 + 4 * (G.sn1 - 4);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncell) return;
+  BoundCell b = bound_cell(G, t, 4);
+  const int i = b.i, j = b.j;
+  const bool rghost = i < G.istart || i > G.istop;
+  const int ci = i < G.istart ? G.istart : (i > G.istop ? G.istop : i);
+  int js = j;
+  bool flip = false;
+  if (j >= G.jstart && j <= G.jstop) {
+    if (!rghost) return;
+  } else {
+    const bool low = j < G.jstart;
+    js = low ? (j == G.jstart - 1 ? G.jstart : G.jstart + 1) : (j == G.jstop + 1 ? G.jstop : G.jstop - 1);
+    flip = true;
+  }
+  const long c = cidx(G, 0, i, j), cs = cidx(G, 0, ci, js);
+  double lg[8], lv[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    lg[k] = lam[k * G.nc + c];
+    lam[k * G.nc + c] = 0.;
+  }
+  if (rghost) {
+    D8 v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      double s = X[k * G.nc + cs];
+      if (flip && (k == U2 || k == B2)) s *= -1.;
+      v[k] = D8::seed(s, k);
+    }
+    Geo q;
+    load_geo(geo_at(geo, G, L_CENT), G.ng, (long)i * G.sn2 + j, q);
+    int fail = 0;
+    inflow_check(v, q, i < G.istart ? 0 : 1, &fail);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      double s = 0.;
+#pragma unroll
+      for (int o = 0; o < 8; o++) s += lg[o] * v[o].d[k];
+      lv[k] = s;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 8; k++) lv[k] = lg[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    double s = (flip && (k == U2 || k == B2)) ? -lv[k] : lv[k];
+    if (s != 0.) atomicAdd(&lam[k * G.nc + cs], s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// fixup_utoprim (fixup.c:432-538) transposed.  One block: the failed zones of
+// the half step (pflag != 0 after the first bound_prim) are listed in loop
+// order, the repairs are replayed on a working copy exactly as the step made
+// them (each stencil chosen from the flags as earlier repairs left them), and
+// then undone in reverse order, so a last-resort average that read an earlier
+// repair passes its adjoint on to that repair's stencil.
+
+__global__ void __launch_bounds__(FU_THREADS) k_adj_fixup_utoprim(Grid G, const double *__restrict__ X1,
+                                                                  const signed char *__restrict__ fl1,
+                                                                  const double *__restrict__ geo,
+                                                                  const double *__restrict__ floors, double *W,
+                                                                  signed char *Wf, int *list, double *vbuf,
+                                                                  signed char *kinds, double *lam, int *err)
+{
+  __shared__ int cnt[FU_THREADS];
+  __shared__ int nsh;
+  const int tid = threadIdx.x;
+  const long nact = (long)G.n1 * G.n2;
+  const long per = (nact + FU_THREADS - 1) / FU_THREADS;
+  const long a0 = tid * per, a1 = a0 + per < nact ? a0 + per : nact;
+  int m = 0;
+  for (long t = a0; t < a1; t++) {
+    const int i = G.istart + (int)(t / G.n2), j = G.jstart + (int)(t % G.n2);
+    if (fl1[cidx(G, 0, i, j)] != 0) m++;
+  }
+  cnt[tid] = m;
+  __syncthreads();
+  if (tid == 0) {
+    int s = 0;
+    for (int k = 0; k < FU_THREADS; k++) {
+      const int v = cnt[k];
+      cnt[k] = s;
+      s += v;
+    }
+    nsh = s;
+  }
+  __syncthreads();
+  const int n = nsh;
+  if (n == 0) return;
+  if (n > FAIL_CAP) {
+    if (tid == 0) atomicOr(err, ERR_FAILS);
+    return;
+  }
+  int o = cnt[tid];
+  for (long t = a0; t < a1; t++) {
+    const int i = G.istart + (int)(t / G.n2), j = G.jstart + (int)(t % G.n2);
+    const long c = cidx(G, 0, i, j);
+    if (fl1[c] != 0) list[o++] = (int)c;
+  }
+  for (long c = tid; c < G.nc; c += FU_THREADS) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) W[k * G.nc + c] = X1[k * G.nc + c];
+    Wf[c] = (signed char)(!fl1[c]);  // k_fu_flip
+  }
+  __syncthreads();
+  if (tid != 0) return;
+  const double *gC = geo_at(geo, G, L_CENT);
+  for (int t = 0; t < n; t++) {
+    const long c = list[t];
+    const int kind = stencil_kind(G, Wf, c);
+    double v[8];
+    repair_zone(G, W, c, kind, v);
+    for (int k = 0; k < 8; k++) vbuf[(long)t * 8 + k] = v[k];
+    kinds[t] = (signed char)kind;
+    const int i = (int)((c / G.sn2) % G.sn1), j = (int)(c % G.sn2);
+    const long gi = (long)i * G.sn2 + j;
+    Geo q;
+    load_geo(gC, G.ng, gi, q);
+    int fail = 0;
+    const bool g33 = fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
+    for (int k = 0; k < 8; k++) W[k * G.nc + c] = v[k];
+    Wf[c] = g33 ? (signed char)-33 : (signed char)0;
+  }
+  const long s = G.sn2;
+  for (int t = n - 1; t >= 0; t--) {
+    const long c = list[t];
+    const int kind = kinds[t];
+    const int i = (int)((c / G.sn2) % G.sn1), j = (int)(c % G.sn2);
+    const long gi = (long)i * G.sn2 + j;
+    Geo q;
+    load_geo(gC, G.ng, gi, q);
+    D8 v[8];
+    for (int k = 0; k < 8; k++) v[k] = D8::seed(vbuf[(long)t * 8 + k], k);
+    int fail = 0;
+    fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
+    double lo[8], lv[8];
+    for (int k = 0; k < 8; k++) lo[k] = lam[k * G.nc + c];
+    for (int k = 0; k < 8; k++) {
+      double a = 0.;
+      for (int r = 0; r < 8; r++) a += lo[r] * v[r].d[k];
+      lv[k] = a;
+    }
+    // the repair keeps the zone's fields and replaces the rest
+    for (int k = 0; k < 8; k++) lam[k * G.nc + c] = k >= B1 ? lv[k] : 0.;
+    if (kind == 0) {
+      for (int k = 0; k < B1; k++) {
+        double *L = lam + k * G.nc;
+        const double a = 0.25 * lv[k];
+        L[c + 1] += a; L[c - 1] += a; L[c - s] += a; L[c + s] += a;
+      }
+    } else if (kind == 1) {
+      for (int k = 0; k < B1; k++) {
+        double *L = lam + k * G.nc;
+        const double a = 0.25 * lv[k];
+        L[c + s + 1] += a; L[c + s - 1] += a; L[c - s + 1] += a; L[c - s - 1] += a;
+      }
+    } else {
+      for (int k = RHO; k <= UU; k++) {
+        double *L = lam + k * G.nc;
+        const double a = 0.5 * 0.25 * lv[k];
+        L[c + 1] += a; L[c - 1] += a; L[c - s] += a; L[c + s] += a;
+        L[c + s + 1] += a; L[c + s - 1] += a; L[c - s + 1] += a; L[c - s - 1] += a;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the inversion and fixup() of one zone (k_invert) transposed
+
+// x with A^T x = b, A[o][k] row-major 8x8; Gaussian elimination with partial pivoting
+__device__ bool solve8t(const double (*A)[8], const double *b, double *x)
+{
+  double M[8][9];
+  for (int r = 0; r < 8; r++) {
+    for (int c = 0; c < 8; c++) M[r][c] = A[c][r];
+    M[r][8] = b[r];
+  }
+  for (int col = 0; col < 8; col++) {
+    int piv = col;
+    double best = fabs(M[col][col]);
+    for (int r = col + 1; r < 8; r++)
+      if (fabs(M[r][col]) > best) { best = fabs(M[r][col]); piv = r; }
+    if (!(best > 0.)) return false;
+    if (piv != col)
+      for (int c = col; c < 9; c++) { double t = M[col][c]; M[col][c] = M[piv][c]; M[piv][c] = t; }
+    for (int r = col + 1; r < 8; r++) {
+      const double f = M[r][col] / M[col][col];
+      for (int c = col; c < 9; c++) M[r][c] -= f * M[col][c];
+    }
+  }
+  for (int r = 7; r >= 0; r--) {
+    double s = M[r][8];
+    for (int c = r + 1; c < 8; c++) s -= M[r][c] * x[c];
+    x[r] = s / M[r][r];
+  }
+  return true;
+}
+
+// lamf: adjoint of the half step's output pf (its active cells are consumed);
+// lamU: adjoint of the conserved variables the update formed; lampi: adjoint of
+// the inversion's guess pi (a failed zone keeps it)
+__global__ void __launch_bounds__(128) k_adj_invert(Grid G, const double *__restrict__ Ub, const double *__restrict__ pi,
+                                                    const double *__restrict__ geo, const double *__restrict__ floors,
+                                                    const double *__restrict__ katm, double *lamf, double *lamU,
+                                                    double *lampi, int *err)
+{
+  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
+  if (i > G.istop || j > G.jstop) return;
+  const long c = cidx(G, 0, i, j);
+  const long gi = (long)i * G.sn2 + j;
+  Geo q;
+  load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
+  double U[8], z[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    U[k] = Ub[k * G.nc + c];
+    z[k] = pi[k * G.nc + c];
+  }
+  // the step's inversion, repeated on the recorded U and guess (step_ch.c:265-300)
+  const double K = katm[i];
+  int which = 0;
+  int flag = utoprim<0>(G.gam, 0., U, q, z);
+  if (flag) {
+    which = 1;
+    flag = utoprim<1>(G.gam, K, U, q, z);
+    if (flag) {
+      which = 2;
+      flag = utoprim<2>(G.gam, K, U, q, z);
+    }
+  }
+  double lo[8], lz[8], lu[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    lo[k] = lamf[k * G.nc + c];
+    lamf[k * G.nc + c] = 0.;
+  }
+  {
+    D8 v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] = D8::seed(z[k], k);
+    int fail = 0;
+    fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      double a = 0.;
+#pragma unroll
+      for (int o = 0; o < 8; o++) a += lo[o] * v[o].d[k];
+      lz[k] = a;
+    }
+  }
+  if (flag == 0) {
+    double M[8][8];
+    {
+      D8 v[8], Uo[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) v[k] = D8::seed(z[k], k);
+      StateT<D8> s;
+      int fail = 0;
+      get_state(v, q, s, &fail);
+      primtoflux(G.gam, v, s, 0, q.g, Uo);
+#pragma unroll
+      for (int o = 0; o < 8; o++)
+#pragma unroll
+        for (int k = 0; k < 8; k++) M[o][k] = Uo[o].d[k];
+    }
+    if (which) {
+      // Utoprim_1dvsq2fix1 / Utoprim_1dfix1 solve with u = K rho^gam / (gam - 1)
+      // in place of the energy equation
+#pragma unroll
+      for (int k = 0; k < 8; k++) M[UU][k] = 0.;
+      M[UU][UU] = 1.;
+      M[UU][RHO] = -K * G.gam * pow(z[RHO], G.gam - 1.) / (G.gam - 1.);
+    }
+    if (!solve8t(M, lz, lu)) {
+      atomicOr(err, ERR_SINGULAR);
+#pragma unroll
+      for (int k = 0; k < 8; k++) lu[k] = 0.;
+    }
+    if (which) lu[UU] = 0.;
+  } else {
+#pragma unroll
+    for (int k = 0; k < B1; k++) {
+      lampi[k * G.nc + c] += lz[k];
+      lu[k] = 0.;
+    }
+#pragma unroll
+    for (int k = B1; k < 8; k++) lu[k] = lz[k] / q.g;
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++) lamU[k * G.nc + c] = lu[k];
+}
+
+// ---------------------------------------------------------------------------
+// the update (k_cons: primtoU, source, flux-CT, flux divergence) transposed
+
+// adjoint of one corner EMF (step_ch.c:546-547) onto the raw face fluxes,
+// through fix_flux's polar reflection of F1[B2] (coord.c:284-301)
+__device__ __forceinline__ void add_f1b2(const Grid &G, int i, int j, double a, double *lamF1)
+{
+  if (j == G.jstart - 1) atomicAdd(&lamF1[B2 * G.nc + cidx(G, 0, i, G.jstart)], -a);
+  else if (j == G.jstop + 1) atomicAdd(&lamF1[B2 * G.nc + cidx(G, 0, i, G.jstop)], -a);
+  else atomicAdd(&lamF1[B2 * G.nc + cidx(G, 0, i, j)], a);
+}
+
+__device__ __forceinline__ void emf_adjoint(const Grid &G, int i, int j, double l, double *lamF1, double *lamF2)
+{
+  if (l == 0.) return;
+  const double a = 0.25 * l;
+  add_f1b2(G, i, j, a, lamF1);
+  add_f1b2(G, i, j - 1, a, lamF1);
+  atomicAdd(&lamF2[B1 * G.nc + cidx(G, 0, i, j)], -a);
+  atomicAdd(&lamF2[B1 * G.nc + cidx(G, 0, i - 1, j)], -a);
+}
+
+// U = primtoU(pi) + Dt (-dF1/dx1 - dF2/dx2 + source(pb)) (step_ch.c:247-263);
+// FULL: the corrector (pi = p^n, pb = ph), else the predictor (pi = pb = p^n)
+template <bool FULL>
+__global__ void __launch_bounds__(128) k_adj_cons(Grid G, const double *__restrict__ pi, const double *__restrict__ pb,
+                                                  const double *__restrict__ Ub, const double *__restrict__ F1rho,
+                                                  const double *__restrict__ geo, const double *__restrict__ conn,
+                                                  const double *__restrict__ lamU, double *lampi, double *lampb,
+                                                  double *lamF1, double *lamF2, double Dt, double *lamDt)
+{
+  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
+  double lDt = 0.;
+  if (i <= G.istop && j <= G.jstop) {
+    const long c = cidx(G, 0, i, j);
+    const long gi = (long)i * G.sn2 + j;
+    Geo q;
+    load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
+    double lu[8], P0[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) lu[k] = lamU[k * G.nc + c];
+    int fail = 0;
+    {
+      D8 v[8], U0[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) v[k] = D8::seed(pi[k * G.nc + c], k);
+      StateT<D8> s;
+      get_state(v, q, s, &fail);
+      primtoflux(G.gam, v, s, 0, q.g, U0);
+      double li[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        double a = 0.;
+#pragma unroll
+        for (int o = 0; o < 8; o++) a += lu[o] * U0[o].d[k];
+        li[k] = a;
+      }
+#pragma unroll
+      for (int o = 0; o < 8; o++) P0[o] = U0[o].v;
+      if (!FULL) {
+        D8 dU[8];
+        source_of_state(G.gam, v, s, q, conn, G.ng, gi, dU);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          double a = 0.;
+#pragma unroll
+          for (int o = 0; o < 8; o++) a += lu[o] * dU[o].d[k];
+          li[k] += Dt * a;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 8; k++) lampi[k * G.nc + c] += li[k];
+    }
+    if (FULL) {
+      D8 v[8], dU[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) v[k] = D8::seed(pb[k * G.nc + c], k);
+      StateT<D8> s;
+      get_state(v, q, s, &fail);
+      source_of_state(G.gam, v, s, q, conn, G.ng, gi, dU);
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        double a = 0.;
+#pragma unroll
+        for (int o = 0; o < 8; o++) a += lu[o] * dU[o].d[k];
+        lampb[k * G.nc + c] += Dt * a;
+      }
+    }
+    // dU/dDt = (U - primtoU(pi)) / Dt, the step's own flux divergence plus source
+#pragma unroll
+    for (int o = 0; o < 8; o++) lDt += lu[o] * ((Ub[o * G.nc + c] - P0[o]) / Dt);
+
+    // the zone's processed face fluxes
+    const double a1 = Dt / G.dx1, a2 = Dt / G.dx2;
+    double g1m[8], g1p[8], g2m[8], g2p[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      g1m[k] = lu[k] * a1;
+      g1p[k] = -lu[k] * a1;
+      g2m[k] = lu[k] * a2;
+      g2p[k] = -lu[k] * a2;
+    }
+    // no inflow of mass through the radial boundaries (coord.c:307-321)
+    if (i == G.istart && F1rho[cidx(G, 0, i, j)] > 0) g1m[RHO] = 0.;
+    if (i == G.istop && F1rho[cidx(G, 0, i + 1, j)] < 0) g1p[RHO] = 0.;
+    const long c1p = cidx(G, 0, i + 1, j), c2p = cidx(G, 0, i, j + 1);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      if (k == B1 || k == B2) continue;
+      atomicAdd(&lamF1[k * G.nc + c], g1m[k]);
+      atomicAdd(&lamF1[k * G.nc + c1p], g1p[k]);
+      atomicAdd(&lamF2[k * G.nc + c], g2m[k]);
+      atomicAdd(&lamF2[k * G.nc + c2p], g2p[k]);
+    }
+    // flux-CT (step_ch.c:514-629): f1m[B2] = (eA+eB)/2, f1p[B2] = (eC+eD)/2,
+    // f2m[B1] = -(eA+eC)/2, f2p[B1] = -(eB+eD)/2 with the corner EMFs
+    // A (i,j), B (i,j+1), C (i+1,j), D (i+1,j+1)
+    emf_adjoint(G, i, j, 0.5 * g1m[B2] - 0.5 * g2m[B1], lamF1, lamF2);
+    emf_adjoint(G, i, j + 1, 0.5 * g1m[B2] - 0.5 * g2p[B1], lamF1, lamF2);
+    emf_adjoint(G, i + 1, j, 0.5 * g1p[B2] - 0.5 * g2m[B1], lamF1, lamF2);
+    emf_adjoint(G, i + 1, j + 1, 0.5 * g1p[B2] - 0.5 * g2p[B1], lamF1, lamF2);
+  }
+  __shared__ double red[4];
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  double v = warp_sum(lDt);
+  if ((t & 31) == 0) red[t >> 5] = v;
+  __syncthreads();
+  if (t == 0) atomicAdd(lamDt, (red[0] + red[1]) + (red[2] + red[3]));
+}
+
+// ---------------------------------------------------------------------------
+// the face fluxes (k_flux: limited face states, LF flux) transposed; FULL: the
+// corrector, whose Courant minimum n_d (recorded) gets adjoint lnd
+
+template <int DIR, bool FULL>
+__global__ void __launch_bounds__(128) k_adj_flux(Grid G, const double *__restrict__ pb, const double *__restrict__ geo,
+                                                  const double *__restrict__ lamF, double *lamp, double lnd,
+                                                  double nmin, int *claim)
+{
+  const int j = (DIR == 2 ? G.jstart : G.jstart - 1) + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (DIR == 1 ? G.istart : G.istart - 1) + blockIdx.y * blockDim.y + threadIdx.y;
+  if (i > G.istop + 1 || j > G.jstop + 1) return;
+  if (DIR == 2 && (j == G.jstart || j == G.jstop + 1)) return;  // polar faces carry no flux
+  const long c = cidx(G, 0, i, j);
+  double lF[8];
+  bool any = false;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    lF[k] = lamF[k * G.nc + c];
+    any |= lF[k] != 0.;
+  }
+  const bool act = FULL && i >= G.istart && i <= G.istop && j >= G.jstart && j <= G.jstop;
+  if (!any && !(act && lnd != 0.)) return;
+  const long o1 = DIR == 1 ? c - 2 * G.sn2 : c - 2, o2 = DIR == 1 ? c - G.sn2 : c - 1,
+             o3 = DIR == 1 ? c + G.sn2 : c + 1;
+  // limited face states (interp.c:49-93) and their derivatives in (p[-2], p[-1], p[0], p[+1])
+  double pl[8], pr[8], dl[8][4], dr[8][4];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const double *P = pb + k * G.nc;
+    Dual<4> a = Dual<4>::seed(P[o1], 0), b = Dual<4>::seed(P[o2], 1), z = Dual<4>::seed(P[c], 2),
+            e = Dual<4>::seed(P[o3], 3);
+    Dual<4> L = b + 0.5 * slope_lim(G.lim, a, b, z);
+    Dual<4> R = z - 0.5 * slope_lim(G.lim, b, z, e);
+    pl[k] = L.v;
+    pr[k] = R.v;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      dl[k][m] = L.d[m];
+      dr[k][m] = R.d[m];
+    }
+  }
+  Geo q;
+  load_geo(geo_at(geo, G, DIR == 1 ? L_FACE1 : L_FACE2), G.ng, (long)i * G.sn2 + j, q);
+  double lpl[8], lpr[8], lct = 0.;
+  for (int c0 = 0; c0 < 16; c0 += NWF) {
+    using DF = Dual<NWF>;
+    DF L[8], R[8], F[8], ct;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      L[k] = DF::seed(pl[k], k - c0);
+      R[k] = DF::seed(pr[k], 8 + k - c0);
+    }
+    int fail = 0;
+    face_flux<DIR>(G.gam, L, R, q, F, ct, &fail);
+    if (c0 == 0 && act && lnd != 0.) {
+      const double dxd = DIR == 1 ? G.dx1 : G.dx2;
+      if (G.cour * dxd / ct.v == nmin && atomicCAS(claim, 0, 1) == 0) lct = -lnd * nmin / ct.v;
+    }
+#pragma unroll
+    for (int m = 0; m < NWF; m++) {
+      double s = lct * ct.d[m];
+#pragma unroll
+      for (int k = 0; k < 8; k++) s += lF[k] * F[k].d[m];
+      const int in = c0 + m;
+      if (in < 8) lpl[in] = s;
+      else lpr[in - 8] = s;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    double *L = lamp + k * G.nc;
+    const double la = lpl[k] * dl[k][0] + lpr[k] * dr[k][0];
+    const double lb = lpl[k] * dl[k][1] + lpr[k] * dr[k][1];
+    const double lz = lpl[k] * dl[k][2] + lpr[k] * dr[k][2];
+    const double le = lpl[k] * dl[k][3] + lpr[k] * dr[k][3];
+    if (la != 0.) atomicAdd(L + o1, la);
+    if (lb != 0.) atomicAdd(L + o2, lb);
+    if (lz != 0.) atomicAdd(L + c, lz);
+    if (le != 0.) atomicAdd(L + o3, le);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+struct DevBuf {
+  std::vector<void *> ptrs;
+  ~DevBuf()
+  {
+    for (void *p : ptrs) cudaFree(p);
+  }
+  template <class T>
+  T *get(size_t n)
+  {
+    void *p = nullptr;
+    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    return (T *)p;
+  }
+};
+
+static double bits_to_double(unsigned long long b)
+{
+  double d;
+  std::memcpy(&d, &b, sizeof d);
+  return d;
+}
+
+static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, double *ms)
+{
+  const Grid &G = x->G;
+  const size_t nc = (size_t)G.nc, pl = 8 * nc;
+  // the dual-number kernels keep up to ~2.3 KB per thread in local memory
+  size_t stack = 0;
+  CK(cudaDeviceGetLimit(&stack, cudaLimitStackSize));
+  if (stack < 4096) CK(cudaDeviceSetLimit(cudaLimitStackSize, 4096));
+  const int nseg = (nsteps + every - 1) / every;
+  const int nrec = every < nsteps ? every : nsteps;
+  DevBuf B;
+  // checkpoints, per-step records of one segment, adjoint state
+  double *ck = B.get<double>(pl * nseg);
+  DevScalars *cks = B.get<DevScalars>(nseg + 1);
+  double *pend = B.get<double>(pl);
+  double *recp = B.get<double>(pl * (nrec + 1));
+  double *recd = B.get<double>((size_t)nrec * (5 * pl + 2 * nc));
+  signed char *recf = B.get<signed char>((size_t)nrec * 2 * nc);
+  DevScalars *recs = B.get<DevScalars>((size_t)nrec * 2);
+  double *lam = B.get<double>(6 * pl);  // next, cur, ph, U, F1, F2
+  double *W = B.get<double>(pl);
+  signed char *Wf = B.get<signed char>(nc);
+  int *list = B.get<int>(FAIL_CAP);
+  double *vbuf = B.get<double>((size_t)FAIL_CAP * 8);
+  signed char *kinds = B.get<signed char>(FAIL_CAP);
+  int *ierr = B.get<int>(4);  // err, claim[2]
+  double *lamDt = B.get<double>(2);
+  if (!ck || !cks || !pend || !recp || !recd || !recf || !recs || !lam || !W || !Wf || !list || !vbuf || !kinds ||
+      !ierr || !lamDt)
+    return fail_with(HARM_E_CUDA, "device memory for the adjoint");
+  std::vector<StepRec> rec(nrec);
+  for (int r = 0; r < nrec; r++) {
+    double *d = recd + (size_t)r * (5 * pl + 2 * nc);
+    StepRec &s = rec[r];
+    s.X1[0] = d; s.X1[1] = d + pl; s.Ub[0] = d + 2 * pl; s.Ub[1] = d + 3 * pl; s.ph = d + 4 * pl;
+    s.F1rho[0] = d + 5 * pl; s.F1rho[1] = d + 5 * pl + nc;
+    s.fl1[0] = recf + (size_t)r * 2 * nc; s.fl1[1] = s.fl1[0] + nc;
+    s.sc[0] = recs + 2 * r; s.sc[1] = recs + 2 * r + 1;
+  }
+  double *lnext = lam, *lcur = lam + pl, *lh = lam + 2 * pl, *lU = lam + 3 * pl, *lF1 = lam + 4 * pl,
+         *lF2 = lam + 5 * pl;
+  int *err = ierr, *claim = ierr + 1;
+  cudaStream_t st = x->stream;
+  cudaEvent_t e0, e1, e2;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventCreate(&e2));
+  struct EvGuard {
+    cudaEvent_t a, b, c;
+    ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); }
+  } eg{e0, e1, e2};
+
+  // forward pass, keeping a checkpoint every `every` steps
+  CK(cudaMemsetAsync(ierr, 0, 4 * sizeof(int), st));
+  CK(cudaEventRecord(e0, st));
+  for (int n = 0; n < nsteps; n++) {
+    if (n % every == 0) {
+      CK(cudaMemcpyAsync(ck + (size_t)(n / every) * pl, x->p, pl * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      CK(cudaMemcpyAsync(cks + n / every, x->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, st));
+    }
+    int rc = exact::launch_step(x);
+    if (rc) return rc;
+  }
+  CK(cudaEventRecord(e1, st));
+  CK(cudaMemcpyAsync(pend, x->p, pl * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(cks + nseg, x->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, st));
+  DevScalars s0, s1;
+  CK(cudaMemcpyAsync(&s0, cks, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&s1, cks + nseg, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (s1.fail_code || s1.halted)
+    return fail_with(HARM_E_ADJOINT, "the forward steps failed (fail code " + std::to_string(s1.fail_code) + ")");
+  *J = s1.mass_in - s0.mass_in;
+
+  // reverse sweep
+  CK(cudaMemsetAsync(lam, 0, 6 * pl * sizeof(double), st));
+  const dim3 tile(32, 4);
+  const dim3 zg((G.n2 + 31) / 32, (G.n1 + 3) / 4, 1);
+  const dim3 g1((G.n2 + 2 + 31) / 32, (G.n1 + 1 + 3) / 4, 1);
+  const dim3 g2((G.n2 + 1 + 31) / 32, (G.n1 + 2 + 3) / 4, 1);
+  const int nbc = 4 * G.sn2 + 4 * (G.sn1 - 4);
+  double lam_dt_next = 0.;
+  std::vector<DevScalars> hs(2 * (size_t)nrec);
+  for (int seg = nseg - 1; seg >= 0; seg--) {
+    const int n0 = seg * every, n1 = n0 + every < nsteps ? n0 + every : nsteps;
+    CK(cudaMemcpyAsync(x->p, ck + (size_t)seg * pl, pl * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(x->sc, cks + seg, sizeof(DevScalars), cudaMemcpyDeviceToDevice, st));
+    for (int n = n0; n < n1; n++) {
+      CK(cudaMemcpyAsync(recp + (size_t)(n - n0) * pl, x->p, pl * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      int rc = exact::launch_step_rec(x, rec[n - n0]);
+      if (rc) return rc;
+    }
+    CK(cudaMemcpyAsync(recp + (size_t)(n1 - n0) * pl, x->p, pl * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(hs.data(), recs, 2 * (size_t)(n1 - n0) * sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int n = n1 - 1; n >= n0; n--) {
+      const StepRec &r = rec[n - n0];
+      const DevScalars &sa = hs[2 * (n - n0)], &sb = hs[2 * (n - n0) + 1];
+      const double *pn = recp + (size_t)(n - n0) * pl, *pnext = recp + (size_t)(n - n0 + 1) * pl;
+      const double dt = sa.dt, din = sb.mdot_in, ndt = sb.ndt;
+      const double n1v = bits_to_double(sa.ndt_bits[0]), n2v = bits_to_double(sa.ndt_bits[1]);
+      if (sb.fail_code) return fail_with(HARM_E_ADJOINT, "a recomputed step failed");
+      if (sb.dt != (ndt > SAFE * dt ? SAFE * dt : ndt))
+        return fail_with(HARM_E_ARG, "the steps reach tf: the adjoint needs dt = min(ndt, 1.3 dt) throughout");
+      // dt^{n+1} = min(ndt, 1.3 dt^n), ndt = defcon / (1/n1 + 1/n2) (step_ch.c:126-137)
+      double lam_dt = din, lam_ndt = 0.;
+      if (ndt > SAFE * dt) lam_dt += SAFE * lam_dt_next;
+      else lam_ndt = lam_dt_next;
+      const double S = 1. / n1v + 1. / n2v;
+      const double ln1 = lam_ndt * G.defcon / (n1v * n1v) / (S * S);
+      const double ln2 = lam_ndt * G.defcon / (n2v * n2v) / (S * S);
+      CK(cudaMemsetAsync(lamDt, 0, 2 * sizeof(double), st));
+      CK(cudaMemsetAsync(claim, 0, 2 * sizeof(int), st));
+      // objective term on the step's result
+      k_adj_din<<<(G.n2 + 127) / 128, 128, 0, st>>>(G, pnext, x->geo, lnext, dt);
+      // corrector: bound_prim, fixup_utoprim, bound_prim, inversion, update, fluxes
+      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, pnext, x->geo, lnext);
+      k_adj_fixup_utoprim<<<1, FU_THREADS, 0, st>>>(G, r.X1[1], r.fl1[1], x->geo, x->floors, W, Wf, list, vbuf,
+                                                   kinds, lnext, err);
+      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, r.X1[1], x->geo, lnext);
+      k_adj_invert<<<zg, tile, 0, st>>>(G, r.Ub[1], pn, x->geo, x->floors, x->katm, lnext, lU, lcur, err);
+      CK(cudaMemsetAsync(lF1, 0, 2 * pl * sizeof(double), st));
+      k_adj_cons<true><<<zg, tile, 0, st>>>(G, pn, r.ph, r.Ub[1], r.F1rho[1], x->geo, x->conn, lU, lcur, lh, lF1,
+                                            lF2, dt, lamDt + 1);
+      k_adj_flux<1, true><<<g1, tile, 0, st>>>(G, r.ph, x->geo, lF1, lh, ln1, n1v, claim);
+      k_adj_flux<2, true><<<g2, tile, 0, st>>>(G, r.ph, x->geo, lF2, lh, ln2, n2v, claim + 1);
+      // predictor, from p^n into ph
+      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, r.ph, x->geo, lh);
+      k_adj_fixup_utoprim<<<1, FU_THREADS, 0, st>>>(G, r.X1[0], r.fl1[0], x->geo, x->floors, W, Wf, list, vbuf,
+                                                   kinds, lh, err);
+      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, r.X1[0], x->geo, lh);
+      k_adj_invert<<<zg, tile, 0, st>>>(G, r.Ub[0], pn, x->geo, x->floors, x->katm, lh, lU, lcur, err);
+      CK(cudaMemsetAsync(lF1, 0, 2 * pl * sizeof(double), st));
+      k_adj_cons<false><<<zg, tile, 0, st>>>(G, pn, pn, r.Ub[0], r.F1rho[0], x->geo, x->conn, lU, lcur, lcur, lF1,
+                                             lF2, 0.5 * dt, lamDt);
+      k_adj_flux<1, false><<<g1, tile, 0, st>>>(G, pn, x->geo, lF1, lcur, 0., 0., claim);
+      k_adj_flux<2, false><<<g2, tile, 0, st>>>(G, pn, x->geo, lF2, lcur, 0., 0., claim);
+      CK(cudaGetLastError());
+      double hDt[2];
+      CK(cudaMemcpyAsync(hDt, lamDt, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      lam_dt_next = lam_dt + 0.5 * hDt[0] + hDt[1];
+      // the adjoint of p^n becomes the next (earlier) step's output adjoint
+      double *t = lnext;
+      lnext = lcur;
+      lcur = t;
+      CK(cudaMemsetAsync(lcur, 0, pl * sizeof(double), st));
+      CK(cudaMemsetAsync(lh, 0, pl * sizeof(double), st));
+    }
+  }
+  CK(cudaEventRecord(e2, st));
+  int herr = 0;
+  CK(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (herr & ERR_FAILS) return fail_with(HARM_E_ADJOINT, "more failed inversions in a half step than the adjoint lists");
+  if (herr & ERR_SINGULAR) return fail_with(HARM_E_ADJOINT, "a singular primtoU Jacobian in the adjoint of an inversion");
+  if (ms) {
+    float a, b;
+    CK(cudaEventElapsedTime(&a, e0, e1));
+    CK(cudaEventElapsedTime(&b, e1, e2));
+    ms[0] = a;
+    ms[1] = b;
+  }
+  int rc = get_prims(x, lnext, grad, nullptr);
+  if (rc) return rc;
+  // leave the context where the forward pass ended
+  CK(cudaMemcpyAsync(x->p, pend, pl * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(x->sc, cks + nseg, sizeof(DevScalars), cudaMemcpyDeviceToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  return HARM_OK;
+}
+
+}  // namespace adj
+}  // namespace harm
+
+extern "C" int harm_adjoint_mass_in(harm_ctx *h, int nsteps, int checkpoint_every, double *J, double *grad,
+                                    double *ms)
+{
+  using namespace harm;
+  if (!h || !J || !grad) return fail_with(HARM_E_ARG, "null argument");
+  Ctx *x = &h->x;
+  if (nsteps < 1 || checkpoint_every < 1) return fail_with(HARM_E_ARG, "nsteps and checkpoint_every must be >= 1");
+  if (x->G.n3 != 1) return fail_with(HARM_E_ARG, "the adjoint covers the 2D step (N3 = 1)");
+  if (x->cool) return fail_with(HARM_E_ARG, "the adjoint covers the gamma-law step, not COOL_EOS");
+  if (x->mode != HARM_FP64) return fail_with(HARM_E_ARG, "the adjoint runs on the FP64 step");
+  if (x->ntr) return fail_with(HARM_E_ARG, "the adjoint's recomputation would move the tracers again: detach them");
+  return adj::run_adjoint(x, nsteps, checkpoint_every, J, grad, ms);
+}

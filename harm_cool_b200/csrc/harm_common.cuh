@@ -161,8 +161,21 @@ int fail_with(int code, const std::string &msg);
 
 inline dim3 zone_grid(const Grid &G) { return dim3((G.n2 + 31) / 32, (G.n1 + 3) / 4, G.n3); }
 
+// What the discrete adjoint (harm_adjoint.cu) keeps of one recomputed step;
+// index 0 is the predictor, 1 the corrector.  Device pointers, [8][nc] planes
+// unless noted.
+struct StepRec {
+  double *X1[2];                 // the inversion's output after the first bound_prim
+  double *Ub[2];                 // the conserved variables the update formed
+  double *F1rho[2];              // raw radial mass flux [nc] (the no-inflow fix reads its sign)
+  signed char *fl1[2];           // pflag after the first bound_prim [nc]
+  double *ph;                    // the predictor's final state
+  DevScalars *sc[2];             // the run state before k_finalize (the corrector's Courant minima) and after
+};
+
 // kernels shared by both precisions (harm_api.cu)
 int launch_bound(Ctx *x, double *P);
+int get_prims(Ctx *x, const double *src, double *p, signed char *pflag);  // device planes -> host layout
 int launch_fixup_utoprim(Ctx *x, double *P);
 void launch_mass(Ctx *x);
 int sync_status(Ctx *x);
@@ -175,6 +188,7 @@ void invalidate_graph(Ctx *x);   // a captured step no longer matches the contex
 // one step and the per-kernel timing of each precision variant
 namespace exact {
 int launch_step(Ctx *x);
+int launch_step_rec(Ctx *x, const StepRec &r);  // launch_step, keeping r
 int time_kernels(Ctx *x, int reps, double *ms);
 }
 namespace mixed {

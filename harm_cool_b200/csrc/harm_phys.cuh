@@ -52,12 +52,19 @@ __device__ __forceinline__ void load_geo(const double *__restrict__ G, long ng, 
   q.alpha = __ldg(G + 18 * ng + gi);
 }
 
-struct State {
-  double ucon[4], ucov[4], bcon[4], bcov[4];
+// The routines below that the discrete adjoint linearises are templates on
+// the scalar type R: double for the step itself, a forward-mode dual number
+// (harm_dual.cuh) for the adjoint's local Jacobians.  The double
+// instantiation is the reference's expression order unchanged.
+template <class R>
+struct StateT {
+  R ucon[4], ucov[4], bcon[4], bcov[4];
 };
+using State = StateT<double>;
 
 // lower() (metric.c:210-231)
-__device__ __forceinline__ void lower(const double *u, const Geo &q, double *d)
+template <class R>
+__device__ __forceinline__ void lower(const R *u, const Geo &q, R *d)
 {
   d[0] = q.v00 * u[0] + q.v01 * u[1] + q.v03 * u[3];
   d[1] = q.v01 * u[0] + q.v11 * u[1] + q.v13 * u[3];
@@ -65,15 +72,17 @@ __device__ __forceinline__ void lower(const double *u, const Geo &q, double *d)
   d[3] = q.v03 * u[0] + q.v13 * u[1] + q.v33 * u[3];
 }
 
-__device__ __forceinline__ double dot4(const double *a, const double *b)
+template <class R>
+__device__ __forceinline__ R dot4(const R *a, const R *b)
 {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3];
 }
 
 // gamma_calc() (phys.c:300-324); returns 1 on failure
-__device__ __forceinline__ int gamma_calc(const double *pr, const Geo &q, double &gamma)
+template <class R>
+__device__ __forceinline__ int gamma_calc(const R *pr, const Geo &q, R &gamma)
 {
-  double qsq = q.v11 * pr[U1] * pr[U1] + q.v22 * pr[U2] * pr[U2] + q.v33 * pr[U3] * pr[U3]
+  R qsq = q.v11 * pr[U1] * pr[U1] + q.v22 * pr[U2] * pr[U2] + q.v33 * pr[U3] * pr[U3]
                + 2. * (q.v13 * pr[U1] * pr[U3]);
   if (qsq < 0.) {
     if (fabs(qsq) > 1.E-10) { gamma = 1.; return 1; }
@@ -84,11 +93,12 @@ __device__ __forceinline__ int gamma_calc(const double *pr, const Geo &q, double
 }
 
 // ucon_calc() (phys.c:232-252); sets *fail on a gamma failure
-__device__ __forceinline__ void ucon_calc(const double *pr, const Geo &q, double *ucon, int *fail)
+template <class R>
+__device__ __forceinline__ void ucon_calc(const R *pr, const Geo &q, R *ucon, int *fail)
 {
   const double alpha = q.alpha;
   double b1 = q.n01 * alpha * alpha, b2 = 0. * alpha * alpha, b3 = q.n03 * alpha * alpha;
-  double gamma;
+  R gamma;
   if (gamma_calc(pr, q, gamma)) *fail = FAIL_GAMMA;
   ucon[0] = gamma / alpha;
   ucon[1] = pr[U1] - gamma * b1 / alpha;
@@ -97,7 +107,8 @@ __device__ __forceinline__ void ucon_calc(const double *pr, const Geo &q, double
 }
 
 // bcon_calc() (phys.c:108-117)
-__device__ __forceinline__ void bcon_calc(const double *pr, const double *ucon, const double *ucov, double *bcon)
+template <class R>
+__device__ __forceinline__ void bcon_calc(const R *pr, const R *ucon, const R *ucov, R *bcon)
 {
   bcon[0] = pr[B1] * ucov[1] + pr[B2] * ucov[2] + pr[B3] * ucov[3];
   bcon[1] = (pr[B1] + bcon[0] * ucon[1]) / ucon[0];
@@ -106,7 +117,8 @@ __device__ __forceinline__ void bcon_calc(const double *pr, const double *ucon, 
 }
 
 // get_state() (phys.c:219-229)
-__device__ __forceinline__ void get_state(const double *pr, const Geo &q, State &s, int *fail)
+template <class R>
+__device__ __forceinline__ void get_state(const R *pr, const Geo &q, StateT<R> &s, int *fail)
 {
   ucon_calc(pr, q, s.ucon, fail);
   lower(s.ucon, q, s.ucov);
@@ -115,24 +127,25 @@ __device__ __forceinline__ void get_state(const double *pr, const Geo &q, State 
 }
 
 // mhd_calc() (phys.c:143-161): one row T^dir_nu of the stress tensor
-__device__ __forceinline__ void mhd_calc(double gam, const double *pr, int dir, const State &s, double *mhd)
+template <class R>
+__device__ __forceinline__ void mhd_calc(double gam, const R *pr, int dir, const StateT<R> &s, R *mhd)
 {
-  double r = pr[RHO], u = pr[UU];
-  double P = (gam - 1.) * u;
-  double w = P + r + u;
-  double bsq = dot4(s.bcon, s.bcov);
-  double eta = w + bsq;
-  double ptot = P + 0.5 * bsq;
+  R r = pr[RHO], u = pr[UU];
+  R P = (gam - 1.) * u;
+  R w = P + r + u;
+  R bsq = dot4(s.bcon, s.bcov);
+  R eta = w + bsq;
+  R ptot = P + 0.5 * bsq;
 #pragma unroll
   for (int j = 0; j < 4; j++)
     mhd[j] = eta * s.ucon[dir] * s.ucov[j] + ptot * (dir == j ? 1. : 0.) - s.bcon[dir] * s.bcov[j];
 }
 
 // primtoflux() (phys.c:59-96)
-__device__ __forceinline__ void primtoflux(double gam, const double *pr, const State &s, int dir, double g,
-                                           double *flux)
+template <class R>
+__device__ __forceinline__ void primtoflux(double gam, const R *pr, const StateT<R> &s, int dir, double g, R *flux)
 {
-  double mhd[4];
+  R mhd[4];
   flux[RHO] = pr[RHO] * s.ucon[dir];
   mhd_calc(gam, pr, dir, s, mhd);
   flux[UU] = mhd[0] + flux[RHO];
@@ -159,44 +172,107 @@ __device__ __forceinline__ double gcon_t(const Geo &q, int js)
 // vchar() (phys.c:337-476, gamma-law): with A = e^js and B = e^t the
 // contractions reduce to metric entries: A.A = g^{js js}, B.B = g^{tt},
 // A.u = u^js, B.u = u^t, A.B = g^{t js}
-__device__ __forceinline__ void vchar(double gam, const double *pr, const State &s, const Geo &q, int js,
-                                      double &vmax, double &vmin, int *fail)
+template <class R>
+__device__ __forceinline__ void vchar(double gam, const R *pr, const StateT<R> &s, const Geo &q, int js, R &vmax,
+                                      R &vmin, int *fail)
 {
-  double bsq = dot4(s.bcon, s.bcov);
-  double rho = pr[RHO], u = pr[UU];
-  double EF = rho + gam * u;
-  double EE = bsq + EF;
-  double va2 = bsq / EE;
-  double cs2 = gam * (gam - 1.) * u / EF;
-  double cms2 = cs2 + va2 - cs2 * va2;
+  R bsq = dot4(s.bcon, s.bcov);
+  R rho = pr[RHO], u = pr[UU];
+  R EF = rho + gam * u;
+  R EE = bsq + EF;
+  R va2 = bsq / EE;
+  R cs2 = gam * (gam - 1.) * u / EF;
+  R cms2 = cs2 + va2 - cs2 * va2;
   if (cms2 < 0.) { *fail = FAIL_COEFF_NEG; cms2 = SMALL; }
   if (cms2 > 1.) { *fail = FAIL_COEFF_SUP; cms2 = 1.; }
   double Asq = gcon_diag(q, js), Bsq = q.n00;
-  double Au = s.ucon[js], Bu = s.ucon[0], AB = gcon_t(q, js);
-  double Au2 = Au * Au, Bu2 = Bu * Bu, AuBu = Au * Bu;
-  double A = Bu2 - (Bsq + Bu2) * cms2;
-  double B = 2. * (AuBu - (AB + AuBu) * cms2);
-  double C = Au2 - (Asq + Au2) * cms2;
-  double discr = B * B - 4. * A * C;
+  R Au = s.ucon[js], Bu = s.ucon[0];
+  double AB = gcon_t(q, js);
+  R Au2 = Au * Au, Bu2 = Bu * Bu, AuBu = Au * Bu;
+  R A = Bu2 - (Bsq + Bu2) * cms2;
+  R B = 2. * (AuBu - (AB + AuBu) * cms2);
+  R C = Au2 - (Asq + Au2) * cms2;
+  R discr = B * B - 4. * A * C;
   if ((discr < 0.0) && (discr > -1.e-10)) discr = 0.0;
   else if (discr < -1.e-10) { *fail = FAIL_VCHAR_DISCR; discr = 0.; }
   discr = sqrt(discr);
-  double vp = -(-B + discr) / (2. * A);
-  double vm = -(-B - discr) / (2. * A);
+  R vp = -(-B + discr) / (2. * A);
+  R vm = -(-B - discr) / (2. * A);
   if (vp > vm) { vmax = vp; vmin = vm; }
   else { vmax = vm; vmin = vp; }
 }
 
-// slope_lim() (interp.c:49-93)
-__device__ __forceinline__ double slope_lim(int lim, double y1, double y2, double y3)
+// The local Lax-Friedrichs flux of one face (step_ch.c:431-473, HLLF = 0 and
+// LAXF = 1 at :66-67) from the reconstructed states pl, pr: F and the face's
+// wave speed ctop.
+template <int DIR, class R>
+__device__ __forceinline__ void face_flux(double gam, const R *pl, const R *pr, const Geo &q, R *F, R &ctop,
+                                          int *fail)
 {
-  double Dqm, Dqp, s;
+  StateT<R> s;
+  R Fl[8], Ul[8], cmaxl, cminl, cmaxr, cminr;
+  get_state(pl, q, s, fail);
+  primtoflux(gam, pl, s, DIR, q.g, Fl);
+  primtoflux(gam, pl, s, 0, q.g, Ul);
+  vchar(gam, pl, s, q, DIR, cmaxl, cminl, fail);
+  get_state(pr, q, s, fail);
+  {
+    R Fr[8], Ur[8];
+    primtoflux(gam, pr, s, DIR, q.g, Fr);
+    primtoflux(gam, pr, s, 0, q.g, Ur);
+    vchar(gam, pr, s, q, DIR, cmaxr, cminr, fail);
+    R t1 = 0. > cmaxl ? R(0.) : cmaxl;
+    R cmax = fabs(t1 > cmaxr ? t1 : cmaxr);
+    R t2 = 0. > -cminl ? R(0.) : -cminl;
+    R cmin = fabs(t2 > -cminr ? t2 : -cminr);
+    ctop = cmax > cmin ? cmax : cmin;
+#pragma unroll
+    for (int k = 0; k < 8; k++) F[k] = 0.5 * (Fl[k] + Fr[k] - ctop * (Ur[k] - Ul[k]));
+  }
+}
+
+// source() (phys.c:165-207); conn stored as [k][min(nu,j)][max(nu,j)]
+__device__ __forceinline__ int conn_slot(int k, int a, int b)
+{
+  int lo = a < b ? a : b, hi = a < b ? b : a;
+  // pairs (lo,hi) with lo <= hi in row order: 00 01 02 03 11 12 13 22 23 33
+  int pair = lo == 0 ? hi : lo == 1 ? 3 + hi : lo == 2 ? 5 + hi : 9;
+  return k * 10 + pair;
+}
+
+template <class R>
+__device__ __forceinline__ void source_of_state(double gam, const R *pb, const StateT<R> &s, const Geo &q,
+                                                const double *__restrict__ conn, long ng, long gi, R *dU)
+{
+  R mhd[4][4];
+#pragma unroll
+  for (int d = 0; d < 4; d++) mhd_calc(gam, pb, d, s, mhd[d]);
+#pragma unroll
+  for (int k = 0; k < 8; k++) dU[k] = 0.;
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      dU[UU] += mhd[j][k] * __ldg(conn + conn_slot(k, 0, j) * ng + gi);
+      dU[U1] += mhd[j][k] * __ldg(conn + conn_slot(k, 1, j) * ng + gi);
+      dU[U2] += mhd[j][k] * __ldg(conn + conn_slot(k, 2, j) * ng + gi);
+      dU[U3] += mhd[j][k] * __ldg(conn + conn_slot(k, 3, j) * ng + gi);
+    }
+#pragma unroll
+  for (int k = 0; k < 8; k++) dU[k] *= q.g;
+}
+
+// slope_lim() (interp.c:49-93)
+template <class R>
+__device__ __forceinline__ R slope_lim(int lim, R y1, R y2, R y3)
+{
+  R Dqm, Dqp, s;
   if (lim == 0) {
     Dqm = 2. * (y2 - y1);
     Dqp = 2. * (y3 - y2);
-    double Dqc = 0.5 * (y3 - y1);
+    R Dqc = 0.5 * (y3 - y1);
     s = Dqm * Dqp;
-    if (s <= 0.) return 0.;
+    if (s <= 0.) return R(0.);
     if (fabs(Dqm) < fabs(Dqp) && fabs(Dqm) < fabs(Dqc)) return Dqm;
     if (fabs(Dqp) < fabs(Dqc)) return Dqp;
     return Dqc;
@@ -204,7 +280,7 @@ __device__ __forceinline__ double slope_lim(int lim, double y1, double y2, doubl
   Dqm = (y2 - y1);
   Dqp = (y3 - y2);
   s = Dqm * Dqp;
-  if (s <= 0.) return 0.;
+  if (s <= 0.) return R(0.);
   if (lim == 1) return 2. * s / (Dqm + Dqp);
   if (fabs(Dqm) < fabs(Dqp)) return Dqm;
   return Dqp;
@@ -616,75 +692,78 @@ __device__ __forceinline__ int utoprim(double gam, double K, const double *U, co
 // (get_rho_u_floor, fixup.c:117-140, evaluated on the host with the same pow)
 
 // phys.c:273-297
-__device__ __forceinline__ double ut_calc_3vel(const double *v, const Geo &q)
+template <class R>
+__device__ __forceinline__ R ut_calc_3vel(const R *v, const Geo &q)
 {
   double AA = q.v00;
-  double BB = 2. * (q.v01 * v[1] + q.v03 * v[3]);
-  double CC = q.v11 * v[1] * v[1] + q.v22 * v[2] * v[2] + q.v33 * v[3] * v[3] + 2. * (q.v13 * v[1] * v[3]);
-  double DD = -1. / (AA + BB + CC);
+  R BB = 2. * (q.v01 * v[1] + q.v03 * v[3]);
+  R CC = q.v11 * v[1] * v[1] + q.v22 * v[2] * v[2] + q.v33 * v[3] * v[3] + 2. * (q.v13 * v[1] * v[3]);
+  R DD = -1. / (AA + BB + CC);
   double one_over_alpha_sq = -q.n00;
   if (DD < one_over_alpha_sq) DD = one_over_alpha_sq;
   return sqrt(DD);
 }
 
 // returns true if the zone's pflag must be set to -33 (gamma failure)
-static __device__ bool fixup1zone(double gam, double rhoflr, double uuflr, const Geo &q, double *pv, int *fail)
+template <class R>
+static __device__ bool fixup1zone(double gam, double rho_floor, double uu_floor, const Geo &q, R *pv, int *fail)
 {
-  double pre[8];
+  R pre[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) pre[k] = pv[k];
-  State s;
+  StateT<R> s;
   get_state(pv, q, s, fail);
-  double bsq = dot4(s.bcon, s.bcov);
+  R bsq = dot4(s.bcon, s.bcov);
+  R rhoflr = rho_floor, uuflr = uu_floor;
   if (rhoflr < bsq / BSQORHOMAX) rhoflr = bsq / BSQORHOMAX;
   if (uuflr < bsq / BSQOUMAX) uuflr = bsq / BSQOUMAX;
   if (rhoflr < pv[UU] / UORHOMAX) rhoflr = pv[UU] / UORHOMAX;
   bool dofloor = false;
   if (pv[RHO] < rhoflr) { pv[RHO] = rhoflr; dofloor = true; }
   if (pv[UU] < uuflr) { pv[UU] = uuflr; dofloor = true; }
-  double trans;
+  R trans;
   if (dofloor && (trans = 10. * bsq / (pv[RHO] < pv[UU] ? pv[RHO] : pv[UU]) - 1.) > 0.) {
     if (trans > 1.) trans = 1.;
-    double betapar = -s.bcon[0] / ((bsq + SMALL) * s.ucon[0]);
-    double betasq = betapar * betapar * bsq;
+    R betapar = -s.bcon[0] / ((bsq + SMALL) * s.ucon[0]);
+    R betasq = betapar * betapar * bsq;
     double betasqmax = 1. - 1. / (GAMMAMAX * GAMMAMAX);
     if (betasq > betasqmax) betasq = betasqmax;
-    double gdr = 1. / sqrt(1 - betasq);
-    double ucondr[4], Bcon[4], Bcov[4], vcon[4], ucon[4];
+    R gdr = 1. / sqrt(1 - betasq);
+    R ucondr[4], Bcon[4], Bcov[4], vcon[4], ucon[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) ucondr[k] = gdr * (s.ucon[k] + betapar * s.bcon[k]);
     Bcon[0] = 0.;
     Bcon[1] = pv[B1]; Bcon[2] = pv[B2]; Bcon[3] = pv[B3];
     lower(Bcon, q, Bcov);
-    double udotB = dot4(s.ucon, Bcov);
-    double Bsq = dot4(Bcon, Bcov);
-    double B = sqrt(Bsq);
-    double wold = pre[RHO] + pre[UU] * gam;
-    double QdotB = udotB * wold * s.ucon[0];
-    double wnew = pv[RHO] + pv[UU] * gam;
-    double x = 2. * QdotB / (B * wnew * ucondr[0] + SMALL);
-    double vpar = x / (ucondr[0] * (1. + sqrt(1. + x * x)));
-    double one_over_ucondr_t = 1. / ucondr[0];
+    R udotB = dot4(s.ucon, Bcov);
+    R Bsq = dot4(Bcon, Bcov);
+    R B = sqrt(Bsq);
+    R wold = pre[RHO] + pre[UU] * gam;
+    R QdotB = udotB * wold * s.ucon[0];
+    R wnew = pv[RHO] + pv[UU] * gam;
+    R x = 2. * QdotB / (B * wnew * ucondr[0] + SMALL);
+    R vpar = x / (ucondr[0] * (1. + sqrt(1. + x * x)));
+    R one_over_ucondr_t = 1. / ucondr[0];
     vcon[0] = 1.;
 #pragma unroll
     for (int k = 1; k < 4; k++) vcon[k] = vpar * Bcon[k] / (B + SMALL) + ucondr[k] * one_over_ucondr_t;
-    double ut = ut_calc_3vel(vcon, q);
+    R ut = ut_calc_3vel(vcon, q);
 #pragma unroll
     for (int k = 0; k < 4; k++) ucon[k] = ut * vcon[k];
     // ucon_to_utcon (phys.c:255-270)
     const double alpha = q.alpha;
-    double gm = alpha * ucon[0];
+    R gm = alpha * ucon[0];
     double be[4] = {0., q.n01 * alpha * alpha, 0. * alpha * alpha, q.n03 * alpha * alpha};
 #pragma unroll
     for (int k = 1; k < 4; k++) {
-      double utc = ucon[k] + gm * be[k] / alpha;
+      R utc = ucon[k] + gm * be[k] / alpha;
       pv[k + UU] = utc * trans + pre[k + UU] * (1. - trans);
     }
   }
-  double gamma;
+  R gamma;
   if (gamma_calc(pv, q, gamma)) return true;
   if (gamma > GAMMAMAX) {
-    double f = sqrt((GAMMAMAX * GAMMAMAX - 1.) / (gamma * gamma - 1.));
+    R f = sqrt((GAMMAMAX * GAMMAMAX - 1.) / (gamma * gamma - 1.));
     pv[U1] *= f;
     pv[U2] *= f;
     pv[U3] *= f;
@@ -693,12 +772,13 @@ static __device__ bool fixup1zone(double gam, double rhoflr, double uuflr, const
 }
 
 // inflow_check() (bounds.c:333-378)
-__device__ __forceinline__ void inflow_check(double *pr, const Geo &q, int type, int *fail)
+template <class R>
+__device__ __forceinline__ void inflow_check(R *pr, const Geo &q, int type, int *fail)
 {
-  double ucon[4];
+  R ucon[4];
   ucon_calc(pr, q, ucon, fail);
   if (((ucon[1] > 0.) && (type == 0)) || ((ucon[1] < 0.) && (type == 1))) {
-    double gamma;
+    R gamma;
     if (gamma_calc(pr, q, gamma)) *fail = FAIL_GAMMA;
     pr[U1] /= gamma;
     pr[U2] /= gamma;
@@ -706,8 +786,8 @@ __device__ __forceinline__ void inflow_check(double *pr, const Geo &q, int type,
     const double alpha = q.alpha;
     double beta1 = q.n01 * alpha * alpha;
     pr[U1] = beta1 / alpha;
-    double a = pr[U1], b = pr[U2], d = pr[U3];
-    double vsq = q.v11 * a * a + q.v13 * a * d + q.v22 * b * b + q.v13 * d * a + q.v33 * d * d;
+    R a = pr[U1], b = pr[U2], d = pr[U3];
+    R vsq = q.v11 * a * a + q.v13 * a * d + q.v22 * b * b + q.v13 * d * a + q.v33 * d * d;
     if (fabs(vsq) < 1.e-13) vsq = 1.e-13;
     if (vsq >= 1.) vsq = 1. - 1. / (GAMMAMAX * GAMMAMAX);
     gamma = 1. / sqrt(1. - vsq);

@@ -53,35 +53,6 @@ using flux_t = float;
 using flux_t = double;
 #endif
 
-#if !HARM_STEP_MIXED
-template <int DIR>
-__device__ __forceinline__ void face_flux(double gam, const double *pl, const double *pr, const Geo &q, double *F,
-                                          double &ctop, int *fail)
-{
-  State s;
-  double Fl[8], Ul[8], cmaxl, cminl, cmaxr, cminr;
-  get_state(pl, q, s, fail);
-  primtoflux(gam, pl, s, DIR, q.g, Fl);
-  primtoflux(gam, pl, s, 0, q.g, Ul);
-  vchar(gam, pl, s, q, DIR, cmaxl, cminl, fail);
-  get_state(pr, q, s, fail);
-  {
-    double Fr[8], Ur[8];
-    primtoflux(gam, pr, s, DIR, q.g, Fr);
-    primtoflux(gam, pr, s, 0, q.g, Ur);
-    vchar(gam, pr, s, q, DIR, cmaxr, cminr, fail);
-    double t1 = 0. > cmaxl ? 0. : cmaxl;
-    double cmax = fabs(t1 > cmaxr ? t1 : cmaxr);
-    double t2 = 0. > -cminl ? 0. : -cminl;
-    double cmin = fabs(t2 > -cminr ? t2 : -cminr);
-    ctop = cmax > cmin ? cmax : cmin;
-    // HLLF = 0, LAXF = 1 (step_ch.c:66-67): the local Lax-Friedrichs flux
-#pragma unroll
-    for (int k = 0; k < 8; k++) F[k] = 0.5 * (Fl[k] + Fr[k] - ctop * (Ur[k] - Ul[k]));
-  }
-}
-
-#endif
 
 // One thread per face of direction DIR.  Face ranges (step_ch.c:407): dir 1
 // i in [istart, istop+1], j in [jstart-1, jstop+1]; dir 2 i in [istart-1,
@@ -276,36 +247,6 @@ __device__ void zone_fluxes(const Flux &FX, int h, int i, int j, double *f1m, do
     f3p[B2] = -0.5 * (e1b + e1d);
     f3p[B3] = 0.;
   }
-}
-
-// source() (phys.c:165-207); conn stored as [k][min(nu,j)][max(nu,j)]
-__device__ __forceinline__ int conn_slot(int k, int a, int b)
-{
-  int lo = a < b ? a : b, hi = a < b ? b : a;
-  // pairs (lo,hi) with lo <= hi in row order: 00 01 02 03 11 12 13 22 23 33
-  int pair = lo == 0 ? hi : lo == 1 ? 3 + hi : lo == 2 ? 5 + hi : 9;
-  return k * 10 + pair;
-}
-
-__device__ __forceinline__ void source_of_state(double gam, const double *pb, const State &s, const Geo &q,
-                                                const double *__restrict__ conn, long ng, long gi, double *dU)
-{
-  double mhd[4][4];
-#pragma unroll
-  for (int d = 0; d < 4; d++) mhd_calc(gam, pb, d, s, mhd[d]);
-#pragma unroll
-  for (int k = 0; k < 8; k++) dU[k] = 0.;
-#pragma unroll
-  for (int j = 0; j < 4; j++)
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      dU[UU] += mhd[j][k] * __ldg(conn + conn_slot(k, 0, j) * ng + gi);
-      dU[U1] += mhd[j][k] * __ldg(conn + conn_slot(k, 1, j) * ng + gi);
-      dU[U2] += mhd[j][k] * __ldg(conn + conn_slot(k, 2, j) * ng + gi);
-      dU[U3] += mhd[j][k] * __ldg(conn + conn_slot(k, 3, j) * ng + gi);
-    }
-#pragma unroll
-  for (int k = 0; k < 8; k++) dU[k] *= q.g;
 }
 
 __device__ void source(double gam, const double *pb, const Geo &q, const double *__restrict__ conn, long ng, long gi,
@@ -563,6 +504,42 @@ int launch_step(Ctx *x)
   CK(cudaGetLastError());
   return HARM_OK;
 }
+
+#if !HARM_STEP_MIXED
+// launch_half and launch_step as above, also keeping what the discrete adjoint
+// reads back (StepRec); the same kernels in the same order, so the recomputed
+// step is the step
+template <bool FULL>
+static void launch_half_rec(Ctx *x, const double *pi, const double *pb, double *pf, const StepRec &r)
+{
+  const int s = FULL ? 1 : 0;
+  const size_t nc = (size_t)x->G.nc;
+  Bufs B = bufs(x);
+  launch_flux<FULL>(x->G, dim3(x->tbx, x->tby), x->stream, pb, B.F1, B.F2, B.F3, x->geo, x->geo32, x->sc);
+  cudaMemcpyAsync(r.F1rho[s], B.F1 + RHO * nc, nc * sizeof(double), cudaMemcpyDeviceToDevice, x->stream);
+  launch_update<FULL>(x, pi, pb, pf);
+  cudaMemcpyAsync(r.Ub[s], x->Ubuf, 8 * nc * sizeof(double), cudaMemcpyDeviceToDevice, x->stream);
+  if (FULL) k_diag_flux<<<1, 1024, 0, x->stream>>>(x->G, B.F1, x->sc);
+  launch_bound(x, pf);
+  cudaMemcpyAsync(r.X1[s], pf, 8 * nc * sizeof(double), cudaMemcpyDeviceToDevice, x->stream);
+  cudaMemcpyAsync(r.fl1[s], x->pflag, nc, cudaMemcpyDeviceToDevice, x->stream);
+  launch_fixup_utoprim(x, pf);
+  launch_bound(x, pf);
+}
+
+int launch_step_rec(Ctx *x, const StepRec &r)
+{
+  launch_half_rec<false>(x, x->p, x->p, x->ph, r);
+  cudaMemcpyAsync(r.ph, x->ph, 8 * (size_t)x->G.nc * sizeof(double), cudaMemcpyDeviceToDevice, x->stream);
+  launch_half_rec<true>(x, x->p, x->ph, x->p, r);
+  // the corrector's Courant minima, before k_finalize resets them
+  cudaMemcpyAsync(r.sc[0], x->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, x->stream);
+  launch_mass(x);
+  cudaMemcpyAsync(r.sc[1], x->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, x->stream);
+  CK(cudaGetLastError());
+  return HARM_OK;
+}
+#endif
 
 // reps ordinary steps, one kernel at a time with an event after each, so
 // every kernel is timed inside the sequence it runs in; slots: flux, update,

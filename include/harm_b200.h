@@ -35,7 +35,8 @@ enum {
   HARM_E_CUDA = -2,     /* a CUDA runtime call failed */
   HARM_E_NODEV = -3,    /* no usable sm_100 device */
   HARM_E_DT = -11,      /* dt < 1e-9: where the reference calls exit(11) (step_ch.c:126-129) */
-  HARM_E_TIMEOUT = -12  /* a bounded device-side wait ran out */
+  HARM_E_TIMEOUT = -12, /* a bounded device-side wait ran out */
+  HARM_E_ADJOINT = -13  /* the adjoint cannot follow the steps (a step failed; see harm_last_error) */
 };
 
 /* Arithmetic of the step (harm_set_precision). */
@@ -204,6 +205,21 @@ int harm_restart_read(harm_ctx *ctx, const char *path, const harm_grid_spec *g, 
    the reference does.  g gives R0 and hslope.  With COOL_EOS the zones'
    temperature guesses move as the reference's dump() moves them. */
 int harm_dump_write(harm_ctx *ctx, const harm_restart_header *hdr, const harm_grid_spec *g, const char *path);
+
+/* Discrete adjoint of nsteps steps of step_ch() (2D gamma-law FP64 step; no
+   reference counterpart).  Runs the steps from the context's state (the
+   context ends where they end, as after harm_run), sets *J to the mass that
+   crossed the inner radial boundary meanwhile -- the change of mass_in
+   (diag.c:578, mass_in += mdot_in*Dt) -- and grad to dJ/dp of the state at the
+   call, in harm_get_prims' layout (every cell and primitive, ghosts included).
+   Reverse sweep: states kept every checkpoint_every steps, each segment
+   recomputed by the step's own kernels, then transposed step by step (limiter
+   branches, floors and wave-speed choices frozen at the forward's; the
+   inversion differentiated through primtoU at its converged solution).  ms,
+   if not NULL, gets the device time of the forward pass (ms[0]) and of the
+   reverse sweep with its recomputation (ms[1]).  Refused for 3D, COOL_EOS,
+   the mixed step and attached tracers; HARM_E_ADJOINT if a step fails. */
+int harm_adjoint_mass_in(harm_ctx *ctx, int nsteps, int checkpoint_every, double *J, double *grad, double *ms);
 
 /* ---- diagnostics ---- */
 

@@ -25,6 +25,7 @@ files).  Fixtures hold only generated numbers:
 Each configuration runs in its own process: the reference keeps its state in
 globals.
 """
+import ctypes
 import hashlib
 import os
 import subprocess
@@ -347,6 +348,46 @@ def cool_config(cfg):
     np.savez_compressed(os.path.join(HERE, "cool_%s.npz" % cfg), **out)
 
 
+def adjoint_config(cfg, m=16, seed=3, nsteps=10):
+    """Central differences, taken on the reference's own step, of J = the change
+    of mass_in (diag.c:578) over nsteps steps with respect to the amplitudes of
+    the seeded density modes of harm_cool_b200.adjoint.Modes, and J at zero
+    amplitudes: the check of the device adjoint's dJ/dA_m.  h = 1e-9: the
+    atmosphere sits within ~1e-7 of its density floor, and a larger step
+    straddles the floor's kink (fixup.c:142-187)."""
+    sys.path.insert(0, ROOT)
+    from oracle.pyoracle import Reference
+    from harm_cool_b200.adjoint import Modes
+    ref = Reference(cfg)
+    assert ref.n3 == 1 and ref.n1 == ref.n2
+    p0 = ref.p.copy()
+    t0, dt0 = ref.get("t"), ref.get("dt")
+    modes = Modes(ref.n1, ref.n2, m=m, seed=seed)
+
+    def J(amps):
+        ref.p[...] = p0
+        ref.set("t", t0)
+        ref.set("dt", dt0)
+        modes.apply(ref.p, amps)
+        ref.lib.ref_bound_prim(ref.p.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        m0 = ref.get("mass_in")
+        for _ in range(nsteps):
+            ref.step()
+        return ref.get("mass_in") - m0
+
+    J0 = J(np.zeros(m))
+    h = 1e-9
+    fd = np.zeros(m)
+    for k in range(m):
+        a = np.zeros(m)
+        a[k] = h
+        jp = J(a)
+        a[k] = -h
+        fd[k] = (jp - J(a)) / (2 * h)
+    np.savez_compressed(os.path.join(HERE, "adjoint_%s.npz" % cfg), setup=np.array([ref.n1, m, seed, nsteps]),
+                        J=np.array(J0), fd=fd)
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1:
         if sys.argv[1] == "kat":
@@ -363,6 +404,8 @@ if __name__ == "__main__":
             cool_config(sys.argv[1][len("cool_"):])
         elif sys.argv[1].startswith("dump_"):
             dump_config(sys.argv[1][len("dump_"):])
+        elif sys.argv[1].startswith("adjoint_"):
+            adjoint_config(sys.argv[1][len("adjoint_"):])
         else:
             one_config(sys.argv[1])
         sys.exit(0)
@@ -371,7 +414,7 @@ if __name__ == "__main__":
     for cfg in ("t2d", "t3d", "r2d", "r3d", "ce2d", "ce3d"):
         build_ref.build_config(cfg, force=True)
     for arg in ("t2d", "t3d", "kat", "tracers_r2d", "tracers_r3d", "diag_t2d", "diag_t3d",
-                "restart_r2d", "restart_t3d", "eos_ce2d", "cool_ce2d", "cool_ce3d", "dump_t2d", "dump_t3d"):
+                "restart_r2d", "restart_t3d", "eos_ce2d", "cool_ce2d", "cool_ce3d", "dump_t2d", "dump_t3d", "adjoint_t2d"):
         subprocess.run([sys.executable, os.path.abspath(__file__), arg], check=True,
                        stderr=subprocess.DEVNULL)
     for f in sorted(os.listdir(HERE)):

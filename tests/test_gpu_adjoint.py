@@ -1,0 +1,137 @@
+"""The discrete adjoint of the 2D gamma-law step (harm_adjoint_mass_in) against
+central differences of the step itself.
+
+J is the mass that crosses the inner radial boundary during K steps (mass_in,
+diag.c:578).  The step is bit-identical to the reference's, so a central
+difference of the device step is a central difference of the reference code;
+tests/golden/adjoint_t2d.npz also holds differences taken on the reference
+itself (make_golden.py).  Tolerance: 1e-4 relative to the largest component
+of the gradient compared.
+
+Step of the differences: h = 1e-9 relative.  The torus' atmosphere sits within
+~1e-7 (relative) of its density floor, which fixup() re-applies every step, so
+a difference with h = 1e-6 straddles the floor's kink in many zones and
+averages a slope of 1 with a slope of 0; the adjoint gives the derivative of
+the branch the step took, which the smaller step resolves.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import harm_cool_b200 as hc
+from harm_cool_b200 import adjoint as ad
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+TOL = 1e-4
+H = 1e-9
+
+
+def _context(n1, n2):
+    return hc.Context(hc.torus_problem(n1, n2, 1))
+
+
+def _mass_in_from(ctx, p, nsteps):
+    ctx.init_torus()  # t, dt and the counters as at the start
+    ctx.put_prims(p)
+    m0 = ctx.diag()["mass_in"]
+    for _ in range(nsteps):
+        ctx.step_ch()
+    ctx.sync()
+    return ctx.diag()["mass_in"] - m0
+
+
+def _smooth_direction(shape, seed):
+    """a smooth random field per primitive on the active zones of plane 0"""
+    rng = np.random.default_rng(seed)
+    _, sn1, sn2, _ = shape
+    n1, n2 = sn1 - 4, sn2 - 4
+    x1 = (np.arange(n1) + 0.5) / n1
+    x2 = (np.arange(n2) + 0.5) / n2
+    v = np.zeros(shape)
+    for k in range(8):
+        f = np.zeros((n1, n2))
+        for _ in range(3):
+            a, b = rng.integers(1, 5, size=2)
+            f += rng.normal() * np.outer(np.sin(np.pi * a * x1 + rng.uniform(0, 6.28)), np.sin(np.pi * b * x2))
+        v[0, 2:2 + n1, 2:2 + n2, k] = f
+    return v
+
+
+@pytest.mark.parametrize("nsteps,every", [(6, 4), (12, 5)])
+def test_state_direction_against_central_difference(nsteps, every):
+    ctx = _context(48, 48)
+    ctx.init_torus()
+    p0 = ctx.get_prims()
+    v = _smooth_direction(p0.shape, seed=nsteps)
+    # perturbations relative to each cell's own value (velocities and fields:
+    # plus a thousandth of their scale on the grid, many start at zero)
+    scale = np.array([np.abs(p0[..., k]).max() for k in range(8)])
+    v *= np.abs(p0) + 1e-3 * scale * (np.arange(8) >= 2)
+    J, lam, ms = ctx.adjoint_mass_in(nsteps, every)
+    # the context has advanced: J again by the plain steps
+    J0 = _mass_in_from(ctx, p0, nsteps)
+    assert J == J0
+    h = H
+    Jp = _mass_in_from(ctx, p0 + h * v, nsteps)
+    Jm = _mass_in_from(ctx, p0 - h * v, nsteps)
+    fd = (Jp - Jm) / (2 * h)
+    ad_ = float(np.sum(lam * v))
+    assert abs(ad_ - fd) <= TOL * abs(fd), (ad_, fd)
+
+
+def test_checkpoint_spacing_does_not_change_the_gradient():
+    ctx = _context(32, 32)
+    ctx.init_torus()
+    p0 = ctx.get_prims()
+    J1, l1, _ = ctx.adjoint_mass_in(9, 9)
+    ctx.init_torus()
+    ctx.put_prims(p0)
+    J2, l2, _ = ctx.adjoint_mass_in(9, 2)
+    assert J1 == J2
+    np.testing.assert_allclose(l2, l1, rtol=1e-12, atol=1e-12 * np.abs(l1).max())
+
+
+def test_parameter_gradient_against_central_difference():
+    """dJ/d(rmax, beta, A_1..A_16) on a 48x48 torus over 10 steps"""
+    ctx = _context(48, 48)
+    modes = ad.Modes(48, 48, m=16, seed=3)
+    amps = np.zeros(16)
+    J, g, info = ad.mass_in_gradient(ctx, modes, 12.0, 100.0, amps, 10, checkpoint_every=4, rel_step=H)
+    theta = np.concatenate([[12.0, 100.0], amps])
+    fd = np.zeros_like(g)
+    for k in range(len(theta)):
+        h = H * max(abs(theta[k]), 1.0)
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += h
+        tm[k] -= h
+        fd[k] = (ad.mass_in(ctx, modes, tp[0], tp[1], tp[2:], 10) - ad.mass_in(ctx, modes, tm[0], tm[1], tm[2:], 10)) / (2 * h)
+    scale = np.abs(fd).max()
+    assert scale > 0
+    np.testing.assert_allclose(g, fd, rtol=0, atol=TOL * scale)
+
+
+def test_against_reference_central_differences():
+    """dJ/dA_m against central differences taken on the reference's own step
+    (32x32 torus, 10 steps; fixture written by make_golden.py)"""
+    f = np.load(os.path.join(HERE, "golden", "adjoint_t2d.npz"))
+    n, m, seed, nsteps = (int(x) for x in f["setup"])
+    ctx = _context(n, n)
+    modes = ad.Modes(n, n, m=m, seed=seed)
+    J, g, _ = ad.mass_in_gradient(ctx, modes, 12.0, 100.0, np.zeros(m), nsteps, checkpoint_every=4, rel_step=H)
+    assert J == f["J"]
+    fd = f["fd"]
+    np.testing.assert_allclose(g[2:], fd, rtol=0, atol=TOL * np.abs(fd).max())
+
+
+def test_refusals():
+    ctx3 = hc.Context(hc.torus_problem(16, 16, 4))
+    ctx3.init_torus()
+    with pytest.raises(hc.HarmError):
+        ctx3.adjoint_mass_in(2, 1)
+    ctx = _context(16, 16)
+    ctx.init_torus()
+    ctx.set_precision(hc.Context.MIXED)
+    with pytest.raises(hc.HarmError):
+        ctx.adjoint_mass_in(2, 1)
