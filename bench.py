@@ -361,6 +361,63 @@ def run_ensemble(args):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args):
+    """The discrete adjoint on a 2D gamma-law torus (192x192, K = 50 steps,
+    checkpoint every 10): J = the mass that crosses the inner boundary over the K
+    steps (mass_in, diag.c:578), dJ/d(rmax, beta, A_1..A_16) -- A the amplitudes
+    of 16 seeded density modes -- through one adjoint sweep, against central
+    differences of the step (h = 1e-9, which resolves the branches the step takes;
+    h = 1e-6 straddles the density floor that the atmosphere sits within ~1e-7
+    of).  Cost: the adjoint's device time (forward with checkpoints, reverse sweep
+    with its recomputation) over the plain forward's (graph replay of K steps)."""
+    import numpy as np
+    import harm_cool_b200 as hc
+    from harm_cool_b200 import adjoint as ad
+    n, K, every = args.adj_n, args.adj_steps, args.adj_every
+    ctx = hc.Context(hc.torus_problem(n, n, 1))
+    modes = ad.Modes(n, n, m=16, seed=args.seed)
+    amps = np.zeros(16)
+    theta = np.concatenate([[12.0, 100.0], amps])
+    sampler = ClockSampler(0)
+    sampler.start()
+    fwd = []
+    for r in range(args.warmup + 5):
+        ad.initial_state(ctx, modes, 12.0, 100.0, amps)
+        fwd.append(ctx.run_timed(K))
+    fwd_ms = sorted(fwd[args.warmup:])[2]
+    runs = []
+    for r in range(args.warmup + 5):
+        ad.initial_state(ctx, modes, 12.0, 100.0, amps)
+        J, lam, ms = ctx.adjoint_mass_in(K, every)
+        runs.append(ms)
+    clocks = sampler.stop()
+    runs = sorted(runs[args.warmup:], key=lambda m: m[0] + m[1])
+    ms = runs[2]
+    J, g, info = ad.mass_in_gradient(ctx, modes, 12.0, 100.0, amps, K, every, rel_step=1e-9)
+    fd = {}
+    for hr in (1e-9, 1e-6):
+        d = np.zeros(len(theta))
+        for k in range(len(theta)):
+            h = hr * max(abs(theta[k]), 1.0)
+            tp, tm = theta.copy(), theta.copy()
+            tp[k] += h
+            tm[k] -= h
+            d[k] = (ad.mass_in(ctx, modes, tp[0], tp[1], tp[2:], K) - ad.mass_in(ctx, modes, tm[0], tm[1], tm[2:], K)) / (2 * h)
+        fd[hr] = d
+    scale = float(np.abs(fd[1e-9]).max())
+    err = {("h=%g" % hr): float(np.abs(g - d).max() / scale) for hr, d in fd.items()}
+    line = {"metric": "adjoint / forward device time, 2D %dx%d torus, K=%d" % (n, n, K), "value": (ms[0] + ms[1]) / fwd_ms,
+            "unit": "x", "n_gpus": 1, "steps": K, "warmup": args.warmup, "higher_is_better": False, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "adjoint of %d steps of the 2D gamma-law step, %dx%d torus "
+                                                        "a=0.9375 rin=6 rmax=12 beta=100, checkpoint every %d, 16 density "
+                                                        "modes seed %d" % (K, n, n, every, args.seed)},
+            "forward_ms": fwd_ms, "adjoint_ms": {"forward_with_checkpoints": ms[0], "reverse_sweep": ms[1]},
+            "J": J, "parameters": ["rmax", "beta"] + ["A%d" % (m + 1) for m in range(16)],
+            "gradient": g.tolist(), "central_difference": {("h=%g" % hr): d.tolist() for hr, d in fd.items()},
+            "max_abs_error_over_max_gradient": err, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
 def tracers_by_density(np, pr, p, n, seed):
     """n tracer particles at zone centres drawn with probability proportional to
     the zone's rest mass rho sqrt(-g) dV (seeded); labels (i, j, h) of the zone."""
@@ -501,7 +558,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
-    ap.add_argument("--workload", choices=("torus", "ensemble", "cool"), default="torus",
+    ap.add_argument("--workload", choices=("torus", "ensemble", "cool", "adjoint"), default="torus",
                     help="torus: the 288x256x256 step (default); ensemble: 64 seeded 2D tori; "
                          "cool: the 256x256 COOL_EOS step")
     ap.add_argument("--cool-n", type=int, default=256)
@@ -510,6 +567,9 @@ def main():
                     help="reference: cooleos.c's 72x72 tables and units; baseline: 200x200 tables over "
                          "rho 1e4-1e14, T 1e8-1e12 with the torus maximum at 1e11 g/cm^3")
     ap.add_argument("--dump-cool", default=None, help="save the FP64 and mixed COOL_EOS states (npz)")
+    ap.add_argument("--adj-n", type=int, default=192, help="adjoint workload: N1 = N2")
+    ap.add_argument("--adj-steps", type=int, default=50, help="adjoint workload: steps K")
+    ap.add_argument("--adj-every", type=int, default=10, help="adjoint workload: checkpoint spacing")
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--seed", type=int, default=0)
     args = ap.parse_args()
@@ -524,6 +584,9 @@ def main():
         return
     if args.workload == "cool":
         run_cool(args)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args)
         return
     world, rank, local = dist_setup()
     try:

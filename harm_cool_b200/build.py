@@ -58,9 +58,15 @@ def build(force=False, verbose=False):
           os.path.join(CSRC, "host_setup.cpp"), "-o", host_o] + inc)
     objs = [host_o]
 
+    # a unit is recompiled when its object is older than the unit or any header
+    headers = max(os.path.getmtime(f) for f in _sources() if not f.endswith((".cu", ".cpp")))
+
     def compile_unit(item):
         unit, flags = item
         o = os.path.join(BUILD, unit.replace(".cu", ".o"))
+        src = os.path.join(CSRC, unit)
+        if not force and os.path.exists(o) and os.path.getmtime(o) >= max(os.path.getmtime(src), headers):
+            return o, ""
         out = _run([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xptxas", "-v", "-Xcompiler", "-fPIC",
                                     "-Xcompiler", "-ffp-contract=off", "-c", os.path.join(CSRC, unit),
                                     "-o", o] + flags + inc)

@@ -33,7 +33,6 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <cstring>
 #include <vector>
 
 #include "harm_common.cuh"
@@ -43,17 +42,50 @@
 namespace harm {
 namespace adj {
 
-constexpr int NWF = 4;  // tangent directions per pass of a face flux (16 inputs: 4 passes)
 constexpr int FU_THREADS = 1024;
 enum { ERR_FAILS = 1, ERR_SINGULAR = 2 };
 
 using D8 = Dual<8>;
 
+// the adjoint's scalar chain through the time step, kept on the device
+struct AdjScalars {
+  double lam_dt_next;  // dJ/d dt^{n+1} (all later steps)
+  double ln[2];        // adjoints of the corrector's Courant minima n1, n2
+  double lDt[2];       // dJ/dDt of the predictor's and the corrector's update
+  int claim[2];        // the face that set each minimum has been found
+};
+
+// before step n's reverse: dt^{n+1} = min(ndt, 1.3 dt^n), ndt = defcon / (1/n1 + 1/n2)
+// (step_ch.c:126-137); sa is the run state before k_finalize, sb after
+__global__ void k_adj_dt_pre(const DevScalars *sa, const DevScalars *sb, double defcon, AdjScalars *a)
+{
+  const double dt = sa->dt, ndt = sb->ndt;
+  const double n1 = __longlong_as_double((long long)sa->ndt_bits[0]);
+  const double n2 = __longlong_as_double((long long)sa->ndt_bits[1]);
+  const double lam_ndt = ndt > SAFE * dt ? 0. : a->lam_dt_next;
+  const double S = 1. / n1 + 1. / n2;
+  a->ln[0] = lam_ndt * defcon / (n1 * n1) / (S * S);
+  a->ln[1] = lam_ndt * defcon / (n2 * n2) / (S * S);
+  a->lDt[0] = a->lDt[1] = 0.;
+  a->claim[0] = a->claim[1] = 0;
+}
+
+// after it: dJ/d dt^n = din^n (J = sum dt din) + the ramp + both updates' Dt
+__global__ void k_adj_dt_post(const DevScalars *sa, const DevScalars *sb, AdjScalars *a)
+{
+  const double dt = sa->dt, ndt = sb->ndt;
+  double l = sb->mdot_in + 0.5 * a->lDt[0] + a->lDt[1];
+  if (ndt > SAFE * dt) l += SAFE * a->lam_dt_next;
+  a->lam_dt_next = l;
+}
+
 // ---------------------------------------------------------------------------
 // objective: dt^n * din^n on the inner ghost row of p^{n+1} (diag.c:499)
 
-__global__ void k_adj_din(Grid G, const double *__restrict__ P, const double *__restrict__ geo, double *lam, double w)
+__global__ void k_adj_din(Grid G, const double *__restrict__ P, const double *__restrict__ geo, double *lam,
+                          const DevScalars *sa)
 {
+  const double w = sa->dt;
   const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
   if (j > G.jstop) return;
   const int i = G.istart - 1;
@@ -159,7 +191,7 @@ __global__ void __launch_bounds__(FU_THREADS) k_adj_fixup_utoprim(Grid G, const 
     if (fl1[cidx(G, 0, i, j)] != 0) m++;
   }
   cnt[tid] = m;
-  __syncthreads();
+  if (__syncthreads_or(m) == 0) return;  // no failed zone: nothing was repaired
   if (tid == 0) {
     int s = 0;
     for (int k = 0; k < FU_THREADS; k++) {
@@ -284,8 +316,10 @@ __device__ bool solve8t(const double (*A)[8], const double *b, double *x)
 
 // lamf: adjoint of the half step's output pf (its active cells are consumed);
 // lamU: adjoint of the conserved variables the update formed; lampi: adjoint of
-// the inversion's guess pi (a failed zone keeps it)
-__global__ void __launch_bounds__(128) k_adj_invert(Grid G, const double *__restrict__ Ub, const double *__restrict__ pi,
+// the inversion's guess pi (a failed zone keeps it).  Zr, wz: the inversion's
+// output before fixup() and which inversion gave it, as the step recorded them.
+__global__ void __launch_bounds__(128) k_adj_invert(Grid G, const double *__restrict__ Zr,
+                                                    const signed char *__restrict__ wz,
                                                     const double *__restrict__ geo, const double *__restrict__ floors,
                                                     const double *__restrict__ katm, double *lamf, double *lamU,
                                                     double *lampi, int *err)
@@ -297,24 +331,12 @@ __global__ void __launch_bounds__(128) k_adj_invert(Grid G, const double *__rest
   const long gi = (long)i * G.sn2 + j;
   Geo q;
   load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
-  double U[8], z[8];
+  double z[8];
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    U[k] = Ub[k * G.nc + c];
-    z[k] = pi[k * G.nc + c];
-  }
-  // the step's inversion, repeated on the recorded U and guess (step_ch.c:265-300)
+  for (int k = 0; k < 8; k++) z[k] = Zr[k * G.nc + c];
+  const int w = wz[c];
+  const int flag = w < 0, which = w < 0 ? 0 : w;
   const double K = katm[i];
-  int which = 0;
-  int flag = utoprim<0>(G.gam, 0., U, q, z);
-  if (flag) {
-    which = 1;
-    flag = utoprim<1>(G.gam, K, U, q, z);
-    if (flag) {
-      which = 2;
-      flag = utoprim<2>(G.gam, K, U, q, z);
-    }
-  }
   double lo[8], lz[8], lu[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) {
@@ -322,17 +344,30 @@ __global__ void __launch_bounds__(128) k_adj_invert(Grid G, const double *__rest
     lamf[k * G.nc + c] = 0.;
   }
   {
-    D8 v[8];
+    // fixup() leaves most zones alone: there its Jacobian is the identity
+    double v0[8];
+    bool same = true;
 #pragma unroll
-    for (int k = 0; k < 8; k++) v[k] = D8::seed(z[k], k);
+    for (int k = 0; k < 8; k++) v0[k] = z[k];
     int fail = 0;
-    fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
+    fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v0, &fail);
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      double a = 0.;
+    for (int k = 0; k < 8; k++) same &= v0[k] == z[k];
+    if (same) {
 #pragma unroll
-      for (int o = 0; o < 8; o++) a += lo[o] * v[o].d[k];
-      lz[k] = a;
+      for (int k = 0; k < 8; k++) lz[k] = lo[k];
+    } else {
+      D8 v[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) v[k] = D8::seed(z[k], k);
+      fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        double a = 0.;
+#pragma unroll
+        for (int o = 0; o < 8; o++) a += lo[o] * v[o].d[k];
+        lz[k] = a;
+      }
     }
   }
   if (flag == 0) {
@@ -406,8 +441,11 @@ __global__ void __launch_bounds__(128) k_adj_cons(Grid G, const double *__restri
                                                   const double *__restrict__ Ub, const double *__restrict__ F1rho,
                                                   const double *__restrict__ geo, const double *__restrict__ conn,
                                                   const double *__restrict__ lamU, double *lampi, double *lampb,
-                                                  double *lamF1, double *lamF2, double Dt, double *lamDt)
+                                                  double *lamF1, double *lamF2, const DevScalars *sa,
+                                                  AdjScalars *as)
 {
+  const double Dt = FULL ? sa->dt : 0.5 * sa->dt;
+  double *lamDt = &as->lDt[FULL ? 1 : 0];
   const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
   const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
   double lDt = 0.;
@@ -514,8 +552,8 @@ __global__ void __launch_bounds__(128) k_adj_cons(Grid G, const double *__restri
 
 template <int DIR, bool FULL>
 __global__ void __launch_bounds__(128) k_adj_flux(Grid G, const double *__restrict__ pb, const double *__restrict__ geo,
-                                                  const double *__restrict__ lamF, double *lamp, double lnd,
-                                                  double nmin, int *claim)
+                                                  const double *__restrict__ lamF, double *lamp,
+                                                  const DevScalars *sa, AdjScalars *as)
 {
   const int j = (DIR == 2 ? G.jstart : G.jstart - 1) + blockIdx.x * blockDim.x + threadIdx.x;
   const int i = (DIR == 1 ? G.istart : G.istart - 1) + blockIdx.y * blockDim.y + threadIdx.y;
@@ -530,6 +568,9 @@ __global__ void __launch_bounds__(128) k_adj_flux(Grid G, const double *__restri
     any |= lF[k] != 0.;
   }
   const bool act = FULL && i >= G.istart && i <= G.istop && j >= G.jstart && j <= G.jstop;
+  const double lnd = FULL ? as->ln[DIR - 1] : 0.;
+  const double nmin = FULL ? __longlong_as_double((long long)sa->ndt_bits[DIR - 1]) : 0.;
+  const double dxd = DIR == 1 ? G.dx1 : G.dx2;
   if (!any && !(act && lnd != 0.)) return;
   const long o1 = DIR == 1 ? c - 2 * G.sn2 : c - 2, o2 = DIR == 1 ? c - G.sn2 : c - 1,
              o3 = DIR == 1 ? c + G.sn2 : c + 1;
@@ -552,29 +593,39 @@ __global__ void __launch_bounds__(128) k_adj_flux(Grid G, const double *__restri
   }
   Geo q;
   load_geo(geo_at(geo, G, DIR == 1 ? L_FACE1 : L_FACE2), G.ng, (long)i * G.sn2 + j, q);
-  double lpl[8], lpr[8], lct = 0.;
-  for (int c0 = 0; c0 < 16; c0 += NWF) {
-    using DF = Dual<NWF>;
-    DF L[8], R[8], F[8], ct;
+  // plain values of both sides: the other side's constants in each
+  // linearisation below, and the face's wave speed
+  double Flv[8], Ulv[8], cxl, cnl, Frv[8], Urv[8], cxr, cnr, Fz[8], ctz;
+  int f0 = 0;
+  face_side<DIR>(G.gam, pl, q, Flv, Ulv, cxl, cnl, &f0);
+  face_side<DIR>(G.gam, pr, q, Frv, Urv, cxr, cnr, &f0);
+  lf_flux(Flv, Ulv, cxl, cnl, Frv, Urv, cxr, cnr, Fz, ctz);
+  // the face that set the Courant minimum gets the adjoint of its wave speed
+  double lct = 0.;
+  if (act && lnd != 0. && G.cour * dxd / ctz == nmin && atomicCAS(&as->claim[DIR - 1], 0, 1) == 0)
+    lct = -lnd * nmin / ctz;
+  if (!any && lct == 0.) return;
+  double lpl[8], lpr[8];
+  for (int side = 0; side < 2; side++) {
+    const double *pv = side ? pr : pl;
+    D8 P[8], Fs[8], Us[8], cx, cn, Fo[8], Uo[8], F[8], ct;
+#pragma unroll
+    for (int k = 0; k < 8; k++) P[k] = D8::seed(pv[k], k);
+    face_side<DIR>(G.gam, P, q, Fs, Us, cx, cn, &f0);
 #pragma unroll
     for (int k = 0; k < 8; k++) {
-      L[k] = DF::seed(pl[k], k - c0);
-      R[k] = DF::seed(pr[k], 8 + k - c0);
+      Fo[k] = D8(side ? Flv[k] : Frv[k]);
+      Uo[k] = D8(side ? Ulv[k] : Urv[k]);
     }
-    int fail = 0;
-    face_flux<DIR>(G.gam, L, R, q, F, ct, &fail);
-    if (c0 == 0 && act && lnd != 0.) {
-      const double dxd = DIR == 1 ? G.dx1 : G.dx2;
-      if (G.cour * dxd / ct.v == nmin && atomicCAS(claim, 0, 1) == 0) lct = -lnd * nmin / ct.v;
-    }
+    if (side == 0) lf_flux(Fs, Us, cx, cn, Fo, Uo, D8(cxr), D8(cnr), F, ct);
+    else lf_flux(Fo, Uo, D8(cxl), D8(cnl), Fs, Us, cx, cn, F, ct);
+    double *out = side ? lpr : lpl;
 #pragma unroll
-    for (int m = 0; m < NWF; m++) {
-      double s = lct * ct.d[m];
+    for (int m = 0; m < 8; m++) {
+      double a = lct * ct.d[m];
 #pragma unroll
-      for (int k = 0; k < 8; k++) s += lF[k] * F[k].d[m];
-      const int in = c0 + m;
-      if (in < 8) lpl[in] = s;
-      else lpr[in - 8] = s;
+      for (int k = 0; k < 8; k++) a += lF[k] * F[k].d[m];
+      out[m] = a;
     }
   }
 #pragma unroll
@@ -610,13 +661,6 @@ struct DevBuf {
   }
 };
 
-static double bits_to_double(unsigned long long b)
-{
-  double d;
-  std::memcpy(&d, &b, sizeof d);
-  return d;
-}
-
 static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, double *ms)
 {
   const Grid &G = x->G;
@@ -633,8 +677,8 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
   DevScalars *cks = B.get<DevScalars>(nseg + 1);
   double *pend = B.get<double>(pl);
   double *recp = B.get<double>(pl * (nrec + 1));
-  double *recd = B.get<double>((size_t)nrec * (5 * pl + 2 * nc));
-  signed char *recf = B.get<signed char>((size_t)nrec * 2 * nc);
+  double *recd = B.get<double>((size_t)nrec * (7 * pl + 2 * nc));
+  signed char *recf = B.get<signed char>((size_t)nrec * 4 * nc);
   DevScalars *recs = B.get<DevScalars>((size_t)nrec * 2);
   double *lam = B.get<double>(6 * pl);  // next, cur, ph, U, F1, F2
   double *W = B.get<double>(pl);
@@ -642,23 +686,25 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
   int *list = B.get<int>(FAIL_CAP);
   double *vbuf = B.get<double>((size_t)FAIL_CAP * 8);
   signed char *kinds = B.get<signed char>(FAIL_CAP);
-  int *ierr = B.get<int>(4);  // err, claim[2]
-  double *lamDt = B.get<double>(2);
+  int *err = B.get<int>(1);
+  AdjScalars *as = B.get<AdjScalars>(1);
   if (!ck || !cks || !pend || !recp || !recd || !recf || !recs || !lam || !W || !Wf || !list || !vbuf || !kinds ||
-      !ierr || !lamDt)
+      !err || !as)
     return fail_with(HARM_E_CUDA, "device memory for the adjoint");
   std::vector<StepRec> rec(nrec);
   for (int r = 0; r < nrec; r++) {
-    double *d = recd + (size_t)r * (5 * pl + 2 * nc);
+    double *d = recd + (size_t)r * (7 * pl + 2 * nc);
     StepRec &s = rec[r];
     s.X1[0] = d; s.X1[1] = d + pl; s.Ub[0] = d + 2 * pl; s.Ub[1] = d + 3 * pl; s.ph = d + 4 * pl;
-    s.F1rho[0] = d + 5 * pl; s.F1rho[1] = d + 5 * pl + nc;
-    s.fl1[0] = recf + (size_t)r * 2 * nc; s.fl1[1] = s.fl1[0] + nc;
+    s.Z[0] = d + 5 * pl; s.Z[1] = d + 6 * pl;
+    s.F1rho[0] = d + 7 * pl; s.F1rho[1] = d + 7 * pl + nc;
+    s.fl1[0] = recf + (size_t)r * 4 * nc; s.fl1[1] = s.fl1[0] + nc;
+    s.wz[0] = s.fl1[0] + 2 * nc; s.wz[1] = s.fl1[0] + 3 * nc;
     s.sc[0] = recs + 2 * r; s.sc[1] = recs + 2 * r + 1;
   }
-  double *lnext = lam, *lcur = lam + pl, *lh = lam + 2 * pl, *lU = lam + 3 * pl, *lF1 = lam + 4 * pl,
-         *lF2 = lam + 5 * pl;
-  int *err = ierr, *claim = ierr + 1;
+  // the adjoint of the state after the step being undone (A) and before it (B)
+  double *const A = lam, *const Bl = lam + pl, *lh = lam + 2 * pl, *lU = lam + 3 * pl, *lF1 = lam + 4 * pl,
+                *lF2 = lam + 5 * pl;
   cudaStream_t st = x->stream;
   cudaEvent_t e0, e1, e2;
   CK(cudaEventCreate(&e0));
@@ -668,20 +714,119 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
     cudaEvent_t a, b, c;
     ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); }
   } eg{e0, e1, e2};
-
-  // forward pass, keeping a checkpoint every `every` steps
-  CK(cudaMemsetAsync(ierr, 0, 4 * sizeof(int), st));
-  CK(cudaEventRecord(e0, st));
-  for (int n = 0; n < nsteps; n++) {
-    if (n % every == 0) {
-      CK(cudaMemcpyAsync(ck + (size_t)(n / every) * pl, x->p, pl * sizeof(double), cudaMemcpyDeviceToDevice, st));
-      CK(cudaMemcpyAsync(cks + n / every, x->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, st));
+  struct Graph {
+    cudaGraphExec_t e = nullptr;
+    ~Graph() { if (e) cudaGraphExecDestroy(e); }
+  };
+  auto capture = [&](Graph &g, auto &&body) -> int {
+    cudaGraph_t gr;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = body();
+    cudaError_t e = cudaStreamEndCapture(st, &gr);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail_with(HARM_E_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&g.e, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) return fail_with(HARM_E_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+    return HARM_OK;
+  };
+  const size_t pb = pl * sizeof(double);
+  // one segment's steps, recorded (recomputation): states before each step and after the last
+  auto record = [&](int len) -> int {
+    for (int r = 0; r < len; r++) {
+      CK(cudaMemcpyAsync(recp + (size_t)r * pl, x->p, pb, cudaMemcpyDeviceToDevice, st));
+      int rc = exact::launch_step_rec(x, rec[r]);
+      if (rc) return rc;
     }
-    int rc = exact::launch_step(x);
+    CK(cudaMemcpyAsync(recp + (size_t)len * pl, x->p, pb, cudaMemcpyDeviceToDevice, st));
+    return HARM_OK;
+  };
+
+  const dim3 tile(32, 4);
+  const dim3 zg((G.n2 + 31) / 32, (G.n1 + 3) / 4, 1);
+  const dim3 g1((G.n2 + 2 + 31) / 32, (G.n1 + 1 + 3) / 4, 1);
+  const dim3 g2((G.n2 + 1 + 31) / 32, (G.n1 + 2 + 3) / 4, 1);
+  const int nbc = 4 * G.sn2 + 4 * (G.sn1 - 4);
+  // the reverse of one recorded segment of len steps: the adjoint of its last
+  // state in A on entry, of its first state in A on exit, B zero both times
+  auto reverse = [&](int len) -> int {
+    double *lnext = A, *lcur = Bl;
+    for (int r = len - 1; r >= 0; r--) {
+      const StepRec &q = rec[r];
+      const DevScalars *sa = q.sc[0], *sb = q.sc[1];
+      const double *pn = recp + (size_t)r * pl, *pnext = recp + (size_t)(r + 1) * pl;
+      k_adj_dt_pre<<<1, 1, 0, st>>>(sa, sb, G.defcon, as);
+      // objective term on the step's result
+      k_adj_din<<<(G.n2 + 127) / 128, 128, 0, st>>>(G, pnext, x->geo, lnext, sa);
+      // corrector: bound_prim, fixup_utoprim, bound_prim, inversion, update, fluxes
+      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, pnext, x->geo, lnext);
+      k_adj_fixup_utoprim<<<1, FU_THREADS, 0, st>>>(G, q.X1[1], q.fl1[1], x->geo, x->floors, W, Wf, list, vbuf,
+                                                   kinds, lnext, err);
+      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, q.X1[1], x->geo, lnext);
+      k_adj_invert<<<zg, tile, 0, st>>>(G, q.Z[1], q.wz[1], x->geo, x->floors, x->katm, lnext, lU, lcur, err);
+      CK(cudaMemsetAsync(lF1, 0, 2 * pb, st));
+      k_adj_cons<true><<<zg, tile, 0, st>>>(G, pn, q.ph, q.Ub[1], q.F1rho[1], x->geo, x->conn, lU, lcur, lh, lF1,
+                                            lF2, sa, as);
+      k_adj_flux<1, true><<<g1, tile, 0, st>>>(G, q.ph, x->geo, lF1, lh, sa, as);
+      k_adj_flux<2, true><<<g2, tile, 0, st>>>(G, q.ph, x->geo, lF2, lh, sa, as);
+      // predictor, from p^n into ph
+      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, q.ph, x->geo, lh);
+      k_adj_fixup_utoprim<<<1, FU_THREADS, 0, st>>>(G, q.X1[0], q.fl1[0], x->geo, x->floors, W, Wf, list, vbuf,
+                                                   kinds, lh, err);
+      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, q.X1[0], x->geo, lh);
+      k_adj_invert<<<zg, tile, 0, st>>>(G, q.Z[0], q.wz[0], x->geo, x->floors, x->katm, lh, lU, lcur, err);
+      CK(cudaMemsetAsync(lF1, 0, 2 * pb, st));
+      k_adj_cons<false><<<zg, tile, 0, st>>>(G, pn, pn, q.Ub[0], q.F1rho[0], x->geo, x->conn, lU, lcur, lcur, lF1,
+                                             lF2, sa, as);
+      k_adj_flux<1, false><<<g1, tile, 0, st>>>(G, pn, x->geo, lF1, lcur, sa, as);
+      k_adj_flux<2, false><<<g2, tile, 0, st>>>(G, pn, x->geo, lF2, lcur, sa, as);
+      k_adj_dt_post<<<1, 1, 0, st>>>(sa, sb, as);
+      CK(cudaGetLastError());
+      // the adjoint of p^n becomes the next (earlier) step's output adjoint
+      double *t = lnext;
+      lnext = lcur;
+      lcur = t;
+      CK(cudaMemsetAsync(lcur, 0, pb, st));
+      CK(cudaMemsetAsync(lh, 0, pb, st));
+    }
+    if (lnext != A) {
+      CK(cudaMemcpyAsync(A, lnext, pb, cudaMemcpyDeviceToDevice, st));
+      CK(cudaMemsetAsync(lnext, 0, pb, st));
+    }
+    return HARM_OK;
+  };
+
+  CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(as, 0, sizeof(AdjScalars), st));
+  CK(cudaMemsetAsync(lam, 0, 6 * pb, st));
+  const int last0 = (nseg - 1) * every, lastlen = nsteps - last0;
+  Graph gstep, grec, grev;
+  int rc = capture(gstep, [&] { return exact::launch_step(x); });
+  if (rc) return rc;
+  if (nseg > 1) {
+    rc = capture(grec, [&] { return record(every); });
     if (rc) return rc;
   }
+  rc = capture(grev, [&] { return reverse(every); });
+  if (rc) return rc;
+
+  // forward pass: a checkpoint every `every` steps; the last segment is
+  // recorded on the way, so it needs no recomputation
+  CK(cudaEventRecord(e0, st));
+  for (int seg = 0; seg < nseg; seg++) {
+    CK(cudaMemcpyAsync(ck + (size_t)seg * pl, x->p, pb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(cks + seg, x->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, st));
+    if (seg < nseg - 1) {
+      for (int r = 0; r < every; r++) CK(cudaGraphLaunch(gstep.e, st));
+    } else if (lastlen == every && nseg > 1) {
+      CK(cudaGraphLaunch(grec.e, st));
+    } else {
+      rc = record(lastlen);
+      if (rc) return rc;
+    }
+  }
   CK(cudaEventRecord(e1, st));
-  CK(cudaMemcpyAsync(pend, x->p, pl * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(pend, x->p, pb, cudaMemcpyDeviceToDevice, st));
   CK(cudaMemcpyAsync(cks + nseg, x->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, st));
   DevScalars s0, s1;
   CK(cudaMemcpyAsync(&s0, cks, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
@@ -691,88 +836,39 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
     return fail_with(HARM_E_ADJOINT, "the forward steps failed (fail code " + std::to_string(s1.fail_code) + ")");
   *J = s1.mass_in - s0.mass_in;
 
-  // reverse sweep
-  CK(cudaMemsetAsync(lam, 0, 6 * pl * sizeof(double), st));
-  const dim3 tile(32, 4);
-  const dim3 zg((G.n2 + 31) / 32, (G.n1 + 3) / 4, 1);
-  const dim3 g1((G.n2 + 2 + 31) / 32, (G.n1 + 1 + 3) / 4, 1);
-  const dim3 g2((G.n2 + 1 + 31) / 32, (G.n1 + 2 + 3) / 4, 1);
-  const int nbc = 4 * G.sn2 + 4 * (G.sn1 - 4);
-  double lam_dt_next = 0.;
+  // reverse sweep, segment by segment from the last
   std::vector<DevScalars> hs(2 * (size_t)nrec);
   for (int seg = nseg - 1; seg >= 0; seg--) {
-    const int n0 = seg * every, n1 = n0 + every < nsteps ? n0 + every : nsteps;
-    CK(cudaMemcpyAsync(x->p, ck + (size_t)seg * pl, pl * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    CK(cudaMemcpyAsync(x->sc, cks + seg, sizeof(DevScalars), cudaMemcpyDeviceToDevice, st));
-    for (int n = n0; n < n1; n++) {
-      CK(cudaMemcpyAsync(recp + (size_t)(n - n0) * pl, x->p, pl * sizeof(double), cudaMemcpyDeviceToDevice, st));
-      int rc = exact::launch_step_rec(x, rec[n - n0]);
-      if (rc) return rc;
+    const int n0 = seg * every, len = seg == nseg - 1 ? lastlen : every;
+    if (seg < nseg - 1) {
+      CK(cudaMemcpyAsync(x->p, ck + (size_t)seg * pl, pb, cudaMemcpyDeviceToDevice, st));
+      CK(cudaMemcpyAsync(x->sc, cks + seg, sizeof(DevScalars), cudaMemcpyDeviceToDevice, st));
+      CK(cudaGraphLaunch(grec.e, st));
     }
-    CK(cudaMemcpyAsync(recp + (size_t)(n1 - n0) * pl, x->p, pl * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    CK(cudaMemcpyAsync(hs.data(), recs, 2 * (size_t)(n1 - n0) * sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hs.data(), recs, 2 * (size_t)len * sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    for (int n = n1 - 1; n >= n0; n--) {
-      const StepRec &r = rec[n - n0];
-      const DevScalars &sa = hs[2 * (n - n0)], &sb = hs[2 * (n - n0) + 1];
-      const double *pn = recp + (size_t)(n - n0) * pl, *pnext = recp + (size_t)(n - n0 + 1) * pl;
-      const double dt = sa.dt, din = sb.mdot_in, ndt = sb.ndt;
-      const double n1v = bits_to_double(sa.ndt_bits[0]), n2v = bits_to_double(sa.ndt_bits[1]);
+    for (int r = 0; r < len; r++) {
+      const DevScalars &sa = hs[2 * r], &sb = hs[2 * r + 1];
       if (sb.fail_code) return fail_with(HARM_E_ADJOINT, "a recomputed step failed");
-      if (sb.dt != (ndt > SAFE * dt ? SAFE * dt : ndt))
+      if (sb.dt != (sb.ndt > SAFE * sa.dt ? SAFE * sa.dt : sb.ndt))
         return fail_with(HARM_E_ARG, "the steps reach tf: the adjoint needs dt = min(ndt, 1.3 dt) throughout");
-      // dt^{n+1} = min(ndt, 1.3 dt^n), ndt = defcon / (1/n1 + 1/n2) (step_ch.c:126-137)
-      double lam_dt = din, lam_ndt = 0.;
-      if (ndt > SAFE * dt) lam_dt += SAFE * lam_dt_next;
-      else lam_ndt = lam_dt_next;
-      const double S = 1. / n1v + 1. / n2v;
-      const double ln1 = lam_ndt * G.defcon / (n1v * n1v) / (S * S);
-      const double ln2 = lam_ndt * G.defcon / (n2v * n2v) / (S * S);
-      CK(cudaMemsetAsync(lamDt, 0, 2 * sizeof(double), st));
-      CK(cudaMemsetAsync(claim, 0, 2 * sizeof(int), st));
-      // objective term on the step's result
-      k_adj_din<<<(G.n2 + 127) / 128, 128, 0, st>>>(G, pnext, x->geo, lnext, dt);
-      // corrector: bound_prim, fixup_utoprim, bound_prim, inversion, update, fluxes
-      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, pnext, x->geo, lnext);
-      k_adj_fixup_utoprim<<<1, FU_THREADS, 0, st>>>(G, r.X1[1], r.fl1[1], x->geo, x->floors, W, Wf, list, vbuf,
-                                                   kinds, lnext, err);
-      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, r.X1[1], x->geo, lnext);
-      k_adj_invert<<<zg, tile, 0, st>>>(G, r.Ub[1], pn, x->geo, x->floors, x->katm, lnext, lU, lcur, err);
-      CK(cudaMemsetAsync(lF1, 0, 2 * pl * sizeof(double), st));
-      k_adj_cons<true><<<zg, tile, 0, st>>>(G, pn, r.ph, r.Ub[1], r.F1rho[1], x->geo, x->conn, lU, lcur, lh, lF1,
-                                            lF2, dt, lamDt + 1);
-      k_adj_flux<1, true><<<g1, tile, 0, st>>>(G, r.ph, x->geo, lF1, lh, ln1, n1v, claim);
-      k_adj_flux<2, true><<<g2, tile, 0, st>>>(G, r.ph, x->geo, lF2, lh, ln2, n2v, claim + 1);
-      // predictor, from p^n into ph
-      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, r.ph, x->geo, lh);
-      k_adj_fixup_utoprim<<<1, FU_THREADS, 0, st>>>(G, r.X1[0], r.fl1[0], x->geo, x->floors, W, Wf, list, vbuf,
-                                                   kinds, lh, err);
-      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, r.X1[0], x->geo, lh);
-      k_adj_invert<<<zg, tile, 0, st>>>(G, r.Ub[0], pn, x->geo, x->floors, x->katm, lh, lU, lcur, err);
-      CK(cudaMemsetAsync(lF1, 0, 2 * pl * sizeof(double), st));
-      k_adj_cons<false><<<zg, tile, 0, st>>>(G, pn, pn, r.Ub[0], r.F1rho[0], x->geo, x->conn, lU, lcur, lcur, lF1,
-                                             lF2, 0.5 * dt, lamDt);
-      k_adj_flux<1, false><<<g1, tile, 0, st>>>(G, pn, x->geo, lF1, lcur, 0., 0., claim);
-      k_adj_flux<2, false><<<g2, tile, 0, st>>>(G, pn, x->geo, lF2, lcur, 0., 0., claim);
-      CK(cudaGetLastError());
-      double hDt[2];
-      CK(cudaMemcpyAsync(hDt, lamDt, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
-      CK(cudaStreamSynchronize(st));
-      lam_dt_next = lam_dt + 0.5 * hDt[0] + hDt[1];
-      // the adjoint of p^n becomes the next (earlier) step's output adjoint
-      double *t = lnext;
-      lnext = lcur;
-      lcur = t;
-      CK(cudaMemsetAsync(lcur, 0, pl * sizeof(double), st));
-      CK(cudaMemsetAsync(lh, 0, pl * sizeof(double), st));
+    }
+    (void)n0;
+    if (len == every) {
+      CK(cudaGraphLaunch(grev.e, st));
+    } else {
+      rc = reverse(len);
+      if (rc) return rc;
     }
   }
   CK(cudaEventRecord(e2, st));
   int herr = 0;
   CK(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  if (herr & ERR_FAILS) return fail_with(HARM_E_ADJOINT, "more failed inversions in a half step than the adjoint lists");
-  if (herr & ERR_SINGULAR) return fail_with(HARM_E_ADJOINT, "a singular primtoU Jacobian in the adjoint of an inversion");
+  if (herr & ERR_FAILS)
+    return fail_with(HARM_E_ADJOINT, "more failed inversions in a half step than the adjoint lists");
+  if (herr & ERR_SINGULAR)
+    return fail_with(HARM_E_ADJOINT, "a singular primtoU Jacobian in the adjoint of an inversion");
   if (ms) {
     float a, b;
     CK(cudaEventElapsedTime(&a, e0, e1));
@@ -780,10 +876,10 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
     ms[0] = a;
     ms[1] = b;
   }
-  int rc = get_prims(x, lnext, grad, nullptr);
+  rc = get_prims(x, A, grad, nullptr);
   if (rc) return rc;
   // leave the context where the forward pass ended
-  CK(cudaMemcpyAsync(x->p, pend, pl * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(x->p, pend, pb, cudaMemcpyDeviceToDevice, st));
   CK(cudaMemcpyAsync(x->sc, cks + nseg, sizeof(DevScalars), cudaMemcpyDeviceToDevice, st));
   CK(cudaStreamSynchronize(st));
   return HARM_OK;

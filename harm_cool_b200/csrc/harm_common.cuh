@@ -167,6 +167,8 @@ inline dim3 zone_grid(const Grid &G) { return dim3((G.n2 + 31) / 32, (G.n1 + 3) 
 struct StepRec {
   double *X1[2];                 // the inversion's output after the first bound_prim
   double *Ub[2];                 // the conserved variables the update formed
+  double *Z[2];                  // the inversion's output before fixup()
+  signed char *wz[2];            // which inversion gave it: 0 Utoprim_2d, 1 and 2 the fall-backs, -1 none [nc]
   double *F1rho[2];              // raw radial mass flux [nc] (the no-inflow fix reads its sign)
   signed char *fl1[2];           // pflag after the first bound_prim [nc]
   double *ph;                    // the predictor's final state

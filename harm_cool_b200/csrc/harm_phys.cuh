@@ -203,8 +203,33 @@ __device__ __forceinline__ void vchar(double gam, const R *pr, const StateT<R> &
 }
 
 // The local Lax-Friedrichs flux of one face (step_ch.c:431-473, HLLF = 0 and
-// LAXF = 1 at :66-67) from the reconstructed states pl, pr: F and the face's
-// wave speed ctop.
+// LAXF = 1 at :66-67): lf_flux combines the two sides' fluxes F^dir, conserved
+// variables U and wave speeds into F and the face's wave speed ctop;
+// face_side evaluates one side; face_flux is both sides and the combination.
+template <class R>
+__device__ __forceinline__ void lf_flux(const R *Fl, const R *Ul, const R &cmaxl, const R &cminl, const R *Fr,
+                                        const R *Ur, const R &cmaxr, const R &cminr, R *F, R &ctop)
+{
+  R t1 = 0. > cmaxl ? R(0.) : cmaxl;
+  R cmax = fabs(t1 > cmaxr ? t1 : cmaxr);
+  R t2 = 0. > -cminl ? R(0.) : -cminl;
+  R cmin = fabs(t2 > -cminr ? t2 : -cminr);
+  ctop = cmax > cmin ? cmax : cmin;
+#pragma unroll
+  for (int k = 0; k < 8; k++) F[k] = 0.5 * (Fl[k] + Fr[k] - ctop * (Ur[k] - Ul[k]));
+}
+
+template <int DIR, class R>
+__device__ __forceinline__ void face_side(double gam, const R *p, const Geo &q, R *F, R *U, R &cmax, R &cmin,
+                                          int *fail)
+{
+  StateT<R> s;
+  get_state(p, q, s, fail);
+  primtoflux(gam, p, s, DIR, q.g, F);
+  primtoflux(gam, p, s, 0, q.g, U);
+  vchar(gam, p, s, q, DIR, cmax, cmin, fail);
+}
+
 template <int DIR, class R>
 __device__ __forceinline__ void face_flux(double gam, const R *pl, const R *pr, const Geo &q, R *F, R &ctop,
                                           int *fail)
@@ -221,13 +246,7 @@ __device__ __forceinline__ void face_flux(double gam, const R *pl, const R *pr, 
     primtoflux(gam, pr, s, DIR, q.g, Fr);
     primtoflux(gam, pr, s, 0, q.g, Ur);
     vchar(gam, pr, s, q, DIR, cmaxr, cminr, fail);
-    R t1 = 0. > cmaxl ? R(0.) : cmaxl;
-    R cmax = fabs(t1 > cmaxr ? t1 : cmaxr);
-    R t2 = 0. > -cminl ? R(0.) : -cminl;
-    R cmin = fabs(t2 > -cminr ? t2 : -cminr);
-    ctop = cmax > cmin ? cmax : cmin;
-#pragma unroll
-    for (int k = 0; k < 8; k++) F[k] = 0.5 * (Fl[k] + Fr[k] - ctop * (Ur[k] - Ul[k]));
+    lf_flux(Fl, Ul, cmaxl, cminl, Fr, Ur, cmaxr, cminr, F, ctop);
   }
 }
 

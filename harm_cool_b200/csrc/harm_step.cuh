@@ -371,13 +371,18 @@ static __device__ __noinline__ int inversion_fallbacks(double gam, double kap, c
   return flag;
 }
 
+// REC: also keep the inversion's output before fixup() and which inversion
+// gave it (zrec, wrec), for the discrete adjoint's recomputation
+template <bool REC>
 __global__ void __launch_bounds__(128, HARM_INV_MINB) k_invert(Grid G, const double *__restrict__ pi,
                                                                const double *__restrict__ Ub,
                                                                double *__restrict__ pf,
                                                                signed char *__restrict__ pflag,
                                                                const double *__restrict__ geo,
                                                                const double *__restrict__ floors,
-                                                               const double *__restrict__ katm, DevScalars *sc)
+                                                               const double *__restrict__ katm, DevScalars *sc,
+                                                               double *__restrict__ zrec,
+                                                               signed char *__restrict__ wrec)
 {
   if (sc->halted) return;
   const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
@@ -397,7 +402,22 @@ __global__ void __launch_bounds__(128, HARM_INV_MINB) k_invert(Grid G, const dou
     pz[k] = __ldg(pi + k * G.nc + c);
   }
   int flag = utoprim<0, (bool)HARM_STEP_MIXED>(G.gam, 0., U, q, pz);
-  if (flag) flag = inversion_fallbacks(G.gam, __ldg(katm + i), U, q, pz);
+  if (REC) {
+    int which = 0;
+    if (flag) {
+      which = 1;
+      flag = utoprim<1>(G.gam, __ldg(katm + i), U, q, pz);
+      if (flag) {
+        which = 2;
+        flag = utoprim<2>(G.gam, __ldg(katm + i), U, q, pz);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) zrec[k * G.nc + c] = pz[k];
+    wrec[c] = (signed char)(flag ? -1 : which);
+  } else if (flag) {
+    flag = inversion_fallbacks(G.gam, __ldg(katm + i), U, q, pz);
+  }
   signed char fl = (signed char)flag;
   if (fixup1zone(G.gam, __ldg(floors + gi), __ldg(floors + G.ng + gi), q, pz, &fail)) fl = -33;
 #pragma unroll
@@ -467,7 +487,8 @@ inline Bufs bufs(Ctx *x)
 }
 
 template <bool FULL>
-void launch_update(Ctx *x, const double *pi, const double *pb, double *pf)
+void launch_update(Ctx *x, const double *pi, const double *pb, double *pf, double *zrec = nullptr,
+                   signed char *wrec = nullptr)
 {
   const Grid &G = x->G;
   Bufs B = bufs(x);
@@ -479,8 +500,14 @@ void launch_update(Ctx *x, const double *pi, const double *pb, double *pf)
   else
     k_cons<FULL, false><<<zg, tile, 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn, x->geo32,
                                                     x->conn32, x->Ubuf, x->sc);
-  k_invert<<<zg, tile, 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->katm,
-                                                        x->sc);
+#if !HARM_STEP_MIXED
+  if (zrec)
+    k_invert<true><<<zg, tile, 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->katm, x->sc,
+                                               zrec, wrec);
+  else
+#endif
+    k_invert<false><<<zg, tile, 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->katm, x->sc,
+                                                nullptr, nullptr);
 }
 
 // advance() + fixup + bound_prim + fixup_utoprim + bound_prim (step_ch.c:101-117)
@@ -517,7 +544,7 @@ static void launch_half_rec(Ctx *x, const double *pi, const double *pb, double *
   Bufs B = bufs(x);
   launch_flux<FULL>(x->G, dim3(x->tbx, x->tby), x->stream, pb, B.F1, B.F2, B.F3, x->geo, x->geo32, x->sc);
   cudaMemcpyAsync(r.F1rho[s], B.F1 + RHO * nc, nc * sizeof(double), cudaMemcpyDeviceToDevice, x->stream);
-  launch_update<FULL>(x, pi, pb, pf);
+  launch_update<FULL>(x, pi, pb, pf, r.Z[s], r.wz[s]);
   cudaMemcpyAsync(r.Ub[s], x->Ubuf, 8 * nc * sizeof(double), cudaMemcpyDeviceToDevice, x->stream);
   if (FULL) k_diag_flux<<<1, 1024, 0, x->stream>>>(x->G, B.F1, x->sc);
   launch_bound(x, pf);

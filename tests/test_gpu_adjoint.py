@@ -82,15 +82,18 @@ def test_state_direction_against_central_difference(nsteps, every):
 
 
 def test_checkpoint_spacing_does_not_change_the_gradient():
+    """one segment recorded on the forward pass (9), full segments of odd and
+    even length replayed from graphs (3, 2, 4), partial last segments (2, 4)"""
     ctx = _context(32, 32)
     ctx.init_torus()
     p0 = ctx.get_prims()
     J1, l1, _ = ctx.adjoint_mass_in(9, 9)
-    ctx.init_torus()
-    ctx.put_prims(p0)
-    J2, l2, _ = ctx.adjoint_mass_in(9, 2)
-    assert J1 == J2
-    np.testing.assert_allclose(l2, l1, rtol=1e-12, atol=1e-12 * np.abs(l1).max())
+    for every in (2, 3, 4):
+        ctx.init_torus()
+        ctx.put_prims(p0)
+        J2, l2, _ = ctx.adjoint_mass_in(9, every)
+        assert J1 == J2
+        np.testing.assert_allclose(l2, l1, rtol=1e-12, atol=1e-12 * np.abs(l1).max())
 
 
 def test_parameter_gradient_against_central_difference():
