@@ -138,3 +138,41 @@ def test_refusals():
     ctx.set_precision(hc.Context.MIXED)
     with pytest.raises(hc.HarmError):
         ctx.adjoint_mass_in(2, 1)
+
+
+class _MassInFunction:
+    """J(theta) as a torch.autograd.Function over the device adjoint: the test
+    harness's thin wrapper (the library itself has no torch dependency)."""
+
+    @staticmethod
+    def make(ctx, modes, nsteps, every):
+        import torch
+
+        class MassIn(torch.autograd.Function):
+            @staticmethod
+            def forward(fctx, theta):
+                th = theta.detach().cpu().numpy()
+                J, g, _ = ad.mass_in_gradient(ctx, modes, th[0], th[1], th[2:], nsteps, every, rel_step=H)
+                fctx.save_for_backward(torch.as_tensor(g, dtype=theta.dtype))
+                return theta.new_tensor(J)
+
+            @staticmethod
+            def backward(fctx, gout):
+                (g,) = fctx.saved_tensors
+                return gout * g
+
+        return MassIn.apply
+
+
+def test_torch_autograd_wrapper():
+    torch = pytest.importorskip("torch")
+    ctx = _context(32, 32)
+    modes = ad.Modes(32, 32, m=16, seed=3)
+    f = _MassInFunction.make(ctx, modes, 6, 3)
+    theta = torch.tensor([12.0, 100.0] + [0.0] * 16, dtype=torch.float64, requires_grad=True)
+    J = f(theta)
+    (g,) = torch.autograd.grad(J, theta)
+    J2, g2, _ = ad.mass_in_gradient(ctx, modes, 12.0, 100.0, np.zeros(16), 6, 3, rel_step=H)
+    assert float(J) == J2
+    # atomic accumulation order may move the last bits between two sweeps
+    np.testing.assert_allclose(g.numpy(), g2, rtol=1e-10, atol=1e-10 * np.abs(g2).max())
