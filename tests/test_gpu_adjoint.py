@@ -176,3 +176,35 @@ def test_torch_autograd_wrapper():
     assert float(J) == J2
     # atomic accumulation order may move the last bits between two sweeps
     np.testing.assert_allclose(g.numpy(), g2, rtol=1e-10, atol=1e-10 * np.abs(g2).max())
+
+
+def test_repaired_zones_against_central_difference():
+    """A 3x3 block of strong radial field six zones from the inner boundary
+    makes the inversion fail in 8 zones of the first step, and fixup_utoprim
+    repairs them from their neighbours with corner and last-resort stencils
+    (fixup.c:432-538): the adjoint replays those repairs and transposes them,
+    and the failed inversions keep their guess.  (With the block against the
+    boundary, J itself is rough at the inversion tolerance, ~1e-10 relative,
+    and no central difference resolves a slope there.)"""
+    n, i0 = 48, 8
+    ctx = _context(n, n)
+    ctx.init_torus()
+    p0 = ctx.get_prims()
+    blk = (0, slice(i0, i0 + 3), slice(2 + n // 2 - 1, 2 + n // 2 + 2), 5)
+    p0[blk] = 1e3 * np.abs(p0[..., 5]).max()
+    ctx.init_torus()
+    ctx.put_prims(p0)
+    ctx.step_ch()
+    ctx.sync()
+    _, fl = ctx.get_prims(with_flags=True)
+    assert np.sum(fl[0, 2:n + 2, 2:n + 2] != 1) > 0  # the step repaired zones
+    v = _smooth_direction(p0.shape, seed=7)
+    scale = np.array([np.abs(p0[..., k]).max() for k in range(8)])
+    v *= np.abs(p0) + 1e-3 * scale * (np.arange(8) >= 2)
+    ctx.init_torus()
+    ctx.put_prims(p0)
+    J, lam, _ = ctx.adjoint_mass_in(4, 3)
+    assert J == _mass_in_from(ctx, p0, 4)
+    fd = (_mass_in_from(ctx, p0 + H * v, 4) - _mass_in_from(ctx, p0 - H * v, 4)) / (2 * H)
+    ad_ = float(np.sum(lam * v))
+    assert abs(ad_ - fd) <= TOL * abs(fd), (ad_, fd)
