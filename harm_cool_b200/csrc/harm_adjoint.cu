@@ -44,6 +44,11 @@ namespace adj {
 
 constexpr int FU_THREADS = 1024;
 enum { ERR_FAILS = 1, ERR_SINGULAR = 2 };
+// resident blocks of 128 threads per SM the face adjoint's register budget
+// allows (1, 255 registers, measured faster on a B200 than 3 at 168)
+#ifndef HARM_ADJ_FLUX_MINB
+#define HARM_ADJ_FLUX_MINB 1
+#endif
 
 using D8 = Dual<8>;
 
@@ -548,15 +553,25 @@ __global__ void __launch_bounds__(128) k_adj_cons(Grid G, const double *__restri
 
 // ---------------------------------------------------------------------------
 // the face fluxes (k_flux: limited face states, LF flux) transposed; FULL: the
-// corrector, whose Courant minimum n_d (recorded) gets adjoint lnd
+// corrector, whose Courant minimum n_d (recorded) gets adjoint as->ln.
+// Four lanes per face: lane t takes side t >> 1 (0 left, 1 right) and that
+// side's primitives 4 (t & 1) .. 4 (t & 1) + 3 as its tangent directions, so
+// each lane finishes its own derivatives and the face's work spreads over
+// four threads (a 2D grid alone leaves few warps per SM for this FP64-latency
+// bound work).
 
 template <int DIR, bool FULL>
-__global__ void __launch_bounds__(128) k_adj_flux(Grid G, const double *__restrict__ pb, const double *__restrict__ geo,
-                                                  const double *__restrict__ lamF, double *lamp,
-                                                  const DevScalars *sa, AdjScalars *as)
+__global__ void __launch_bounds__(128, HARM_ADJ_FLUX_MINB) k_adj_flux(Grid G, const double *__restrict__ pb,
+                                                                      const double *__restrict__ geo,
+                                                                      const double *__restrict__ lamF, double *lamp,
+                                                                      const DevScalars *sa, AdjScalars *as)
 {
-  const int j = (DIR == 2 ? G.jstart : G.jstart - 1) + blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = (DIR == 1 ? G.istart : G.istart - 1) + blockIdx.y * blockDim.y + threadIdx.y;
+  using D4 = Dual<4>;
+  const int t = threadIdx.x & 3, side = t >> 1, grp = t & 1;
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask = 0xFu << (lane & ~3);
+  const int j = (DIR == 2 ? G.jstart : G.jstart - 1) + blockIdx.x * (blockDim.x >> 2) + (threadIdx.x >> 2);
+  const int i = (DIR == 1 ? G.istart : G.istart - 1) + blockIdx.y;
   if (i > G.istop + 1 || j > G.jstop + 1) return;
   if (DIR == 2 && (j == G.jstart || j == G.jstop + 1)) return;  // polar faces carry no flux
   const long c = cidx(G, 0, i, j);
@@ -571,70 +586,58 @@ __global__ void __launch_bounds__(128) k_adj_flux(Grid G, const double *__restri
   const double lnd = FULL ? as->ln[DIR - 1] : 0.;
   const double nmin = FULL ? __longlong_as_double((long long)sa->ndt_bits[DIR - 1]) : 0.;
   const double dxd = DIR == 1 ? G.dx1 : G.dx2;
-  if (!any && !(act && lnd != 0.)) return;
+  if (!any && !(act && lnd != 0.)) return;  // the same for the face's four lanes
   const long o1 = DIR == 1 ? c - 2 * G.sn2 : c - 2, o2 = DIR == 1 ? c - G.sn2 : c - 1,
              o3 = DIR == 1 ? c + G.sn2 : c + 1;
-  // limited face states (interp.c:49-93) and their derivatives in (p[-2], p[-1], p[0], p[+1])
-  double pl[8], pr[8], dl[8][4], dr[8][4];
+  // limited face states (interp.c:49-93); the derivatives of this lane's four
+  // components of its side in (p[-2], p[-1], p[0], p[+1])
+  double pl[8], pr[8], dlim[4][4];
 #pragma unroll
   for (int k = 0; k < 8; k++) {
     const double *P = pb + k * G.nc;
-    Dual<4> a = Dual<4>::seed(P[o1], 0), b = Dual<4>::seed(P[o2], 1), z = Dual<4>::seed(P[c], 2),
-            e = Dual<4>::seed(P[o3], 3);
-    Dual<4> L = b + 0.5 * slope_lim(G.lim, a, b, z);
-    Dual<4> R = z - 0.5 * slope_lim(G.lim, b, z, e);
+    D4 a = D4::seed(P[o1], 0), b = D4::seed(P[o2], 1), z = D4::seed(P[c], 2), e = D4::seed(P[o3], 3);
+    D4 L = b + 0.5 * slope_lim(G.lim, a, b, z);
+    D4 R = z - 0.5 * slope_lim(G.lim, b, z, e);
     pl[k] = L.v;
     pr[k] = R.v;
+    if ((k >> 2) == grp) {
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-      dl[k][m] = L.d[m];
-      dr[k][m] = R.d[m];
+      for (int m = 0; m < 4; m++) dlim[k & 3][m] = side ? R.d[m] : L.d[m];
     }
   }
   Geo q;
   load_geo(geo_at(geo, G, DIR == 1 ? L_FACE1 : L_FACE2), G.ng, (long)i * G.sn2 + j, q);
-  // plain values of both sides: the other side's constants in each
-  // linearisation below, and the face's wave speed
-  double Flv[8], Ulv[8], cxl, cnl, Frv[8], Urv[8], cxr, cnr, Fz[8], ctz;
   int f0 = 0;
-  face_side<DIR>(G.gam, pl, q, Flv, Ulv, cxl, cnl, &f0);
-  face_side<DIR>(G.gam, pr, q, Frv, Urv, cxr, cnr, &f0);
-  lf_flux(Flv, Ulv, cxl, cnl, Frv, Urv, cxr, cnr, Fz, ctz);
-  // the face that set the Courant minimum gets the adjoint of its wave speed
-  double lct = 0.;
-  if (act && lnd != 0. && G.cour * dxd / ctz == nmin && atomicCAS(&as->claim[DIR - 1], 0, 1) == 0)
-    lct = -lnd * nmin / ctz;
-  if (!any && lct == 0.) return;
-  double lpl[8], lpr[8];
-  for (int side = 0; side < 2; side++) {
-    const double *pv = side ? pr : pl;
-    D8 P[8], Fs[8], Us[8], cx, cn, Fo[8], Uo[8], F[8], ct;
-#pragma unroll
-    for (int k = 0; k < 8; k++) P[k] = D8::seed(pv[k], k);
-    face_side<DIR>(G.gam, P, q, Fs, Us, cx, cn, &f0);
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      Fo[k] = D8(side ? Flv[k] : Frv[k]);
-      Uo[k] = D8(side ? Ulv[k] : Urv[k]);
-    }
-    if (side == 0) lf_flux(Fs, Us, cx, cn, Fo, Uo, D8(cxr), D8(cnr), F, ct);
-    else lf_flux(Fo, Uo, D8(cxl), D8(cnl), Fs, Us, cx, cn, F, ct);
-    double *out = side ? lpr : lpl;
-#pragma unroll
-    for (int m = 0; m < 8; m++) {
-      double a = lct * ct.d[m];
-#pragma unroll
-      for (int k = 0; k < 8; k++) a += lF[k] * F[k].d[m];
-      out[m] = a;
-    }
-  }
+  // the other side, plain: constants of this side's linearisation
+  double Fo[8], Uo[8], cxo, cno;
+  face_side<DIR>(G.gam, side ? pl : pr, q, Fo, Uo, cxo, cno, &f0);
+  D4 P[8], Fs[8], Us[8], cx, cn, Fc[8], Uc[8], F[8], ct;
 #pragma unroll
   for (int k = 0; k < 8; k++) {
-    double *L = lamp + k * G.nc;
-    const double la = lpl[k] * dl[k][0] + lpr[k] * dr[k][0];
-    const double lb = lpl[k] * dl[k][1] + lpr[k] * dr[k][1];
-    const double lz = lpl[k] * dl[k][2] + lpr[k] * dr[k][2];
-    const double le = lpl[k] * dl[k][3] + lpr[k] * dr[k][3];
+    P[k] = D4::seed(side ? pr[k] : pl[k], k - 4 * grp);
+    Fc[k] = D4(Fo[k]);
+    Uc[k] = D4(Uo[k]);
+  }
+  face_side<DIR>(G.gam, P, q, Fs, Us, cx, cn, &f0);
+  if (side == 0) lf_flux(Fs, Us, cx, cn, Fc, Uc, D4(cxo), D4(cno), F, ct);
+  else lf_flux(Fc, Uc, D4(cxo), D4(cno), Fs, Us, cx, cn, F, ct);
+  // the face that set the Courant minimum gets the adjoint of its wave speed
+  // (ct.v is the face's wave speed exactly as the step computed it)
+  double lct = 0.;
+  if (act && lnd != 0.) {
+    int win = 0;
+    if (t == 0 && G.cour * dxd / ct.v == nmin) win = atomicCAS(&as->claim[DIR - 1], 0, 1) == 0;
+    win = __shfl_sync(gmask, win, lane & ~3);
+    if (win) lct = -lnd * nmin / ct.v;
+  }
+  if (!any && lct == 0.) return;
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    double a = lct * ct.d[m];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a += lF[k] * F[k].d[m];
+    double *L = lamp + (4 * grp + m) * G.nc;
+    const double la = a * dlim[m][0], lb = a * dlim[m][1], lz = a * dlim[m][2], le = a * dlim[m][3];
     if (la != 0.) atomicAdd(L + o1, la);
     if (lb != 0.) atomicAdd(L + o2, lb);
     if (lz != 0.) atomicAdd(L + c, lz);
@@ -744,8 +747,10 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
 
   const dim3 tile(32, 4);
   const dim3 zg((G.n2 + 31) / 32, (G.n1 + 3) / 4, 1);
-  const dim3 g1((G.n2 + 2 + 31) / 32, (G.n1 + 1 + 3) / 4, 1);
-  const dim3 g2((G.n2 + 1 + 31) / 32, (G.n1 + 2 + 3) / 4, 1);
+  // face kernels: 32 faces along theta per block, four lanes each; one r row per block
+  const dim3 ftile(128, 1);
+  const dim3 g1((G.n2 + 2 + 31) / 32, G.n1 + 1, 1);
+  const dim3 g2((G.n2 + 1 + 31) / 32, G.n1 + 2, 1);
   const int nbc = 4 * G.sn2 + 4 * (G.sn1 - 4);
   // the reverse of one recorded segment of len steps: the adjoint of its last
   // state in A on entry, of its first state in A on exit, B zero both times
@@ -767,8 +772,8 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       CK(cudaMemsetAsync(lF1, 0, 2 * pb, st));
       k_adj_cons<true><<<zg, tile, 0, st>>>(G, pn, q.ph, q.Ub[1], q.F1rho[1], x->geo, x->conn, lU, lcur, lh, lF1,
                                             lF2, sa, as);
-      k_adj_flux<1, true><<<g1, tile, 0, st>>>(G, q.ph, x->geo, lF1, lh, sa, as);
-      k_adj_flux<2, true><<<g2, tile, 0, st>>>(G, q.ph, x->geo, lF2, lh, sa, as);
+      k_adj_flux<1, true><<<g1, ftile, 0, st>>>(G, q.ph, x->geo, lF1, lh, sa, as);
+      k_adj_flux<2, true><<<g2, ftile, 0, st>>>(G, q.ph, x->geo, lF2, lh, sa, as);
       // predictor, from p^n into ph
       k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, q.ph, x->geo, lh);
       k_adj_fixup_utoprim<<<1, FU_THREADS, 0, st>>>(G, q.X1[0], q.fl1[0], x->geo, x->floors, W, Wf, list, vbuf,
@@ -778,8 +783,8 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       CK(cudaMemsetAsync(lF1, 0, 2 * pb, st));
       k_adj_cons<false><<<zg, tile, 0, st>>>(G, pn, pn, q.Ub[0], q.F1rho[0], x->geo, x->conn, lU, lcur, lcur, lF1,
                                              lF2, sa, as);
-      k_adj_flux<1, false><<<g1, tile, 0, st>>>(G, pn, x->geo, lF1, lcur, sa, as);
-      k_adj_flux<2, false><<<g2, tile, 0, st>>>(G, pn, x->geo, lF2, lcur, sa, as);
+      k_adj_flux<1, false><<<g1, ftile, 0, st>>>(G, pn, x->geo, lF1, lcur, sa, as);
+      k_adj_flux<2, false><<<g2, ftile, 0, st>>>(G, pn, x->geo, lF2, lcur, sa, as);
       k_adj_dt_post<<<1, 1, 0, st>>>(sa, sb, as);
       CK(cudaGetLastError());
       // the adjoint of p^n becomes the next (earlier) step's output adjoint
