@@ -44,11 +44,6 @@ namespace adj {
 
 constexpr int FU_THREADS = 1024;
 enum { ERR_FAILS = 1, ERR_SINGULAR = 2 };
-// resident blocks of 128 threads per SM the face adjoint's register budget
-// allows (1, 255 registers, measured faster on a B200 than 3 at 168)
-#ifndef HARM_ADJ_FLUX_MINB
-#define HARM_ADJ_FLUX_MINB 1
-#endif
 
 using D8 = Dual<8>;
 
@@ -552,25 +547,163 @@ __global__ void __launch_bounds__(128) k_adj_cons(Grid G, const double *__restri
 }
 
 // ---------------------------------------------------------------------------
-// the face fluxes (k_flux: limited face states, LF flux) transposed; FULL: the
-// corrector, whose Courant minimum n_d (recorded) gets adjoint as->ln.
-// Four lanes per face: lane t takes side t >> 1 (0 left, 1 right) and that
-// side's primitives 4 (t & 1) .. 4 (t & 1) + 3 as its tangent directions, so
-// each lane finishes its own derivatives and the face's work spreads over
-// four threads (a 2D grid alone leaves few warps per SM for this FP64-latency
-// bound work).
+// the face fluxes (k_flux: limited face states, LF flux) transposed
 
+// Reverse mode of face_side (harm_phys.cuh): get_state (phys.c:219-252,
+// 108-117, metric.c:210-231), primtoflux for DIR and for t (phys.c:59-96,
+// 143-161) and vchar (phys.c:337-476), differentiated by hand.  Given the
+// adjoints of the side's outputs aF (F^DIR), aU (F^t), acx (vmax) and acn
+// (vmin), it returns the adjoint of the side's primitives ap.  The values are
+// recomputed with the step's own routines, so every clamp and selection takes
+// the step's branch; a clamped quantity passes no derivative.
+template <int DIR>
+__device__ __forceinline__ void face_side_rev(double gam, const double *p, const Geo &q, const double *aF,
+                                              const double *aU, double acx, double acn, double *ap)
+{
+  StateT<double> s;
+  int fail = 0;
+  get_state(p, q, s, &fail);
+  const double rho = p[RHO], u = p[UU], w1 = p[U1], w2 = p[U2], w3 = p[U3];
+  const double qsq = q.v11 * w1 * w1 + q.v22 * w2 * w2 + q.v33 * w3 * w3 + 2. * (q.v13 * w1 * w3);
+  const double gamma = s.ucon[0] * q.alpha;  // u^t = gamma / alpha
+  const double bsq = dot4(s.bcon, s.bcov);
+
+  // vchar, values as it forms them
+  const double EF = rho + gam * u, EE = bsq + EF, va2 = bsq / EE, cs2 = gam * (gam - 1.) * u / EF;
+  double cms2 = cs2 + va2 - cs2 * va2;
+  bool clive = true;
+  if (cms2 < 0.) { cms2 = SMALL; clive = false; }
+  if (cms2 > 1.) { cms2 = 1.; clive = false; }
+  const double Asq = gcon_diag(q, DIR), Bsq = q.n00, AB = gcon_t(q, DIR);
+  const double Au = s.ucon[DIR], Bu = s.ucon[0];
+  const double Au2 = Au * Au, Bu2 = Bu * Bu, AuBu = Au * Bu;
+  const double A = Bu2 - (Bsq + Bu2) * cms2;
+  const double B = 2. * (AuBu - (AB + AuBu) * cms2);
+  const double C = Au2 - (Asq + Au2) * cms2;
+  double discr = B * B - 4. * A * C;
+  const bool dlive = !(discr < 0.);
+  if (!dlive) discr = 0.;
+  const double dd = sqrt(discr);
+  const double vp = -(-B + dd) / (2. * A), vm = -(-B - dd) / (2. * A);
+
+  // vchar reversed: vmax, vmin -> A, B, C -> u^DIR, u^t, cms2 -> rho, u, b^2
+  const double avp = vp > vm ? acx : acn, avm = vp > vm ? acn : acx;
+  double aA = -(avp * vp + avm * vm) / A;
+  double aB = (avp + avm) / (2. * A);
+  const double adisc = (dlive && dd > 0.) ? ((avm - avp) / (2. * A)) * 0.5 / dd : 0.;
+  aB += 2. * B * adisc;
+  aA += -4. * C * adisc;
+  const double aC = -4. * A * adisc;
+  double auc[4] = {0., 0., 0., 0.}, aucv[4] = {0., 0., 0., 0.}, abc[4] = {0., 0., 0., 0.},
+         abcv[4] = {0., 0., 0., 0.};
+  auc[DIR] += aC * 2. * Au * (1. - cms2) + aB * 2. * (1. - cms2) * Bu;
+  auc[0] += aA * 2. * Bu * (1. - cms2) + aB * 2. * (1. - cms2) * Au;
+  const double acms = clive ? -aA * (Bsq + Bu2) - aB * 2. * (AB + AuBu) - aC * (Asq + Au2) : 0.;
+  const double acs2 = acms * (1. - va2), ava2 = acms * (1. - cs2);
+  double a_u = acs2 * gam * (gam - 1.) / EF;
+  double aEF = -acs2 * cs2 / EF;
+  double absq = ava2 / EE;
+  const double aEE = -ava2 * va2 / EE;
+  absq += aEE;
+  aEF += aEE;
+  double a_rho = aEF;
+  a_u += gam * aEF;
+
+  // the two fluxes reversed (primtoflux, mhd_calc); g multiplies every component
+  const double P = (gam - 1.) * u, eta = P + rho + u + bsq;
+  double aeta = 0., aptot = 0.;
+#pragma unroll
+  for (int pass = 0; pass < 2; pass++) {
+    const int d = pass ? 0 : DIR;
+    const double *af = pass ? aU : aF;
+    double f[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) f[k] = af[k] * q.g;
+    const double f0 = f[RHO] + f[UU];  // F[UU] = T^d_t + F[RHO]
+    a_rho += f0 * s.ucon[d];
+    auc[d] += f0 * rho;
+#pragma unroll
+    for (int jj = 0; jj < 4; jj++) {
+      const double am = f[UU + jj];
+      aeta += am * s.ucon[d] * s.ucov[jj];
+      auc[d] += am * eta * s.ucov[jj];
+      aucv[jj] += am * eta * s.ucon[d];
+      abc[d] -= am * s.bcov[jj];
+      abcv[jj] -= am * s.bcon[d];
+      if (jj == d) aptot += am;
+    }
+#pragma unroll
+    for (int ii = 1; ii < 4; ii++) {  // F[B_i] = b^i u^d - b^d u^i
+      const double fb = f[B1 + ii - 1];
+      abc[ii] += fb * s.ucon[d];
+      auc[d] += fb * s.bcon[ii];
+      abc[d] -= fb * s.ucon[ii];
+      auc[ii] -= fb * s.bcon[d];
+    }
+  }
+  // eta = P + rho + u + b^2, ptot = P + b^2/2, P = (gam - 1) u
+  absq += aeta + 0.5 * aptot;
+  const double aP = aeta + aptot;
+  a_rho += aeta;
+  a_u += aeta + (gam - 1.) * aP;
+  // b^2 = b^mu b_mu
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    abc[k] += absq * s.bcov[k];
+    abcv[k] += absq * s.bcon[k];
+  }
+  // b_mu = lower(b^mu)
+  abc[0] += q.v00 * abcv[0] + q.v01 * abcv[1] + q.v03 * abcv[3];
+  abc[1] += q.v01 * abcv[0] + q.v11 * abcv[1] + q.v13 * abcv[3];
+  abc[2] += q.v22 * abcv[2];
+  abc[3] += q.v03 * abcv[0] + q.v13 * abcv[1] + q.v33 * abcv[3];
+  // b^i = (B^i + b^t u^i) / u^t, b^t = B^i u_i
+  double aBf[3], abt = abc[0];
+#pragma unroll
+  for (int ii = 1; ii < 4; ii++) {
+    aBf[ii - 1] = abc[ii] / s.ucon[0];
+    abt += abc[ii] * s.ucon[ii] / s.ucon[0];
+    auc[ii] += abc[ii] * s.bcon[0] / s.ucon[0];
+    auc[0] -= abc[ii] * s.bcon[ii] / s.ucon[0];
+  }
+#pragma unroll
+  for (int ii = 1; ii < 4; ii++) {
+    aBf[ii - 1] += abt * s.ucov[ii];
+    aucv[ii] += abt * p[B1 + ii - 1];
+  }
+  // u_mu = lower(u^mu)
+  auc[0] += q.v00 * aucv[0] + q.v01 * aucv[1] + q.v03 * aucv[3];
+  auc[1] += q.v01 * aucv[0] + q.v11 * aucv[1] + q.v13 * aucv[3];
+  auc[2] += q.v22 * aucv[2];
+  auc[3] += q.v03 * aucv[0] + q.v13 * aucv[1] + q.v33 * aucv[3];
+  // u^t = gamma / alpha, u^i = w^i - gamma beta^i / alpha (beta^2 = 0),
+  // gamma = sqrt(1 + qsq) unless gamma_calc clamps qsq
+  const double alpha = q.alpha, b1 = q.n01 * alpha * alpha, b3 = q.n03 * alpha * alpha;
+  const double agam = auc[0] / alpha - auc[1] * b1 / alpha - auc[3] * b3 / alpha;
+  const double aq = qsq < 0. ? 0. : agam * 0.5 / gamma;
+  ap[RHO] = a_rho;
+  ap[UU] = a_u;
+  ap[U1] = auc[1] + aq * (2. * q.v11 * w1 + 2. * q.v13 * w3);
+  ap[U2] = auc[2] + aq * 2. * q.v22 * w2;
+  ap[U3] = auc[3] + aq * (2. * q.v33 * w3 + 2. * q.v13 * w1);
+  ap[B1] = aBf[0];
+  ap[B2] = aBf[1];
+  ap[B3] = aBf[2];
+}
+
+// FULL: the corrector, whose Courant minimum n_d (recorded) gets adjoint
+// as->ln.  Two lanes per face, one per side of the Lax-Friedrichs flux; they
+// swap their sides' values and each reverses its own side.
 template <int DIR, bool FULL>
-__global__ void __launch_bounds__(128, HARM_ADJ_FLUX_MINB) k_adj_flux(Grid G, const double *__restrict__ pb,
-                                                                      const double *__restrict__ geo,
-                                                                      const double *__restrict__ lamF, double *lamp,
-                                                                      const DevScalars *sa, AdjScalars *as)
+__global__ void __launch_bounds__(128) k_adj_flux(Grid G, const double *__restrict__ pb,
+                                                  const double *__restrict__ geo,
+                                                  const double *__restrict__ lamF, double *lamp,
+                                                  const DevScalars *sa, AdjScalars *as)
 {
   using D4 = Dual<4>;
-  const int t = threadIdx.x & 3, side = t >> 1, grp = t & 1;
-  const int lane = threadIdx.x & 31;
-  const unsigned gmask = 0xFu << (lane & ~3);
-  const int j = (DIR == 2 ? G.jstart : G.jstart - 1) + blockIdx.x * (blockDim.x >> 2) + (threadIdx.x >> 2);
+  const int side = threadIdx.x & 1, lane = threadIdx.x & 31;
+  const unsigned pmask = 0x3u << (lane & ~1);
+  const int j = (DIR == 2 ? G.jstart : G.jstart - 1) + blockIdx.x * (blockDim.x >> 1) + (threadIdx.x >> 1);
   const int i = (DIR == 1 ? G.istart : G.istart - 1) + blockIdx.y;
   if (i > G.istop + 1 || j > G.jstop + 1) return;
   if (DIR == 2 && (j == G.jstart || j == G.jstop + 1)) return;  // polar faces carry no flux
@@ -586,58 +719,79 @@ __global__ void __launch_bounds__(128, HARM_ADJ_FLUX_MINB) k_adj_flux(Grid G, co
   const double lnd = FULL ? as->ln[DIR - 1] : 0.;
   const double nmin = FULL ? __longlong_as_double((long long)sa->ndt_bits[DIR - 1]) : 0.;
   const double dxd = DIR == 1 ? G.dx1 : G.dx2;
-  if (!any && !(act && lnd != 0.)) return;  // the same for the face's four lanes
+  if (!any && !(act && lnd != 0.)) return;  // the same for both lanes of the face
   const long o1 = DIR == 1 ? c - 2 * G.sn2 : c - 2, o2 = DIR == 1 ? c - G.sn2 : c - 1,
              o3 = DIR == 1 ? c + G.sn2 : c + 1;
-  // limited face states (interp.c:49-93); the derivatives of this lane's four
-  // components of its side in (p[-2], p[-1], p[0], p[+1])
-  double pl[8], pr[8], dlim[4][4];
+  // limited face states (interp.c:49-93); the derivatives of this lane's side
+  // in (p[-2], p[-1], p[0], p[+1])
+  double ps[8], dlim[8][4];
 #pragma unroll
   for (int k = 0; k < 8; k++) {
     const double *P = pb + k * G.nc;
     D4 a = D4::seed(P[o1], 0), b = D4::seed(P[o2], 1), z = D4::seed(P[c], 2), e = D4::seed(P[o3], 3);
-    D4 L = b + 0.5 * slope_lim(G.lim, a, b, z);
-    D4 R = z - 0.5 * slope_lim(G.lim, b, z, e);
-    pl[k] = L.v;
-    pr[k] = R.v;
-    if ((k >> 2) == grp) {
+    D4 v = side ? z - 0.5 * slope_lim(G.lim, b, z, e) : b + 0.5 * slope_lim(G.lim, a, b, z);
+    ps[k] = v.v;
 #pragma unroll
-      for (int m = 0; m < 4; m++) dlim[k & 3][m] = side ? R.d[m] : L.d[m];
-    }
+    for (int m = 0; m < 4; m++) dlim[k][m] = v.d[m];
   }
   Geo q;
   load_geo(geo_at(geo, G, DIR == 1 ? L_FACE1 : L_FACE2), G.ng, (long)i * G.sn2 + j, q);
   int f0 = 0;
-  // the other side, plain: constants of this side's linearisation
-  double Fo[8], Uo[8], cxo, cno;
-  face_side<DIR>(G.gam, side ? pl : pr, q, Fo, Uo, cxo, cno, &f0);
-  D4 P[8], Fs[8], Us[8], cx, cn, Fc[8], Uc[8], F[8], ct;
+  double Fs[8], Us[8], cxs, cns, Fo[8], Uo[8];
+  face_side<DIR>(G.gam, ps, q, Fs, Us, cxs, cns, &f0);
 #pragma unroll
   for (int k = 0; k < 8; k++) {
-    P[k] = D4::seed(side ? pr[k] : pl[k], k - 4 * grp);
-    Fc[k] = D4(Fo[k]);
-    Uc[k] = D4(Uo[k]);
+    Fo[k] = __shfl_xor_sync(pmask, Fs[k], 1);
+    Uo[k] = __shfl_xor_sync(pmask, Us[k], 1);
   }
-  face_side<DIR>(G.gam, P, q, Fs, Us, cx, cn, &f0);
-  if (side == 0) lf_flux(Fs, Us, cx, cn, Fc, Uc, D4(cxo), D4(cno), F, ct);
-  else lf_flux(Fc, Uc, D4(cxo), D4(cno), Fs, Us, cx, cn, F, ct);
+  const double cxo = __shfl_xor_sync(pmask, cxs, 1), cno = __shfl_xor_sync(pmask, cns, 1);
+  const double *Fl = side ? Fo : Fs, *Ul = side ? Uo : Us, *Fr = side ? Fs : Fo, *Ur = side ? Us : Uo;
+  const double cxl = side ? cxo : cxs, cnl = side ? cno : cns, cxr = side ? cxs : cxo, cnr = side ? cns : cno;
+  // lf_flux's wave speed and the branches it takes
+  const double t1 = 0. > cxl ? 0. : cxl;
+  const double cmv = t1 > cxr ? t1 : cxr, cmax = fabs(cmv);
+  const double t2 = 0. > -cnl ? 0. : -cnl;
+  const double cnv = t2 > -cnr ? t2 : -cnr, cmin = fabs(cnv);
+  const double ctop = cmax > cmin ? cmax : cmin;
   // the face that set the Courant minimum gets the adjoint of its wave speed
-  // (ct.v is the face's wave speed exactly as the step computed it)
   double lct = 0.;
   if (act && lnd != 0.) {
     int win = 0;
-    if (t == 0 && G.cour * dxd / ct.v == nmin) win = atomicCAS(&as->claim[DIR - 1], 0, 1) == 0;
-    win = __shfl_sync(gmask, win, lane & ~3);
-    if (win) lct = -lnd * nmin / ct.v;
+    if (side == 0 && G.cour * dxd / ctop == nmin) win = atomicCAS(&as->claim[DIR - 1], 0, 1) == 0;
+    win = __shfl_sync(pmask, win, lane & ~1);
+    if (win) lct = -lnd * nmin / ctop;
   }
   if (!any && lct == 0.) return;
+  // lf_flux reversed: F = (Fl + Fr - ctop (Ur - Ul)) / 2
+  double act_ = lct;
 #pragma unroll
-  for (int m = 0; m < 4; m++) {
-    double a = lct * ct.d[m];
+  for (int k = 0; k < 8; k++) act_ -= 0.5 * lF[k] * (Ur[k] - Ul[k]);
+  const double acmv = cmax > cmin ? (cmv < 0. ? -act_ : act_) : 0.;
+  const double acnv = cmax > cmin ? 0. : (cnv < 0. ? -act_ : act_);
+  double acxl = 0., acxr = 0., acnl = 0., acnr = 0.;
+  if (t1 > cxr) {
+    if (!(0. > cxl)) acxl = acmv;
+  } else {
+    acxr = acmv;
+  }
+  if (t2 > -cnr) {
+    if (!(0. > -cnl)) acnl = -acnv;
+  } else {
+    acnr = -acnv;
+  }
+  double aF[8], aU[8], ap[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) a += lF[k] * F[k].d[m];
-    double *L = lamp + (4 * grp + m) * G.nc;
-    const double la = a * dlim[m][0], lb = a * dlim[m][1], lz = a * dlim[m][2], le = a * dlim[m][3];
+  for (int k = 0; k < 8; k++) {
+    aF[k] = 0.5 * lF[k];
+    aU[k] = (side ? -0.5 : 0.5) * ctop * lF[k];
+  }
+  face_side_rev<DIR>(G.gam, ps, q, aF, aU, side ? acxr : acxl, side ? acnr : acnl, ap);
+  // and through the limiter onto the four cells
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    double *L = lamp + k * G.nc;
+    const double la = ap[k] * dlim[k][0], lb = ap[k] * dlim[k][1], lz = ap[k] * dlim[k][2],
+                 le = ap[k] * dlim[k][3];
     if (la != 0.) atomicAdd(L + o1, la);
     if (lb != 0.) atomicAdd(L + o2, lb);
     if (lz != 0.) atomicAdd(L + c, lz);
@@ -747,10 +901,10 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
 
   const dim3 tile(32, 4);
   const dim3 zg((G.n2 + 31) / 32, (G.n1 + 3) / 4, 1);
-  // face kernels: 32 faces along theta per block, four lanes each; one r row per block
+  // face kernels: 64 faces along theta per block, two lanes each; one r row per block
   const dim3 ftile(128, 1);
-  const dim3 g1((G.n2 + 2 + 31) / 32, G.n1 + 1, 1);
-  const dim3 g2((G.n2 + 1 + 31) / 32, G.n1 + 2, 1);
+  const dim3 g1((G.n2 + 2 + 63) / 64, G.n1 + 1, 1);
+  const dim3 g2((G.n2 + 1 + 63) / 64, G.n1 + 2, 1);
   const int nbc = 4 * G.sn2 + 4 * (G.sn1 - 4);
   // the reverse of one recorded segment of len steps: the adjoint of its last
   // state in A on entry, of its first state in A on exit, B zero both times
