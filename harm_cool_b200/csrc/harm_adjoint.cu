@@ -13,11 +13,13 @@
 // step's own kernels (exact::launch_step_rec), keeping the intermediates of
 // every step (StepRec), and then walks the steps backwards.  Each part of a
 // step is transposed where it is linear (flux-CT averaging, the flux
-// divergence, bound_prim copies, fixup_utoprim stencils) and linearised with
-// forward-mode dual numbers (harm_dual.cuh) where it is not: the limited face
-// states and the Lax-Friedrichs flux (limiter branches and the wave-speed
-// choice frozen at the forward's), primtoU, the connection source, fixup()
-// floors and inflow_check().  The inversion is differentiated through its
+// divergence, bound_prim copies, fixup_utoprim stencils).  The face fluxes
+// (get_state, primtoflux, vchar and the Lax-Friedrichs combination), primtoU
+// and the connection source are differentiated by hand in reverse mode.  The
+// limiter, fixup() floors, inflow_check(), the objective and the primtoU
+// Jacobian of the inversion are linearised with forward-mode dual numbers
+// (harm_dual.cuh).  Limiter branches, clamps and the wave-speed choice are
+// frozen at the forward's.  The inversion is differentiated through its
 // converged solution by the implicit-function theorem: Utoprim_2d returns the
 // z with primtoU(z) = U, so dz/dU = (dprimtoU/dz)^-1; the isentropic
 // fall-backs replace the energy row by their constraint u = K rho^gam/(gam-1).
@@ -413,6 +415,138 @@ __global__ void __launch_bounds__(128) k_adj_invert(Grid G, const double *__rest
 }
 
 // ---------------------------------------------------------------------------
+// Reverse mode, differentiated by hand, of the state routines the update and
+// the face fluxes use.  Values are recomputed with the step's own routines, so
+// every clamp and selection takes the step's branch; a clamped quantity passes
+// no derivative.
+
+// adjoints of get_state's outputs and of the primitives read directly
+struct StateAdj {
+  double uc[4], ucv[4], bc[4], bcv[4], rho, u, bsq;
+};
+
+__device__ __forceinline__ void adj_zero(StateAdj &a)
+{
+#pragma unroll
+  for (int k = 0; k < 4; k++) a.uc[k] = a.ucv[k] = a.bc[k] = a.bcv[k] = 0.;
+  a.rho = a.u = a.bsq = 0.;
+}
+
+// one row T^d_j of mhd_calc (phys.c:143-161), given its adjoint am[j]; eta is
+// the row's rho + u + p + b^2
+__device__ __forceinline__ void mhd_rev(double gam, const StateT<double> &s, double eta, int d, const double *am,
+                                        StateAdj &a)
+{
+  double aeta = 0.;
+#pragma unroll
+  for (int jj = 0; jj < 4; jj++) {
+    aeta += am[jj] * s.ucon[d] * s.ucov[jj];
+    a.uc[d] += am[jj] * eta * s.ucov[jj];
+    a.ucv[jj] += am[jj] * eta * s.ucon[d];
+    a.bc[d] -= am[jj] * s.bcov[jj];
+    a.bcv[jj] -= am[jj] * s.bcon[d];
+  }
+  const double aptot = am[d];  // ptot = p + b^2/2 on the diagonal
+  a.bsq += aeta + 0.5 * aptot;
+  a.rho += aeta;
+  a.u += aeta + (gam - 1.) * (aeta + aptot);  // eta and ptot through p = (gam - 1) u
+}
+
+// primtoflux for direction d (phys.c:59-96), given the adjoint af of its result
+__device__ __forceinline__ void flux_rev(double gam, const double *p, const Geo &q, const StateT<double> &s,
+                                         double eta, int d, const double *af, StateAdj &a)
+{
+  double f[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) f[k] = af[k] * q.g;
+  const double f0 = f[RHO] + f[UU];  // F[UU] = T^d_t + F[RHO]
+  a.rho += f0 * s.ucon[d];
+  a.uc[d] += f0 * p[RHO];
+  mhd_rev(gam, s, eta, d, f + UU, a);
+#pragma unroll
+  for (int ii = 1; ii < 4; ii++) {  // F[B_i] = b^i u^d - b^d u^i
+    const double fb = f[B1 + ii - 1];
+    a.bc[ii] += fb * s.ucon[d];
+    a.uc[d] += fb * s.bcon[ii];
+    a.bc[d] -= fb * s.ucon[ii];
+    a.uc[ii] -= fb * s.bcon[d];
+  }
+}
+
+// get_state (phys.c:219-252, 108-117, metric.c:210-231) and b^2 reversed:
+// the primitives' adjoint ap
+__device__ __forceinline__ void state_rev(const double *p, const Geo &q, const StateT<double> &s, StateAdj &a,
+                                          double *ap)
+{
+  // b^2 = b^mu b_mu
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    a.bc[k] += a.bsq * s.bcov[k];
+    a.bcv[k] += a.bsq * s.bcon[k];
+  }
+  // b_mu = lower(b^mu)
+  a.bc[0] += q.v00 * a.bcv[0] + q.v01 * a.bcv[1] + q.v03 * a.bcv[3];
+  a.bc[1] += q.v01 * a.bcv[0] + q.v11 * a.bcv[1] + q.v13 * a.bcv[3];
+  a.bc[2] += q.v22 * a.bcv[2];
+  a.bc[3] += q.v03 * a.bcv[0] + q.v13 * a.bcv[1] + q.v33 * a.bcv[3];
+  // b^i = (B^i + b^t u^i) / u^t, b^t = B^i u_i
+  double aBf[3], abt = a.bc[0];
+#pragma unroll
+  for (int ii = 1; ii < 4; ii++) {
+    aBf[ii - 1] = a.bc[ii] / s.ucon[0];
+    abt += a.bc[ii] * s.ucon[ii] / s.ucon[0];
+    a.uc[ii] += a.bc[ii] * s.bcon[0] / s.ucon[0];
+    a.uc[0] -= a.bc[ii] * s.bcon[ii] / s.ucon[0];
+  }
+#pragma unroll
+  for (int ii = 1; ii < 4; ii++) {
+    aBf[ii - 1] += abt * s.ucov[ii];
+    a.ucv[ii] += abt * p[B1 + ii - 1];
+  }
+  // u_mu = lower(u^mu)
+  a.uc[0] += q.v00 * a.ucv[0] + q.v01 * a.ucv[1] + q.v03 * a.ucv[3];
+  a.uc[1] += q.v01 * a.ucv[0] + q.v11 * a.ucv[1] + q.v13 * a.ucv[3];
+  a.uc[2] += q.v22 * a.ucv[2];
+  a.uc[3] += q.v03 * a.ucv[0] + q.v13 * a.ucv[1] + q.v33 * a.ucv[3];
+  // u^t = gamma / alpha, u^i = w^i - gamma beta^i / alpha (beta^2 = 0),
+  // gamma = sqrt(1 + qsq) unless gamma_calc clamps qsq
+  const double w1 = p[U1], w2 = p[U2], w3 = p[U3];
+  const double qsq = q.v11 * w1 * w1 + q.v22 * w2 * w2 + q.v33 * w3 * w3 + 2. * (q.v13 * w1 * w3);
+  const double alpha = q.alpha, b1 = q.n01 * alpha * alpha, b3 = q.n03 * alpha * alpha;
+  const double gamma = s.ucon[0] * alpha;
+  const double agam = a.uc[0] / alpha - a.uc[1] * b1 / alpha - a.uc[3] * b3 / alpha;
+  const double aq = qsq < 0. ? 0. : agam * 0.5 / gamma;
+  ap[RHO] = a.rho;
+  ap[UU] = a.u;
+  ap[U1] = a.uc[1] + aq * (2. * q.v11 * w1 + 2. * q.v13 * w3);
+  ap[U2] = a.uc[2] + aq * 2. * q.v22 * w2;
+  ap[U3] = a.uc[3] + aq * (2. * q.v33 * w3 + 2. * q.v13 * w1);
+  ap[B1] = aBf[0];
+  ap[B2] = aBf[1];
+  ap[B3] = aBf[2];
+}
+
+// source() (phys.c:165-207) reversed: dU_nu = g sum_{j,k} T^j_k conn[k][nu][j]
+// for nu = t..phi in U[UU..U3]; w * lu is the adjoint of dU
+__device__ __forceinline__ void source_rev(double gam, const Geo &q, const StateT<double> &s, double eta,
+                                           const double *__restrict__ conn, long ng, long gi, const double *lu,
+                                           double w, StateAdj &a)
+{
+#pragma unroll
+  for (int jj = 0; jj < 4; jj++) {
+    double am[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      double x = 0.;
+#pragma unroll
+      for (int nu = 0; nu < 4; nu++) x += lu[UU + nu] * __ldg(conn + conn_slot(k, nu, jj) * ng + gi);
+      am[k] = w * q.g * x;
+    }
+    mhd_rev(gam, s, eta, jj, am, a);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // the update (k_cons: primtoU, source, flux-CT, flux divergence) transposed
 
 // adjoint of one corner EMF (step_ch.c:546-547) onto the raw face fluxes,
@@ -459,50 +593,37 @@ __global__ void __launch_bounds__(128) k_adj_cons(Grid G, const double *__restri
     for (int k = 0; k < 8; k++) lu[k] = lamU[k * G.nc + c];
     int fail = 0;
     {
-      D8 v[8], U0[8];
+      // primtoU at pi and, in the predictor (pi = pb), the source at the same state
+      double pz[8];
 #pragma unroll
-      for (int k = 0; k < 8; k++) v[k] = D8::seed(pi[k * G.nc + c], k);
-      StateT<D8> s;
-      get_state(v, q, s, &fail);
-      primtoflux(G.gam, v, s, 0, q.g, U0);
+      for (int k = 0; k < 8; k++) pz[k] = pi[k * G.nc + c];
+      StateT<double> s;
+      get_state(pz, q, s, &fail);
+      primtoflux(G.gam, pz, s, 0, q.g, P0);
+      const double eta = (G.gam - 1.) * pz[UU] + pz[RHO] + pz[UU] + dot4(s.bcon, s.bcov);
+      StateAdj a;
+      adj_zero(a);
+      flux_rev(G.gam, pz, q, s, eta, 0, lu, a);
+      if (!FULL) source_rev(G.gam, q, s, eta, conn, G.ng, gi, lu, Dt, a);
       double li[8];
-#pragma unroll
-      for (int k = 0; k < 8; k++) {
-        double a = 0.;
-#pragma unroll
-        for (int o = 0; o < 8; o++) a += lu[o] * U0[o].d[k];
-        li[k] = a;
-      }
-#pragma unroll
-      for (int o = 0; o < 8; o++) P0[o] = U0[o].v;
-      if (!FULL) {
-        D8 dU[8];
-        source_of_state(G.gam, v, s, q, conn, G.ng, gi, dU);
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          double a = 0.;
-#pragma unroll
-          for (int o = 0; o < 8; o++) a += lu[o] * dU[o].d[k];
-          li[k] += Dt * a;
-        }
-      }
+      state_rev(pz, q, s, a, li);
 #pragma unroll
       for (int k = 0; k < 8; k++) lampi[k * G.nc + c] += li[k];
     }
     if (FULL) {
-      D8 v[8], dU[8];
+      double pz[8];
 #pragma unroll
-      for (int k = 0; k < 8; k++) v[k] = D8::seed(pb[k * G.nc + c], k);
-      StateT<D8> s;
-      get_state(v, q, s, &fail);
-      source_of_state(G.gam, v, s, q, conn, G.ng, gi, dU);
+      for (int k = 0; k < 8; k++) pz[k] = pb[k * G.nc + c];
+      StateT<double> s;
+      get_state(pz, q, s, &fail);
+      const double eta = (G.gam - 1.) * pz[UU] + pz[RHO] + pz[UU] + dot4(s.bcon, s.bcov);
+      StateAdj a;
+      adj_zero(a);
+      source_rev(G.gam, q, s, eta, conn, G.ng, gi, lu, Dt, a);
+      double lb[8];
+      state_rev(pz, q, s, a, lb);
 #pragma unroll
-      for (int k = 0; k < 8; k++) {
-        double a = 0.;
-#pragma unroll
-        for (int o = 0; o < 8; o++) a += lu[o] * dU[o].d[k];
-        lampb[k * G.nc + c] += Dt * a;
-      }
+      for (int k = 0; k < 8; k++) lampb[k * G.nc + c] += lb[k];
     }
     // dU/dDt = (U - primtoU(pi)) / Dt, the step's own flux divergence plus source
 #pragma unroll
@@ -549,13 +670,9 @@ __global__ void __launch_bounds__(128) k_adj_cons(Grid G, const double *__restri
 // ---------------------------------------------------------------------------
 // the face fluxes (k_flux: limited face states, LF flux) transposed
 
-// Reverse mode of face_side (harm_phys.cuh): get_state (phys.c:219-252,
-// 108-117, metric.c:210-231), primtoflux for DIR and for t (phys.c:59-96,
-// 143-161) and vchar (phys.c:337-476), differentiated by hand.  Given the
-// adjoints of the side's outputs aF (F^DIR), aU (F^t), acx (vmax) and acn
-// (vmin), it returns the adjoint of the side's primitives ap.  The values are
-// recomputed with the step's own routines, so every clamp and selection takes
-// the step's branch; a clamped quantity passes no derivative.
+// face_side (harm_phys.cuh: get_state, primtoflux for DIR and for t, vchar
+// (phys.c:337-476)) reversed: given the adjoints of its outputs aF (F^DIR),
+// aU (F^t), acx (vmax) and acn (vmin), the adjoint of the side's primitives
 template <int DIR>
 __device__ __forceinline__ void face_side_rev(double gam, const double *p, const Geo &q, const double *aF,
                                               const double *aU, double acx, double acn, double *ap)
@@ -563,9 +680,7 @@ __device__ __forceinline__ void face_side_rev(double gam, const double *p, const
   StateT<double> s;
   int fail = 0;
   get_state(p, q, s, &fail);
-  const double rho = p[RHO], u = p[UU], w1 = p[U1], w2 = p[U2], w3 = p[U3];
-  const double qsq = q.v11 * w1 * w1 + q.v22 * w2 * w2 + q.v33 * w3 * w3 + 2. * (q.v13 * w1 * w3);
-  const double gamma = s.ucon[0] * q.alpha;  // u^t = gamma / alpha
+  const double rho = p[RHO], u = p[UU];
   const double bsq = dot4(s.bcon, s.bcov);
 
   // vchar, values as it forms them
@@ -587,6 +702,8 @@ __device__ __forceinline__ void face_side_rev(double gam, const double *p, const
   const double vp = -(-B + dd) / (2. * A), vm = -(-B - dd) / (2. * A);
 
   // vchar reversed: vmax, vmin -> A, B, C -> u^DIR, u^t, cms2 -> rho, u, b^2
+  StateAdj a;
+  adj_zero(a);
   const double avp = vp > vm ? acx : acn, avm = vp > vm ? acn : acx;
   double aA = -(avp * vp + avm * vm) / A;
   double aB = (avp + avm) / (2. * A);
@@ -594,101 +711,23 @@ __device__ __forceinline__ void face_side_rev(double gam, const double *p, const
   aB += 2. * B * adisc;
   aA += -4. * C * adisc;
   const double aC = -4. * A * adisc;
-  double auc[4] = {0., 0., 0., 0.}, aucv[4] = {0., 0., 0., 0.}, abc[4] = {0., 0., 0., 0.},
-         abcv[4] = {0., 0., 0., 0.};
-  auc[DIR] += aC * 2. * Au * (1. - cms2) + aB * 2. * (1. - cms2) * Bu;
-  auc[0] += aA * 2. * Bu * (1. - cms2) + aB * 2. * (1. - cms2) * Au;
+  a.uc[DIR] += aC * 2. * Au * (1. - cms2) + aB * 2. * (1. - cms2) * Bu;
+  a.uc[0] += aA * 2. * Bu * (1. - cms2) + aB * 2. * (1. - cms2) * Au;
   const double acms = clive ? -aA * (Bsq + Bu2) - aB * 2. * (AB + AuBu) - aC * (Asq + Au2) : 0.;
   const double acs2 = acms * (1. - va2), ava2 = acms * (1. - cs2);
-  double a_u = acs2 * gam * (gam - 1.) / EF;
+  a.u += acs2 * gam * (gam - 1.) / EF;
   double aEF = -acs2 * cs2 / EF;
-  double absq = ava2 / EE;
   const double aEE = -ava2 * va2 / EE;
-  absq += aEE;
+  a.bsq += ava2 / EE + aEE;
   aEF += aEE;
-  double a_rho = aEF;
-  a_u += gam * aEF;
+  a.rho += aEF;
+  a.u += gam * aEF;
 
-  // the two fluxes reversed (primtoflux, mhd_calc); g multiplies every component
-  const double P = (gam - 1.) * u, eta = P + rho + u + bsq;
-  double aeta = 0., aptot = 0.;
-#pragma unroll
-  for (int pass = 0; pass < 2; pass++) {
-    const int d = pass ? 0 : DIR;
-    const double *af = pass ? aU : aF;
-    double f[8];
-#pragma unroll
-    for (int k = 0; k < 8; k++) f[k] = af[k] * q.g;
-    const double f0 = f[RHO] + f[UU];  // F[UU] = T^d_t + F[RHO]
-    a_rho += f0 * s.ucon[d];
-    auc[d] += f0 * rho;
-#pragma unroll
-    for (int jj = 0; jj < 4; jj++) {
-      const double am = f[UU + jj];
-      aeta += am * s.ucon[d] * s.ucov[jj];
-      auc[d] += am * eta * s.ucov[jj];
-      aucv[jj] += am * eta * s.ucon[d];
-      abc[d] -= am * s.bcov[jj];
-      abcv[jj] -= am * s.bcon[d];
-      if (jj == d) aptot += am;
-    }
-#pragma unroll
-    for (int ii = 1; ii < 4; ii++) {  // F[B_i] = b^i u^d - b^d u^i
-      const double fb = f[B1 + ii - 1];
-      abc[ii] += fb * s.ucon[d];
-      auc[d] += fb * s.bcon[ii];
-      abc[d] -= fb * s.ucon[ii];
-      auc[ii] -= fb * s.bcon[d];
-    }
-  }
-  // eta = P + rho + u + b^2, ptot = P + b^2/2, P = (gam - 1) u
-  absq += aeta + 0.5 * aptot;
-  const double aP = aeta + aptot;
-  a_rho += aeta;
-  a_u += aeta + (gam - 1.) * aP;
-  // b^2 = b^mu b_mu
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    abc[k] += absq * s.bcov[k];
-    abcv[k] += absq * s.bcon[k];
-  }
-  // b_mu = lower(b^mu)
-  abc[0] += q.v00 * abcv[0] + q.v01 * abcv[1] + q.v03 * abcv[3];
-  abc[1] += q.v01 * abcv[0] + q.v11 * abcv[1] + q.v13 * abcv[3];
-  abc[2] += q.v22 * abcv[2];
-  abc[3] += q.v03 * abcv[0] + q.v13 * abcv[1] + q.v33 * abcv[3];
-  // b^i = (B^i + b^t u^i) / u^t, b^t = B^i u_i
-  double aBf[3], abt = abc[0];
-#pragma unroll
-  for (int ii = 1; ii < 4; ii++) {
-    aBf[ii - 1] = abc[ii] / s.ucon[0];
-    abt += abc[ii] * s.ucon[ii] / s.ucon[0];
-    auc[ii] += abc[ii] * s.bcon[0] / s.ucon[0];
-    auc[0] -= abc[ii] * s.bcon[ii] / s.ucon[0];
-  }
-#pragma unroll
-  for (int ii = 1; ii < 4; ii++) {
-    aBf[ii - 1] += abt * s.ucov[ii];
-    aucv[ii] += abt * p[B1 + ii - 1];
-  }
-  // u_mu = lower(u^mu)
-  auc[0] += q.v00 * aucv[0] + q.v01 * aucv[1] + q.v03 * aucv[3];
-  auc[1] += q.v01 * aucv[0] + q.v11 * aucv[1] + q.v13 * aucv[3];
-  auc[2] += q.v22 * aucv[2];
-  auc[3] += q.v03 * aucv[0] + q.v13 * aucv[1] + q.v33 * aucv[3];
-  // u^t = gamma / alpha, u^i = w^i - gamma beta^i / alpha (beta^2 = 0),
-  // gamma = sqrt(1 + qsq) unless gamma_calc clamps qsq
-  const double alpha = q.alpha, b1 = q.n01 * alpha * alpha, b3 = q.n03 * alpha * alpha;
-  const double agam = auc[0] / alpha - auc[1] * b1 / alpha - auc[3] * b3 / alpha;
-  const double aq = qsq < 0. ? 0. : agam * 0.5 / gamma;
-  ap[RHO] = a_rho;
-  ap[UU] = a_u;
-  ap[U1] = auc[1] + aq * (2. * q.v11 * w1 + 2. * q.v13 * w3);
-  ap[U2] = auc[2] + aq * 2. * q.v22 * w2;
-  ap[U3] = auc[3] + aq * (2. * q.v33 * w3 + 2. * q.v13 * w1);
-  ap[B1] = aBf[0];
-  ap[B2] = aBf[1];
-  ap[B3] = aBf[2];
+  // the two fluxes, then the state
+  const double eta = (gam - 1.) * u + rho + u + bsq;
+  flux_rev(gam, p, q, s, eta, DIR, aF, a);
+  flux_rev(gam, p, q, s, eta, 0, aU, a);
+  state_rev(p, q, s, a, ap);
 }
 
 // FULL: the corrector, whose Courant minimum n_d (recorded) gets adjoint
