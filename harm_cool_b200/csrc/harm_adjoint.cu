@@ -316,11 +316,160 @@ __device__ bool solve8t(const double (*A)[8], const double *b, double *x)
   return true;
 }
 
+// The adjoint of Utoprim_2d's result with respect to U (utoprim_2d.c:126-624),
+// through the implicit-function theorem on its own two-variable Newton
+// system: the residuals r1 = t11, r2 = t18 of func_vsq (utoprim_2d.c:562-624,
+// gamma-law :645-678) vanish at the converged (W, v^2), which the returned
+// primitives give back (rho = D sqrt(1 - v^2), u = (w - rho)/gam,
+// W = w / (1 - v^2)).  lz: adjoint of the returned primitives z; lu: adjoint
+// of the conserved variables U.
+__device__ __forceinline__ void u2p_ift_rev(double gam, const double *U, const double *z, const Geo &q,
+                                            const double *lz, double *lu)
+{
+  // the rescaled U and the scalars the inversion forms from it (utoprim_2d.c:126-176, 229-262)
+  const double alpha = q.alpha, f = alpha / q.g;
+  double Ut[8];
+  Ut[RHO] = alpha * U[RHO] / q.g;
+  Ut[UU] = alpha * (U[UU] - U[RHO]) / q.g;
+#pragma unroll
+  for (int k = U1; k <= B3; k++) Ut[k] = alpha * U[k] / q.g;
+  U2P c;
+  c.gam = gam;
+  c.K_atm = 0.;
+  double Bcon[4], Qcon[4], ncon[4], QdotB;
+  u2p_scalars(c, Ut, q, Bcon, Qcon, ncon, QdotB);
+  const double Bsq = c.Bsq, QdotBsq = c.QdotBsq, Qdotn = c.Qdotn, D = c.D;
+  const double Qcov[4] = {Ut[UU], Ut[U1], Ut[U2], Ut[U3]};
+  const double ncov0 = -sqrt(-1. / q.n00);
+  // the converged W and v^2
+  const double rho = z[RHO], u = z[UU];
+  const double gtmp = rho / D, om = gtmp * gtmp, vsq = 1. - om, w = gam * u + rho, W = w / om;
+  const double gamma = 1. / gtmp, WB = W + Bsq;
+  double aD = 0., aW = 0., av = 0., aBsq = 0., aQdotB = 0., aQdotn = 0., agamma = 0.;
+  double aQcon[4] = {0., 0., 0., 0.}, aBc[4] = {0., 0., 0., 0.};
+  // u^i = gamma / (W + B^2) (Qt^i + (Q.B) B^i / W), Qt^i = Q^i + n^i (Q.n)  (u2p_velocities)
+#pragma unroll
+  for (int ii = 1; ii < 4; ii++) {
+    const double Qt = Qcon[ii] + ncon[ii] * Qdotn;
+    const double X = Qt + QdotB * Bcon[ii] / W;
+    const double ui = gamma / WB * X;
+    const double a = lz[U1 + ii - 1];
+    agamma += a * X / WB;
+    aW -= a * ui / WB;
+    aBsq -= a * ui / WB;
+    const double aX = a * gamma / WB;
+    aQcon[ii] += aX;
+    aQdotn += aX * ncon[ii];
+    aQdotB += aX * Bcon[ii] / W;
+    aBc[ii] += aX * QdotB / W;
+    aW -= aX * QdotB * Bcon[ii] / (W * W);
+  }
+  // u = (w - rho) / gam, rho = D gtmp, w = W (1 - v^2), gamma = 1 / gtmp, gtmp = sqrt(1 - v^2)
+  const double aw = lz[UU] / gam, arho = lz[RHO] - lz[UU] / gam;
+  aD += arho * gtmp;
+  const double agtmp = arho * D - agamma / om;
+  aW += aw * om;
+  av -= aw * W + agtmp * 0.5 / gtmp;
+  // implicit-function theorem: J^T mu = (aW, av), then a_theta = -(mu1 dr1/dtheta + mu2 dr2/dtheta)
+  const double W2 = W * W, W3 = W2 * W;
+  const double r1W = -2. * vsq * WB + 2. * QdotBsq / W2 - 2. * QdotBsq * (Bsq + 2. * W) / W3;
+  const double r1v = -WB * WB;
+  const double r2W = -QdotBsq / W3 - 1. + (gam - 1.) * om / gam;
+  const double r2v = -0.5 * Bsq + (gam - 1.) * (0.5 * D / gtmp - W) / gam;
+  const double det = r1W * r2v - r2W * r1v;
+  const double mu1 = (aW * r2v - r2W * av) / det, mu2 = (r1W * av - r1v * aW) / det;
+  const double aQtsq = -mu1;
+  aBsq -= mu1 * (-2. * vsq * WB + QdotBsq / W2) - mu2 * 0.5 * (1. + vsq);
+  const double aQdotBsq = -(mu1 * (Bsq + 2. * W) / W2 + mu2 * 0.5 / W2);
+  aQdotn += mu2;
+  aD += mu2 * (gam - 1.) * gtmp / gam;
+  // Qtsq = Q.Q + (Q.n)^2, Q.n = Q^t n_t, (Q.B)^2
+  aQdotB += 2. * QdotB * aQdotBsq;
+  aQdotn += 2. * Qdotn * aQtsq;
+  double aQcov[4];
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    aQcov[m] = aQtsq * Qcon[m];
+    aQcon[m] += aQtsq * Qcov[m];
+  }
+  aQcon[0] += aQdotn * ncov0;
+  // Q^mu = g^{mu nu} Q_nu
+  aQcov[0] += q.n00 * aQcon[0] + q.n10 * aQcon[1] + q.n30 * aQcon[3];
+  aQcov[1] += q.n01 * aQcon[0] + q.n11 * aQcon[1] + q.n31 * aQcon[3];
+  aQcov[2] += q.n22 * aQcon[2];
+  aQcov[3] += q.n03 * aQcon[0] + q.n13 * aQcon[1] + q.n33 * aQcon[3];
+  // Q.B = Q_i B^i and B^2 = B^i B_i (B^t = 0)
+  const double Bcov[4] = {0., q.v11 * Bcon[1] + q.v13 * Bcon[3], q.v22 * Bcon[2], q.v13 * Bcon[1] + q.v33 * Bcon[3]};
+#pragma unroll
+  for (int ii = 1; ii < 4; ii++) {
+    aQcov[ii] += aQdotB * Bcon[ii];
+    aBc[ii] += aQdotB * Qcov[ii] + 2. * aBsq * Bcov[ii];
+  }
+  // back to U: D = Ut[RHO], Q_t = Ut[UU], Q_i = Ut[U_i], B^i = Ut[B_i]; the fields' own prim[B] = U[B]/gdet
+  lu[RHO] = f * (aD - aQcov[0]);
+  lu[UU] = f * aQcov[0];
+#pragma unroll
+  for (int ii = 1; ii < 4; ii++) {
+    lu[UU + ii] = f * aQcov[ii];
+    lu[B1 + ii - 1] = f * aBc[ii] + lz[B1 + ii - 1] / q.g;
+  }
+}
+
+// lz = (d fixup1zone / dz)^T lo for a zone the floors changed (dual numbers;
+// out of line: most zones are left alone and skip it)
+static __device__ __noinline__ void fixup_vjp(double gam, double rho_floor, double uu_floor, const Geo &q,
+                                              const double *z, const double *lo, double *lz)
+{
+  D8 v[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) v[k] = D8::seed(z[k], k);
+  int fail = 0;
+  fixup1zone(gam, rho_floor, uu_floor, q, v, &fail);
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    double a = 0.;
+#pragma unroll
+    for (int o = 0; o < 8; o++) a += lo[o] * v[o].d[k];
+    lz[k] = a;
+  }
+}
+
+// A fall-back inversion's adjoint (Utoprim_1dvsq2fix1 / Utoprim_1dfix1 solve with
+// u = K rho^gam / (gam - 1) in place of the energy equation): the
+// implicit-function theorem on primtoU with that row replaced, an 8x8 solve.
+// Rare, so kept out of line.
+static __device__ __noinline__ bool ift_fallback(double gam, double K, const double *z, const Geo &q,
+                                                 const double *lz, double *lu)
+{
+  double M[8][8];
+  {
+    D8 v[8], Uo[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] = D8::seed(z[k], k);
+    StateT<D8> s;
+    int fail = 0;
+    get_state(v, q, s, &fail);
+    primtoflux(gam, v, s, 0, q.g, Uo);
+#pragma unroll
+    for (int o = 0; o < 8; o++)
+#pragma unroll
+      for (int k = 0; k < 8; k++) M[o][k] = Uo[o].d[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++) M[UU][k] = 0.;
+  M[UU][UU] = 1.;
+  M[UU][RHO] = -K * gam * pow(z[RHO], gam - 1.) / (gam - 1.);
+  const bool ok = solve8t(M, lz, lu);
+  lu[UU] = 0.;
+  return ok;
+}
+
 // lamf: adjoint of the half step's output pf (its active cells are consumed);
 // lamU: adjoint of the conserved variables the update formed; lampi: adjoint of
 // the inversion's guess pi (a failed zone keeps it).  Zr, wz: the inversion's
 // output before fixup() and which inversion gave it, as the step recorded them.
-__global__ void __launch_bounds__(128) k_adj_invert(Grid G, const double *__restrict__ Zr,
+__global__ void __launch_bounds__(128) k_adj_invert(Grid G, const double *__restrict__ Ub,
+                                                    const double *__restrict__ Zr,
                                                     const signed char *__restrict__ wz,
                                                     const double *__restrict__ geo, const double *__restrict__ floors,
                                                     const double *__restrict__ katm, double *lamf, double *lamU,
@@ -359,48 +508,20 @@ __global__ void __launch_bounds__(128) k_adj_invert(Grid G, const double *__rest
 #pragma unroll
       for (int k = 0; k < 8; k++) lz[k] = lo[k];
     } else {
-      D8 v[8];
-#pragma unroll
-      for (int k = 0; k < 8; k++) v[k] = D8::seed(z[k], k);
-      fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
-#pragma unroll
-      for (int k = 0; k < 8; k++) {
-        double a = 0.;
-#pragma unroll
-        for (int o = 0; o < 8; o++) a += lo[o] * v[o].d[k];
-        lz[k] = a;
-      }
+      fixup_vjp(G.gam, floors[gi], floors[G.ng + gi], q, z, lo, lz);
     }
   }
-  if (flag == 0) {
-    double M[8][8];
-    {
-      D8 v[8], Uo[8];
+  if (flag == 0 && which == 0) {
+    double U[8];
 #pragma unroll
-      for (int k = 0; k < 8; k++) v[k] = D8::seed(z[k], k);
-      StateT<D8> s;
-      int fail = 0;
-      get_state(v, q, s, &fail);
-      primtoflux(G.gam, v, s, 0, q.g, Uo);
-#pragma unroll
-      for (int o = 0; o < 8; o++)
-#pragma unroll
-        for (int k = 0; k < 8; k++) M[o][k] = Uo[o].d[k];
-    }
-    if (which) {
-      // Utoprim_1dvsq2fix1 / Utoprim_1dfix1 solve with u = K rho^gam / (gam - 1)
-      // in place of the energy equation
-#pragma unroll
-      for (int k = 0; k < 8; k++) M[UU][k] = 0.;
-      M[UU][UU] = 1.;
-      M[UU][RHO] = -K * G.gam * pow(z[RHO], G.gam - 1.) / (G.gam - 1.);
-    }
-    if (!solve8t(M, lz, lu)) {
+    for (int k = 0; k < 8; k++) U[k] = Ub[k * G.nc + c];
+    u2p_ift_rev(G.gam, U, z, q, lz, lu);
+  } else if (flag == 0) {
+    if (!ift_fallback(G.gam, K, z, q, lz, lu)) {
       atomicOr(err, ERR_SINGULAR);
 #pragma unroll
       for (int k = 0; k < 8; k++) lu[k] = 0.;
     }
-    if (which) lu[UU] = 0.;
   } else {
 #pragma unroll
     for (int k = 0; k < B1; k++) {
@@ -961,7 +1082,7 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       k_adj_fixup_utoprim<<<1, FU_THREADS, 0, st>>>(G, q.X1[1], q.fl1[1], x->geo, x->floors, W, Wf, list, vbuf,
                                                    kinds, lnext, err);
       k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, q.X1[1], x->geo, lnext);
-      k_adj_invert<<<zg, tile, 0, st>>>(G, q.Z[1], q.wz[1], x->geo, x->floors, x->katm, lnext, lU, lcur, err);
+      k_adj_invert<<<zg, tile, 0, st>>>(G, q.Ub[1], q.Z[1], q.wz[1], x->geo, x->floors, x->katm, lnext, lU, lcur, err);
       CK(cudaMemsetAsync(lF1, 0, 2 * pb, st));
       k_adj_cons<true><<<zg, tile, 0, st>>>(G, pn, q.ph, q.Ub[1], q.F1rho[1], x->geo, x->conn, lU, lcur, lh, lF1,
                                             lF2, sa, as);
@@ -972,7 +1093,7 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       k_adj_fixup_utoprim<<<1, FU_THREADS, 0, st>>>(G, q.X1[0], q.fl1[0], x->geo, x->floors, W, Wf, list, vbuf,
                                                    kinds, lh, err);
       k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, q.X1[0], x->geo, lh);
-      k_adj_invert<<<zg, tile, 0, st>>>(G, q.Z[0], q.wz[0], x->geo, x->floors, x->katm, lh, lU, lcur, err);
+      k_adj_invert<<<zg, tile, 0, st>>>(G, q.Ub[0], q.Z[0], q.wz[0], x->geo, x->floors, x->katm, lh, lU, lcur, err);
       CK(cudaMemsetAsync(lF1, 0, 2 * pb, st));
       k_adj_cons<false><<<zg, tile, 0, st>>>(G, pn, pn, q.Ub[0], q.F1rho[0], x->geo, x->conn, lU, lcur, lcur, lF1,
                                              lF2, sa, as);
