@@ -285,6 +285,118 @@ __global__ void __launch_bounds__(FU_THREADS) k_adj_fixup_utoprim(Grid G, const 
 }
 
 // ---------------------------------------------------------------------------
+// Reverse mode, differentiated by hand, of the state routines the update and
+// the face fluxes use.  Values are recomputed with the step's own routines, so
+// every clamp and selection takes the step's branch; a clamped quantity passes
+// no derivative.
+
+// adjoints of get_state's outputs and of the primitives read directly
+struct StateAdj {
+  double uc[4], ucv[4], bc[4], bcv[4], rho, u, bsq;
+};
+
+__device__ __forceinline__ void adj_zero(StateAdj &a)
+{
+#pragma unroll
+  for (int k = 0; k < 4; k++) a.uc[k] = a.ucv[k] = a.bc[k] = a.bcv[k] = 0.;
+  a.rho = a.u = a.bsq = 0.;
+}
+
+// one row T^d_j of mhd_calc (phys.c:143-161), given its adjoint am[j]; eta is
+// the row's rho + u + p + b^2
+__device__ __forceinline__ void mhd_rev(double gam, const StateT<double> &s, double eta, int d, const double *am,
+                                        StateAdj &a)
+{
+  double aeta = 0.;
+#pragma unroll
+  for (int jj = 0; jj < 4; jj++) {
+    aeta += am[jj] * s.ucon[d] * s.ucov[jj];
+    a.uc[d] += am[jj] * eta * s.ucov[jj];
+    a.ucv[jj] += am[jj] * eta * s.ucon[d];
+    a.bc[d] -= am[jj] * s.bcov[jj];
+    a.bcv[jj] -= am[jj] * s.bcon[d];
+  }
+  const double aptot = am[d];  // ptot = p + b^2/2 on the diagonal
+  a.bsq += aeta + 0.5 * aptot;
+  a.rho += aeta;
+  a.u += aeta + (gam - 1.) * (aeta + aptot);  // eta and ptot through p = (gam - 1) u
+}
+
+// primtoflux for direction d (phys.c:59-96), given the adjoint af of its result
+__device__ __forceinline__ void flux_rev(double gam, const double *p, const Geo &q, const StateT<double> &s,
+                                         double eta, int d, const double *af, StateAdj &a)
+{
+  double f[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) f[k] = af[k] * q.g;
+  const double f0 = f[RHO] + f[UU];  // F[UU] = T^d_t + F[RHO]
+  a.rho += f0 * s.ucon[d];
+  a.uc[d] += f0 * p[RHO];
+  mhd_rev(gam, s, eta, d, f + UU, a);
+#pragma unroll
+  for (int ii = 1; ii < 4; ii++) {  // F[B_i] = b^i u^d - b^d u^i
+    const double fb = f[B1 + ii - 1];
+    a.bc[ii] += fb * s.ucon[d];
+    a.uc[d] += fb * s.bcon[ii];
+    a.bc[d] -= fb * s.ucon[ii];
+    a.uc[ii] -= fb * s.bcon[d];
+  }
+}
+
+// get_state (phys.c:219-252, 108-117, metric.c:210-231) and b^2 reversed:
+// the primitives' adjoint ap
+__device__ __forceinline__ void state_rev(const double *p, const Geo &q, const StateT<double> &s, StateAdj &a,
+                                          double *ap)
+{
+  // b^2 = b^mu b_mu
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    a.bc[k] += a.bsq * s.bcov[k];
+    a.bcv[k] += a.bsq * s.bcon[k];
+  }
+  // b_mu = lower(b^mu)
+  a.bc[0] += q.v00 * a.bcv[0] + q.v01 * a.bcv[1] + q.v03 * a.bcv[3];
+  a.bc[1] += q.v01 * a.bcv[0] + q.v11 * a.bcv[1] + q.v13 * a.bcv[3];
+  a.bc[2] += q.v22 * a.bcv[2];
+  a.bc[3] += q.v03 * a.bcv[0] + q.v13 * a.bcv[1] + q.v33 * a.bcv[3];
+  // b^i = (B^i + b^t u^i) / u^t, b^t = B^i u_i
+  double aBf[3], abt = a.bc[0];
+#pragma unroll
+  for (int ii = 1; ii < 4; ii++) {
+    aBf[ii - 1] = a.bc[ii] / s.ucon[0];
+    abt += a.bc[ii] * s.ucon[ii] / s.ucon[0];
+    a.uc[ii] += a.bc[ii] * s.bcon[0] / s.ucon[0];
+    a.uc[0] -= a.bc[ii] * s.bcon[ii] / s.ucon[0];
+  }
+#pragma unroll
+  for (int ii = 1; ii < 4; ii++) {
+    aBf[ii - 1] += abt * s.ucov[ii];
+    a.ucv[ii] += abt * p[B1 + ii - 1];
+  }
+  // u_mu = lower(u^mu)
+  a.uc[0] += q.v00 * a.ucv[0] + q.v01 * a.ucv[1] + q.v03 * a.ucv[3];
+  a.uc[1] += q.v01 * a.ucv[0] + q.v11 * a.ucv[1] + q.v13 * a.ucv[3];
+  a.uc[2] += q.v22 * a.ucv[2];
+  a.uc[3] += q.v03 * a.ucv[0] + q.v13 * a.ucv[1] + q.v33 * a.ucv[3];
+  // u^t = gamma / alpha, u^i = w^i - gamma beta^i / alpha (beta^2 = 0),
+  // gamma = sqrt(1 + qsq) unless gamma_calc clamps qsq
+  const double w1 = p[U1], w2 = p[U2], w3 = p[U3];
+  const double qsq = q.v11 * w1 * w1 + q.v22 * w2 * w2 + q.v33 * w3 * w3 + 2. * (q.v13 * w1 * w3);
+  const double alpha = q.alpha, b1 = q.n01 * alpha * alpha, b3 = q.n03 * alpha * alpha;
+  const double gamma = s.ucon[0] * alpha;
+  const double agam = a.uc[0] / alpha - a.uc[1] * b1 / alpha - a.uc[3] * b3 / alpha;
+  const double aq = qsq < 0. ? 0. : agam * 0.5 / gamma;
+  ap[RHO] = a.rho;
+  ap[UU] = a.u;
+  ap[U1] = a.uc[1] + aq * (2. * q.v11 * w1 + 2. * q.v13 * w3);
+  ap[U2] = a.uc[2] + aq * 2. * q.v22 * w2;
+  ap[U3] = a.uc[3] + aq * (2. * q.v33 * w3 + 2. * q.v13 * w1);
+  ap[B1] = aBf[0];
+  ap[B2] = aBf[1];
+  ap[B3] = aBf[2];
+}
+
+// ---------------------------------------------------------------------------
 // the inversion and fixup() of one zone (k_invert) transposed
 
 // x with A^T x = b, A[o][k] row-major 8x8; Gaussian elimination with partial pivoting
@@ -415,6 +527,65 @@ __device__ __forceinline__ void u2p_ift_rev(double gam, const double *U, const d
   }
 }
 
+// fixup1zone (fixup.c:142-383) reversed by hand where its drift-frame branch
+// is not taken: the density and energy floors (each the largest of the radial
+// floor, b^2 / BSQORHOMAX or BSQOUMAX, and for the density u / UORHOMAX) and
+// the Lorentz-factor limit.  lz = (d fixup1zone / dz)^T lo.  Returns false,
+// leaving lz alone, where the drift-frame branch applies.
+__device__ __forceinline__ bool fixup_rev(double gam, double rho_floor, double uu_floor, const Geo &q,
+                                          const double *z, const double *lo, double *lz)
+{
+  StateT<double> s;
+  int fail = 0;
+  get_state(z, q, s, &fail);
+  const double bsq = dot4(s.bcon, s.bcov);
+  double rflr = rho_floor, uflr = uu_floor;
+  int rsrc = 0, usrc = 0;  // 0: the radial floor, 1: b^2, 2 (density only): u
+  if (rflr < bsq / BSQORHOMAX) { rflr = bsq / BSQORHOMAX; rsrc = 1; }
+  if (uflr < bsq / BSQOUMAX) { uflr = bsq / BSQOUMAX; usrc = 1; }
+  if (rflr < z[UU] / UORHOMAX) { rflr = z[UU] / UORHOMAX; rsrc = 2; }
+  const bool rfl = z[RHO] < rflr, ufl = z[UU] < uflr;
+  const double r1 = rfl ? rflr : z[RHO], u1 = ufl ? uflr : z[UU];
+  if ((rfl || ufl) && 10. * bsq / (r1 < u1 ? r1 : u1) - 1. > 0.) return false;
+  double a[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) a[k] = lo[k];
+  // the Lorentz-factor limit: w^i -> f w^i, f = sqrt((GAMMAMAX^2 - 1) / qsq)
+  const double w1 = z[U1], w2 = z[U2], w3 = z[U3];
+  const double qsq = q.v11 * w1 * w1 + q.v22 * w2 * w2 + q.v33 * w3 * w3 + 2. * (q.v13 * w1 * w3);
+  if (qsq >= 0. && sqrt(1. + qsq) > GAMMAMAX) {
+    const double f = sqrt((GAMMAMAX * GAMMAMAX - 1.) / qsq);
+    const double S = (a[U1] * w1 + a[U2] * w2 + a[U3] * w3) * (-0.5 * f / qsq);
+    a[U1] = f * a[U1] + S * (2. * q.v11 * w1 + 2. * q.v13 * w3);
+    a[U2] = f * a[U2] + S * 2. * q.v22 * w2;
+    a[U3] = f * a[U3] + S * (2. * q.v33 * w3 + 2. * q.v13 * w1);
+  }
+  // the floors
+  double absq = 0.;
+  const double arho = a[RHO], auu = a[UU];
+  if (rfl) {
+    a[RHO] = 0.;
+    if (rsrc == 1) absq += arho / BSQORHOMAX;
+  }
+  if (ufl) {
+    a[UU] = 0.;
+    if (usrc == 1) absq += auu / BSQOUMAX;
+  }
+  if (rfl && rsrc == 2) a[UU] += arho / UORHOMAX;
+  if (absq != 0.) {
+    StateAdj sa;
+    adj_zero(sa);
+    sa.bsq = absq;
+    double ab[8];
+    state_rev(z, q, s, sa, ab);
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] += ab[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++) lz[k] = a[k];
+  return true;
+}
+
 // lz = (d fixup1zone / dz)^T lo for a zone the floors changed (dual numbers;
 // out of line: most zones are left alone and skip it)
 static __device__ __noinline__ void fixup_vjp(double gam, double rho_floor, double uu_floor, const Geo &q,
@@ -507,7 +678,7 @@ __global__ void __launch_bounds__(128) k_adj_invert(Grid G, const double *__rest
     if (same) {
 #pragma unroll
       for (int k = 0; k < 8; k++) lz[k] = lo[k];
-    } else {
+    } else if (!fixup_rev(G.gam, floors[gi], floors[G.ng + gi], q, z, lo, lz)) {
       fixup_vjp(G.gam, floors[gi], floors[G.ng + gi], q, z, lo, lz);
     }
   }
@@ -533,118 +704,6 @@ __global__ void __launch_bounds__(128) k_adj_invert(Grid G, const double *__rest
   }
 #pragma unroll
   for (int k = 0; k < 8; k++) lamU[k * G.nc + c] = lu[k];
-}
-
-// ---------------------------------------------------------------------------
-// Reverse mode, differentiated by hand, of the state routines the update and
-// the face fluxes use.  Values are recomputed with the step's own routines, so
-// every clamp and selection takes the step's branch; a clamped quantity passes
-// no derivative.
-
-// adjoints of get_state's outputs and of the primitives read directly
-struct StateAdj {
-  double uc[4], ucv[4], bc[4], bcv[4], rho, u, bsq;
-};
-
-__device__ __forceinline__ void adj_zero(StateAdj &a)
-{
-#pragma unroll
-  for (int k = 0; k < 4; k++) a.uc[k] = a.ucv[k] = a.bc[k] = a.bcv[k] = 0.;
-  a.rho = a.u = a.bsq = 0.;
-}
-
-// one row T^d_j of mhd_calc (phys.c:143-161), given its adjoint am[j]; eta is
-// the row's rho + u + p + b^2
-__device__ __forceinline__ void mhd_rev(double gam, const StateT<double> &s, double eta, int d, const double *am,
-                                        StateAdj &a)
-{
-  double aeta = 0.;
-#pragma unroll
-  for (int jj = 0; jj < 4; jj++) {
-    aeta += am[jj] * s.ucon[d] * s.ucov[jj];
-    a.uc[d] += am[jj] * eta * s.ucov[jj];
-    a.ucv[jj] += am[jj] * eta * s.ucon[d];
-    a.bc[d] -= am[jj] * s.bcov[jj];
-    a.bcv[jj] -= am[jj] * s.bcon[d];
-  }
-  const double aptot = am[d];  // ptot = p + b^2/2 on the diagonal
-  a.bsq += aeta + 0.5 * aptot;
-  a.rho += aeta;
-  a.u += aeta + (gam - 1.) * (aeta + aptot);  // eta and ptot through p = (gam - 1) u
-}
-
-// primtoflux for direction d (phys.c:59-96), given the adjoint af of its result
-__device__ __forceinline__ void flux_rev(double gam, const double *p, const Geo &q, const StateT<double> &s,
-                                         double eta, int d, const double *af, StateAdj &a)
-{
-  double f[8];
-#pragma unroll
-  for (int k = 0; k < 8; k++) f[k] = af[k] * q.g;
-  const double f0 = f[RHO] + f[UU];  // F[UU] = T^d_t + F[RHO]
-  a.rho += f0 * s.ucon[d];
-  a.uc[d] += f0 * p[RHO];
-  mhd_rev(gam, s, eta, d, f + UU, a);
-#pragma unroll
-  for (int ii = 1; ii < 4; ii++) {  // F[B_i] = b^i u^d - b^d u^i
-    const double fb = f[B1 + ii - 1];
-    a.bc[ii] += fb * s.ucon[d];
-    a.uc[d] += fb * s.bcon[ii];
-    a.bc[d] -= fb * s.ucon[ii];
-    a.uc[ii] -= fb * s.bcon[d];
-  }
-}
-
-// get_state (phys.c:219-252, 108-117, metric.c:210-231) and b^2 reversed:
-// the primitives' adjoint ap
-__device__ __forceinline__ void state_rev(const double *p, const Geo &q, const StateT<double> &s, StateAdj &a,
-                                          double *ap)
-{
-  // b^2 = b^mu b_mu
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    a.bc[k] += a.bsq * s.bcov[k];
-    a.bcv[k] += a.bsq * s.bcon[k];
-  }
-  // b_mu = lower(b^mu)
-  a.bc[0] += q.v00 * a.bcv[0] + q.v01 * a.bcv[1] + q.v03 * a.bcv[3];
-  a.bc[1] += q.v01 * a.bcv[0] + q.v11 * a.bcv[1] + q.v13 * a.bcv[3];
-  a.bc[2] += q.v22 * a.bcv[2];
-  a.bc[3] += q.v03 * a.bcv[0] + q.v13 * a.bcv[1] + q.v33 * a.bcv[3];
-  // b^i = (B^i + b^t u^i) / u^t, b^t = B^i u_i
-  double aBf[3], abt = a.bc[0];
-#pragma unroll
-  for (int ii = 1; ii < 4; ii++) {
-    aBf[ii - 1] = a.bc[ii] / s.ucon[0];
-    abt += a.bc[ii] * s.ucon[ii] / s.ucon[0];
-    a.uc[ii] += a.bc[ii] * s.bcon[0] / s.ucon[0];
-    a.uc[0] -= a.bc[ii] * s.bcon[ii] / s.ucon[0];
-  }
-#pragma unroll
-  for (int ii = 1; ii < 4; ii++) {
-    aBf[ii - 1] += abt * s.ucov[ii];
-    a.ucv[ii] += abt * p[B1 + ii - 1];
-  }
-  // u_mu = lower(u^mu)
-  a.uc[0] += q.v00 * a.ucv[0] + q.v01 * a.ucv[1] + q.v03 * a.ucv[3];
-  a.uc[1] += q.v01 * a.ucv[0] + q.v11 * a.ucv[1] + q.v13 * a.ucv[3];
-  a.uc[2] += q.v22 * a.ucv[2];
-  a.uc[3] += q.v03 * a.ucv[0] + q.v13 * a.ucv[1] + q.v33 * a.ucv[3];
-  // u^t = gamma / alpha, u^i = w^i - gamma beta^i / alpha (beta^2 = 0),
-  // gamma = sqrt(1 + qsq) unless gamma_calc clamps qsq
-  const double w1 = p[U1], w2 = p[U2], w3 = p[U3];
-  const double qsq = q.v11 * w1 * w1 + q.v22 * w2 * w2 + q.v33 * w3 * w3 + 2. * (q.v13 * w1 * w3);
-  const double alpha = q.alpha, b1 = q.n01 * alpha * alpha, b3 = q.n03 * alpha * alpha;
-  const double gamma = s.ucon[0] * alpha;
-  const double agam = a.uc[0] / alpha - a.uc[1] * b1 / alpha - a.uc[3] * b3 / alpha;
-  const double aq = qsq < 0. ? 0. : agam * 0.5 / gamma;
-  ap[RHO] = a.rho;
-  ap[UU] = a.u;
-  ap[U1] = a.uc[1] + aq * (2. * q.v11 * w1 + 2. * q.v13 * w3);
-  ap[U2] = a.uc[2] + aq * 2. * q.v22 * w2;
-  ap[U3] = a.uc[3] + aq * (2. * q.v33 * w3 + 2. * q.v13 * w1);
-  ap[B1] = aBf[0];
-  ap[B2] = aBf[1];
-  ap[B3] = aBf[2];
 }
 
 // source() (phys.c:165-207) reversed: dU_nu = g sum_{j,k} T^j_k conn[k][nu][j]
