@@ -956,15 +956,12 @@ __global__ void __launch_bounds__(128) k_adj_flux(Grid G, const double *__restri
   Geo q;
   load_geo(geo_at(geo, G, DIR == 1 ? L_FACE1 : L_FACE2), G.ng, (long)i * G.sn2 + j, q);
   int f0 = 0;
-  double Fs[8], Us[8], cxs, cns, Fo[8], Uo[8];
+  double Fs[8], Us[8], cxs, cns, Uo[8];
   face_side<DIR>(G.gam, ps, q, Fs, Us, cxs, cns, &f0);
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    Fo[k] = __shfl_xor_sync(pmask, Fs[k], 1);
-    Uo[k] = __shfl_xor_sync(pmask, Us[k], 1);
-  }
+  for (int k = 0; k < 8; k++) Uo[k] = __shfl_xor_sync(pmask, Us[k], 1);
   const double cxo = __shfl_xor_sync(pmask, cxs, 1), cno = __shfl_xor_sync(pmask, cns, 1);
-  const double *Fl = side ? Fo : Fs, *Ul = side ? Uo : Us, *Fr = side ? Fs : Fo, *Ur = side ? Us : Uo;
+  const double *Ul = side ? Uo : Us, *Ur = side ? Us : Uo;
   const double cxl = side ? cxo : cxs, cnl = side ? cno : cns, cxr = side ? cxs : cxo, cnr = side ? cns : cno;
   // lf_flux's wave speed and the branches it takes
   const double t1 = 0. > cxl ? 0. : cxl;
@@ -1048,14 +1045,23 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
   const int nseg = (nsteps + every - 1) / every;
   const int nrec = every < nsteps ? every : nsteps;
   DevBuf B;
-  // checkpoints, per-step records of one segment, adjoint state
+  // checkpoints; per-step records of a segment, twice (segments alternate
+  // between the two sets, so one is recomputed while the other is reversed);
+  // the run state of every step; the adjoint state
   double *ck = B.get<double>(pl * nseg);
   DevScalars *cks = B.get<DevScalars>(nseg + 1);
   double *pend = B.get<double>(pl);
-  double *recp = B.get<double>(pl * (nrec + 1));
-  double *recd = B.get<double>((size_t)nrec * (7 * pl + 2 * nc));
-  signed char *recf = B.get<signed char>((size_t)nrec * 4 * nc);
-  DevScalars *recs = B.get<DevScalars>((size_t)nrec * 2);
+  DevScalars *scall = B.get<DevScalars>(2 * (size_t)nsteps);
+  double *recp[2], *recd[2];
+  signed char *recf[2];
+  DevScalars *recs[2];
+  for (int b = 0; b < 2; b++) {
+    recp[b] = B.get<double>(pl * (nrec + 1));
+    recd[b] = B.get<double>((size_t)nrec * (7 * pl + 2 * nc));
+    recf[b] = B.get<signed char>((size_t)nrec * 4 * nc);
+    recs[b] = B.get<DevScalars>((size_t)nrec * 2);
+    if (!recp[b] || !recd[b] || !recf[b] || !recs[b]) return fail_with(HARM_E_CUDA, "device memory for the adjoint");
+  }
   double *lam = B.get<double>(6 * pl);  // next, cur, ph, U, F1, F2
   double *W = B.get<double>(pl);
   signed char *Wf = B.get<signed char>(nc);
@@ -1064,32 +1070,47 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
   signed char *kinds = B.get<signed char>(FAIL_CAP);
   int *err = B.get<int>(1);
   AdjScalars *as = B.get<AdjScalars>(1);
-  if (!ck || !cks || !pend || !recp || !recd || !recf || !recs || !lam || !W || !Wf || !list || !vbuf || !kinds ||
-      !err || !as)
+  if (!ck || !cks || !pend || !scall || !lam || !W || !Wf || !list || !vbuf || !kinds || !err || !as)
     return fail_with(HARM_E_CUDA, "device memory for the adjoint");
-  std::vector<StepRec> rec(nrec);
-  for (int r = 0; r < nrec; r++) {
-    double *d = recd + (size_t)r * (7 * pl + 2 * nc);
-    StepRec &s = rec[r];
-    s.X1[0] = d; s.X1[1] = d + pl; s.Ub[0] = d + 2 * pl; s.Ub[1] = d + 3 * pl; s.ph = d + 4 * pl;
-    s.Z[0] = d + 5 * pl; s.Z[1] = d + 6 * pl;
-    s.F1rho[0] = d + 7 * pl; s.F1rho[1] = d + 7 * pl + nc;
-    s.fl1[0] = recf + (size_t)r * 4 * nc; s.fl1[1] = s.fl1[0] + nc;
-    s.wz[0] = s.fl1[0] + 2 * nc; s.wz[1] = s.fl1[0] + 3 * nc;
-    s.sc[0] = recs + 2 * r; s.sc[1] = recs + 2 * r + 1;
+  std::vector<StepRec> rec[2];
+  for (int b = 0; b < 2; b++) {
+    rec[b].resize(nrec);
+    for (int r = 0; r < nrec; r++) {
+      double *d = recd[b] + (size_t)r * (7 * pl + 2 * nc);
+      StepRec &s = rec[b][r];
+      s.X1[0] = d; s.X1[1] = d + pl; s.Ub[0] = d + 2 * pl; s.Ub[1] = d + 3 * pl; s.ph = d + 4 * pl;
+      s.Z[0] = d + 5 * pl; s.Z[1] = d + 6 * pl;
+      s.F1rho[0] = d + 7 * pl; s.F1rho[1] = d + 7 * pl + nc;
+      s.fl1[0] = recf[b] + (size_t)r * 4 * nc; s.fl1[1] = s.fl1[0] + nc;
+      s.wz[0] = s.fl1[0] + 2 * nc; s.wz[1] = s.fl1[0] + 3 * nc;
+      s.sc[0] = recs[b] + 2 * r; s.sc[1] = recs[b] + 2 * r + 1;
+    }
   }
   // the adjoint of the state after the step being undone (A) and before it (B)
   double *const A = lam, *const Bl = lam + pl, *lh = lam + 2 * pl, *lU = lam + 3 * pl, *lF1 = lam + 4 * pl,
                 *lF2 = lam + 5 * pl;
-  cudaStream_t st = x->stream;
-  cudaEvent_t e0, e1, e2;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
-  CK(cudaEventCreate(&e2));
-  struct EvGuard {
-    cudaEvent_t a, b, c;
-    ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); }
-  } eg{e0, e1, e2};
+  // the context's stream runs the forward pass and the recomputation, rs the
+  // reverse sweep
+  cudaStream_t st = x->stream, rs = nullptr;
+  CK(cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking));
+  cudaEvent_t e0, e1, e2, efwd, erec[2], erev[2];  // timing; forward done; records ready; reverse done
+  struct Guard {
+    cudaStream_t s;
+    std::vector<cudaEvent_t> e;
+    ~Guard()
+    {
+      for (cudaEvent_t v : e) cudaEventDestroy(v);
+      if (s) cudaStreamDestroy(s);
+    }
+  } guard{rs, {}};
+  for (cudaEvent_t *e : {&e0, &e1, &e2}) {
+    CK(cudaEventCreate(e));
+    guard.e.push_back(*e);
+  }
+  for (cudaEvent_t *e : {&efwd, &erec[0], &erec[1], &erev[0], &erev[1]}) {
+    CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    guard.e.push_back(*e);
+  }
   struct Graph {
     cudaGraphExec_t e = nullptr;
     ~Graph() { if (e) cudaGraphExecDestroy(e); }
@@ -1107,14 +1128,15 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
     return HARM_OK;
   };
   const size_t pb = pl * sizeof(double);
-  // one segment's steps, recorded (recomputation): states before each step and after the last
-  auto record = [&](int len) -> int {
+  // one segment's steps, recorded into set b (recomputation): states before
+  // each step and after the last
+  auto record = [&](int b, int len) -> int {
     for (int r = 0; r < len; r++) {
-      CK(cudaMemcpyAsync(recp + (size_t)r * pl, x->p, pb, cudaMemcpyDeviceToDevice, st));
-      int rc = exact::launch_step_rec(x, rec[r]);
+      CK(cudaMemcpyAsync(recp[b] + (size_t)r * pl, x->p, pb, cudaMemcpyDeviceToDevice, st));
+      int rc = exact::launch_step_rec(x, rec[b][r]);
       if (rc) return rc;
     }
-    CK(cudaMemcpyAsync(recp + (size_t)len * pl, x->p, pb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(recp[b] + (size_t)len * pl, x->p, pb, cudaMemcpyDeviceToDevice, st));
     return HARM_OK;
   };
 
@@ -1125,51 +1147,53 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
   const dim3 g1((G.n2 + 2 + 63) / 64, G.n1 + 1, 1);
   const dim3 g2((G.n2 + 1 + 63) / 64, G.n1 + 2, 1);
   const int nbc = 4 * G.sn2 + 4 * (G.sn1 - 4);
-  // the reverse of one recorded segment of len steps: the adjoint of its last
-  // state in A on entry, of its first state in A on exit, B zero both times
-  auto reverse = [&](int len) -> int {
+  // the reverse of one segment of len steps recorded in set b, on stream q:
+  // the adjoint of its last state in A on entry, of its first state in A on
+  // exit, B zero both times
+  auto reverse = [&](int b, int len, cudaStream_t q) -> int {
     double *lnext = A, *lcur = Bl;
     for (int r = len - 1; r >= 0; r--) {
-      const StepRec &q = rec[r];
-      const DevScalars *sa = q.sc[0], *sb = q.sc[1];
-      const double *pn = recp + (size_t)r * pl, *pnext = recp + (size_t)(r + 1) * pl;
-      k_adj_dt_pre<<<1, 1, 0, st>>>(sa, sb, G.defcon, as);
+      const StepRec &R = rec[b][r];
+      const DevScalars *sa = R.sc[0], *sb = R.sc[1];
+      const double *pn = recp[b] + (size_t)r * pl, *pnext = recp[b] + (size_t)(r + 1) * pl;
+      k_adj_dt_pre<<<1, 1, 0, q>>>(sa, sb, G.defcon, as);
       // objective term on the step's result
-      k_adj_din<<<(G.n2 + 127) / 128, 128, 0, st>>>(G, pnext, x->geo, lnext, sa);
+      k_adj_din<<<(G.n2 + 127) / 128, 128, 0, q>>>(G, pnext, x->geo, lnext, sa);
       // corrector: bound_prim, fixup_utoprim, bound_prim, inversion, update, fluxes
-      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, pnext, x->geo, lnext);
-      k_adj_fixup_utoprim<<<1, FU_THREADS, 0, st>>>(G, q.X1[1], q.fl1[1], x->geo, x->floors, W, Wf, list, vbuf,
-                                                   kinds, lnext, err);
-      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, q.X1[1], x->geo, lnext);
-      k_adj_invert<<<zg, tile, 0, st>>>(G, q.Ub[1], q.Z[1], q.wz[1], x->geo, x->floors, x->katm, lnext, lU, lcur, err);
-      CK(cudaMemsetAsync(lF1, 0, 2 * pb, st));
-      k_adj_cons<true><<<zg, tile, 0, st>>>(G, pn, q.ph, q.Ub[1], q.F1rho[1], x->geo, x->conn, lU, lcur, lh, lF1,
-                                            lF2, sa, as);
-      k_adj_flux<1, true><<<g1, ftile, 0, st>>>(G, q.ph, x->geo, lF1, lh, sa, as);
-      k_adj_flux<2, true><<<g2, ftile, 0, st>>>(G, q.ph, x->geo, lF2, lh, sa, as);
+      k_adj_bound<<<(nbc + 127) / 128, 128, 0, q>>>(G, pnext, x->geo, lnext);
+      k_adj_fixup_utoprim<<<1, FU_THREADS, 0, q>>>(G, R.X1[1], R.fl1[1], x->geo, x->floors, W, Wf, list, vbuf,
+                                                  kinds, lnext, err);
+      k_adj_bound<<<(nbc + 127) / 128, 128, 0, q>>>(G, R.X1[1], x->geo, lnext);
+      k_adj_invert<<<zg, tile, 0, q>>>(G, R.Ub[1], R.Z[1], R.wz[1], x->geo, x->floors, x->katm, lnext, lU, lcur,
+                                       err);
+      CK(cudaMemsetAsync(lF1, 0, 2 * pb, q));
+      k_adj_cons<true><<<zg, tile, 0, q>>>(G, pn, R.ph, R.Ub[1], R.F1rho[1], x->geo, x->conn, lU, lcur, lh, lF1,
+                                           lF2, sa, as);
+      k_adj_flux<1, true><<<g1, ftile, 0, q>>>(G, R.ph, x->geo, lF1, lh, sa, as);
+      k_adj_flux<2, true><<<g2, ftile, 0, q>>>(G, R.ph, x->geo, lF2, lh, sa, as);
       // predictor, from p^n into ph
-      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, q.ph, x->geo, lh);
-      k_adj_fixup_utoprim<<<1, FU_THREADS, 0, st>>>(G, q.X1[0], q.fl1[0], x->geo, x->floors, W, Wf, list, vbuf,
-                                                   kinds, lh, err);
-      k_adj_bound<<<(nbc + 127) / 128, 128, 0, st>>>(G, q.X1[0], x->geo, lh);
-      k_adj_invert<<<zg, tile, 0, st>>>(G, q.Ub[0], q.Z[0], q.wz[0], x->geo, x->floors, x->katm, lh, lU, lcur, err);
-      CK(cudaMemsetAsync(lF1, 0, 2 * pb, st));
-      k_adj_cons<false><<<zg, tile, 0, st>>>(G, pn, pn, q.Ub[0], q.F1rho[0], x->geo, x->conn, lU, lcur, lcur, lF1,
-                                             lF2, sa, as);
-      k_adj_flux<1, false><<<g1, ftile, 0, st>>>(G, pn, x->geo, lF1, lcur, sa, as);
-      k_adj_flux<2, false><<<g2, ftile, 0, st>>>(G, pn, x->geo, lF2, lcur, sa, as);
-      k_adj_dt_post<<<1, 1, 0, st>>>(sa, sb, as);
+      k_adj_bound<<<(nbc + 127) / 128, 128, 0, q>>>(G, R.ph, x->geo, lh);
+      k_adj_fixup_utoprim<<<1, FU_THREADS, 0, q>>>(G, R.X1[0], R.fl1[0], x->geo, x->floors, W, Wf, list, vbuf,
+                                                  kinds, lh, err);
+      k_adj_bound<<<(nbc + 127) / 128, 128, 0, q>>>(G, R.X1[0], x->geo, lh);
+      k_adj_invert<<<zg, tile, 0, q>>>(G, R.Ub[0], R.Z[0], R.wz[0], x->geo, x->floors, x->katm, lh, lU, lcur, err);
+      CK(cudaMemsetAsync(lF1, 0, 2 * pb, q));
+      k_adj_cons<false><<<zg, tile, 0, q>>>(G, pn, pn, R.Ub[0], R.F1rho[0], x->geo, x->conn, lU, lcur, lcur, lF1,
+                                            lF2, sa, as);
+      k_adj_flux<1, false><<<g1, ftile, 0, q>>>(G, pn, x->geo, lF1, lcur, sa, as);
+      k_adj_flux<2, false><<<g2, ftile, 0, q>>>(G, pn, x->geo, lF2, lcur, sa, as);
+      k_adj_dt_post<<<1, 1, 0, q>>>(sa, sb, as);
       CK(cudaGetLastError());
       // the adjoint of p^n becomes the next (earlier) step's output adjoint
       double *t = lnext;
       lnext = lcur;
       lcur = t;
-      CK(cudaMemsetAsync(lcur, 0, pb, st));
-      CK(cudaMemsetAsync(lh, 0, pb, st));
+      CK(cudaMemsetAsync(lcur, 0, pb, q));
+      CK(cudaMemsetAsync(lh, 0, pb, q));
     }
     if (lnext != A) {
-      CK(cudaMemcpyAsync(A, lnext, pb, cudaMemcpyDeviceToDevice, st));
-      CK(cudaMemsetAsync(lnext, 0, pb, st));
+      CK(cudaMemcpyAsync(A, lnext, pb, cudaMemcpyDeviceToDevice, q));
+      CK(cudaMemsetAsync(lnext, 0, pb, q));
     }
     return HARM_OK;
   };
@@ -1177,16 +1201,24 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
   CK(cudaMemsetAsync(err, 0, sizeof(int), st));
   CK(cudaMemsetAsync(as, 0, sizeof(AdjScalars), st));
   CK(cudaMemsetAsync(lam, 0, 6 * pb, st));
-  const int last0 = (nseg - 1) * every, lastlen = nsteps - last0;
-  Graph gstep, grec, grev;
+  const int last0 = (nseg - 1) * every, lastlen = nsteps - last0, blast = (nseg - 1) & 1;
+  Graph gstep, grec[2], grev[2];
   int rc = capture(gstep, [&] { return exact::launch_step(x); });
   if (rc) return rc;
-  if (nseg > 1) {
-    rc = capture(grec, [&] { return record(every); });
+  for (int b = 0; b < 2; b++) {
+    if (nseg > 1) {
+      rc = capture(grec[b], [&] { return record(b, every); });
+      if (rc) return rc;
+    }
+    rc = capture(grev[b], [&] { return reverse(b, every, st); });
     if (rc) return rc;
   }
-  rc = capture(grev, [&] { return reverse(every); });
-  if (rc) return rc;
+  // the run state recorded with segment seg's steps, kept for the checks at the end
+  auto keep_scalars = [&](int seg, int len) -> int {
+    CK(cudaMemcpyAsync(scall + 2 * (size_t)seg * every, recs[seg & 1], 2 * (size_t)len * sizeof(DevScalars),
+                       cudaMemcpyDeviceToDevice, st));
+    return HARM_OK;
+  };
 
   // forward pass: a checkpoint every `every` steps; the last segment is
   // recorded on the way, so it needs no recomputation
@@ -1197,15 +1229,18 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
     if (seg < nseg - 1) {
       for (int r = 0; r < every; r++) CK(cudaGraphLaunch(gstep.e, st));
     } else if (lastlen == every && nseg > 1) {
-      CK(cudaGraphLaunch(grec.e, st));
+      CK(cudaGraphLaunch(grec[blast].e, st));
     } else {
-      rc = record(lastlen);
+      rc = record(blast, lastlen);
       if (rc) return rc;
     }
   }
   CK(cudaEventRecord(e1, st));
+  rc = keep_scalars(nseg - 1, lastlen);
+  if (rc) return rc;
   CK(cudaMemcpyAsync(pend, x->p, pb, cudaMemcpyDeviceToDevice, st));
   CK(cudaMemcpyAsync(cks + nseg, x->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, st));
+  CK(cudaEventRecord(efwd, st));
   DevScalars s0, s1;
   CK(cudaMemcpyAsync(&s0, cks, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(&s1, cks + nseg, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
@@ -1214,35 +1249,45 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
     return fail_with(HARM_E_ADJOINT, "the forward steps failed (fail code " + std::to_string(s1.fail_code) + ")");
   *J = s1.mass_in - s0.mass_in;
 
-  // reverse sweep, segment by segment from the last
-  std::vector<DevScalars> hs(2 * (size_t)nrec);
+  // reverse sweep, segment by segment from the last; each segment's reverse
+  // (rs) overlaps the recomputation of the segment before it (st)
+  CK(cudaStreamWaitEvent(rs, efwd, 0));
   for (int seg = nseg - 1; seg >= 0; seg--) {
-    const int n0 = seg * every, len = seg == nseg - 1 ? lastlen : every;
-    if (seg < nseg - 1) {
-      CK(cudaMemcpyAsync(x->p, ck + (size_t)seg * pl, pb, cudaMemcpyDeviceToDevice, st));
-      CK(cudaMemcpyAsync(x->sc, cks + seg, sizeof(DevScalars), cudaMemcpyDeviceToDevice, st));
-      CK(cudaGraphLaunch(grec.e, st));
-    }
-    CK(cudaMemcpyAsync(hs.data(), recs, 2 * (size_t)len * sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    for (int r = 0; r < len; r++) {
-      const DevScalars &sa = hs[2 * r], &sb = hs[2 * r + 1];
-      if (sb.fail_code) return fail_with(HARM_E_ADJOINT, "a recomputed step failed");
-      if (sb.dt != (sb.ndt > SAFE * sa.dt ? SAFE * sa.dt : sb.ndt))
-        return fail_with(HARM_E_ARG, "the steps reach tf: the adjoint needs dt = min(ndt, 1.3 dt) throughout");
-    }
-    (void)n0;
+    const int b = seg & 1, len = seg == nseg - 1 ? lastlen : every;
+    if (seg < nseg - 1) CK(cudaStreamWaitEvent(rs, erec[b], 0));
     if (len == every) {
-      CK(cudaGraphLaunch(grev.e, st));
+      CK(cudaGraphLaunch(grev[b].e, rs));
     } else {
-      rc = reverse(len);
+      rc = reverse(b, len, rs);
       if (rc) return rc;
     }
+    CK(cudaEventRecord(erev[b], rs));
+    if (seg > 0) {
+      // recompute segment seg - 1 into the other set, once the reverse that
+      // last read that set (segment seg + 1's) is done
+      const int bp = (seg - 1) & 1;
+      if (seg + 1 <= nseg - 1) CK(cudaStreamWaitEvent(st, erev[bp], 0));
+      CK(cudaMemcpyAsync(x->p, ck + (size_t)(seg - 1) * pl, pb, cudaMemcpyDeviceToDevice, st));
+      CK(cudaMemcpyAsync(x->sc, cks + seg - 1, sizeof(DevScalars), cudaMemcpyDeviceToDevice, st));
+      CK(cudaGraphLaunch(grec[bp].e, st));
+      rc = keep_scalars(seg - 1, every);
+      if (rc) return rc;
+      CK(cudaEventRecord(erec[bp], st));
+    }
   }
-  CK(cudaEventRecord(e2, st));
+  CK(cudaEventRecord(e2, rs));
+  CK(cudaStreamWaitEvent(st, e2, 0));
   int herr = 0;
+  std::vector<DevScalars> hs(2 * (size_t)nsteps);
   CK(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(hs.data(), scall, hs.size() * sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  for (int n = 0; n < nsteps; n++) {
+    const DevScalars &sa = hs[2 * n], &sb = hs[2 * n + 1];
+    if (sb.fail_code) return fail_with(HARM_E_ADJOINT, "a recomputed step failed");
+    if (sb.dt != (sb.ndt > SAFE * sa.dt ? SAFE * sa.dt : sb.ndt))
+      return fail_with(HARM_E_ARG, "the steps reach tf: the adjoint needs dt = min(ndt, 1.3 dt) throughout");
+  }
   if (herr & ERR_FAILS)
     return fail_with(HARM_E_ADJOINT, "more failed inversions in a half step than the adjoint lists");
   if (herr & ERR_SINGULAR)
