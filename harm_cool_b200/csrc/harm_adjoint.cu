@@ -1091,23 +1091,28 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
                 *lF2 = lam + 5 * pl;
   // the context's stream runs the forward pass and the recomputation, rs the
   // reverse sweep
-  cudaStream_t st = x->stream, rs = nullptr;
+  cudaStream_t st = x->stream, rs = nullptr, fs = nullptr;
   CK(cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking));
   cudaEvent_t e0, e1, e2, efwd, erec[2], erev[2];  // timing; forward done; records ready; reverse done
+  cudaEvent_t efork[2], ejoin[2];                   // the two face directions, side by side
   struct Guard {
-    cudaStream_t s;
+    cudaStream_t s, f;
     std::vector<cudaEvent_t> e;
     ~Guard()
     {
       for (cudaEvent_t v : e) cudaEventDestroy(v);
       if (s) cudaStreamDestroy(s);
+      if (f) cudaStreamDestroy(f);
     }
-  } guard{rs, {}};
+  } guard{rs, nullptr, {}};
+  CK(cudaStreamCreateWithFlags(&fs, cudaStreamNonBlocking));
+  guard.f = fs;
   for (cudaEvent_t *e : {&e0, &e1, &e2}) {
     CK(cudaEventCreate(e));
     guard.e.push_back(*e);
   }
-  for (cudaEvent_t *e : {&efwd, &erec[0], &erec[1], &erev[0], &erev[1]}) {
+  for (cudaEvent_t *e :
+       {&efwd, &erec[0], &erec[1], &erev[0], &erev[1], &efork[0], &efork[1], &ejoin[0], &ejoin[1]}) {
     CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     guard.e.push_back(*e);
   }
@@ -1169,8 +1174,13 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       CK(cudaMemsetAsync(lF1, 0, 2 * pb, q));
       k_adj_cons<true><<<zg, tile, 0, q>>>(G, pn, R.ph, R.Ub[1], R.F1rho[1], x->geo, x->conn, lU, lcur, lh, lF1,
                                            lF2, sa, as);
+      // the two directions run side by side (fs), each adding into the state adjoint
+      CK(cudaEventRecord(efork[0], q));
+      CK(cudaStreamWaitEvent(fs, efork[0], 0));
       k_adj_flux<1, true><<<g1, ftile, 0, q>>>(G, R.ph, x->geo, lF1, lh, sa, as);
-      k_adj_flux<2, true><<<g2, ftile, 0, q>>>(G, R.ph, x->geo, lF2, lh, sa, as);
+      k_adj_flux<2, true><<<g2, ftile, 0, fs>>>(G, R.ph, x->geo, lF2, lh, sa, as);
+      CK(cudaEventRecord(ejoin[0], fs));
+      CK(cudaStreamWaitEvent(q, ejoin[0], 0));
       // predictor, from p^n into ph
       k_adj_bound<<<(nbc + 127) / 128, 128, 0, q>>>(G, R.ph, x->geo, lh);
       k_adj_fixup_utoprim<<<1, FU_THREADS, 0, q>>>(G, R.X1[0], R.fl1[0], x->geo, x->floors, W, Wf, list, vbuf,
@@ -1180,8 +1190,12 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       CK(cudaMemsetAsync(lF1, 0, 2 * pb, q));
       k_adj_cons<false><<<zg, tile, 0, q>>>(G, pn, pn, R.Ub[0], R.F1rho[0], x->geo, x->conn, lU, lcur, lcur, lF1,
                                             lF2, sa, as);
+      CK(cudaEventRecord(efork[1], q));
+      CK(cudaStreamWaitEvent(fs, efork[1], 0));
       k_adj_flux<1, false><<<g1, ftile, 0, q>>>(G, pn, x->geo, lF1, lcur, sa, as);
-      k_adj_flux<2, false><<<g2, ftile, 0, q>>>(G, pn, x->geo, lF2, lcur, sa, as);
+      k_adj_flux<2, false><<<g2, ftile, 0, fs>>>(G, pn, x->geo, lF2, lcur, sa, as);
+      CK(cudaEventRecord(ejoin[1], fs));
+      CK(cudaStreamWaitEvent(q, ejoin[1], 0));
       k_adj_dt_post<<<1, 1, 0, q>>>(sa, sb, as);
       CK(cudaGetLastError());
       // the adjoint of p^n becomes the next (earlier) step's output adjoint
