@@ -111,11 +111,9 @@ __global__ void k_adj_din(Grid G, const double *__restrict__ P, const double *__
 // inflow_check(); the ghost's own adjoint ends (its old value was overwritten).
 // X holds the values bound_prim copied (its active cells).
 
-__global__ void k_adj_bound(Grid G, const double *__restrict__ X, const double *__restrict__ geo, double *lam)
+__device__ __forceinline__ void bound_rev_cell(const Grid &G, const double *__restrict__ X,
+                                               const double *__restrict__ geo, double *lam, int t)
 {
-  const int ncell = 4 * G.sn2 + 4 * (G.sn1 - 4);
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ncell) return;
   BoundCell b = bound_cell(G, t, 4);
   const int i = b.i, j = b.j;
   const bool rghost = i < G.istart || i > G.istop;
@@ -166,15 +164,25 @@ __global__ void k_adj_bound(Grid G, const double *__restrict__ X, const double *
   }
 }
 
+__global__ void k_adj_bound(Grid G, const double *__restrict__ X, const double *__restrict__ geo, double *lam)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < 4 * G.sn2 + 4 * (G.sn1 - 4)) bound_rev_cell(G, X, geo, lam, t);
+}
+
 // ---------------------------------------------------------------------------
 // fixup_utoprim (fixup.c:432-538) transposed.  One block: the failed zones of
 // the half step (pflag != 0 after the first bound_prim) are listed in loop
 // order, the repairs are replayed on a working copy exactly as the step made
 // them (each stencil chosen from the flags as earlier repairs left them), and
 // then undone in reverse order, so a last-resort average that read an earlier
-// repair passes its adjoint on to that repair's stencil.
+// repair passes its adjoint on to that repair's stencil.  The kernel then
+// transposes the bound_prim that came before the repairs (the repairs may
+// read ghost cells).  Without a repair the ghosts' adjoint is already zero
+// (the later bound_prim's transpose cleared it), so that bound_prim's
+// transpose has nothing to do either, and the kernel ends after its scan.
 
-__global__ void __launch_bounds__(FU_THREADS) k_adj_fixup_utoprim(Grid G, const double *__restrict__ X1,
+__global__ void __launch_bounds__(FU_THREADS) k_adj_fixup_bound(Grid G, const double *__restrict__ X1,
                                                                   const signed char *__restrict__ fl1,
                                                                   const double *__restrict__ geo,
                                                                   const double *__restrict__ floors, double *W,
@@ -184,6 +192,16 @@ __global__ void __launch_bounds__(FU_THREADS) k_adj_fixup_utoprim(Grid G, const 
   __shared__ int cnt[FU_THREADS];
   __shared__ int nsh;
   const int tid = threadIdx.x;
+  {
+    // any failed zone at all? (coalesced)
+    int any = 0;
+    const int na = G.n1 * G.n2;
+    for (int t = tid; t < na; t += FU_THREADS) {
+      const int ii = t / G.n2, jj = t - ii * G.n2;
+      any |= fl1[cidx(G, 0, G.istart + ii, G.jstart + jj)] != 0;
+    }
+    if (__syncthreads_or(any) == 0) return;
+  }
   const long nact = (long)G.n1 * G.n2;
   const long per = (nact + FU_THREADS - 1) / FU_THREADS;
   const long a0 = tid * per, a1 = a0 + per < nact ? a0 + per : nact;
@@ -193,7 +211,7 @@ __global__ void __launch_bounds__(FU_THREADS) k_adj_fixup_utoprim(Grid G, const 
     if (fl1[cidx(G, 0, i, j)] != 0) m++;
   }
   cnt[tid] = m;
-  if (__syncthreads_or(m) == 0) return;  // no failed zone: nothing was repaired
+  __syncthreads();
   if (tid == 0) {
     int s = 0;
     for (int k = 0; k < FU_THREADS; k++) {
@@ -222,66 +240,70 @@ __global__ void __launch_bounds__(FU_THREADS) k_adj_fixup_utoprim(Grid G, const 
     Wf[c] = (signed char)(!fl1[c]);  // k_fu_flip
   }
   __syncthreads();
-  if (tid != 0) return;
-  const double *gC = geo_at(geo, G, L_CENT);
-  for (int t = 0; t < n; t++) {
-    const long c = list[t];
-    const int kind = stencil_kind(G, Wf, c);
-    double v[8];
-    repair_zone(G, W, c, kind, v);
-    for (int k = 0; k < 8; k++) vbuf[(long)t * 8 + k] = v[k];
-    kinds[t] = (signed char)kind;
-    const int i = (int)((c / G.sn2) % G.sn1), j = (int)(c % G.sn2);
-    const long gi = (long)i * G.sn2 + j;
-    Geo q;
-    load_geo(gC, G.ng, gi, q);
-    int fail = 0;
-    const bool g33 = fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
-    for (int k = 0; k < 8; k++) W[k * G.nc + c] = v[k];
-    Wf[c] = g33 ? (signed char)-33 : (signed char)0;
-  }
-  const long s = G.sn2;
-  for (int t = n - 1; t >= 0; t--) {
-    const long c = list[t];
-    const int kind = kinds[t];
-    const int i = (int)((c / G.sn2) % G.sn1), j = (int)(c % G.sn2);
-    const long gi = (long)i * G.sn2 + j;
-    Geo q;
-    load_geo(gC, G.ng, gi, q);
-    D8 v[8];
-    for (int k = 0; k < 8; k++) v[k] = D8::seed(vbuf[(long)t * 8 + k], k);
-    int fail = 0;
-    fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
-    double lo[8], lv[8];
-    for (int k = 0; k < 8; k++) lo[k] = lam[k * G.nc + c];
-    for (int k = 0; k < 8; k++) {
-      double a = 0.;
-      for (int r = 0; r < 8; r++) a += lo[r] * v[r].d[k];
-      lv[k] = a;
+  if (tid == 0) {
+    const double *gC = geo_at(geo, G, L_CENT);
+    for (int t = 0; t < n; t++) {
+      const long c = list[t];
+      const int kind = stencil_kind(G, Wf, c);
+      double v[8];
+      repair_zone(G, W, c, kind, v);
+      for (int k = 0; k < 8; k++) vbuf[(long)t * 8 + k] = v[k];
+      kinds[t] = (signed char)kind;
+      const int i = (int)((c / G.sn2) % G.sn1), j = (int)(c % G.sn2);
+      const long gi = (long)i * G.sn2 + j;
+      Geo q;
+      load_geo(gC, G.ng, gi, q);
+      int fail = 0;
+      const bool g33 = fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
+      for (int k = 0; k < 8; k++) W[k * G.nc + c] = v[k];
+      Wf[c] = g33 ? (signed char)-33 : (signed char)0;
     }
-    // the repair keeps the zone's fields and replaces the rest
-    for (int k = 0; k < 8; k++) lam[k * G.nc + c] = k >= B1 ? lv[k] : 0.;
-    if (kind == 0) {
-      for (int k = 0; k < B1; k++) {
-        double *L = lam + k * G.nc;
-        const double a = 0.25 * lv[k];
-        L[c + 1] += a; L[c - 1] += a; L[c - s] += a; L[c + s] += a;
+    const long s = G.sn2;
+    for (int t = n - 1; t >= 0; t--) {
+      const long c = list[t];
+      const int kind = kinds[t];
+      const int i = (int)((c / G.sn2) % G.sn1), j = (int)(c % G.sn2);
+      const long gi = (long)i * G.sn2 + j;
+      Geo q;
+      load_geo(gC, G.ng, gi, q);
+      D8 v[8];
+      for (int k = 0; k < 8; k++) v[k] = D8::seed(vbuf[(long)t * 8 + k], k);
+      int fail = 0;
+      fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail);
+      double lo[8], lv[8];
+      for (int k = 0; k < 8; k++) lo[k] = lam[k * G.nc + c];
+      for (int k = 0; k < 8; k++) {
+        double a = 0.;
+        for (int r = 0; r < 8; r++) a += lo[r] * v[r].d[k];
+        lv[k] = a;
       }
-    } else if (kind == 1) {
-      for (int k = 0; k < B1; k++) {
-        double *L = lam + k * G.nc;
-        const double a = 0.25 * lv[k];
-        L[c + s + 1] += a; L[c + s - 1] += a; L[c - s + 1] += a; L[c - s - 1] += a;
-      }
-    } else {
-      for (int k = RHO; k <= UU; k++) {
-        double *L = lam + k * G.nc;
-        const double a = 0.5 * 0.25 * lv[k];
-        L[c + 1] += a; L[c - 1] += a; L[c - s] += a; L[c + s] += a;
-        L[c + s + 1] += a; L[c + s - 1] += a; L[c - s + 1] += a; L[c - s - 1] += a;
+      // the repair keeps the zone's fields and replaces the rest
+      for (int k = 0; k < 8; k++) lam[k * G.nc + c] = k >= B1 ? lv[k] : 0.;
+      if (kind == 0) {
+        for (int k = 0; k < B1; k++) {
+          double *L = lam + k * G.nc;
+          const double a = 0.25 * lv[k];
+          L[c + 1] += a; L[c - 1] += a; L[c - s] += a; L[c + s] += a;
+        }
+      } else if (kind == 1) {
+        for (int k = 0; k < B1; k++) {
+          double *L = lam + k * G.nc;
+          const double a = 0.25 * lv[k];
+          L[c + s + 1] += a; L[c + s - 1] += a; L[c - s + 1] += a; L[c - s - 1] += a;
+        }
+      } else {
+        for (int k = RHO; k <= UU; k++) {
+          double *L = lam + k * G.nc;
+          const double a = 0.5 * 0.25 * lv[k];
+          L[c + 1] += a; L[c - 1] += a; L[c - s] += a; L[c + s] += a;
+          L[c + s + 1] += a; L[c + s - 1] += a; L[c - s + 1] += a; L[c - s - 1] += a;
+        }
       }
     }
   }
+  __syncthreads();
+  // the bound_prim before the repairs, transposed
+  for (int t = tid; t < 4 * G.sn2 + 4 * (G.sn1 - 4); t += FU_THREADS) bound_rev_cell(G, X1, geo, lam, t);
 }
 
 // ---------------------------------------------------------------------------
@@ -1166,9 +1188,8 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       k_adj_din<<<(G.n2 + 127) / 128, 128, 0, q>>>(G, pnext, x->geo, lnext, sa);
       // corrector: bound_prim, fixup_utoprim, bound_prim, inversion, update, fluxes
       k_adj_bound<<<(nbc + 127) / 128, 128, 0, q>>>(G, pnext, x->geo, lnext);
-      k_adj_fixup_utoprim<<<1, FU_THREADS, 0, q>>>(G, R.X1[1], R.fl1[1], x->geo, x->floors, W, Wf, list, vbuf,
-                                                  kinds, lnext, err);
-      k_adj_bound<<<(nbc + 127) / 128, 128, 0, q>>>(G, R.X1[1], x->geo, lnext);
+      k_adj_fixup_bound<<<1, FU_THREADS, 0, q>>>(G, R.X1[1], R.fl1[1], x->geo, x->floors, W, Wf, list, vbuf, kinds,
+                                                lnext, err);
       k_adj_invert<<<zg, tile, 0, q>>>(G, R.Ub[1], R.Z[1], R.wz[1], x->geo, x->floors, x->katm, lnext, lU, lcur,
                                        err);
       CK(cudaMemsetAsync(lF1, 0, 2 * pb, q));
@@ -1183,9 +1204,8 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       CK(cudaStreamWaitEvent(q, ejoin[0], 0));
       // predictor, from p^n into ph
       k_adj_bound<<<(nbc + 127) / 128, 128, 0, q>>>(G, R.ph, x->geo, lh);
-      k_adj_fixup_utoprim<<<1, FU_THREADS, 0, q>>>(G, R.X1[0], R.fl1[0], x->geo, x->floors, W, Wf, list, vbuf,
-                                                  kinds, lh, err);
-      k_adj_bound<<<(nbc + 127) / 128, 128, 0, q>>>(G, R.X1[0], x->geo, lh);
+      k_adj_fixup_bound<<<1, FU_THREADS, 0, q>>>(G, R.X1[0], R.fl1[0], x->geo, x->floors, W, Wf, list, vbuf, kinds,
+                                                lh, err);
       k_adj_invert<<<zg, tile, 0, q>>>(G, R.Ub[0], R.Z[0], R.wz[0], x->geo, x->floors, x->katm, lh, lU, lcur, err);
       CK(cudaMemsetAsync(lF1, 0, 2 * pb, q));
       k_adj_cons<false><<<zg, tile, 0, q>>>(G, pn, pn, R.Ub[0], R.F1rho[0], x->geo, x->conn, lU, lcur, lcur, lF1,
