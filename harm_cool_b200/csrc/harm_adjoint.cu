@@ -57,9 +57,10 @@ struct AdjScalars {
   int claim[2];        // the face that set each minimum has been found
 };
 
-// before step n's reverse: dt^{n+1} = min(ndt, 1.3 dt^n), ndt = defcon / (1/n1 + 1/n2)
-// (step_ch.c:126-137); sa is the run state before k_finalize, sb after
-__global__ void k_adj_dt_pre(const DevScalars *sa, const DevScalars *sb, double defcon, AdjScalars *a)
+// before step n's reverse (run by k_adj_din_bound): dt^{n+1} = min(ndt, 1.3 dt^n),
+// ndt = defcon / (1/n1 + 1/n2) (step_ch.c:126-137); sa is the run state before
+// k_finalize, sb after
+__device__ __forceinline__ void adj_dt_pre(const DevScalars *sa, const DevScalars *sb, double defcon, AdjScalars *a)
 {
   const double dt = sa->dt, ndt = sb->ndt;
   const double n1 = __longlong_as_double((long long)sa->ndt_bits[0]);
@@ -84,12 +85,10 @@ __global__ void k_adj_dt_post(const DevScalars *sa, const DevScalars *sb, AdjSca
 // ---------------------------------------------------------------------------
 // objective: dt^n * din^n on the inner ghost row of p^{n+1} (diag.c:499)
 
-__global__ void k_adj_din(Grid G, const double *__restrict__ P, const double *__restrict__ geo, double *lam,
-                          const DevScalars *sa)
+// the seed of one inner ghost cell (i = istart - 1, active j), weight w = dt^n
+__device__ __forceinline__ void din_seed(const Grid &G, const double *__restrict__ P, const double *__restrict__ geo,
+                                         double *lam, int j, double w)
 {
-  const double w = sa->dt;
-  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
-  if (j > G.jstop) return;
   const int i = G.istart - 1;
   const long c = cidx(G, 0, i, j);
   D8 pr[8];
@@ -168,6 +167,21 @@ __global__ void k_adj_bound(Grid G, const double *__restrict__ X, const double *
 {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < 4 * G.sn2 + 4 * (G.sn1 - 4)) bound_rev_cell(G, X, geo, lam, t);
+}
+
+// The start of one step's reverse: the time step's chain (adj_dt_pre), the
+// objective's seed dt^n d(rho u^1 sqrt(-g))/dp on the inner ghost row of the
+// step's result P, and the transpose of the bound_prim that produced those
+// ghosts -- each ghost cell seeded and transposed by the same thread.
+__global__ void k_adj_din_bound(Grid G, const double *__restrict__ P, const double *__restrict__ geo, double *lam,
+                                const DevScalars *sa, const DevScalars *sb, AdjScalars *as)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) adj_dt_pre(sa, sb, G.defcon, as);
+  if (t >= 4 * G.sn2 + 4 * (G.sn1 - 4)) return;
+  const BoundCell b = bound_cell(G, t, 4);
+  if (b.i == G.istart - 1 && b.j >= G.jstart && b.j <= G.jstop) din_seed(G, P, geo, lam, b.j, sa->dt);
+  bound_rev_cell(G, P, geo, lam, t);
 }
 
 // ---------------------------------------------------------------------------
@@ -1183,11 +1197,9 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       const StepRec &R = rec[b][r];
       const DevScalars *sa = R.sc[0], *sb = R.sc[1];
       const double *pn = recp[b] + (size_t)r * pl, *pnext = recp[b] + (size_t)(r + 1) * pl;
-      k_adj_dt_pre<<<1, 1, 0, q>>>(sa, sb, G.defcon, as);
-      // objective term on the step's result
-      k_adj_din<<<(G.n2 + 127) / 128, 128, 0, q>>>(G, pnext, x->geo, lnext, sa);
-      // corrector: bound_prim, fixup_utoprim, bound_prim, inversion, update, fluxes
-      k_adj_bound<<<(nbc + 127) / 128, 128, 0, q>>>(G, pnext, x->geo, lnext);
+      // the time step's chain, the objective's seed on the step's result, and
+      // the corrector's bound_prim, fixup_utoprim, bound_prim, inversion, update, fluxes
+      k_adj_din_bound<<<(nbc + 127) / 128, 128, 0, q>>>(G, pnext, x->geo, lnext, sa, sb, as);
       k_adj_fixup_bound<<<1, FU_THREADS, 0, q>>>(G, R.X1[1], R.fl1[1], x->geo, x->floors, W, Wf, list, vbuf, kinds,
                                                 lnext, err);
       k_adj_invert<<<zg, tile, 0, q>>>(G, R.Ub[1], R.Z[1], R.wz[1], x->geo, x->floors, x->katm, lnext, lU, lcur,
