@@ -887,15 +887,13 @@ __global__ void __launch_bounds__(128) k_adj_cons(Grid G, const double *__restri
 // the face fluxes (k_flux: limited face states, LF flux) transposed
 
 // face_side (harm_phys.cuh: get_state, primtoflux for DIR and for t, vchar
-// (phys.c:337-476)) reversed: given the adjoints of its outputs aF (F^DIR),
-// aU (F^t), acx (vmax) and acn (vmin), the adjoint of the side's primitives
+// (phys.c:337-476)) reversed: given the side's state s (get_state of p) and the
+// adjoints of its outputs aF (F^DIR), aU (F^t), acx (vmax) and acn (vmin), the
+// adjoint of the side's primitives
 template <int DIR>
-__device__ __forceinline__ void face_side_rev(double gam, const double *p, const Geo &q, const double *aF,
-                                              const double *aU, double acx, double acn, double *ap)
+__device__ __forceinline__ void face_side_rev(double gam, const double *p, const Geo &q, const StateT<double> &s,
+                                              const double *aF, const double *aU, double acx, double acn, double *ap)
 {
-  StateT<double> s;
-  int fail = 0;
-  get_state(p, q, s, &fail);
   const double rho = p[RHO], u = p[UU];
   const double bsq = dot4(s.bcon, s.bcov);
 
@@ -991,9 +989,13 @@ __global__ void __launch_bounds__(128) k_adj_flux(Grid G, const double *__restri
   }
   Geo q;
   load_geo(geo_at(geo, G, DIR == 1 ? L_FACE1 : L_FACE2), G.ng, (long)i * G.sn2 + j, q);
+  // this side's state, conserved variables and wave speeds (face_side without F^DIR)
   int f0 = 0;
-  double Fs[8], Us[8], cxs, cns, Uo[8];
-  face_side<DIR>(G.gam, ps, q, Fs, Us, cxs, cns, &f0);
+  StateT<double> ss;
+  get_state(ps, q, ss, &f0);
+  double Us[8], cxs, cns, Uo[8];
+  primtoflux(G.gam, ps, ss, 0, q.g, Us);
+  vchar(G.gam, ps, ss, q, DIR, cxs, cns, &f0);
 #pragma unroll
   for (int k = 0; k < 8; k++) Uo[k] = __shfl_xor_sync(pmask, Us[k], 1);
   const double cxo = __shfl_xor_sync(pmask, cxs, 1), cno = __shfl_xor_sync(pmask, cns, 1);
@@ -1037,7 +1039,7 @@ __global__ void __launch_bounds__(128) k_adj_flux(Grid G, const double *__restri
     aF[k] = 0.5 * lF[k];
     aU[k] = (side ? -0.5 : 0.5) * ctop * lF[k];
   }
-  face_side_rev<DIR>(G.gam, ps, q, aF, aU, side ? acxr : acxl, side ? acnr : acnl, ap);
+  face_side_rev<DIR>(G.gam, ps, q, ss, aF, aU, side ? acxr : acxl, side ? acnr : acnl, ap);
   // and through the limiter onto the four cells
 #pragma unroll
   for (int k = 0; k < 8; k++) {
