@@ -215,10 +215,14 @@ int harm_dump_write(harm_ctx *ctx, const harm_restart_header *hdr, const harm_gr
    Reverse sweep: states kept every checkpoint_every steps, each segment
    recomputed by the step's own kernels, then transposed step by step (limiter
    branches, floors and wave-speed choices frozen at the forward's; the
-   inversion differentiated through primtoU at its converged solution).  ms,
-   if not NULL, gets the device time of the forward pass (ms[0]) and of the
-   reverse sweep with its recomputation (ms[1]).  Refused for 3D, COOL_EOS,
-   the mixed step and attached tracers; HARM_E_ADJOINT if a step fails. */
+   inversion differentiated through its converged Newton system).  ms, if not
+   NULL, gets the device time of the forward pass (ms[0]) and of the reverse
+   sweep with its recomputation (ms[1]).  The call allocates device memory for
+   the checkpoints and for two segments' records (about 18 MB per step of a
+   segment at 192x192), works on the context's stream and on two streams of
+   its own, and returns when the results are in J and grad.  Refused for 3D,
+   COOL_EOS, the mixed step and attached tracers; HARM_E_ADJOINT if a step
+   fails. */
 int harm_adjoint_mass_in(harm_ctx *ctx, int nsteps, int checkpoint_every, double *J, double *grad, double *ms);
 
 /* ---- diagnostics ---- */
