@@ -218,7 +218,7 @@ int harm_dump_write(harm_ctx *ctx, const harm_restart_header *hdr, const harm_gr
    inversion differentiated through its converged Newton system).  ms, if not
    NULL, gets the device time of the forward pass (ms[0]) and of the reverse
    sweep with its recomputation (ms[1]).  The call allocates device memory for
-   the checkpoints and for two segments' records (about 18 MB per step of a
+   the checkpoints and for two segments' records (about 20 MB per step of a
    segment at 192x192), works on the context's stream and on two streams of
    its own, and returns when the results are in J and grad.  Refused for 3D,
    COOL_EOS, the mixed step and attached tracers; HARM_E_ADJOINT if a step
