@@ -785,14 +785,14 @@ __device__ __forceinline__ void emf_adjoint(const Grid &G, int i, int j, double 
 }
 
 // U = primtoU(pi) + Dt (-dF1/dx1 - dF2/dx2 + source(pb)) (step_ch.c:247-263);
-// FULL: the corrector (pi = p^n, pb = ph), else the predictor (pi = pb = p^n)
+// FULL: the corrector (pi = p^n, pb = ph), whose source at ph is
+// k_adj_source's, else the predictor (pi = pb = p^n)
 template <bool FULL>
-__global__ void __launch_bounds__(128) k_adj_cons(Grid G, const double *__restrict__ pi, const double *__restrict__ pb,
+__global__ void __launch_bounds__(128) k_adj_cons(Grid G, const double *__restrict__ pi,
                                                   const double *__restrict__ Ub, const double *__restrict__ F1rho,
                                                   const double *__restrict__ geo, const double *__restrict__ conn,
-                                                  const double *__restrict__ lamU, double *lampi, double *lampb,
-                                                  double *lamF1, double *lamF2, const DevScalars *sa,
-                                                  AdjScalars *as)
+                                                  const double *__restrict__ lamU, double *lampi, double *lamF1,
+                                                  double *lamF2, const DevScalars *sa, AdjScalars *as)
 {
   const double Dt = FULL ? sa->dt : 0.5 * sa->dt;
   double *lamDt = &as->lDt[FULL ? 1 : 0];
@@ -825,21 +825,6 @@ __global__ void __launch_bounds__(128) k_adj_cons(Grid G, const double *__restri
       state_rev(pz, q, s, a, li);
 #pragma unroll
       for (int k = 0; k < 8; k++) lampi[k * G.nc + c] += li[k];
-    }
-    if (FULL) {
-      double pz[8];
-#pragma unroll
-      for (int k = 0; k < 8; k++) pz[k] = pb[k * G.nc + c];
-      StateT<double> s;
-      get_state(pz, q, s, &fail);
-      const double eta = (G.gam - 1.) * pz[UU] + pz[RHO] + pz[UU] + dot4(s.bcon, s.bcov);
-      StateAdj a;
-      adj_zero(a);
-      source_rev(G.gam, q, s, eta, conn, G.ng, gi, lu, Dt, a);
-      double lb[8];
-      state_rev(pz, q, s, a, lb);
-#pragma unroll
-      for (int k = 0; k < 8; k++) lampb[k * G.nc + c] += lb[k];
     }
     // dU/dDt = (U - primtoU(pi)) / Dt, the step's own flux divergence plus source
 #pragma unroll
@@ -881,6 +866,39 @@ __global__ void __launch_bounds__(128) k_adj_cons(Grid G, const double *__restri
   if ((t & 31) == 0) red[t >> 5] = v;
   __syncthreads();
   if (t == 0) atomicAdd(lamDt, (red[0] + red[1]) + (red[2] + red[3]));
+}
+
+// the corrector's source at pb = ph (its part of k_cons), reversed: the adjoint
+// of ph gets dt (d source / d ph)^T lamU; runs beside k_adj_cons<true>
+__global__ void __launch_bounds__(128) k_adj_source(Grid G, const double *__restrict__ pb,
+                                                    const double *__restrict__ geo, const double *__restrict__ conn,
+                                                    const double *__restrict__ lamU, double *lampb,
+                                                    const DevScalars *sa)
+{
+  const int j = G.jstart + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
+  if (i > G.istop || j > G.jstop) return;
+  const long c = cidx(G, 0, i, j);
+  const long gi = (long)i * G.sn2 + j;
+  Geo q;
+  load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
+  double lu[8], pz[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    lu[k] = lamU[k * G.nc + c];
+    pz[k] = pb[k * G.nc + c];
+  }
+  StateT<double> s;
+  int fail = 0;
+  get_state(pz, q, s, &fail);
+  const double eta = (G.gam - 1.) * pz[UU] + pz[RHO] + pz[UU] + dot4(s.bcon, s.bcov);
+  StateAdj a;
+  adj_zero(a);
+  source_rev(G.gam, q, s, eta, conn, G.ng, gi, lu, sa->dt, a);
+  double lb[8];
+  state_rev(pz, q, s, a, lb);
+#pragma unroll
+  for (int k = 0; k < 8; k++) lampb[k * G.nc + c] += lb[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -1133,6 +1151,7 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
   CK(cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking));
   cudaEvent_t e0, e1, e2, efwd, erec[2], erev[2];  // timing; forward done; records ready; reverse done
   cudaEvent_t efork[2], ejoin[2];                   // the two face directions, side by side
+  cudaEvent_t ecf, ecj;                             // the corrector's update and source, side by side
   struct Guard {
     cudaStream_t s, f;
     std::vector<cudaEvent_t> e;
@@ -1150,7 +1169,7 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
     guard.e.push_back(*e);
   }
   for (cudaEvent_t *e :
-       {&efwd, &erec[0], &erec[1], &erev[0], &erev[1], &efork[0], &efork[1], &ejoin[0], &ejoin[1]}) {
+       {&efwd, &erec[0], &erec[1], &erev[0], &erev[1], &efork[0], &efork[1], &ejoin[0], &ejoin[1], &ecf, &ecj}) {
     CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     guard.e.push_back(*e);
   }
@@ -1207,8 +1226,13 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       k_adj_invert<<<zg, tile, 0, q>>>(G, R.Ub[1], R.Z[1], R.wz[1], x->geo, x->floors, x->katm, lnext, lU, lcur,
                                        err);
       CK(cudaMemsetAsync(lF1, 0, 2 * pb, q));
-      k_adj_cons<true><<<zg, tile, 0, q>>>(G, pn, R.ph, R.Ub[1], R.F1rho[1], x->geo, x->conn, lU, lcur, lh, lF1,
-                                           lF2, sa, as);
+      // primtoU(p^n) and the face fluxes' adjoints beside the source at ph (fs)
+      CK(cudaEventRecord(ecf, q));
+      CK(cudaStreamWaitEvent(fs, ecf, 0));
+      k_adj_cons<true><<<zg, tile, 0, q>>>(G, pn, R.Ub[1], R.F1rho[1], x->geo, x->conn, lU, lcur, lF1, lF2, sa, as);
+      k_adj_source<<<zg, tile, 0, fs>>>(G, R.ph, x->geo, x->conn, lU, lh, sa);
+      CK(cudaEventRecord(ecj, fs));
+      CK(cudaStreamWaitEvent(q, ecj, 0));
       // the two directions run side by side (fs), each adding into the state adjoint
       CK(cudaEventRecord(efork[0], q));
       CK(cudaStreamWaitEvent(fs, efork[0], 0));
@@ -1222,8 +1246,8 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
                                                 lh, err);
       k_adj_invert<<<zg, tile, 0, q>>>(G, R.Ub[0], R.Z[0], R.wz[0], x->geo, x->floors, x->katm, lh, lU, lcur, err);
       CK(cudaMemsetAsync(lF1, 0, 2 * pb, q));
-      k_adj_cons<false><<<zg, tile, 0, q>>>(G, pn, pn, R.Ub[0], R.F1rho[0], x->geo, x->conn, lU, lcur, lcur, lF1,
-                                            lF2, sa, as);
+      k_adj_cons<false><<<zg, tile, 0, q>>>(G, pn, R.Ub[0], R.F1rho[0], x->geo, x->conn, lU, lcur, lF1, lF2, sa,
+                                            as);
       CK(cudaEventRecord(efork[1], q));
       CK(cudaStreamWaitEvent(fs, efork[1], 0));
       k_adj_flux<1, false><<<g1, ftile, 0, q>>>(G, pn, x->geo, lF1, lcur, sa, as);
