@@ -11,27 +11,31 @@
 // Method.  The state p^n of every checkpoint_every-th step is kept on a forward
 // pass; the reverse sweep recomputes each segment from its checkpoint with the
 // step's own kernels (exact::launch_step_rec), keeping the intermediates of
-// every step (StepRec), and then walks the steps backwards.  Each part of a
-// step is transposed where it is linear (flux-CT averaging, the flux
-// divergence, bound_prim copies, fixup_utoprim stencils).  The face fluxes
-// (get_state, primtoflux, vchar and the Lax-Friedrichs combination), primtoU
-// and the connection source are differentiated by hand in reverse mode.  The
-// limiter, fixup() floors, inflow_check(), the objective and the primtoU
-// Jacobian of the inversion are linearised with forward-mode dual numbers
+// every step (StepRec), and then walks the steps backwards.  The recomputation
+// of one segment runs on the context's stream while the next is reversed on
+// another.  Each part of a step is transposed where it is linear (flux-CT
+// averaging, the flux divergence, bound_prim copies, fixup_utoprim stencils).
+// The face fluxes (get_state, primtoflux, vchar and the Lax-Friedrichs
+// combination), primtoU, the connection source and fixup()'s floors (outside
+// its drift-frame branch) are differentiated by hand in reverse mode.  The
+// limiter, inflow_check(), the objective, the drift-frame floors and the
+// fall-back inversions are linearised with forward-mode dual numbers
 // (harm_dual.cuh).  Limiter branches, clamps and the wave-speed choice are
 // frozen at the forward's.  The inversion is differentiated through its
-// converged solution by the implicit-function theorem: Utoprim_2d returns the
-// z with primtoU(z) = U, so dz/dU = (dprimtoU/dz)^-1; the isentropic
-// fall-backs replace the energy row by their constraint u = K rho^gam/(gam-1).
-// A zone whose inversion failed keeps its guess (the step's p^n) and U[B]/gdet.
-// The time step is part of the chain: dt^{n+1} = min(ndt, 1.3 dt^n) with
-// ndt = defcon/(1/n1 + 1/n2) and n_d the Courant minimum over the corrector's
-// faces (step_ch.c:126-137, 477-484), so the face that set each minimum gets
-// the adjoint of its wave speed.
+// converged solution by the implicit-function theorem: Utoprim_2d's Newton
+// residuals vanish at the converged (W, v^2), so its adjoint is a transposed
+// 2x2 solve; the isentropic fall-backs replace primtoU's energy row by their
+// constraint u = K rho^gam/(gam-1), an 8x8 solve.  A zone whose inversion
+// failed keeps its guess (the step's p^n) and U[B]/gdet.  The time step is
+// part of the chain: dt^{n+1} = min(ndt, 1.3 dt^n) with ndt = defcon/(1/n1 +
+// 1/n2) and n_d the Courant minimum over the corrector's faces
+// (step_ch.c:126-137, 477-484), so the face that set each minimum gets the
+// adjoint of its wave speed.
 //
-// Every kernel of the reverse sweep reads recorded values only; the values
-// the dual numbers carry are the step's own (the same IEEE operations), so
-// every branch the linearisation takes is the branch the step took.
+// Every kernel of the reverse sweep reads recorded values only.  The values
+// the dual numbers carry, and those the reverse-mode routines recompute, are
+// the step's own (the same IEEE operations), so every branch the
+// linearisation takes is the branch the step took.
 #include <cuda_runtime.h>
 
 #include <cmath>
