@@ -973,7 +973,8 @@ template <int DIR, bool FULL>
 __global__ void __launch_bounds__(128) k_adj_flux(Grid G, const double *__restrict__ pb,
                                                   const double *__restrict__ geo,
                                                   const double *__restrict__ lamF, double *lamp,
-                                                  const DevScalars *sa, AdjScalars *as)
+                                                  const DevScalars *sa, AdjScalars *as,
+                                                  const double *__restrict__ ctrec)
 {
   using D4 = Dual<4>;
   const int side = threadIdx.x & 1, lane = threadIdx.x & 31;
@@ -995,6 +996,9 @@ __global__ void __launch_bounds__(128) k_adj_flux(Grid G, const double *__restri
   const double nmin = FULL ? __longlong_as_double((long long)sa->ndt_bits[DIR - 1]) : 0.;
   const double dxd = DIR == 1 ? G.dx1 : G.dx2;
   if (!any && !(act && lnd != 0.)) return;  // the same for both lanes of the face
+  // a face without flux adjoint matters only if it set the Courant minimum
+  // (its wave speed as the recomputed step kept it)
+  if (FULL && !any && !(G.cour * dxd / ctrec[(DIR - 1) * G.nc + c] == nmin)) return;
   const long o1 = DIR == 1 ? c - 2 * G.sn2 : c - 2, o2 = DIR == 1 ? c - G.sn2 : c - 1,
              o3 = DIR == 1 ? c + G.sn2 : c + 1;
   // limited face states (interp.c:49-93); the derivatives of this lane's side
@@ -1117,7 +1121,7 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
   DevScalars *recs[2];
   for (int b = 0; b < 2; b++) {
     recp[b] = B.get<double>(pl * (nrec + 1));
-    recd[b] = B.get<double>((size_t)nrec * (7 * pl + 2 * nc));
+    recd[b] = B.get<double>((size_t)nrec * (7 * pl + 4 * nc));
     recf[b] = B.get<signed char>((size_t)nrec * 4 * nc);
     recs[b] = B.get<DevScalars>((size_t)nrec * 2);
     if (!recp[b] || !recd[b] || !recf[b] || !recs[b]) return fail_with(HARM_E_CUDA, "device memory for the adjoint");
@@ -1136,11 +1140,11 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
   for (int b = 0; b < 2; b++) {
     rec[b].resize(nrec);
     for (int r = 0; r < nrec; r++) {
-      double *d = recd[b] + (size_t)r * (7 * pl + 2 * nc);
+      double *d = recd[b] + (size_t)r * (7 * pl + 4 * nc);
       StepRec &s = rec[b][r];
       s.X1[0] = d; s.X1[1] = d + pl; s.Ub[0] = d + 2 * pl; s.Ub[1] = d + 3 * pl; s.ph = d + 4 * pl;
       s.Z[0] = d + 5 * pl; s.Z[1] = d + 6 * pl;
-      s.F1rho[0] = d + 7 * pl; s.F1rho[1] = d + 7 * pl + nc;
+      s.F1rho[0] = d + 7 * pl; s.F1rho[1] = d + 7 * pl + nc; s.ctop = d + 7 * pl + 2 * nc;
       s.fl1[0] = recf[b] + (size_t)r * 4 * nc; s.fl1[1] = s.fl1[0] + nc;
       s.wz[0] = s.fl1[0] + 2 * nc; s.wz[1] = s.fl1[0] + 3 * nc;
       s.sc[0] = recs[b] + 2 * r; s.sc[1] = recs[b] + 2 * r + 1;
@@ -1240,8 +1244,8 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       // the two directions run side by side (fs), each adding into the state adjoint
       CK(cudaEventRecord(efork[0], q));
       CK(cudaStreamWaitEvent(fs, efork[0], 0));
-      k_adj_flux<1, true><<<g1, ftile, 0, q>>>(G, R.ph, x->geo, lF1, lh, sa, as);
-      k_adj_flux<2, true><<<g2, ftile, 0, fs>>>(G, R.ph, x->geo, lF2, lh, sa, as);
+      k_adj_flux<1, true><<<g1, ftile, 0, q>>>(G, R.ph, x->geo, lF1, lh, sa, as, R.ctop);
+      k_adj_flux<2, true><<<g2, ftile, 0, fs>>>(G, R.ph, x->geo, lF2, lh, sa, as, R.ctop);
       CK(cudaEventRecord(ejoin[0], fs));
       CK(cudaStreamWaitEvent(q, ejoin[0], 0));
       // predictor, from p^n into ph
@@ -1254,8 +1258,8 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
                                             as);
       CK(cudaEventRecord(efork[1], q));
       CK(cudaStreamWaitEvent(fs, efork[1], 0));
-      k_adj_flux<1, false><<<g1, ftile, 0, q>>>(G, pn, x->geo, lF1, lcur, sa, as);
-      k_adj_flux<2, false><<<g2, ftile, 0, fs>>>(G, pn, x->geo, lF2, lcur, sa, as);
+      k_adj_flux<1, false><<<g1, ftile, 0, q>>>(G, pn, x->geo, lF1, lcur, sa, as, nullptr);
+      k_adj_flux<2, false><<<g2, ftile, 0, fs>>>(G, pn, x->geo, lF2, lcur, sa, as, nullptr);
       CK(cudaEventRecord(ejoin[1], fs));
       CK(cudaStreamWaitEvent(q, ejoin[1], 0));
       k_adj_dt_post<<<1, 1, 0, q>>>(sa, sb, as);

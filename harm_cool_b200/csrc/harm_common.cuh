@@ -170,6 +170,7 @@ struct StepRec {
   double *Z[2];                  // the inversion's output before fixup()
   signed char *wz[2];            // which inversion gave it: 0 Utoprim_2d, 1 and 2 the fall-backs, -1 none [nc]
   double *F1rho[2];              // raw radial mass flux [nc] (the no-inflow fix reads its sign)
+  double *ctop;                  // the corrector's face wave speeds, directions 1 and 2 [2][nc]
   signed char *fl1[2];           // pflag after the first bound_prim [nc]
   double *ph;                    // the predictor's final state
   DevScalars *sc[2];             // the run state before k_finalize (the corrector's Courant minima) and after

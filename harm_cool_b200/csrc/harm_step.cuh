@@ -58,10 +58,12 @@ using flux_t = double;
 // i in [istart, istop+1], j in [jstart-1, jstop+1]; dir 2 i in [istart-1,
 // istop+1], j in [jstart, jstop+1] (the polar faces jstart and jstop+1 carry
 // no flux, :412-416); dir 3 i in [istart-1, istop+1], j in [jstart-1, jstop+1].
-template <int DIR, bool FULL>
+// REC (the discrete adjoint's recomputation): also keep the wave speed of every
+// face that takes part in the Courant minimum, in ctrec[(DIR - 1) nc + cell].
+template <int DIR, bool FULL, bool REC = false>
 __global__ void __launch_bounds__(128, HARM_FLUX_MINB) k_flux(Grid G, const double *__restrict__ pb, flux_t *__restrict__ F,
                                               const double *__restrict__ geo, const float *__restrict__ geo32,
-                                              DevScalars *sc)
+                                              DevScalars *sc, double *__restrict__ ctrec)
 {
   if (sc->halted) return;
   const int j = (DIR == 2 ? G.jstart : G.jstart - 1) + blockIdx.x * blockDim.x + threadIdx.x;
@@ -119,6 +121,7 @@ __global__ void __launch_bounds__(128, HARM_FLUX_MINB) k_flux(Grid G, const doub
       if (FULL && i >= G.istart && i <= G.istop && j >= G.jstart && j <= G.jstop) {
         const double dxd = DIR == 1 ? G.dx1 : DIR == 2 ? G.dx2 : G.dx3;
         dtmin = fmin(dtmin, G.cour * dxd / ctop);
+        if (REC) ctrec[(DIR - 1) * G.nc + c] = ctop;
       }
     }
   }
@@ -135,17 +138,26 @@ __global__ void __launch_bounds__(128, HARM_FLUX_MINB) k_flux(Grid G, const doub
   }
 }
 
+// ctrec (the adjoint's recomputation of a corrector, 2D): keep the faces'
+// wave speeds there
 template <bool FULL>
 void launch_flux(const Grid &G, dim3 b, cudaStream_t st, const double *pb, flux_t *F1, flux_t *F2, flux_t *F3,
-                 const double *geo, const float *geo32, DevScalars *sc)
+                 const double *geo, const float *geo32, DevScalars *sc, double *ctrec = nullptr)
 {
   const int gz = (G.n3 + HARM_HB_FLUX - 1) / HARM_HB_FLUX;
   dim3 g1((G.n2 + 2 + b.x - 1) / b.x, (G.n1 + 1 + b.y - 1) / b.y, gz);
   dim3 g2((G.n2 + 1 + b.x - 1) / b.x, (G.n1 + 2 + b.y - 1) / b.y, gz);
   dim3 g3((G.n2 + 2 + b.x - 1) / b.x, (G.n1 + 2 + b.y - 1) / b.y, gz);
-  k_flux<1, FULL><<<g1, b, 0, st>>>(G, pb, F1, geo, geo32, sc);
-  k_flux<2, FULL><<<g2, b, 0, st>>>(G, pb, F2, geo, geo32, sc);
-  if (G.n3 > 1) k_flux<3, FULL><<<g3, b, 0, st>>>(G, pb, F3, geo, geo32, sc);
+#if !HARM_STEP_MIXED
+  if (FULL && ctrec) {
+    k_flux<1, true, true><<<g1, b, 0, st>>>(G, pb, F1, geo, geo32, sc, ctrec);
+    k_flux<2, true, true><<<g2, b, 0, st>>>(G, pb, F2, geo, geo32, sc, ctrec);
+    return;
+  }
+#endif
+  k_flux<1, FULL><<<g1, b, 0, st>>>(G, pb, F1, geo, geo32, sc, nullptr);
+  k_flux<2, FULL><<<g2, b, 0, st>>>(G, pb, F2, geo, geo32, sc, nullptr);
+  if (G.n3 > 1) k_flux<3, FULL><<<g3, b, 0, st>>>(G, pb, F3, geo, geo32, sc, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -542,7 +554,8 @@ static void launch_half_rec(Ctx *x, const double *pi, const double *pb, double *
   const int s = FULL ? 1 : 0;
   const size_t nc = (size_t)x->G.nc;
   Bufs B = bufs(x);
-  launch_flux<FULL>(x->G, dim3(x->tbx, x->tby), x->stream, pb, B.F1, B.F2, B.F3, x->geo, x->geo32, x->sc);
+  launch_flux<FULL>(x->G, dim3(x->tbx, x->tby), x->stream, pb, B.F1, B.F2, B.F3, x->geo, x->geo32, x->sc,
+                    FULL ? r.ctop : nullptr);
   cudaMemcpyAsync(r.F1rho[s], B.F1 + RHO * nc, nc * sizeof(double), cudaMemcpyDeviceToDevice, x->stream);
   launch_update<FULL>(x, pi, pb, pf, r.Z[s], r.wz[s]);
   cudaMemcpyAsync(r.Ub[s], x->Ubuf, 8 * nc * sizeof(double), cudaMemcpyDeviceToDevice, x->stream);
