@@ -201,6 +201,42 @@ def measured_traffic(kernel, zones):
     return d[kernel]["bytes_per_zone"] * zones
 
 
+def fp64_counts():
+    """FP64 pipe instructions per zone of each launch group (flux, update) and per
+    zone-cycle, from the committed ncu capture of the step kernels."""
+    path = os.path.join(ROOT, "profiles", "fp64_inst_per_zone.json")
+    if not os.path.exists(path):
+        return None
+    return json.load(open(path))
+
+
+def fp64_roofline(hc, local, kms, zones, dom, ms_step):
+    """The FP64-pipe roofline of the dominant launch group and of the whole step:
+    FP64 thread instructions (DADD, DMUL, DFMA; the step is built without FMA
+    contraction, so its arithmetic issues as separate DADD and DMUL) per second
+    against the device's measured FP64 instruction rate, and the step's
+    zone-cycles/s ceiling at that rate."""
+    counts = fp64_counts()
+    peaks = hc.fp64_peak(local)
+    peak = min(peaks["dfma_inst_per_s"], peaks["dadd_inst_per_s"], peaks["dmul_inst_per_s"])
+    out = {"peak_inst_per_s": peak, "peak_dfma_flop_per_s": 2 * peaks["dfma_inst_per_s"],
+           "measured_rates": peaks, "peak_source": "measured live (harm_fp64_peak)"}
+    if counts is None:
+        return out
+    g = counts["groups"][dom]
+    inst = g["fp64_inst_per_zone"] * zones
+    flop = g["fp64_flop_per_zone"] * zones
+    t = kms[dom] / 1e3
+    per_cycle = counts["step"]["fp64_inst_per_zone_cycle"]
+    out.update({"kernel": dom, "achieved_inst_per_s": inst / t, "fp64_frac": inst / t / peak,
+                "achieved_flop_per_s": flop / t,
+                "step_frac": per_cycle * zones / (ms_step / 1e3) / peak,
+                "fp64_inst_per_zone_cycle": per_cycle,
+                "fp64_ceiling_zcps": peak / per_cycle,
+                "counts_source": counts["source"]})
+    return out
+
+
 def l1_errors(pa, pb):
     """L1 of (pb - pa) over the active zones relative to the L1 of pa: for rho and
     u, and for the velocity (u1..u3) and field (B1..B3) vectors as wholes, since a
@@ -227,6 +263,28 @@ def timed_run(hc, pr, local, world, steps, warmup, mixed):
     clocks = sampler.stop()
     barrier(world)
     return ctx, reduce_max(ms, world, local), clocks
+
+
+def mixed_l1_leg(hc, pr, local, nsteps, act):
+    """The mixed path's accuracy contract on the benchmark torus: both paths
+    advance nsteps from the same initial state; L1 of the mixed state against
+    the FP64 state, with the device time of each run (dt ramp included)."""
+    out = {}
+    states = {}
+    for name, mixed in (("fp64", False), ("mixed", True)):
+        c = hc.Context(pr, device=local)
+        c.init_torus()
+        if mixed:
+            c.set_precision(hc.Context.MIXED)
+        ms = c.run_timed(nsteps)
+        states[name] = c.get_prims()[act]
+        out["ms_per_step_%s_%d_steps" % (name, nsteps)] = ms / nsteps
+        out["fail_code_%s_%d_steps" % (name, nsteps)] = c.diag()["fail_code"]
+        c.close()
+    out["l1_vs_fp64"] = l1_errors(states["fp64"], states["mixed"])
+    out["l1_after_steps"] = nsteps
+    out["l1_bound_rho"] = 1e-4
+    return out
 
 
 def run_ours(args, world, rank, local):
@@ -270,16 +328,21 @@ def run_ours(args, world, rank, local):
                          "algorithmic_bytes": alg, "peak_source": peak_kind,
                          "step_frac": zones * STATE_BYTES_PER_ZONE_CYCLE / (ms / args.steps / 1e3) / 1e9 / peak},
             "kernel_ms": kms, "clocks": clocks, "sim_time": ctx.time(), "fail_code": d["fail_code"]}
+    line["roofline"]["fp64"] = fp64_roofline(hc, local, kms, zones, dom, ms / args.steps)
+    act = (slice(1, -1) if args.n3 > 1 else slice(None), slice(2, -2), slice(2, -2))
     if not args.no_mixed:
         ctx.close()
         ctxm, msm, clocksm = timed_run(hc, pr, local, world, args.steps, args.warmup, mixed=True)
         pb = ctxm.get_prims()
-        act = (slice(1, -1) if args.n3 > 1 else slice(None), slice(2, -2), slice(2, -2))
         line["mixed"] = {"value": zones * args.steps * world / (msm / 1e3), "ms_per_step": msm / args.steps,
                          "speedup_vs_fp64": ms / msm, "clocks": clocksm,
-                         "l1_vs_fp64": l1_errors(pa[act], pb[act]), "l1_after_steps": args.warmup + args.steps,
+                         "l1_vs_fp64_timed_run": l1_errors(pa[act], pb[act]),
+                         "timed_run_steps": args.warmup + args.steps,
                          "kernel_ms": ctxm.time_kernels(reps=3), "fail_code": ctxm.diag()["fail_code"]}
         ctxm.close()
+        del pa, pb
+        if args.l1_steps > 0:
+            line["mixed"].update(mixed_l1_leg(hc, pr, local, args.l1_steps, act))
     else:
         ctx.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -558,6 +621,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
+    ap.add_argument("--l1-steps", type=int, default=1000,
+                    help="steps of the FP64 and mixed runs whose L1 difference the mixed line reports (0: skip)")
     ap.add_argument("--workload", choices=("torus", "ensemble", "cool", "adjoint"), default="torus",
                     help="torus: the 288x256x256 step (default); ensemble: 64 seeded 2D tori; "
                          "cool: the 256x256 COOL_EOS step")

@@ -21,7 +21,8 @@ __all__ = ["HarmError", "Params", "GridSpec", "TorusSpec", "Diag", "Problem", "C
 
 NPR, NPG = 8, 5
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libharm_b200.so")
+# HARM_B200_LIB names another build of the library (a variant built for comparison)
+LIB_PATH = os.environ.get("HARM_B200_LIB") or os.path.join(HERE, "libharm_b200.so")
 
 
 class HarmError(RuntimeError):
@@ -167,6 +168,9 @@ _SIGNATURES = {
                                        ctypes.c_char_p]),
     "harm_get_eos_guess": (ctypes.c_int, [ctypes.c_void_p, _DP]),
     "harm_put_eos_guess": (ctypes.c_int, [ctypes.c_void_p, _DP]),
+    "harm_fp64_peak": (ctypes.c_int, [ctypes.c_int, _DP]),
+    "harm_div_check": (ctypes.c_int, [ctypes.c_int, ctypes.c_long, ctypes.c_ulonglong,
+                                      ctypes.POINTER(ctypes.c_ulonglong)]),
 }
 
 
@@ -183,6 +187,23 @@ def library():
             fn.argtypes = args
         _lib = lib
     return _lib
+
+
+def fp64_peak(device=0):
+    """Measured FP64 pipe rates of the device: DFMA, DADD and DMUL thread
+    instructions per second, IEEE divisions and reciprocals per second."""
+    out = np.zeros(5)
+    _check(library().harm_fp64_peak(device, _dp(out)))
+    return {"dfma_inst_per_s": out[0], "dadd_inst_per_s": out[1], "dmul_inst_per_s": out[2],
+            "ddiv_per_s": out[3], "drcp_per_s": out[4]}
+
+
+def div_check(n, seed=1, device=0):
+    """The library's shared-divisor division against IEEE division on the device:
+    (samples that differ, near-midpoint samples drawn)."""
+    c = (ctypes.c_ulonglong * 2)()
+    _check(library().harm_div_check(device, n, seed, c))
+    return int(c[0]), int(c[1])
 
 
 def _check(rc):

@@ -23,6 +23,21 @@ def _sources():
         os.path.join(ROOT, "include", "harm_b200.h")]
 
 
+def _includes(path, seen=None):
+    """The file and every local header it includes, transitively."""
+    import re
+    seen = set() if seen is None else seen
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    for name in re.findall(r'^#include "([^"]+)"', open(path).read(), re.M):
+        for d in (CSRC, os.path.join(ROOT, "include")):
+            if os.path.exists(os.path.join(d, name)):
+                _includes(os.path.join(d, name), seen)
+                break
+    return seen
+
+
 def _run(cmd):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -43,6 +58,7 @@ UNITS = {
     "harm_cool.cu": ["-fmad=false"],     # the COOL_EOS step and Utoprim_5d
     "harm_dump.cu": ["-fmad=false"],     # the ASCII dump format
     "harm_adjoint.cu": ["-fmad=false"],  # the discrete adjoint (values identical to the step's)
+    "harm_peak.cu": ["-fmad=false"],     # measured FP64 pipe rates (roofline denominators)
 }
 
 
@@ -58,14 +74,13 @@ def build(force=False, verbose=False):
           os.path.join(CSRC, "host_setup.cpp"), "-o", host_o] + inc)
     objs = [host_o]
 
-    # a unit is recompiled when its object is older than the unit or any header
-    headers = max(os.path.getmtime(f) for f in _sources() if not f.endswith((".cu", ".cpp")))
-
+    # a unit is recompiled when its object is older than the unit or any header it includes
     def compile_unit(item):
         unit, flags = item
         o = os.path.join(BUILD, unit.replace(".cu", ".o"))
         src = os.path.join(CSRC, unit)
-        if not force and os.path.exists(o) and os.path.getmtime(o) >= max(os.path.getmtime(src), headers):
+        newest = max(os.path.getmtime(f) for f in _includes(src))
+        if not force and os.path.exists(o) and os.path.getmtime(o) >= newest:
             return o, ""
         out = _run([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xptxas", "-v", "-Xcompiler", "-fPIC",
                                     "-Xcompiler", "-ffp-contract=off", "-c", os.path.join(CSRC, unit),

@@ -427,6 +427,8 @@ __global__ void k_utoprim_batch(const double *U, const double *gcov, const doubl
   q.n30 = b[12]; q.n31 = b[13]; q.n33 = b[15];
   q.alpha = 1. / sqrt(-q.n00);
   q.g = gdet[t];
+  q.ialpha = 1. / q.alpha;
+  q.ig = 1. / q.g;
   double u[8], p[8];
   for (int k = 0; k < 8; k++) { u[k] = U[t * 8 + k]; p[k] = prim[t * 8 + k]; }
   ret[t] = utoprim<0>(gam, 0., u, q, p);
@@ -582,6 +584,7 @@ extern "C" int harm_create(const harm_params *prm, const double *gcov, const dou
   G.lim = prm->lim;
   G.gam = prm->gam; G.cour = prm->cour; G.defcon = prm->defcon; G.tf = prm->tf;
   G.dx1 = prm->dx[1]; G.dx2 = prm->dx[2]; G.dx3 = prm->dx[3];
+  G.idx1 = 1. / G.dx1; G.idx2 = 1. / G.dx2; G.idx3 = 1. / G.dx3;
   // the mixed path keeps the connection source in FP64 within 2 r_H of the
   // black hole (r from the Boyer-Lindquist coordinates of the zone centres)
   {
@@ -622,9 +625,10 @@ extern "C" int harm_create(const harm_params *prm, const double *gcov, const dou
   for (int L = 0; L < 4; L++)
     for (long c = 0; c < G.ng; c++) {
       const double *a = gcov + (c * 5 + locs[L]) * 16, *b = gcon + (c * 5 + locs[L]) * 16;
+      const double alpha = 1. / sqrt(-b[0]), g = gdet[c * 5 + locs[L]];
       const double vals[GEO_N] = {a[0], a[1], a[3], a[5], a[7], a[10], a[15],
                                   b[0], b[1], b[3], b[4], b[5], b[7], b[10], b[12], b[13], b[15],
-                                  gdet[c * 5 + locs[L]], 1. / sqrt(-b[0])};
+                                  g, alpha, 1. / alpha, 1. / g};
       for (int e = 0; e < GEO_N; e++) hg[((size_t)L * GEO_N + e) * G.ng + c] = vals[e];
     }
   for (long c = 0; c < G.ng; c++)

@@ -39,6 +39,7 @@ struct Grid {
   int lim;
   double gam, cour, defcon, tf;
   double dx1, dx2, dx3;
+  double idx1, idx2, idx3;  // 1/dx rounded to nearest: the divisors of div_rn in the flux divergence
   int isrc32;  // mixed path: first radial index whose connection source runs in float (r >= 2 r_H)
 };
 

@@ -279,9 +279,10 @@ __global__ void __launch_bounds__(128, HARM_COOL_CONS_MINB) k_cons_cool(Grid G, 
 #pragma unroll
     for (int k = 0; k < 8; k++) {
       if (THREE_D)
-        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 - (f3p[k] - f3m[k]) / G.dx3 + dU[k]);
+        U[k] += Dt * (-div_rn(f1p[k] - f1m[k], G.dx1, G.idx1) - div_rn(f2p[k] - f2m[k], G.dx2, G.idx2)
+                      - div_rn(f3p[k] - f3m[k], G.dx3, G.idx3) + dU[k]);
       else
-        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 + dU[k]);
+        U[k] += Dt * (-div_rn(f1p[k] - f1m[k], G.dx1, G.idx1) - div_rn(f2p[k] - f2m[k], G.dx2, G.idx2) + dU[k]);
     }
   }
 #pragma unroll
@@ -387,6 +388,8 @@ __global__ void k_utoprim_5d_batch(EosDev E, const double *U, const double *gcov
   q.n30 = b[12]; q.n31 = b[13]; q.n33 = b[15];
   q.alpha = 1. / sqrt(-q.n00);
   q.g = gdet[t];
+  q.ialpha = 1. / q.alpha;
+  q.ig = 1. / q.g;
   double u[8], p[8];
   for (int k = 0; k < 8; k++) { u[k] = U[t * 8 + k]; p[k] = prim[t * 8 + k]; }
   EosCursor c = eos_cursor(tab[t], lastT[t]);

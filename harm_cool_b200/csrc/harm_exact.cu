@@ -6,7 +6,7 @@
 #define HARM_FLUX_MINB 7   // 72 registers
 #endif
 #ifndef HARM_CONS_MINB
-#define HARM_CONS_MINB 4   // 128 registers
+#define HARM_CONS_MINB 5   // 102 registers
 #endif
 #ifndef HARM_INV_MINB
 #define HARM_INV_MINB 5    // 102 registers

@@ -77,6 +77,8 @@ __global__ void k_utoprim_batch_fixed(double *S, long n, double gam)
   q.n30 = b[12]; q.n31 = b[13]; q.n33 = b[15];
   q.alpha = 1. / sqrt(-q.n00);
   q.g = S[kOffDet + t];
+  q.ialpha = 1. / q.alpha;
+  q.ig = 1. / q.g;
   double u[8], p[8];
   for (int k = 0; k < 8; k++) { u[k] = S[kOffU + t * 8 + k]; p[k] = S[kOffPrim + t * 8 + k]; }
   reinterpret_cast<int *>(S + kOffRet)[t] = utoprim<0>(gam, 0., u, q, p);

@@ -36,8 +36,76 @@ struct Geo {
   double n00, n01, n03, n10, n11, n13, n22, n30, n31, n33;       // gcon
   double g;                                                      // sqrt(-det g)
   double alpha;  // 1/sqrt(-g^tt), as ucon_calc and the inversion form it (phys.c:238)
+  double ialpha; // 1/alpha rounded to nearest: the divisor of div_rn for alpha
+  double ig;     // 1/g rounded to nearest (zone centres; where g = 0 it is not used)
 };
-constexpr int GEO_N = 19;
+constexpr int GEO_N = 21;
+
+// ---------------------------------------------------------------------------
+// Division by a divisor that many divisions share.
+//
+// The step divides by the same few numbers again and again: the lapse alpha
+// (ucon_calc), sqrt(-g) (the inversion's rescaling), the cell widths (the flux
+// divergence), the adiabatic index (the Noble pressure), u^t (bcon_calc).  An
+// IEEE double division costs about 14 FP64 issue slots on sm_100; with
+// y = 1/b rounded to nearest formed once, div_rn returns the same correctly
+// rounded quotient in 6:
+//  * q = a y is within two ulps of a/b, and one FMA correction
+//    q + (a - b q) y (Markstein, IBM J. Res. Dev. 34:111-119, 1990) brings it
+//    within one ulp: q is then a faithful quotient;
+//  * for a faithful q the remainder r = a - b q is a double, so fma(-q, b, a)
+//    forms it exactly (Boldo and Daumas, ARITH-16, 2003);
+//  * a/b = q + r/b, so q is the nearest double to a/b exactly when |r| is
+//    below b times half the gap between q and its neighbour on the side of a/b
+//    (a power of two, so that product is exact); otherwise the neighbour is.
+//    a/b is never halfway between two doubles, so there is no tie.
+// y must be RN(1/b).  Divisors other than b > 0 in [2^-60, 2^61), and
+// numerators outside [2^-800, 2^800] in magnitude (subnormal, huge, inf, NaN),
+// take the IEEE division; a zero numerator gives a y, the signed zero a/b is.
+__device__ __forceinline__ double div_rn(double a, double b, double y)
+{
+  const long long ia = __double_as_longlong(a);
+  const unsigned ea = (unsigned)(ia >> 52) & 0x7ffu;
+  const unsigned eb = (unsigned)(__double_as_longlong(b) >> 52) & 0xfffu;  // sign bit included
+  const bool okb = eb - 963u <= 120u;                                      // b > 0, 2^-60 <= b < 2^61
+  if (!okb || ea - 223u > 1600u) return (okb && (ia << 1) == 0) ? a * y : a / b;
+  double q = a * y;
+  double r = fma(-q, b, a);
+  q = fma(r, y, q);
+  r = fma(-q, b, a);
+  long long iq = __double_as_longlong(q);
+  const bool up = (r > 0.) == (q > 0.);                     // |a/b| > |q|
+  const int eq = (int)((iq >> 52) & 0x7ff);
+  // half the gap to the neighbour towards a/b: a quarter ulp below a power of two
+  const int eh = eq - 53 - ((!up && (iq & 0xfffffffffffffLL) == 0) ? 1 : 0);
+  const double hb = __longlong_as_double((long long)eh << 52) * b;
+  if (fabs(r) > hb) {
+    iq += up ? 1 : -1;
+    q = __longlong_as_double(iq);
+  }
+  return q;
+}
+
+// div_rn for a divisor formed at run time: its reciprocal is one IEEE division,
+// worth it from two quotients on; divisors outside [2^-60, 2^60] divide directly
+__device__ __forceinline__ bool div_rn_ok(double b)
+{
+  const unsigned eb = (unsigned)(__double_as_longlong(b) >> 52) & 0xfffu;  // sign bit included
+  return eb - 963u <= 120u;                                                 // b > 0, 2^-60 <= b < 2^61
+}
+
+// a/b for the step's scalar type: div_rn for double, plain division for the
+// adjoint's dual numbers (whose value part is the same correctly rounded quotient)
+template <class R>
+__device__ __forceinline__ R div_by(const R &a, double b, double y)
+{
+  return a / b;
+}
+template <>
+__device__ __forceinline__ double div_by<double>(const double &a, double b, double y)
+{
+  return div_rn(a, b, y);
+}
 
 // geometry planes: [GEO_N][ng], entry e of point gi at G[e*ng + gi]
 __device__ __forceinline__ void load_geo(const double *__restrict__ G, long ng, long gi, Geo &q)
@@ -50,6 +118,8 @@ __device__ __forceinline__ void load_geo(const double *__restrict__ G, long ng, 
   q.n22 = __ldg(G + 13 * ng + gi); q.n30 = __ldg(G + 14 * ng + gi); q.n31 = __ldg(G + 15 * ng + gi);
   q.n33 = __ldg(G + 16 * ng + gi); q.g = __ldg(G + 17 * ng + gi);
   q.alpha = __ldg(G + 18 * ng + gi);
+  q.ialpha = __ldg(G + 19 * ng + gi);
+  q.ig = __ldg(G + 20 * ng + gi);
 }
 
 // The routines below that the discrete adjoint linearises are templates on
@@ -97,13 +167,16 @@ template <class R>
 __device__ __forceinline__ void ucon_calc(const R *pr, const Geo &q, R *ucon, int *fail)
 {
   const double alpha = q.alpha;
-  double b1 = q.n01 * alpha * alpha, b2 = 0. * alpha * alpha, b3 = q.n03 * alpha * alpha;
+  double b1 = q.n01 * alpha * alpha, b3 = q.n03 * alpha * alpha;
   R gamma;
   if (gamma_calc(pr, q, gamma)) *fail = FAIL_GAMMA;
-  ucon[0] = gamma / alpha;
-  ucon[1] = pr[U1] - gamma * b1 / alpha;
-  ucon[2] = pr[U2] - gamma * b2 / alpha;
-  ucon[3] = pr[U3] - gamma * b3 / alpha;
+  ucon[0] = div_by(gamma, alpha, q.ialpha);
+  ucon[1] = pr[U1] - div_by(gamma * b1, alpha, q.ialpha);
+  // the reference's pr[U2] - gamma * b2 / alpha with b2 = g^{t theta} alpha^2 = 0*alpha*alpha:
+  // gamma * (+0) / alpha is +0 for finite gamma and NaN otherwise, and so is
+  // gamma - gamma, which takes two operations instead of a division
+  ucon[2] = pr[U2] - (gamma - gamma);
+  ucon[3] = pr[U3] - div_by(gamma * b3, alpha, q.ialpha);
 }
 
 // bcon_calc() (phys.c:108-117)
@@ -114,6 +187,24 @@ __device__ __forceinline__ void bcon_calc(const R *pr, const R *ucon, const R *u
   bcon[1] = (pr[B1] + bcon[0] * ucon[1]) / ucon[0];
   bcon[2] = (pr[B2] + bcon[0] * ucon[2]) / ucon[0];
   bcon[3] = (pr[B3] + bcon[0] * ucon[3]) / ucon[0];
+}
+// the double form: three quotients by u^t share one reciprocal
+template <>
+__device__ __forceinline__ void bcon_calc<double>(const double *pr, const double *ucon, const double *ucov,
+                                                  double *bcon)
+{
+  bcon[0] = pr[B1] * ucov[1] + pr[B2] * ucov[2] + pr[B3] * ucov[3];
+  const double u0 = ucon[0];
+  if (div_rn_ok(u0)) {
+    const double y = 1. / u0;
+    bcon[1] = div_rn(pr[B1] + bcon[0] * ucon[1], u0, y);
+    bcon[2] = div_rn(pr[B2] + bcon[0] * ucon[2], u0, y);
+    bcon[3] = div_rn(pr[B3] + bcon[0] * ucon[3], u0, y);
+  } else {
+    bcon[1] = (pr[B1] + bcon[0] * ucon[1]) / u0;
+    bcon[2] = (pr[B2] + bcon[0] * ucon[2]) / u0;
+    bcon[3] = (pr[B3] + bcon[0] * ucon[3]) / u0;
+  }
 }
 
 // get_state() (phys.c:219-229)
@@ -309,7 +400,7 @@ __device__ __forceinline__ R slope_lim(int lim, R y1, R y2, R y3)
 // conserved -> primitive (utoprim_2d.c, utoprim_1dvsq2fix1.c, utoprim_1dfix1.c)
 
 struct U2P {
-  double gam, Bsq, QdotBsq, Qtsq, Qdotn, D, K_atm;
+  double gam, igam, Bsq, QdotBsq, Qtsq, Qdotn, D, K_atm;
   double W_for_gnr2, rho_for_gnr2;
 };
 
@@ -364,9 +455,9 @@ __device__ __forceinline__ void func_vsq(const U2P &c, const double *x, double *
   const double GAMMA = c.gam, Bsq = c.Bsq, QdotBsq = c.QdotBsq, Qtsq = c.Qtsq, Qdotn = c.Qdotn, D = c.D;
   double W = x[0], vsq = x[1], Wsq = W * W;
   double gtmp = 1. - vsq;
-  double p_tmp = (GAMMA - 1.) * (W * gtmp - D * sqrt(gtmp)) / GAMMA;
-  double dPdW = (GAMMA - 1.) * (1. - vsq) / GAMMA;
-  double dPdvsq = (GAMMA - 1.) * (0.5 * D / sqrt(1. - vsq) - W) / GAMMA;
+  double p_tmp = div_rn((GAMMA - 1.) * (W * gtmp - D * sqrt(gtmp)), GAMMA, c.igam);
+  double dPdW = div_rn((GAMMA - 1.) * (1. - vsq), GAMMA, c.igam);
+  double dPdvsq = div_rn((GAMMA - 1.) * (0.5 * D / sqrt(1. - vsq) - W), GAMMA, c.igam);
   double t2 = -0.5 * Bsq + dPdvsq;
   double t3 = Bsq + W;
   double t4 = t3 * t3;
@@ -470,7 +561,7 @@ __device__ __forceinline__ int u2p_body_2d(U2P &c, const double *U, const Geo &q
   gamma = 1. / gtmp;
   rho0 = c.D * gtmp;
   w = W * (1. - vsq);
-  p = (c.gam - 1.) * (w - rho0) / c.gam;
+  p = div_rn((c.gam - 1.) * (w - rho0), c.gam, c.igam);
   u = w - (rho0 + p);
   if ((rho0 <= 0.) || (u <= 0.)) return 5;
   prim[RHO] = rho0;
@@ -679,21 +770,22 @@ template <int which, bool MIXED = false>
 __device__ __forceinline__ int utoprim(double gam, double K, const double *U, const Geo &q, double *prim)
 {
   double Ut[8], pt[8];
-  prim[B1] = U[B1] / q.g;
-  prim[B2] = U[B2] / q.g;
-  prim[B3] = U[B3] / q.g;
+  prim[B1] = div_rn(U[B1], q.g, q.ig);
+  prim[B2] = div_rn(U[B2], q.g, q.ig);
+  prim[B3] = div_rn(U[B3], q.g, q.ig);
   if (U[0] <= 0.) return -100;
   const double alpha = q.alpha;
-  Ut[RHO] = alpha * U[RHO] / q.g;
-  Ut[UU] = alpha * (U[UU] - U[RHO]) / q.g;
+  Ut[RHO] = div_rn(alpha * U[RHO], q.g, q.ig);
+  Ut[UU] = div_rn(alpha * (U[UU] - U[RHO]), q.g, q.ig);
 #pragma unroll
-  for (int i = U1; i <= B3; i++) Ut[i] = alpha * U[i] / q.g;
+  for (int i = U1; i <= B3; i++) Ut[i] = div_rn(alpha * U[i], q.g, q.ig);
 #pragma unroll
   for (int i = 0; i < B1; i++) pt[i] = prim[i];
 #pragma unroll
   for (int i = B1; i <= B3; i++) pt[i] = alpha * prim[i];
   U2P c;
   c.gam = gam;
+  c.igam = 1. / gam;
   c.K_atm = K;
   int ret;
   if (which == 0) ret = u2p_body_2d<MIXED>(c, Ut, q, pt);

@@ -54,6 +54,12 @@ using flux_t = double;
 #endif
 
 
+// faces of direction DIR per theta row and rows per phi plane (step_ch.c:407)
+template <int DIR>
+__host__ __device__ __forceinline__ int faces_per_row(const Grid &G) { return DIR == 2 ? G.n2 + 1 : G.n2 + 2; }
+template <int DIR>
+__host__ __device__ __forceinline__ int face_rows(const Grid &G) { return DIR == 1 ? G.n1 + 1 : G.n1 + 2; }
+
 // One thread per face of direction DIR.  Face ranges (step_ch.c:407): dir 1
 // i in [istart, istop+1], j in [jstart-1, jstop+1]; dir 2 i in [istart-1,
 // istop+1], j in [jstart, jstop+1] (the polar faces jstart and jstop+1 carry
@@ -66,11 +72,15 @@ __global__ void __launch_bounds__(128, HARM_FLUX_MINB) k_flux(Grid G, const doub
                                               DevScalars *sc, double *__restrict__ ctrec)
 {
   if (sc->halted) return;
-  const int j = (DIR == 2 ? G.jstart : G.jstart - 1) + blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = (DIR == 1 ? G.istart : G.istart - 1) + blockIdx.y * blockDim.y + threadIdx.y;
+  // faces of one phi plane numbered row by row (theta fastest), 128 per block,
+  // so that only the plane's last warp has idle lanes
+  const int nj = faces_per_row<DIR>(G);
+  const int f = blockIdx.x * 128 + threadIdx.y * blockDim.x + threadIdx.x;
+  const int j = (DIR == 2 ? G.jstart : G.jstart - 1) + f % nj;
+  const int i = (DIR == 1 ? G.istart : G.istart - 1) + f / nj;
   const int h0 = blockIdx.z * HARM_HB_FLUX, h1 = min(G.n3, h0 + HARM_HB_FLUX);
   double dtmin = 1.e9;
-  const bool in = (i <= G.istop + 1) && (j <= G.jstop + 1);
+  const bool in = i <= G.istop + 1;
   if (in) for (int h = h0; h < h1; h++) {
     const long c = cidx(G, h, i, j);
     if (DIR == 2 && (j == G.jstart || j == G.jstop + 1)) {
@@ -138,6 +148,7 @@ __global__ void __launch_bounds__(128, HARM_FLUX_MINB) k_flux(Grid G, const doub
   }
 }
 
+
 // ctrec (the adjoint's recomputation of a corrector, 2D): keep the faces'
 // wave speeds there
 template <bool FULL>
@@ -145,9 +156,10 @@ void launch_flux(const Grid &G, dim3 b, cudaStream_t st, const double *pb, flux_
                  const double *geo, const float *geo32, DevScalars *sc, double *ctrec = nullptr)
 {
   const int gz = (G.n3 + HARM_HB_FLUX - 1) / HARM_HB_FLUX;
-  dim3 g1((G.n2 + 2 + b.x - 1) / b.x, (G.n1 + 1 + b.y - 1) / b.y, gz);
-  dim3 g2((G.n2 + 1 + b.x - 1) / b.x, (G.n1 + 2 + b.y - 1) / b.y, gz);
-  dim3 g3((G.n2 + 2 + b.x - 1) / b.x, (G.n1 + 2 + b.y - 1) / b.y, gz);
+  // 128 faces per block whatever the tile's shape
+  dim3 g1((faces_per_row<1>(G) * face_rows<1>(G) + 127) / 128, 1, gz);
+  dim3 g2((faces_per_row<2>(G) * face_rows<2>(G) + 127) / 128, 1, gz);
+  dim3 g3((faces_per_row<3>(G) * face_rows<3>(G) + 127) / 128, 1, gz);
 #if !HARM_STEP_MIXED
   if (FULL && ctrec) {
     k_flux<1, true, true><<<g1, b, 0, st>>>(G, pb, F1, geo, geo32, sc, ctrec);
@@ -261,6 +273,65 @@ __device__ void zone_fluxes(const Flux &FX, int h, int i, int j, double *f1m, do
   }
 }
 
+#ifndef HARM_CONS_V2
+#define HARM_CONS_V2 1
+#endif
+
+// The flux divergence of the update (step_ch.c:247-263) one conserved
+// component at a time, U[k] += Dt (-dF1/dx1 - dF2/dx2 [- dF3/dx3] + dU[k]), with
+// the same face fluxes zone_fluxes forms (the no-inflow mass-flux fix, and the
+// field components rebuilt from the corner EMFs of flux_ct), so only one
+// component's six face values are live at a time.
+template <bool THREE_D>
+__device__ __forceinline__ void flux_update(const Flux &FX, int h, int i, int j, double Dt, const double *dU, double *U)
+{
+  const Grid &G = FX.G;
+  const int hp = THREE_D ? hwrap(G, h + 1) : 0;
+  auto upd = [&](int k, double f1m, double f1p, double f2m, double f2p, double f3m, double f3p) {
+#if HARM_STEP_MIXED
+    const double idx1 = 1. / G.dx1, idx2 = 1. / G.dx2, idx3 = 1. / G.dx3;
+    if (THREE_D)
+      U[k] += Dt * (-(f1p - f1m) * idx1 - (f2p - f2m) * idx2 - (f3p - f3m) * idx3 + dU[k]);
+    else
+      U[k] += Dt * (-(f1p - f1m) * idx1 - (f2p - f2m) * idx2 + dU[k]);
+#else
+    if (THREE_D)
+      U[k] += Dt * (-div_rn(f1p - f1m, G.dx1, G.idx1) - div_rn(f2p - f2m, G.dx2, G.idx2)
+                    - div_rn(f3p - f3m, G.dx3, G.idx3) + dU[k]);
+    else
+      U[k] += Dt * (-div_rn(f1p - f1m, G.dx1, G.idx1) - div_rn(f2p - f2m, G.dx2, G.idx2) + dU[k]);
+#endif
+  };
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    double f1m = FX.raw(1, k, h, i, j), f1p = FX.raw(1, k, h, i + 1, j);
+    if (k == RHO) {
+      // no inflow of mass through the radial boundaries (coord.c:307-321)
+      if (i == G.istart && f1m > 0) f1m = 0;
+      if (i + 1 == G.istop + 1 && f1p < 0) f1p = 0;
+    }
+    const double f2m = FX.raw(2, k, h, i, j), f2p = FX.raw(2, k, h, i, j + 1);
+    const double f3m = THREE_D ? FX.raw(3, k, h, i, j) : 0., f3p = THREE_D ? FX.raw(3, k, hp, i, j) : 0.;
+    upd(k, f1m, f1p, f2m, f2p, f3m, f3p);
+  }
+  if (!THREE_D) {
+    const double eA = FX.emf2(i, j), eB = FX.emf2(i, j + 1), eC = FX.emf2(i + 1, j), eD = FX.emf2(i + 1, j + 1);
+    upd(B1, 0., 0., -0.5 * (eA + eC), -0.5 * (eB + eD), 0., 0.);
+    upd(B2, 0.5 * (eA + eB), 0.5 * (eC + eD), 0., 0., 0., 0.);
+    upd(B3, FX.raw(1, B3, 0, i, j), FX.raw(1, B3, 0, i + 1, j), FX.raw(2, B3, 0, i, j), FX.raw(2, B3, 0, i, j + 1),
+        0., 0.);
+  } else {
+    {
+      const double e3a = FX.e3(h, i, j), e3b = FX.e3(h, i, j + 1), e3c = FX.e3(h, i + 1, j), e3d = FX.e3(h, i + 1, j + 1);
+      const double e2a = FX.e2(h, i, j), e2b = FX.e2(hp, i, j), e2c = FX.e2(h, i + 1, j), e2d = FX.e2(hp, i + 1, j);
+      upd(B1, 0., 0., -0.5 * (e3a + e3c), -0.5 * (e3b + e3d), 0.5 * (e2a + e2c), 0.5 * (e2b + e2d));
+      const double e1a = FX.e1(h, i, j), e1b = FX.e1(hp, i, j), e1c = FX.e1(h, i, j + 1), e1d = FX.e1(hp, i, j + 1);
+      upd(B2, 0.5 * (e3a + e3b), 0.5 * (e3c + e3d), 0., 0., -0.5 * (e1a + e1c), -0.5 * (e1b + e1d));
+      upd(B3, -0.5 * (e2a + e2b), -0.5 * (e2c + e2d), 0.5 * (e1a + e1b), 0.5 * (e1c + e1d), 0., 0.);
+    }
+  }
+}
+
 __device__ void source(double gam, const double *pb, const Geo &q, const double *__restrict__ conn, long ng, long gi,
                        double *dU, int *fail)
 {
@@ -346,6 +417,9 @@ __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const doub
     get_state(pz, q, s, &fail);
     primtoflux(G.gam, pz, s, 0, q.g, U);
   }
+#if HARM_CONS_V2
+  flux_update<THREE_D>(Flux{F1, F2, F3, G}, h, i, j, Dt, dU, U);
+#else
   {
     Flux FX{F1, F2, F3, G};
     double f1m[8], f1p[8], f2m[8], f2p[8], f3m[8], f3p[8];
@@ -360,12 +434,14 @@ __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const doub
         U[k] += Dt * (-(f1p[k] - f1m[k]) * idx1 - (f2p[k] - f2m[k]) * idx2 + dU[k]);
 #else
       if (THREE_D)
-        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 - (f3p[k] - f3m[k]) / G.dx3 + dU[k]);
+        U[k] += Dt * (-div_rn(f1p[k] - f1m[k], G.dx1, G.idx1) - div_rn(f2p[k] - f2m[k], G.dx2, G.idx2)
+                      - div_rn(f3p[k] - f3m[k], G.dx3, G.idx3) + dU[k]);
       else
-        U[k] += Dt * (-(f1p[k] - f1m[k]) / G.dx1 - (f2p[k] - f2m[k]) / G.dx2 + dU[k]);
+        U[k] += Dt * (-div_rn(f1p[k] - f1m[k], G.dx1, G.idx1) - div_rn(f2p[k] - f2m[k], G.dx2, G.idx2) + dU[k]);
 #endif
     }
   }
+#endif
 #pragma unroll
   for (int k = 0; k < 8; k++) Ub[k * G.nc + c] = U[k];
   if (fail) record_fail(sc, fail, h + (THREE_D ? 1 : 0), i, j);

@@ -325,6 +325,21 @@ int harm_utoprim_2d_batch(const double *U, const double *gcov, const double *gco
 int harm_utoprim_2d_batch_noalloc(const double *U, const double *gcov, const double *gcon,
                                   const double *gdet, double *prim, int *ret, long n, double gam);
 
+/* Measured FP64 pipe rates of a device, the denominators of the step
+   kernels' FP64 roofline: out[0] DFMA, out[1] DADD, out[2] DMUL instructions
+   per second (thread instructions, all SMs), out[3] IEEE divisions and out[4]
+   IEEE reciprocals per second.
+   Runs about 50 ms of device work.  A measurement helper with no counterpart
+   in the reference. */
+int harm_fp64_peak(int device, double *out);
+
+/* Self-check of the library's division by shared divisors on a device: n
+   seeded samples (random, special and near-midpoint numerators) of div_rn
+   against the IEEE division a / b.  counts[0]: samples that differ in any bit
+   (0 expected); counts[1]: near-midpoint samples drawn.  A self-check with no
+   counterpart in the reference. */
+int harm_div_check(int device, long n, unsigned long long seed, unsigned long long *counts);
+
 /* ---- run-time COOL_EOS (cooleos.c, cache4d.c, akima.c, mnewt.h) ---- */
 
 /* Tables of one EOS: per radial index t (the reference's cacheT[t],

@@ -99,6 +99,48 @@ def test_3d_steps_match_oracle(hc, oracle_built):
     assert np.array_equal(fg, fc)
 
 
+@pytest.mark.parametrize("shape", [(288, 256, 4), (288, 256, 8)])
+def test_benchmark_grid_steps_match_oracle(shape, hc, oracle_built):
+    """The r-theta grid of the 288x256x256 benchmark -- 288 radial zones out to
+    Rout = 100, hslope = 0.3 clustering towards the equator, the same polar rows --
+    with 4 and 8 phi planes, 2 steps on the device and on the oracle from the same
+    initial state (the oracle is pinned to the reference's own 288x256x4 build)."""
+    pr = hc.torus_problem(*shape)
+    ctx, o, g, c, fg, fc = run_both(hc, pr, 2)
+    err = field_rel_err(g, c)
+    exact = float(np.mean(g == c))
+    print(shape, "after 2 steps: max field-relative error", err, "exact fraction", exact)
+    assert np.all(err <= 2 * TOL_STEP), err
+    assert np.array_equal(fg, fc)
+    assert ctx.time() == o.time()
+    d, od = ctx.diag(), o.diag()
+    assert d["fail_code"] == 0
+    for k in ("mdot", "edot", "ldot"):
+        assert abs(d[k] - od[k]) <= 1e-12 * max(abs(od[k]), 1e-300), k
+    ctx.close()
+
+
+@pytest.mark.parametrize("lim", [1, 2])
+@pytest.mark.parametrize("shape,nsteps", [((64, 64, 1), 20), ((24, 24, 4), 5)])
+def test_van_leer_and_minmod_match_oracle(lim, shape, nsteps, hc, oracle_built):
+    """slope_lim's van Leer (lim 1) and minmod (lim 2) branches (interp.c:71-87);
+    the oracle's are pinned to the reference's with the same lim."""
+    pr = hc.torus_problem(*shape, lim=lim)
+    ctx, o, g, c, fg, fc = run_both(hc, pr, nsteps)
+    err = field_rel_err(g, c)
+    print("lim", lim, shape, "max field-relative error", err, "exact fraction", float(np.mean(g == c)))
+    assert np.all(err <= nsteps * TOL_STEP), err
+    assert np.array_equal(fg, fc)
+    assert ctx.time() == o.time()
+    ctx.close()
+    # the limiter is live: the MC run from the same initial state ends elsewhere
+    mc = hc.Context(hc.torus_problem(*shape))
+    mc.init_torus()
+    mc.run(nsteps)
+    assert not np.array_equal(active(pr, mc.get_prims()), g)
+    mc.close()
+
+
 def _state_after_steps(hc, pr, n):
     ctx = hc.Context(pr)
     ctx.init_torus()
