@@ -609,6 +609,25 @@ def run_cool(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile(args):
+    """A case for ncu: the torus at the given size and precision, --warmup steps,
+    then --steps more; the step kernels of the last steps are the ones to capture
+    (each step launches 5 flux/update kernels per half step in 3D: -s 10*warmup)."""
+    import harm_cool_b200 as hc
+    pr = hc.torus_problem(args.n1, args.n2, args.n3)
+    ctx = hc.Context(pr)
+    ctx.init_torus()
+    if args.precision == "mixed":
+        ctx.set_precision(hc.Context.MIXED)
+    ctx.run(args.warmup)
+    ctx.sync()
+    ms = ctx.run_timed(args.steps)
+    print(json.dumps({"workload": "profile case %dx%dx%d %s" % (args.n1, args.n2, args.n3, args.precision),
+                      "warmup": args.warmup, "steps": args.steps, "ms_per_step": ms / args.steps,
+                      "fail_code": ctx.diag()["fail_code"]}), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -623,7 +642,9 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
     ap.add_argument("--l1-steps", type=int, default=1000,
                     help="steps of the FP64 and mixed runs whose L1 difference the mixed line reports (0: skip)")
-    ap.add_argument("--workload", choices=("torus", "ensemble", "cool", "adjoint"), default="torus",
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64",
+                    help="precision of the profile workload")
+    ap.add_argument("--workload", choices=("torus", "ensemble", "cool", "adjoint", "profile"), default="torus",
                     help="torus: the 288x256x256 step (default); ensemble: 64 seeded 2D tori; "
                          "cool: the 256x256 COOL_EOS step")
     ap.add_argument("--cool-n", type=int, default=256)
@@ -652,6 +673,9 @@ def main():
         return
     if args.workload == "adjoint":
         run_adjoint(args)
+        return
+    if args.workload == "profile":
+        run_profile(args)
         return
     world, rank, local = dist_setup()
     try:

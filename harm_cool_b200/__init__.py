@@ -133,8 +133,12 @@ _SIGNATURES = {
     "harm_fixup": (ctypes.c_int, [ctypes.c_void_p, _DP]),
     "harm_bound_prim": (ctypes.c_int, [ctypes.c_void_p, _DP]),
     "harm_fixup_utoprim": (ctypes.c_int, [ctypes.c_void_p, _DP]),
+    "harm_fixup1zone": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long, ctypes.POINTER(ctypes.c_int), _DP, _BP]),
     "harm_utoprim_2d_batch": (ctypes.c_int, [_DP, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int),
                                              ctypes.c_long, ctypes.c_double]),
+    "harm_utoprim_fix_batch": (ctypes.c_int, [ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int),
+                                              ctypes.c_long, ctypes.c_double]),
+    "harm_pow_batch": (ctypes.c_int, [ctypes.c_int, _DP, _DP, _DP, ctypes.c_long]),
     "harm_restart_write": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RestartHeader), ctypes.POINTER(GridSpec),
                                           ctypes.c_char_p]),
     "harm_restart_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(GridSpec),
@@ -196,6 +200,30 @@ def fp64_peak(device=0):
     _check(library().harm_fp64_peak(device, _dp(out)))
     return {"dfma_inst_per_s": out[0], "dadd_inst_per_s": out[1], "dmul_inst_per_s": out[2],
             "ddiv_per_s": out[3], "drcp_per_s": out[4]}
+
+
+def utoprim_fix_batch(which, U, gcov, gcon, gdet, K, prim, gam):
+    """Utoprim_1dvsq2fix1 (which 1) or Utoprim_1dfix1 (which 2) over zones; prim
+    (the guess) is updated in place; returns the reference's return codes."""
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    gcov = np.ascontiguousarray(gcov, dtype=np.float64)
+    gcon = np.ascontiguousarray(gcon, dtype=np.float64)
+    gdet = np.ascontiguousarray(gdet, dtype=np.float64)
+    K = np.ascontiguousarray(K, dtype=np.float64)
+    assert prim.flags["C_CONTIGUOUS"] and prim.dtype == np.float64
+    ret = np.zeros(len(U), dtype=np.int32)
+    _check(library().harm_utoprim_fix_batch(which, _dp(U), _dp(gcov), _dp(gcon), _dp(gdet), _dp(K), _dp(prim),
+                                            ret.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(U), gam))
+    return ret
+
+
+def pow_batch(x, y, device=0):
+    """The device's correctly rounded x**y (the fall-back inversions' power)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    out = np.zeros_like(x)
+    _check(library().harm_pow_batch(device, _dp(x), _dp(y), _dp(out), len(x)))
+    return out
 
 
 def div_check(n, seed=1, device=0):

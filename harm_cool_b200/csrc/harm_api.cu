@@ -435,6 +435,33 @@ __global__ void k_utoprim_batch(const double *U, const double *gcov, const doubl
   for (int k = 0; k < 8; k++) prim[t * 8 + k] = p[k];
 }
 
+// Utoprim_1dvsq2fix1 (which 1) or Utoprim_1dfix1 (which 2) over independent zones
+__global__ void k_utoprim_fix_batch(int which, const double *U, const double *gcov, const double *gcon,
+                                    const double *gdet, const double *K, double *prim, int *ret, long n, double gam)
+{
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double *a = gcov + t * 16, *b = gcon + t * 16;
+  Geo q;
+  q.v00 = a[0]; q.v01 = a[1]; q.v03 = a[3]; q.v11 = a[5]; q.v13 = a[7]; q.v22 = a[10]; q.v33 = a[15];
+  q.n00 = b[0]; q.n01 = b[1]; q.n03 = b[3]; q.n10 = b[4]; q.n11 = b[5]; q.n13 = b[7]; q.n22 = b[10];
+  q.n30 = b[12]; q.n31 = b[13]; q.n33 = b[15];
+  q.alpha = 1. / sqrt(-q.n00);
+  q.g = gdet[t];
+  q.ialpha = 1. / q.alpha;
+  q.ig = 1. / q.g;
+  double u[8], p[8];
+  for (int k = 0; k < 8; k++) { u[k] = U[t * 8 + k]; p[k] = prim[t * 8 + k]; }
+  ret[t] = which == 1 ? utoprim<1>(gam, K[t], u, q, p) : utoprim<2>(gam, K[t], u, q, p);
+  for (int k = 0; k < 8; k++) prim[t * 8 + k] = p[k];
+}
+
+__global__ void k_pow_batch(const double *x, const double *y, double *out, long n)
+{
+  long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t < n) out[t] = pow_cr(x[t], y[t]);
+}
+
 // torus set-up: b^2 maximum over the active zones, and the field rescaling (init.c:368-403)
 __global__ void k_bsq_max(Grid G, const double *__restrict__ P, const double *__restrict__ geo, DevScalars *sc)
 {
@@ -903,6 +930,60 @@ static int on_host_array(harm_ctx *h, double *pv, int which)
   return get_prims(x, x->ph, pv, nullptr);
 }
 
+// fixup1zone() (fixup.c:142-383) at listed zones of the context's grid
+__global__ void k_fixup_zones(Grid G, long n, const int *__restrict__ hij, double *pv, signed char *flag,
+                              const double *__restrict__ geo, const double *__restrict__ floors, DevScalars *sc)
+{
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int h = hij[3 * t], i = hij[3 * t + 1], j = hij[3 * t + 2];
+  const long gi = (long)i * G.sn2 + j;
+  Geo q;
+  load_geo(geo_at(geo, G, L_CENT), G.ng, gi, q);
+  double v[8];
+  for (int k = 0; k < 8; k++) v[k] = pv[8 * t + k];
+  int fail = 0;
+  flag[t] = fixup1zone(G.gam, floors[gi], floors[G.ng + gi], q, v, &fail) ? -33 : 0;
+  if (fail) record_fail(sc, fail, h, i, j);
+  for (int k = 0; k < 8; k++) pv[8 * t + k] = v[k];
+}
+
+extern "C" int harm_fixup1zone(harm_ctx *h, long n, const int *hij, double *pv, signed char *flag)
+{
+  if (!h || !hij || !pv || !flag || n < 0) return fail_with(HARM_E_ARG, "harm_fixup1zone: bad arguments");
+  if (n == 0) return HARM_OK;
+  Ctx *x = &h->x;
+  const Grid &G = x->G;
+  for (long t = 0; t < n; t++) {
+    const int hh = hij[3 * t], i = hij[3 * t + 1], j = hij[3 * t + 2];
+    if (hh < 0 || hh >= x->D.sn3 || i < 0 || i >= G.sn1 || j < 0 || j >= G.sn2)
+      return fail_with(HARM_E_ARG, "harm_fixup1zone: zone outside the grid");
+  }
+  CK(cudaSetDevice(x->device));
+  int *dh = nullptr;
+  double *dp = nullptr;
+  signed char *df = nullptr;
+  CK(cudaMalloc(&dh, 3 * n * sizeof(int)));
+  CK(cudaMalloc(&dp, 8 * n * sizeof(double)));
+  CK(cudaMalloc(&df, n));
+  int rc = HARM_OK;
+  if (cudaMemcpyAsync(dh, hij, 3 * n * sizeof(int), cudaMemcpyHostToDevice, x->stream) != cudaSuccess ||
+      cudaMemcpyAsync(dp, pv, 8 * n * sizeof(double), cudaMemcpyHostToDevice, x->stream) != cudaSuccess)
+    rc = fail_with(HARM_E_CUDA, "harm_fixup1zone: upload");
+  if (rc == HARM_OK) {
+    k_fixup_zones<<<(unsigned)((n + 127) / 128), 128, 0, x->stream>>>(G, n, dh, dp, df, x->geo, x->floors, x->sc);
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(pv, dp, 8 * n * sizeof(double), cudaMemcpyDeviceToHost, x->stream) != cudaSuccess ||
+        cudaMemcpyAsync(flag, df, n, cudaMemcpyDeviceToHost, x->stream) != cudaSuccess ||
+        cudaStreamSynchronize(x->stream) != cudaSuccess)
+      rc = fail_with(HARM_E_CUDA, "harm_fixup1zone: launch");
+  }
+  cudaFree(dh);
+  cudaFree(dp);
+  cudaFree(df);
+  return rc;
+}
+
 extern "C" int harm_fixup(harm_ctx *h, double *pv) { return on_host_array(h, pv, 0); }
 extern "C" int harm_bound_prim(harm_ctx *h, double *pv) { return on_host_array(h, pv, 1); }
 extern "C" int harm_fixup_utoprim(harm_ctx *h, double *pv) { return on_host_array(h, pv, 2); }
@@ -935,6 +1016,57 @@ extern "C" int harm_utoprim_2d_batch(const double *U, const double *gcov, const 
   CK(cudaGetLastError());
   CK(cudaMemcpy(prim, dp, n * 64, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(ret, dr, n * sizeof(int), cudaMemcpyDeviceToHost));
+  return HARM_OK;
+}
+
+extern "C" int harm_utoprim_fix_batch(int which, const double *U, const double *gcov, const double *gcon,
+                                      const double *gdet, const double *K, double *prim, int *ret, long n, double gam)
+{
+  if ((which != 1 && which != 2) || !U || !gcov || !gcon || !gdet || !K || !prim || !ret || n < 0)
+    return fail_with(HARM_E_ARG, "harm_utoprim_fix_batch: bad arguments");
+  if (n == 0) return HARM_OK;
+  struct Buffers {
+    double *dU = nullptr, *da = nullptr, *db = nullptr, *dg = nullptr, *dk = nullptr, *dp = nullptr;
+    int *dr = nullptr;
+    ~Buffers() { cudaFree(dU); cudaFree(da); cudaFree(db); cudaFree(dg); cudaFree(dk); cudaFree(dp); cudaFree(dr); }
+  } B;
+  CK(cudaMalloc(&B.dU, n * 8 * 8));
+  CK(cudaMalloc(&B.da, n * 16 * 8));
+  CK(cudaMalloc(&B.db, n * 16 * 8));
+  CK(cudaMalloc(&B.dg, n * 8));
+  CK(cudaMalloc(&B.dk, n * 8));
+  CK(cudaMalloc(&B.dp, n * 8 * 8));
+  CK(cudaMalloc(&B.dr, n * sizeof(int)));
+  CK(cudaMemcpy(B.dU, U, n * 64, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(B.da, gcov, n * 128, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(B.db, gcon, n * 128, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(B.dg, gdet, n * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(B.dk, K, n * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(B.dp, prim, n * 64, cudaMemcpyHostToDevice));
+  k_utoprim_fix_batch<<<(unsigned)((n + 127) / 128), 128>>>(which, B.dU, B.da, B.db, B.dg, B.dk, B.dp, B.dr, n, gam);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(prim, B.dp, n * 64, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ret, B.dr, n * sizeof(int), cudaMemcpyDeviceToHost));
+  return HARM_OK;
+}
+
+extern "C" int harm_pow_batch(int device, const double *x, const double *y, double *out, long n)
+{
+  if (!x || !y || !out || n < 0) return fail_with(HARM_E_ARG, "harm_pow_batch: bad arguments");
+  if (n == 0) return HARM_OK;
+  CK(cudaSetDevice(device));
+  struct Buffers {
+    double *dx = nullptr, *dy = nullptr, *dz = nullptr;
+    ~Buffers() { cudaFree(dx); cudaFree(dy); cudaFree(dz); }
+  } B;
+  CK(cudaMalloc(&B.dx, n * 8));
+  CK(cudaMalloc(&B.dy, n * 8));
+  CK(cudaMalloc(&B.dz, n * 8));
+  CK(cudaMemcpy(B.dx, x, n * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(B.dy, y, n * 8, cudaMemcpyHostToDevice));
+  k_pow_batch<<<(unsigned)((n + 127) / 128), 128>>>(B.dx, B.dy, B.dz, n);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(out, B.dz, n * 8, cudaMemcpyDeviceToHost));
   return HARM_OK;
 }
 

@@ -7,12 +7,9 @@
 #define HARM_FLUX_MINB 8   // 64 registers
 #endif
 #ifndef HARM_CONS_MINB
-#define HARM_CONS_MINB 4   // 128 registers
+#define HARM_CONS_MINB 5   // 102 registers
 #endif
 #ifndef HARM_INV_MINB
 #define HARM_INV_MINB 5    // 102 registers
-#endif
-#ifndef HARM_HB_FLUX
-#define HARM_HB_FLUX 4
 #endif
 #include "harm_step.cuh"

@@ -8,10 +8,14 @@
 //    coordinates (g_{t theta}, g_{r theta}, g_{theta phi} and their inverse
 //    counterparts) are not stored, so the x*0 terms the reference adds are
 //    skipped -- this can only change the sign of an exactly-zero result;
-//  * pow() in the rare isentropic fall-back inversions is CUDA's, which may
-//    differ from glibc's in the last bit.
+//  * the isentropic fall-back inversions raise densities to the adiabatic
+//    index with pow_cr (harm_pow.cuh), the correctly rounded power, where the
+//    reference calls the host libm's pow(), correctly rounded in all but rare
+//    cases.
 #pragma once
 #include <cstdint>
+
+#include "harm_pow.cuh"
 
 namespace harm {
 
@@ -64,6 +68,9 @@ constexpr int GEO_N = 21;
 // take the IEEE division; a zero numerator gives a y, the signed zero a/b is.
 __device__ __forceinline__ double div_rn(double a, double b, double y)
 {
+#ifdef HARM_DBG_IEEE_DIV
+  return a / b;
+#endif
   const long long ia = __double_as_longlong(a);
   const unsigned ea = (unsigned)(ia >> 52) & 0x7ffu;
   const unsigned eb = (unsigned)(__double_as_longlong(b) >> 52) & 0xfffu;  // sign bit included
@@ -175,7 +182,11 @@ __device__ __forceinline__ void ucon_calc(const R *pr, const Geo &q, R *ucon, in
   // the reference's pr[U2] - gamma * b2 / alpha with b2 = g^{t theta} alpha^2 = 0*alpha*alpha:
   // gamma * (+0) / alpha is +0 for finite gamma and NaN otherwise, and so is
   // gamma - gamma, which takes two operations instead of a division
+#ifdef HARM_DBG_B2
+  ucon[2] = pr[U2] - gamma * (0. * alpha * alpha) / alpha;
+#else
   ucon[2] = pr[U2] - (gamma - gamma);
+#endif
   ucon[3] = pr[U3] - div_by(gamma * b3, alpha, q.ialpha);
 }
 
@@ -576,7 +587,7 @@ __device__ __forceinline__ double W_of_vsq_fix(const U2P &c, double vsq, double 
 {
   double gtmp = (1. - vsq);
   rho = c.D * sqrt(gtmp);
-  p = c.K_atm * pow(rho, c.gam);
+  p = c.K_atm * pow_cr(rho, c.gam);
   u = p / (c.gam - 1.);
   return (rho + u + p) / gtmp;
 }
@@ -651,7 +662,7 @@ static __device__ __noinline__ int gnr2_rho(const U2P &c, double &x)
     double B = B0 / (GAMMA - 1.);
     double rho = x;
     double W = c.W_for_gnr2;
-    double C = pow(rho, GAMMA - 1.);
+    double C = pow_cr(rho, GAMMA - 1.);
     double r0 = rho * W - A - B * C;
     double j00 = W - B0 * C / rho;
     double dx = -r0 / j00;
@@ -688,7 +699,7 @@ static __device__ __noinline__ void func_1d_orig1(U2P &c, double W, double &dx, 
          t21 = W * W, t23 = rho * rho, t26 = 1. / t1;
   double r0 = (t3 + (2.0 * t2 + ((Qtsq - t5) * t1 + (-2.0 * t8 - t10) * W) * W) * W
                + (t5 + (2.0 * Bsq + W) * W) * t21 * t23) * t26 / t21;
-  double t29 = t1 * t1, t30 = QdotBsq * t29, t32 = GAMMA * K_atm, t33 = pow(rho, 1.0 * GAMMA), t34 = t32 * t33,
+  double t29 = t1 * t1, t30 = QdotBsq * t29, t32 = GAMMA * K_atm, t33 = pow_cr(rho, 1.0 * GAMMA), t34 = t32 * t33,
          t38 = t23 * t33, t51 = GAMMA * t1 * K_atm * t33, t67 = t21 * W;
   double j00 = -2.0 * (t30 * Bsq * t34
                        + (t30 * t34 + ((-t38 * Bsq * t32 + Bsq * GAMMA * t1 * K_atm * t33) * t1
@@ -708,7 +719,7 @@ static __device__ __noinline__ int u2p_body_fix1(U2P &c, const double *U, const 
   double gammasq = 1. + utsq;
   double gamma = sqrt(gammasq);
   double rho0 = c.D / gamma;
-  double p = c.K_atm * pow(rho0, c.gam);
+  double p = c.K_atm * pow_cr(rho0, c.gam);
   double u = p / (c.gam - 1.);
   double w = rho0 + u + p;
   double W_last = w * gammasq;
@@ -755,7 +766,7 @@ static __device__ __noinline__ int u2p_body_fix1(U2P &c, const double *U, const 
   double gtmp = sqrt(1. - vsq);
   gamma = 1. / gtmp;
   rho0 = c.D * gtmp;
-  p = c.K_atm * pow(rho0, c.gam);
+  p = c.K_atm * pow_cr(rho0, c.gam);
   u = p / (c.gam - 1.);
   if ((rho0 <= 0.) || (u <= 0.)) return 5;
   prim[RHO] = rho0;

@@ -303,12 +303,32 @@ int harm_ensemble_run_timed(harm_ensemble *ens, int nsteps, double *ms);
 int harm_fixup(harm_ctx *ctx, double *pv);                        /* fixup.c:51-60, decs.h:567 */
 int harm_bound_prim(harm_ctx *ctx, double *pv);                   /* bounds.c:54, decs.h:548 */
 int harm_fixup_utoprim(harm_ctx *ctx, double *pv);                /* fixup.c:432, decs.h:569 */
+/* fixup1zone() (fixup.c:142-383, decs.h:568) at n zones of the context's grid:
+   hij[n][3] = (h, i, j) in the reference's indices, pv[n][8] the primitives
+   (floored in place), flag[n] = -33 where the reference sets pflag to -33 (a
+   gamma failure, left to fixup_utoprim), else 0.  Host arrays. */
+int harm_fixup1zone(harm_ctx *ctx, long n, const int *hij, double *pv, signed char *flag);
 
 /* Utoprim_2d() (utoprim_2d.c:126, decs.h:608) over n independent zones on the
    device: U[n][8], gcov[n][16], gcon[n][16], gdet[n], prim[n][8] (guess in,
    result out), ret[n] (the reference's return code).  Host arrays. */
 int harm_utoprim_2d_batch(const double *U, const double *gcov, const double *gcon,
                           const double *gdet, double *prim, int *ret, long n, double gam);
+
+/* The isentropic fall-back inversions over n independent zones: which = 1
+   Utoprim_1dvsq2fix1() (utoprim_1dvsq2fix1.c:143, decs.h:609), which = 2
+   Utoprim_1dfix1() (utoprim_1dfix1.c:137, decs.h:611), with K[n] the entropy
+   constant of each zone (the reference passes Katm[i], step_ch.c:277-300);
+   arrays as harm_utoprim_2d_batch.  Host arrays. */
+int harm_utoprim_fix_batch(int which, const double *U, const double *gcov, const double *gcon,
+                           const double *gdet, const double *K, double *prim, int *ret, long n, double gam);
+
+/* x[k]^y[k] rounded to nearest as the fall-back inversions compute it on the
+   device (double-double exp(y ln x)), in place of the host libm's pow()
+   (utoprim_1dvsq2fix1.c:583-616, utoprim_1dfix1.c:864-880).  Host arrays.  A
+   check of the device arithmetic with no counterpart of its own in the
+   reference. */
+int harm_pow_batch(int device, const double *x, const double *y, double *out, long n);
 
 /* The same inversion as harm_utoprim_2d_batch, for callers that cannot
    allocate device memory: hosts whose GPU memory is already committed to a

@@ -33,7 +33,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = "/root/reference/src"
+ROOT = os.path.dirname(HERE)
+# the reference tree's src/ directory; HARM_REFERENCE_SRC names another copy
+REF_SRC = os.environ.get("HARM_REFERENCE_SRC", "/root/reference/src")
 OUT = os.path.join(HERE, "_ref")
 
 # name -> (N1, N2, N3, spin a, torus rin, torus rmax, beta)
@@ -59,6 +61,12 @@ CONFIGS["ce3d"] = (16, 16, 4, 0.6, 4.0, 11.8, 50.0)
 # the 256x256 COOL_EOS torus, for the CPU timing beside the device step
 CONFIGS["ce256"] = (256, 256, 1, 0.6, 4.0, 11.8, 50.0)
 COOL_CONFIGS = ("ce2d", "ce3d", "ce256")
+# the drop-in: the reference's host code with harm_cool_b200/shim/harm_gpu.cpp in
+# place of step_ch.c, bounds.c, fixup.c and utoprim_2d.c, linked to libharm_b200
+CONFIGS["g2d"] = CONFIGS["t2d"]
+CONFIGS["g3d"] = CONFIGS["t3d"]
+SHIM_CONFIGS = ("g2d", "g3d")
+SHIM_REPLACES = ("step_ch", "bounds", "fixup", "utoprim_2d")
 
 SOURCES = ["bounds", "coord", "diag", "dump", "fixup", "image", "interp", "main",
            "metric", "lu", "phys", "ranc", "restart", "step_ch", "u2p_util",
@@ -121,7 +129,7 @@ def build_config(name, force=False):
     obj = os.path.join(cdir, "obj")
     lib = os.path.join(cdir, "libharmref.so")
     exe = os.path.join(cdir, "refbench")
-    if not force and os.path.exists(lib) and os.path.exists(exe):
+    if not force and os.path.exists(lib) and os.path.exists(exe) and not (name in SHIM_CONFIGS and shim_stale(name)):
         return lib
     os.makedirs(gen, exist_ok=True)
     os.makedirs(obj, exist_ok=True)
@@ -158,8 +166,10 @@ def build_config(name, force=False):
     flags = ["g++", "-O2", "-ffp-contract=off", "-fPIC", "-w", "-DMPI_USED",
              "-Dmain=harm_reference_main", "-I" + gen, "-I-",
              "-I" + os.path.join(HERE, "fakempi"), "-I" + REF_SRC]
+    shim = name in SHIM_CONFIGS
     objs = []
-    for s in SOURCES + (["tracers"] if tracers else []) + (["cache4d", "akima"] if cool else []):
+    sources = [s for s in SOURCES if not (shim and s in SHIM_REPLACES)]
+    for s in sources + (["tracers"] if tracers else []) + (["cache4d", "akima"] if cool else []):
         o = os.path.join(obj, s + ".o")
         run(flags + ["-x", "c++", "-c", os.path.join(REF_SRC, s + ".c"), "-o", o])
         objs.append(o)
@@ -174,8 +184,16 @@ def build_config(name, force=False):
         run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-c", os.path.join(HERE, "eos_standin.c"), "-o", o])
         objs.append(o)
     o = os.path.join(obj, "refdrv.o")
-    run(flags + ["-c", os.path.join(HERE, "refdrv.cpp"), "-o", o])
+    run(flags + (["-DHARM_SHIM_BUILD"] if shim else []) + ["-c", os.path.join(HERE, "refdrv.cpp"), "-o", o])
     objs.append(o)
+    libs = []
+    if shim:
+        pkg = os.path.join(ROOT, "harm_cool_b200")
+        o = os.path.join(obj, "harm_gpu.o")
+        run(flags + ["-I" + os.path.join(ROOT, "include"), "-c", os.path.join(pkg, "shim", "harm_gpu.cpp"),
+                     "-o", o])
+        objs.append(o)
+        libs = ["-L" + pkg, "-lharm_b200", "-Wl,-rpath,$ORIGIN/../../../harm_cool_b200"]
     if tracers:
         # tracers.c scales its dump files by RHO_UNIT and T_UNIT, defined in cooleos.c,
         # which needs the Fortran EOS; the checker reads no dump file
@@ -185,7 +203,7 @@ def build_config(name, force=False):
     o = os.path.join(obj, "fakempi.o")
     run(["gcc", "-O2", "-fPIC", "-c", os.path.join(HERE, "fakempi", "fakempi.c"), "-o", o])
     objs.append(o)
-    run(["g++", "-shared", "-o", lib] + objs + ["-lm"])
+    run(["g++", "-shared", "-o", lib] + objs + libs + ["-lm"])
     run(["g++", "-O2", "-o", exe, os.path.join(HERE, "refbench.cpp"), lib,
          "-Wl,-rpath,$ORIGIN", "-lm"])
     return lib
@@ -195,6 +213,14 @@ def build_all(force=False):
     if not os.path.isdir(REF_SRC):
         return []
     return [build_config(n, force) for n in CONFIGS]
+
+
+def shim_stale(name):
+    """The drop-in build is older than the shim or the library it links."""
+    lib = os.path.join(OUT, name, "libharmref.so")
+    deps = [os.path.join(ROOT, "harm_cool_b200", "shim", "harm_gpu.cpp"),
+            os.path.join(ROOT, "harm_cool_b200", "libharm_b200.so"), os.path.join(ROOT, "include", "harm_b200.h")]
+    return not os.path.exists(lib) or os.path.getmtime(lib) < max(os.path.getmtime(d) for d in deps if os.path.exists(d))
 
 
 if __name__ == "__main__":

@@ -190,6 +190,8 @@ void ref_prim_to_U(double *pr, int i, int j, double *U)
 void ref_fixup(double *pv) { fixup(pv); }
 void ref_bound_prim(double *pv) { bound_prim(pv); }
 void ref_fixup_utoprim(double *pv) { fixup_utoprim(pv); }
+#ifndef HARM_SHIM_BUILD
+/* (the drop-in build has no advance(): step_ch.c is not linked) */
 double ref_advance(double *pi, double *pb, double Dt, double *pf, int fullstep)
 {
   quiet(1);
@@ -197,6 +199,7 @@ double ref_advance(double *pi, double *pb, double Dt, double *pf, int fullstep)
   quiet(0);
   return r;
 }
+#endif
 
 /* diag(INIT_OUT) (diag.c:59-375) run in directory dir (which must hold a dumps/
    subdirectory): it appends the energy line to dir/ener.out and writes its LOG
