@@ -1106,6 +1106,15 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
   size_t stack = 0;
   CK(cudaDeviceGetLimit(&stack, cudaLimitStackSize));
   if (stack < 4096) CK(cudaDeviceSetLimit(cudaLimitStackSize, 4096));
+  // the caller's stack limit again on every return (after B's buffers are freed)
+  struct RestoreStack {
+    size_t s;
+    bool on;
+    ~RestoreStack()
+    {
+      if (on) cudaDeviceSetLimit(cudaLimitStackSize, s);
+    }
+  } restore_stack{stack, stack < 4096};
   const int nseg = (nsteps + every - 1) / every;
   const int nrec = every < nsteps ? every : nsteps;
   DevBuf B;

@@ -27,8 +27,12 @@
 // host it names a stand-in object, and a kernel given that address would
 // fault or read the wrong memory.  The first call on each device therefore
 // asks the runtime for the array's device address (cudaGetSymbolAddress, with
-// that device current) and keeps it for later calls.  Make that first call
-// before any stream capture is begun on the device.
+// that device current) and creates one non-blocking stream for the calls
+// (so they do not serialise with the host's blocking streams), and keeps both
+// for later calls.  Make that first call before any stream capture is begun on
+// the device.  Both belong to the device's primary context: a host that
+// resets the device (cudaDeviceReset) after the first call must not call this
+// entry point again in that process.
 #include <mutex>
 
 #include "harm_common.cuh"
@@ -45,9 +49,10 @@ static __device__ __align__(256) double g_u2p_scratch[kDoubles];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-double *g_addr[kMaxDevices];  // device address of g_u2p_scratch, per device
+double *g_addr[kMaxDevices];          // device address of g_u2p_scratch, per device
+cudaStream_t g_stream[kMaxDevices];   // the calls' stream, per device
 
-int scratch_address(double **out)
+int scratch_address(double **out, cudaStream_t *st)
 {
   int dev = 0;
   CK(cudaGetDevice(&dev));
@@ -58,9 +63,14 @@ int scratch_address(double **out)
     cudaError_t e = cudaGetSymbolAddress(&p, g_u2p_scratch);
     if (e != cudaSuccess)
       return fail_with(HARM_E_CUDA, std::string("cudaGetSymbolAddress(g_u2p_scratch): ") + cudaGetErrorString(e));
+    cudaStream_t s = nullptr;
+    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail_with(HARM_E_CUDA, std::string("cudaStreamCreateWithFlags: ") + cudaGetErrorString(e));
+    g_stream[dev] = s;
     g_addr[dev] = static_cast<double *>(p);
   }
   *out = g_addr[dev];
+  *st = g_stream[dev];
   return HARM_OK;
 }
 
@@ -100,9 +110,9 @@ extern "C" int harm_utoprim_2d_batch_noalloc(const double *U, const double *gcov
                                      std::to_string(kMax) + " zones; split the batch");
   if (n == 0) return HARM_OK;
   double *S = nullptr;
-  int rc = scratch_address(&S);
+  cudaStream_t st = nullptr;
+  int rc = scratch_address(&S, &st);
   if (rc) return rc;
-  cudaStream_t st = 0;
   CK(cudaMemcpyAsync(S + kOffU, U, n * 8 * sizeof(double), cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(S + kOffCov, gcov, n * 16 * sizeof(double), cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(S + kOffCon, gcon, n * 16 * sizeof(double), cudaMemcpyHostToDevice, st));

@@ -149,8 +149,8 @@ __global__ void __launch_bounds__(128, HARM_FLUX_MINB) k_flux(Grid G, const doub
 }
 
 
-// ctrec (the adjoint's recomputation of a corrector, 2D): keep the faces'
-// wave speeds there
+// ctrec (the adjoint's recomputation of a corrector): keep the direction-1
+// and -2 faces' wave speeds there
 template <bool FULL>
 void launch_flux(const Grid &G, dim3 b, cudaStream_t st, const double *pb, flux_t *F1, flux_t *F2, flux_t *F3,
                  const double *geo, const float *geo32, DevScalars *sc, double *ctrec = nullptr)
@@ -162,8 +162,11 @@ void launch_flux(const Grid &G, dim3 b, cudaStream_t st, const double *pb, flux_
   dim3 g3((faces_per_row<3>(G) * face_rows<3>(G) + 127) / 128, 1, gz);
 #if !HARM_STEP_MIXED
   if (FULL && ctrec) {
+    // ctrec holds directions 1 and 2 (the adjoint that reads it is 2D); a 3D
+    // step still gets its phi fluxes, without a record
     k_flux<1, true, true><<<g1, b, 0, st>>>(G, pb, F1, geo, geo32, sc, ctrec);
     k_flux<2, true, true><<<g2, b, 0, st>>>(G, pb, F2, geo, geo32, sc, ctrec);
+    if (G.n3 > 1) k_flux<3, true><<<g3, b, 0, st>>>(G, pb, F3, geo, geo32, sc, nullptr);
     return;
   }
 #endif

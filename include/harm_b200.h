@@ -35,7 +35,6 @@ enum {
   HARM_E_CUDA = -2,     /* a CUDA runtime call failed */
   HARM_E_NODEV = -3,    /* no usable sm_100 device */
   HARM_E_DT = -11,      /* dt < 1e-9: where the reference calls exit(11) (step_ch.c:126-129) */
-  HARM_E_TIMEOUT = -12, /* a bounded device-side wait ran out */
   HARM_E_ADJOINT = -13  /* the adjoint cannot follow the steps (a step failed; see harm_last_error) */
 };
 
@@ -337,8 +336,10 @@ int harm_pow_batch(int device, const double *x, const double *y, double *out, lo
    run.  The device copies live in one fixed array inside the library (about
    6.2 MiB per GPU, held until exit), so the call allocates nothing.  At most
    HARM_U2P_NOALLOC_MAX zones per call (HARM_E_ARG beyond).  The first call on
-   a device looks up the array's device address; make it before any stream
-   capture.  Calls share the array, so calls that overlap on the GPU race.
+   a device looks up the array's device address and creates the non-blocking
+   stream the calls run on; make it before any stream capture, and do not call
+   again after resetting the device.  Calls share the array, so calls that
+   overlap on the GPU race.
    Blocks until the results are in prim and ret.  No counterpart in the
    reference. */
 #define HARM_U2P_NOALLOC_MAX 16384
@@ -370,7 +371,9 @@ int harm_div_check(int device, long n, unsigned long long seed, unsigned long lo
    cooleos.c:171-194); the units and ranges are cooleos.c's constants
    (cooleos.c:83-135, 840-940); gam is the gamma-law fall-back's index.
    hdfac[ntab] (each table's HdFac, cooleos.c:945-960) and l_unit serve the
-   cooling values of harm_diag_integrals; hdfac may be NULL without them. */
+   cooling values of harm_diag_integrals; hdfac may be NULL without them.
+   Creating an EOS raises the device's per-thread stack limit to 4 KiB for the
+   rest of the process (the EOS calls nest deeper than the default allows). */
 typedef struct harm_eos harm_eos;
 typedef struct harm_eos_desc {
   int nx, ny, ntab;
