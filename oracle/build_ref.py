@@ -209,10 +209,50 @@ def build_config(name, force=False):
     return lib
 
 
+# Timing builds: the reference's own objects at -O3, the fastest of the flag
+# sets tried for the CPU baseline on this path's 288x256x4 step (Xeon with
+# AVX-512, g++ 13): -O3 3.2e5 zone-cycles/s per core, -O3 -march=x86-64-v3
+# (AVX2) 3.0e5, -O2 2.8e5, -O3 -march=x86-64-v4 (AVX-512, what -march=native
+# selects there) 2.5e5.  Not a parity build: the parity builds above keep -O2
+# -ffp-contract=off.
+TIMING_CONFIGS = ("c2s",)
+TIMING_FLAGS = ["-O3"]
+
+
+def build_timing(name, force=False):
+    """oracle/_ref/<name>/refbench_o3 (with libharmref_o3.so)."""
+    cdir = os.path.join(OUT, name)
+    gen = os.path.join(cdir, "gen")
+    obj = os.path.join(cdir, "obj_o3")
+    lib = os.path.join(cdir, "libharmref_o3.so")
+    exe = os.path.join(cdir, "refbench_o3")
+    if not force and os.path.exists(lib) and os.path.exists(exe):
+        return exe
+    build_config(name)   # the patched headers in gen/
+    os.makedirs(obj, exist_ok=True)
+    flags = ["g++"] + TIMING_FLAGS + ["-fPIC", "-w", "-DMPI_USED", "-Dmain=harm_reference_main", "-I" + gen, "-I-",
+                                      "-I" + os.path.join(HERE, "fakempi"), "-I" + REF_SRC]
+    objs = []
+    for s in SOURCES:
+        o = os.path.join(obj, s + ".o")
+        run(flags + ["-x", "c++", "-c", os.path.join(REF_SRC, s + ".c"), "-o", o])
+        objs.append(o)
+    for src, o in ((os.path.join(gen, "init.c"), "init.o"), (os.path.join(HERE, "refdrv.cpp"), "refdrv.o")):
+        o = os.path.join(obj, o)
+        run(flags + (["-x", "c++"] if src.endswith(".c") else []) + ["-c", src, "-o", o])
+        objs.append(o)
+    o = os.path.join(obj, "fakempi.o")
+    run(["gcc"] + TIMING_FLAGS + ["-fPIC", "-c", os.path.join(HERE, "fakempi", "fakempi.c"), "-o", o])
+    objs.append(o)
+    run(["g++", "-shared", "-o", lib] + objs + ["-lm"])
+    run(["g++", "-O2", "-o", exe, os.path.join(HERE, "refbench.cpp"), lib, "-Wl,-rpath,$ORIGIN", "-lm"])
+    return exe
+
+
 def build_all(force=False):
     if not os.path.isdir(REF_SRC):
         return []
-    return [build_config(n, force) for n in CONFIGS]
+    return [build_config(n, force) for n in CONFIGS] + [build_timing(n, force) for n in TIMING_CONFIGS]
 
 
 def shim_stale(name):
