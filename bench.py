@@ -34,11 +34,11 @@ sys.path.insert(0, ROOT)
 
 def kernels_per_step(n3):
     """Kernel launches of one step: per half step one flux kernel per direction,
-    the conserved update and the inversion, bound_prim, the flag flip, the two
-    repair kernels (list and wavefront), bound_prim; the corrector adds the flux
-    diagnostics; then the mass diagnostics and the dt update."""
+    the corner EMFs, the conserved update and the inversion, bound_prim, the flag
+    flip, the two repair kernels (list and wavefront), bound_prim; the corrector
+    adds the flux diagnostics; then the mass diagnostics and the dt update."""
     nflux = 3 if n3 > 1 else 2
-    return 2 * (nflux + 7) + 1 + 2
+    return 2 * (nflux + 8) + 1 + 2
 METRIC = "zone-cycles/s 288x256x256 GRMHD step_ch: FP64, mixed precision beside it"
 STATE_BYTES_PER_ZONE_CYCLE = 320  # p read twice, ph written and read, p written; 8 FP64 prims
 

@@ -643,6 +643,7 @@ extern "C" int harm_create(const harm_params *prm, const double *gcov, const dou
   rc |= al((void **)&x->partials, 3 * x->nparts * sizeof(double));
   rc |= al((void **)&x->sc, sizeof(DevScalars));
   rc |= al((void **)&x->Ubuf, st);
+  rc |= al((void **)&x->emf, 3 * G.nc * sizeof(double));
   rc |= al((void **)&x->coolgeo, 2 * G.ng * sizeof(double));
   if (rc != HARM_OK) { harm_destroy(h); return HARM_E_CUDA; }
   if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) { harm_destroy(h); return fail_with(HARM_E_CUDA, "stream"); }
@@ -704,7 +705,7 @@ extern "C" void harm_destroy(harm_ctx *h)
   if (x->graph_exec) cudaGraphExecDestroy(x->graph_exec);
   void *ptrs[] = {x->p, x->ph, x->F1, x->F2, x->F3, x->pflag, x->geo, x->conn, x->floors, x->katm,
                   x->stage, x->stage_flag, x->fail_list, x->fix_buf, x->partials, x->sc,
-                  x->F1f, x->F2f, x->F3f, x->geo32, x->conn32, x->Ubuf, x->trX, x->trids, x->trst,
+                  x->F1f, x->F2f, x->F3f, x->geo32, x->conn32, x->Ubuf, x->emf, x->trX, x->trids, x->trst,
                   x->lastT, x->coolgeo, x->cooldiag};
   for (void *p : ptrs)
     if (p) cudaFree(p);

@@ -84,6 +84,7 @@ struct Ctx {
   float *geo32;                  // mixed mode: FP32 geometry [4 locations][GEO_N][ng]
   float *conn32;                 // mixed mode: FP32 connection [40][ng]
   double *Ubuf;                  // conserved variables between the two update launches [8][nc]
+  double *emf;                   // flux_ct's corner EMFs e1, e2, e3 [3][nc] (k_emf)
   int tbx, tby;                  // tile of the zone and face kernels: theta x r threads, 128 in all
   long ntr;                      // tracer particles
   double *trX;                   // [3][ntr] code coordinates X1, X2, X3

@@ -276,17 +276,40 @@ __device__ void zone_fluxes(const Flux &FX, int h, int i, int j, double *f1m, do
   }
 }
 
-#ifndef HARM_CONS_V2
-#define HARM_CONS_V2 1
-#endif
+// flux_ct's corner EMFs (step_ch.c:514-629 in 2D, 726-798 in 3D), each
+// formed once from the raw face fluxes, for the update of the four zones that
+// share the corner: emf[2 nc + cell] e3 (2D: the one EMF), and in 3D emf[cell]
+// e1, emf[nc + cell] e2.  Corners i in [istart, istop+1], j in [jstart,
+// jstop+1], every phi plane.
+template <bool THREE_D>
+__global__ void __launch_bounds__(128) k_emf(Grid G, const flux_t *__restrict__ F1, const flux_t *__restrict__ F2,
+                                             const flux_t *__restrict__ F3, double *__restrict__ emf, DevScalars *sc)
+{
+  if (sc->halted) return;
+  const int nj = G.n2 + 1;
+  const int f = blockIdx.x * 128 + threadIdx.x;
+  const int j = G.jstart + f % nj, i = G.istart + f / nj;
+  if (i > G.istop + 1) return;
+  const int h = blockIdx.z;
+  const Flux FX{F1, F2, F3, G};
+  const long c = cidx(G, h, i, j);
+  if (THREE_D) {
+    emf[c] = FX.e1(h, i, j);
+    emf[G.nc + c] = FX.e2(h, i, j);
+    emf[2 * G.nc + c] = FX.e3(h, i, j);
+  } else {
+    emf[2 * G.nc + c] = FX.emf2(i, j);
+  }
+}
 
 // The flux divergence of the update (step_ch.c:247-263) one conserved
 // component at a time, U[k] += Dt (-dF1/dx1 - dF2/dx2 [- dF3/dx3] + dU[k]), with
 // the same face fluxes zone_fluxes forms (the no-inflow mass-flux fix, and the
-// field components rebuilt from the corner EMFs of flux_ct), so only one
-// component's six face values are live at a time.
+// field components rebuilt from the corner EMFs of flux_ct, read from k_emf's
+// planes), so only one component's six face values are live at a time.
 template <bool THREE_D>
-__device__ __forceinline__ void flux_update(const Flux &FX, int h, int i, int j, double Dt, const double *dU, double *U)
+__device__ __forceinline__ void flux_update(const Flux &FX, const double *__restrict__ emf, int h, int i, int j,
+                                            double Dt, const double *dU, double *U)
 {
   const Grid &G = FX.G;
   const int hp = THREE_D ? hwrap(G, h + 1) : 0;
@@ -317,21 +340,24 @@ __device__ __forceinline__ void flux_update(const Flux &FX, int h, int i, int j,
     const double f3m = THREE_D ? FX.raw(3, k, h, i, j) : 0., f3p = THREE_D ? FX.raw(3, k, hp, i, j) : 0.;
     upd(k, f1m, f1p, f2m, f2p, f3m, f3p);
   }
+  const double *E1 = emf, *E2 = emf + G.nc, *E3 = emf + 2 * G.nc;
   if (!THREE_D) {
-    const double eA = FX.emf2(i, j), eB = FX.emf2(i, j + 1), eC = FX.emf2(i + 1, j), eD = FX.emf2(i + 1, j + 1);
+    const double eA = __ldg(E3 + cidx(G, 0, i, j)), eB = __ldg(E3 + cidx(G, 0, i, j + 1));
+    const double eC = __ldg(E3 + cidx(G, 0, i + 1, j)), eD = __ldg(E3 + cidx(G, 0, i + 1, j + 1));
     upd(B1, 0., 0., -0.5 * (eA + eC), -0.5 * (eB + eD), 0., 0.);
     upd(B2, 0.5 * (eA + eB), 0.5 * (eC + eD), 0., 0., 0., 0.);
     upd(B3, FX.raw(1, B3, 0, i, j), FX.raw(1, B3, 0, i + 1, j), FX.raw(2, B3, 0, i, j), FX.raw(2, B3, 0, i, j + 1),
         0., 0.);
   } else {
-    {
-      const double e3a = FX.e3(h, i, j), e3b = FX.e3(h, i, j + 1), e3c = FX.e3(h, i + 1, j), e3d = FX.e3(h, i + 1, j + 1);
-      const double e2a = FX.e2(h, i, j), e2b = FX.e2(hp, i, j), e2c = FX.e2(h, i + 1, j), e2d = FX.e2(hp, i + 1, j);
-      upd(B1, 0., 0., -0.5 * (e3a + e3c), -0.5 * (e3b + e3d), 0.5 * (e2a + e2c), 0.5 * (e2b + e2d));
-      const double e1a = FX.e1(h, i, j), e1b = FX.e1(hp, i, j), e1c = FX.e1(h, i, j + 1), e1d = FX.e1(hp, i, j + 1);
-      upd(B2, 0.5 * (e3a + e3b), 0.5 * (e3c + e3d), 0., 0., -0.5 * (e1a + e1c), -0.5 * (e1b + e1d));
-      upd(B3, -0.5 * (e2a + e2b), -0.5 * (e2c + e2d), 0.5 * (e1a + e1b), 0.5 * (e1c + e1d), 0., 0.);
-    }
+    const double e3a = __ldg(E3 + cidx(G, h, i, j)), e3b = __ldg(E3 + cidx(G, h, i, j + 1));
+    const double e3c = __ldg(E3 + cidx(G, h, i + 1, j)), e3d = __ldg(E3 + cidx(G, h, i + 1, j + 1));
+    const double e2a = __ldg(E2 + cidx(G, h, i, j)), e2b = __ldg(E2 + cidx(G, hp, i, j));
+    const double e2c = __ldg(E2 + cidx(G, h, i + 1, j)), e2d = __ldg(E2 + cidx(G, hp, i + 1, j));
+    upd(B1, 0., 0., -0.5 * (e3a + e3c), -0.5 * (e3b + e3d), 0.5 * (e2a + e2c), 0.5 * (e2b + e2d));
+    const double e1a = __ldg(E1 + cidx(G, h, i, j)), e1b = __ldg(E1 + cidx(G, hp, i, j));
+    const double e1c = __ldg(E1 + cidx(G, h, i, j + 1)), e1d = __ldg(E1 + cidx(G, hp, i, j + 1));
+    upd(B2, 0.5 * (e3a + e3b), 0.5 * (e3c + e3d), 0., 0., -0.5 * (e1a + e1c), -0.5 * (e1b + e1d));
+    upd(B3, -0.5 * (e2a + e2b), -0.5 * (e2c + e2d), 0.5 * (e1a + e1b), 0.5 * (e1c + e1d), 0., 0.);
   }
 }
 
@@ -361,6 +387,7 @@ __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const doub
                                                               const double *__restrict__ conn,
                                                               const float *__restrict__ geo32,
                                                               const float *__restrict__ conn32,
+                                                              const double *__restrict__ emf,
                                                               double *__restrict__ Ub, DevScalars *sc)
 {
   if (sc->halted) return;
@@ -368,9 +395,6 @@ __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const doub
   const int i = G.istart + blockIdx.y * blockDim.y + threadIdx.y;
   if (i > G.istop || j > G.jstop) return;
   const double Dt = FULL ? sc->dt : 0.5 * sc->dt;
-#if HARM_STEP_MIXED
-  const double idx1 = 1. / G.dx1, idx2 = 1. / G.dx2, idx3 = 1. / G.dx3;
-#endif
   const int h0 = blockIdx.z * HARM_HB_ZONE, h1 = min(G.n3, h0 + HARM_HB_ZONE);
   for (int h = h0; h < h1; h++) {
   const long c = cidx(G, h, i, j);
@@ -420,31 +444,7 @@ __global__ void __launch_bounds__(128, HARM_CONS_MINB) k_cons(Grid G, const doub
     get_state(pz, q, s, &fail);
     primtoflux(G.gam, pz, s, 0, q.g, U);
   }
-#if HARM_CONS_V2
-  flux_update<THREE_D>(Flux{F1, F2, F3, G}, h, i, j, Dt, dU, U);
-#else
-  {
-    Flux FX{F1, F2, F3, G};
-    double f1m[8], f1p[8], f2m[8], f2p[8], f3m[8], f3p[8];
-    zone_fluxes<THREE_D>(FX, h, i, j, f1m, f1p, f2m, f2p, f3m, f3p);
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-#if HARM_STEP_MIXED
-      // reciprocal multiplies in place of the divisions: same sum, last-bit rounding
-      if (THREE_D)
-        U[k] += Dt * (-(f1p[k] - f1m[k]) * idx1 - (f2p[k] - f2m[k]) * idx2 - (f3p[k] - f3m[k]) * idx3 + dU[k]);
-      else
-        U[k] += Dt * (-(f1p[k] - f1m[k]) * idx1 - (f2p[k] - f2m[k]) * idx2 + dU[k]);
-#else
-      if (THREE_D)
-        U[k] += Dt * (-div_rn(f1p[k] - f1m[k], G.dx1, G.idx1) - div_rn(f2p[k] - f2m[k], G.dx2, G.idx2)
-                      - div_rn(f3p[k] - f3m[k], G.dx3, G.idx3) + dU[k]);
-      else
-        U[k] += Dt * (-div_rn(f1p[k] - f1m[k], G.dx1, G.idx1) - div_rn(f2p[k] - f2m[k], G.dx2, G.idx2) + dU[k]);
-#endif
-    }
-  }
-#endif
+  flux_update<THREE_D>(Flux{F1, F2, F3, G}, emf, h, i, j, Dt, dU, U);
 #pragma unroll
   for (int k = 0; k < 8; k++) Ub[k * G.nc + c] = U[k];
   if (fail) record_fail(sc, fail, h + (THREE_D ? 1 : 0), i, j);
@@ -585,12 +585,16 @@ void launch_update(Ctx *x, const double *pi, const double *pb, double *pf, doubl
   Bufs B = bufs(x);
   const dim3 tile(x->tbx, x->tby);
   const dim3 zg = zone_grid_hb(G, tile);
-  if (G.n3 > 1)
+  const dim3 eg(((G.n2 + 1) * (G.n1 + 1) + 127) / 128, 1, G.n3);
+  if (G.n3 > 1) {
+    k_emf<true><<<eg, 128, 0, x->stream>>>(G, B.F1, B.F2, B.F3, x->emf, x->sc);
     k_cons<FULL, true><<<zg, tile, 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn, x->geo32,
-                                                   x->conn32, x->Ubuf, x->sc);
-  else
+                                                   x->conn32, x->emf, x->Ubuf, x->sc);
+  } else {
+    k_emf<false><<<eg, 128, 0, x->stream>>>(G, B.F1, B.F2, B.F3, x->emf, x->sc);
     k_cons<FULL, false><<<zg, tile, 0, x->stream>>>(G, pi, pb, B.F1, B.F2, B.F3, x->geo, x->conn, x->geo32,
-                                                    x->conn32, x->Ubuf, x->sc);
+                                                    x->conn32, x->emf, x->Ubuf, x->sc);
+  }
 #if !HARM_STEP_MIXED
   if (zrec)
     k_invert<true><<<zg, tile, 0, x->stream>>>(G, pi, x->Ubuf, pf, x->pflag, x->geo, x->floors, x->katm, x->sc,
