@@ -625,7 +625,13 @@ def run_profile(args):
     then --steps more; the step kernels of the last steps are the ones to capture
     (each step launches 5 flux/update kernels per half step in 3D: -s 10*warmup)."""
     import harm_cool_b200 as hc
-    pr = hc.torus_problem(args.n1, args.n2, args.n3)
+    if args.member >= 0:
+        # one draw of the ensemble workload (--members, --seed) alone
+        pr, desc = hc.ensemble_problems(args.members, seed=args.seed)[args.member]
+        name = "ensemble member %d of seed %d: %s" % (args.member, args.seed, json.dumps(desc))
+    else:
+        pr = hc.torus_problem(args.n1, args.n2, args.n3)
+        name = "torus %dx%dx%d" % (args.n1, args.n2, args.n3)
     ctx = hc.Context(pr)
     ctx.init_torus()
     if args.precision == "mixed":
@@ -633,7 +639,7 @@ def run_profile(args):
     ctx.run(args.warmup)
     ctx.sync()
     ms = ctx.run_timed(args.steps)
-    print(json.dumps({"workload": "profile case %dx%dx%d %s" % (args.n1, args.n2, args.n3, args.precision),
+    print(json.dumps({"workload": "profile case, %s, %s" % (name, args.precision),
                       "warmup": args.warmup, "steps": args.steps, "ms_per_step": ms / args.steps,
                       "fail_code": ctx.diag()["fail_code"]}), flush=True)
     ctx.close()
@@ -668,6 +674,7 @@ def main():
     ap.add_argument("--adj-steps", type=int, default=50, help="adjoint workload: steps K")
     ap.add_argument("--adj-every", type=int, default=10, help="adjoint workload: checkpoint spacing")
     ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--member", type=int, default=-1, help="profile workload: this ensemble draw alone")
     ap.add_argument("--seed", type=int, default=0)
     args = ap.parse_args()
     if args.warmup < 3:
