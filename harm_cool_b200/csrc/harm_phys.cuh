@@ -68,8 +68,10 @@ constexpr int GEO_N = 21;
 // take the IEEE division; a zero numerator gives a y, the signed zero a/b is.
 __device__ __forceinline__ double div_rn(double a, double b, double y)
 {
-#ifdef HARM_DBG_IEEE_DIV
-  return a / b;
+#if HARM_STEP_MIXED
+  // the mixed-precision step: the reciprocal multiply, within an ulp of a/b
+  // (that step answers for its L1 accuracy against the FP64 step, not for bits)
+  return a * y;
 #endif
   const long long ia = __double_as_longlong(a);
   const unsigned ea = (unsigned)(ia >> 52) & 0x7ffu;
@@ -182,11 +184,7 @@ __device__ __forceinline__ void ucon_calc(const R *pr, const Geo &q, R *ucon, in
   // the reference's pr[U2] - gamma * b2 / alpha with b2 = g^{t theta} alpha^2 = 0*alpha*alpha:
   // gamma * (+0) / alpha is +0 for finite gamma and NaN otherwise, and so is
   // gamma - gamma, which takes two operations instead of a division
-#ifdef HARM_DBG_B2
-  ucon[2] = pr[U2] - gamma * (0. * alpha * alpha) / alpha;
-#else
   ucon[2] = pr[U2] - (gamma - gamma);
-#endif
   ucon[3] = pr[U3] - div_by(gamma * b3, alpha, q.ialpha);
 }
 
