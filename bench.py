@@ -339,7 +339,10 @@ def run_ours(args, world, rank, local):
                          "algorithmic_bytes": alg, "peak_source": peak_kind,
                          "step_frac": zones * STATE_BYTES_PER_ZONE_CYCLE / (ms / args.steps / 1e3) / 1e9 / peak},
             "kernel_ms": kms, "clocks": clocks, "sim_time": ctx.time(), "fail_code": d["fail_code"]}
-    line["roofline"]["fp64"] = fp64_roofline(hc, local, kms, zones, dom, ms / args.steps)
+    line["roofline"]["fp64"] = f64 = fp64_roofline(hc, local, kms, zones, dom, ms / args.steps)
+    # the roofline that binds this FP64 path: the FP64 pipe (HBM is far from busy)
+    line["roofline"]["fp64_frac"] = f64.get("fp64_frac")
+    line["roofline"]["fp64_ceiling_zcps"] = f64.get("fp64_ceiling_zcps")
     act = (slice(1, -1) if args.n3 > 1 else slice(None), slice(2, -2), slice(2, -2))
     if not args.no_mixed:
         ctx.close()
