@@ -198,28 +198,22 @@ __global__ void k_adj_din_bound(Grid G, const double *__restrict__ P, const doub
 // transposes the bound_prim that came before the repairs (the repairs may
 // read ghost cells).  Without a repair the ghosts' adjoint is already zero
 // (the later bound_prim's transpose cleared it), so that bound_prim's
-// transpose has nothing to do either, and the kernel ends after its scan.
+// transpose has nothing to do either: the kernel returns at once when the
+// count of failed zones the recomputed step kept (nfail) is zero.
 
 __global__ void __launch_bounds__(FU_THREADS) k_adj_fixup_bound(Grid G, const double *__restrict__ X1,
                                                                   const signed char *__restrict__ fl1,
                                                                   const double *__restrict__ geo,
                                                                   const double *__restrict__ floors, double *W,
                                                                   signed char *Wf, int *list, double *vbuf,
-                                                                  signed char *kinds, double *lam, int *err)
+                                                                  signed char *kinds, double *lam, int *err,
+                                                                  const int *__restrict__ nfail)
 {
   __shared__ int cnt[FU_THREADS];
   __shared__ int nsh;
   const int tid = threadIdx.x;
-  {
-    // any failed zone at all? (coalesced)
-    int any = 0;
-    const int na = G.n1 * G.n2;
-    for (int t = tid; t < na; t += FU_THREADS) {
-      const int ii = t / G.n2, jj = t - ii * G.n2;
-      any |= fl1[cidx(G, 0, G.istart + ii, G.jstart + jj)] != 0;
-    }
-    if (__syncthreads_or(any) == 0) return;
-  }
+  // the step's fixup_utoprim met no failed zone (its count, kept by the recomputation)
+  if (*nfail == 0) return;
   const long nact = (long)G.n1 * G.n2;
   const long per = (nact + FU_THREADS - 1) / FU_THREADS;
   const long a0 = tid * per, a1 = a0 + per < nact ? a0 + per : nact;
@@ -1128,12 +1122,15 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
   double *recp[2], *recd[2];
   signed char *recf[2];
   DevScalars *recs[2];
+  int *recn[2];
   for (int b = 0; b < 2; b++) {
     recp[b] = B.get<double>(pl * (nrec + 1));
     recd[b] = B.get<double>((size_t)nrec * (7 * pl + 4 * nc));
     recf[b] = B.get<signed char>((size_t)nrec * 4 * nc);
     recs[b] = B.get<DevScalars>((size_t)nrec * 2);
-    if (!recp[b] || !recd[b] || !recf[b] || !recs[b]) return fail_with(HARM_E_CUDA, "device memory for the adjoint");
+    recn[b] = B.get<int>((size_t)nrec * 2);
+    if (!recp[b] || !recd[b] || !recf[b] || !recs[b] || !recn[b])
+      return fail_with(HARM_E_CUDA, "device memory for the adjoint");
   }
   double *lam = B.get<double>(6 * pl);  // next, cur, ph, U, F1, F2
   double *W = B.get<double>(pl);
@@ -1157,6 +1154,7 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       s.fl1[0] = recf[b] + (size_t)r * 4 * nc; s.fl1[1] = s.fl1[0] + nc;
       s.wz[0] = s.fl1[0] + 2 * nc; s.wz[1] = s.fl1[0] + 3 * nc;
       s.sc[0] = recs[b] + 2 * r; s.sc[1] = recs[b] + 2 * r + 1;
+      s.nfail[0] = recn[b] + 2 * r; s.nfail[1] = recn[b] + 2 * r + 1;
     }
   }
   // the adjoint of the state after the step being undone (A) and before it (B)
@@ -1239,7 +1237,7 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       // the corrector's bound_prim, fixup_utoprim, bound_prim, inversion, update, fluxes
       k_adj_din_bound<<<(nbc + 127) / 128, 128, 0, q>>>(G, pnext, x->geo, lnext, sa, sb, as);
       k_adj_fixup_bound<<<1, FU_THREADS, 0, q>>>(G, R.X1[1], R.fl1[1], x->geo, x->floors, W, Wf, list, vbuf, kinds,
-                                                lnext, err);
+                                                lnext, err, R.nfail[1]);
       k_adj_invert<<<zg, tile, 0, q>>>(G, R.Ub[1], R.Z[1], R.wz[1], x->geo, x->floors, x->katm, lnext, lU, lcur,
                                        err);
       CK(cudaMemsetAsync(lF1, 0, 2 * pb, q));
@@ -1260,7 +1258,7 @@ static int run_adjoint(Ctx *x, int nsteps, int every, double *J, double *grad, d
       // predictor, from p^n into ph
       k_adj_bound<<<(nbc + 127) / 128, 128, 0, q>>>(G, R.ph, x->geo, lh);
       k_adj_fixup_bound<<<1, FU_THREADS, 0, q>>>(G, R.X1[0], R.fl1[0], x->geo, x->floors, W, Wf, list, vbuf, kinds,
-                                                lh, err);
+                                                lh, err, R.nfail[0]);
       k_adj_invert<<<zg, tile, 0, q>>>(G, R.Ub[0], R.Z[0], R.wz[0], x->geo, x->floors, x->katm, lh, lU, lcur, err);
       CK(cudaMemsetAsync(lF1, 0, 2 * pb, q));
       k_adj_cons<false><<<zg, tile, 0, q>>>(G, pn, R.Ub[0], R.F1rho[0], x->geo, x->conn, lU, lcur, lF1, lF2, sa,

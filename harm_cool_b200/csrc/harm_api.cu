@@ -514,10 +514,12 @@ int launch_bound(Ctx *x, double *P)
   return HARM_OK;
 }
 
-int launch_fixup_utoprim(Ctx *x, double *P)
+int launch_fixup_utoprim(Ctx *x, double *P, int *nfail_out)
 {
   const Grid &G = x->G;
   k_fu_flip<<<148 * 8, 256, 0, x->stream>>>(G, x->pflag, x->fail_list, x->sc);
+  // the number of failed zones, kept for the discrete adjoint before the repair clears it
+  if (nfail_out) CK(cudaMemcpyAsync(nfail_out, &x->sc->nfail, sizeof(int), cudaMemcpyDeviceToDevice, x->stream));
   k_fu_fix<<<1, NTHR_FIX, 0, x->stream>>>(G, P, x->pflag, x->fail_list, x->fix_buf, x->geo, x->floors, x->sc);
   k_fu_wave<<<G.n3, 256, 0, x->stream>>>(G, P, x->pflag, x->geo, x->floors, x->sc);
   return HARM_OK;

@@ -174,6 +174,7 @@ struct StepRec {
   double *F1rho[2];              // raw radial mass flux [nc] (the no-inflow fix reads its sign)
   double *ctop;                  // the corrector's face wave speeds, directions 1 and 2 [2][nc]
   signed char *fl1[2];           // pflag after the first bound_prim [nc]
+  int *nfail[2];                 // the failed zones fixup_utoprim then met (device int)
   double *ph;                    // the predictor's final state
   DevScalars *sc[2];             // the run state before k_finalize (the corrector's Courant minima) and after
 };
@@ -181,7 +182,7 @@ struct StepRec {
 // kernels shared by both precisions (harm_api.cu)
 int launch_bound(Ctx *x, double *P);
 int get_prims(Ctx *x, const double *src, double *p, signed char *pflag);  // device planes -> host layout
-int launch_fixup_utoprim(Ctx *x, double *P);
+int launch_fixup_utoprim(Ctx *x, double *P, int *nfail_out = nullptr);
 void launch_mass(Ctx *x);
 int sync_status(Ctx *x);
 

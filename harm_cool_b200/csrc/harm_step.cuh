@@ -646,7 +646,7 @@ static void launch_half_rec(Ctx *x, const double *pi, const double *pb, double *
   launch_bound(x, pf);
   cudaMemcpyAsync(r.X1[s], pf, 8 * nc * sizeof(double), cudaMemcpyDeviceToDevice, x->stream);
   cudaMemcpyAsync(r.fl1[s], x->pflag, nc, cudaMemcpyDeviceToDevice, x->stream);
-  launch_fixup_utoprim(x, pf);
+  launch_fixup_utoprim(x, pf, r.nfail[s]);
   launch_bound(x, pf);
 }
 
