@@ -115,6 +115,39 @@ def test_parameter_gradient_against_central_difference():
     np.testing.assert_allclose(g, fd, rtol=0, atol=TOL * scale)
 
 
+def test_rmax_and_beta_gradients_once_the_torus_reaches_the_inner_boundary():
+    """dJ/drmax and dJ/dbeta over a window long enough for the torus's own matter
+    to reach the inner boundary: 64x64 torus, K = 800 steps (t ~ 35 M),
+    checkpoint every 100.  Over the 10 to 50 steps of the other tests only the
+    atmosphere flows in and both are exactly zero.  The central differences are
+    noisy here: the atmosphere sits at its density floor, whose kink a difference
+    straddles in some zones, and the differences spread by about 1e-3 (rmax) and
+    a few percent (beta) between h = 3e-9 and 1e-7.  So the adjoint is checked
+    against the median difference over those steps, to 2e-3 for rmax and 2e-2
+    for beta; beyond about 1500 steps the flow turns chaotic and neither the
+    differences nor the derivative mean anything."""
+    n, K = 64, 800
+    ctx = _context(n, n)
+    modes = ad.Modes(n, n, m=2, seed=0)
+    amps = np.zeros(2)
+    J, g, info = ad.mass_in_gradient(ctx, modes, 12.0, 100.0, amps, K, checkpoint_every=100, rel_step=1e-7)
+    theta = np.array([12.0, 100.0])
+    fd = np.zeros((4, 2))
+    for a, hr in enumerate((1e-7, 3e-8, 1e-8, 3e-9)):
+        for k in range(2):
+            h = hr * theta[k]
+            tp, tm = theta.copy(), theta.copy()
+            tp[k] += h
+            tm[k] -= h
+            fd[a, k] = (ad.mass_in(ctx, modes, tp[0], tp[1], amps, K) - ad.mass_in(ctx, modes, tm[0], tm[1], amps, K)) / (2 * h)
+    med = np.median(fd, axis=0)
+    print("K = %d: adjoint dJ/drmax %.6e dJ/dbeta %.6e; central differences" % (K, g[0], g[1]), fd.tolist())
+    # clearly non-zero: the torus's matter reaches the boundary within the window
+    assert abs(med[0]) > 1e-5 and abs(med[1]) > 1e-9
+    assert abs(g[0] - med[0]) <= 2e-3 * abs(med[0]), (g[0], med[0])
+    assert abs(g[1] - med[1]) <= 2e-2 * abs(med[1]), (g[1], med[1])
+
+
 def test_against_reference_central_differences():
     """dJ/dA_m against central differences taken on the reference's own step
     (32x32 torus, 10 steps; fixture written by make_golden.py)"""
