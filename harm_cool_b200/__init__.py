@@ -175,6 +175,12 @@ _SIGNATURES = {
     "harm_fp64_peak": (ctypes.c_int, [ctypes.c_int, _DP]),
     "harm_div_check": (ctypes.c_int, [ctypes.c_int, ctypes.c_long, ctypes.c_ulonglong,
                                       ctypes.POINTER(ctypes.c_ulonglong)]),
+    "harm_nu_rules": (ctypes.c_int, [_DP]),
+    "harm_nu_fermi": (ctypes.c_int, [_DP, _DP, ctypes.c_long, _DP]),
+    "harm_nu_abundance": (ctypes.c_int, [_DP, _DP, _DP, ctypes.c_long, ctypes.c_int, _DP]),
+    "harm_nu_abundance_dev": (ctypes.c_int, [ctypes.c_int, _DP, _DP, _DP, ctypes.c_long, _DP]),
+    "harm_nu_tables": (ctypes.c_int, [ctypes.c_int, _DP, ctypes.c_int, _DP, ctypes.c_int, _DP, ctypes.c_int,
+                                      ctypes.c_long, _DP, ctypes.POINTER(ctypes.c_float)]),
 }
 
 
@@ -232,6 +238,53 @@ def div_check(n, seed=1, device=0):
     c = (ctypes.c_ulonglong * 2)()
     _check(library().harm_div_check(device, n, seed, c))
     return int(c[0]), int(c[1])
+
+
+def nu_rules():
+    """The quadrature rules of the COOL_EOS generator: 20- and 40-point
+    Gauss-Legendre (positive abscissae, weights) and 20-point Gauss-Laguerre
+    (abscissae, weights times e^x)."""
+    out = np.zeros(100)
+    _check(library().harm_nu_rules(_dp(out)))
+    return {"l20": (out[0:10], out[10:20]), "l40": (out[20:40], out[40:60]), "g20": (out[60:80], out[80:100])}
+
+
+def nu_fermi(eta, theta):
+    """F_k(eta, theta) for k = 1/2, 3/2, 5/2, 7/2 (host): shape (n, 4)."""
+    eta = np.ascontiguousarray(eta, dtype=np.float64).ravel()
+    theta = np.ascontiguousarray(np.broadcast_to(theta, eta.shape), dtype=np.float64)
+    F = np.zeros((len(eta), 4))
+    _check(library().harm_nu_fermi(_dp(eta), _dp(theta), len(eta), _dp(F)))
+    return F
+
+
+_NU_FIELDS = ("e", "p", "qnu", "tau", "nee", "nep", "xp")
+
+
+def nu_abundance(rho, T, hdfac, threads=0, device=None):
+    """abundance() at the given nodes, on the host's cores (device None) or on a
+    GPU: a dict of arrays e, p (erg/cm^3), qnu (erg/cm^2/s), tau, nee, nep
+    (fm^-3) and xp (proton fraction of the free nucleons)."""
+    rho, T, hdfac = (np.ascontiguousarray(a, dtype=np.float64).ravel() for a in np.broadcast_arrays(rho, T, hdfac))
+    out = np.zeros((len(rho), 7))
+    if device is None:
+        _check(library().harm_nu_abundance(_dp(rho), _dp(T), _dp(hdfac), len(rho), threads, _dp(out)))
+    else:
+        _check(library().harm_nu_abundance_dev(device, _dp(rho), _dp(T), _dp(hdfac), len(rho), _dp(out)))
+    return {k: out[:, i].copy() for i, k in enumerate(_NU_FIELDS)}
+
+
+def nu_tables(xaxis, yaxis, hdfac, device=0, slice_nodes=0):
+    """Every node of the per-radius tables on the GPU: values[ntab][nx][ny][5]
+    (e, p, Qnu, tau, Yee) and the build's device time in ms."""
+    xaxis = np.ascontiguousarray(xaxis, dtype=np.float64)
+    yaxis = np.ascontiguousarray(yaxis, dtype=np.float64)
+    hdfac = np.ascontiguousarray(hdfac, dtype=np.float64)
+    val = np.zeros((len(hdfac), len(xaxis), len(yaxis), 5))
+    ms = ctypes.c_float(0.)
+    _check(library().harm_nu_tables(device, _dp(xaxis), len(xaxis), _dp(yaxis), len(yaxis), _dp(hdfac), len(hdfac),
+                                     slice_nodes, _dp(val), ctypes.byref(ms)))
+    return val, ms.value
 
 
 def _check(rc):

@@ -59,7 +59,11 @@ UNITS = {
     "harm_dump.cu": ["-fmad=false"],     # the ASCII dump format
     "harm_adjoint.cu": ["-fmad=false"],  # the discrete adjoint (values identical to the step's)
     "harm_peak.cu": ["-fmad=false"],     # measured FP64 pipe rates (roofline denominators)
+    "harm_nu.cu": ["-fmad=false"],       # COOL_EOS table generator on the device
 }
+
+# host-only units, compiled by g++ with the reference's -O2 and no contraction
+HOST_UNITS = ["host_setup.cpp", "harm_nu_host.cpp"]
 
 
 def build(force=False, verbose=False):
@@ -69,10 +73,12 @@ def build(force=False, verbose=False):
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     inc = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
-    host_o = os.path.join(BUILD, "host_setup.o")
-    _run(["g++", "-O2", "-ffp-contract=off", "-fPIC", "-std=c++17", "-c",
-          os.path.join(CSRC, "host_setup.cpp"), "-o", host_o] + inc)
-    objs = [host_o]
+    objs = []
+    for unit in HOST_UNITS:
+        host_o = os.path.join(BUILD, unit.replace(".cpp", ".o"))
+        _run(["g++", "-O2", "-ffp-contract=off", "-fPIC", "-std=c++17", "-c",
+              os.path.join(CSRC, unit), "-o", host_o] + inc)
+        objs.append(host_o)
 
     # a unit is recompiled when its object is older than the unit or any header it includes
     def compile_unit(item):
@@ -94,7 +100,7 @@ def build(force=False, verbose=False):
                 print(out)
             objs.append(o)
     tmp = LIB + ".tmp"
-    _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"])
+    _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart", "-lpthread"])
     os.replace(tmp, LIB)
     return LIB
 

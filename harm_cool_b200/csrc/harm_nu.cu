@@ -1,0 +1,186 @@
+// The COOL_EOS table generator on the device: abundance() (harm_nu.cuh) at
+// every node of the per-radius (rho, T) tables, one thread per node.
+//
+// The reference fills the same tables lazily on the host, node by node, with
+// six worker threads calling its Fortran abundance_() (cooleos.c:171-194,
+// 805-820; cache4d.c) and caches them in files.  Here every node of every
+// table is computed in one pass before the run: the nodes are independent,
+// each a nest of Newton solves over Fermi integrals in FP64, which is
+// latency-bound scalar work that the 148 SMs run side by side.
+//
+// The cost of a node varies by four orders of magnitude, with the
+// temperature above all: where free nucleons are a trace (T of a few 1e8 K)
+// the proton-fraction solve runs all 200 of its trials, each over three
+// nested solves.  So a warp holds the nodes of one temperature (the density
+// varies across its lanes), and the tables are launched one per kernel over
+// several streams without waiting in between: the blocks of a table still
+// running on its slowest nodes share the SMs with the next tables' blocks.
+// Every loop in the physics has a fixed trip count or the 200-trial cap of
+// the Newton solver, so every thread ends.
+#include "harm_b200.h"
+#include "harm_common.cuh"
+#include "harm_nu.cuh"
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+namespace harm {
+namespace nu {
+const Rules *host_rules();
+
+__constant__ Rules c_rules;
+
+// node k of the slice [k0, k0 + n), with k = (t ny + j) nx + i for table t,
+// T index j and rho index i; values packed as calc_cache_val packs them
+// (cooleos.c:171-194) at values[t][i][j]: e, p, Qnu, tau,
+// Yee = (n_e- - n_e+) / n_b
+__global__ void __launch_bounds__(128) k_tables(const double *xaxis, int nx, const double *yaxis, int ny,
+                                                const double *hdfac, long k0, long n, double *values)
+{
+  const long k = k0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= k0 + n) return;
+  const int i = (int)(k % nx);
+  const long tj = k / nx;
+  const int j = (int)(tj % ny), t = (int)(tj / ny);
+  const double rho = xaxis[i];
+  const Abundance a = abundance(c_rules, rho, yaxis[j], hdfac[t]);
+  double *v = values + 5 * (((long)t * nx + i) * ny + j);
+  v[0] = a.e;
+  v[1] = a.p;
+  v[2] = a.qnu;
+  v[3] = a.tau;
+  v[4] = (a.nee - a.nep) / (rho / 1.66e15);
+}
+
+// abundance() at a list of nodes, for checks against the host
+__global__ void __launch_bounds__(128) k_nodes(const double *rho, const double *T, const double *hdfac, long n,
+                                               double *out)
+{
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const Abundance a = abundance(c_rules, rho[k], T[k], hdfac[k]);
+  double *o = out + 7 * k;
+  o[0] = a.e;
+  o[1] = a.p;
+  o[2] = a.qnu;
+  o[3] = a.tau;
+  o[4] = a.nee;
+  o[5] = a.nep;
+  o[6] = a.xp;
+}
+
+static int upload_rules(int device)
+{
+  static int done[64];
+  if (device < 0 || device >= 64) return fail_with(HARM_E_ARG, "harm_nu: bad device");
+  if (done[device]) return HARM_OK;
+  const Rules *R = host_rules();
+  if (!R) return fail_with(HARM_E_ARG, "harm_nu: quadrature root search failed");
+  CK(cudaMemcpyToSymbol(c_rules, R, sizeof(Rules)));
+  done[device] = 1;
+  return HARM_OK;
+}
+
+// device buffers freed on every return path
+struct DevBufs {
+  std::vector<void *> p;
+  ~DevBufs()
+  {
+    for (void *q : p) cudaFree(q);
+  }
+  template <class T>
+  cudaError_t alloc(T **ptr, size_t count)
+  {
+    void *q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+    if (e == cudaSuccess) p.push_back(q);
+    *ptr = (T *)q;
+    return e;
+  }
+};
+
+}  // namespace nu
+}  // namespace harm
+
+using namespace harm;
+
+extern "C" int harm_nu_tables(int device, const double *xaxis, int nx, const double *yaxis, int ny,
+                              const double *hdfac, int ntab, long slice, double *values, float *ms)
+{
+  if (nx <= 0 || ny <= 0 || ntab <= 0 || !xaxis || !yaxis || !hdfac || !values)
+    return fail_with(HARM_E_ARG, "harm_nu_tables: bad arguments");
+  CK(cudaSetDevice(device));
+  int rc = nu::upload_rules(device);
+  if (rc != HARM_OK) return rc;
+  const long n = (long)nx * ny * ntab;
+  if (slice <= 0) slice = (long)nx * ny;  // a table per launch
+  nu::DevBufs b;
+  double *dx, *dy, *dh, *dv;
+  CK(b.alloc(&dx, nx));
+  CK(b.alloc(&dy, ny));
+  CK(b.alloc(&dh, ntab));
+  CK(b.alloc(&dv, 5 * n));
+  CK(cudaMemcpy(dx, xaxis, nx * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dy, yaxis, ny * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dh, hdfac, ntab * sizeof(double), cudaMemcpyHostToDevice));
+  // slices on NS streams, each stream's first slice after e0 and e1 after
+  // every stream's last
+  const int NS = 8;
+  cudaStream_t st[NS];
+  cudaEvent_t e0, e1, done[NS];
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  for (int s = 0; s < NS; s++) {
+    CK(cudaStreamCreateWithFlags(&st[s], cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&done[s], cudaEventDisableTiming));
+  }
+  CK(cudaDeviceSynchronize());
+  CK(cudaEventRecord(e0, st[0]));
+  for (int s = 1; s < NS; s++) CK(cudaStreamWaitEvent(st[s], e0, 0));
+  int q = 0;
+  for (long k0 = 0; k0 < n; k0 += slice, q = (q + 1) % NS) {
+    const long m = (n - k0 < slice) ? n - k0 : slice;
+    nu::k_tables<<<(unsigned)((m + 127) / 128), 128, 0, st[q]>>>(dx, nx, dy, ny, dh, k0, m, dv);
+    CK(cudaGetLastError());
+  }
+  for (int s = 1; s < NS; s++) {
+    CK(cudaEventRecord(done[s], st[s]));
+    CK(cudaStreamWaitEvent(st[0], done[s], 0));
+  }
+  CK(cudaEventRecord(e1, st[0]));
+  CK(cudaEventSynchronize(e1));
+  float t = 0.f;
+  CK(cudaEventElapsedTime(&t, e0, e1));
+  if (ms) *ms = t;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (int s = 0; s < NS; s++) {
+    cudaEventDestroy(done[s]);
+    cudaStreamDestroy(st[s]);
+  }
+  CK(cudaMemcpy(values, dv, 5 * n * sizeof(double), cudaMemcpyDeviceToHost));
+  return HARM_OK;
+}
+
+extern "C" int harm_nu_abundance_dev(int device, const double *rho, const double *T, const double *hdfac, long n,
+                                     double *out)
+{
+  if (n <= 0 || !rho || !T || !hdfac || !out) return fail_with(HARM_E_ARG, "harm_nu_abundance_dev: bad arguments");
+  CK(cudaSetDevice(device));
+  int rc = nu::upload_rules(device);
+  if (rc != HARM_OK) return rc;
+  nu::DevBufs b;
+  double *dr, *dt, *dh, *dout;
+  CK(b.alloc(&dr, n));
+  CK(b.alloc(&dt, n));
+  CK(b.alloc(&dh, n));
+  CK(b.alloc(&dout, 7 * n));
+  CK(cudaMemcpy(dr, rho, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dt, T, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dh, hdfac, n * sizeof(double), cudaMemcpyHostToDevice));
+  nu::k_nodes<<<(unsigned)((n + 127) / 128), 128>>>(dr, dt, dh, n, dout);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(out, dout, 7 * n * sizeof(double), cudaMemcpyDeviceToHost));
+  return HARM_OK;
+}

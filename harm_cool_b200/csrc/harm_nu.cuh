@@ -1,0 +1,627 @@
+// The equation of state and neutrino rates behind HARM-COOL's COOL_EOS
+// tables: nucleons, electron-positron pairs, helium, radiation and trapped
+// neutrinos in beta equilibrium, at a given baryon density, temperature and
+// disc scale-height factor.  A restatement of the reference's Fortran table
+// generator, abundance() (abundance.f90:6-243), and of the routines it
+// calls, written once for the host and the device:
+//
+//   abundance.f90:6-243       abundance()        node values e, p, Qnu, tau, n_e-, n_e+
+//   chem_eq.f90:49-191        chem_eq, eqnucl, nuclear, funcnb, neutrino
+//   chem_eq.f90:193-431       the rate integrands func1k .. func3r
+//   chem_eq.f90:433-490       rtbis_funcnb (Newton on funcnb)
+//   number_den.f90:26-397     fxnn, fxnp, neta, peta, eeta, lepton
+//   eos.f90:32-183            eos_npe, eos_rad, eos_neu, eos_he
+//   accretion.f90:24-117      xnuc, h_dep, opt_dep, b_neu
+//   neu_rate.f90:30-261       pair, urca, func1 .. func3, brem, plasmon
+//   gauss_integral.f90:26-219 the 40-point Gauss-Legendre and 20-point
+//                             Gauss-Laguerre rules of the rate integrals
+//   gauss_integral.f90:241-438 dfermi and its integrands
+//   mnewtf.f90:94-150         mnewt, for one unknown
+//
+// Units are the reference's: densities in fm^-3, energies and temperatures
+// in MeV, until abundance() converts e and p to erg cm^-3.
+//
+// Fidelity.  The reference is gfortran code; no Fortran compiler exists
+// here, so this restatement is not compared with its output.  It keeps the
+// reference's formulae, their order of operations and its constants, and
+// three properties of the Fortran that move results at the 1e-8 level:
+//  - literals written without a kind (3.1415926535897932, 197.3269718e0,
+//    5.6e-5, 0.557, 13.8, 2.0/3.0, 1./3.) are single precision in Fortran;
+//    they appear here as float literals (HNU_F);
+//  - arguments pass by reference: h_dep() scales its caller's p and e, and
+//    opt_dep() zeroes its caller's b1 before b_neu() sets it again;
+//  - mnewt() with one unknown: a zero or NaN derivative skips the solve and
+//    steps by the residual itself (ludcmp's singular branch).
+// Integer powers are products and x**1.5-style powers are pow(); the
+// Fermi-integral kernels take x^k as x^(k-1/2) sqrt(x), and compute the four
+// indices of one (eta, theta) in one pass over the nodes (the breakpoints
+// depend on eta alone).  These change results in the last bits only.
+#pragma once
+
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define HNU __host__ __device__ __forceinline__
+#define HNU_NOINLINE static __host__ __device__ __noinline__
+#else
+#define HNU inline
+#define HNU_NOINLINE static
+#endif
+
+// a Fortran default-real literal, as the real(8) value it converts to
+#define HNU_F(x) ((double)(x##f))
+
+namespace harm {
+namespace nu {
+
+// const_mod.f90
+constexpr double PI = HNU_F(3.1415926535897932);
+constexpr double HC = HNU_F(197.3269718);  // MeV fm
+constexpr double SIGMASB = HNU_F(5.6e-5);
+constexpr double XME = 0.510998910, XMP = 938.272013, XMN = 939.56536;  // MeV
+
+// Quadrature rules.  Abscissae and weights are computed on the host by
+// harm_nu_rules() (harm_nu.cu) from the definitions of the rules; the
+// Gauss-Laguerre weights carry the factor e^x, as the integrands include the
+// weight function.
+struct Rules {
+  double l20x[10], l20w[10];  // 20-point Gauss-Legendre on (-1, 1): positive abscissae
+  double l40x[20], l40w[20];  // 40-point Gauss-Legendre on (-1, 1): positive abscissae
+  double g20x[20], g20w[20];  // 20-point Gauss-Laguerre on (0, inf)
+};
+
+HNU double sq(double x) { return x * x; }
+HNU double cube(double x) { return x * x * x; }
+
+// ---------------------------------------------------------------------------
+// Generalised Fermi-Dirac integrals
+//   F_k(eta, theta) = int_0^inf x^k sqrt(1 + theta x / 2) / (e^(x - eta) + 1) dx
+// for k = 1/2, 3/2, 5/2, 7/2, by Aparicio's four-interval quadrature (ApJS 117,
+// 627, 1998) as in dfermi (gauss_integral.f90:241-349): 20-point
+// Gauss-Legendre on [0, sqrt(s1)] in z = sqrt(x), on [s1, s2] and [s2, s3], and
+// 20-point Gauss-Laguerre on [s3, inf), with breakpoints that follow eta.
+// F[m] = F_{m + 1/2} for m < nk.
+// ---------------------------------------------------------------------------
+
+// the integrand without its power of x (fdfunc1, gauss_integral.f90:354-393)
+HNU double fd_kernel(double x, double eta, double theta)
+{
+  const double dxst = sqrt(1.0 + 0.5 * x * theta);
+  if (x - eta < 1.0e2) return dxst / (exp(x - eta) + 1.0);
+  return dxst * exp(eta - x);
+}
+
+// nk indices at one node of the x integrals: x^(1/2), x^(3/2), ...
+HNU void fd_add_x(double x, double w, double eta, double theta, int nk, double *acc)
+{
+  double xk = sqrt(x);
+  const double g = fd_kernel(x, eta, theta);
+  for (int m = 0; m < nk; m++) {
+    acc[m] += xk * g * w;
+    xk *= x;
+  }
+}
+
+// the z = sqrt(x) integrand (fdfunc2, gauss_integral.f90:398-438): 2 z^(2k+1) ...
+HNU void fd_add_z(double z, double w, double eta, double theta, int nk, double *acc)
+{
+  const double zsq = z * z;
+  const double dxst = sqrt(1.0 + 0.5 * zsq * theta);
+  const double g = (zsq - eta < 1.0e2) ? dxst / (exp(zsq - eta) + 1.0) : dxst * exp(eta - zsq);
+  double zk = zsq;  // z^(2k+1), k = 1/2
+  for (int m = 0; m < nk; m++) {
+    acc[m] += 2.0 * zk * g * w;
+    zk *= zsq;
+  }
+}
+
+HNU void fermi(const Rules &R, double eta, double theta, int nk, double *F)
+{
+  // breakpoint fit of Aparicio (1998)
+  const double d = 3.3609, sg = 9.1186e-2;
+  const double a1 = 6.7774, b1 = 1.1418, c1 = 2.9826;
+  const double a2 = 3.7601, b2 = 9.3719e-2, c2 = 2.1063e-2, d2 = 3.1084e1, e2 = 1.0056;
+  const double a3 = 7.5669, b3 = 1.1695, c3 = 7.5416e-1, d3 = 6.6558, e3 = -1.2819e-1;
+  const double eta1 = sg * (eta - d);
+  const double xi = (eta1 <= 5.0e1) ? log(1.0 + exp(eta1)) / sg : eta - d;
+  const double xi2 = xi * xi;
+  const double x1 = (a1 + b1 * xi + c1 * xi2) / (1.0 + c1 * xi);
+  const double x2 = (a2 + b2 * xi + c2 * d2 * xi2) / (1.0 + e2 * xi + c2 * xi2);
+  const double x3 = (a3 + b3 * xi + c3 * d3 * xi2) / (1.0 + e3 * xi + c3 * xi2);
+  const double s1 = x1 - x2, s2 = x1, s3 = x1 + x3, s12 = sqrt(s1);
+
+  double r1[4] = {0., 0., 0., 0.}, r2[4] = {0., 0., 0., 0.}, r3[4] = {0., 0., 0., 0.}, r4[4] = {0., 0., 0., 0.};
+  // the three Gauss-Legendre pieces (dqleg020): sums of node pairs, then the half-length
+  {
+    const double c = 0.5 * s12, h = 0.5 * s12;
+    for (int j = 0; j < 10; j++) {
+      double p[4] = {0., 0., 0., 0.};
+      fd_add_z(c + h * R.l20x[j], 1.0, eta, theta, nk, p);
+      fd_add_z(c - h * R.l20x[j], 1.0, eta, theta, nk, p);
+      for (int m = 0; m < nk; m++) r1[m] += p[m] * R.l20w[j];
+    }
+    for (int m = 0; m < nk; m++) r1[m] *= h;
+  }
+  {
+    const double c = 0.5 * (s1 + s2), h = 0.5 * (s2 - s1);
+    for (int j = 0; j < 10; j++) {
+      double p[4] = {0., 0., 0., 0.};
+      fd_add_x(c + h * R.l20x[j], 1.0, eta, theta, nk, p);
+      fd_add_x(c - h * R.l20x[j], 1.0, eta, theta, nk, p);
+      for (int m = 0; m < nk; m++) r2[m] += p[m] * R.l20w[j];
+    }
+    for (int m = 0; m < nk; m++) r2[m] *= h;
+  }
+  {
+    const double c = 0.5 * (s2 + s3), h = 0.5 * (s3 - s2);
+    for (int j = 0; j < 10; j++) {
+      double p[4] = {0., 0., 0., 0.};
+      fd_add_x(c + h * R.l20x[j], 1.0, eta, theta, nk, p);
+      fd_add_x(c - h * R.l20x[j], 1.0, eta, theta, nk, p);
+      for (int m = 0; m < nk; m++) r3[m] += p[m] * R.l20w[j];
+    }
+    for (int m = 0; m < nk; m++) r3[m] *= h;
+  }
+  // the Gauss-Laguerre tail (dqlag020) on [s3, inf), scale 1
+  for (int j = 0; j < 20; j++) fd_add_x(s3 + R.g20x[j], R.g20w[j], eta, theta, nk, r4);
+  for (int m = 0; m < nk; m++) F[m] = r1[m] + r2[m] + r3[m] + r4[m];
+}
+
+// ---------------------------------------------------------------------------
+// Number densities (number_den.f90)
+// ---------------------------------------------------------------------------
+
+// n = c (F_1/2 + beta F_3/2), c = sqrt2/pi^2 (m/hc)^3 beta^1.5: free fermions of
+// mass m (MeV) at temperature kt and degeneracy eta (eq. 20; fxnn, fxnp)
+HNU double fermion_density(const Rules &R, double m, double kt, double eta)
+{
+  const double beta = kt / m;
+  const double c = sqrt(2.0) / sq(PI) * cube(m / HC) * pow(beta, 1.5);
+  double F[2];
+  fermi(R, eta, beta, 2, F);
+  return c * (F[0] + beta * F[1]);
+}
+
+// electrons and positrons at electron degeneracy etae (lepton, number_den.f90:374-395):
+// returns n_e- - n_e+
+HNU double lepton(const Rules &R, double kt, double etae, double *nee, double *nep)
+{
+  const double beta = kt / XME;
+  const double c = sqrt(2.0) / sq(PI) * cube(XME / HC) * pow(beta, 1.5);
+  double F[2];
+  fermi(R, etae, beta, 2, F);
+  *nee = c * (F[0] + beta * F[1]);
+  fermi(R, -etae - 2.0 / beta, beta, 2, F);
+  *nep = c * (F[0] + beta * F[1]);
+  return *nee - *nep;
+}
+
+// mnewt (mnewtf.f90:108-150) with one unknown and the central-difference
+// Jacobian of the usrfun_* routines: solve G(x) = target from x, up to 200
+// trials, stopping when |G(x) - target| <= tolf or the step is <= 1e-20.
+// G is a functor double(double).
+template <class G>
+HNU double newton1(const G &g, double x, double target, double tolf)
+{
+  for (int k = 0; k < 200; k++) {
+    double xacc = fabs(x) * 1.0e-8;
+    if (xacc < 1.0e-50) xacc = 1.0e-50;
+    const double f = target - g(x);
+    const double fp = target - g(x + xacc);
+    const double fm = target - g(x - xacc);
+    const double fjac = (fp - fm) / (2.0 * xacc);
+    double dx = -f;
+    if (fabs(dx) <= tolf) return x;
+    if (fabs(fjac) > 0.) dx = dx / fjac;  // else ludcmp finds it singular: the step is the residual
+    const double xn = x + dx;
+    if (fabs(dx) <= 1.0e-20) return xn;
+    // x is the whole state of the iteration: once a step leaves it unchanged,
+    // every later trial repeats that step, and the 200th returns this x
+    if (xn == x && signbit(xn) == signbit(x)) return x;
+    x = xn;
+  }
+  return x;
+}
+
+HNU double newton_tol(double n)
+{
+  const double tol = 1.0e-8 * n;
+  return tol < 1.0e-50 ? 1.0e-50 : tol;
+}
+
+struct FermionN {
+  const Rules &R;
+  double m, kt;
+  HNU double operator()(double eta) const { return fermion_density(R, m, kt, eta); }
+};
+struct LeptonN {
+  const Rules &R;
+  double kt;
+  HNU double operator()(double eta) const
+  {
+    double a, b;
+    return lepton(R, kt, eta, &a, &b);
+  }
+};
+
+// degeneracy of neutrons and protons of density n (neta, peta): Newton from -10
+HNU double neta(const Rules &R, double kt, double n) { return newton1(FermionN{R, XMN, kt}, -10.0, n, newton_tol(n)); }
+HNU double peta(const Rules &R, double kt, double n) { return newton1(FermionN{R, XMP, kt}, -10.0, n, newton_tol(n)); }
+
+// electron degeneracy for the net lepton density n (eeta): Newton from m_e/kt,
+// capped at 0
+HNU double eeta(const Rules &R, double kt, double n)
+{
+  const double e = newton1(LeptonN{R, kt}, 0.510998910 / kt, n, newton_tol(n));
+  return e > 0.0 ? 0.0 : e;
+}
+
+// ---------------------------------------------------------------------------
+// Equations of state (eos.f90), e and p in MeV fm^-3
+// ---------------------------------------------------------------------------
+
+// one fermion species (eos_npe's blocks): p = cp (F_3/2 + beta/2 F_5/2),
+// e = 3/2 cp (F_3/2 + beta F_5/2), cp = 2/3 sqrt2/pi^2 (m/hc)^3 m beta^2.5
+HNU void fermion_ep(const Rules &R, double m, double kt, double eta, double *e, double *p)
+{
+  const double beta = kt / m;
+  const double cp = (double)(2.0f / 3.0f) * sqrt(2.0) / sq(PI) * cube(m / HC) * m * pow(beta, 2.5);
+  const double ce = 3.0 / 2.0 * cp;
+  double F[3];
+  fermi(R, eta, beta, 3, F);  // F_1/2 is computed and unused
+  *p = cp * (F[1] + 0.5 * beta * F[2]);
+  *e = ce * (F[1] + beta * F[2]);
+}
+
+// nucleons and pairs (eos_npe, eos.f90:32-112); the positrons count only where
+// the electron density is positive
+HNU void eos_npe(const Rules &R, double kt, double etan, double etap, double etae, double nee, double *e,
+                 double *p)
+{
+  double ee, pe, eep = 0., pep = 0., epr, ppr, en, pn;
+  fermion_ep(R, XME, kt, etae, &ee, &pe);
+  if (nee > 0.0) fermion_ep(R, XME, kt, -etae - 2.0 / (kt / XME), &eep, &pep);
+  fermion_ep(R, XMP, kt, etap, &epr, &ppr);
+  fermion_ep(R, XMN, kt, etan, &en, &pn);
+  *p = pe + pep + ppr + pn;
+  *e = ee + eep + epr + en;
+}
+
+// black-body radiation (eos_rad) and trapped neutrinos with blocking b1, b2 (eos_neu)
+HNU double p_rad(double kt) { return PI * PI / 15.0 * kt * cube(kt / HC) / 3.0; }
+HNU double p_neu(double kt, double b1, double b2)
+{
+  return 7.0 / 8.0 * (b1 + b2) * PI * PI / 15.0 * kt * cube(kt / HC) / 3.0;
+}
+
+// helium nuclei as an ideal gas, dropped where the Sackur-Tetrode entropy is
+// not positive (eos_he)
+HNU void eos_he(double kt, double nhe, double *e, double *p)
+{
+  *e = *p = 0.0;
+  if (nhe <= 0.0) return;
+  const double mhe = 3755.6740;
+  const double s = nhe * (2.5 + 1.5 * log(mhe * kt / sq(HC) / 2.0 / PI) - log(nhe));
+  if (s <= 0.0) return;
+  *e = 1.5 * nhe * kt;
+  *p = nhe * kt;
+}
+
+// ---------------------------------------------------------------------------
+// The disc (accretion.f90)
+// ---------------------------------------------------------------------------
+
+// mass fraction of free nucleons (Popham et al. 1999) (xnuc)
+HNU double xnuc(double nb, double kt)
+{
+  const double rho10 = nb * 1.66e5;
+  const double t11 = kt * 1.16059e-1;
+  double x = 295.5 / pow(rho10, 0.75) * pow(t11, 1.125) * exp(-0.8209 / t11);
+  if (x > 1.0) x = 1.0;
+  if (x < 0.0) x = 0.0;
+  return x;
+}
+
+// scale height HdFac * c_s (h_dep); p and e come back in erg cm^-3, as the
+// Fortran routine rescales its caller's arguments
+HNU double h_dep(double hdfac, double nb, double &p, double &e)
+{
+  const double CC = 2.99792458e10;
+  const double rho = nb * 1.66e15;
+  p = p * 1.6021772e33;
+  e = e * 1.6021772e33;
+  double cs = CC * sqrt(p / (rho * CC * CC + e));
+  if (cs > CC) cs = CC;
+  return hdfac * cs;
+}
+
+// ---------------------------------------------------------------------------
+// Neutrino emissivities, erg cm^-3 s^-1 (neu_rate.f90)
+// ---------------------------------------------------------------------------
+
+// e+ e- annihilation into electron and into mu (= tau) neutrinos (pair)
+HNU void pair(const Rules &R, double kt, double etae, double *ev1, double *ev2)
+{
+  const double QC = 1.023e23;
+  const double beta = kt / 0.510998910;
+  double cv = 2.0 * 0.23 + 0.5, ca = 0.5;
+  const double cv1e = cv * cv + ca * ca, cv2e = cv * cv - ca * ca;
+  cv = 2.0 * 0.23 - 0.5;
+  ca = -0.5;
+  const double cv1m = cv * cv + ca * ca, cv2m = cv * cv - ca * ca;
+  double F[4];
+  fermi(R, etae, beta, 4, F);
+  const double u_1 = F[0], u0 = F[0] + beta * F[1], u1 = F[0] + 2.0 * beta * F[1] + beta * beta * F[2];
+  const double u2 = F[0] + 3.0 * beta * F[1] + 3.0 * beta * beta * F[2] + cube(beta) * F[3];
+  fermi(R, -etae - 2.0 / beta, beta, 4, F);
+  const double f_1 = F[0], f0 = F[0] + beta * F[1], f1 = F[0] + 2.0 * beta * F[1] + beta * beta * F[2];
+  const double f2 = F[0] + 3.0 * beta * F[1] + 3.0 * beta * beta * F[2] + cube(beta) * F[3];
+  const double a = 8.0 * (f1 * u2 + f2 * u1) - 2.0 * (f_1 * u2 + f2 * u_1) + 7.0 * (f0 * u1 + f1 * u0) +
+                   5.0 * (f0 * u_1 + f_1 * u0);
+  const double b = f0 * (u1 + u_1) + (f_1 + f1) * u0;
+  const double pre = QC / (36.0 * PI) * (2.0 / (sq(PI) * sq(PI))) * cube(beta);
+  *ev1 = pre * (cv1e * a + 9.0 * cv2e * b);
+  *ev2 = pre * (cv1m * a + 9.0 * cv2m * b);
+}
+
+// The six weak rates of an integrand family: x sqrt(x^2 - 1/beta^2) (q -+ x)^n
+// times a lepton occupation and a neutrino blocking factor, over the electron
+// energy x in units of kt.  K selects the reaction: 1 n -> p e nu~ on [1/beta, q];
+// 2 p e- -> n nu and 3 n e+ -> p nu~ on [x0, inf).  KIND 0: |1 - b1 f| blocking
+// (func1..3, func1k..3k); 1: |b1 f| absorption (func1r..3r).
+template <int K, int KIND, int POW>
+struct Rate {
+  double kt, eta, b1;
+  HNU double operator()(double x) const
+  {
+    const double beta = kt / XME;
+    const double q = (XMN - XMP) / kt;
+    double xe, en;
+    if (K == 1) {
+      xe = KIND == 0 ? eta - (x - 1.0 / beta) : (x - 1.0 / beta) - eta;
+      en = q - x;
+    } else if (K == 2) {
+      xe = KIND == 0 ? -eta + (x - 1.0 / beta) : +eta - (x - 1.0 / beta);
+      en = x - q;
+    } else {
+      xe = KIND == 0 ? -eta + (x - 1.0 / beta) : eta - (x - 1.0 / beta);
+      en = x + q;
+    }
+    const double f1 = 1.0 / (exp(xe) + 1.0);
+    const double ex = K == 1 ? exp(q - x) : (K == 2 ? exp(x - q) : exp(x + q));
+    const double f2 = KIND == 0 ? fabs(1.0 - b1 / (ex + 1.0)) : fabs(b1 / (ex + 1.0));
+    const double enp = POW == 3 ? en * en * en : en * en;
+    return x * sqrt(x * x - 1.0 / (beta * beta)) * enp * f1 * f2;
+  }
+};
+
+// 40-point Gauss-Legendre on [a, b] (gauss_legendre, gauss_integral.f90:118-219)
+template <class Fn>
+HNU double legendre40(const Rules &R, const Fn &f, double a, double b)
+{
+  const double c = 0.5 * (a + b), h = 0.5 * (b - a);
+  double s = 0.0;
+  for (int j = 0; j < 20; j++) s = s + (f(c + h * R.l40x[j]) + f(c - h * R.l40x[j])) * R.l40w[j];
+  return s * h;
+}
+
+// 20-point Gauss-Laguerre on [a, inf), scale 1 (gauss_laguerre, gauss_integral.f90:26-113)
+template <class Fn>
+HNU double laguerre20(const Rules &R, const Fn &f, double a)
+{
+  double s = 0.0;
+  for (int j = 0; j < 20; j++) s = s + f(a + 1.0 * R.g20x[j]) * R.g20w[j];
+  return s * 1.0;
+}
+
+// URCA emissivities without blocking (urca, neu_rate.f90:110-160):
+// n -> p e nu~ (evn), p e- -> n nu (evep), n e+ -> p nu~ (even)
+HNU void urca(const Rules &R, double kt, double nn, double np, double etae, double etaep, double *evep,
+              double *even, double *evn)
+{
+  const double t11 = kt * 1.16059e-1;
+  const double t6 = cube(t11) * cube(t11);
+  *evn = 1.14473926e37 * t6 * nn * legendre40(R, Rate<1, 0, 3>{kt, etae, 0.0}, XME / kt, (XMN - XMP) / kt);
+  *evep = 1.14473926e37 * t6 * np * laguerre20(R, Rate<2, 0, 3>{kt, etae, 0.0}, (XMN - XMP) / kt);
+  *even = 1.14473926e37 * t6 * nn * laguerre20(R, Rate<3, 0, 3>{kt, etaep, 0.0}, XME / kt);
+}
+
+// nucleon-nucleon bremsstrahlung (brem) and plasmon decay (plasmon)
+HNU double brem(double nb, double kt)
+{
+  const double rho10 = nb * 1.66e5, t11 = kt * 1.16059e-1;
+  return 3.35e27 * (rho10 * rho10) * pow(t11, 5.5);
+}
+HNU double plasmon(double kt, double etae)
+{
+  const double t11 = kt * 1.16059e-1;
+  const double eta = etae + 0.510998910 / kt;
+  const double gp = 5.565e-2 * sqrt((sq(PI) + 3.0 * sq(eta)) / 3.0);
+  const double t9 = sq(sq(t11)) * sq(sq(t11)) * t11;
+  return 1.5e32 * t9 * (cube(gp) * cube(gp)) * exp(-gp) * (1.0 + gp) * (2.0 + sq(gp) / (1.0 + gp));
+}
+
+// Emissivities of electron neutrinos (qe) and of one heavy-lepton flavour
+// (qo), erg cm^-3 s^-1, as opt_dep sums them (accretion.f90:65-84): pairs,
+// URCA without blocking, bremsstrahlung and plasmons.  None depends on the
+// scale height or the blocking factors, so the ten trapping iterations of
+// abundance() and funcnb(), which the reference runs through opt_dep() with
+// the same arguments each time, take them from one evaluation.
+struct Emission {
+  double qe, qo;
+};
+
+HNU Emission emission(const Rules &R, double kt, double nnucl, double nn, double np, double etae, double etaep)
+{
+  double ev1, ev2, evep, even, evn;
+  pair(R, kt, etae, &ev1, &ev2);
+  urca(R, kt, nn, np, etae, etaep, &evep, &even, &evn);
+  const double evbrem = brem(nnucl, kt);
+  const double evpl = plasmon(kt, etae);
+  return {ev1 + evep + even + evn + evbrem / 3.0 + evpl, ev2 + evbrem / 3.0};
+}
+
+// absorption and scattering optical depths over the scale height hd
+// (opt_dep, accretion.f90:65-100)
+HNU void opt_dep(const Emission &q, double hd, double kt, double nn, double np, double *ta1, double *ta2,
+                 double *ts)
+{
+  const double t11 = kt * 1.16059e-1;
+  const double xl = 5.67051e39 * 4.0 * 7.0 / 8.0 * (sq(t11) * sq(t11));
+  *ta1 = q.qe * hd / xl;
+  *ta2 = q.qo * hd / xl;
+  const double cv = (double)(0.5f + 2.0f * 0.23f);
+  const double alph = 1.25, xme = 0.510998910;
+  const double csn = (1.0 + 5.0 * sq(alph)) / 24.0;
+  const double csp = (4.0 * sq(cv - 1.0) + 5.0 * sq(alph)) / 24.0;
+  const double tsn = csn * 1.76e-5 * nn * hd * HNU_F(13.8) * sq(kt / xme);
+  const double tsp = csp * 1.76e-5 * np * hd * HNU_F(13.8) * sq(kt / xme);
+  *ts = tsn + tsp;
+}
+
+// blocking factors of electron and heavy-lepton neutrinos (b_neu)
+HNU void b_neu(double ta1, double ta2, double ts, double *b1, double *b2)
+{
+  const double te = ta1 + ts, tt = ta2 + ts, r3 = sqrt(3.0);
+  const double third = (double)(1.0f / 3.0f);
+  *b1 = (te / 2.0 + 1.0 / r3) / (te / 2.0 + 1.0 / r3 + third / ta1);
+  *b2 = (tt / 2.0 + 1.0 / r3) / (tt / 2.0 + 1.0 / r3 + third / ta2);
+  if (ta1 <= 0.0 || ta2 <= 0.0) *b1 = *b2 = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Chemical equilibrium (chem_eq.f90)
+// ---------------------------------------------------------------------------
+
+// the state shared by funcnb's evaluations (the Fortran common block /nucl/)
+struct Nucl {
+  double nnucl, kt, ne0, hdfac, nb0;
+};
+
+// the net rate of the six neutron-proton reactions, relative to p e- -> n nu,
+// with neutrino blocking b1 (neutrino, chem_eq.f90:194-253)
+HNU double net_rate(const Rules &R, double b1, double kt, double nn, double np, double etae)
+{
+  const double etaep = -etae - 2.0 * XME / kt;
+  const double t11 = kt * 1.16059e-1;
+  const double t5 = sq(t11) * sq(t11) * t11;
+  if (nn < 0.0) nn = 0.0;
+  if (np < 0.0) np = 0.0;
+  const double a = XME / kt, b = (XMN - XMP) / kt;
+  const double f1 = legendre40(R, Rate<1, 0, 2>{kt, etae, b1}, a, b);
+  const double f1r = legendre40(R, Rate<1, 1, 2>{kt, etae, b1}, a, b);
+  const double evn = 2.03813046e35 * t5 * nn * (f1 + f1r);
+  const double f2 = laguerre20(R, Rate<2, 0, 2>{kt, etae, b1}, b);
+  const double f2r = laguerre20(R, Rate<2, 1, 2>{kt, etae, b1}, b);
+  const double evep = 2.03813046e35 * t5 * np * (f2 + f2r);
+  const double f3 = laguerre20(R, Rate<3, 0, 2>{kt, etaep, b1}, a);
+  const double f3r = laguerre20(R, Rate<3, 1, 2>{kt, etaep, b1}, a);
+  const double even = 2.03813046e35 * t5 * nn * (f3 + f3r);
+  if (fabs(evep) < 1.0e-80) return (evep - even - evn) / (fabs(evep) + 1.0e-80);
+  return (evep - even - evn) / fabs(evep);
+}
+
+// degeneracies of the nucleons for proton fraction xp (nuclear)
+HNU void nuclear(const Rules &R, double kt, double nb, double xp, double *etan, double *etap)
+{
+  double np = nb * xp, nn = nb - np;
+  if (np <= 0.0) np = 0.0;
+  *etap = peta(R, kt, np);
+  if (nn <= 0.0) nn = 0.0;
+  *etan = neta(R, kt, nn);
+}
+
+// the energy balance of the gas at proton fraction xp, with the neutrino
+// trapping iterated ten times (funcnb, chem_eq.f90:140-192)
+HNU_NOINLINE double funcnb(const Rules &R, const Nucl &c, double xp)
+{
+  const double beta = c.kt / XME;
+  double etan, etap;
+  nuclear(R, c.kt, c.nnucl, xp, &etan, &etap);
+  const double nhe = c.ne0 / 2.0;
+  const double np = c.nnucl * xp, nn = c.nnucl - np;
+  const double ne = c.nnucl * xp + c.ne0;
+  const double etae = eeta(R, c.kt, ne);
+  const double etaep = -etae - 2.0 / beta;
+  double b1 = 0.0, b2 = 0.0, nee, nep;
+  lepton(R, c.kt, etae, &nee, &nep);
+  double e, p, ehe, phe;
+  eos_npe(R, c.kt, etan, etap, etae, nee, &e, &p);
+  const double pr = p_rad(c.kt), er = 3.0 * pr;
+  eos_he(c.kt, nhe, &ehe, &phe);
+  const double p1 = p + pr + phe, e1 = e + er + ehe;
+  const Emission q = emission(R, c.kt, c.nnucl, nn, np, etae, etaep);
+  for (int i = 0; i < 10; i++) {
+    const double pneu = p_neu(c.kt, b1, b2);
+    double pp = p1 + pneu, ee = e1 + 3.0 * pneu;
+    const double hd = h_dep(c.hdfac, c.nb0, pp, ee);
+    double ta1, ta2, ts;
+    opt_dep(q, hd, c.kt, nn, np, &ta1, &ta2, &ts);
+    b_neu(ta1, ta2, ts, &b1, &b2);
+  }
+  return net_rate(R, b1, c.kt, nn, np, etae);
+}
+
+struct FuncNb {
+  const Rules &R;
+  const Nucl &c;
+  HNU double operator()(double xp) const { return funcnb(R, c, xp); }
+};
+
+struct Abundance {
+  double e, p, qnu, tau, nee, nep;  // erg cm^-3, erg cm^-3, erg cm^-2 s^-1, -, fm^-3, fm^-3
+  double xp;                        // proton fraction of the free nucleons
+};
+
+// abundance() at density rho (g cm^-3), temperature T (K) and scale-height
+// factor hdfac (abundance.f90:6-243, with chem_eq and eqnucl, chem_eq.f90:49-102)
+HNU_NOINLINE Abundance abundance(const Rules &R, double rho, double T, double hdfac)
+{
+  const double nb = rho / 1.66e15;
+  const double kt = T / 1.16059e10;
+  const double beta = kt / XME;
+  const double xn = xnuc(nb, kt);
+  const double nnuc = nb * xn;
+  const double nhe = (nb - nnuc) / 4.0;
+
+  // eqnucl: the proton fraction by Newton on funcnb from 1/2, kept in [0, 1]
+  const Nucl c{nb * xn, kt, fabs(1.0 - xn) * nb / 2.0, hdfac, nb};
+  double xp = newton1(FuncNb{R, c}, (1.0 - 0.0) / 2.0, 0.0, newton_tol(c.nnucl));
+  if (xp < 0.0) xp = 0.0;
+  if (xp > 1.0) xp = 1.0;
+  double etan, etap;
+  nuclear(R, kt, c.nnucl, xp, &etan, &etap);
+  const double np = c.nnucl * xp, nn = c.nnucl - np;
+  const double etae = eeta(R, kt, np + c.ne0);
+
+  const double etaep = -etae - 2.0 / beta;
+  Abundance a;
+  lepton(R, kt, etae, &a.nee, &a.nep);
+  double enucl, pnucl, ehe, phe;
+  eos_npe(R, kt, etan, etap, etae, a.nee, &enucl, &pnucl);
+  const double prad = p_rad(kt), erad = 3.0 * prad;
+  eos_he(kt, nhe, &ehe, &phe);
+  const double p1 = pnucl + prad + phe, e1 = enucl + erad + ehe;
+  double b1 = 0.0, b2 = 0.0, ta1 = 0.0, ta2 = 0.0, ts = 0.0;
+  const Emission q = emission(R, kt, nnuc, nn, np, etae, etaep);
+  for (int i = 0; i < 10; i++) {
+    const double pneu = p_neu(kt, b1, b2);
+    double p = p1 + pneu, e = e1 + 3.0 * pneu;
+    const double hd = h_dep(hdfac, nb, p, e);
+    opt_dep(q, hd, kt, nn, np, &ta1, &ta2, &ts);
+    b_neu(ta1, ta2, ts, &b1, &b2);
+  }
+  const double pneu = p_neu(kt, b1, b2), eneu = 3.0 * pneu;
+  const double T4 = sq(T) * sq(T);
+  a.qnu = 7.0 / 8.0 * SIGMASB * T4 / 0.75 *
+          (1. / (0.5 * ta1 + 0.5 * ts + HNU_F(0.557) + HNU_F(0.3) / ta1) +
+           1. / (0.5 * ta2 + 0.5 * ts + HNU_F(0.557) + HNU_F(0.3) / ta2));
+  a.tau = ts + ta1 + ta2;
+  a.p = (pnucl + prad + pneu + phe) * 1.6021772e33;
+  a.e = (enucl + erad + eneu + ehe) * 1.6021772e33;
+  a.xp = xp;
+  return a;
+}
+
+}  // namespace nu
+}  // namespace harm

@@ -424,6 +424,40 @@ int harm_set_eos(harm_ctx *ctx, const harm_eos *eos);
 int harm_get_eos_guess(harm_ctx *ctx, double *lastT);
 int harm_put_eos_guess(harm_ctx *ctx, const double *lastT);
 
+/* ---- The COOL_EOS table generator ----
+   The equation of state and neutrino rates the tables hold: nucleons,
+   electron-positron pairs, helium, radiation and trapped neutrinos in beta
+   equilibrium (the reference's Fortran abundance(), abundance.f90:6-243, and
+   its modules).  Units as abundance() returns them: e and p in erg cm^-3, Qnu
+   in erg cm^-2 s^-1, tau dimensionless, n_e- and n_e+ in fm^-3. */
+
+/* abundance() at n nodes on the host's cores (threads <= 0: all of them):
+   out[7n] = e, p, Qnu, tau, n_e-, n_e+ and the proton fraction of the free
+   nucleons per node.  The library's counterpart of the reference's
+   abundance_(rho, T, HdFac, e, p, Qnu, tau, xnee, xnep) (cooleos.c:58-59),
+   node by node. */
+int harm_nu_abundance(const double *rho, const double *T, const double *hdfac, long n, int threads,
+                      double *out);
+/* The same on a GPU (host arrays in and out). */
+int harm_nu_abundance_dev(int device, const double *rho, const double *T, const double *hdfac, long n,
+                          double *out);
+/* Every node of ntab tables on a GPU: values[ntab][nx][ny][5] = e, p, Qnu, tau,
+   Yee at rho = xaxis[i] (g cm^-3), T = yaxis[j] (K) and the table's HdFac, as
+   calc_cache_val packs them (cooleos.c:171-194), ready for harm_eos_create.
+   slice: nodes per kernel launch (<= 0: one table).  *ms (may be NULL): the
+   device time of the build. */
+int harm_nu_tables(int device, const double *xaxis, int nx, const double *yaxis, int ny, const double *hdfac,
+                   int ntab, long slice, double *values, float *ms);
+/* The generator's quadrature rules, 100 doubles: 20-point Gauss-Legendre
+   (10 positive abscissae, 10 weights), 40-point Gauss-Legendre (20, 20),
+   20-point Gauss-Laguerre (20 abscissae, 20 weights times e^x). */
+int harm_nu_rules(double *out);
+/* Generalised Fermi-Dirac integrals F_k(eta, theta) = int_0^inf x^k
+   sqrt(1 + theta x / 2) / (e^(x - eta) + 1) dx, k = 1/2, 3/2, 5/2, 7/2, as the
+   generator computes them (dfermi, gauss_integral.f90:241-349), on the host:
+   F[4n]. */
+int harm_nu_fermi(const double *eta, const double *theta, long n, double *F);
+
 #ifdef __cplusplus
 }
 #endif
