@@ -514,6 +514,48 @@ def tracers_by_density(np, pr, p, n, seed):
     return ids, X
 
 
+def generator_cpu_rate(np, hc, xa, ya, hd, seed, nodes=96):
+    """abundance() on the host's cores over a random sample of the generated
+    nodes: the CPU rate beside the device's (the reference's own generator is
+    Fortran, which this box cannot compile)."""
+    rng = np.random.default_rng(seed)
+    i, j, t = rng.integers(len(xa), size=nodes), rng.integers(len(ya), size=nodes), rng.integers(len(hd), size=nodes)
+    t0 = time.perf_counter()
+    hc.nu_abundance(xa[i], ya[j], hd[t])
+    s = time.perf_counter() - t0
+    return {"cpu_nodes_per_s": nodes / s, "cpu_cores": os.cpu_count(),
+            "cpu_sample": "%d random nodes of the generated rows, all cores" % nodes}
+
+
+def floor_rows_read(np, hc, eos_tables, pr, xa, ya, val, consts, gen, ids, X, pa, nsteps):
+    """Whether the run read a table row below the generated ones: the same steps
+    (nsteps: the step counts of the run's calls) again with those rows filled
+    by the synthetic stand-in instead of NaN.  A
+    temperature solve that reads NaN falls back to the gamma law, one that
+    reads the stand-in converges on it, so the two runs part wherever such a
+    row was read, and end bit-identical where none was."""
+    j0 = gen["first_row"]
+    if j0 == 0:
+        return False
+    val2 = val.copy()
+    R, TT = np.meshgrid(xa, ya[:j0], indexing="ij")
+    e, p, qnu, tau, nee, nep = eos_tables.ideal_gas_radiation(R, TT, 1.0)
+    for t in range(val.shape[0]):
+        val2[t, :, :j0, 0], val2[t, :, :j0, 1], val2[t, :, :j0, 2], val2[t, :, :j0, 3] = e, p, qnu, tau
+        val2[t, :, :j0, 4] = (nee - nep) / (R / 1.66e15)
+    eos2 = hc.Eos(xa, ya, val2, consts)
+    c2 = hc.Context(pr)
+    c2.init_torus()
+    c2.set_eos(eos2)
+    c2.tracers_put(ids, X)
+    for k in nsteps:  # the seeding step, the warm-up and the timed steps, as the run took them
+        c2.run(k)
+    pb = c2.get_prims()
+    c2.close()
+    eos2.close()
+    return not np.array_equal(pa, pb, equal_nan=True)
+
+
 def run_cool(args):
     """The COOL_EOS step on the 256x256 torus of the reference's init.c literals
     (a=0.6, rin=4, rmax=11.8, beta=50; cooleos.c's 3 Msun hole and units), FP64,
@@ -534,8 +576,13 @@ def run_cool(args):
     else:
         # 200 x 200 over rho 1e4..1e14 g/cm^3, T 1e8..1e12 K, and a density unit that
         # puts the torus maximum (rho = 1 in code units) at 1e11 g/cm^3
-        xa, ya, val, consts = eos_tables.build_tables(eos_tables.zone_radii(pr), nx=200, ny=200,
-                                                      rho=(1.e4, 1.e14), T=(1.e8, 1.e12), gam=pr.params.gam)
+        grid = dict(nx=200, ny=200, rho=(1.e4, 1.e14), T=(1.e8, 1.e12), gam=pr.params.gam)
+        if args.cool_tables == "physics":
+            floor = args.cool_t_floor if args.cool_t_floor > 0 else None
+            xa, ya, val, consts, gen = eos_tables.physical_tables(eos_tables.zone_radii(pr), t_floor=floor, **grid)
+            gen.update(generator_cpu_rate(np, hc, xa, ya[gen["first_row"]:], consts["hdfac"], args.seed))
+        else:
+            xa, ya, val, consts = eos_tables.build_tables(eos_tables.zone_radii(pr), **grid)
         consts["rho_unit"] = 1.e11
         consts["u_unit"] = consts["p_unit"] = 1.e11 * eos_tables.CL * eos_tables.CL
         tables = "200x200 per-radius tables (rho 1e4-1e14, T 1e8-1e12), torus maximum at 1e11 g/cm^3"
@@ -574,8 +621,10 @@ def run_cool(args):
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": "FM torus %dx%d (a=0.6, rin=4, rmax=11.8, beta=50), COOL_EOS, %s, "
-                                   "synthetic generator, %d tracers seeded by rest mass"
-                                   % (n, n, tables, args.cool_tracers),
+                                   "%s, %d tracers seeded by rest mass"
+                                   % (n, n, tables, "generator tables (abundance() on the GPU)"
+                                      if args.cool_tables == "physics" else "synthetic generator",
+                                      args.cool_tracers),
                        "l2": ("tables (%.0f MB) %s; state per step is small"
                               % (val.nbytes / 1e6, "fit in L2" if val.nbytes < 126e6 else "exceed L2 (126 MB)"))},
             "seeding_step_s": seed_s,
@@ -588,8 +637,20 @@ def run_cool(args):
                          "peak_source": peak_kind,
                          "note": "the T solves make these kernels FP64-latency bound, not HBM bound"},
             "kernel_ms": kms, "clocks": clocks, "sim_time": ctx.time(), "fail_code": d["fail_code"]}
+    if args.cool_tables == "physics":
+        lastT = ctx.eos_guess()
+        seen = lastT[lastT > 0]
+        gen["zone_T_range_K"] = [float(seen.min()), float(seen.max())] if seen.size else None
+        gen["floor_rows_read"] = floor_rows_read(np, hc, eos_tables, pr, xa, ya, val, consts, gen, ids, X, pa,
+                                                 (1, args.warmup - 1, args.steps))
+        line["tables"] = gen
     ctx.close()
-    if not args.no_mixed:
+    if not args.no_mixed and args.cool_tables == "physics":
+        # the FP32 copies are scaled per plane by a power of two, which NaN rows
+        # and 240 binary orders of magnitude defeat
+        line["mixed"] = {"unavailable": "the FP32 table copies are scaled per plane from the values' range, "
+                                        "which the NaN rows below the generated ones leave undefined"}
+    elif not args.no_mixed:
         # the face physics' EOS calls in FP32, the same steps
         cm = hc.Context(pr)
         cm.init_torus()
@@ -669,9 +730,12 @@ def main():
                          "cool: the 256x256 COOL_EOS step")
     ap.add_argument("--cool-n", type=int, default=256)
     ap.add_argument("--cool-tracers", type=int, default=100000)
-    ap.add_argument("--cool-tables", choices=("reference", "baseline"), default="reference",
+    ap.add_argument("--cool-tables", choices=("reference", "baseline", "physics"), default="reference",
                     help="reference: cooleos.c's 72x72 tables and units; baseline: 200x200 tables over "
-                         "rho 1e4-1e14, T 1e8-1e12 with the torus maximum at 1e11 g/cm^3")
+                         "rho 1e4-1e14, T 1e8-1e12 with the torus maximum at 1e11 g/cm^3; physics: the "
+                         "baseline grid filled by the library's abundance() on the GPU")
+    ap.add_argument("--cool-t-floor", type=float, default=2e9,
+                    help="physics tables: generate the rows at or above this T (K) only, NaN below (0: all)")
     ap.add_argument("--dump-cool", default=None, help="save the FP64 and mixed COOL_EOS states (npz)")
     ap.add_argument("--adj-n", type=int, default=192, help="adjoint workload: N1 = N2")
     ap.add_argument("--adj-steps", type=int, default=50, help="adjoint workload: steps K")

@@ -1,22 +1,27 @@
 // The COOL_EOS table generator on the device: abundance() (harm_nu.cuh) at
-// every node of the per-radius (rho, T) tables, one thread per node.
+// every node of the per-radius (rho, T) tables, one warp per node.
 //
 // The reference fills the same tables lazily on the host, node by node, with
 // six worker threads calling its Fortran abundance_() (cooleos.c:171-194,
 // 805-820; cache4d.c) and caches them in files.  Here every node of every
-// table is computed in one pass before the run: the nodes are independent,
-// each a nest of Newton solves over Fermi integrals in FP64, which is
-// latency-bound scalar work that the 148 SMs run side by side.
+// table is computed in one pass before the run.  A node is a nest of Newton
+// solves whose trials evaluate Fermi and rate integrals by Gauss quadrature,
+// in FP64; its cost varies by four orders of magnitude with the temperature
+// (where free nucleons are a trace, at a few 1e8 K, the proton-fraction solve
+// runs all 200 of its trials, each over three nested solves).  A thread per
+// node would leave a warp waiting on its slowest lane and run each
+// quadrature's terms one after another; a warp per node keeps its lanes on
+// one control flow and spreads the terms of every quadrature over them
+// (lane_sum, harm_nu.cuh).
 //
-// The cost of a node varies by four orders of magnitude, with the
-// temperature above all: where free nucleons are a trace (T of a few 1e8 K)
-// the proton-fraction solve runs all 200 of its trials, each over three
-// nested solves.  So a warp holds the nodes of one temperature (the density
-// varies across its lanes), and the tables are launched one per kernel over
-// several streams without waiting in between: the blocks of a table still
-// running on its slowest nodes share the SMs with the next tables' blocks.
-// Every loop in the physics has a fixed trip count or the 200-trial cap of
-// the Newton solver, so every thread ends.
+// Four blocks of four warps per SM (128 registers a thread): the warps' long
+// FP64 latency chains (exp, log, division) need that many to fill the FP64
+// pipe, measured 1.44x faster than three blocks at 168 registers.
+//
+// Tables are launched one per kernel over several streams without waiting in
+// between, so the blocks of a table still on its slowest nodes share the SMs
+// with the next tables' blocks.  Every loop in the physics has a fixed trip
+// count or the 200-trial cap of the Newton solver, so every warp ends.
 #include "harm_b200.h"
 #include "harm_common.cuh"
 #include "harm_nu.cuh"
@@ -31,43 +36,61 @@ const Rules *host_rules();
 
 __constant__ Rules c_rules;
 
-// node k of the slice [k0, k0 + n), with k = (t ny + j) nx + i for table t,
-// T index j and rho index i; values packed as calc_cache_val packs them
-// (cooleos.c:171-194) at values[t][i][j]: e, p, Qnu, tau,
+// the quadrature rules into shared memory: the lanes of a warp read different
+// nodes of a rule at once, which the constant cache would serialise
+__device__ __forceinline__ void load_rules(Rules &R)
+{
+  for (int q = threadIdx.x; q < (int)(sizeof(Rules) / sizeof(double)); q += blockDim.x)
+    reinterpret_cast<double *>(&R)[q] = reinterpret_cast<const double *>(&c_rules)[q];
+  __syncthreads();
+}
+
+// node k of the slice [k0, k0 + n) on warp k - k0, with k = (t ny + j) nx + i
+// for table t, T index j and rho index i; values packed as calc_cache_val
+// packs them (cooleos.c:171-194) at values[t][i][j]: e, p, Qnu, tau,
 // Yee = (n_e- - n_e+) / n_b
-__global__ void __launch_bounds__(128) k_tables(const double *xaxis, int nx, const double *yaxis, int ny,
+__global__ void __launch_bounds__(128, 4) k_tables(const double *xaxis, int nx, const double *yaxis, int ny,
                                                 const double *hdfac, long k0, long n, double *values)
 {
-  const long k = k0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= k0 + n) return;
+  __shared__ Rules R;
+  load_rules(R);
+  const long w = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= n) return;  // whole warps: the lanes of a node stay together
+  const long k = k0 + w;
   const int i = (int)(k % nx);
   const long tj = k / nx;
   const int j = (int)(tj % ny), t = (int)(tj / ny);
   const double rho = xaxis[i];
-  const Abundance a = abundance(c_rules, rho, yaxis[j], hdfac[t]);
-  double *v = values + 5 * (((long)t * nx + i) * ny + j);
-  v[0] = a.e;
-  v[1] = a.p;
-  v[2] = a.qnu;
-  v[3] = a.tau;
-  v[4] = (a.nee - a.nep) / (rho / 1.66e15);
+  const Abundance a = abundance(R, rho, yaxis[j], hdfac[t]);
+  if ((threadIdx.x & 31) == 0) {
+    double *v = values + 5 * (((long)t * nx + i) * ny + j);
+    v[0] = a.e;
+    v[1] = a.p;
+    v[2] = a.qnu;
+    v[3] = a.tau;
+    v[4] = (a.nee - a.nep) / (rho / 1.66e15);
+  }
 }
 
-// abundance() at a list of nodes, for checks against the host
-__global__ void __launch_bounds__(128) k_nodes(const double *rho, const double *T, const double *hdfac, long n,
+// abundance() at a list of nodes, a warp per node, for checks against the host
+__global__ void __launch_bounds__(128, 4) k_nodes(const double *rho, const double *T, const double *hdfac, long n,
                                                double *out)
 {
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ Rules R;
+  load_rules(R);
+  const long k = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (k >= n) return;
-  const Abundance a = abundance(c_rules, rho[k], T[k], hdfac[k]);
-  double *o = out + 7 * k;
-  o[0] = a.e;
-  o[1] = a.p;
-  o[2] = a.qnu;
-  o[3] = a.tau;
-  o[4] = a.nee;
-  o[5] = a.nep;
-  o[6] = a.xp;
+  const Abundance a = abundance(R, rho[k], T[k], hdfac[k]);
+  if ((threadIdx.x & 31) == 0) {
+    double *o = out + 7 * k;
+    o[0] = a.e;
+    o[1] = a.p;
+    o[2] = a.qnu;
+    o[3] = a.tau;
+    o[4] = a.nee;
+    o[5] = a.nep;
+    o[6] = a.xp;
+  }
 }
 
 static int upload_rules(int device)
@@ -141,7 +164,7 @@ extern "C" int harm_nu_tables(int device, const double *xaxis, int nx, const dou
   int q = 0;
   for (long k0 = 0; k0 < n; k0 += slice, q = (q + 1) % NS) {
     const long m = (n - k0 < slice) ? n - k0 : slice;
-    nu::k_tables<<<(unsigned)((m + 127) / 128), 128, 0, st[q]>>>(dx, nx, dy, ny, dh, k0, m, dv);
+    nu::k_tables<<<(unsigned)((m + 3) / 4), 128, 0, st[q]>>>(dx, nx, dy, ny, dh, k0, m, dv);
     CK(cudaGetLastError());
   }
   for (int s = 1; s < NS; s++) {
@@ -179,7 +202,7 @@ extern "C" int harm_nu_abundance_dev(int device, const double *rho, const double
   CK(cudaMemcpy(dr, rho, n * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dt, T, n * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dh, hdfac, n * sizeof(double), cudaMemcpyHostToDevice));
-  nu::k_nodes<<<(unsigned)((n + 127) / 128), 128>>>(dr, dt, dh, n, dout);
+  nu::k_nodes<<<(unsigned)((n + 3) / 4), 128>>>(dr, dt, dh, n, dout);
   CK(cudaGetLastError());
   CK(cudaMemcpy(out, dout, 7 * n * sizeof(double), cudaMemcpyDeviceToHost));
   return HARM_OK;

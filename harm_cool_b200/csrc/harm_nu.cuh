@@ -21,6 +21,17 @@
 // Units are the reference's: densities in fm^-3, energies and temperatures
 // in MeV, until abundance() converts e and p to erg cm^-3.
 //
+// One node, one warp.  A node is a nest of Newton solves whose every trial
+// evaluates Fermi integrals or rate integrals by Gauss quadrature.  All 32
+// lanes of a warp run the node's scalar code together, with the same values,
+// and split each quadrature's terms between them (lane_sum): lane l adds
+// terms l, l + 32, ... and a butterfly over the lanes combines the partial
+// sums, so that every lane holds the same sum and the control flow stays
+// uniform.  The quadratures a Newton trial needs at x, x + dx and x - dx, or
+// that a routine needs for several species, go into one such sum.  The host
+// build runs the 32 lanes one after another and the same butterfly, so both
+// builds add the terms in the same order.
+//
 // Fidelity.  The reference is gfortran code; no Fortran compiler exists
 // here, so this restatement is not compared with its output.  It keeps the
 // reference's formulae, their order of operations and its constants, and
@@ -32,10 +43,12 @@
 //    opt_dep() zeroes its caller's b1 before b_neu() sets it again;
 //  - mnewt() with one unknown: a zero or NaN derivative skips the solve and
 //    steps by the residual itself (ludcmp's singular branch).
-// Integer powers are products and x**1.5-style powers are pow(); the
-// Fermi-integral kernels take x^k as x^(k-1/2) sqrt(x), and compute the four
-// indices of one (eta, theta) in one pass over the nodes (the breakpoints
-// depend on eta alone).  These change results in the last bits only.
+// What differs in the last bits only: integer powers are products and
+// x**1.5-style powers are pow(); the Fermi kernels take x^k as
+// x^(k-1/2) sqrt(x) and fold each interval's half-length into the weights;
+// quadrature terms are summed in the lane order above rather than node by
+// node; and the emissivities of the trapping iteration are evaluated once
+// (they do not depend on its unknowns).
 #pragma once
 
 #include <math.h>
@@ -61,7 +74,7 @@ constexpr double SIGMASB = HNU_F(5.6e-5);
 constexpr double XME = 0.510998910, XMP = 938.272013, XMN = 939.56536;  // MeV
 
 // Quadrature rules.  Abscissae and weights are computed on the host by
-// harm_nu_rules() (harm_nu.cu) from the definitions of the rules; the
+// harm_nu_rules() (harm_nu_host.cpp) from the definitions of the rules; the
 // Gauss-Laguerre weights carry the factor e^x, as the integrands include the
 // weight function.
 struct Rules {
@@ -74,48 +87,67 @@ HNU double sq(double x) { return x * x; }
 HNU double cube(double x) { return x * x * x; }
 
 // ---------------------------------------------------------------------------
+// Sums over the lanes of a warp
+// ---------------------------------------------------------------------------
+
+// out[a] = sum over terms e < NTERM of what term(e, i, acc) adds to acc[a],
+// for NA accumulators.  Lane l takes terms e = l + 32 i, i = 0, 1, ... (i is
+// a constant in each unrolled step of the device loop); the butterfly adds,
+// on lanes l and l ^ d, the same two partial sums, so all lanes end equal.
+template <int NA, int NTERM, class Term>
+HNU void lane_sum(const Term &term, double *out)
+{
+  constexpr int NI = (NTERM + 31) / 32;
+#if defined(__CUDA_ARCH__)
+  const int l = threadIdx.x & 31;
+  double part[NA];
+#pragma unroll
+  for (int a = 0; a < NA; a++) part[a] = 0.0;
+#pragma unroll
+  for (int i = 0; i < NI; i++) {
+    const int e = l + 32 * i;
+    if (e < NTERM) term(e, i, part);
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1)
+#pragma unroll
+    for (int a = 0; a < NA; a++) part[a] += __shfl_xor_sync(0xffffffffu, part[a], d);
+#pragma unroll
+  for (int a = 0; a < NA; a++) out[a] = part[a];
+#else
+  double part[32][NA];
+  for (int l = 0; l < 32; l++) {
+    for (int a = 0; a < NA; a++) part[l][a] = 0.0;
+    for (int i = 0; i < NI; i++) {
+      const int e = l + 32 * i;
+      if (e < NTERM) term(e, i, part[l]);
+    }
+  }
+  // lane 0's butterfly: at distance d it adds lane d's partial, which holds the
+  // same sums over lanes d .. 2d-1 that lanes 0 .. d-1 hold over 0 .. d-1
+  for (int d = 16; d > 0; d >>= 1)
+    for (int l = 0; l < d; l++)
+      for (int a = 0; a < NA; a++) part[l][a] = part[l][a] + part[l + d][a];
+  for (int a = 0; a < NA; a++) out[a] = part[0][a];
+#endif
+}
+
+// ---------------------------------------------------------------------------
 // Generalised Fermi-Dirac integrals
 //   F_k(eta, theta) = int_0^inf x^k sqrt(1 + theta x / 2) / (e^(x - eta) + 1) dx
 // for k = 1/2, 3/2, 5/2, 7/2, by Aparicio's four-interval quadrature (ApJS 117,
 // 627, 1998) as in dfermi (gauss_integral.f90:241-349): 20-point
 // Gauss-Legendre on [0, sqrt(s1)] in z = sqrt(x), on [s1, s2] and [s2, s3], and
 // 20-point Gauss-Laguerre on [s3, inf), with breakpoints that follow eta.
-// F[m] = F_{m + 1/2} for m < nk.
 // ---------------------------------------------------------------------------
 
-// the integrand without its power of x (fdfunc1, gauss_integral.f90:354-393)
-HNU double fd_kernel(double x, double eta, double theta)
-{
-  const double dxst = sqrt(1.0 + 0.5 * x * theta);
-  if (x - eta < 1.0e2) return dxst / (exp(x - eta) + 1.0);
-  return dxst * exp(eta - x);
-}
+// the intervals of one (eta, theta): centres and half-lengths of the three
+// Gauss-Legendre pieces (the first in z) and the start of the tail
+struct FdSpan {
+  double eta, theta, c[3], h[3], s3;
+};
 
-// nk indices at one node of the x integrals: x^(1/2), x^(3/2), ...
-HNU void fd_add_x(double x, double w, double eta, double theta, int nk, double *acc)
-{
-  double xk = sqrt(x);
-  const double g = fd_kernel(x, eta, theta);
-  for (int m = 0; m < nk; m++) {
-    acc[m] += xk * g * w;
-    xk *= x;
-  }
-}
-
-// the z = sqrt(x) integrand (fdfunc2, gauss_integral.f90:398-438): 2 z^(2k+1) ...
-HNU void fd_add_z(double z, double w, double eta, double theta, int nk, double *acc)
-{
-  const double zsq = z * z;
-  const double dxst = sqrt(1.0 + 0.5 * zsq * theta);
-  const double g = (zsq - eta < 1.0e2) ? dxst / (exp(zsq - eta) + 1.0) : dxst * exp(eta - zsq);
-  double zk = zsq;  // z^(2k+1), k = 1/2
-  for (int m = 0; m < nk; m++) {
-    acc[m] += 2.0 * zk * g * w;
-    zk *= zsq;
-  }
-}
-
-HNU void fermi(const Rules &R, double eta, double theta, int nk, double *F)
+HNU FdSpan fd_span(double eta, double theta)
 {
   // breakpoint fit of Aparicio (1998)
   const double d = 3.3609, sg = 9.1186e-2;
@@ -129,86 +161,140 @@ HNU void fermi(const Rules &R, double eta, double theta, int nk, double *F)
   const double x2 = (a2 + b2 * xi + c2 * d2 * xi2) / (1.0 + e2 * xi + c2 * xi2);
   const double x3 = (a3 + b3 * xi + c3 * d3 * xi2) / (1.0 + e3 * xi + c3 * xi2);
   const double s1 = x1 - x2, s2 = x1, s3 = x1 + x3, s12 = sqrt(s1);
+  FdSpan s;
+  s.eta = eta;
+  s.theta = theta;
+  s.c[0] = 0.5 * s12;
+  s.h[0] = 0.5 * s12;
+  s.c[1] = 0.5 * (s1 + s2);
+  s.h[1] = 0.5 * (s2 - s1);
+  s.c[2] = 0.5 * (s2 + s3);
+  s.h[2] = 0.5 * (s3 - s2);
+  s.s3 = s3;
+  return s;
+}
 
-  double r1[4] = {0., 0., 0., 0.}, r2[4] = {0., 0., 0., 0.}, r3[4] = {0., 0., 0., 0.}, r4[4] = {0., 0., 0., 0.};
-  // the three Gauss-Legendre pieces (dqleg020): sums of node pairs, then the half-length
+// M Fermi integral sets of NK indices each, 80 terms per set laid out in 96
+// slots (three steps of the lanes; slots 80..95 are empty), so that the set of
+// a step is the constant i / 3.  Term r of a set: pieces r / 20 = 0, 1, 2 are
+// the Gauss-Legendre intervals, node (r % 20) / 2 on the side (r % 20) & 1;
+// piece 3 is the Gauss-Laguerre node r % 20.  The integrands are fdfunc1 and,
+// in z = sqrt(x), fdfunc2 (gauss_integral.f90:354-438), with the overflow
+// guard at x - eta = 100.
+template <int M, int NK>
+struct FdTerms {
+  const Rules &R;
+  const FdSpan *s;
+  HNU void operator()(int e, int i, double *acc) const
   {
-    const double c = 0.5 * s12, h = 0.5 * s12;
-    for (int j = 0; j < 10; j++) {
-      double p[4] = {0., 0., 0., 0.};
-      fd_add_z(c + h * R.l20x[j], 1.0, eta, theta, nk, p);
-      fd_add_z(c - h * R.l20x[j], 1.0, eta, theta, nk, p);
-      for (int m = 0; m < nk; m++) r1[m] += p[m] * R.l20w[j];
+    const int m = i / 3, r = e - 96 * m;
+    if (r >= 80) return;
+    const int piece = r / 20, q = r % 20;
+    const FdSpan &S = s[m];
+    double x, w;
+    if (piece < 3) {
+      const int j = q >> 1;
+      const double c = piece == 0 ? S.c[0] : (piece == 1 ? S.c[1] : S.c[2]);
+      const double h = piece == 0 ? S.h[0] : (piece == 1 ? S.h[1] : S.h[2]);
+      x = c + ((q & 1) ? -h : h) * R.l20x[j];
+      w = R.l20w[j] * h;
+    } else {
+      x = S.s3 + R.g20x[q];
+      w = R.g20w[q];
     }
-    for (int m = 0; m < nk; m++) r1[m] *= h;
-  }
-  {
-    const double c = 0.5 * (s1 + s2), h = 0.5 * (s2 - s1);
-    for (int j = 0; j < 10; j++) {
-      double p[4] = {0., 0., 0., 0.};
-      fd_add_x(c + h * R.l20x[j], 1.0, eta, theta, nk, p);
-      fd_add_x(c - h * R.l20x[j], 1.0, eta, theta, nk, p);
-      for (int m = 0; m < nk; m++) r2[m] += p[m] * R.l20w[j];
+    double *a = acc + m * NK;
+    if (piece == 0) {  // z = x here: 2 z^(2k+1) sqrt(1 + theta z^2 / 2) / (e^(z^2 - eta) + 1)
+      const double zsq = x * x;
+      const double dxst = sqrt(1.0 + 0.5 * zsq * S.theta);
+      const double g = (zsq - S.eta < 1.0e2) ? dxst / (exp(zsq - S.eta) + 1.0) : dxst * exp(S.eta - zsq);
+      double zk = zsq;
+#pragma unroll
+      for (int k = 0; k < NK; k++) {
+        a[k] += 2.0 * zk * g * w;
+        zk *= zsq;
+      }
+    } else {
+      const double dxst = sqrt(1.0 + 0.5 * x * S.theta);
+      const double g = (x - S.eta < 1.0e2) ? dxst / (exp(x - S.eta) + 1.0) : dxst * exp(S.eta - x);
+      double xk = sqrt(x);
+#pragma unroll
+      for (int k = 0; k < NK; k++) {
+        a[k] += xk * g * w;
+        xk *= x;
+      }
     }
-    for (int m = 0; m < nk; m++) r2[m] *= h;
   }
-  {
-    const double c = 0.5 * (s2 + s3), h = 0.5 * (s3 - s2);
-    for (int j = 0; j < 10; j++) {
-      double p[4] = {0., 0., 0., 0.};
-      fd_add_x(c + h * R.l20x[j], 1.0, eta, theta, nk, p);
-      fd_add_x(c - h * R.l20x[j], 1.0, eta, theta, nk, p);
-      for (int m = 0; m < nk; m++) r3[m] += p[m] * R.l20w[j];
-    }
-    for (int m = 0; m < nk; m++) r3[m] *= h;
-  }
-  // the Gauss-Laguerre tail (dqlag020) on [s3, inf), scale 1
-  for (int j = 0; j < 20; j++) fd_add_x(s3 + R.g20x[j], R.g20w[j], eta, theta, nk, r4);
-  for (int m = 0; m < nk; m++) F[m] = r1[m] + r2[m] + r3[m] + r4[m];
+};
+
+// F[m NK + k] = F_{k+1/2}(eta[m], theta[m])
+template <int M, int NK>
+HNU void fermi(const Rules &R, const double *eta, const double *theta, double *F)
+{
+  FdSpan s[M];
+#pragma unroll
+  for (int m = 0; m < M; m++) s[m] = fd_span(eta[m], theta[m]);
+  lane_sum<M * NK, 96 * M>(FdTerms<M, NK>{R, s}, F);
 }
 
 // ---------------------------------------------------------------------------
 // Number densities (number_den.f90)
 // ---------------------------------------------------------------------------
 
-// n = c (F_1/2 + beta F_3/2), c = sqrt2/pi^2 (m/hc)^3 beta^1.5: free fermions of
-// mass m (MeV) at temperature kt and degeneracy eta (eq. 20; fxnn, fxnp)
-HNU double fermion_density(const Rules &R, double m, double kt, double eta)
+// c in n = c (F_1/2 + beta F_3/2) for fermions of mass m (MeV) and
+// beta = kt / m: sqrt2/pi^2 (m/hc)^3 beta^1.5 (eq. 20; fxnn, fxnp, lepton)
+HNU double density_coef(double m, double beta) { return sqrt(2.0) / sq(PI) * cube(m / HC) * pow(beta, 1.5); }
+
+// the density of nucleons of mass m at degeneracies eta[0..2] (fxnn, fxnp)
+HNU void fermion_density3(const Rules &R, double m, double kt, const double *eta, double *n)
 {
   const double beta = kt / m;
-  const double c = sqrt(2.0) / sq(PI) * cube(m / HC) * pow(beta, 1.5);
-  double F[2];
-  fermi(R, eta, beta, 2, F);
-  return c * (F[0] + beta * F[1]);
+  const double c = density_coef(m, beta);
+  const double th[3] = {beta, beta, beta};
+  double F[3 * 2];
+  fermi<3, 2>(R, eta, th, F);
+  for (int i = 0; i < 3; i++) n[i] = c * (F[2 * i] + beta * F[2 * i + 1]);
 }
 
-// electrons and positrons at electron degeneracy etae (lepton, number_den.f90:374-395):
-// returns n_e- - n_e+
-HNU double lepton(const Rules &R, double kt, double etae, double *nee, double *nep)
+// electrons and positrons at electron degeneracies etae[0..N) (lepton,
+// number_den.f90:374-395): nl = n_e- - n_e+, and the two densities
+template <int N>
+HNU void lepton(const Rules &R, double kt, const double *etae, double *nl, double *nee, double *nep)
 {
   const double beta = kt / XME;
-  const double c = sqrt(2.0) / sq(PI) * cube(XME / HC) * pow(beta, 1.5);
-  double F[2];
-  fermi(R, etae, beta, 2, F);
-  *nee = c * (F[0] + beta * F[1]);
-  fermi(R, -etae - 2.0 / beta, beta, 2, F);
-  *nep = c * (F[0] + beta * F[1]);
-  return *nee - *nep;
+  const double c = density_coef(XME, beta);
+  double eta[2 * N], th[2 * N];
+  for (int i = 0; i < N; i++) {
+    eta[2 * i] = etae[i];
+    eta[2 * i + 1] = -etae[i] - 2.0 / beta;
+    th[2 * i] = th[2 * i + 1] = beta;
+  }
+  double F[2 * N * 2];
+  fermi<2 * N, 2>(R, eta, th, F);
+  for (int i = 0; i < N; i++) {
+    const double ne = c * (F[4 * i] + beta * F[4 * i + 1]);
+    const double np = c * (F[4 * i + 2] + beta * F[4 * i + 3]);
+    if (nee) nee[i] = ne;
+    if (nep) nep[i] = np;
+    nl[i] = ne - np;
+  }
 }
 
 // mnewt (mnewtf.f90:108-150) with one unknown and the central-difference
 // Jacobian of the usrfun_* routines: solve G(x) = target from x, up to 200
 // trials, stopping when |G(x) - target| <= tolf or the step is <= 1e-20.
-// G is a functor double(double).
-template <class G>
-HNU double newton1(const G &g, double x, double target, double tolf)
+// g(xs, ys) evaluates G at x, x + xacc and x - xacc together.
+template <class G3>
+HNU double newton1(const G3 &g, double x, double target, double tolf)
 {
   for (int k = 0; k < 200; k++) {
     double xacc = fabs(x) * 1.0e-8;
     if (xacc < 1.0e-50) xacc = 1.0e-50;
-    const double f = target - g(x);
-    const double fp = target - g(x + xacc);
-    const double fm = target - g(x - xacc);
+    const double xs[3] = {x, x + xacc, x - xacc};
+    double ys[3];
+    g(xs, ys);
+    const double f = target - ys[0];
+    const double fp = target - ys[1];
+    const double fm = target - ys[2];
     const double fjac = (fp - fm) / (2.0 * xacc);
     double dx = -f;
     if (fabs(dx) <= tolf) return x;
@@ -229,30 +315,32 @@ HNU double newton_tol(double n)
   return tol < 1.0e-50 ? 1.0e-50 : tol;
 }
 
-struct FermionN {
+struct FermionN3 {
   const Rules &R;
   double m, kt;
-  HNU double operator()(double eta) const { return fermion_density(R, m, kt, eta); }
+  HNU void operator()(const double *x, double *y) const { fermion_density3(R, m, kt, x, y); }
 };
-struct LeptonN {
+struct LeptonN3 {
   const Rules &R;
   double kt;
-  HNU double operator()(double eta) const
-  {
-    double a, b;
-    return lepton(R, kt, eta, &a, &b);
-  }
+  HNU void operator()(const double *x, double *y) const { lepton<3>(R, kt, x, y, nullptr, nullptr); }
 };
 
 // degeneracy of neutrons and protons of density n (neta, peta): Newton from -10
-HNU double neta(const Rules &R, double kt, double n) { return newton1(FermionN{R, XMN, kt}, -10.0, n, newton_tol(n)); }
-HNU double peta(const Rules &R, double kt, double n) { return newton1(FermionN{R, XMP, kt}, -10.0, n, newton_tol(n)); }
+HNU double neta(const Rules &R, double kt, double n)
+{
+  return newton1(FermionN3{R, XMN, kt}, -10.0, n, newton_tol(n));
+}
+HNU double peta(const Rules &R, double kt, double n)
+{
+  return newton1(FermionN3{R, XMP, kt}, -10.0, n, newton_tol(n));
+}
 
 // electron degeneracy for the net lepton density n (eeta): Newton from m_e/kt,
 // capped at 0
 HNU double eeta(const Rules &R, double kt, double n)
 {
-  const double e = newton1(LeptonN{R, kt}, 0.510998910 / kt, n, newton_tol(n));
+  const double e = newton1(LeptonN3{R, kt}, 0.510998910 / kt, n, newton_tol(n));
   return e > 0.0 ? 0.0 : e;
 }
 
@@ -260,31 +348,30 @@ HNU double eeta(const Rules &R, double kt, double n)
 // Equations of state (eos.f90), e and p in MeV fm^-3
 // ---------------------------------------------------------------------------
 
-// one fermion species (eos_npe's blocks): p = cp (F_3/2 + beta/2 F_5/2),
-// e = 3/2 cp (F_3/2 + beta F_5/2), cp = 2/3 sqrt2/pi^2 (m/hc)^3 m beta^2.5
-HNU void fermion_ep(const Rules &R, double m, double kt, double eta, double *e, double *p)
-{
-  const double beta = kt / m;
-  const double cp = (double)(2.0f / 3.0f) * sqrt(2.0) / sq(PI) * cube(m / HC) * m * pow(beta, 2.5);
-  const double ce = 3.0 / 2.0 * cp;
-  double F[3];
-  fermi(R, eta, beta, 3, F);  // F_1/2 is computed and unused
-  *p = cp * (F[1] + 0.5 * beta * F[2]);
-  *e = ce * (F[1] + beta * F[2]);
-}
-
-// nucleons and pairs (eos_npe, eos.f90:32-112); the positrons count only where
-// the electron density is positive
+// nucleons and pairs (eos_npe, eos.f90:32-112): for each fermion species
+// p = cp (F_3/2 + beta/2 F_5/2), e = 3/2 cp (F_3/2 + beta F_5/2),
+// cp = 2/3 sqrt2/pi^2 (m/hc)^3 m beta^2.5; the positrons count only where the
+// electron density is positive
 HNU void eos_npe(const Rules &R, double kt, double etan, double etap, double etae, double nee, double *e,
                  double *p)
 {
-  double ee, pe, eep = 0., pep = 0., epr, ppr, en, pn;
-  fermion_ep(R, XME, kt, etae, &ee, &pe);
-  if (nee > 0.0) fermion_ep(R, XME, kt, -etae - 2.0 / (kt / XME), &eep, &pep);
-  fermion_ep(R, XMP, kt, etap, &epr, &ppr);
-  fermion_ep(R, XMN, kt, etan, &en, &pn);
-  *p = pe + pep + ppr + pn;
-  *e = ee + eep + epr + en;
+  const double mass[4] = {XME, XME, XMP, XMN};
+  const double eta[4] = {etae, -etae - 2.0 / (kt / XME), etap, etan};
+  double th[4];
+  for (int s = 0; s < 4; s++) th[s] = kt / mass[s];
+  double F[4 * 3];
+  fermi<4, 3>(R, eta, th, F);  // F_1/2 is computed and unused
+  double ps[4], es[4];
+  for (int s = 0; s < 4; s++) {
+    const double m = mass[s], beta = th[s];
+    const double cp = (double)(2.0f / 3.0f) * sqrt(2.0) / sq(PI) * cube(m / HC) * m * pow(beta, 2.5);
+    const double ce = 3.0 / 2.0 * cp;
+    ps[s] = cp * (F[3 * s + 1] + 0.5 * beta * F[3 * s + 2]);
+    es[s] = ce * (F[3 * s + 1] + beta * F[3 * s + 2]);
+  }
+  if (nee <= 0.0) ps[1] = es[1] = 0.0;
+  *p = ps[0] + ps[1] + ps[2] + ps[3];
+  *e = es[0] + es[1] + es[2] + es[3];
 }
 
 // black-body radiation (eos_rad) and trapped neutrinos with blocking b1, b2 (eos_neu)
@@ -349,13 +436,15 @@ HNU void pair(const Rules &R, double kt, double etae, double *ev1, double *ev2)
   cv = 2.0 * 0.23 - 0.5;
   ca = -0.5;
   const double cv1m = cv * cv + ca * ca, cv2m = cv * cv - ca * ca;
-  double F[4];
-  fermi(R, etae, beta, 4, F);
-  const double u_1 = F[0], u0 = F[0] + beta * F[1], u1 = F[0] + 2.0 * beta * F[1] + beta * beta * F[2];
-  const double u2 = F[0] + 3.0 * beta * F[1] + 3.0 * beta * beta * F[2] + cube(beta) * F[3];
-  fermi(R, -etae - 2.0 / beta, beta, 4, F);
-  const double f_1 = F[0], f0 = F[0] + beta * F[1], f1 = F[0] + 2.0 * beta * F[1] + beta * beta * F[2];
-  const double f2 = F[0] + 3.0 * beta * F[1] + 3.0 * beta * beta * F[2] + cube(beta) * F[3];
+  const double eta[2] = {etae, -etae - 2.0 / beta}, th[2] = {beta, beta};
+  double F[2 * 4];
+  fermi<2, 4>(R, eta, th, F);
+  const double *G = F;
+  const double u_1 = G[0], u0 = G[0] + beta * G[1], u1 = G[0] + 2.0 * beta * G[1] + beta * beta * G[2];
+  const double u2 = G[0] + 3.0 * beta * G[1] + 3.0 * beta * beta * G[2] + cube(beta) * G[3];
+  G = F + 4;
+  const double f_1 = G[0], f0 = G[0] + beta * G[1], f1 = G[0] + 2.0 * beta * G[1] + beta * beta * G[2];
+  const double f2 = G[0] + 3.0 * beta * G[1] + 3.0 * beta * beta * G[2] + cube(beta) * G[3];
   const double a = 8.0 * (f1 * u2 + f2 * u1) - 2.0 * (f_1 * u2 + f2 * u_1) + 7.0 * (f0 * u1 + f1 * u0) +
                    5.0 * (f0 * u_1 + f_1 * u0);
   const double b = f0 * (u1 + u_1) + (f_1 + f1) * u0;
@@ -364,55 +453,67 @@ HNU void pair(const Rules &R, double kt, double etae, double *ev1, double *ev2)
   *ev2 = pre * (cv1m * a + 9.0 * cv2m * b);
 }
 
-// The six weak rates of an integrand family: x sqrt(x^2 - 1/beta^2) (q -+ x)^n
-// times a lepton occupation and a neutrino blocking factor, over the electron
-// energy x in units of kt.  K selects the reaction: 1 n -> p e nu~ on [1/beta, q];
-// 2 p e- -> n nu and 3 n e+ -> p nu~ on [x0, inf).  KIND 0: |1 - b1 f| blocking
-// (func1..3, func1k..3k); 1: |b1 f| absorption (func1r..3r).
+// The weak-rate integrands: x sqrt(x^2 - 1/beta^2) (q -+ x)^POW times an
+// electron or positron occupation and a neutrino blocking factor, over the
+// electron energy x in units of kt.  K selects the reaction: 1 n -> p e nu~
+// on [1/beta, q]; 2 p e- -> n nu and 3 n e+ -> p nu~ on [x0, inf).  KIND 0:
+// the |1 - b1 f| blocking (func1..3, func1k..3k); 1: |b1 f| absorption
+// (func1r..3r).
 template <int K, int KIND, int POW>
-struct Rate {
-  double kt, eta, b1;
-  HNU double operator()(double x) const
+HNU double rate(double x, double kt, double eta, double b1)
+{
+  const double beta = kt / XME;
+  const double q = (XMN - XMP) / kt;
+  double xe, en;
+  if (K == 1) {
+    xe = KIND == 0 ? eta - (x - 1.0 / beta) : (x - 1.0 / beta) - eta;
+    en = q - x;
+  } else if (K == 2) {
+    xe = KIND == 0 ? -eta + (x - 1.0 / beta) : +eta - (x - 1.0 / beta);
+    en = x - q;
+  } else {
+    xe = KIND == 0 ? -eta + (x - 1.0 / beta) : eta - (x - 1.0 / beta);
+    en = x + q;
+  }
+  const double f1 = 1.0 / (exp(xe) + 1.0);
+  const double ex = K == 1 ? exp(q - x) : (K == 2 ? exp(x - q) : exp(x + q));
+  const double f2 = KIND == 0 ? fabs(1.0 - b1 / (ex + 1.0)) : fabs(b1 / (ex + 1.0));
+  const double enp = POW == 3 ? en * en * en : en * en;
+  return x * sqrt(x * x - 1.0 / (beta * beta)) * enp * f1 * f2;
+}
+
+// The rate integrals of one routine as 80 terms: 0..39 the 40-point
+// Gauss-Legendre rule on [a, b] = [m_e, m_n - m_p] / kt for reaction 1
+// (gauss_legendre, gauss_integral.f90:118-219: node e / 2 on the side e & 1,
+// centre c and half-length h), 40..59 the 20-point Gauss-Laguerre rule from
+// (m_n - m_p) / kt for reaction 2 and 60..79 from m_e / kt for reaction 3
+// (gauss_laguerre, gauss_integral.f90:26-113, scale 1).  RK: also the
+// absorption integrands of neutrino() (chem_eq.f90), into accumulators 3..5.
+// The Legendre sums still take the half-length factor.
+template <int POW, bool RK>
+struct RateTerms {
+  const Rules &R;
+  double kt, etae, etaep, b1, c, h;
+  HNU void operator()(int e, int, double *acc) const
   {
-    const double beta = kt / XME;
-    const double q = (XMN - XMP) / kt;
-    double xe, en;
-    if (K == 1) {
-      xe = KIND == 0 ? eta - (x - 1.0 / beta) : (x - 1.0 / beta) - eta;
-      en = q - x;
-    } else if (K == 2) {
-      xe = KIND == 0 ? -eta + (x - 1.0 / beta) : +eta - (x - 1.0 / beta);
-      en = x - q;
+    if (e < 40) {
+      const int j = e >> 1;
+      const double x = c + ((e & 1) ? -h : h) * R.l40x[j];
+      acc[0] += rate<1, 0, POW>(x, kt, etae, b1) * R.l40w[j];
+      if (RK) acc[3] += rate<1, 1, POW>(x, kt, etae, b1) * R.l40w[j];
+    } else if (e < 60) {
+      const int j = e - 40;
+      const double x = (XMN - XMP) / kt + 1.0 * R.g20x[j];
+      acc[1] += rate<2, 0, POW>(x, kt, etae, b1) * R.g20w[j];
+      if (RK) acc[4] += rate<2, 1, POW>(x, kt, etae, b1) * R.g20w[j];
     } else {
-      xe = KIND == 0 ? -eta + (x - 1.0 / beta) : eta - (x - 1.0 / beta);
-      en = x + q;
+      const int j = e - 60;
+      const double x = XME / kt + 1.0 * R.g20x[j];
+      acc[2] += rate<3, 0, POW>(x, kt, etaep, b1) * R.g20w[j];
+      if (RK) acc[5] += rate<3, 1, POW>(x, kt, etaep, b1) * R.g20w[j];
     }
-    const double f1 = 1.0 / (exp(xe) + 1.0);
-    const double ex = K == 1 ? exp(q - x) : (K == 2 ? exp(x - q) : exp(x + q));
-    const double f2 = KIND == 0 ? fabs(1.0 - b1 / (ex + 1.0)) : fabs(b1 / (ex + 1.0));
-    const double enp = POW == 3 ? en * en * en : en * en;
-    return x * sqrt(x * x - 1.0 / (beta * beta)) * enp * f1 * f2;
   }
 };
-
-// 40-point Gauss-Legendre on [a, b] (gauss_legendre, gauss_integral.f90:118-219)
-template <class Fn>
-HNU double legendre40(const Rules &R, const Fn &f, double a, double b)
-{
-  const double c = 0.5 * (a + b), h = 0.5 * (b - a);
-  double s = 0.0;
-  for (int j = 0; j < 20; j++) s = s + (f(c + h * R.l40x[j]) + f(c - h * R.l40x[j])) * R.l40w[j];
-  return s * h;
-}
-
-// 20-point Gauss-Laguerre on [a, inf), scale 1 (gauss_laguerre, gauss_integral.f90:26-113)
-template <class Fn>
-HNU double laguerre20(const Rules &R, const Fn &f, double a)
-{
-  double s = 0.0;
-  for (int j = 0; j < 20; j++) s = s + f(a + 1.0 * R.g20x[j]) * R.g20w[j];
-  return s * 1.0;
-}
 
 // URCA emissivities without blocking (urca, neu_rate.f90:110-160):
 // n -> p e nu~ (evn), p e- -> n nu (evep), n e+ -> p nu~ (even)
@@ -421,9 +522,12 @@ HNU void urca(const Rules &R, double kt, double nn, double np, double etae, doub
 {
   const double t11 = kt * 1.16059e-1;
   const double t6 = cube(t11) * cube(t11);
-  *evn = 1.14473926e37 * t6 * nn * legendre40(R, Rate<1, 0, 3>{kt, etae, 0.0}, XME / kt, (XMN - XMP) / kt);
-  *evep = 1.14473926e37 * t6 * np * laguerre20(R, Rate<2, 0, 3>{kt, etae, 0.0}, (XMN - XMP) / kt);
-  *even = 1.14473926e37 * t6 * nn * laguerre20(R, Rate<3, 0, 3>{kt, etaep, 0.0}, XME / kt);
+  const double a = XME / kt, b = (XMN - XMP) / kt, h = 0.5 * (b - a);
+  double I[3];
+  lane_sum<3, 80>(RateTerms<3, false>{R, kt, etae, etaep, 0.0, 0.5 * (a + b), h}, I);
+  *evn = 1.14473926e37 * t6 * nn * (I[0] * h);
+  *evep = 1.14473926e37 * t6 * np * (I[1] * 1.0);
+  *even = 1.14473926e37 * t6 * nn * (I[2] * 1.0);
 }
 
 // nucleon-nucleon bremsstrahlung (brem) and plasmon decay (plasmon)
@@ -507,16 +611,12 @@ HNU double net_rate(const Rules &R, double b1, double kt, double nn, double np, 
   const double t5 = sq(t11) * sq(t11) * t11;
   if (nn < 0.0) nn = 0.0;
   if (np < 0.0) np = 0.0;
-  const double a = XME / kt, b = (XMN - XMP) / kt;
-  const double f1 = legendre40(R, Rate<1, 0, 2>{kt, etae, b1}, a, b);
-  const double f1r = legendre40(R, Rate<1, 1, 2>{kt, etae, b1}, a, b);
-  const double evn = 2.03813046e35 * t5 * nn * (f1 + f1r);
-  const double f2 = laguerre20(R, Rate<2, 0, 2>{kt, etae, b1}, b);
-  const double f2r = laguerre20(R, Rate<2, 1, 2>{kt, etae, b1}, b);
-  const double evep = 2.03813046e35 * t5 * np * (f2 + f2r);
-  const double f3 = laguerre20(R, Rate<3, 0, 2>{kt, etaep, b1}, a);
-  const double f3r = laguerre20(R, Rate<3, 1, 2>{kt, etaep, b1}, a);
-  const double even = 2.03813046e35 * t5 * nn * (f3 + f3r);
+  const double a = XME / kt, b = (XMN - XMP) / kt, h = 0.5 * (b - a);
+  double I[6];
+  lane_sum<6, 80>(RateTerms<2, true>{R, kt, etae, etaep, b1, 0.5 * (a + b), h}, I);
+  const double evn = 2.03813046e35 * t5 * nn * (I[0] * h + I[3] * h);
+  const double evep = 2.03813046e35 * t5 * np * (I[1] * 1.0 + I[4] * 1.0);
+  const double even = 2.03813046e35 * t5 * nn * (I[2] * 1.0 + I[5] * 1.0);
   if (fabs(evep) < 1.0e-80) return (evep - even - evn) / (fabs(evep) + 1.0e-80);
   return (evep - even - evn) / fabs(evep);
 }
@@ -543,8 +643,8 @@ HNU_NOINLINE double funcnb(const Rules &R, const Nucl &c, double xp)
   const double ne = c.nnucl * xp + c.ne0;
   const double etae = eeta(R, c.kt, ne);
   const double etaep = -etae - 2.0 / beta;
-  double b1 = 0.0, b2 = 0.0, nee, nep;
-  lepton(R, c.kt, etae, &nee, &nep);
+  double b1 = 0.0, b2 = 0.0, nl, nee, nep;
+  lepton<1>(R, c.kt, &etae, &nl, &nee, &nep);
   double e, p, ehe, phe;
   eos_npe(R, c.kt, etan, etap, etae, nee, &e, &p);
   const double pr = p_rad(c.kt), er = 3.0 * pr;
@@ -562,10 +662,13 @@ HNU_NOINLINE double funcnb(const Rules &R, const Nucl &c, double xp)
   return net_rate(R, b1, c.kt, nn, np, etae);
 }
 
-struct FuncNb {
+struct FuncNb3 {
   const Rules &R;
   const Nucl &c;
-  HNU double operator()(double xp) const { return funcnb(R, c, xp); }
+  HNU void operator()(const double *x, double *y) const
+  {
+    for (int i = 0; i < 3; i++) y[i] = funcnb(R, c, x[i]);
+  }
 };
 
 struct Abundance {
@@ -586,7 +689,7 @@ HNU_NOINLINE Abundance abundance(const Rules &R, double rho, double T, double hd
 
   // eqnucl: the proton fraction by Newton on funcnb from 1/2, kept in [0, 1]
   const Nucl c{nb * xn, kt, fabs(1.0 - xn) * nb / 2.0, hdfac, nb};
-  double xp = newton1(FuncNb{R, c}, (1.0 - 0.0) / 2.0, 0.0, newton_tol(c.nnucl));
+  double xp = newton1(FuncNb3{R, c}, (1.0 - 0.0) / 2.0, 0.0, newton_tol(c.nnucl));
   if (xp < 0.0) xp = 0.0;
   if (xp > 1.0) xp = 1.0;
   double etan, etap;
@@ -596,7 +699,8 @@ HNU_NOINLINE Abundance abundance(const Rules &R, double rho, double T, double hd
 
   const double etaep = -etae - 2.0 / beta;
   Abundance a;
-  lepton(R, kt, etae, &a.nee, &a.nep);
+  double nl;
+  lepton<1>(R, kt, &etae, &nl, &a.nee, &a.nep);
   double enucl, pnucl, ehe, phe;
   eos_npe(R, kt, etan, etap, etae, a.nee, &enucl, &pnucl);
   const double prad = p_rad(kt), erad = 3.0 * prad;

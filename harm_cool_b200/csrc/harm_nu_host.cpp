@@ -148,7 +148,7 @@ extern "C" int harm_nu_fermi(const double *eta, const double *theta, long n, dou
   if (n < 0 || (n > 0 && (!eta || !theta || !F))) return fail_with(HARM_E_ARG, "harm_nu_fermi: bad arguments");
   const nu::Rules *R = nu::host_rules();
   if (!R) return fail_with(HARM_E_ARG, "harm_nu_fermi: quadrature root search failed");
-  for (long i = 0; i < n; i++) nu::fermi(*R, eta[i], theta[i], 4, F + 4 * i);
+  for (long i = 0; i < n; i++) nu::fermi<1, 4>(*R, eta + i, theta + i, F + 4 * i);
   return HARM_OK;
 }
 

@@ -9,9 +9,10 @@ radius, cooleos.c:945-960) through calc_cache_val (cooleos.c:171-194).  The
 tables are built once on the host and then uploaded (harm_cool_b200.Eos).
 
 build_tables() lays out the grid and HdFac exactly as the reference does and
-takes the generator as a function, so a caller with the Fortran code brings it
-in; ideal_gas_radiation() is a synthetic stand-in for runs without it (no
-neutrino physics: placeholder power laws for Qnu and tau).
+takes the generator as a function; ideal_gas_radiation() is a synthetic
+stand-in (no neutrino physics: placeholder power laws for Qnu and tau).
+physical_tables() fills the same layout from the library's restatement of
+abundance() (harm_nu.cuh), every node computed on the GPU.
 """
 import math
 
@@ -87,3 +88,26 @@ def build_tables(radii, generator=ideal_gas_radiation, nx=72, ny=72, rho=(1.e2, 
     c = constants(gam, rho, T)
     c["hdfac"] = np.array([hdfac(r) for r in radii])
     return xa, ya, val, c
+
+
+def physical_tables(radii, nx=72, ny=72, rho=(1.e2, 1.e15), T=(1.e4, 1.e18), gam=4. / 3., t_floor=None,
+                    device=0):
+    """Tables of the library's abundance() (harm_cool_b200.nu_tables, on the
+    GPU), laid out as build_tables() lays them out: (xaxis, yaxis, values,
+    constants, info).  With t_floor, only the temperature rows at or above it
+    are generated and the rows below hold NaN, so that a run which reads one
+    of them turns NaN instead of using a made-up value; info says how many
+    nodes were generated and how long the device took."""
+    from . import nu_tables
+    xa, ya = log_axis(nx, *rho), log_axis(ny, *T)
+    hd = np.array([hdfac(r) for r in radii])
+    j0 = 0 if t_floor is None else int(np.searchsorted(ya, t_floor))
+    val = np.full((len(radii), nx, ny, 5), np.nan)
+    sub, ms = nu_tables(xa, ya[j0:], hd, device=device)
+    val[:, :, j0:, :] = sub
+    c = constants(gam, rho, T)
+    c["hdfac"] = hd
+    nodes = len(radii) * nx * (ny - j0)
+    info = {"nodes": nodes, "device_ms": ms, "nodes_per_s": nodes / (ms / 1e3), "first_row": j0,
+            "t_first_row": float(ya[j0]) if j0 < ny else None}
+    return xa, ya, val, c, info
