@@ -226,13 +226,38 @@ struct FdTerms {
   }
 };
 
-// F[m NK + k] = F_{k+1/2}(eta[m], theta[m])
+// F[m NK + k] = F_{k+1/2}(eta[m], theta[m]).  On the device lane m works out
+// the intervals of set m and hands them to the other lanes: the same function
+// of the same arguments, so the same bits, for a fraction of the instructions.
 template <int M, int NK>
 HNU void fermi(const Rules &R, const double *eta, const double *theta, double *F)
 {
   FdSpan s[M];
+#if defined(__CUDA_ARCH__)
+  static_assert(M <= 32, "one lane per set");
+  const int l = threadIdx.x & 31;
+  double e = eta[0], th = theta[0];
 #pragma unroll
+  for (int m = 1; m < M; m++)
+    if (l == m) {
+      e = eta[m];
+      th = theta[m];
+    }
+  const FdSpan mine = fd_span(e, th);
+#pragma unroll
+  for (int m = 0; m < M; m++) {
+    s[m].eta = __shfl_sync(0xffffffffu, mine.eta, m);
+    s[m].theta = __shfl_sync(0xffffffffu, mine.theta, m);
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      s[m].c[q] = __shfl_sync(0xffffffffu, mine.c[q], m);
+      s[m].h[q] = __shfl_sync(0xffffffffu, mine.h[q], m);
+    }
+    s[m].s3 = __shfl_sync(0xffffffffu, mine.s3, m);
+  }
+#else
   for (int m = 0; m < M; m++) s[m] = fd_span(eta[m], theta[m]);
+#endif
   lane_sum<M * NK, 96 * M>(FdTerms<M, NK>{R, s}, F);
 }
 
@@ -244,24 +269,23 @@ HNU void fermi(const Rules &R, const double *eta, const double *theta, double *F
 // beta = kt / m: sqrt2/pi^2 (m/hc)^3 beta^1.5 (eq. 20; fxnn, fxnp, lepton)
 HNU double density_coef(double m, double beta) { return sqrt(2.0) / sq(PI) * cube(m / HC) * pow(beta, 1.5); }
 
-// the density of nucleons of mass m at degeneracies eta[0..2] (fxnn, fxnp)
-HNU void fermion_density3(const Rules &R, double m, double kt, const double *eta, double *n)
+// the density of nucleons with beta = kt / m and coefficient c at
+// degeneracies eta[0..2] (fxnn, fxnp)
+HNU void fermion_density3(const Rules &R, double beta, double c, const double *eta, double *n)
 {
-  const double beta = kt / m;
-  const double c = density_coef(m, beta);
   const double th[3] = {beta, beta, beta};
   double F[3 * 2];
   fermi<3, 2>(R, eta, th, F);
   for (int i = 0; i < 3; i++) n[i] = c * (F[2 * i] + beta * F[2 * i + 1]);
 }
 
-// electrons and positrons at electron degeneracies etae[0..N) (lepton,
-// number_den.f90:374-395): nl = n_e- - n_e+, and the two densities
+// electrons and positrons at electron degeneracies etae[0..N), beta = kt / m_e
+// and density coefficient c (lepton, number_den.f90:374-395): nl = n_e- - n_e+,
+// and the two densities
 template <int N>
-HNU void lepton(const Rules &R, double kt, const double *etae, double *nl, double *nee, double *nep)
+HNU void lepton_bc(const Rules &R, double beta, double c, const double *etae, double *nl, double *nee,
+                   double *nep)
 {
-  const double beta = kt / XME;
-  const double c = density_coef(XME, beta);
   double eta[2 * N], th[2 * N];
   for (int i = 0; i < N; i++) {
     eta[2 * i] = etae[i];
@@ -277,6 +301,13 @@ HNU void lepton(const Rules &R, double kt, const double *etae, double *nl, doubl
     if (nep) nep[i] = np;
     nl[i] = ne - np;
   }
+}
+
+template <int N>
+HNU void lepton(const Rules &R, double kt, const double *etae, double *nl, double *nee, double *nep)
+{
+  const double beta = kt / XME;
+  lepton_bc<N>(R, beta, density_coef(XME, beta), etae, nl, nee, nep);
 }
 
 // mnewt (mnewtf.f90:108-150) with one unknown and the central-difference
@@ -315,32 +346,36 @@ HNU double newton_tol(double n)
   return tol < 1.0e-50 ? 1.0e-50 : tol;
 }
 
+// the densities a Newton solve evaluates, with beta and the density
+// coefficient (a pow()) worked out once per solve
 struct FermionN3 {
   const Rules &R;
-  double m, kt;
-  HNU void operator()(const double *x, double *y) const { fermion_density3(R, m, kt, x, y); }
+  double beta, c;
+  HNU FermionN3(const Rules &r, double m, double kt) : R(r), beta(kt / m), c(density_coef(m, kt / m)) {}
+  HNU void operator()(const double *x, double *y) const { fermion_density3(R, beta, c, x, y); }
 };
 struct LeptonN3 {
   const Rules &R;
-  double kt;
-  HNU void operator()(const double *x, double *y) const { lepton<3>(R, kt, x, y, nullptr, nullptr); }
+  double beta, c;
+  HNU LeptonN3(const Rules &r, double kt) : R(r), beta(kt / XME), c(density_coef(XME, kt / XME)) {}
+  HNU void operator()(const double *x, double *y) const { lepton_bc<3>(R, beta, c, x, y, nullptr, nullptr); }
 };
 
 // degeneracy of neutrons and protons of density n (neta, peta): Newton from -10
 HNU double neta(const Rules &R, double kt, double n)
 {
-  return newton1(FermionN3{R, XMN, kt}, -10.0, n, newton_tol(n));
+  return newton1(FermionN3(R, XMN, kt), -10.0, n, newton_tol(n));
 }
 HNU double peta(const Rules &R, double kt, double n)
 {
-  return newton1(FermionN3{R, XMP, kt}, -10.0, n, newton_tol(n));
+  return newton1(FermionN3(R, XMP, kt), -10.0, n, newton_tol(n));
 }
 
 // electron degeneracy for the net lepton density n (eeta): Newton from m_e/kt,
 // capped at 0
 HNU double eeta(const Rules &R, double kt, double n)
 {
-  const double e = newton1(LeptonN3{R, kt}, 0.510998910 / kt, n, newton_tol(n));
+  const double e = newton1(LeptonN3(R, kt), 0.510998910 / kt, n, newton_tol(n));
   return e > 0.0 ? 0.0 : e;
 }
 
