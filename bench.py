@@ -645,9 +645,8 @@ def run_cool(args):
                                                  (1, args.warmup - 1, args.steps))
         line["tables"] = gen
     ctx.close()
-    if not args.no_mixed and args.cool_tables == "physics":
-        # the FP32 copies are scaled per plane by a power of two, which NaN rows
-        # and 240 binary orders of magnitude defeat
+    cm = None
+    if not args.no_mixed and args.cool_tables == "physics" and gen["first_row"] > 0:
         line["mixed"] = {"unavailable": "the FP32 table copies are scaled per plane from the values' range, "
                                         "which the NaN rows below the generated ones leave undefined"}
     elif not args.no_mixed:
@@ -655,7 +654,13 @@ def run_cool(args):
         cm = hc.Context(pr)
         cm.init_torus()
         cm.set_precision(hc.Context.MIXED)
-        cm.set_eos(eos)
+        try:
+            cm.set_eos(eos)
+        except hc.HarmError as ex:  # tables whose values float cannot scale
+            line["mixed"] = {"unavailable": str(ex)}
+            cm.close()
+            cm = None
+    if cm is not None:
         cm.tracers_put(ids, X)
         cm.run(args.warmup)
         sampler = ClockSampler(0)
