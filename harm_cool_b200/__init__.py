@@ -175,6 +175,8 @@ _SIGNATURES = {
     "harm_fp64_peak": (ctypes.c_int, [ctypes.c_int, _DP]),
     "harm_div_check": (ctypes.c_int, [ctypes.c_int, ctypes.c_long, ctypes.c_ulonglong,
                                       ctypes.POINTER(ctypes.c_ulonglong)]),
+    "harm_pow_check": (ctypes.c_int, [ctypes.c_int, ctypes.c_long, ctypes.c_ulonglong,
+                                      ctypes.POINTER(ctypes.c_ulonglong)]),
     "harm_nu_rules": (ctypes.c_int, [_DP]),
     "harm_nu_fermi": (ctypes.c_int, [_DP, _DP, ctypes.c_long, _DP]),
     "harm_nu_abundance": (ctypes.c_int, [_DP, _DP, _DP, ctypes.c_long, ctypes.c_int, _DP]),
@@ -285,6 +287,14 @@ def nu_tables(xaxis, yaxis, hdfac, device=0, slice_nodes=0):
     _check(library().harm_nu_tables(device, _dp(xaxis), len(xaxis), _dp(yaxis), len(yaxis), _dp(hdfac), len(hdfac),
                                      slice_nodes, _dp(val), ctypes.byref(ms)))
     return val, ms.value
+
+
+def pow_check(n, seed=1, device=0):
+    """The fall-back inversions' cube-root power against the general one on the
+    device: (samples that differ, samples left to the general path)."""
+    c = (ctypes.c_ulonglong * 2)()
+    _check(library().harm_pow_check(device, n, seed, c))
+    return int(c[0]), int(c[1])
 
 
 def _check(rc):

@@ -126,7 +126,48 @@ __global__ void k_div_check(long n, unsigned long long seed, unsigned long long 
   atomicAdd(&counts[1], mid);
 }
 
+// pow_third (harm_pow.cuh) against the general double-double path pow_dd:
+// x with a random significand and an exponent in [-700, 699], y = RN(4/3) or
+// RN(4/3) - 1.  counts[0]: samples where pow_third decided and differs from
+// pow_dd in any bit; counts[1]: samples it left to pow_dd.
+__global__ void k_pow_check(long n, unsigned long long seed, unsigned long long *counts)
+{
+  unsigned long long bad = 0, undecided = 0;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    unsigned long long s = seed ^ (0x632be59bd9b4e019ULL * (unsigned long long)(t + 1));
+    const unsigned long long r0 = splitmix64(s), r1 = splitmix64(s);
+    const double x = make_double(r1, (int)(r0 % 1400) - 700, false);
+    const double y = (r0 >> 32) & 1 ? 1.3333333333333333 : 0.33333333333333326;
+    double f;
+    if (pow_third(x, y, f)) {
+      const double g = pow_dd(x, y);
+      if (__double_as_longlong(f) != __double_as_longlong(g)) bad++;
+    } else {
+      undecided++;
+    }
+  }
+  atomicAdd(&counts[0], bad);
+  atomicAdd(&counts[1], undecided);
+}
+
 }  // namespace harm
+
+extern "C" int harm_pow_check(int device, long n, unsigned long long seed, unsigned long long *counts)
+{
+  using namespace harm;
+  if (!counts || n < 0) return fail_with(HARM_E_ARG, "harm_pow_check: bad arguments");
+  CK(cudaSetDevice(device));
+  unsigned long long *d = nullptr;
+  CK(cudaMalloc(&d, 2 * sizeof(unsigned long long)));
+  CK(cudaMemset(d, 0, 2 * sizeof(unsigned long long)));
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  k_pow_check<<<8 * sms, 256>>>(n, seed, d);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(counts, d, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  cudaFree(d);
+  return HARM_OK;
+}
 
 extern "C" int harm_div_check(int device, long n, unsigned long long seed, unsigned long long *counts)
 {

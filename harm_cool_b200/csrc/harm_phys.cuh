@@ -603,6 +603,7 @@ static __device__ __noinline__ int u2p_body_vsq2fix1(U2P &c, const double *U, co
   int n_iter = 0, i_extra = 0, doing_extra = 0;
   bool keep = true;
   while (keep) {
+    if (x != x) return 201;  // as in Utoprim_1dfix1 below: NaN to the end, then failure 201
     double pp, rr, uu;
     double Wc = W_of_vsq_fix(c, x, pp, rr, uu);
     double Wsq = Wc * Wc, W3 = Wc * Wsq;
@@ -655,6 +656,9 @@ static __device__ __noinline__ int gnr2_rho(const U2P &c, double &x)
   int n_iter = 0;
   bool keep = true;
   while (keep) {
+    // a NaN iterate stays NaN through every remaining trial, and the solve
+    // then ends in failure (2) with x NaN: return that now
+    if (x != x) return 2;
     double A = c.D * c.D;
     double B0 = A * GAMMA * c.K_atm;
     double B = B0 / (GAMMA - 1.);
@@ -736,6 +740,10 @@ static __device__ __noinline__ int u2p_body_fix1(U2P &c, const double *U, const 
   int n_iter = 0, i_extra = 0, doing_extra = 0;
   bool keep = true;
   while (keep) {
+    // once W is NaN every remaining trial gives NaN, and the inversion ends in
+    // failure 201 with prim untouched: return that now (c is the caller's
+    // scratch and is discarded)
+    if (x != x) return 201;
     double dx;
     func_1d_orig1(c, x, dx, f, df);
     x += dx;

@@ -15,7 +15,8 @@
 // |s| <= 0.1716 (21 terms reach 2^-107); exp r by r = k ln2 + r', Taylor
 // series of r'/1024 (8 terms) squared ten times.  The constants are 1/(2k+1),
 // 1/n! and ln 2 split into the nearest double and the nearest double to the
-// remainder.
+// remainder.  The two exponents of the gamma = 4/3 law take a cheaper path
+// through the cube root (pow_third), which gives the same rounded results.
 #pragma once
 
 namespace harm {
@@ -120,16 +121,66 @@ __device__ __forceinline__ double dd_exp_rn(DD z)
   return ldexp(t.hi, (int)k);  // t.hi is t rounded to nearest; the scaling is exact
 }
 
+// x^y for the exponents of the gamma = 4/3 law, y = RN(4/3) and RN(4/3) - 1,
+// which the fall-back inversions raise densities to in their inner loops.
+// Both are k/3 + d with k = 4 or 1 and the same offset d = -2^-52/3 exactly
+// (4/3 rounds down by a third of an ulp), so
+//   x^y = (x^(1/3))^k (1 + d ln x + (d ln x)^2/2 + ...),  |d ln x| < 5.2e-14.
+// The cube root is cbrt(x) refined by one Newton step with its residual
+// x - c^3 formed in double-double: the step squares cbrt's relative error
+// (below 2^-51), and the residual and the correction are good to 2^-101.
+// With the product by x and the first-order term, the double-double result
+// is within 2^-88 of x^y.  It is returned rounded when every value within
+// 2^-84 of it rounds the same way, and the exact x^y, within 2^-88, is one of
+// them; otherwise (about once in 2^31 draws) the caller takes the general
+// path.  Arguments: 2^-700 <= x <= 2^700, so that the result and its ulp are
+// normal doubles.
+__device__ __forceinline__ bool pow_third(double x, double y, double &out)
+{
+  int k;
+  if (y == 1.3333333333333333) k = 4;          // RN(4/3)
+  else if (y == 0.33333333333333326) k = 1;    // RN(4/3) - 1, exact
+  else return false;
+  if (!(x >= 0x1p-700 && x <= 0x1p700)) return false;
+  const double c0 = cbrt(x);
+  // c0^3 = q + q_lo to 2^-104; x - q is exact (q is within a factor 2 of x)
+  const double s = c0 * c0, s_lo = fma(c0, c0, -s);
+  const double q = s * c0, q_lo = fma(s, c0, -q) + s_lo * c0;
+  const double r = (x - q) - q_lo;
+  const DD c = dd_fast_two_sum(c0, r / (3.0 * s));
+  const DD P = (k == 4) ? dd_mul_d(c, x) : c;
+  const double t = -(0x1p-52 / 3.0) * log(x);  // d ln x
+  const DD v = dd_add(P, DD{P.hi * t, 0.});
+  // v.hi is v rounded, |v.lo| <= half an ulp of v.hi; the spacing below a power
+  // of two is half the spacing above
+  const long long b = __double_as_longlong(v.hi);
+  const double ulp = __longlong_as_double((((b >> 52) & 0x7ff) - 52) << 52);
+  const double half = (v.lo < 0. && (b & 0xfffffffffffffLL) == 0) ? 0.25 * ulp : 0.5 * ulp;
+  if (fabs(v.lo) + v.hi * 0x1p-84 < half) {
+    out = v.hi;
+    return true;
+  }
+  return false;
+}
+
 // x^y rounded to nearest for finite x > 0 and finite y with |y ln x| <= 700;
 // every other case (zero, negative, infinite or NaN arguments, over- and
-// underflow) goes to pow()
-static __device__ __noinline__ double pow_cr(double x, double y)
+// underflow) goes to pow().  pow_dd is the general path; pow_cr tries
+// pow_third first.
+__device__ __forceinline__ double pow_dd(double x, double y)
 {
   if (!(x > 0.) || !isfinite(x) || !isfinite(y)) return pow(x, y);
   if (y == 0.) return 1.;
   const DD z = dd_mul_d(dd_log(x), y);
   if (!(fabs(z.hi) <= 700.)) return pow(x, y);
   return dd_exp_rn(z);
+}
+
+static __device__ __noinline__ double pow_cr(double x, double y)
+{
+  double r;
+  if (pow_third(x, y, r)) return r;
+  return pow_dd(x, y);
 }
 
 }  // namespace harm

@@ -360,6 +360,11 @@ int harm_fp64_peak(int device, double *out);
    (0 expected); counts[1]: near-midpoint samples drawn.  A self-check with no
    counterpart in the reference. */
 int harm_div_check(int device, long n, unsigned long long seed, unsigned long long *counts);
+/* The fall-back inversions' power for the gamma = 4/3 exponents (a cube root
+   refined in double-double) against the general double-double power, on n
+   seeded random densities: counts[0] = results that differ in any bit,
+   counts[1] = samples the cube-root path left to the general one. */
+int harm_pow_check(int device, long n, unsigned long long seed, unsigned long long *counts);
 
 /* ---- run-time COOL_EOS (cooleos.c, cache4d.c, akima.c, mnewt.h) ---- */
 

@@ -20,7 +20,25 @@ def test_pow_cr_is_the_correctly_rounded_power(harm_lib):
     rng = np.random.default_rng(3)
     n = 4000
     x = 10 ** rng.uniform(-30, 5, n)
-    y = rng.choice([4. / 3., 1. / 3., 5. / 3., 2., 0.5, 1.4], n)
+    y = rng.choice([4. / 3., 4. / 3. - 1., 1. / 3., 5. / 3., 2., 0.5, 1.4], n)
+    got = hc.pow_batch(x, y)
+    want = np.array([correctly_rounded_pow(a, b) for a, b in zip(x, y)])
+    np.testing.assert_array_equal(got, want)
+
+
+def test_cube_root_path_of_the_gamma_law_exponents(harm_lib):
+    """x^RN(4/3) and x^(RN(4/3) - 1), the fall-backs' exponents, through the
+    cube root refined in double-double (pow_third) against the general
+    double-double path, on 2^27 random x in [2^-700, 2^700]: the same bits
+    wherever the cube-root path decides, and it leaves about one draw in 2^31
+    to the general path; then against 50-digit arithmetic over the range."""
+    import harm_cool_b200 as hc
+    bad, undecided = hc.pow_check(1 << 27, seed=11)
+    assert bad == 0
+    assert undecided <= 64, undecided
+    rng = np.random.default_rng(5)
+    x = 2.0 ** rng.uniform(-700, 700, 3000)
+    y = rng.choice([4. / 3., 4. / 3. - 1.], 3000)
     got = hc.pow_batch(x, y)
     want = np.array([correctly_rounded_pow(a, b) for a, b in zip(x, y)])
     np.testing.assert_array_equal(got, want)
@@ -36,7 +54,7 @@ def test_pow_cr_against_the_host_libm(harm_lib):
     rng = np.random.default_rng(4)
     n = 200000
     x = 10 ** rng.uniform(-30, 5, n)
-    y = rng.choice([4. / 3., 1. / 3., 5. / 3.], n)
+    y = rng.choice([4. / 3., 4. / 3. - 1., 1. / 3., 5. / 3.], n)
     got = hc.pow_batch(x, y)
     host = np.array([math.pow(a, b) for a, b in zip(x.tolist(), y.tolist())])
     ulps = np.abs(got.view(np.int64) - host.view(np.int64))
