@@ -129,6 +129,7 @@ _SIGNATURES = {
     "harm_run_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _DP]),
     "harm_adjoint_mass_in": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _DP, _DP, _DP]),
     "harm_step_ch_host_timed": (ctypes.c_int, [ctypes.c_void_p, _DP, ctypes.c_int, _DP]),
+    "harm_run_host": (ctypes.c_int, [ctypes.c_void_p, _DP, ctypes.c_int]),
     "harm_time_kernels": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _DP]),
     "harm_fixup": (ctypes.c_int, [ctypes.c_void_p, _DP]),
     "harm_bound_prim": (ctypes.c_int, [ctypes.c_void_p, _DP]),
@@ -575,7 +576,7 @@ class Context:
         return ms.value
 
     def step_ch_host_timed(self, p, nsteps):
-        """nsteps of step_ch_host() (upload, step, download each) timed on the device, in ms."""
+        """run_host() timed on the device, in ms."""
         assert p.flags["C_CONTIGUOUS"] and p.dtype == np.float64 and p.shape == self.shape + (NPR,)
         ms = ctypes.c_double()
         _check(self.lib.harm_step_ch_host_timed(self.h, _dp(p), nsteps, ctypes.byref(ms)))
@@ -689,6 +690,12 @@ class Context:
         """step_ch() on a host primitive array, in place (upload, step, download)."""
         assert p.flags["C_CONTIGUOUS"] and p.dtype == np.float64 and p.shape == self.shape + (NPR,)
         _check(self.lib.harm_step_ch_host(self.h, _dp(p)))
+
+    def run_host(self, p, nsteps):
+        """nsteps of step_ch_host() on p in place, each step's upload overlapped
+        with the previous step's download (harm_run_host)."""
+        assert p.flags["C_CONTIGUOUS"] and p.dtype == np.float64 and p.shape == self.shape + (NPR,)
+        _check(self.lib.harm_run_host(self.h, _dp(p), nsteps))
 
     def _on_array(self, fn, pv):
         assert pv.flags["C_CONTIGUOUS"] and pv.dtype == np.float64 and pv.shape == self.shape + (NPR,)

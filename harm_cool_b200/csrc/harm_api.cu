@@ -1172,28 +1172,92 @@ extern "C" int harm_run_timed(harm_ctx *h, int nsteps, double *ms)
   return harm_sync(h);
 }
 
+// nsteps of (upload p, step, download into p), the state passing through the
+// host array between steps, as nsteps calls of harm_step_ch_host move it.
+// The copies run on two streams of their own, cut into chunks: the upload of
+// chunk c for step s+1 waits only for the download of chunk c of step s, so
+// the two directions of the link carry the two copies at once.  Both copies
+// go through the staging buffer, chunk by chunk in the same order, and the
+// layout kernels wait for a whole copy.  *ms (may be NULL): the device time
+// from the first upload to the last download.
+static int run_host(Ctx *x, double *p, int nsteps, double *ms)
+{
+  const int h0 = x->D.n3 > 1 ? 1 : 0;
+  const size_t nb = (size_t)8 * x->D.cells() * sizeof(double);
+  constexpr int C = 16;
+  const size_t chunk = ((nb / C + 4095) / 4096) * 4096;
+  struct Res {
+    cudaStream_t up = nullptr, dn = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr, ready = nullptr, uploaded = nullptr, done = nullptr, dc[C] = {};
+    ~Res()
+    {
+      for (cudaEvent_t e : dc)
+        if (e) cudaEventDestroy(e);
+      for (cudaEvent_t e : {t0, t1, ready, uploaded, done})
+        if (e) cudaEventDestroy(e);
+      if (up) cudaStreamDestroy(up);
+      if (dn) cudaStreamDestroy(dn);
+    }
+  } r;
+  CK(cudaStreamCreateWithFlags(&r.up, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&r.dn, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&r.t0));
+  CK(cudaEventCreate(&r.t1));
+  for (cudaEvent_t *e : {&r.ready, &r.uploaded, &r.done}) CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  for (cudaEvent_t &e : r.dc) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  CK(cudaEventRecord(r.t0, x->stream));
+  CK(cudaStreamWaitEvent(r.up, r.t0, 0));
+  for (int s = 0; s < nsteps; s++) {
+    for (int c = 0; c < C; c++) {
+      const size_t off = c * chunk;
+      if (off >= nb) break;
+      if (s > 0) CK(cudaStreamWaitEvent(r.up, r.dc[c], 0));
+      CK(cudaMemcpyAsync((char *)x->stage + off, (const char *)p + off, nb - off < chunk ? nb - off : chunk,
+                         cudaMemcpyHostToDevice, r.up));
+    }
+    CK(cudaEventRecord(r.uploaded, r.up));
+    CK(cudaStreamWaitEvent(x->stream, r.uploaded, 0));
+    k_from_host<<<148 * 8, 256, 0, x->stream>>>(x->G, h0, x->stage, x->p, nullptr, x->pflag);
+    CK(cudaGetLastError());
+    int rc = launch_step(x);
+    if (rc) return rc;
+    k_to_host<<<148 * 8, 256, 0, x->stream>>>(x->G, h0, x->p, x->stage, x->pflag, nullptr);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(r.ready, x->stream));
+    CK(cudaStreamWaitEvent(r.dn, r.ready, 0));
+    for (int c = 0; c < C; c++) {
+      const size_t off = c * chunk;
+      if (off >= nb) break;
+      CK(cudaMemcpyAsync((char *)p + off, (const char *)x->stage + off, nb - off < chunk ? nb - off : chunk,
+                         cudaMemcpyDeviceToHost, r.dn));
+      CK(cudaEventRecord(r.dc[c], r.dn));
+    }
+  }
+  CK(cudaEventRecord(r.done, r.dn));
+  CK(cudaStreamWaitEvent(x->stream, r.done, 0));
+  CK(cudaEventRecord(r.t1, x->stream));
+  CK(cudaEventSynchronize(r.t1));
+  if (ms) {
+    float f;
+    CK(cudaEventElapsedTime(&f, r.t0, r.t1));
+    *ms = f;
+  }
+  return HARM_OK;
+}
+
+extern "C" int harm_run_host(harm_ctx *h, double *p, int nsteps)
+{
+  if (!h || !p || nsteps < 0) return fail_with(HARM_E_ARG, "bad argument");
+  int rc = run_host(&h->x, p, nsteps, nullptr);
+  if (rc) return rc;
+  return harm_sync(h);
+}
+
 extern "C" int harm_step_ch_host_timed(harm_ctx *h, double *p, int nsteps, double *ms)
 {
   if (!h || !p || !ms || nsteps < 0) return fail_with(HARM_E_ARG, "bad argument");
-  Ctx *x = &h->x;
-  EventPair e;
-  CK(cudaEventCreate(&e.a));
-  CK(cudaEventCreate(&e.b));
-  CK(cudaEventRecord(e.a, x->stream));
-  for (int s = 0; s < nsteps; s++) {
-    int rc = put_prims(x, p, nullptr, x->p);
-    if (rc) return rc;
-    rc = launch_step(x);
-    if (rc) return rc;
-    k_to_host<<<148 * 8, 256, 0, x->stream>>>(x->G, x->D.n3 > 1 ? 1 : 0, x->p, x->stage, x->pflag, nullptr);
-    CK(cudaMemcpyAsync(p, x->stage, (size_t)8 * x->D.cells() * sizeof(double), cudaMemcpyDeviceToHost,
-                       x->stream));
-  }
-  CK(cudaEventRecord(e.b, x->stream));
-  CK(cudaEventSynchronize(e.b));
-  float f;
-  CK(cudaEventElapsedTime(&f, e.a, e.b));
-  *ms = f;
+  int rc = run_host(&h->x, p, nsteps, ms);
+  if (rc) return rc;
   return harm_sync(h);
 }
 

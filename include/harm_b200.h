@@ -148,8 +148,14 @@ int harm_step_ch_host(harm_ctx *ctx, double *p);
 /* harm_run() with the elapsed device time of the n graph launches in *ms. */
 int harm_run_timed(harm_ctx *ctx, int nsteps, double *ms);
 
-/* nsteps of harm_step_ch_host() (upload, step, download per step, p in
-   pinned host memory) with the elapsed device time in *ms. */
+/* nsteps steps with the state in the host array p: each step uploads p,
+   steps and downloads into p, as nsteps calls of harm_step_ch_host() do.  The
+   upload of each step's input is cut into chunks that follow the previous
+   step's download chunk by chunk, so that with p in pinned memory the link
+   carries both directions at once.  Returns when p holds the final state. */
+int harm_run_host(harm_ctx *ctx, double *p, int nsteps);
+
+/* harm_run_host() with the elapsed device time in *ms. */
 int harm_step_ch_host_timed(harm_ctx *ctx, double *p, int nsteps, double *ms);
 
 /* Runs reps ordinary steps launched kernel by kernel with a CUDA event after

@@ -259,3 +259,30 @@ def test_fallback_inversions_match_reference_kat(hc):
         ulps = np.abs(a.view(np.int64) - b.view(np.int64))
         assert ulps.max() <= 1, name
         assert np.mean(ulps == 0) >= 0.995, (name, np.mean(ulps == 0))
+
+
+@pytest.mark.parametrize("shape", [(48, 40, 1), (24, 20, 6)])
+def test_host_array_run_matches_step_by_step_calls(shape, hc):
+    """harm_run_host (each step's upload overlapped with the previous step's
+    download, chunk by chunk) leaves the host array exactly where the same
+    number of harm_step_ch_host calls leaves it, and so does its timed form"""
+    pr = hc.torus_problem(*shape)
+    a = hc.Context(pr)
+    a.init_torus()
+    p0 = a.get_prims()
+    pa = p0.copy()
+    for _ in range(4):
+        a.step_ch_host(pa)
+    ta = a.time()
+    b = hc.Context(pr)
+    b.init_torus()
+    pb = p0.copy()
+    b.run_host(pb, 4)
+    assert np.array_equal(pa, pb) and b.time() == ta
+    c = hc.Context(pr)
+    c.init_torus()
+    pc = p0.copy()
+    assert c.step_ch_host_timed(pc, 4) > 0
+    assert np.array_equal(pa, pc) and c.time() == ta
+    for x in (a, b, c):
+        x.close()
