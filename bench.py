@@ -516,61 +516,39 @@ def tracers_by_density(np, pr, p, n, seed):
     return ids, X
 
 
-def generator_cpu_rate(np, hc, xa, ya, hd, seed, nodes=96):
-    """abundance() on the host's cores over a random sample of the generated
-    nodes: the CPU rate beside the device's (the reference's own generator is
-    Fortran, which this box cannot compile)."""
+def generator_cpu_rate(np, hc, xa, ya, hd, mask, seed, nodes=96):
+    """abundance() on the host's cores over a random sample of the computed
+    nodes (mask): the CPU rate beside the device's (the reference's own
+    generator is Fortran, which this box cannot compile)."""
     rng = np.random.default_rng(seed)
-    i, j, t = rng.integers(len(xa), size=nodes), rng.integers(len(ya), size=nodes), rng.integers(len(hd), size=nodes)
+    t, i, j = np.nonzero(mask)
+    pick = rng.choice(len(t), size=min(nodes, len(t)), replace=False)
     t0 = time.perf_counter()
-    hc.nu_abundance(xa[i], ya[j], hd[t])
+    hc.nu_abundance(xa[i[pick]], ya[j[pick]], hd[t[pick]])
     s = time.perf_counter() - t0
-    return {"cpu_nodes_per_s": nodes / s, "cpu_cores": os.cpu_count(),
-            "cpu_sample": "%d random nodes of the generated rows, all cores" % nodes}
-
-
-def floor_rows_read(np, hc, eos_tables, pr, xa, ya, val, consts, gen, ids, X, pa, nsteps):
-    """Whether the run read a table row below the generated ones: the same steps
-    (nsteps: the step counts of the run's calls) again with those rows filled
-    by the synthetic stand-in instead of NaN.  A
-    temperature solve that reads NaN falls back to the gamma law, one that
-    reads the stand-in converges on it, so the two runs part wherever such a
-    row was read, and end bit-identical where none was."""
-    j0 = gen["first_row"]
-    if j0 == 0:
-        return False
-    val2 = val.copy()
-    R, TT = np.meshgrid(xa, ya[:j0], indexing="ij")
-    e, p, qnu, tau, nee, nep = eos_tables.ideal_gas_radiation(R, TT, 1.0)
-    for t in range(val.shape[0]):
-        val2[t, :, :j0, 0], val2[t, :, :j0, 1], val2[t, :, :j0, 2], val2[t, :, :j0, 3] = e, p, qnu, tau
-        val2[t, :, :j0, 4] = (nee - nep) / (R / 1.66e15)
-    eos2 = hc.Eos(xa, ya, val2, consts)
-    c2 = hc.Context(pr)
-    c2.init_torus()
-    c2.set_eos(eos2)
-    c2.tracers_put(ids, X)
-    for k in nsteps:  # the seeding step, the warm-up and the timed steps, as the run took them
-        c2.run(k)
-    pb = c2.get_prims()
-    c2.close()
-    eos2.close()
-    return not np.array_equal(pa, pb, equal_nan=True)
+    return {"cpu_nodes_per_s": len(pick) / s, "cpu_cores": os.cpu_count(),
+            "cpu_sample": "%d random nodes of the computed ones, all cores" % len(pick)}
 
 
 def run_cool(args):
     """The COOL_EOS step on the 256x256 torus of the reference's init.c literals
     (a=0.6, rin=4, rmax=11.8, beta=50; cooleos.c's 3 Msun hole and units), FP64,
-    with the reference's 72x72 per-radius tables built on the host by the
-    synthetic ideal-gas-plus-radiation generator of harm_cool_b200.eos_tables in
-    place of the Fortran EOS, and 1e5 tracer particles seeded in proportion to
-    the rest mass.  The first step seeds the per-zone temperature guesses row by
-    row and runs outside the timed region."""
+    with per-radius tables, and 1e5 tracer particles seeded in proportion to the
+    rest mass.  Tables: the reference's 72x72 grid or BASELINE's 200x200 grid
+    from the synthetic ideal-gas-plus-radiation generator of
+    harm_cool_b200.eos_tables, or ("physics") the 200x200 grid from the
+    library's abundance() on the GPU, its nodes computed as the run reads them
+    (eos_tables.on_demand: the whole run is repeated until it reads no node that
+    is not computed, and that last run is the one reported).  The first step
+    seeds the per-zone temperature guesses row by row and runs outside the
+    timed region."""
     import numpy as np
     import harm_cool_b200 as hc
     from harm_cool_b200 import eos_tables
     n = args.cool_n
     pr = hc.torus_problem(n, n, 1, a=0.6, rin=4.0, rmax=11.8, beta=50.0)
+    args.steps = max(args.steps, 200)  # a few ms per step: enough for the clock sampler to see the run
+    gen = None
     if args.cool_tables == "reference":
         # cooleos.c:924-940: 72 x 72 over rho 1e2..1e15 g/cm^3, T 1e4..1e18 K
         xa, ya, val, consts = eos_tables.build_tables(eos_tables.zone_radii(pr), gam=pr.params.gam)
@@ -578,59 +556,79 @@ def run_cool(args):
     else:
         # 200 x 200 over rho 1e4..1e14 g/cm^3, T 1e8..1e12 K, and a density unit that
         # puts the torus maximum (rho = 1 in code units) at 1e11 g/cm^3
-        grid = dict(nx=200, ny=200, rho=(1.e4, 1.e14), T=(1.e8, 1.e12), gam=pr.params.gam)
         if args.cool_tables == "physics":
-            floor = args.cool_t_floor if args.cool_t_floor > 0 else None
-            xa, ya, val, consts, gen = eos_tables.physical_tables(eos_tables.zone_radii(pr), t_floor=floor, **grid)
-            gen.update(generator_cpu_rate(np, hc, xa, ya[gen["first_row"]:], consts["hdfac"], args.seed))
+            xa, ya = eos_tables.log_axis(200, 1.e4, 1.e14), eos_tables.log_axis(200, 1.e8, 1.e12)
+            consts = eos_tables.constants(pr.params.gam, (1.e4, 1.e14), (1.e8, 1.e12))
+            consts["hdfac"] = np.array([eos_tables.hdfac(r) for r in eos_tables.zone_radii(pr)])
+            val = None
         else:
-            xa, ya, val, consts = eos_tables.build_tables(eos_tables.zone_radii(pr), **grid)
+            xa, ya, val, consts = eos_tables.build_tables(eos_tables.zone_radii(pr), nx=200, ny=200,
+                                                          rho=(1.e4, 1.e14), T=(1.e8, 1.e12), gam=pr.params.gam)
         consts["rho_unit"] = 1.e11
         consts["u_unit"] = consts["p_unit"] = 1.e11 * eos_tables.CL * eos_tables.CL
         tables = "200x200 per-radius tables (rho 1e4-1e14, T 1e8-1e12), torus maximum at 1e11 g/cm^3"
-    eos = hc.Eos(xa, ya, val, consts)
-    ctx = hc.Context(pr)
-    ctx.init_torus()
-    ctx.set_eos(eos)
-    ids, X = tracers_by_density(np, pr, ctx.get_prims(), args.cool_tracers, args.seed)
-    ctx.tracers_put(ids, X)
-    t0 = time.perf_counter()
-    ctx.run(1)                       # the seeding step
-    seed_s = time.perf_counter() - t0
-    ctx.run(args.warmup - 1)
-    # a few ms per step: time enough steps for the clock sampler to see the run
-    args.steps = max(args.steps, 200)
-    sampler = ClockSampler(0)
-    sampler.start()
-    ms = ctx.run_timed(args.steps)
-    clocks = sampler.stop()
-    pa = ctx.get_prims()          # after warmup + steps, for the mixed run's L1
     zones = pr.zones
+    tracer_seed = {}
+
+    def fp64_run(eos):
+        """seeding step, warm-up, timed steps, kernel timings and the host-array run"""
+        ctx = hc.Context(pr)
+        ctx.init_torus()
+        ctx.set_eos(eos)
+        if "ids" not in tracer_seed:
+            tracer_seed["ids"], tracer_seed["X"] = tracers_by_density(np, pr, ctx.get_prims(), args.cool_tracers,
+                                                                      args.seed)
+        ctx.tracers_put(tracer_seed["ids"], tracer_seed["X"])
+        t0 = time.perf_counter()
+        ctx.run(1)                       # the seeding step
+        r = {"seed_s": time.perf_counter() - t0}
+        ctx.run(args.warmup - 1)
+        sampler = ClockSampler(0)
+        sampler.start()
+        r["ms"] = ctx.run_timed(args.steps)
+        r["clocks"] = sampler.stop()
+        r["pa"] = ctx.get_prims()        # after warmup + steps, for the mixed run's L1
+        r["lastT"] = ctx.eos_guess()
+        r["kms"] = ctx.time_kernels(reps=2)
+        import torch
+        pinned = torch.empty(pr.shape + (8,), dtype=torch.float64, pin_memory=True).numpy()
+        pinned[...] = ctx.get_prims()
+        r["ms_e2e"] = ctx.step_ch_host_timed(pinned, args.e2e_steps)
+        r["diag"], r["time"] = ctx.diag(), ctx.time()
+        ctx.close()
+        return r
+
+    if args.cool_tables == "physics":
+        res, how, have = eos_tables.on_demand(fp64_run, xa, ya, consts)
+        seen = res["lastT"][res["lastT"] > 0]
+        gen = dict(how, zone_T_range_K=[float(seen.min()), float(seen.max())] if seen.size else None)
+        gen["nodes_per_s"] = gen["nodes"] / gen["generation_s"] if gen["generation_s"] > 0 else None
+        gen.update(generator_cpu_rate(np, hc, xa, ya, consts["hdfac"], have, args.seed))
+        eos = None
+    else:
+        eos = hc.Eos(xa, ya, val, consts)
+        res = fp64_run(eos)
+    ms, kms, pa = res["ms"], res["kms"], res["pa"]
     value = zones * args.steps / (ms / 1e3)
-    kms = ctx.time_kernels(reps=2)
-    import torch
-    pinned = torch.empty(pr.shape + (8,), dtype=torch.float64, pin_memory=True).numpy()
-    pinned[...] = ctx.get_prims()
-    ms_e2e = ctx.step_ch_host_timed(pinned, args.e2e_steps)
     bytes_host = int(np.prod(pr.shape)) * 8 * 8
     dom = max(("flux", "update"), key=lambda k: kms[k])
     peak, peak_kind = measured_peaks()
     alg = alg_bytes_per_zone(dom, 1) * zones
     achieved = alg / (kms[dom] / 1e3) / 1e9
-    d = ctx.diag()
+    tbytes = len(consts["hdfac"]) * len(xa) * len(ya) * 5 * 8
     line = {"metric": "zone-cycles/s %dx%d GRMHD step_ch with COOL_EOS" % (n, n), "value": value,
             "unit": "zone-cycles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": "FM torus %dx%d (a=0.6, rin=4, rmax=11.8, beta=50), COOL_EOS, %s, "
                                    "%s, %d tracers seeded by rest mass"
-                                   % (n, n, tables, "generator tables (abundance() on the GPU)"
-                                      if args.cool_tables == "physics" else "synthetic generator",
-                                      args.cool_tracers),
+                                   % (n, n, tables, "generator tables (abundance() on the GPU, nodes computed as "
+                                      "the run reads them)" if args.cool_tables == "physics"
+                                      else "synthetic generator", args.cool_tracers),
                        "l2": ("tables (%.0f MB) %s; state per step is small"
-                              % (val.nbytes / 1e6, "fit in L2" if val.nbytes < 126e6 else "exceed L2 (126 MB)"))},
-            "seeding_step_s": seed_s,
-            "e2e": {"value": zones * args.e2e_steps / (ms_e2e / 1e3), "unit": "zone-cycles/s",
+                              % (tbytes / 1e6, "fit in L2" if tbytes < 126e6 else "exceed L2 (126 MB)"))},
+            "seeding_step_s": res["seed_s"],
+            "e2e": {"value": zones * args.e2e_steps / (res["ms_e2e"] / 1e3), "unit": "zone-cycles/s",
                     "h2d_bytes_per_step": bytes_host, "d2h_bytes_per_step": bytes_host,
                     "steps": args.e2e_steps,
                     "path": "harm_run_host: per step upload, step, download, each upload overlapped with the "
@@ -640,32 +638,19 @@ def run_cool(args):
                          "frac": achieved / peak, "traffic": None, "algorithmic_bytes": alg,
                          "peak_source": peak_kind,
                          "note": "the T solves make these kernels FP64-latency bound, not HBM bound"},
-            "kernel_ms": kms, "clocks": clocks, "sim_time": ctx.time(), "fail_code": d["fail_code"]}
-    if args.cool_tables == "physics":
-        lastT = ctx.eos_guess()
-        seen = lastT[lastT > 0]
-        gen["zone_T_range_K"] = [float(seen.min()), float(seen.max())] if seen.size else None
-        gen["floor_rows_read"] = floor_rows_read(np, hc, eos_tables, pr, xa, ya, val, consts, gen, ids, X, pa,
-                                                 (1, args.warmup - 1, args.steps))
+            "kernel_ms": kms, "clocks": res["clocks"], "sim_time": res["time"], "fail_code": res["diag"]["fail_code"]}
+    if gen is not None:
         line["tables"] = gen
-    ctx.close()
-    cm = None
-    if not args.no_mixed and args.cool_tables == "physics" and gen["first_row"] > 0:
+    if not args.no_mixed and eos is None:
         line["mixed"] = {"unavailable": "the FP32 table copies are scaled per plane from the values' range, "
-                                        "which the NaN rows below the generated ones leave undefined"}
+                                        "which the nodes the run never read (NaN) leave undefined"}
     elif not args.no_mixed:
         # the face physics' EOS calls in FP32, the same steps
         cm = hc.Context(pr)
         cm.init_torus()
         cm.set_precision(hc.Context.MIXED)
-        try:
-            cm.set_eos(eos)
-        except hc.HarmError as ex:  # tables whose values float cannot scale
-            line["mixed"] = {"unavailable": str(ex)}
-            cm.close()
-            cm = None
-    if cm is not None:
-        cm.tracers_put(ids, X)
+        cm.set_eos(eos)
+        cm.tracers_put(tracer_seed["ids"], tracer_seed["X"])
         cm.run(args.warmup)
         sampler = ClockSampler(0)
         sampler.start()
@@ -674,14 +659,14 @@ def run_cool(args):
         pb = cm.get_prims()
         act = (slice(None), slice(2, -2), slice(2, -2))
         if args.dump_cool:
-            import numpy as np
             np.savez_compressed(args.dump_cool, fp64=pa, mixed=pb)
         line["mixed"] = {"value": zones * args.steps / (msm / 1e3), "ms_per_step": msm / args.steps,
                          "speedup_vs_fp64": ms / msm, "clocks": clocksm, "kernel_ms": cm.time_kernels(reps=2),
                          "l1_vs_fp64": l1_errors(pa[act], pb[act]), "l1_after_steps": args.warmup + args.steps,
                          "fail_code": cm.diag()["fail_code"]}
         cm.close()
-    eos.close()
+    if eos is not None:
+        eos.close()
     if not args.no_cpu_baseline and args.cool_tables == "reference":
         exe = os.path.join(ROOT, "oracle", "_ref", "ce%d" % n, "refbench")
         if os.path.exists(exe):
@@ -743,9 +728,7 @@ def main():
     ap.add_argument("--cool-tables", choices=("reference", "baseline", "physics"), default="reference",
                     help="reference: cooleos.c's 72x72 tables and units; baseline: 200x200 tables over "
                          "rho 1e4-1e14, T 1e8-1e12 with the torus maximum at 1e11 g/cm^3; physics: the "
-                         "baseline grid filled by the library's abundance() on the GPU")
-    ap.add_argument("--cool-t-floor", type=float, default=2e9,
-                    help="physics tables: generate the rows at or above this T (K) only, NaN below (0: all)")
+                         "baseline grid filled by the library's abundance() on the GPU as the run reads it")
     ap.add_argument("--dump-cool", default=None, help="save the FP64 and mixed COOL_EOS states (npz)")
     ap.add_argument("--adj-n", type=int, default=192, help="adjoint workload: N1 = N2")
     ap.add_argument("--adj-steps", type=int, default=50, help="adjoint workload: steps K")

@@ -164,6 +164,8 @@ _SIGNATURES = {
     "harm_eos_create": (ctypes.c_int, [ctypes.POINTER(EosDesc), _DP, _DP, _DP, _DP,
                                        ctypes.POINTER(ctypes.c_void_p)]),
     "harm_eos_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "harm_eos_track_missing": (ctypes.c_int, [ctypes.c_void_p]),
+    "harm_eos_missing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "harm_eos_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_long,
                                       ctypes.POINTER(ctypes.c_int), _DP, _DP, _DP, _DP]),
     "harm_utoprim_5d_batch": (ctypes.c_int, [ctypes.c_void_p, _DP, _DP, _DP, _DP, ctypes.POINTER(ctypes.c_int), _DP,
@@ -439,6 +441,16 @@ class Eos:
 
     def pressure(self, tab, rho0, u, lastT):
         return self.batch("pressure", tab, rho0, u, lastT)
+
+    def track_missing(self):
+        """Mark the NaN nodes that FP64 reads meet from now on (before set_eos)."""
+        _check(library().harm_eos_track_missing(self.h))
+
+    def missing(self):
+        """The marked nodes: bool [ntab][nx][ny]."""
+        m = np.zeros((self.ntab, len(self.xaxis), len(self.yaxis)), dtype=np.uint8)
+        _check(library().harm_eos_missing(self.h, m.ctypes.data))
+        return m.astype(bool)
 
     def utoprim_5d(self, U, gcov, gcon, gdet, tab, lastT, prim):
         """Utoprim_5d (utoprim_5d.c:179) for n independent zones with tables tab[n]

@@ -213,5 +213,6 @@ struct harm_eos {
   double *axes = nullptr;  // xa[nx] then ya[ny]
   double *vals = nullptr;  // [EOS_ND][ntab][nx][ny]
   float *f32 = nullptr;    // xa32[nx], ya32[ny], e32 and p32 [ntab][nx][ny]
+  unsigned char *miss = nullptr;  // [ntab][nx][ny] NaN nodes read (harm_eos_track_missing)
   int device = 0;
 };

@@ -139,6 +139,7 @@ extern "C" int harm_eos_create(const harm_eos_desc *dsc, const double *xaxis, co
   d.gam = dsc->gam;
   d.hdfac = hdfac ? e->axes + nx + ny : nullptr;
   d.l_unit = dsc->l_unit;
+  d.miss = nullptr;
   *out = e;
   return HARM_OK;
 }
@@ -149,7 +150,27 @@ extern "C" int harm_eos_destroy(harm_eos *e)
   cudaFree(e->axes);
   cudaFree(e->vals);
   cudaFree(e->f32);
+  cudaFree(e->miss);
   delete e;
+  return HARM_OK;
+}
+
+extern "C" int harm_eos_track_missing(harm_eos *e)
+{
+  if (!e) return fail_with(HARM_E_ARG, "null argument");
+  const size_t n = (size_t)e->d.ntab * e->d.nx * e->d.ny;
+  if (!e->miss) CK(cudaMalloc(&e->miss, n));
+  CK(cudaMemset(e->miss, 0, n));
+  e->d.miss = e->miss;
+  return HARM_OK;
+}
+
+extern "C" int harm_eos_missing(const harm_eos *e, unsigned char *out)
+{
+  if (!e || !out) return fail_with(HARM_E_ARG, "null argument");
+  if (!e->miss) return fail_with(HARM_E_ARG, "missing nodes are not tracked (harm_eos_track_missing)");
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(out, e->miss, (size_t)e->d.ntab * e->d.nx * e->d.ny, cudaMemcpyDeviceToHost));
   return HARM_OK;
 }
 

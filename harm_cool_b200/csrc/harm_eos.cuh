@@ -46,7 +46,20 @@ struct EosDev {
   // given) and L_UNIT
   const double *hdfac;
   double l_unit;
+  // [ntab][nx][ny]: set to 1 where an FP64 table read met a NaN node (tables
+  // filled on demand leave the nodes not yet generated NaN); null when not tracked
+  unsigned char *miss;
 };
+
+// record the NaN nodes of a loaded row of n nodes, table tab, rho node x, T nodes from y0
+template <int N>
+__device__ __forceinline__ void eos_note_missing(const EosDev &E, int tab, int x, int y0, const double *ys)
+{
+  if (!E.miss) return;
+#pragma unroll
+  for (int k = 0; k < N; k++)
+    if (ys[k] != ys[k]) E.miss[((long)tab * E.nx + x) * E.ny + y0 + k] = 1;
+}
 
 // the cubic of interval i (akima.c:115-135): its left node, value, slope and
 // the two higher coefficients
@@ -235,6 +248,7 @@ __device__ __noinline__ void eos_value_w(const EosDev &E, const double *__restri
     } else {
 #pragma unroll
       for (int k = 0; k < SY; k++) ys[k] = __ldg(src + k);
+      eos_note_missing<SY>(E, tab, x0 + r, y0, ys);
       akima_slopes<SY>(yw, ys, mm);
       have = true;
       c = akima_cubic<SY>(yw, ys, mm, i);
@@ -248,6 +262,7 @@ __device__ __noinline__ void eos_value_w(const EosDev &E, const double *__restri
       if ((im != i || ip != i) && !have) {
 #pragma unroll
         for (int k = 0; k < SY; k++) ys[k] = __ldg(src + k);
+        eos_note_missing<SY>(E, tab, x0 + r, y0, ys);
         akima_slopes<SY>(yw, ys, mm);
       }
       const double vm = im == i ? c.at(tm) : akima_cubic<SY>(yw, ys, mm, im).at(tm);

@@ -12,7 +12,8 @@ build_tables() lays out the grid and HdFac exactly as the reference does and
 takes the generator as a function; ideal_gas_radiation() is a synthetic
 stand-in (no neutrino physics: placeholder power laws for Qnu and tau).
 physical_tables() fills the same layout from the library's restatement of
-abundance() (harm_nu.cuh), every node computed on the GPU.
+abundance() (harm_nu.cuh), every node computed on the GPU; on_demand() computes
+only the nodes a run reads, as the reference's cache does.
 """
 import math
 
@@ -90,24 +91,72 @@ def build_tables(radii, generator=ideal_gas_radiation, nx=72, ny=72, rho=(1.e2, 
     return xa, ya, val, c
 
 
-def physical_tables(radii, nx=72, ny=72, rho=(1.e2, 1.e15), T=(1.e4, 1.e18), gam=4. / 3., t_floor=None,
-                    device=0):
+def physical_tables(radii, nx=72, ny=72, rho=(1.e2, 1.e15), T=(1.e4, 1.e18), gam=4. / 3., device=0):
     """Tables of the library's abundance() (harm_cool_b200.nu_tables, on the
-    GPU), laid out as build_tables() lays them out: (xaxis, yaxis, values,
-    constants, info).  With t_floor, only the temperature rows at or above it
-    are generated and the rows below hold NaN, so that a run which reads one
-    of them turns NaN instead of using a made-up value; info says how many
-    nodes were generated and how long the device took."""
+    GPU), every node computed, laid out as build_tables() lays them out:
+    (xaxis, yaxis, values, constants, info); info gives the nodes and the
+    device time.  on_demand() computes only the nodes a run reads."""
     from . import nu_tables
     xa, ya = log_axis(nx, *rho), log_axis(ny, *T)
     hd = np.array([hdfac(r) for r in radii])
-    j0 = 0 if t_floor is None else int(np.searchsorted(ya, t_floor))
-    val = np.full((len(radii), nx, ny, 5), np.nan)
-    sub, ms = nu_tables(xa, ya[j0:], hd, device=device)
-    val[:, :, j0:, :] = sub
+    val, ms = nu_tables(xa, ya, hd, device=device)
     c = constants(gam, rho, T)
     c["hdfac"] = hd
-    nodes = len(radii) * nx * (ny - j0)
-    info = {"nodes": nodes, "device_ms": ms, "nodes_per_s": nodes / (ms / 1e3), "first_row": j0,
-            "t_first_row": float(ya[j0]) if j0 < ny else None}
-    return xa, ya, val, c, info
+    nodes = len(radii) * nx * ny
+    return xa, ya, val, c, {"nodes": nodes, "device_ms": ms, "nodes_per_s": nodes / (ms / 1e3)}
+
+
+def fill_nodes(val, xa, ya, hd, mask, device=0):
+    """Compute the nodes where mask is set ([ntab][nx][ny]) with the library's
+    abundance() on the GPU and write them into val, packed as calc_cache_val
+    packs them; returns (nodes, device seconds)."""
+    from . import nu_abundance
+    import time
+    t, i, j = np.nonzero(mask)
+    if len(t) == 0:
+        return 0, 0.0
+    rho = xa[i]
+    t0 = time.perf_counter()
+    a = nu_abundance(rho, ya[j], hd[t], device=device)
+    s = time.perf_counter() - t0
+    val[t, i, j, 0], val[t, i, j, 1], val[t, i, j, 2], val[t, i, j, 3] = a["e"], a["p"], a["qnu"], a["tau"]
+    val[t, i, j, 4] = (a["nee"] - a["nep"]) / (rho / 1.66e15)
+    return len(t), s
+
+
+def on_demand(run, xa, ya, consts, margin=2, max_passes=40, device=0):
+    """A run on tables filled as it reads them, the way the reference's cache
+    fills its nodes.  run(eos) makes a fresh run on the given tables and
+    returns its result.  Every node starts as NaN; after each run the nodes it
+    read as NaN, with margin nodes around them in rho and T, are computed on
+    the GPU, and the run starts again.  The first run that reads no NaN node
+    read only computed nodes, so it is the run on complete tables.  Returns its
+    result, a summary of the passes and the mask of computed nodes."""
+    from . import Eos
+    hd = np.asarray(consts["hdfac"])
+    val = np.full((len(hd), len(xa), len(ya), 5), np.nan)
+    have = np.zeros(val.shape[:3], dtype=bool)
+    passes = []
+    for _ in range(max_passes):
+        eos = Eos(xa, ya, val, consts)
+        eos.track_missing()
+        result = run(eos)
+        miss = eos.missing()
+        eos.close()
+        if not miss.any():
+            info = {"passes": len(passes) + 1, "nodes": int(have.sum()), "nodes_total": int(have.size),
+                    "generation_s": sum(p[1] for p in passes), "per_pass": passes}
+            return result, info, have
+        grow = miss.copy()
+        for _ in range(margin):
+            g = grow.copy()
+            g[:, 1:, :] |= grow[:, :-1, :]
+            g[:, :-1, :] |= grow[:, 1:, :]
+            g[:, :, 1:] |= grow[:, :, :-1]
+            g[:, :, :-1] |= grow[:, :, 1:]
+            grow = g
+        grow &= ~have
+        n, s = fill_nodes(val, xa, ya, hd, grow, device)
+        have |= grow
+        passes.append((n, s))
+    raise RuntimeError("tables still missing nodes after %d passes" % max_passes)

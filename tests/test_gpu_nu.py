@@ -48,3 +48,38 @@ def test_tables_pack_the_nodes_as_calc_cache_val():
         a = hc.nu_abundance(R.ravel(), T.ravel(), hd[t], device=0)
         want = np.stack([a["e"], a["p"], a["qnu"], a["tau"], (a["nee"] - a["nep"]) / (R.ravel() / 1.66e15)], axis=1)
         np.testing.assert_array_equal(val[t].reshape(-1, 5), want)
+
+
+def test_tables_filled_on_demand_give_the_run_on_complete_tables():
+    """A 16x16 COOL_EOS torus (1e11 g/cm^3 scale) on 24x24 generator tables over
+    rho 1e4-1e14, T 1e8-1e12: filling the nodes as the run reads them
+    (eos_tables.on_demand, which marks NaN reads with harm_eos_track_missing)
+    ends in the state, flags and temperature guesses of the same 6 steps on
+    complete tables, bit for bit, having computed fewer nodes."""
+    pr = hc.torus_problem(16, 16, 1, a=0.6, rin=4.0, rmax=11.8, beta=50.0)
+    grid = dict(nx=24, ny=24, rho=(1.e4, 1.e14), T=(1.e8, 1.e12), gam=pr.params.gam)
+    xa, ya, val, consts, info = et.physical_tables(et.zone_radii(pr), **grid)
+    for c in (consts,):
+        c["rho_unit"] = 1.e11
+        c["u_unit"] = c["p_unit"] = 1.e11 * et.CL * et.CL
+
+    def run(eos):
+        ctx = hc.Context(pr)
+        ctx.init_torus()
+        ctx.set_eos(eos)
+        ctx.run(1)
+        ctx.run(5)
+        p, fl = ctx.get_prims(with_flags=True)
+        out = (p, fl, ctx.eos_guess(), ctx.diag()["fail_code"])
+        ctx.close()
+        return out
+
+    E = hc.Eos(xa, ya, val, consts)
+    full = run(E)
+    E.close()
+    lazy, how, have = et.on_demand(run, xa, ya, consts, margin=2)
+    print("on demand:", how["passes"], "passes,", how["nodes"], "of", how["nodes_total"], "nodes")
+    assert how["nodes"] < how["nodes_total"] and how["nodes"] == have.sum()
+    assert full[3] == 0 and lazy[3] == 0
+    for a, b in zip(full[:3], lazy[:3]):
+        assert np.array_equal(a, b)
