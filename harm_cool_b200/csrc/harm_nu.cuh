@@ -21,6 +21,12 @@
 // Units are the reference's: densities in fm^-3, energies and temperatures
 // in MeV, until abundance() converts e and p to erg cm^-3.
 //
+// Code size.  The quadratures are unrolled over the lanes' terms, so each
+// Fermi-integral shape, each Newton solver and each rate routine is kept out
+// of line (HNU_NOINLINE) and exists once in the kernel: inlined at every call
+// site, the kernel outgrew the instruction cache and its warps waited on
+// instruction fetch more than on anything else.
+//
 // One node, one warp.  A node is a nest of Newton solves whose every trial
 // evaluates Fermi integrals or rate integrals by Gauss quadrature.  All 32
 // lanes of a warp run the node's scalar code together, with the same values,
@@ -230,7 +236,7 @@ struct FdTerms {
 // the intervals of set m and hands them to the other lanes: the same function
 // of the same arguments, so the same bits, for a fraction of the instructions.
 template <int M, int NK>
-HNU void fermi(const Rules &R, const double *eta, const double *theta, double *F)
+HNU_NOINLINE void fermi(const Rules &R, const double *eta, const double *theta, double *F)
 {
   FdSpan s[M];
 #if defined(__CUDA_ARCH__)
@@ -362,18 +368,18 @@ struct LeptonN3 {
 };
 
 // degeneracy of neutrons and protons of density n (neta, peta): Newton from -10
-HNU double neta(const Rules &R, double kt, double n)
+HNU_NOINLINE double neta(const Rules &R, double kt, double n)
 {
   return newton1(FermionN3(R, XMN, kt), -10.0, n, newton_tol(n));
 }
-HNU double peta(const Rules &R, double kt, double n)
+HNU_NOINLINE double peta(const Rules &R, double kt, double n)
 {
   return newton1(FermionN3(R, XMP, kt), -10.0, n, newton_tol(n));
 }
 
 // electron degeneracy for the net lepton density n (eeta): Newton from m_e/kt,
 // capped at 0
-HNU double eeta(const Rules &R, double kt, double n)
+HNU_NOINLINE double eeta(const Rules &R, double kt, double n)
 {
   const double e = newton1(LeptonN3(R, kt), 0.510998910 / kt, n, newton_tol(n));
   return e > 0.0 ? 0.0 : e;
@@ -387,7 +393,7 @@ HNU double eeta(const Rules &R, double kt, double n)
 // p = cp (F_3/2 + beta/2 F_5/2), e = 3/2 cp (F_3/2 + beta F_5/2),
 // cp = 2/3 sqrt2/pi^2 (m/hc)^3 m beta^2.5; the positrons count only where the
 // electron density is positive
-HNU void eos_npe(const Rules &R, double kt, double etan, double etap, double etae, double nee, double *e,
+HNU_NOINLINE void eos_npe(const Rules &R, double kt, double etan, double etap, double etae, double nee, double *e,
                  double *p)
 {
   const double mass[4] = {XME, XME, XMP, XMN};
@@ -590,7 +596,8 @@ struct Emission {
   double qe, qo;
 };
 
-HNU Emission emission(const Rules &R, double kt, double nnucl, double nn, double np, double etae, double etaep)
+HNU_NOINLINE Emission emission(const Rules &R, double kt, double nnucl, double nn, double np, double etae,
+                                double etaep)
 {
   double ev1, ev2, evep, even, evn;
   pair(R, kt, etae, &ev1, &ev2);
@@ -639,7 +646,7 @@ struct Nucl {
 
 // the net rate of the six neutron-proton reactions, relative to p e- -> n nu,
 // with neutrino blocking b1 (neutrino, chem_eq.f90:194-253)
-HNU double net_rate(const Rules &R, double b1, double kt, double nn, double np, double etae)
+HNU_NOINLINE double net_rate(const Rules &R, double b1, double kt, double nn, double np, double etae)
 {
   const double etaep = -etae - 2.0 * XME / kt;
   const double t11 = kt * 1.16059e-1;
