@@ -21,11 +21,11 @@
 // Units are the reference's: densities in fm^-3, energies and temperatures
 // in MeV, until abundance() converts e and p to erg cm^-3.
 //
-// Code size.  The quadratures are unrolled over the lanes' terms, so each
-// Fermi-integral shape, each Newton solver and each rate routine is kept out
-// of line (HNU_NOINLINE) and exists once in the kernel: inlined at every call
-// site, the kernel outgrew the instruction cache and its warps waited on
-// instruction fetch more than on anything else.
+// Code size.  Each Fermi-integral shape, each Newton solver and each rate
+// routine is kept out of line (HNU_NOINLINE) and exists once in the kernel,
+// and a lane's loop over its quadrature terms stays rolled: inlined at every
+// call site and unrolled, the kernel outgrew the instruction cache and its
+// warps waited on instruction fetch more than on anything else.
 //
 // One node, one warp.  A node is a nest of Newton solves whose every trial
 // evaluates Fermi integrals or rate integrals by Gauss quadrature.  All 32
@@ -96,24 +96,13 @@ HNU double cube(double x) { return x * x * x; }
 // Sums over the lanes of a warp
 // ---------------------------------------------------------------------------
 
-// out[a] = sum over terms e < NTERM of what term(e, i, acc) adds to acc[a],
-// for NA accumulators.  Lane l takes terms e = l + 32 i, i = 0, 1, ... (i is
-// a constant in each unrolled step of the device loop); the butterfly adds,
-// on lanes l and l ^ d, the same two partial sums, so all lanes end equal.
-template <int NA, int NTERM, class Term>
-HNU void lane_sum(const Term &term, double *out)
+// Combine the lanes' partial sums: out[a] = the sum over lanes of part[a].  The
+// butterfly adds, on lanes l and l ^ d, the same two partial sums, so all lanes
+// end equal.  On the host, part holds the 32 lanes' partials, [32][NA].
+template <int NA>
+HNU void lane_reduce(double *part, double *out)
 {
-  constexpr int NI = (NTERM + 31) / 32;
 #if defined(__CUDA_ARCH__)
-  const int l = threadIdx.x & 31;
-  double part[NA];
-#pragma unroll
-  for (int a = 0; a < NA; a++) part[a] = 0.0;
-#pragma unroll
-  for (int i = 0; i < NI; i++) {
-    const int e = l + 32 * i;
-    if (e < NTERM) term(e, i, part);
-  }
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1)
 #pragma unroll
@@ -121,20 +110,36 @@ HNU void lane_sum(const Term &term, double *out)
 #pragma unroll
   for (int a = 0; a < NA; a++) out[a] = part[a];
 #else
-  double part[32][NA];
-  for (int l = 0; l < 32; l++) {
-    for (int a = 0; a < NA; a++) part[l][a] = 0.0;
-    for (int i = 0; i < NI; i++) {
-      const int e = l + 32 * i;
-      if (e < NTERM) term(e, i, part[l]);
-    }
-  }
   // lane 0's butterfly: at distance d it adds lane d's partial, which holds the
   // same sums over lanes d .. 2d-1 that lanes 0 .. d-1 hold over 0 .. d-1
   for (int d = 16; d > 0; d >>= 1)
     for (int l = 0; l < d; l++)
-      for (int a = 0; a < NA; a++) part[l][a] = part[l][a] + part[l + d][a];
-  for (int a = 0; a < NA; a++) out[a] = part[0][a];
+      for (int a = 0; a < NA; a++) part[l * NA + a] = part[l * NA + a] + part[(l + d) * NA + a];
+  for (int a = 0; a < NA; a++) out[a] = part[a];
+#endif
+}
+
+// out[a] = sum over terms e < NTERM of what term(e, acc) adds to acc[a], for
+// NA accumulators: lane l takes terms l, l + 32, ... in that order.  The
+// loop over a lane's terms stays rolled: one copy of the term's code.
+template <int NA, int NTERM, class Term>
+HNU void lane_sum(const Term &term, double *out)
+{
+#if defined(__CUDA_ARCH__)
+  const int l = threadIdx.x & 31;
+  double part[NA];
+#pragma unroll
+  for (int a = 0; a < NA; a++) part[a] = 0.0;
+#pragma unroll 1
+  for (int e = l; e < NTERM; e += 32) term(e, part);
+  lane_reduce<NA>(part, out);
+#else
+  double part[32 * NA];
+  for (int l = 0; l < 32; l++) {
+    for (int a = 0; a < NA; a++) part[l * NA + a] = 0.0;
+    for (int e = l; e < NTERM; e += 32) term(e, part + l * NA);
+  }
+  lane_reduce<NA>(part, out);
 #endif
 }
 
@@ -180,23 +185,18 @@ HNU FdSpan fd_span(double eta, double theta)
   return s;
 }
 
-// M Fermi integral sets of NK indices each, 80 terms per set laid out in 96
-// slots (three steps of the lanes; slots 80..95 are empty), so that the set of
-// a step is the constant i / 3.  Term r of a set: pieces r / 20 = 0, 1, 2 are
-// the Gauss-Legendre intervals, node (r % 20) / 2 on the side (r % 20) & 1;
-// piece 3 is the Gauss-Laguerre node r % 20.  The integrands are fdfunc1 and,
-// in z = sqrt(x), fdfunc2 (gauss_integral.f90:354-438), with the overflow
-// guard at x - eta = 100.
-template <int M, int NK>
+// The 80 terms of one Fermi integral set of NK indices: terms r / 20 = 0, 1,
+// 2 are the Gauss-Legendre intervals, node (r % 20) / 2 on the side
+// (r % 20) & 1; piece 3 is the Gauss-Laguerre node r % 20.  The integrands
+// are fdfunc1 and, in z = sqrt(x), fdfunc2 (gauss_integral.f90:354-438), with
+// the overflow guard at x - eta = 100.
+template <int NK>
 struct FdTerms {
   const Rules &R;
-  const FdSpan *s;
-  HNU void operator()(int e, int i, double *acc) const
+  const FdSpan &S;
+  HNU void operator()(int r, double *a) const
   {
-    const int m = i / 3, r = e - 96 * m;
-    if (r >= 80) return;
     const int piece = r / 20, q = r % 20;
-    const FdSpan &S = s[m];
     double x, w;
     if (piece < 3) {
       const int j = q >> 1;
@@ -208,7 +208,6 @@ struct FdTerms {
       x = S.s3 + R.g20x[q];
       w = R.g20w[q];
     }
-    double *a = acc + m * NK;
     if (piece == 0) {  // z = x here: 2 z^(2k+1) sqrt(1 + theta z^2 / 2) / (e^(z^2 - eta) + 1)
       const double zsq = x * x;
       const double dxst = sqrt(1.0 + 0.5 * zsq * S.theta);
@@ -261,10 +260,29 @@ HNU_NOINLINE void fermi(const Rules &R, const double *eta, const double *theta, 
     }
     s[m].s3 = __shfl_sync(0xffffffffu, mine.s3, m);
   }
+  // lane l adds terms l, l + 32, l + 64 of each set into that set's partials
+  double part[M * NK];
+#pragma unroll
+  for (int a = 0; a < M * NK; a++) part[a] = 0.0;
+#pragma unroll
+  for (int m = 0; m < M; m++) {
+    const FdTerms<NK> t{R, s[m]};
+#pragma unroll 1
+    for (int r = l; r < 80; r += 32) t(r, part + m * NK);
+  }
+  lane_reduce<M * NK>(part, F);
 #else
   for (int m = 0; m < M; m++) s[m] = fd_span(eta[m], theta[m]);
+  double part[32 * M * NK];
+  for (int l = 0; l < 32; l++) {
+    for (int a = 0; a < M * NK; a++) part[l * M * NK + a] = 0.0;
+    for (int m = 0; m < M; m++) {
+      const FdTerms<NK> t{R, s[m]};
+      for (int r = l; r < 80; r += 32) t(r, part + l * M * NK + m * NK);
+    }
+  }
+  lane_reduce<M * NK>(part, F);
 #endif
-  lane_sum<M * NK, 96 * M>(FdTerms<M, NK>{R, s}, F);
 }
 
 // ---------------------------------------------------------------------------
@@ -535,7 +553,7 @@ template <int POW, bool RK>
 struct RateTerms {
   const Rules &R;
   double kt, etae, etaep, b1, c, h;
-  HNU void operator()(int e, int, double *acc) const
+  HNU void operator()(int e, double *acc) const
   {
     if (e < 40) {
       const int j = e >> 1;
