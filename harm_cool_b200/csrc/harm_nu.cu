@@ -14,9 +14,10 @@
 // one control flow and spreads the terms of every quadrature over them
 // (lane_sum, harm_nu.cuh).
 //
-// Four blocks of four warps per SM (128 registers a thread): the warps' long
-// FP64 latency chains (exp, log, division) need that many to fill the FP64
-// pipe, measured 1.44x faster than three blocks at 168 registers.
+// Six blocks of four warps per SM (80 registers a thread): the warps' long
+// FP64 latency chains (exp, log, division) need that many to keep the FP64
+// pipe busy; measured 1.13x faster than four blocks at 128 registers, which
+// were 1.44x faster than three at 168.
 //
 // Tables are launched one per kernel over several streams without waiting in
 // between, so the blocks of a table still on its slowest nodes share the SMs
@@ -49,7 +50,7 @@ __device__ __forceinline__ void load_rules(Rules &R)
 // for table t, T index j and rho index i; values packed as calc_cache_val
 // packs them (cooleos.c:171-194) at values[t][i][j]: e, p, Qnu, tau,
 // Yee = (n_e- - n_e+) / n_b
-__global__ void __launch_bounds__(128, 4) k_tables(const double *xaxis, int nx, const double *yaxis, int ny,
+__global__ void __launch_bounds__(128, 6) k_tables(const double *xaxis, int nx, const double *yaxis, int ny,
                                                 const double *hdfac, long k0, long n, double *values)
 {
   __shared__ Rules R;
@@ -73,7 +74,7 @@ __global__ void __launch_bounds__(128, 4) k_tables(const double *xaxis, int nx, 
 }
 
 // abundance() at a list of nodes, a warp per node, for checks against the host
-__global__ void __launch_bounds__(128, 4) k_nodes(const double *rho, const double *T, const double *hdfac, long n,
+__global__ void __launch_bounds__(128, 6) k_nodes(const double *rho, const double *T, const double *hdfac, long n,
                                                double *out)
 {
   __shared__ Rules R;
