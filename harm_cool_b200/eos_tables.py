@@ -124,21 +124,25 @@ def fill_nodes(val, xa, ya, hd, mask, device=0):
     return len(t), s
 
 
-def on_demand(run, xa, ya, consts, margin=2, max_passes=40, device=0):
+def on_demand(run, xa, ya, consts, margin=2, max_passes=40, device=0, make_eos=None, fill=None):
     """A run on tables filled as it reads them, the way the reference's cache
     fills its nodes.  run(eos) makes a fresh run on the given tables and
     returns its result.  Every node starts as NaN; after each run the nodes it
     read as NaN, with margin nodes around them in rho and T, are computed on
     the GPU, and the run starts again.  The first run that reads no NaN node
     read only computed nodes, so it is the run on complete tables.  Returns its
-    result, a summary of the passes and the mask of computed nodes."""
-    from . import Eos
+    result, a summary of the passes and the mask of computed nodes.
+    make_eos(xa, ya, val, consts) and fill(val, xa, ya, hd, mask, device) stand
+    in for harm_cool_b200.Eos and fill_nodes (tests drive the loop with them)."""
+    if make_eos is None:
+        from . import Eos as make_eos
+    fill = fill_nodes if fill is None else fill
     hd = np.asarray(consts["hdfac"])
     val = np.full((len(hd), len(xa), len(ya), 5), np.nan)
     have = np.zeros(val.shape[:3], dtype=bool)
     passes = []
     for _ in range(max_passes):
-        eos = Eos(xa, ya, val, consts)
+        eos = make_eos(xa, ya, val, consts)
         eos.track_missing()
         result = run(eos)
         miss = eos.missing()
@@ -156,7 +160,7 @@ def on_demand(run, xa, ya, consts, margin=2, max_passes=40, device=0):
             g[:, :, :-1] |= grow[:, :, 1:]
             grow = g
         grow &= ~have
-        n, s = fill_nodes(val, xa, ya, hd, grow, device)
+        n, s = fill(val, xa, ya, hd, grow, device)
         have |= grow
         passes.append((n, s))
     raise RuntimeError("tables still missing nodes after %d passes" % max_passes)
