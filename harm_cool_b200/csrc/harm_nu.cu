@@ -149,40 +149,45 @@ extern "C" int harm_nu_tables(int device, const double *xaxis, int nx, const dou
   CK(cudaMemcpy(dy, yaxis, ny * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dh, hdfac, ntab * sizeof(double), cudaMemcpyHostToDevice));
   // slices on NS streams, each stream's first slice after e0 and e1 after
-  // every stream's last
-  const int NS = 8;
-  cudaStream_t st[NS];
-  cudaEvent_t e0, e1, done[NS];
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
+  // every stream's last; streams and events released on every return path
+  constexpr int NS = 8;
+  struct Res {
+    cudaStream_t st[NS] = {};
+    cudaEvent_t e0 = nullptr, e1 = nullptr, done[NS] = {};
+    ~Res()
+    {
+      for (int s = 0; s < NS; s++) {
+        if (done[s]) cudaEventDestroy(done[s]);
+        if (st[s]) cudaStreamDestroy(st[s]);
+      }
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+    }
+  } r;
+  CK(cudaEventCreate(&r.e0));
+  CK(cudaEventCreate(&r.e1));
   for (int s = 0; s < NS; s++) {
-    CK(cudaStreamCreateWithFlags(&st[s], cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&done[s], cudaEventDisableTiming));
+    CK(cudaStreamCreateWithFlags(&r.st[s], cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&r.done[s], cudaEventDisableTiming));
   }
   CK(cudaDeviceSynchronize());
-  CK(cudaEventRecord(e0, st[0]));
-  for (int s = 1; s < NS; s++) CK(cudaStreamWaitEvent(st[s], e0, 0));
+  CK(cudaEventRecord(r.e0, r.st[0]));
+  for (int s = 1; s < NS; s++) CK(cudaStreamWaitEvent(r.st[s], r.e0, 0));
   int q = 0;
   for (long k0 = 0; k0 < n; k0 += slice, q = (q + 1) % NS) {
     const long m = (n - k0 < slice) ? n - k0 : slice;
-    nu::k_tables<<<(unsigned)((m + 3) / 4), 128, 0, st[q]>>>(dx, nx, dy, ny, dh, k0, m, dv);
+    nu::k_tables<<<(unsigned)((m + 3) / 4), 128, 0, r.st[q]>>>(dx, nx, dy, ny, dh, k0, m, dv);
     CK(cudaGetLastError());
   }
   for (int s = 1; s < NS; s++) {
-    CK(cudaEventRecord(done[s], st[s]));
-    CK(cudaStreamWaitEvent(st[0], done[s], 0));
+    CK(cudaEventRecord(r.done[s], r.st[s]));
+    CK(cudaStreamWaitEvent(r.st[0], r.done[s], 0));
   }
-  CK(cudaEventRecord(e1, st[0]));
-  CK(cudaEventSynchronize(e1));
+  CK(cudaEventRecord(r.e1, r.st[0]));
+  CK(cudaEventSynchronize(r.e1));
   float t = 0.f;
-  CK(cudaEventElapsedTime(&t, e0, e1));
+  CK(cudaEventElapsedTime(&t, r.e0, r.e1));
   if (ms) *ms = t;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  for (int s = 0; s < NS; s++) {
-    cudaEventDestroy(done[s]);
-    cudaStreamDestroy(st[s]);
-  }
   CK(cudaMemcpy(values, dv, 5 * n * sizeof(double), cudaMemcpyDeviceToHost));
   return HARM_OK;
 }
