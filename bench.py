@@ -534,8 +534,8 @@ def run_cool(args):
     """The COOL_EOS step on the 256x256 torus of the reference's init.c literals
     (a=0.6, rin=4, rmax=11.8, beta=50; cooleos.c's 3 Msun hole and units), FP64,
     with per-radius tables, and 1e5 tracer particles seeded in proportion to the
-    rest mass.  Tables: the reference's 72x72 grid or BASELINE's 200x200 grid
-    from the synthetic ideal-gas-plus-radiation generator of
+    rest mass.  Tables: the reference's 72x72 grid or a 200x200 grid over rho
+    1e4-1e14 g/cm^3 and T 1e8-1e12 K from the synthetic ideal-gas-plus-radiation generator of
     harm_cool_b200.eos_tables, or ("physics") the 200x200 grid from the
     library's abundance() on the GPU, its nodes computed as the run reads them
     (eos_tables.on_demand: the whole run is repeated until it reads no node that
