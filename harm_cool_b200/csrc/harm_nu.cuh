@@ -231,58 +231,63 @@ struct FdTerms {
   }
 };
 
-// F[m NK + k] = F_{k+1/2}(eta[m], theta[m]).  On the device lane m works out
-// the intervals of set m and hands them to the other lanes: the same function
-// of the same arguments, so the same bits, for a fraction of the instructions.
-template <int M, int NK>
-HNU_NOINLINE void fermi(const Rules &R, const double *eta, const double *theta, double *F)
+// F[m NK + k] = F_{k+1/2}(eta[m], theta[m]) for m < M <= 32.  On the device
+// lane m works out the intervals of set m and hands them to the other lanes:
+// the same function of the same arguments, so the same bits, for a fraction
+// of the instructions.  The sets go one after another through one copy of the
+// term code; lane l adds terms l, l + 32, l + 64 of each set into that set's
+// partials, which the butterfly then combines.
+template <int NK>
+HNU_NOINLINE void fermi_sets(const Rules &R, int M, const double *eta, const double *theta, double *F)
 {
-  FdSpan s[M];
 #if defined(__CUDA_ARCH__)
-  static_assert(M <= 32, "one lane per set");
   const int l = threadIdx.x & 31;
   double e = eta[0], th = theta[0];
-#pragma unroll
-  for (int m = 1; m < M; m++)
-    if (l == m) {
-      e = eta[m];
-      th = theta[m];
+#pragma unroll 1
+  for (int q = 1; q < M; q++)
+    if (l == q) {
+      e = eta[q];
+      th = theta[q];
     }
   const FdSpan mine = fd_span(e, th);
-#pragma unroll
+#pragma unroll 1
   for (int m = 0; m < M; m++) {
-    s[m].eta = __shfl_sync(0xffffffffu, mine.eta, m);
-    s[m].theta = __shfl_sync(0xffffffffu, mine.theta, m);
+    FdSpan S;
+    S.eta = __shfl_sync(0xffffffffu, mine.eta, m);
+    S.theta = __shfl_sync(0xffffffffu, mine.theta, m);
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      s[m].c[q] = __shfl_sync(0xffffffffu, mine.c[q], m);
-      s[m].h[q] = __shfl_sync(0xffffffffu, mine.h[q], m);
+      S.c[q] = __shfl_sync(0xffffffffu, mine.c[q], m);
+      S.h[q] = __shfl_sync(0xffffffffu, mine.h[q], m);
     }
-    s[m].s3 = __shfl_sync(0xffffffffu, mine.s3, m);
-  }
-  // lane l adds terms l, l + 32, l + 64 of each set into that set's partials
-  double part[M * NK];
+    S.s3 = __shfl_sync(0xffffffffu, mine.s3, m);
+    double part[NK];
 #pragma unroll
-  for (int a = 0; a < M * NK; a++) part[a] = 0.0;
-#pragma unroll
-  for (int m = 0; m < M; m++) {
-    const FdTerms<NK> t{R, s[m]};
+    for (int a = 0; a < NK; a++) part[a] = 0.0;
+    const FdTerms<NK> t{R, S};
 #pragma unroll 1
-    for (int r = l; r < 80; r += 32) t(r, part + m * NK);
+    for (int r = l; r < 80; r += 32) t(r, part);
+    lane_reduce<NK>(part, F + m * NK);
   }
-  lane_reduce<M * NK>(part, F);
 #else
-  for (int m = 0; m < M; m++) s[m] = fd_span(eta[m], theta[m]);
-  double part[32 * M * NK];
-  for (int l = 0; l < 32; l++) {
-    for (int a = 0; a < M * NK; a++) part[l * M * NK + a] = 0.0;
-    for (int m = 0; m < M; m++) {
-      const FdTerms<NK> t{R, s[m]};
-      for (int r = l; r < 80; r += 32) t(r, part + l * M * NK + m * NK);
+  for (int m = 0; m < M; m++) {
+    const FdSpan S = fd_span(eta[m], theta[m]);
+    const FdTerms<NK> t{R, S};
+    double part[32 * NK];
+    for (int l = 0; l < 32; l++) {
+      for (int a = 0; a < NK; a++) part[l * NK + a] = 0.0;
+      for (int r = l; r < 80; r += 32) t(r, part + l * NK);
     }
+    lane_reduce<NK>(part, F + m * NK);
   }
-  lane_reduce<M * NK>(part, F);
 #endif
+}
+
+template <int M, int NK>
+HNU void fermi(const Rules &R, const double *eta, const double *theta, double *F)
+{
+  static_assert(M <= 32, "one lane per set");
+  fermi_sets<NK>(R, M, eta, theta, F);
 }
 
 // ---------------------------------------------------------------------------
