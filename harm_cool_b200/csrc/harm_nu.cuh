@@ -21,11 +21,12 @@
 // Units are the reference's: densities in fm^-3, energies and temperatures
 // in MeV, until abundance() converts e and p to erg cm^-3.
 //
-// Code size.  Each Fermi-integral shape, each Newton solver and each rate
-// routine is kept out of line (HNU_NOINLINE) and exists once in the kernel,
-// and a lane's loop over its quadrature terms stays rolled: inlined at every
-// call site and unrolled, the kernel outgrew the instruction cache and its
-// warps waited on instruction fetch more than on anything else.
+// Code size.  Each Newton solver and each rate routine is kept out of line
+// (HNU_NOINLINE) and exists once in the kernel, the Fermi integrals have one
+// copy of their term code per number of indices, whatever the number of sets
+// a call asks for, and a lane's loop over its quadrature terms stays rolled:
+// inlined at every call site and unrolled, the kernel outgrew the instruction
+// cache and its warps waited on instruction fetch more than on anything else.
 //
 // One node, one warp.  A node is a nest of Newton solves whose every trial
 // evaluates Fermi integrals or rate integrals by Gauss quadrature.  All 32
