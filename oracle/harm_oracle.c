@@ -519,6 +519,20 @@ static int u2p_wrap(u2p_t *c, u2p_body_fn body, const double *U, const double gc
   return ret;
 }
 
+/* Branch counts for the tests (ora_branch_counts): [0] floors that took the
+   drift-frame branch, [1] inversions that Utoprim_1dvsq2fix1 rescued, [2]
+   inversions that Utoprim_1dfix1 rescued.  They show which paths a test state
+   exercises; the device step takes the same branches bit for bit. */
+long ora_counts[3];
+
+void ora_branch_counts(long *out, int reset)
+{
+  for (int k = 0; k < 3; k++) {
+    out[k] = ora_counts[k];
+    if (reset) ora_counts[k] = 0;
+  }
+}
+
 /* --- Utoprim_1dvsq2fix1 (utoprim_1dvsq2fix1.c) --- */
 
 /* :583-606 */
@@ -857,6 +871,7 @@ static void fixup1zone(ora_state *s, int h, int i, int j, double *pv)
   if (pv[UU] < uuflr) { pv[UU] = uuflr; dofloor = 1; }
   double trans;
   if (dofloor && (trans = 10. * bsq / (pv[RHO] < pv[UU] ? pv[RHO] : pv[UU]) - 1.) > 0.) {
+    ora_counts[0]++;
     if (trans > 1.) trans = 1.;
     double betapar = -q.bcon[0] / ((bsq + SMALL) * q.ucon[0]);
     double betasq = betapar * betapar * bsq;
@@ -1351,7 +1366,11 @@ double ora_advance(ora_state *s, double *pi, double *pb, double Dt, double *pf, 
     if (*fl) {
       double kappa = s->katm[i];
       *fl = (signed char)ora_utoprim_1dvsq2fix1(gam, U, &g.gcov[0][0], &g.gcon[0][0], g.g, pz, kappa);
-      if (*fl) *fl = (signed char)ora_utoprim_1dfix1(gam, U, &g.gcov[0][0], &g.gcon[0][0], g.g, pz, kappa);
+      if (!*fl) ora_counts[1]++;
+      else {
+        *fl = (signed char)ora_utoprim_1dfix1(gam, U, &g.gcov[0][0], &g.gcon[0][0], g.g, pz, kappa);
+        if (!*fl) ora_counts[2]++;
+      }
     }
   }
   if (n3 > 2) return s->prm.defcon * 1. / (1. / ndt1 + 1. / ndt2 + 1. / ndt3);

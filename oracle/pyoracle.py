@@ -138,6 +138,13 @@ class Oracle:
     def step(self):
         return self.lib.ora_step_ch(self.h)
 
+    def branch_counts(self, reset=True):
+        """floors in the drift frame, inversions rescued by Utoprim_1dvsq2fix1 and by
+        Utoprim_1dfix1, since the last reset (process-wide counts)"""
+        out = (ctypes.c_long * 3)()
+        self.lib.ora_branch_counts(out, 1 if reset else 0)
+        return list(out)
+
     def diag_integrals(self):
         """diag()'s sums (mass, angular momentum, energy), divbmax and its zone."""
         out = np.zeros(4)

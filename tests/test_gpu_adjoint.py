@@ -148,13 +148,19 @@ def test_rmax_and_beta_gradients_once_the_torus_reaches_the_inner_boundary():
     assert abs(g[1] - med[1]) <= 2e-2 * abs(med[1]), (g[1], med[1])
 
 
-def test_against_reference_central_differences():
+def test_against_reference_central_differences(oracle_built):
     """dJ/dA_m against central differences taken on the reference's own step
-    (32x32 torus, 10 steps; fixture written by make_golden.py)"""
+    (32x32 torus, 10 steps; fixture written by make_golden.py).  Over these
+    steps Utoprim_1dvsq2fix1 rescues failed inversions (the oracle counts
+    them), so the fall-back adjoint (ift_fallback) is part of what matches."""
     f = np.load(os.path.join(HERE, "golden", "adjoint_t2d.npz"))
     n, m, seed, nsteps = (int(x) for x in f["setup"])
     ctx = _context(n, n)
     modes = ad.Modes(n, n, m=m, seed=seed)
+    ad.initial_state(ctx, modes, 12.0, 100.0, np.zeros(m))
+    drift, rescued1, rescued2 = _oracle_branches(ctx.problem, ctx.get_prims(), ctx.time(), nsteps)
+    print("fall-back rescues %d + %d, drift-frame floors %d" % (rescued1, rescued2, drift))
+    assert rescued1 > 0
     J, g, _ = ad.mass_in_gradient(ctx, modes, 12.0, 100.0, np.zeros(m), nsteps, checkpoint_every=4, rel_step=H)
     assert J == f["J"]
     fd = f["fd"]
@@ -211,12 +217,30 @@ def test_torch_autograd_wrapper():
     np.testing.assert_allclose(g.numpy(), g2, rtol=1e-10, atol=1e-10 * np.abs(g2).max())
 
 
-def test_repaired_zones_against_central_difference():
+def _oracle_branches(pr, p0, t_dt, nsteps):
+    """The oracle's counts of floors in the drift frame and of inversions rescued
+    by Utoprim_1dvsq2fix1 and Utoprim_1dfix1 over nsteps from p0: the device
+    step takes the same branches bit for bit, so these are the paths the
+    adjoint of the same steps goes through."""
+    from helpers import make_oracle
+    o = make_oracle(pr)
+    o.p[...] = p0
+    o.pflag[...] = 0
+    o.set_time(*t_dt)
+    o.branch_counts(reset=True)
+    for _ in range(nsteps):
+        o.step()
+    return o.branch_counts(reset=True)
+
+
+def test_repaired_zones_against_central_difference(oracle_built):
     """A 3x3 block of strong radial field six zones from the inner boundary
     makes the inversion fail in 8 zones of the first step, and fixup_utoprim
     repairs them from their neighbours with corner and last-resort stencils
     (fixup.c:432-538): the adjoint replays those repairs and transposes them,
-    and the failed inversions keep their guess.  (With the block against the
+    and the failed inversions keep their guess.  The same steps floor zones in
+    the drift frame (fixup_vjp) and rescue inversions with Utoprim_1dvsq2fix1
+    (ift_fallback), as the oracle's branch counts show.  (With the block against the
     boundary, J itself is rough at the inversion tolerance, ~1e-10 relative,
     and no central difference resolves a slope there.)"""
     n, i0 = 48, 8
@@ -236,6 +260,9 @@ def test_repaired_zones_against_central_difference():
     v *= np.abs(p0) + 1e-3 * scale * (np.arange(8) >= 2)
     ctx.init_torus()
     ctx.put_prims(p0)
+    drift, rescued1, rescued2 = _oracle_branches(ctx.problem, p0, ctx.time(), 4)
+    print("drift-frame floors %d, fall-back rescues %d + %d" % (drift, rescued1, rescued2))
+    assert drift > 0 and rescued1 > 0  # the floors' drift frame and ift_fallback are exercised
     J, lam, _ = ctx.adjoint_mass_in(4, 3)
     assert J == _mass_in_from(ctx, p0, 4)
     fd = (_mass_in_from(ctx, p0 + H * v, 4) - _mass_in_from(ctx, p0 - H * v, 4)) / (2 * H)
