@@ -598,8 +598,29 @@ def run_cool(args):
         ctx.close()
         return r
 
+    def mixed_run(eos):
+        """the face physics' EOS calls in FP32, the same steps as the FP64 run"""
+        cm = hc.Context(pr)
+        cm.init_torus()
+        cm.set_precision(hc.Context.MIXED)
+        cm.set_eos(eos)
+        cm.tracers_put(tracer_seed["ids"], tracer_seed["X"])
+        cm.run(args.warmup)
+        sampler = ClockSampler(0)
+        sampler.start()
+        r = {"ms": cm.run_timed(args.steps)}
+        r["clocks"] = sampler.stop()
+        r["pb"] = cm.get_prims()
+        r["kms"] = cm.time_kernels(reps=2)
+        r["fail_code"] = cm.diag()["fail_code"]
+        cm.close()
+        return r
+
+    mixed = None
     if args.cool_tables == "physics":
-        res, how, have = eos_tables.on_demand(fp64_run, xa, ya, consts)
+        def both(eos):
+            return fp64_run(eos), (None if args.no_mixed else mixed_run(eos))
+        (res, mixed), how, have = eos_tables.on_demand(both, xa, ya, consts)
         seen = res["lastT"][res["lastT"] > 0]
         gen = dict(how, zone_T_range_K=[float(seen.min()), float(seen.max())] if seen.size else None)
         gen["nodes_per_s"] = gen["nodes"] / gen["generation_s"] if gen["generation_s"] > 0 else None
@@ -641,30 +662,17 @@ def run_cool(args):
             "kernel_ms": kms, "clocks": res["clocks"], "sim_time": res["time"], "fail_code": res["diag"]["fail_code"]}
     if gen is not None:
         line["tables"] = gen
-    if not args.no_mixed and eos is None:
-        line["mixed"] = {"unavailable": "the FP32 table copies are scaled per plane from the values' range, "
-                                        "which the nodes the run never read (NaN) leave undefined"}
-    elif not args.no_mixed:
-        # the face physics' EOS calls in FP32, the same steps
-        cm = hc.Context(pr)
-        cm.init_torus()
-        cm.set_precision(hc.Context.MIXED)
-        cm.set_eos(eos)
-        cm.tracers_put(tracer_seed["ids"], tracer_seed["X"])
-        cm.run(args.warmup)
-        sampler = ClockSampler(0)
-        sampler.start()
-        msm = cm.run_timed(args.steps)
-        clocksm = sampler.stop()
-        pb = cm.get_prims()
+    if not args.no_mixed:
+        if mixed is None:
+            mixed = mixed_run(eos)
+        pb = mixed["pb"]
         act = (slice(None), slice(2, -2), slice(2, -2))
         if args.dump_cool:
             np.savez_compressed(args.dump_cool, fp64=pa, mixed=pb)
-        line["mixed"] = {"value": zones * args.steps / (msm / 1e3), "ms_per_step": msm / args.steps,
-                         "speedup_vs_fp64": ms / msm, "clocks": clocksm, "kernel_ms": cm.time_kernels(reps=2),
+        line["mixed"] = {"value": zones * args.steps / (mixed["ms"] / 1e3), "ms_per_step": mixed["ms"] / args.steps,
+                         "speedup_vs_fp64": ms / mixed["ms"], "clocks": mixed["clocks"], "kernel_ms": mixed["kms"],
                          "l1_vs_fp64": l1_errors(pa[act], pb[act]), "l1_after_steps": args.warmup + args.steps,
-                         "fail_code": cm.diag()["fail_code"]}
-        cm.close()
+                         "fail_code": mixed["fail_code"]}
     if eos is not None:
         eos.close()
     if not args.no_cpu_baseline and args.cool_tables == "reference":

@@ -443,7 +443,7 @@ class Eos:
         return self.batch("pressure", tab, rho0, u, lastT)
 
     def track_missing(self):
-        """Mark the NaN nodes that FP64 reads meet from now on (before set_eos)."""
+        """Mark the NaN nodes that table reads meet from now on (before set_eos)."""
         _check(library().harm_eos_track_missing(self.h))
 
     def missing(self):

@@ -32,12 +32,14 @@ __global__ void k_eos_batch(EosDev E, int what, int f32, long n, const int *__re
 }
 
 // the power of two that centres a plane's magnitudes (log scale) in the float
-// range; 0 when they span more than float can hold
+// range; 0 when they span more than float can hold.  NaN nodes (tables filled
+// on demand, nodes not computed yet) stay NaN in the copy and do not count.
 static double f32_scale(const std::vector<double> &v, size_t off, size_t n)
 {
   double lo = 0., hi = 0.;
   for (size_t k = 0; k < n; k++) {
     double a = fabs(v[off + k]);
+    if (a != a) continue;
     if (!(a < 1e308)) return 0.;
     if (a > 0. && (lo == 0. || a < lo)) lo = a;
     if (a > hi) hi = a;

@@ -46,14 +46,15 @@ struct EosDev {
   // given) and L_UNIT
   const double *hdfac;
   double l_unit;
-  // [ntab][nx][ny]: set to 1 where an FP64 table read met a NaN node (tables
-  // filled on demand leave the nodes not yet generated NaN); null when not tracked
+  // [ntab][nx][ny]: set to 1 where a table read (FP64, or FP32 of the mixed
+  // path) met a NaN node (tables filled on demand leave the nodes not yet
+  // generated NaN); null when not tracked
   unsigned char *miss;
 };
 
 // record the NaN nodes of a loaded row of n nodes, table tab, rho node x, T nodes from y0
-template <int N>
-__device__ __forceinline__ void eos_note_missing(const EosDev &E, int tab, int x, int y0, const double *ys)
+template <int N, class T>
+__device__ __forceinline__ void eos_note_missing(const EosDev &E, int tab, int x, int y0, const T *ys)
 {
   if (!E.miss) return;
 #pragma unroll
@@ -553,8 +554,8 @@ __device__ __forceinline__ void akima_window_f(const float *x, const float *y, f
 }
 
 template <int SX, int SY, bool DER>
-__device__ __noinline__ void eos_value_wf(const EosDev &E, const float *__restrict__ plane, int x0, int y0, float rho,
-                                          float T, float &val, float &der)
+__device__ __noinline__ void eos_value_wf(const EosDev &E, const float *__restrict__ plane, int tab, int x0, int y0,
+                                          float rho, float T, float &val, float &der)
 {
   float xw[SX], yw[SY], row[SX], rowd[SX];
 #pragma unroll
@@ -567,6 +568,7 @@ __device__ __noinline__ void eos_value_wf(const EosDev &E, const float *__restri
     float ys[SY];
 #pragma unroll
     for (int k = 0; k < SY; k++) ys[k] = __ldg(src + k);
+    eos_note_missing<SY>(E, tab, x0 + r, y0, ys);
     float d = 0.f;
     akima_window_f<SY, DER>(yw, ys, T, row[r], d);
     rowd[r] = d;
@@ -585,11 +587,11 @@ __device__ __forceinline__ bool eos_value_f(const EosDev &E, int tab, const floa
   eos_window_f(E.ny, E.ya32, T, y0, sy);
   const float *plane = planes + (long)tab * E.nx * E.ny;
   if (sx == 4) {
-    if (sy == 4) eos_value_wf<4, 4, DER>(E, plane, x0, y0, rho, T, val, der);
-    else eos_value_wf<4, 3, DER>(E, plane, x0, y0, rho, T, val, der);
+    if (sy == 4) eos_value_wf<4, 4, DER>(E, plane, tab, x0, y0, rho, T, val, der);
+    else eos_value_wf<4, 3, DER>(E, plane, tab, x0, y0, rho, T, val, der);
   } else {
-    if (sy == 4) eos_value_wf<3, 4, DER>(E, plane, x0, y0, rho, T, val, der);
-    else eos_value_wf<3, 3, DER>(E, plane, x0, y0, rho, T, val, der);
+    if (sy == 4) eos_value_wf<3, 4, DER>(E, plane, tab, x0, y0, rho, T, val, der);
+    else eos_value_wf<3, 3, DER>(E, plane, tab, x0, y0, rho, T, val, der);
   }
   return true;
 }

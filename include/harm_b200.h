@@ -403,8 +403,8 @@ int harm_eos_destroy(harm_eos *eos);
 /* Tables filled on demand, as the reference's cache fills its nodes as the
    run reads them: nodes not yet computed hold NaN.  After
    harm_eos_track_missing (call it before harm_set_eos: a context keeps the
-   tables' description as it was then), every FP64 table read that meets a NaN
-   node marks that node; harm_eos_missing copies the marks, [ntab][nx][ny] of
+   tables' description as it was then), every table read, FP64 or the mixed
+   path's FP32, that meets a NaN node marks that node; harm_eos_missing copies the marks, [ntab][nx][ny] of
    0 or 1, to the host.  A run that marked nothing read only computed nodes. */
 int harm_eos_track_missing(harm_eos *eos);
 int harm_eos_missing(const harm_eos *eos, unsigned char *marks);
